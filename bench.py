@@ -1,0 +1,393 @@
+"""Benchmark: closest-hit Mrays/s of the BVH hot path on one B200 (or N replicas).
+
+Workload (the reference's soup configuration): LBVH + 3 treelet rounds over a seeded
+1,000,000-triangle FP32 soup; each step traces 4,194,304 closest-hit rays (origins
+uniform in [-0.1,1.1]^3, directions uniform on the sphere, tmax = inf) against the
+resident BVH.  `value` is device-timed closest-hit Mrays/s with rays already in HBM
+(L2 flushed between steps); `e2e` is the same metric through the C ABI's host-buffer
+entry point (pinned host rays in, hits out, copies inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun: every rank builds its own replica and traces its own rays
+(the path has no exchange step), time is the max over ranks.  `--impl reference` times
+the reference algorithm on the host cores (the C oracle port of BVH::build and
+BVH::intersect, all OpenMP threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_TRI = 1_000_000
+N_RAYS = 4 * 1024 * 1024
+ROUNDS = 3
+METRIC = "closest-hit Mrays/s"
+UNIT = "Mrays/s"
+WORKLOAD = "soup_1M_tris_3_treelet_rounds_4M_closest_rays"
+RAY_BYTES = 32
+HIT_BYTES = 16  # prim id 4 + t 4 + uv 8
+NODE_BYTES = 64
+TRI_BYTES = 48
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"cav_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = [r.split(",") for r in self.path.read_text().splitlines() if r.strip()]
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip() == "Active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per launch of the closest-hit kernel from the committed ncu summary, or None."""
+    p = ROOT / "profiles" / "trace_closest_soup1m.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("dram_bytes_per_launch")
+    return None
+
+
+# ------------------------------------------------------------------------- ours
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", local if world > 1 else 0)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    ctx = cav.Context(dev.index)
+    pos, idx = scenes.soup(N_TRI, seed=2)
+    d_pos = torch.from_numpy(pos).to(dev)
+    d_idx = torch.from_numpy(idx).to(dev)
+
+    # build throughput (secondary): full build incl. 3 treelet rounds, device events
+    builds_ms = []
+    stage = None
+    for k in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b = ctx.build(d_pos, d_idx, rounds=ROUNDS)
+        e1.record()
+        torch.cuda.synchronize()
+        if k > 0:
+            builds_ms.append(e0.elapsed_time(e1))
+            stage = b.stage_times()
+        b.free()
+    bvh = ctx.build(d_pos, d_idx, rounds=ROUNDS)
+    torch.cuda.synchronize()
+    ctx.sync_check()
+
+    rays_np = scenes.closest_rays(N_RAYS, seed=20 + rank)
+    rays = torch.from_numpy(rays_np).to(dev)
+    prim = torch.empty(N_RAYS, dtype=torch.int32, device=dev)
+    tt = torch.empty(N_RAYS, dtype=torch.float32, device=dev)
+    uv = torch.empty((N_RAYS, 2), dtype=torch.float32, device=dev)
+    out = (prim, tt, uv)
+    nodes_v, tris_t = bvh.trace_stats(rays)
+    nodes_per_ray = nodes_v / N_RAYS
+    tris_per_ray = tris_t / N_RAYS
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+
+    for _ in range(args.warmup):
+        bvh.trace_closest(rays, out=out)
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(dev.index)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record()
+        bvh.trace_closest(rays, out=out)
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    barrier()
+    wall = time.perf_counter() - t_wall0
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    if world > 1:
+        tm = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        total_ms = float(tm.item())
+    ctx.sync_check()
+    ms_per_step = total_ms / args.steps
+    value = N_RAYS * world / (ms_per_step * 1e-3) / 1e6
+
+    # any-hit (secondary)
+    srays_np, lim_np = scenes.shadow_rays(N_RAYS, seed=21 + rank)
+    srays = torch.from_numpy(srays_np).to(dev)
+    lim = torch.from_numpy(lim_np).to(dev)
+    occ = torch.empty(N_RAYS, dtype=torch.uint8, device=dev)
+    for _ in range(2):
+        bvh.trace_any(srays, lim, out=occ)
+    any_ms = []
+    for k in range(max(3, args.steps // 2)):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        bvh.trace_any(srays, lim, out=occ)
+        b.record()
+        torch.cuda.synchronize()
+        any_ms.append(a.elapsed_time(b))
+
+    # e2e through the host-buffer C-ABI entry point (pinned host memory)
+    h_rays = torch.from_numpy(rays_np).pin_memory()
+    h_prim = torch.empty(N_RAYS, dtype=torch.int32).pin_memory()
+    h_t = torch.empty(N_RAYS, dtype=torch.float32).pin_memory()
+    h_uv = torch.empty((N_RAYS, 2), dtype=torch.float32).pin_memory()
+    hout = (h_prim, h_t, h_uv)
+    for _ in range(2):
+        bvh.trace_closest_host(h_rays, out=hout)
+    barrier()
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for k in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        bvh.trace_closest_host(h_rays, out=hout)
+        b.record()
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        tm = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        e2e_total = float(tm.item())
+    assert np.array_equal(h_prim.numpy(), prim.cpu().numpy()), "host-buffer path disagrees with device path"
+    e2e_value = N_RAYS * world / (e2e_total / args.steps * 1e-3) / 1e6
+
+    peak, peak_kind = measured_peaks()
+    bytes_per_ray = RAY_BYTES + HIT_BYTES + NODE_BYTES * nodes_per_ray + TRI_BYTES * tris_per_ray
+    achieved = bytes_per_ray * N_RAYS / (ms_per_step * 1e-3) / 1e9
+    traffic = committed_traffic()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(bvh, pos, idx, rays_np)
+
+    result = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded triangle soup and rays, generated in-process)",
+        "config": {
+            "workload": WORKLOAD,
+            "triangles": N_TRI,
+            "rays_per_step": N_RAYS,
+            "treelet_rounds": ROUNDS,
+            "trace_mode": "exact (reference order and pruning)",
+            "l2": "flushed between timed steps (256 MiB write); rays 128 MiB > L2",
+            "parallelism": f"replicas x{world}",
+        },
+        "gpu_launches": args.steps,
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * RAY_BYTES,
+                "d2h_bytes_per_step": N_RAYS * HIT_BYTES},
+        "roofline": {
+            "bound": "hbm",
+            "achieved": round(achieved, 1),
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "traffic": traffic,
+            "peak_kind": peak_kind,
+            "algorithmic_bytes_per_ray": round(bytes_per_ray, 2),
+            "nodes_per_ray": round(nodes_per_ray, 3),
+            "tris_per_ray": round(tris_per_ray, 3),
+            "kernel": "k_closest<false,false>",
+        },
+        "clocks": clk,
+        "anyhit_mrays_s": round(N_RAYS / (statistics.mean(any_ms) * 1e-3) / 1e6, 2),
+        "build": {
+            "ms": round(statistics.mean(builds_ms), 3),
+            "builds_per_s": round(1000.0 / statistics.mean(builds_ms), 2),
+            "stage_ms": {k: round(v, 4) for k, v in zip(
+                ["boxes_morton", "sort", "radix_tree", "refit", "treelet_rounds", "layout"], stage)},
+        },
+        "wall_s_timed_region": round(wall, 3),
+    }
+    if cpu is not None:
+        result["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(result))
+    bvh.free()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _oracle_nodes_from_export(nodes):
+    from oracle import pyoracle as po
+
+    o = np.zeros(len(nodes), po.ONODE_DTYPE)
+    for f in ("bmin", "bmax", "left", "right", "is_leaf"):
+        o[f] = nodes[f]
+    o["begin"] = nodes["prim_begin"]
+    o["end"] = nodes["prim_end"]
+    return o
+
+
+def cpu_baseline(bvh, pos, idx, rays_np, target_s: float = 10.0):
+    """The C oracle's BVH::intersect port on all host threads, over the same tree."""
+    from oracle import pyoracle as po
+
+    onodes = _oracle_nodes_from_export(bvh.export_nodes())
+    m = 1 << 16
+    t0 = time.perf_counter()
+    po.trace_closest(onodes, pos, idx, rays_np[:m])
+    dt = time.perf_counter() - t0
+    m2 = int(min(len(rays_np), max(m, m * target_s / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    po.trace_closest(onodes, pos, idx, rays_np[:m2])
+    dt = time.perf_counter() - t0
+    return {"value": round(m2 / dt / 1e6, 3), "unit": UNIT, "cores": po.num_threads(), "kind": "port",
+            "sample": f"{m2} of the step's {len(rays_np)} closest-hit rays on the same tree, "
+                      f"{dt:.1f} s wall, OpenMP"}
+
+
+# -------------------------------------------------------------------- reference
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cavalry_b200 import scenes
+    from oracle import pyoracle as po
+
+    pos, idx = scenes.soup(N_TRI, seed=2)
+    o = po.build(pos, idx, rounds=ROUNDS)
+    rays = scenes.closest_rays(N_RAYS, seed=20)
+    m = 1 << 16
+    t0 = time.perf_counter()
+    po.trace_closest(o["final"], pos, idx, rays[:m])
+    dt = time.perf_counter() - t0
+    sample = int(min(N_RAYS, max(m, m * 4.0 / max(dt, 1e-3))))  # ~4 s per step
+    for _ in range(args.warmup):
+        po.trace_closest(o["final"], pos, idx, rays[:min(sample, 1 << 16)])
+    times = []
+    for k in range(args.steps):
+        off = (k * sample) % max(1, N_RAYS - sample + 1)
+        t0 = time.perf_counter()
+        po.trace_closest(o["final"], pos, idx, rays[off:off + sample])
+        times.append(time.perf_counter() - t0)
+    ms = statistics.mean(times) * 1e3
+    value = sample / (ms * 1e-3) / 1e6
+    cores = po.num_threads()
+    print(json.dumps({
+        "impl": "reference",
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded triangle soup and rays)",
+        "config": {"workload": WORKLOAD, "triangles": N_TRI, "rays_per_step": sample, "treelet_rounds": ROUNDS},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{sample} of {N_RAYS} closest-hit rays per step (C port of BVH::build "
+                                   f"+ BVH::intersect, OpenMP)"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,275 @@
+"""cavalry_b200: B200-native BVH build and ray queries behind Cavalry's BVH interface.
+
+The CUDA library ``libcavalry_b200.so`` (sm_100a, built in-tree by
+``python -m cavalry_b200.build_ext``) exports the C ABI of ``include/cavalry.h``.
+This module binds it with ctypes and adds torch-tensor conveniences; torch only
+supplies device memory and streams.  There is no CPU fallback: importing the
+bindings fails loudly when the library is missing.
+
+Reference interfaces mirrored (paths inside AmesingFlank/Cavalry):
+  ``Context.build``      BVH::build(Triangle*, int, const AABB&, int)   BVH/BVH.cu:317
+  ``Bvh.trace_closest``  BVH::intersect                                 BVH/BVH.h:23-107
+  ``Bvh.trace_any``      BVH::testVisibility                            BVH/BVH.h:109-189
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = ["CavError", "Context", "Bvh", "lib", "REF_NODE_DTYPE", "TRACE_EXACT", "TRACE_CULL_ON_POP"]
+
+_PKG = Path(__file__).resolve().parent
+_LIB_PATH = _PKG / "libcavalry_b200.so"
+
+TRACE_EXACT = 0
+TRACE_CULL_ON_POP = 1
+
+STATUS = {
+    0: "ok",
+    1: "invalid argument",
+    2: "CUDA error",
+    3: "out of device memory",
+    4: "device-side wait timed out",
+    5: "traversal stack overflow",
+    6: "not ready",
+}
+
+# cav_ref_node (include/cavalry.h), the reference's BVHNode fields (BVH/BVHNode.h:8-21)
+REF_NODE_DTYPE = np.dtype(
+    [("bmin", "<f4", (3,)), ("bmax", "<f4", (3,)), ("prim_begin", "<i4"), ("prim_end", "<i4"),
+     ("left", "<i4"), ("right", "<i4"), ("is_leaf", "<i4")]
+)
+assert REF_NODE_DTYPE.itemsize == 44
+
+
+class CavError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded CUDA library.  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise ImportError(
+            f"{_LIB_PATH} is missing; build it with `python -m cavalry_b200.build_ext` "
+            "(there is no CPU fallback)"
+        )
+    L = ctypes.CDLL(str(_LIB_PATH))
+    P, I64, I32, U32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_uint32
+    sig = {
+        "cav_version": ([], ctypes.c_int),
+        "cav_ctx_create": ([ctypes.c_int, ctypes.POINTER(P)], ctypes.c_int),
+        "cav_ctx_destroy": ([P], ctypes.c_int),
+        "cav_last_error": ([P], ctypes.c_char_p),
+        "cav_status_string": ([ctypes.c_int], ctypes.c_char_p),
+        "cav_sync_check": ([P, P], ctypes.c_int),
+        "cav_bvh_build": ([P, P, I64, P, P, I64, P, ctypes.c_int, P, ctypes.POINTER(P)], ctypes.c_int),
+        "cav_bvh_free": ([P], ctypes.c_int),
+        "cav_bvh_num_triangles": ([P], I64),
+        "cav_bvh_depth": ([P, P, P, ctypes.POINTER(I32)], ctypes.c_int),
+        "cav_bvh_export_nodes": ([P, P, P, P], ctypes.c_int),
+        "cav_bvh_export_stages": ([P, P, P, P, P, P], ctypes.c_int),
+        "cav_bvh_stage_times": ([P, P, P], ctypes.c_int),
+        "cav_trace_closest": ([P, P, P, I64, P, P, P, U32, P], ctypes.c_int),
+        "cav_trace_any": ([P, P, P, P, P, I64, P, U32, P], ctypes.c_int),
+        "cav_trace_closest_host": ([P, P, P, I64, P, P, P, U32], ctypes.c_int),
+        "cav_trace_any_host": ([P, P, P, P, P, I64, P, U32], ctypes.c_int),
+        "cav_set_trace_config": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "cav_trace_stats": ([P, P, P, I64, ctypes.c_int, P, P, U32, P, P], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _ptr(t) -> int | None:
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data
+    return t.data_ptr()
+
+
+def _stream_ptr(stream) -> int | None:
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream or None
+
+
+class Context:
+    """A cav_ctx on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        h = ctypes.c_void_p()
+        st = lib().cav_ctx_create(device, ctypes.byref(h))
+        if st != 0:
+            raise CavError(st, "cav_ctx_create")
+        self.handle = h
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            msg = lib().cav_last_error(self.handle) or b""
+            raise CavError(st, f"{what}: {msg.decode(errors='replace')}")
+
+    def close(self):
+        if self.handle:
+            lib().cav_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync_check(self, stream=None):
+        self._check(lib().cav_sync_check(self.handle, _stream_ptr(stream)), "cav_sync_check")
+
+    def set_trace_config(self, block_threads: int = 0, blocks_per_sm: int = 0, batch: int = 0):
+        self._check(lib().cav_set_trace_config(self.handle, block_threads, blocks_per_sm, batch),
+                    "cav_set_trace_config")
+
+    def build(self, positions, indices, mesh_ids=None, scene_bounds=None, rounds: int = 0, stream=None) -> "Bvh":
+        """LBVH + ``rounds`` treelet rounds over device tensors.
+
+        positions: float32 [V,3] CUDA; indices: int32 [T,3] CUDA; mesh_ids: int32 [T] CUDA or None;
+        scene_bounds: 6 floats (min xyz, max xyz) or None (computed on the device).
+        """
+        import torch
+
+        assert positions.is_cuda and positions.dtype == torch.float32 and positions.is_contiguous()
+        assert indices.is_cuda and indices.dtype == torch.int32 and indices.is_contiguous()
+        if mesh_ids is not None:
+            assert mesh_ids.is_cuda and mesh_ids.dtype == torch.int32 and mesh_ids.is_contiguous()
+        nb = None
+        if scene_bounds is not None:
+            nb = np.ascontiguousarray(np.asarray(scene_bounds, dtype=np.float32).reshape(6))
+        h = ctypes.c_void_p()
+        st = lib().cav_bvh_build(
+            self.handle, _ptr(positions), positions.numel() // 3, _ptr(indices), _ptr(mesh_ids),
+            indices.numel() // 3, None if nb is None else nb.ctypes.data, int(rounds), _stream_ptr(stream),
+            ctypes.byref(h),
+        )
+        self._check(st, "cav_bvh_build")
+        return Bvh(self, h, indices.numel() // 3, keep=(positions, indices, mesh_ids))
+
+
+class Bvh:
+    """A built BVH (cav_bvh).  Device memory is released by :meth:`free`."""
+
+    def __init__(self, ctx: Context, handle, n: int, keep=()):
+        self.ctx = ctx
+        self.handle = handle
+        self.n = n
+        self._keep = keep
+
+    def free(self):
+        if self.handle:
+            lib().cav_bvh_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def export_nodes(self, stream=None) -> np.ndarray:
+        out = np.zeros(2 * self.n - 1, dtype=REF_NODE_DTYPE)
+        self.ctx._check(lib().cav_bvh_export_nodes(self.ctx.handle, self.handle, _stream_ptr(stream), out.ctypes.data),
+                        "cav_bvh_export_nodes")
+        return out
+
+    def export_stages(self, stream=None):
+        mu = np.zeros(self.n, np.uint64)
+        ms = np.zeros(self.n, np.uint64)
+        pr = np.zeros(self.n, np.int32)
+        self.ctx._check(lib().cav_bvh_export_stages(self.ctx.handle, self.handle, _stream_ptr(stream), mu.ctypes.data,
+                                                    ms.ctypes.data, pr.ctypes.data), "cav_bvh_export_stages")
+        return mu, ms, pr
+
+    def depth(self, stream=None) -> int:
+        d = ctypes.c_int32()
+        self.ctx._check(lib().cav_bvh_depth(self.ctx.handle, self.handle, _stream_ptr(stream), ctypes.byref(d)),
+                        "cav_bvh_depth")
+        return d.value
+
+    def stage_times(self) -> list[float]:
+        ms = np.zeros(6, np.float32)
+        self.ctx._check(lib().cav_bvh_stage_times(self.ctx.handle, self.handle, ms.ctypes.data), "cav_bvh_stage_times")
+        return [float(x) for x in ms]
+
+    def trace_closest(self, rays, flags: int = TRACE_EXACT, stream=None, out=None):
+        """rays: float32 [n,8] CUDA (o.xyz, tmin, d.xyz, tmax).  Returns (prim int32, t float32, uv float32 [n,2])."""
+        import torch
+
+        assert rays.is_cuda and rays.dtype == torch.float32 and rays.is_contiguous() and rays.shape[-1] == 8
+        n = rays.shape[0]
+        if out is None:
+            prim = torch.empty(n, dtype=torch.int32, device=rays.device)
+            t = torch.empty(n, dtype=torch.float32, device=rays.device)
+            uv = torch.empty((n, 2), dtype=torch.float32, device=rays.device)
+        else:
+            prim, t, uv = out
+        st = lib().cav_trace_closest(self.ctx.handle, self.handle, _ptr(rays), n, _ptr(prim), _ptr(t), _ptr(uv),
+                                     int(flags), _stream_ptr(stream))
+        self.ctx._check(st, "cav_trace_closest")
+        return prim, t, uv
+
+    def trace_any(self, rays, limit=None, excl=None, flags: int = TRACE_EXACT, stream=None, out=None):
+        """Any hit.  limit: float32 [n] or None; excl: int32 [n,2] (source, target mesh) or None."""
+        import torch
+
+        assert rays.is_cuda and rays.dtype == torch.float32 and rays.is_contiguous() and rays.shape[-1] == 8
+        n = rays.shape[0]
+        occ = out if out is not None else torch.empty(n, dtype=torch.uint8, device=rays.device)
+        st = lib().cav_trace_any(self.ctx.handle, self.handle, _ptr(rays), _ptr(limit), _ptr(excl), n, _ptr(occ),
+                                 int(flags), _stream_ptr(stream))
+        self.ctx._check(st, "cav_trace_any")
+        return occ
+
+    def trace_stats(self, rays, any_hit: bool = False, limit=None, excl=None, flags: int = TRACE_EXACT, stream=None):
+        """(node records fetched, triangles tested) totals of one instrumented traversal."""
+        out = np.zeros(2, np.uint64)
+        st = lib().cav_trace_stats(self.ctx.handle, self.handle, _ptr(rays), rays.shape[0], int(any_hit), _ptr(limit),
+                                   _ptr(excl), int(flags), _stream_ptr(stream), out.ctypes.data)
+        self.ctx._check(st, "cav_trace_stats")
+        return int(out[0]), int(out[1])
+
+    def trace_closest_host(self, rays: np.ndarray, flags: int = TRACE_EXACT, out=None):
+        """Host-buffer variant (numpy in and out; pinned torch CPU tensors also accepted)."""
+        n = rays.shape[0]
+        if out is None:
+            prim = np.empty(n, np.int32)
+            t = np.empty(n, np.float32)
+            uv = np.empty((n, 2), np.float32)
+        else:
+            prim, t, uv = out
+        st = lib().cav_trace_closest_host(self.ctx.handle, self.handle, _ptr(rays), n, _ptr(prim), _ptr(t), _ptr(uv),
+                                          int(flags))
+        self.ctx._check(st, "cav_trace_closest_host")
+        return prim, t, uv
+
+    def trace_any_host(self, rays, limit=None, excl=None, flags: int = TRACE_EXACT, out=None):
+        n = rays.shape[0]
+        occ = out if out is not None else np.empty(n, np.uint8)
+        st = lib().cav_trace_any_host(self.ctx.handle, self.handle, _ptr(rays), _ptr(limit), _ptr(excl), n, _ptr(occ),
+                                      int(flags))
+        self.ctx._check(st, "cav_trace_any_host")
+        return occ

@@ -1,0 +1,750 @@
+// LBVH construction for sm_100a: leaf boxes + Morton codes, onesweep radix sort,
+// Karras radix tree, fenced atomic bottom-up refit, and the traversal layout.
+//
+// Semantics follow the reference's BVH::build (BVH/BVH.cu:317-370) so that Morton
+// codes, the sorted order and the node array come out bit-identical; the
+// implementation is this project's own (see the per-kernel comments for the
+// reference lines each one reproduces).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "cav_internal.cuh"
+
+namespace cav {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// Order-preserving float <-> int32 map for atomic min/max of floats (exact; NaN-free input).
+__device__ inline int32_t f2ord(float f) {
+    int32_t i = __float_as_int(f);
+    return i >= 0 ? i : (i ^ 0x7fffffff);
+}
+__host__ __device__ inline float ord2f(int32_t i) {
+    int32_t b = i >= 0 ? i : (i ^ 0x7fffffff);
+#ifdef __CUDA_ARCH__
+    return __int_as_float(b);
+#else
+    float f;
+    memcpy(&f, &b, 4);
+    return f;
+#endif
+}
+
+struct Bounds6 {
+    float v[6];
+};
+
+// Leaf boxes, Core/Triangle.h:242-268 (min/max of the three vertices), written as
+// 6 floats per triangle in triangle order, plus an optional scene-bounds reduction
+// (the union that Core/Scene.cu:131-135 folds on the host).
+__global__ void __launch_bounds__(kThreads) k_leaf_boxes(const float* __restrict__ pos, const int32_t* __restrict__ idx,
+                                                         int64_t n, float* __restrict__ box, int32_t* bounds_ord) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    bool valid = i < n;
+    if (valid) {
+        int32_t a = __ldg(idx + 3 * i), b = __ldg(idx + 3 * i + 1), c = __ldg(idx + 3 * i + 2);
+        float v0[3], v1[3], v2[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v0[k] = __ldg(pos + 3 * (int64_t)a + k);
+            v1[k] = __ldg(pos + 3 * (int64_t)b + k);
+            v2[k] = __ldg(pos + 3 * (int64_t)c + k);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = fminf(v0[k], fminf(v1[k], v2[k]));
+            hi[k] = fmaxf(v0[k], fmaxf(v1[k], v2[k]));
+        }
+        float* o = box + 6 * i;
+        o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
+        o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
+    }
+    if (bounds_ord == nullptr) return;
+    // block reduction of the ordered ints
+    __shared__ int32_t red[6][kThreads / 32];
+    int32_t v[6];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        v[k] = valid ? f2ord(lo[k]) : INT32_MAX;
+        v[3 + k] = valid ? f2ord(hi[k]) : INT32_MIN;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        v[k] = __reduce_min_sync(0xffffffffu, v[k]);
+        v[3 + k] = __reduce_max_sync(0xffffffffu, v[3 + k]);
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) red[k][w] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            int32_t x = l < kThreads / 32 ? red[k][l] : (k < 3 ? INT32_MAX : INT32_MIN);
+            x = k < 3 ? __reduce_min_sync(0xffffffffu, x) : __reduce_max_sync(0xffffffffu, x);
+            if (l == 0) {
+                if (k < 3) atomicMin(bounds_ord + k, x);
+                else atomicMax(bounds_ord + k, x);
+            }
+        }
+    }
+}
+
+__global__ void k_bounds_init(int32_t* bounds_ord) {
+    int k = threadIdx.x;
+    if (k < 6) bounds_ord[k] = k < 3 ? INT32_MAX : INT32_MIN;
+}
+
+__global__ void k_bounds_decode(const int32_t* bounds_ord, float* bounds) {
+    int k = threadIdx.x;
+    if (k < 6) bounds[k] = ord2f(bounds_ord[k]);
+}
+
+// fillLeafMortonCodes + shiftMorton, BVH/BVH.cu:59-92.  Same expression for the
+// normalised centroid (fast-math division, as in the reference) and the same float
+// -> uint64 conversion (negative values become 0).  The 21-bit spread is the
+// standard 3-D Morton interleave (bit k -> bit 3k); the clamp value 1<<20 is the
+// reference's `1 << MORTEN_BITS_PER_DIMENSION - 1`.
+__device__ inline uint64_t spread3(uint64_t x) {
+    if (x >= (1ull << 21)) x = 1ull << 20;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+
+__global__ void __launch_bounds__(kThreads) k_morton(const float* __restrict__ box, int64_t n, const float* dev_bounds,
+                                                     Bounds6 host_bounds, int use_dev, uint64_t* __restrict__ codes,
+                                                     uint64_t* __restrict__ codes_copy, uint32_t* __restrict__ vals) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f3 slo, shi;
+    if (use_dev) {
+        slo = mk(dev_bounds[0], dev_bounds[1], dev_bounds[2]);
+        shi = mk(dev_bounds[3], dev_bounds[4], dev_bounds[5]);
+    } else {
+        slo = mk(host_bounds.v[0], host_bounds.v[1], host_bounds.v[2]);
+        shi = mk(host_bounds.v[3], host_bounds.v[4], host_bounds.v[5]);
+    }
+    const float* b = box + 6 * i;
+    f3 lo = mk(b[0], b[1], b[2]), hi = mk(b[3], b[4], b[5]);
+    f3 centroid = ((lo + hi) * 0.5f - (slo + shi) * 0.5f) / (shi - slo);
+    uint64_t factor = (uint64_t)(1L << 21);
+    uint64_t x = centroid.x * factor;
+    uint64_t y = centroid.y * factor;
+    uint64_t z = centroid.z * factor;
+    uint64_t code = (spread3(x) << 2) | (spread3(y) << 1) | spread3(z);
+    codes[i] = code;
+    codes_copy[i] = code;
+    vals[i] = (uint32_t)i;
+}
+
+// ------------------------------------------------------------ onesweep sort
+// Stable LSD radix sort of 64-bit keys with 32-bit payloads, 8 passes of 8 bits.
+// One histogram kernel counts every digit of every pass in a single read; each pass is
+// then one kernel: a tile ranks its keys stably (warp match + per-warp counters), and
+// finds its global offsets by decoupled look-back over the previous tiles' published
+// counts (Merrill & Garland's single-pass prefix scan, as used by Onesweep).
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagInc = 2u << 30;
+constexpr uint32_t kCountMask = (1u << 30) - 1;
+
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint64_t* __restrict__ keys, int64_t n,
+                                                            uint32_t* __restrict__ hist /*8x256*/) {
+    __shared__ uint32_t h[8][256];
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+    __syncthreads();
+    int lane = threadIdx.x & 31;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i - lane < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        bool valid = i < n;
+        uint64_t k = valid ? keys[i] : 0;
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            uint32_t d = (uint32_t)(k >> (8 * p)) & 255u;
+            uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) {
+        uint32_t c = (&h[0][0])[i];
+        if (c) atomicAdd(hist + i, c);
+    }
+}
+
+__device__ inline uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct SortSmem {
+    uint64_t keys[kSortTile];
+    uint32_t vals[kSortTile];
+    uint32_t warp_hist[kSortWarps][256];
+    uint32_t tile_start[256];
+    uint32_t gbase[256];
+    uint32_t scan_tmp[256];
+    int tile;
+};
+
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __restrict__ kin,
+                                                           const uint32_t* __restrict__ vin,
+                                                           uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                           int64_t n, int shift, const uint32_t* __restrict__ hist,
+                                                           uint32_t* status /*tiles x 256*/, uint32_t* tile_counter,
+                                                           int* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) S.tile = (int)atomicAdd(tile_counter, 1u);
+    for (int i = tid; i < kSortWarps * 256; i += kSortThreads) (&S.warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    const int tile = S.tile;
+    const int64_t base = (int64_t)tile * kSortTile;
+
+    uint64_t key[kSortItems];
+    uint32_t val[kSortItems];
+    uint32_t rank[kSortItems];
+    const int64_t wbase = base + (int64_t)warp * 32 * kSortItems;
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        int64_t g = wbase + k * 32 + lane;
+        bool valid = g < n;
+        key[k] = valid ? kin[g] : ~0ull;
+        val[k] = valid ? vin[g] : 0u;
+    }
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        int64_t g = wbase + k * 32 + lane;
+        bool valid = g < n;
+        uint32_t d = (uint32_t)(key[k] >> shift) & 255u;
+        uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u);
+        int leader = __ffs(peers) - 1;
+        uint32_t old = 0;
+        if (valid && lane == leader) {
+            old = S.warp_hist[warp][d];
+            S.warp_hist[warp][d] = old + (uint32_t)__popc(peers);
+        }
+        old = __shfl_sync(0xffffffffu, old, leader);
+        rank[k] = old + (uint32_t)__popc(peers & lt);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive offsets across warps and the tile total
+    const int digit = tid;  // kSortThreads == 256
+    uint32_t total = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+        uint32_t c = S.warp_hist[w][digit];
+        S.warp_hist[w][digit] = total;
+        total += c;
+    }
+    // publish this tile's aggregate, then look back for the exclusive prefix
+    uint32_t* my_status = status + (size_t)tile * 256 + digit;
+    if (tile == 0) {
+        atomicExch(my_status, kFlagInc | total);
+    } else {
+        atomicExch(my_status, kFlagAgg | total);
+    }
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int p = tile - 1;
+        uint64_t t0 = 0;
+        while (p >= 0) {
+            uint32_t s = *((volatile uint32_t*)(status + (size_t)p * 256 + digit));
+            if ((s & ~kCountMask) == 0) {
+                if (t0 == 0) t0 = globaltimer_ns();
+                else if (globaltimer_ns() - t0 > 2000000000ull) {  // 2 s: give up, flag the error
+                    atomicExch(err, 1);
+                    break;
+                }
+                continue;
+            }
+            t0 = 0;
+            excl += s & kCountMask;
+            if ((s & ~kCountMask) == kFlagInc) break;
+            --p;
+        }
+        __threadfence();
+        atomicExch(my_status, kFlagInc | (excl + total));
+    }
+    // exclusive scan of tile totals over digits (Hillis-Steele in shared memory)
+    S.scan_tmp[digit] = total;
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1) {
+        uint32_t v = digit >= off ? S.scan_tmp[digit - off] : 0;
+        __syncthreads();
+        S.scan_tmp[digit] += v;
+        __syncthreads();
+    }
+    uint32_t tstart = S.scan_tmp[digit] - total;
+    S.tile_start[digit] = tstart;
+    // global exclusive offset of this digit over all keys
+    uint32_t h = hist[digit];
+    __syncthreads();
+    S.scan_tmp[digit] = h;
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1) {
+        uint32_t v = digit >= off ? S.scan_tmp[digit - off] : 0;
+        __syncthreads();
+        S.scan_tmp[digit] += v;
+        __syncthreads();
+    }
+    S.gbase[digit] = (S.scan_tmp[digit] - h) + excl;
+    __syncthreads();
+    // scatter into shared memory in tile-sorted order
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        int64_t g = wbase + k * 32 + lane;
+        if (g < n) {
+            uint32_t d = (uint32_t)(key[k] >> shift) & 255u;
+            uint32_t pos = S.tile_start[d] + S.warp_hist[warp][d] + rank[k];
+            if (pos < (uint32_t)kSortTile) {
+                S.keys[pos] = key[k];
+                S.vals[pos] = val[k];
+            } else {
+                atomicExch(err, 3);
+            }
+        }
+    }
+    __syncthreads();
+    int64_t tile_n = n - base < kSortTile ? n - base : kSortTile;
+    for (int i = tid; i < tile_n; i += kSortThreads) {
+        uint64_t k = S.keys[i];
+        uint32_t d = (uint32_t)(k >> shift) & 255u;
+        uint32_t o = S.gbase[d] + (uint32_t)i - S.tile_start[d];
+        if (o < (uint64_t)n) {
+            kout[o] = k;
+            vout[o] = S.vals[i];
+        } else {
+            atomicExch(err, 3);
+        }
+    }
+}
+
+// ------------------------------------------------------------- radix tree
+// commonPrefixLength, BVH/BVH.cu:101-120, via count-leading-zeros: codes use bits 0..62,
+// so differing codes give clz(a^b)-1 equal leading bits; equal codes fall back to
+// 63 + the equal leading bits of the 32-bit indices (95 when i == j).
+__device__ inline int cpl(const uint64_t* __restrict__ m, uint64_t mi, uint32_t i, uint32_t j) {
+    uint64_t mj = __ldg(m + j);
+    if (mi != mj) return __clzll((long long)(mi ^ mj)) - 1;
+    return 63 + __clz((int)(i ^ j));
+}
+
+// buildRadixTree, BVH/BVH.cu:122-215: the same search loops (direction, doubling
+// bound, binary search for the other end, the i == 0 override, the float-ceil split
+// search, and the `rightChild == leavesCount - 1` leaf clause), writing straight into
+// the merged node layout of mergeNodesArray (BVH/BVH.cu:273-302): internal i at i,
+// leaf j at N-1+j.
+__global__ void __launch_bounds__(kThreads) k_radix_tree(const uint64_t* __restrict__ m, int32_t N,
+                                                         BNode* __restrict__ nodes, int* err) {
+    int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N - 1) return;
+    const uint64_t mi = __ldg(m + i);
+    int d = 1;
+    if (i > 0) d = (cpl(m, mi, i, i + 1) - cpl(m, mi, i, i - 1)) >= 0 ? 1 : -1;
+    int minCPL = 0;
+    if (i > 0) minCPL = cpl(m, mi, i, (uint32_t)(i - d));
+    uint32_t maxLength = 2;
+    for (;;) {
+        int64_t jj = (int64_t)i + (int64_t)maxLength * d;
+        if (!(jj >= 0 && jj < N)) break;
+        if (!(cpl(m, mi, i, (uint32_t)jj) > minCPL)) break;
+        maxLength *= 2;
+    }
+    uint32_t length = 0;
+    for (int power = 1;; ++power) {
+        uint32_t t = maxLength >> power;
+        if (t == 0) break;
+        int32_t j = (int32_t)((uint32_t)i + (length + t) * (uint32_t)d);
+        if (j >= 0 && j < N && cpl(m, mi, i, j) > minCPL) length += t;
+    }
+    int32_t j = (int32_t)((uint32_t)i + length * (uint32_t)d);
+    if (i == 0) j = N - 1;
+    int prefix = cpl(m, mi, i, j);
+    uint32_t dist = 0;
+    for (int power = 1;; ++power) {
+        uint32_t t = ceil((float)length / ((float)(1 << power)));
+        int32_t jj = (int32_t)((uint32_t)i + (dist + t) * (uint32_t)d);
+        if (jj >= 0 && jj < N && cpl(m, mi, i, jj) > prefix) dist += t;
+        if (t <= 1) break;
+    }
+    int32_t split = (int32_t)((uint32_t)i + dist * (uint32_t)d) + min(0, d);
+    int32_t lc = split, rc = split + 1;
+    if (lc < 0 || rc > N - 1) {
+        atomicExch(err, 4);
+        return;
+    }
+    bool lleaf = min(i, j) == lc;
+    bool rleaf = (max(i, j) == rc) || (rc == N - 1);
+    int32_t lid = lleaf ? N - 1 + lc : lc;
+    int32_t rid = rleaf ? N - 1 + rc : rc;
+    BNode& nd = nodes[i];
+    nd.left = lid;
+    nd.right = rid;
+    nd.prim = -1;
+    nd.is_leaf = 0;
+    nodes[lid].parent = i;
+    nodes[rid].parent = i;
+    if (i == 0) nd.parent = 0;  // GpuArray zero fill: the root's parent field reads 0
+}
+
+// Leaf records (fillLeafBoundingBoxes + copyLeafNode, BVH/BVH.cu:46-56, 261-271) and
+// computeBounds (BVH/BVH.cu:217-259): the second arrival at a node unions its
+// children.  Child records written by other threads are read through L2 (ld.cg)
+// after an acquire fence; writes are published with a release fence before the
+// arrival counter is bumped (the reference has no fence here).
+__global__ void __launch_bounds__(kThreads) k_refit(const float* __restrict__ box, const uint32_t* __restrict__ perm,
+                                                    int32_t N, BNode* nodes, uint32_t* visited, int* err) {
+    int32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    uint32_t t = perm[j];
+    const float* b = box + 6 * (size_t)t;
+    f3 lo = mk(b[0], b[1], b[2]), hi = mk(b[3], b[4], b[5]);
+    BNode* L = nodes + (N - 1 + j);
+    L->lo_x = lo.x; L->lo_y = lo.y; L->lo_z = lo.z;
+    L->hi_x = hi.x; L->hi_y = hi.y; L->hi_z = hi.z;
+    L->left = 0;
+    L->right = 0;
+    L->prim = (int32_t)t;
+    L->is_leaf = 1;
+    float area = surface_area(lo, hi);
+    L->area = area;
+    L->cost = leaf_cost(area, 1);
+    __threadfence();
+    int32_t curr = L->parent;
+    for (;;) {
+        if (curr < 0 || curr >= N - 1) {
+            atomicExch(err, 5);
+            return;
+        }
+        uint32_t old = atomicAdd(visited + curr, 1u);
+        if (old != 1) return;  // first arrival (or a malformed third) stops here
+        __threadfence();
+        BNode* nd = nodes + curr;
+        int32_t l = __ldcg(&nd->left), r = __ldcg(&nd->right);
+        if (l < 0 || r < 0 || l >= 2 * N - 1 || r >= 2 * N - 1) {
+            atomicExch(err, 5);
+            return;
+        }
+        const BNode* A = nodes + l;
+        const BNode* B = nodes + r;
+        f3 alo = mk(__ldcg(&A->lo_x), __ldcg(&A->lo_y), __ldcg(&A->lo_z));
+        f3 ahi = mk(__ldcg(&A->hi_x), __ldcg(&A->hi_y), __ldcg(&A->hi_z));
+        f3 blo = mk(__ldcg(&B->lo_x), __ldcg(&B->lo_y), __ldcg(&B->lo_z));
+        f3 bhi = mk(__ldcg(&B->hi_x), __ldcg(&B->hi_y), __ldcg(&B->hi_z));
+        float cl = __ldcg(&A->cost), cr = __ldcg(&B->cost);
+        f3 nlo = vmin3(alo, blo), nhi = vmax3(ahi, bhi);
+        nd->lo_x = nlo.x; nd->lo_y = nlo.y; nd->lo_z = nlo.z;
+        nd->hi_x = nhi.x; nd->hi_y = nhi.y; nd->hi_z = nhi.z;
+        float a = surface_area(nlo, nhi);
+        nd->area = a;
+        nd->cost = internal_cost(a, cl, cr);
+        __threadfence();
+        if (curr == 0) return;
+        curr = __ldcg(&nd->parent);
+    }
+}
+
+// ---------------------------------------------------------------- layout
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ inline uint32_t block_excl_scan(uint32_t v, uint32_t* wsum, uint32_t* total) {
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t s = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        wsum[lane] = s;
+    }
+    __syncthreads();
+    uint32_t before = w > 0 ? wsum[w - 1] : 0;
+    if (total) *total = wsum[(blockDim.x >> 5) - 1];
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_count_internal(const BNode* __restrict__ nodes, int64_t count,
+                                                                 uint32_t* __restrict__ block_counts) {
+    __shared__ uint32_t wsum[32];
+    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < count && !nodes[base + k].is_leaf) ++c;
+    uint32_t total;
+    block_excl_scan(c, wsum, &total);
+    if (threadIdx.x == 0) block_counts[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_blocks(uint32_t* counts, int nblocks) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int b0 = 0; b0 < nblocks; b0 += kScanThreads) {
+        int b = b0 + threadIdx.x;
+        uint32_t v = b < nblocks ? counts[b] : 0;
+        uint32_t total;
+        uint32_t e = block_excl_scan(v, wsum, &total);
+        if (b < nblocks) counts[b] = carry + e;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_compact_index(const BNode* __restrict__ nodes, int64_t count,
+                                                                const uint32_t* __restrict__ block_offsets,
+                                                                int32_t* __restrict__ compact) {
+    __shared__ uint32_t wsum[32];
+    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    bool in[kScanItems];
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        in[k] = base + k < count && !nodes[base + k].is_leaf;
+        c += in[k];
+    }
+    uint32_t e = block_excl_scan(c, wsum, nullptr) + block_offsets[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < count) compact[base + k] = in[k] ? (int32_t)(e++) : -1;
+    }
+}
+
+// Triangle records in sorted (Morton) order; slot_of[t] = sorted position of triangle t.
+__global__ void __launch_bounds__(kThreads) k_tri_layout(const float* __restrict__ pos, const int32_t* __restrict__ idx,
+                                                         const int32_t* __restrict__ mesh, const uint32_t* __restrict__ perm,
+                                                         int64_t n, TriRec* __restrict__ tris, int32_t* __restrict__ slot_of) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    uint32_t t = perm[j];
+    int32_t a = idx[3 * (size_t)t], b = idx[3 * (size_t)t + 1], c = idx[3 * (size_t)t + 2];
+    f3 v0 = mk(pos[3 * (size_t)a], pos[3 * (size_t)a + 1], pos[3 * (size_t)a + 2]);
+    f3 v1 = mk(pos[3 * (size_t)b], pos[3 * (size_t)b + 1], pos[3 * (size_t)b + 2]);
+    f3 v2 = mk(pos[3 * (size_t)c], pos[3 * (size_t)c + 1], pos[3 * (size_t)c + 2]);
+    f3 e1 = v1 - v0, e2 = v2 - v0;
+    int32_t m = mesh ? mesh[t] : 0;
+    TriRec r;
+    r.v0 = make_float4(v0.x, v0.y, v0.z, __int_as_float((int)t));
+    r.e1 = make_float4(e1.x, e1.y, e1.z, __int_as_float(m));
+    r.e2 = make_float4(e2.x, e2.y, e2.z, 0.f);
+    tris[j] = r;
+    slot_of[t] = (int32_t)j;
+}
+
+__global__ void __launch_bounds__(kThreads) k_tnode_layout(const BNode* __restrict__ nodes, int64_t count,
+                                                           const int32_t* __restrict__ compact,
+                                                           const int32_t* __restrict__ slot_of,
+                                                           TNode* __restrict__ out, float* __restrict__ root_box) {
+    int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= count) return;
+    const BNode& nd = nodes[x];
+    if (x == 0) {
+        root_box[0] = nd.lo_x; root_box[1] = nd.lo_y; root_box[2] = nd.lo_z;
+        root_box[3] = nd.hi_x; root_box[4] = nd.hi_y; root_box[5] = nd.hi_z;
+    }
+    if (nd.is_leaf) return;
+    const BNode& A = nodes[nd.left];
+    const BNode& B = nodes[nd.right];
+    int32_t lref = A.is_leaf ? ~slot_of[A.prim] : compact[nd.left];
+    int32_t rref = B.is_leaf ? ~slot_of[B.prim] : compact[nd.right];
+    int32_t c = compact[x];
+    if (c < 0 || c >= count / 2) return;  // N-1 internal slots
+    TNode t;
+    t.a = make_float4(A.lo_x, A.lo_y, A.lo_z, A.hi_x);
+    t.b = make_float4(A.hi_y, A.hi_z, B.lo_x, B.lo_y);
+    t.c = make_float4(B.lo_z, B.hi_x, B.hi_y, B.hi_z);
+    t.d = make_int4(lref, rref, 0, 0);
+    out[c] = t;
+}
+
+__global__ void k_merge_error(const int* src, int* dst) {
+    if (threadIdx.x == 0 && src[0] != 0) atomicExch(dst, src[0]);
+}
+
+template <typename T>
+T* carve(unsigned char*& p, size_t count) {
+    size_t off = ((uintptr_t)p + 255) & ~(uintptr_t)255;
+    T* r = reinterpret_cast<T*>(off);
+    p = reinterpret_cast<unsigned char*>(off + sizeof(T) * count);
+    return r;
+}
+
+}  // namespace
+
+cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int32_t* indices,
+                     const int32_t* mesh_ids, int64_t n, const float* bounds, int rounds, cudaStream_t s,
+                     cav_bvh** out) {
+    if (!positions || !indices || !out || nv < 1 || n < 2 || n >= (1ll << 30) || rounds < 0)
+        return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build: invalid argument");
+    const int64_t count = 2 * n - 1;
+    cav_bvh* bvh = new cav_bvh();
+    bvh->n = n;
+    bvh->device = ctx->device;
+
+    // persistent arena
+    size_t need = 0;
+    need += sizeof(BNode) * count + 256;
+    need += 2 * (sizeof(uint64_t) * n + 256);
+    need += sizeof(int32_t) * n + 256;
+    need += sizeof(TNode) * (n - 1) + 256;
+    need += sizeof(TriRec) * n + 256;
+    need += 64 + 256;
+    if (cudaMalloc(&bvh->arena, need) != cudaSuccess) {
+        cudaGetLastError();
+        delete bvh;
+        return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "cav_bvh_build: device allocation failed");
+    }
+    unsigned char* p = (unsigned char*)bvh->arena;
+    bvh->nodes = carve<BNode>(p, count);
+    bvh->codes_unsorted = carve<uint64_t>(p, n);
+    bvh->codes_sorted = carve<uint64_t>(p, n);
+    bvh->perm = carve<int32_t>(p, n);
+    bvh->tnodes = carve<TNode>(p, n - 1);
+    bvh->tris = carve<TriRec>(p, n);
+    bvh->d_root_box = carve<float>(p, 8);
+    bvh->d_depth = carve<int32_t>(p, 8);
+
+    // scratch (stream ordered)
+    const int tiles = div_up(n, kSortTile);
+    size_t scratch = 0;
+    scratch += sizeof(float) * 6 * n + 256;           // leaf boxes
+    scratch += sizeof(uint64_t) * n + 256;            // sort ping-pong keys
+    scratch += sizeof(uint32_t) * n + 256;            // sort vals A
+    scratch += sizeof(uint32_t) * n + 256;            // sort vals B
+    scratch += sizeof(uint32_t) * 8 * 256 + 256;      // histograms
+    scratch += sizeof(uint32_t) * 8 * (size_t)tiles * 256 + 256;  // look-back status
+    scratch += sizeof(uint32_t) * 16 + 256;           // tile counters + bounds ords
+    scratch += sizeof(int32_t) * 8 + 256;             // error flag
+    scratch += sizeof(float) * 8 + 256;               // device bounds
+    scratch += sizeof(uint32_t) * count + 256;        // visited
+    scratch += sizeof(int32_t) * n + 256;             // leaf list
+    scratch += sizeof(int32_t) * count + 256;         // compact index
+    scratch += sizeof(int32_t) * n + 256;             // slot_of
+    scratch += sizeof(uint32_t) * (div_up(count, kScanTile) + 1) + 256;
+    void* sbase = nullptr;
+    cudaError_t e = cudaMallocAsync(&sbase, scratch, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(bvh->arena);
+        delete bvh;
+        return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "cav_bvh_build: scratch allocation failed");
+    }
+    unsigned char* q = (unsigned char*)sbase;
+    float* leafbox = carve<float>(q, 6 * n);
+    uint64_t* keys_b = carve<uint64_t>(q, n);
+    uint32_t* vals_a = carve<uint32_t>(q, n);
+    uint32_t* vals_b = carve<uint32_t>(q, n);
+    uint32_t* hist = carve<uint32_t>(q, 8 * 256);
+    uint32_t* status = carve<uint32_t>(q, 8 * (size_t)tiles * 256);
+    uint32_t* counters = carve<uint32_t>(q, 16);  // [0..7] tile counters, [8..13] bounds ords
+    int32_t* err = carve<int32_t>(q, 8);
+    float* dbounds = carve<float>(q, 8);
+    uint32_t* visited = carve<uint32_t>(q, count);
+    int32_t* leaf_list = carve<int32_t>(q, n);
+    int32_t* compact = carve<int32_t>(q, count);
+    int32_t* slot_of = carve<int32_t>(q, n);
+    uint32_t* blk = carve<uint32_t>(q, div_up(count, kScanTile) + 1);
+
+    for (int k = 0; k < 7; ++k) cudaEventCreate(&bvh->ev[k]);
+    bvh->timed = true;
+
+    CAV_CUDA(ctx, cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(status, 0, sizeof(uint32_t) * 8 * (size_t)tiles * 256, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 16, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(err, 0, sizeof(int32_t) * 8, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(bvh->nodes, 0, sizeof(BNode) * count, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(visited, 0, sizeof(uint32_t) * (n - 1), s));
+
+    cudaEventRecord(bvh->ev[0], s);
+    int32_t* bounds_ord = (int32_t*)(counters + 8);
+    const int gb = div_up(n, kThreads);
+    Bounds6 hb{};
+    int use_dev = bounds ? 0 : 1;
+    if (bounds) {
+        for (int k = 0; k < 6; ++k) hb.v[k] = bounds[k];
+        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, leafbox, nullptr);
+    } else {
+        k_bounds_init<<<1, 32, 0, s>>>(bounds_ord);
+        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, leafbox, bounds_ord);
+        k_bounds_decode<<<1, 32, 0, s>>>(bounds_ord, dbounds);
+    }
+    k_morton<<<gb, kThreads, 0, s>>>(leafbox, n, dbounds, hb, use_dev, bvh->codes_sorted, bvh->codes_unsorted, vals_a);
+    cudaEventRecord(bvh->ev[1], s);
+
+    // sort: 8 passes ping-ponging codes_sorted <-> keys_b, vals_a <-> vals_b; ends in A
+    k_sort_hist<<<std::min(gb, ctx->num_sms * 8), kSortThreads, 0, s>>>(bvh->codes_sorted, n, hist);
+    CAV_CUDA(ctx, cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem)));
+    uint64_t* kin = bvh->codes_sorted;
+    uint64_t* kout = keys_b;
+    uint32_t* vin = vals_a;
+    uint32_t* vout = vals_b;
+    for (int pass = 0; pass < 8; ++pass) {
+        k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, n, 8 * pass, hist + 256 * pass,
+                                                                  status + (size_t)pass * tiles * 256, counters + pass, err);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    cudaEventRecord(bvh->ev[2], s);
+
+    k_radix_tree<<<div_up(n - 1, kThreads), kThreads, 0, s>>>(bvh->codes_sorted, (int32_t)n, bvh->nodes, err);
+    cudaEventRecord(bvh->ev[3], s);
+    k_refit<<<gb, kThreads, 0, s>>>(leafbox, vals_a, (int32_t)n, bvh->nodes, visited, err);
+    cudaEventRecord(bvh->ev[4], s);
+    CAV_CUDA(ctx, cudaMemcpyAsync(bvh->perm, vals_a, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+    CAV_CUDA(ctx, cudaGetLastError());
+
+    cav_status st = treelet_rounds(ctx, bvh->nodes, n, rounds, leaf_list, visited, s);
+    if (st != CAV_OK) return st;
+    cudaEventRecord(bvh->ev[5], s);
+
+    // traversal layout
+    int nblk = div_up(count, kScanTile);
+    k_count_internal<<<nblk, kScanThreads, 0, s>>>(bvh->nodes, count, blk);
+    k_scan_blocks<<<1, kScanThreads, 0, s>>>(blk, nblk);
+    k_compact_index<<<nblk, kScanThreads, 0, s>>>(bvh->nodes, count, blk, compact);
+    k_tri_layout<<<gb, kThreads, 0, s>>>(positions, indices, mesh_ids, vals_a, n, bvh->tris, slot_of);
+    k_tnode_layout<<<div_up(count, kThreads), kThreads, 0, s>>>(bvh->nodes, count, compact, slot_of, bvh->tnodes,
+                                                                bvh->d_root_box);
+    cudaEventRecord(bvh->ev[6], s);
+    CAV_CUDA(ctx, cudaGetLastError());
+    k_merge_error<<<1, 32, 0, s>>>(err, ctx->d_error);
+    CAV_CUDA(ctx, cudaFreeAsync(sbase, s));
+    *out = bvh;
+    return CAV_OK;
+}
+
+}  // namespace cav

@@ -1,0 +1,151 @@
+// Internal declarations shared by the cavalry_b200 CUDA translation units.
+//
+// All translation units are compiled with -use_fast_math (the reference's numerics
+// flags, CMakeLists.txt:5), so divisions, reciprocals and multiply-adds behave as in
+// the reference's kernels; floating-point expressions that feed bit-exact outputs are
+// written in the same operand order as the reference.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/cavalry.h"
+
+namespace cav {
+
+// ----------------------------------------------------------------- vectors
+struct f3 {
+    float x, y, z;
+};
+__host__ __device__ inline f3 mk(float x, float y, float z) { return f3{x, y, z}; }
+__host__ __device__ inline f3 operator+(f3 a, f3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ inline f3 operator-(f3 a, f3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ inline f3 operator*(f3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ inline f3 operator*(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+__host__ __device__ inline f3 operator/(f3 a, f3 b) { return mk(a.x / b.x, a.y / b.y, a.z / b.z); }
+__host__ __device__ inline f3 vmin3(f3 a, f3 b) { return mk(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
+__host__ __device__ inline f3 vmax3(f3 a, f3 b) { return mk(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
+// Same operand order as the reference's cross/dot (helper math of Core/Triangle.h:7-57).
+__host__ __device__ inline f3 cross3(f3 a, f3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ inline float dot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// AABB::computeSurfaceArea, Core/BoundingBox.h:77-80 (same expression).
+__device__ inline float surface_area(f3 lo, f3 hi) {
+    f3 e = hi - lo;
+    return 2.f * (e.x * e.y + e.y * e.z + e.x * e.z);
+}
+// BVH/SAH.h:4-22: FP64 literals, float results.
+__device__ inline float leaf_cost(float area, int n) { return area * 1.0 * n; }
+__device__ inline float internal_cost(float area, float l, float r) { return area * 1.2 + l + r; }
+__device__ inline float internal_cost(float area, float c) { return area * 1.2 + c; }
+
+// ------------------------------------------------------------ node records
+// Build/restructure node (64 bytes).  Internal nodes at [0, N-2] after the build,
+// leaf j (sorted position) at N-1+j; treelet rounds permute roles among ids.
+struct __align__(16) BNode {
+    float lo_x, lo_y, lo_z, hi_x;  // 16
+    float hi_y, hi_z;              // 24
+    int32_t left, right;           // 32
+    int32_t parent, prim;          // 40 (prim: triangle id of a leaf, -1 internal)
+    float area, cost;              // 48
+    int32_t is_leaf, pad0;         // 56
+    int32_t pad1, pad2;            // 64
+};
+static_assert(sizeof(BNode) == 64, "BNode must be 64 bytes");
+
+// Traversal node (64 bytes): both children's boxes, fetched with four 16-byte loads.
+// child ref >= 0: internal node index; < 0: ~(triangle slot).
+struct __align__(16) TNode {
+    float4 a;  // L.lo.x L.lo.y L.lo.z L.hi.x
+    float4 b;  // L.hi.y L.hi.z R.lo.x R.lo.y
+    float4 c;  // R.lo.z R.hi.x R.hi.y R.hi.z
+    int4 d;    // left ref, right ref, 0, 0
+};
+static_assert(sizeof(TNode) == 64, "TNode must be 64 bytes");
+
+// Triangle record (48 bytes) in sorted (Morton) order: v0, e1 = v1-v0, e2 = v2-v0
+// (the same subtractions as Core/Triangle.h:180-183), triangle id and mesh id.
+struct __align__(16) TriRec {
+    float4 v0;  // v0.xyz, id (int bits)
+    float4 e1;  // e1.xyz, mesh id (int bits)
+    float4 e2;  // e2.xyz, 0
+};
+static_assert(sizeof(TriRec) == 48, "TriRec must be 48 bytes");
+
+}  // namespace cav
+
+// ------------------------------------------------------------ host objects
+struct cav_ctx {
+    int device = 0;
+    int num_sms = 148;
+    std::string last_error;
+    // traversal launch configuration (0 = defaults)
+    int trace_block = 0;
+    int trace_blocks_per_sm = 0;
+    int trace_batch = 0;
+    // persistent work counters (device), one per concurrent trace kind
+    unsigned long long* d_counters = nullptr;
+    int* d_error = nullptr;
+    // host-path staging
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    void* dev_stage = nullptr;
+    size_t dev_stage_bytes = 0;
+    cudaStream_t hstream[2] = {nullptr, nullptr};
+    cudaEvent_t hevent[2] = {nullptr, nullptr};
+};
+
+struct cav_bvh {
+    int64_t n = 0;  // triangles
+    int device = 0;
+    // build products
+    cav::BNode* nodes = nullptr;       // 2N-1 restructure records (reference order)
+    uint64_t* codes_unsorted = nullptr;  // N
+    uint64_t* codes_sorted = nullptr;    // N
+    int32_t* perm = nullptr;             // N: sorted position -> triangle id
+    // traversal layout
+    cav::TNode* tnodes = nullptr;  // N-1
+    cav::TriRec* tris = nullptr;   // N
+    float root_box[6];             // copied to the host at build time? no: device copy
+    float* d_root_box = nullptr;   // 6 floats on device
+    int32_t* d_depth = nullptr;    // scratch for cav_bvh_depth
+    float stage_ms[6] = {0, 0, 0, 0, 0, 0};
+    cudaEvent_t ev[7] = {};
+    bool timed = false;
+    void* arena = nullptr;  // one allocation holding the arrays above
+};
+
+namespace cav {
+
+cav_status set_error(cav_ctx* ctx, cav_status s, const std::string& msg);
+cav_status cuda_error(cav_ctx* ctx, cudaError_t e, const char* what);
+
+// build.cu
+cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int32_t* indices,
+                     const int32_t* mesh_ids, int64_t n, const float* bounds, int rounds, cudaStream_t s,
+                     cav_bvh** out);
+// treelet.cu
+cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int32_t* leaf_list, uint32_t* visited,
+                          cudaStream_t s);
+// trace.cu
+cav_status trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int32_t* prim, float* t,
+                         float* uv, uint32_t flags, cudaStream_t s, unsigned long long* counter);
+cav_status trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,
+                     const int32_t* excl, int64_t n, uint8_t* occ, uint32_t flags, cudaStream_t s,
+                     unsigned long long* counter);
+cav_status trace_stats(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
+                       const float* limit, const int32_t* excl, uint32_t flags, cudaStream_t s, uint64_t* host2);
+
+#define CAV_CUDA(ctx, call)                                              \
+    do {                                                                 \
+        cudaError_t e__ = (call);                                        \
+        if (e__ != cudaSuccess) return ::cav::cuda_error(ctx, e__, #call); \
+    } while (0)
+
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+}  // namespace cav

@@ -1,0 +1,390 @@
+// Ray traversal for sm_100a: persistent warps pull 32-ray batches from a device work
+// counter, fetch a node (both children's boxes) with four 128-bit read-only loads and
+// a triangle with three, and keep the traversal stack in thread-local memory.
+//
+// Semantics are the reference's BVH::intersect / BVH::testVisibility
+// (BVH/BVH.h:23-189): identical slab test (signed-integer min/max on float bit
+// patterns, Core/BoundingBox.h:56-74 and Utils/MathsCommons.h:93-100), identical
+// Moller-Trumbore test (Core/Triangle.h:7-57), the same child order and the same
+// pruning decisions, so hit ids and distances are bit-identical to the reference's
+// on the same tree.  The node layout is different: each record holds both children's
+// boxes, so one 64-byte fetch replaces the reference's two 44-byte child loads, and
+// leaves are folded into their parent's child reference.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+
+#include "cav_internal.cuh"
+
+namespace cav {
+
+namespace {
+
+// The reference keeps `int stack[64]` without a bound check (BVH/BVH.h:41, :122).  Only
+// far children wait on this stack, so it never holds more entries than the tree is deep;
+// 128 entries cover the deepest trees the treelet rounds produce on degenerate input, and
+// the push is checked (the ray is flagged instead of writing past the end).
+constexpr int kStack = 128;
+constexpr uint32_t kMaxSteps = 1u << 22;  // node+triangle visits per ray before the ray is flagged
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ inline float imax_f(float a, float b) { return __int_as_float(max(__float_as_int(a), __float_as_int(b))); }
+__device__ inline float imin_f(float a, float b) { return __int_as_float(min(__float_as_int(a), __float_as_int(b))); }
+
+// AABB::intersect: returns the entry distance (>= 0) or -1 on a miss.
+__device__ inline float slab(float lx, float ly, float lz, float hx, float hy, float hz, const f3& o, const f3& inv) {
+    f3 t0 = (mk(lx, ly, lz) - o) * inv;
+    f3 t1 = (mk(hx, hy, hz) - o) * inv;
+    // fmin_fmax(a,b,c) = int max(int min(a,b), c); fmax_fmin(a,b,c) = int min(int max(a,b), c)
+    float maxmin = imax_f(imin_f(t0.x, t1.x), imax_f(imin_f(t0.y, t1.y), fminf(t0.z, t1.z)));
+    float minmax = imin_f(imax_f(t0.x, t1.x), imin_f(imax_f(t0.y, t1.y), fmaxf(t0.z, t1.z)));
+    if (maxmin <= minmax) {
+        if (minmax > 0) return fmaxf(0.f, maxmin);
+    }
+    return -1.f;
+}
+
+// rayTriangleIntersection (Core/Triangle.h:7-57) on precomputed edges.
+__device__ inline bool tri_test(const f3& o, const f3& d, const f3& v0, const f3& e1, const f3& e2, float& t, float& u,
+                                float& v) {
+    f3 tvec = o - v0;
+    f3 pvec = cross3(d, e2);
+    float det = dot3(e1, pvec);
+    if (det == 0) return false;
+    det = 1.f / det;
+    u = dot3(tvec, pvec) * det;
+    if (u < 0.0f || u > 1.0f) return false;
+    f3 qvec = cross3(tvec, e1);
+    v = dot3(d, qvec) * det;
+    if (v < 0.0f || (u + v) > 1.0f) return false;
+    t = dot3(e2, qvec) * det;
+    if (t <= 0.f) return false;
+    return true;
+}
+
+__device__ inline void load_tri(const TriRec* __restrict__ tris, int slot, f3& v0, f3& e1, f3& e2, int& id, int& mesh) {
+    const float4* p = reinterpret_cast<const float4*>(tris + slot);
+    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    v0 = mk(a.x, a.y, a.z);
+    id = __float_as_int(a.w);
+    e1 = mk(b.x, b.y, b.z);
+    mesh = __float_as_int(b.w);
+    e2 = mk(c.x, c.y, c.z);
+}
+
+template <bool kCullPop, bool kStats>
+__device__ void closest_one(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const float* root_box,
+                            const cav_ray* __restrict__ rays, int64_t i, int32_t* prim, float* tout, float* uv,
+                            int* flag, unsigned long long* stats) {
+    uint32_t n_nodes = 0, n_tris = 0;
+    const float4* rp = reinterpret_cast<const float4*>(rays + i);
+    float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+    f3 o = mk(r0.x, r0.y, r0.z);
+    f3 d = mk(r1.x, r1.y, r1.z);
+    float tmax = r1.w;
+    f3 inv = mk(1.f / d.x, 1.f / d.y, 1.f / d.z);
+    bool hit = false;
+    float best = FLT_MAX, bu = 0.f, bv = 0.f;
+    int32_t bid = -1;
+    bool overflow = false;
+    if (slab(root_box[0], root_box[1], root_box[2], root_box[3], root_box[4], root_box[5], o, inv) >= 0.f) {
+        int32_t stack[kStack];
+        float sdist[kCullPop ? kStack : 1];
+        int top = -1;
+        int32_t ref = 0;
+        uint32_t steps = 0;
+        for (;;) {
+            if (++steps > kMaxSteps) {
+                overflow = true;
+                break;
+            }
+            if (ref >= 0) {
+                if (kStats) ++n_nodes;
+                const float4* np = reinterpret_cast<const float4*>(nodes + ref);
+                float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+                int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
+                float ml = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv);
+                float mr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv);
+                bool okl = ml >= 0 && ml < best && !(ml > tmax);
+                bool okr = mr >= 0 && mr < best && !(mr > tmax);
+                if (okl && okr) {
+                    if (top + 1 >= kStack) {
+                        overflow = true;
+                        break;
+                    }
+                    // the reference pushes the farther child first and pops the nearer
+                    if (ml > mr) {
+                        stack[++top] = dd.x;
+                        if (kCullPop) sdist[top] = ml;
+                        ref = dd.y;
+                    } else {
+                        stack[++top] = dd.y;
+                        if (kCullPop) sdist[top] = mr;
+                        ref = dd.x;
+                    }
+                    continue;
+                } else if (okl) {
+                    ref = dd.x;
+                    continue;
+                } else if (okr) {
+                    ref = dd.y;
+                    continue;
+                }
+            } else {
+                if (kStats) ++n_tris;
+                f3 v0, e1, e2;
+                int id, mesh;
+                load_tri(tris, ~ref, v0, e1, e2, id, mesh);
+                float t, u, v;
+                if (tri_test(o, d, v0, e1, e2, t, u, v)) {
+                    if ((!hit || t < best) && !(t > tmax)) {
+                        hit = true;
+                        best = t;
+                        bid = id;
+                        bu = u;
+                        bv = v;
+                    }
+                }
+            }
+            // pop
+            if (kCullPop) {
+                while (top >= 0 && !(sdist[top] < best)) --top;
+            }
+            if (top < 0) break;
+            ref = stack[top--];
+        }
+    }
+    if (overflow) {
+        bid = -2;
+        hit = false;
+        atomicOr(flag, 1);
+    }
+    prim[i] = hit ? bid : (overflow ? -2 : -1);
+    if (tout) tout[i] = hit ? best : __int_as_float(0x7f800000);
+    if (uv) {
+        reinterpret_cast<float2*>(uv)[i] = make_float2(bu, bv);
+    }
+    if (kStats) {
+        atomicAdd(stats, (unsigned long long)n_nodes);
+        atomicAdd(stats + 1, (unsigned long long)n_tris);
+    }
+}
+
+template <bool kCullPop, bool kStats>
+__device__ void any_one(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const cav_ray* __restrict__ rays,
+                        const float* __restrict__ limit, const int32_t* __restrict__ excl, int64_t i, uint8_t* occ,
+                        int* flag, unsigned long long* stats) {
+    uint32_t n_nodes = 0, n_tris = 0;
+    const float4* rp = reinterpret_cast<const float4*>(rays + i);
+    float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+    f3 o = mk(r0.x, r0.y, r0.z);
+    f3 d = mk(r1.x, r1.y, r1.z);
+    f3 inv = mk(1.f / d.x, 1.f / d.y, 1.f / d.z);
+    const bool use_limit = limit != nullptr;
+    const float lim = use_limit ? __ldg(limit + i) : 0.f;
+    int32_t src = -1, dst = -1;
+    if (excl) {
+        int2 e = __ldg(reinterpret_cast<const int2*>(excl) + i);
+        src = e.x;
+        dst = e.y;
+    }
+    // The reference only reports a root-box miss (BVH/BVH.h:116-120) and traverses anyway.
+    int result = 0;
+    int32_t stack[kStack];
+    int top = -1;
+    int32_t ref = 0;
+    uint32_t steps = 0;
+    for (;;) {
+        if (++steps > kMaxSteps) {
+            result = 2;
+            break;
+        }
+        if (ref >= 0) {
+            if (kStats) ++n_nodes;
+            const float4* np = reinterpret_cast<const float4*>(nodes + ref);
+            float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+            int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
+            float ml = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv);
+            float mr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv);
+            bool okl = ml >= 0;
+            bool okr = mr >= 0;
+            if (kCullPop && use_limit) {
+                okl = okl && ml < lim;
+                okr = okr && mr < lim;
+            }
+            if (okl && okr) {
+                if (top + 1 >= kStack) {
+                    result = 2;
+                    break;
+                }
+                if (ml > mr) {
+                    stack[++top] = dd.x;
+                    ref = dd.y;
+                } else {
+                    stack[++top] = dd.y;
+                    ref = dd.x;
+                }
+                continue;
+            } else if (okl) {
+                ref = dd.x;
+                continue;
+            } else if (okr) {
+                ref = dd.y;
+                continue;
+            }
+        } else {
+            if (kStats) ++n_tris;
+            f3 v0, e1, e2;
+            int id, mesh;
+            load_tri(tris, ~ref, v0, e1, e2, id, mesh);
+            if (mesh != src && mesh != dst) {
+                float t, u, v;
+                if (tri_test(o, d, v0, e1, e2, t, u, v)) {
+                    if (!use_limit || t < lim) {
+                        result = 1;
+                        break;
+                    }
+                }
+            }
+        }
+        if (top < 0) break;
+        ref = stack[top--];
+    }
+    if (result == 2) atomicOr(flag, 1);
+    occ[i] = (uint8_t)result;
+    if (kStats) {
+        atomicAdd(stats, (unsigned long long)n_nodes);
+        atomicAdd(stats + 1, (unsigned long long)n_tris);
+    }
+}
+
+template <bool kCullPop, bool kStats>
+__global__ void k_closest(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const float* root_box,
+                          const cav_ray* __restrict__ rays, int64_t n, int32_t* prim, float* tout, float* uv,
+                          unsigned long long* counter, int batch, int* flag, unsigned long long* stats) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(counter, (unsigned long long)batch);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= (unsigned long long)n) break;
+        for (int k = lane; k < batch; k += 32) {
+            int64_t i = (int64_t)base + k;
+            if (i < n) closest_one<kCullPop, kStats>(nodes, tris, root_box, rays, i, prim, tout, uv, flag, stats);
+        }
+    }
+}
+
+template <bool kCullPop, bool kStats>
+__global__ void k_any(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const cav_ray* __restrict__ rays,
+                      const float* __restrict__ limit, const int32_t* __restrict__ excl, int64_t n, uint8_t* occ,
+                      unsigned long long* counter, int batch, int* flag, unsigned long long* stats) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(counter, (unsigned long long)batch);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= (unsigned long long)n) break;
+        for (int k = lane; k < batch; k += 32) {
+            int64_t i = (int64_t)base + k;
+            if (i < n) any_one<kCullPop, kStats>(nodes, tris, rays, limit, excl, i, occ, flag, stats);
+        }
+    }
+}
+
+template <typename K>
+int grid_for(cav_ctx* ctx, K kernel, int block) {
+    int per_sm = ctx->trace_blocks_per_sm;
+    if (per_sm <= 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+        if (per_sm < 1) per_sm = 1;
+    }
+    return ctx->num_sms * per_sm;
+}
+
+template <bool kStats>
+cav_status launch_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int32_t* prim, float* t,
+                          float* uv, uint32_t flags, cudaStream_t s, unsigned long long* counter,
+                          unsigned long long* stats) {
+    const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
+    const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : 32;
+    CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
+    if (flags & CAV_TRACE_CULL_ON_POP) {
+        int grid = grid_for(ctx, k_closest<true, kStats>, block);
+        k_closest<true, kStats><<<grid, block, 0, s>>>(bvh->tnodes, bvh->tris, bvh->d_root_box, rays, n, prim, t, uv,
+                                                       counter, batch, ctx->d_error + 2, stats);
+    } else {
+        int grid = grid_for(ctx, k_closest<false, kStats>, block);
+        k_closest<false, kStats><<<grid, block, 0, s>>>(bvh->tnodes, bvh->tris, bvh->d_root_box, rays, n, prim, t, uv,
+                                                        counter, batch, ctx->d_error + 2, stats);
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    return CAV_OK;
+}
+
+template <bool kStats>
+cav_status launch_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit, const int32_t* excl,
+                      int64_t n, uint8_t* occ, uint32_t flags, cudaStream_t s, unsigned long long* counter,
+                      unsigned long long* stats) {
+    const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
+    const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : 32;
+    CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
+    if (flags & CAV_TRACE_CULL_ON_POP) {
+        int grid = grid_for(ctx, k_any<true, kStats>, block);
+        k_any<true, kStats><<<grid, block, 0, s>>>(bvh->tnodes, bvh->tris, rays, limit, excl, n, occ, counter, batch,
+                                                   ctx->d_error + 3, stats);
+    } else {
+        int grid = grid_for(ctx, k_any<false, kStats>, block);
+        k_any<false, kStats><<<grid, block, 0, s>>>(bvh->tnodes, bvh->tris, rays, limit, excl, n, occ, counter, batch,
+                                                    ctx->d_error + 3, stats);
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    return CAV_OK;
+}
+
+}  // namespace
+
+cav_status trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int32_t* prim, float* t,
+                         float* uv, uint32_t flags, cudaStream_t s, unsigned long long* counter) {
+    if (!bvh || !rays || !prim || n < 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_trace_closest: bad args");
+    if (((uintptr_t)rays & 15) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
+    if (n == 0) return CAV_OK;
+    return launch_closest<false>(ctx, bvh, rays, n, prim, t, uv, flags, s, counter, nullptr);
+}
+
+cav_status trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit, const int32_t* excl,
+                     int64_t n, uint8_t* occ, uint32_t flags, cudaStream_t s, unsigned long long* counter) {
+    if (!bvh || !rays || !occ || n < 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_trace_any: bad args");
+    if (((uintptr_t)rays & 15) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
+    if (excl && ((uintptr_t)excl & 7) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "excl must be 8-byte aligned");
+    if (n == 0) return CAV_OK;
+    return launch_any<false>(ctx, bvh, rays, limit, excl, n, occ, flags, s, counter, nullptr);
+}
+
+cav_status trace_stats(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
+                       const float* limit, const int32_t* excl, uint32_t flags, cudaStream_t s, uint64_t* host2) {
+    if (!bvh || !rays || n <= 0 || !host2) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_trace_stats: bad args");
+    if (((uintptr_t)rays & 15) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
+    void* tmp = nullptr;
+    size_t bytes = 64 + (size_t)n * 16;
+    CAV_CUDA(ctx, cudaMallocAsync(&tmp, bytes, s));
+    unsigned long long* stats = (unsigned long long*)tmp;
+    unsigned char* out = (unsigned char*)tmp + 64;
+    CAV_CUDA(ctx, cudaMemsetAsync(stats, 0, 16, s));
+    cav_status st;
+    if (any_hit)
+        st = launch_any<true>(ctx, bvh, rays, limit, excl, n, out, flags, s, ctx->d_counters + 4, stats);
+    else
+        st = launch_closest<true>(ctx, bvh, rays, n, (int32_t*)out, (float*)(out + 4 * n), nullptr, flags, s,
+                                  ctx->d_counters + 4, stats);
+    if (st != CAV_OK) return st;
+    unsigned long long h[2];
+    CAV_CUDA(ctx, cudaMemcpyAsync(h, stats, 16, cudaMemcpyDeviceToHost, s));
+    CAV_CUDA(ctx, cudaFreeAsync(tmp, s));
+    CAV_CUDA(ctx, cudaStreamSynchronize(s));
+    host2[0] = h[0];
+    host2[1] = h[1];
+    return CAV_OK;
+}
+
+}  // namespace cav

@@ -1,0 +1,431 @@
+// Treelet restructuring (Karras & Aila 2013) for sm_100a: one warp per treelet root,
+// walking bottom-up from the leaves with an arrival counter per node, dynamic
+// programming over the 128 leaf subsets staged in shared memory.
+//
+// Output is bit-identical to the reference's optimizeBVH (BVH/Optimization.cu:467-525
+// with optimizeTreelet :49-462): same treelet formation (expand the largest-area
+// node, first lane on ties), same partition enumeration order per subset, the same
+// warp min-reduction tree for the 6- and 7-leaf subsets, and the same reuse of node
+// ids by lane during reconstruction.  It differs in mechanics only:
+//   * the warps that start a round are the nodes that are leaves when the round starts,
+//     listed by a separate pass (the reference tests `isLeaf` inside the same launch
+//     that restructures the tree, Optimization.cu:479);
+//   * the formation lanes keep their node records in registers, so every read of the
+//     old treelet precedes every write, and the bottom-up box/cost refresh runs on
+//     registers with explicit warp synchronisation (the reference iterates 7 times over
+//     global memory without __syncwarp, :445-460; its converged values are the same);
+//   * subsets of 2..5 leaves are processed grouped by size instead of by the
+//     reference's hand-packed 5-round table (each subset's result depends only on the
+//     smaller subsets, so the order between subsets does not change any value).
+#include <cuda_runtime.h>
+
+#include "cav_internal.cuh"
+
+namespace cav {
+
+namespace {
+
+constexpr int kWarpsPerBlock = 8;
+constexpr unsigned kFull = 0xffffffffu;
+
+struct SubsetTable {
+    unsigned char s[112];
+    int off[5];  // start of popcount 2,3,4,5 and the end
+};
+
+constexpr int popc7(int x) { return (x & 1) + ((x >> 1) & 1) + ((x >> 2) & 1) + ((x >> 3) & 1) + ((x >> 4) & 1) + ((x >> 5) & 1) + ((x >> 6) & 1); }
+
+constexpr SubsetTable make_table() {
+    SubsetTable t{};
+    int k = 0;
+    for (int pc = 2; pc <= 5; ++pc) {
+        t.off[pc - 2] = k;
+        for (int s = 1; s < 128; ++s)
+            if (popc7(s) == pc) t.s[k++] = (unsigned char)s;
+    }
+    t.off[4] = k;
+    return t;
+}
+
+__constant__ SubsetTable kSubsets = make_table();
+
+struct WarpSmem {
+    float area[128];
+    float cost[128];
+    signed char part[128];
+    int leaf_lane[8];
+};
+
+struct Rec {
+    float lo_x, lo_y, lo_z, hi_x, hi_y, hi_z;
+    int32_t left, right, parent, prim;
+    float area, cost;
+    int32_t is_leaf;
+};
+
+__device__ inline Rec load_rec(const BNode* nodes, int32_t id) {
+    const float4* p = reinterpret_cast<const float4*>(nodes + id);
+    float4 a = __ldcg(p), b = __ldcg(p + 1), c = __ldcg(p + 2), d = __ldcg(p + 3);
+    Rec r;
+    r.lo_x = a.x; r.lo_y = a.y; r.lo_z = a.z; r.hi_x = a.w;
+    r.hi_y = b.x; r.hi_z = b.y; r.left = __float_as_int(b.z); r.right = __float_as_int(b.w);
+    r.parent = __float_as_int(c.x); r.prim = __float_as_int(c.y); r.area = c.z; r.cost = c.w;
+    r.is_leaf = __float_as_int(d.x);
+    return r;
+}
+
+__device__ inline void store_rec(BNode* nodes, int32_t id, const Rec& r) {
+    float4* p = reinterpret_cast<float4*>(nodes + id);
+    __stcg(p, make_float4(r.lo_x, r.lo_y, r.lo_z, r.hi_x));
+    __stcg(p + 1, make_float4(r.hi_y, r.hi_z, __int_as_float(r.left), __int_as_float(r.right)));
+    __stcg(p + 2, make_float4(__int_as_float(r.parent), __int_as_float(r.prim), r.area, r.cost));
+    __stcg(p + 3, make_float4(__int_as_float(r.is_leaf), 0.f, 0.f, 0.f));
+}
+
+__device__ inline bool is_pow2(int n) { return (n & (n - 1)) == 0; }
+
+// optimizeTreelet semantics for the subtree rooted at `root`.  Returns false only on
+// an internal inconsistency (recorded in *err by the caller).
+__device__ bool optimize_treelet(BNode* nodes, int32_t root, int32_t count, WarpSmem& S) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+
+    // ---- formation (Optimization.cu:59-107)
+    int32_t nid = -1;
+    Rec rec{};
+    if (lane == 0) {
+        nid = root;
+        rec = load_rec(nodes, root);
+    }
+    bool expanded = false;
+    int size = 1;
+    while (size < 13) {
+        float my_area = rec.area;
+        if (rec.is_leaf || expanded) my_area = -1.f;
+        int max_lane = 0;
+        float max_area = -1.f;
+        for (int i = 0; i < size; ++i) {
+            float a = __shfl_sync(kFull, my_area, i);
+            if (a > max_area) {
+                max_area = a;
+                max_lane = i;
+            }
+        }
+        int stop = __shfl_sync(kFull, (int)(expanded || rec.is_leaf), max_lane);
+        if (stop) return true;  // fewer than 7 leaves reachable: leave the subtree as it is
+        int32_t cl = __shfl_sync(kFull, rec.left, max_lane);
+        int32_t cr = __shfl_sync(kFull, rec.right, max_lane);
+        if (cl < 0 || cr < 0 || cl >= count || cr >= count) return false;
+        if (lane == max_lane) expanded = true;
+        if (lane == size) {
+            nid = cl;
+            rec = load_rec(nodes, cl);
+        }
+        if (lane == size + 1) {
+            nid = cr;
+            rec = load_rec(nodes, cr);
+        }
+        size += 2;
+    }
+    const bool in_treelet = lane < 13;
+    const unsigned leaf_mask = __ballot_sync(kFull, in_treelet && !expanded);
+    const int my_leaf = __popc(leaf_mask & lt);
+    if (in_treelet && !expanded) S.leaf_lane[my_leaf] = lane;
+    __syncwarp();
+
+    // ---- subset areas (Optimization.cu:126-163)
+    float lbox[7][6];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        int src = S.leaf_lane[k];
+        lbox[k][0] = __shfl_sync(kFull, rec.lo_x, src);
+        lbox[k][1] = __shfl_sync(kFull, rec.lo_y, src);
+        lbox[k][2] = __shfl_sync(kFull, rec.lo_z, src);
+        lbox[k][3] = __shfl_sync(kFull, rec.hi_x, src);
+        lbox[k][4] = __shfl_sync(kFull, rec.hi_y, src);
+        lbox[k][5] = __shfl_sync(kFull, rec.hi_z, src);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        int s = (q << 5) | lane;
+        bool any = false;
+        f3 lo = mk(0, 0, 0), hi = mk(0, 0, 0);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            if ((s >> k) & 1) {
+                f3 blo = mk(lbox[k][0], lbox[k][1], lbox[k][2]);
+                f3 bhi = mk(lbox[k][3], lbox[k][4], lbox[k][5]);
+                if (!any) {
+                    lo = blo;
+                    hi = bhi;
+                    any = true;
+                } else {
+                    lo = vmin3(lo, blo);
+                    hi = vmax3(hi, bhi);
+                }
+            }
+        }
+        S.area[s] = any ? surface_area(lo, hi) : 0.f;
+        S.cost[s] = -1.f;
+    }
+    __syncwarp();
+    if (in_treelet && !expanded) S.cost[1 << my_leaf] = rec.cost;
+    __syncwarp();
+
+    // ---- subsets of 2..5 leaves (Optimization.cu:180-216), grouped by size
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+        const int b = kSubsets.off[g], e = kSubsets.off[g + 1];
+#pragma unroll 1
+        for (int k0 = b; k0 < e; k0 += 32) {
+            int k = k0 + lane;
+            if (k < e) {
+                int s = kSubsets.s[k];
+                float best = -1.f;
+                int bestp = 0;
+                int cleared = (s - 1) & s;
+                int p = (0 - cleared) & s;
+                do {
+                    float tc = S.cost[p] + S.cost[s ^ p];
+                    if (best == -1.f || tc < best) {
+                        bestp = p;
+                        best = tc;
+                    }
+                    p = (p - cleared) & s;
+                } while (p != 0);
+                S.cost[s] = internal_cost(S.area[s], best);
+                S.part[s] = (signed char)bestp;
+            }
+        }
+        __syncwarp();
+    }
+
+    // ---- 6-leaf subsets (Optimization.cu:224-266): partition per lane, then the
+    // reference's lane-order min reduction (lane l reads lane min(l+d, 31)).
+#pragma unroll 1
+    for (int eb = 0; eb < 7; ++eb) {
+        int s = 0x7f ^ (1 << eb);
+        int hi = eb <= 5 ? ((lane << 1) & (((1 << (5 - eb)) - 1) << (eb + 1))) : 0;
+        int p = (lane & ((1 << eb) - 1)) | hi;
+        float tc = -1.f;
+        if (p != 0) tc = S.cost[p] + S.cost[s ^ p];
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+            int o = min(lane + d, 31);
+            float oc = __shfl_sync(kFull, tc, o);
+            int op = __shfl_sync(kFull, p, o);
+            if (tc == -1.f || oc < tc) {
+                tc = oc;
+                p = op;
+            }
+        }
+        if (lane == 0) {
+            S.cost[s] = internal_cost(S.area[s], tc);
+            S.part[s] = (signed char)p;
+        }
+        __syncwarp();
+    }
+
+    // ---- all 7 leaves (Optimization.cu:271-324)
+    {
+        const int s = 0x7f;
+        int p = lane;
+        float tc = -1.f;
+        if (p != 0) tc = S.cost[p] + S.cost[s ^ p];
+        int op = lane | 32;
+        float otc = S.cost[op] + S.cost[s ^ op];
+        if (tc == -1.f || otc < tc) {
+            tc = otc;
+            p = op;
+        }
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+            int o = min(lane + d, 31);
+            float oc = __shfl_sync(kFull, tc, o);
+            int opp = __shfl_sync(kFull, p, o);
+            if (tc == -1.f || oc < tc) {
+                tc = oc;
+                p = opp;
+            }
+        }
+        if (lane == 0) {
+            S.cost[s] = internal_cost(S.area[s], tc);
+            S.part[s] = (signed char)p;
+        }
+        __syncwarp();
+    }
+
+    // ---- reconstruction (Optimization.cu:330-394): lane i keeps node nid and takes a role
+    int my_subset = lane == 0 ? 0x7f : -1;
+    int32_t my_parent = lane == 0 ? rec.parent : -1;
+    bool exp_r = false;
+    int cl_lane = lane, cr_lane = lane;
+    int rsize = 1;
+    while (rsize < 13) {
+        bool prop = lane < rsize && !exp_r && !is_pow2(my_subset);
+        unsigned m = __ballot_sync(kFull, prop);
+        if (m == 0) return false;
+        int sel_lane = __ffs(m) - 1;
+        int sel = __shfl_sync(kFull, my_subset, sel_lane);
+        int32_t parent_node = __shfl_sync(kFull, nid, sel_lane);
+        int pp = S.part[sel];
+        if (sel <= 0 || sel > 127 || is_pow2(sel) || pp <= 0 || (pp & ~sel) != 0) return false;
+        if (lane == sel_lane) {
+            exp_r = true;
+            cl_lane = rsize;
+            cr_lane = rsize + 1;
+        }
+        if (lane == rsize) {
+            my_parent = parent_node;
+            my_subset = pp;
+        }
+        if (lane == rsize + 1) {
+            my_parent = parent_node;
+            my_subset = sel ^ pp;
+        }
+        rsize += 2;
+    }
+
+    // ---- new records (Optimization.cu:400-461)
+    int leaf_id = (in_treelet && !exp_r) ? __ffs(my_subset) - 1 : 0;
+    int src = S.leaf_lane[leaf_id];
+    Rec o;
+    o.lo_x = __shfl_sync(kFull, rec.lo_x, src);
+    o.lo_y = __shfl_sync(kFull, rec.lo_y, src);
+    o.lo_z = __shfl_sync(kFull, rec.lo_z, src);
+    o.hi_x = __shfl_sync(kFull, rec.hi_x, src);
+    o.hi_y = __shfl_sync(kFull, rec.hi_y, src);
+    o.hi_z = __shfl_sync(kFull, rec.hi_z, src);
+    o.left = __shfl_sync(kFull, rec.left, src);
+    o.right = __shfl_sync(kFull, rec.right, src);
+    o.prim = __shfl_sync(kFull, rec.prim, src);
+    o.is_leaf = __shfl_sync(kFull, rec.is_leaf, src);
+    int32_t child_l = __shfl_sync(kFull, nid, cl_lane);
+    int32_t child_r = __shfl_sync(kFull, nid, cr_lane);
+
+    Rec nr;
+    nr.parent = my_parent;
+    float ocl = 0.f, ocr = 0.f;
+    if (!exp_r) {
+        nr.lo_x = o.lo_x; nr.lo_y = o.lo_y; nr.lo_z = o.lo_z;
+        nr.hi_x = o.hi_x; nr.hi_y = o.hi_y; nr.hi_z = o.hi_z;
+        nr.left = o.left;
+        nr.right = o.right;
+        nr.prim = o.prim;
+        nr.is_leaf = o.is_leaf;
+        if (in_treelet && !o.is_leaf && o.left >= 0 && o.right >= 0 && o.left < count && o.right < count) {
+            ocl = __ldcg(&nodes[o.left].cost);
+            ocr = __ldcg(&nodes[o.right].cost);
+        }
+    } else {
+        nr.lo_x = nr.lo_y = nr.lo_z = 0.f;
+        nr.hi_x = nr.hi_y = nr.hi_z = 0.f;
+        nr.left = child_l;
+        nr.right = child_r;
+        nr.prim = -1;
+        nr.is_leaf = 0;
+    }
+    // bottom-up boxes: children sit at higher lanes, the treelet is at most 6 deep
+#pragma unroll
+    for (int it = 0; it < 6; ++it) {
+        float a0 = __shfl_sync(kFull, nr.lo_x, cl_lane), b0 = __shfl_sync(kFull, nr.lo_x, cr_lane);
+        float a1 = __shfl_sync(kFull, nr.lo_y, cl_lane), b1 = __shfl_sync(kFull, nr.lo_y, cr_lane);
+        float a2 = __shfl_sync(kFull, nr.lo_z, cl_lane), b2 = __shfl_sync(kFull, nr.lo_z, cr_lane);
+        float a3 = __shfl_sync(kFull, nr.hi_x, cl_lane), b3 = __shfl_sync(kFull, nr.hi_x, cr_lane);
+        float a4 = __shfl_sync(kFull, nr.hi_y, cl_lane), b4 = __shfl_sync(kFull, nr.hi_y, cr_lane);
+        float a5 = __shfl_sync(kFull, nr.hi_z, cl_lane), b5 = __shfl_sync(kFull, nr.hi_z, cr_lane);
+        if (exp_r) {
+            f3 lo = vmin3(mk(a0, a1, a2), mk(b0, b1, b2));
+            f3 hi = vmax3(mk(a3, a4, a5), mk(b3, b4, b5));
+            nr.lo_x = lo.x; nr.lo_y = lo.y; nr.lo_z = lo.z;
+            nr.hi_x = hi.x; nr.hi_y = hi.y; nr.hi_z = hi.z;
+        }
+    }
+    nr.area = surface_area(mk(nr.lo_x, nr.lo_y, nr.lo_z), mk(nr.hi_x, nr.hi_y, nr.hi_z));
+    if (!exp_r) nr.cost = nr.is_leaf ? leaf_cost(nr.area, 1) : internal_cost(nr.area, ocl, ocr);
+    else nr.cost = 0.f;
+#pragma unroll
+    for (int it = 0; it < 6; ++it) {
+        float ca = __shfl_sync(kFull, nr.cost, cl_lane);
+        float cb = __shfl_sync(kFull, nr.cost, cr_lane);
+        if (exp_r) nr.cost = internal_cost(nr.area, ca, cb);
+    }
+    if (in_treelet) {
+        store_rec(nodes, nid, nr);
+        if (!exp_r && !o.is_leaf && o.left >= 0 && o.right >= 0 && o.left < count && o.right < count) {
+            __stcg(&nodes[o.left].parent, nid);
+            __stcg(&nodes[o.right].parent, nid);
+        }
+    }
+    __syncwarp();
+    return true;
+}
+
+__global__ void k_leaf_list(const BNode* __restrict__ nodes, int64_t count, int32_t* __restrict__ list,
+                            uint32_t* __restrict__ counter) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool leaf = i < count && nodes[i].is_leaf;
+    unsigned m = __ballot_sync(kFull, leaf);
+    if (m == 0) return;
+    int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(counter, (uint32_t)__popc(m));
+    base = __shfl_sync(kFull, base, __ffs(m) - 1);
+    uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
+    if (leaf && pos < (uint32_t)((count + 1) / 2)) list[pos] = (int32_t)i;
+}
+
+// optimizeBVHImpl (Optimization.cu:467-507): one warp per starting leaf; the second
+// arrival at a node optimises the treelet rooted there and continues upwards.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_treelet(BNode* nodes, const int32_t* __restrict__ list,
+                                                                 int64_t n, uint32_t* visited, int* err) {
+    __shared__ WarpSmem smem[kWarpsPerBlock];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int64_t gw = (int64_t)blockIdx.x * kWarpsPerBlock + w;
+    if (gw >= n) return;
+    const int32_t count = (int32_t)(2 * n - 1);
+    int32_t curr = list[gw];
+    if (curr < 0 || curr >= count) {
+        if (lane == 0) atomicExch(err, 2);
+        return;
+    }
+    for (;;) {
+        if (curr == 0) break;
+        int32_t parent = __ldcg(&nodes[curr].parent);
+        if (parent < 0 || parent >= count) {
+            if (lane == 0) atomicExch(err, 2);
+            return;
+        }
+        uint32_t old = 0;
+        if (lane == 0) old = atomicAdd(visited + parent, 1u);
+        old = __shfl_sync(kFull, old, 0);
+        if (old != 1) return;  // first arrival stops; the second optimises the parent
+        __threadfence();
+        curr = parent;
+        if (!optimize_treelet(nodes, curr, count, smem[w])) {
+            if (lane == 0) atomicExch(err, 2);
+            return;
+        }
+        __threadfence();
+    }
+}
+
+}  // namespace
+
+cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int32_t* leaf_list, uint32_t* visited,
+                          cudaStream_t s) {
+    if (rounds <= 0) return CAV_OK;
+    const int64_t count = 2 * n - 1;
+    uint32_t* counter = reinterpret_cast<uint32_t*>(ctx->d_counters) + 8;  // scratch word in the ctx block
+    for (int r = 0; r < rounds; ++r) {
+        CAV_CUDA(ctx, cudaMemsetAsync(visited, 0, sizeof(uint32_t) * count, s));
+        CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), s));
+        k_leaf_list<<<div_up(count, 256), 256, 0, s>>>(nodes, count, leaf_list, counter);
+        k_treelet<<<div_up(n, kWarpsPerBlock), kWarpsPerBlock * 32, 0, s>>>(nodes, leaf_list, n, visited,
+                                                                          ctx->d_error + 1);
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    return CAV_OK;
+}
+
+}  // namespace cav

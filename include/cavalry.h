@@ -1,0 +1,173 @@
+/*
+ * cavalry_b200 — C ABI for the BVH build and ray-query hot path (sm_100a).
+ *
+ * Every entry point takes plain pointers and sizes; no C++ or torch types cross
+ * this boundary.  Unless stated otherwise, array arguments are DEVICE pointers
+ * and work is enqueued on the caller's CUDA stream (`stream`, a cudaStream_t;
+ * NULL = legacy default stream) and completes asynchronously.  Functions return
+ * a cav_status; none of them calls exit().  A context is not thread-safe;
+ * independent contexts may be used from different threads.
+ *
+ * Reference interfaces replaced (paths inside AmesingFlank/Cavalry):
+ *   BVH::build                      BVH/BVH.h:19, BVH/BVH.cu:317-370
+ *   BVH::intersect (closest hit)    BVH/BVH.h:23-107  (called via Core/Scene.h:42-51)
+ *   BVH::testVisibility (any hit)   BVH/BVH.h:109-189 (called via Core/Scene.h:53-56)
+ */
+#ifndef CAVALRY_B200_H
+#define CAVALRY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cav_status {
+    CAV_OK = 0,
+    CAV_ERR_INVALID_ARGUMENT = 1, /* bad size, null pointer, unsupported flag */
+    CAV_ERR_CUDA = 2,             /* a CUDA runtime call failed; see cav_last_error */
+    CAV_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed */
+    CAV_ERR_TIMEOUT = 4,          /* a bounded device-side wait gave up */
+    CAV_ERR_STACK_OVERFLOW = 5,   /* traversal stack depth exceeded (rays flagged) */
+    CAV_ERR_NOT_READY = 6
+} cav_status;
+
+typedef struct cav_ctx cav_ctx;
+typedef struct cav_bvh cav_bvh;
+
+/* Context on CUDA device `device` (the device is made current by every call). */
+cav_status cav_ctx_create(int device, cav_ctx** out);
+cav_status cav_ctx_destroy(cav_ctx* ctx);
+/* Human-readable text of the last error recorded on this context ("" if none). */
+const char* cav_last_error(const cav_ctx* ctx);
+const char* cav_status_string(cav_status s);
+/* ABI version: major*10000 + minor*100 + patch. */
+int cav_version(void);
+/* Synchronises `stream` and reports the device-side error flags raised since the last
+ * check (sort look-back timeout, treelet inconsistency, traversal stack overflow),
+ * clearing them.  The reference reports such conditions with device printf only
+ * (Utils/GpuCommons.h:13-20). */
+cav_status cav_sync_check(cav_ctx* ctx, void* stream);
+
+/*
+ * LBVH build + treelet restructuring.  Replaces BVH::build (BVH/BVH.cu:317-370).
+ *
+ * positions : num_vertices*3 floats (x,y,z), device.
+ * indices   : num_triangles*3 int32 vertex indices, device.  Triangle i is the
+ *             i-th entry of the reference's global triangle list (mesh order, then
+ *             triangle index; Core/TriangleMesh.cu:190-195), so leaf primitive ids
+ *             equal the reference's.
+ * mesh_ids  : num_triangles int32 (Triangle::meshIndex), device, or NULL (all 0).
+ *             Used only by cav_trace_any's mesh exclusion.
+ * scene_bounds : 6 host floats (min xyz, max xyz) or NULL.  NULL computes the union
+ *             of the triangle boxes on the device (the value Core/Scene.cu:131-135
+ *             folds on the host).
+ * rounds    : treelet restructuring rounds (>= 0; the reference's
+ *             --bvh-opt-rounds, Core/Scene.cu:141-146 picks 3 or 10 when it is -1).
+ * The call is stream-ordered; the returned handle may be used on `stream` at once.
+ * num_triangles must be in [2, 2^30).
+ */
+cav_status cav_bvh_build(cav_ctx* ctx, const float* positions, int64_t num_vertices, const int32_t* indices,
+                         const int32_t* mesh_ids, int64_t num_triangles, const float* scene_bounds, int rounds,
+                         void* stream, cav_bvh** out);
+cav_status cav_bvh_free(cav_bvh* bvh);
+int64_t cav_bvh_num_triangles(const cav_bvh* bvh);
+/* Tree depth (edges from the root to the deepest leaf); synchronises `stream`. */
+cav_status cav_bvh_depth(cav_ctx* ctx, const cav_bvh* bvh, void* stream, int32_t* depth);
+
+/*
+ * Parity export of the final node array in the reference's BVHNode order
+ * (BVH/BVHNode.h:8-21; BVH/BVH.cu:304-315): 2N-1 records of cav_ref_node, node 0
+ * the root.  Internal-node prim ranges are unspecified in the reference and are
+ * written as -1 here.  HOST output pointer; synchronises `stream`.
+ */
+typedef struct cav_ref_node {
+    float bmin[3];
+    float bmax[3];
+    int32_t prim_begin, prim_end, left, right, is_leaf;
+} cav_ref_node; /* 44 bytes */
+cav_status cav_bvh_export_nodes(cav_ctx* ctx, const cav_bvh* bvh, void* stream, cav_ref_node* host_out);
+
+/*
+ * Parity export of the build's intermediate stages: Morton codes in triangle order
+ * (BVH/BVH.cu:79-92), the sorted codes and the stable sort permutation (the
+ * leaves' primitiveIndexBegin after BVH/BVH.cu:335).  Any pointer may be NULL.
+ * HOST outputs of num_triangles entries; synchronises `stream`.
+ */
+cav_status cav_bvh_export_stages(cav_ctx* ctx, const cav_bvh* bvh, void* stream, uint64_t* morton_unsorted,
+                                 uint64_t* morton_sorted, int32_t* sorted_prims);
+
+/* Ray record: 8 floats = origin.xyz, tmin, direction.xyz, tmax (32 bytes, 16-aligned). */
+typedef struct cav_ray {
+    float ox, oy, oz, tmin;
+    float dx, dy, dz, tmax;
+} cav_ray;
+
+/* trace flags */
+#define CAV_TRACE_EXACT 0u        /* reference order and pruning (BVH/BVH.h); default */
+#define CAV_TRACE_CULL_ON_POP 1u  /* also re-test a popped node against the current hit
+                                     distance / distance limit (fewer visits; results can
+                                     differ from the reference only at exact-t ties) */
+
+/*
+ * Closest hit, BVH::intersect semantics (BVH/BVH.h:23-107): nearest child first,
+ * a child is visited only if its slab distance is >= 0 and < the current hit
+ * distance; the first of equal-t hits in that order wins.  tmin is ignored and
+ * tmax limits the accepted distance (tmax = +inf reproduces the reference, which
+ * has no tmax).  Outputs (device, any may be NULL except prim_id):
+ *   prim_id[i] : hit triangle (reference triangle index) or -1; -2 if the traversal
+ *                stack (128 entries, i.e. trees up to 128 deep) overflowed for that
+ *                ray; cav_sync_check then reports CAV_ERR_STACK_OVERFLOW.
+ *   t[i], uv[2i..2i+1] : hit distance and barycentrics (u, v) of that triangle.
+ */
+cav_status cav_trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int32_t* prim_id,
+                             float* t, float* uv, uint32_t flags, void* stream);
+
+/*
+ * Any hit, BVH::testVisibility semantics (BVH/BVH.h:109-189): triangles whose mesh
+ * id equals the ray's source or target mesh are skipped; with a limit a hit counts
+ * only if its distance is < limit.  limit: n floats or NULL (no limit);
+ * excl_mesh: 2n int32 (source, target; -1 = none) or NULL.  occluded[i] = 1 if
+ * blocked, 0 if visible, 2 if the stack overflowed.
+ */
+cav_status cav_trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,
+                         const int32_t* excl_mesh, int64_t n, uint8_t* occluded, uint32_t flags, void* stream);
+
+/*
+ * Instrumented traversal: runs the closest-hit (any_hit = 0) or any-hit (any_hit = 1)
+ * traversal over `rays` with the same semantics and additionally counts node records
+ * fetched (host_counts[0]) and triangles tested (host_counts[1]).  Results are
+ * discarded; synchronises `stream`.  Used to state the algorithmic bytes per ray.
+ */
+cav_status cav_trace_stats(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
+                           const float* limit, const int32_t* excl_mesh, uint32_t flags, void* stream,
+                           uint64_t* host_counts);
+
+/*
+ * Host-buffer variants: rays/limit/excl and the outputs are HOST pointers (pageable
+ * or pinned).  The context stages them through pinned buffers in chunks, overlapping
+ * copies with traversal, and returns after the results are on the host.
+ */
+cav_status cav_trace_closest_host(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n,
+                                  int32_t* prim_id, float* t, float* uv, uint32_t flags);
+cav_status cav_trace_any_host(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,
+                              const int32_t* excl_mesh, int64_t n, uint8_t* occluded, uint32_t flags);
+
+/*
+ * Launch-shape overrides used by the autotuner (0 = built-in default).
+ *   block_threads : threads per traversal block (multiple of 32, <= 1024)
+ *   blocks_per_sm : resident blocks requested per SM for the persistent grid
+ *   batch         : rays a warp claims per fetch from the work counter (multiple of 32)
+ */
+cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_sm, int batch);
+
+/* Device-side event timing of the last build's stages (ms): leaf boxes + Morton,
+ * sort, radix tree, refit, treelet rounds, layout.  Valid after the stream is synced. */
+cav_status cav_bvh_stage_times(cav_ctx* ctx, const cav_bvh* bvh, float* ms6);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CAVALRY_B200_H */

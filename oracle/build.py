@@ -1,0 +1,49 @@
+"""Test infrastructure: builds the C oracle and (when the reference sources exist) the
+reference harness.
+
+    python -m oracle.build
+
+* ``oracle/_build/libcavoracle.so`` from ``cav_oracle.c`` (gcc; -ffp-contract=off so
+  that only the explicit fmaf/fma calls contract, OpenMP for the timed CPU baseline).
+* ``oracle/_ref/libcavref.so`` from the reference's own BVH sources via
+  ``build_ref.sh`` (nvcc, sm_100a).  Skipped when the reference tree is absent.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+ORACLE_LIB = BUILD / "libcavoracle.so"
+REF_LIB = HERE / "_ref" / "libcavref.so"
+REFERENCE_ROOT = Path(os.environ.get("CAVALRY_REFERENCE", "/root/reference"))
+
+
+def build_oracle(force: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    src = HERE / "cav_oracle.c"
+    if not force and ORACLE_LIB.exists() and ORACLE_LIB.stat().st_mtime >= src.stat().st_mtime:
+        return ORACLE_LIB
+    tmp = ORACLE_LIB.with_suffix(".tmp.so")
+    cmd = ["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared",
+           "-o", str(tmp), str(src), "-lm"]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, ORACLE_LIB)
+    return ORACLE_LIB
+
+
+def build_ref(force: bool = False) -> Path | None:
+    if not (REFERENCE_ROOT / "BVH" / "BVH.cu").exists():
+        return REF_LIB if REF_LIB.exists() else None
+    deps = [HERE / "ref_harness.cu", HERE / "build_ref.sh", *sorted((HERE / "ref_shim").rglob("*.h"))]
+    if not force and REF_LIB.exists() and REF_LIB.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
+        return REF_LIB
+    subprocess.run(["bash", str(HERE / "build_ref.sh"), str(REFERENCE_ROOT)], check=True)
+    return REF_LIB
+
+
+if __name__ == "__main__":
+    print(build_oracle())
+    print(build_ref())

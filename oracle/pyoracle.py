@@ -1,0 +1,235 @@
+"""Test infrastructure: ctypes bindings of the C oracle (``libcavoracle.so``) and of the
+reference-build harness (``_ref/libcavref.so``).
+
+Node arrays use ``ONODE_DTYPE``, the field order of the reference's BVHRestructureNode
+(BVH/BVHNode.h:50-68): box, prim range, children, parent, leaf flag, SAH area and cost.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from . import build as _build
+
+ONODE_DTYPE = np.dtype(
+    [("bmin", "<f4", (3,)), ("bmax", "<f4", (3,)), ("begin", "<i4"), ("end", "<i4"), ("left", "<i4"),
+     ("right", "<i4"), ("parent", "<i4"), ("is_leaf", "<i4"), ("area", "<f4"), ("cost", "<f4")]
+)
+assert ONODE_DTYPE.itemsize == 56
+
+_orc = None
+_ref = None
+
+
+def _c(a):
+    return None if a is None else a.ctypes.data
+
+
+def oracle_lib() -> ctypes.CDLL:
+    global _orc
+    if _orc is None:
+        path = _build.ORACLE_LIB
+        if not path.exists():
+            path = _build.build_oracle()
+        L = ctypes.CDLL(str(path))
+        P, I64 = ctypes.c_void_p, ctypes.c_int64
+        L.orc_build.argtypes = [P, P, I64, P, P, ctypes.c_int, P, P, P, P, P, P]
+        L.orc_build.restype = ctypes.c_int
+        L.orc_trace_closest.argtypes = [P, P, P, P, I64, P, P, P, P]
+        L.orc_trace_any.argtypes = [P, P, P, P, P, P, P, I64, P]
+        L.orc_treelet_rounds.argtypes = [P, I64, ctypes.c_int]
+        L.orc_morton.argtypes = [P, I64, P, P]
+        L.orc_leaf_boxes.argtypes = [P, P, I64, P]
+        L.orc_scene_bounds.argtypes = [P, I64, P]
+        L.orc_num_threads.restype = ctypes.c_int
+        _orc = L
+    return _orc
+
+
+def build(pos: np.ndarray, idx: np.ndarray, bounds=None, codes=None, rounds: int = 0) -> dict:
+    """Oracle LBVH build.  codes: optional unsorted Morton codes to use instead of computing them."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    idx = np.ascontiguousarray(idx, np.int32)
+    n = idx.shape[0]
+    out = {
+        "codes": np.zeros(n, np.uint64),
+        "sorted": np.zeros(n, np.uint64),
+        "perm": np.zeros(n, np.int32),
+        "merged": np.zeros(2 * n - 1, ONODE_DTYPE),
+        "final": np.zeros(2 * n - 1, ONODE_DTYPE),
+        "bounds": np.zeros(6, np.float32),
+    }
+    b = None if bounds is None else np.ascontiguousarray(bounds, np.float32)
+    c = None if codes is None else np.ascontiguousarray(codes, np.uint64)
+    st = oracle_lib().orc_build(_c(pos), _c(idx), n, _c(b), _c(c), int(rounds), _c(out["codes"]), _c(out["sorted"]),
+                                _c(out["perm"]), _c(out["merged"]), _c(out["final"]), _c(out["bounds"]))
+    if st != 0:
+        raise ValueError(f"orc_build failed ({st})")
+    return out
+
+
+def morton(pos, idx, bounds) -> np.ndarray:
+    n = idx.shape[0]
+    box = np.zeros((n, 6), np.float32)
+    pos = np.ascontiguousarray(pos, np.float32)
+    idx = np.ascontiguousarray(idx, np.int32)
+    bounds = np.ascontiguousarray(bounds, np.float32)
+    oracle_lib().orc_leaf_boxes(_c(pos), _c(idx), n, _c(box))
+    codes = np.zeros(n, np.uint64)
+    oracle_lib().orc_morton(_c(box), n, _c(bounds), _c(codes))
+    return codes
+
+
+def treelet_rounds(nodes: np.ndarray, rounds: int) -> np.ndarray:
+    out = np.ascontiguousarray(nodes.copy())
+    oracle_lib().orc_treelet_rounds(_c(out), out.shape[0], int(rounds))
+    return out
+
+
+def rays6(rays8: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(np.concatenate([rays8[:, 0:3], rays8[:, 4:7]], axis=1).astype(np.float32))
+
+
+# Every array handed to C is bound to a local name first: a temporary passed as
+# `_c(np.ascontiguousarray(...))` would be freed before the foreign call reads it.
+def trace_closest(nodes, pos, idx, rays8):
+    n = rays8.shape[0]
+    r6 = rays6(rays8)
+    nodes = np.ascontiguousarray(nodes)
+    pos = np.ascontiguousarray(pos, np.float32)
+    idx = np.ascontiguousarray(idx, np.int32)
+    prim = np.zeros(n, np.int32)
+    t = np.zeros(n, np.float32)
+    u = np.zeros(n, np.float32)
+    v = np.zeros(n, np.float32)
+    oracle_lib().orc_trace_closest(_c(nodes), _c(pos), _c(idx), _c(r6), n, _c(prim), _c(t), _c(u), _c(v))
+    return prim, t, u, v
+
+
+def trace_any(nodes, pos, idx, rays8, limit=None, excl=None, mesh_ids=None):
+    n = rays8.shape[0]
+    r6 = rays6(rays8)
+    nodes = np.ascontiguousarray(nodes)
+    pos = np.ascontiguousarray(pos, np.float32)
+    idx = np.ascontiguousarray(idx, np.int32)
+    occ = np.zeros(n, np.uint8)
+    lim = None if limit is None else np.ascontiguousarray(limit, np.float32)
+    ex = None if excl is None else np.ascontiguousarray(excl, np.int32)
+    mi = None if mesh_ids is None else np.ascontiguousarray(mesh_ids, np.int32)
+    oracle_lib().orc_trace_any(_c(nodes), _c(pos), _c(idx), _c(mi), _c(r6), _c(lim), _c(ex), n, _c(occ))
+    return occ
+
+
+def num_threads() -> int:
+    return int(oracle_lib().orc_num_threads())
+
+
+# ----------------------------------------------------------------- reference harness
+def ref_available() -> bool:
+    return _build.REF_LIB.exists()
+
+
+def ref_lib() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        if not _build.REF_LIB.exists():
+            raise FileNotFoundError(f"{_build.REF_LIB} not built (needs the reference sources)")
+        L = ctypes.CDLL(str(_build.REF_LIB))
+        P, I = ctypes.c_void_p, ctypes.c_int
+        L.ref_build.argtypes = [P, I, P, P, I, I, P, I, P, P, P, P, P, P, P, ctypes.POINTER(P)]
+        L.ref_build.restype = I
+        L.ref_export_nodes.argtypes = [P, P]
+        L.ref_tree_depth.argtypes = [P]
+        L.ref_load_nodes.argtypes = [P, P, I]
+        L.ref_trace_closest.argtypes = [P, P, I, I, P, P, P]
+        L.ref_trace_any.argtypes = [P, P, P, P, I, I, P, P]
+        L.ref_free.argtypes = [P]
+        _ref = L
+    return _ref
+
+
+REF_NODE_OUT = np.dtype(
+    [("bmin", "<f4", (3,)), ("bmax", "<f4", (3,)), ("begin", "<i4"), ("end", "<i4"), ("left", "<i4"),
+     ("right", "<i4"), ("is_leaf", "<i4")]
+)
+
+
+class RefScene:
+    """The reference's own BVH build (BVH/BVH.cu:317-370, replayed stage by stage) on the GPU."""
+
+    def __init__(self, pos, idx, mesh_ids=None, bounds=None, rounds=0, id_mode=1, dump=True):
+        L = ref_lib()
+        pos = np.ascontiguousarray(pos, np.float32)
+        idx = np.ascontiguousarray(idx, np.int32)
+        n = idx.shape[0]
+        mesh = np.zeros(n, np.int32) if mesh_ids is None else np.ascontiguousarray(mesh_ids, np.int32)
+        self.n = n
+        self.codes = np.zeros(n, np.uint64) if dump else None
+        self.sorted = np.zeros(n, np.uint64) if dump else None
+        self.perm = np.zeros(n, np.int32) if dump else None
+        self.merged = np.zeros(2 * n - 1, ONODE_DTYPE) if dump else None
+        self.final_r = np.zeros(2 * n - 1, ONODE_DTYPE) if dump else None
+        self.bounds = np.zeros(6, np.float32)
+        self.stage_ms = np.zeros(8, np.float32)
+        b = None if bounds is None else np.ascontiguousarray(bounds, np.float32)
+        h = ctypes.c_void_p()
+        st = L.ref_build(_c(pos), pos.shape[0], _c(idx), _c(mesh), n, int(id_mode), _c(b), int(rounds),
+                         _c(self.codes), _c(self.sorted), _c(self.perm), _c(self.merged), _c(self.final_r),
+                         _c(self.bounds), _c(self.stage_ms), ctypes.byref(h))
+        if st != 0:
+            raise RuntimeError(f"ref_build failed ({st})")
+        self.h = h
+        self.depth = L.ref_tree_depth(h)
+
+    def nodes(self) -> np.ndarray:
+        out = np.zeros(2 * self.n - 1, REF_NODE_OUT)
+        ref_lib().ref_export_nodes(self.h, _c(out))
+        return out
+
+    def load_nodes(self, nodes):
+        """Run the reference's traversal on `nodes` (any dtype with box, prim range, children, leaf flag)."""
+        out = np.zeros(len(nodes), REF_NODE_OUT)
+        for f in ("bmin", "bmax", "left", "right", "is_leaf"):
+            out[f] = nodes[f]
+        out["begin"] = nodes["begin"] if "begin" in nodes.dtype.names else nodes["prim_begin"]
+        out["end"] = nodes["end"] if "end" in nodes.dtype.names else nodes["prim_end"]
+        st = ref_lib().ref_load_nodes(self.h, _c(out), len(out))
+        if st != 0:
+            raise RuntimeError(f"ref_load_nodes failed ({st})")
+        self.depth = ref_lib().ref_tree_depth(self.h)
+
+    def trace_closest(self, rays8, reps=1):
+        n = rays8.shape[0]
+        prim = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        ms = np.zeros(1, np.float32)
+        r6 = rays6(rays8)
+        st = ref_lib().ref_trace_closest(self.h, _c(r6), n, int(reps), _c(prim), _c(t), _c(ms))
+        if st != 0:
+            raise RuntimeError(f"ref_trace_closest refused or failed ({st}); depth={self.depth}")
+        return prim, t, float(ms[0])
+
+    def trace_any(self, rays8, limit=None, excl=None, reps=1):
+        n = rays8.shape[0]
+        occ = np.zeros(n, np.uint8)
+        ms = np.zeros(1, np.float32)
+        lim = None if limit is None else np.ascontiguousarray(limit, np.float32)
+        ex = None if excl is None else np.ascontiguousarray(excl, np.int32)
+        r6 = rays6(rays8)
+        st = ref_lib().ref_trace_any(self.h, _c(r6), _c(lim), _c(ex), n, int(reps), _c(occ), _c(ms))
+        if st != 0:
+            raise RuntimeError(f"ref_trace_any refused or failed ({st}); depth={self.depth}")
+        return occ, float(ms[0])
+
+    def free(self):
+        if self.h:
+            ref_lib().ref_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
