@@ -120,7 +120,7 @@ const char* cav_last_error(const cav_ctx* ctx) { return ctx ? ctx->last_error.c_
 cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_sm, int batch) {
     if (!ctx) return CAV_ERR_INVALID_ARGUMENT;
     if (block_threads < 0 || block_threads > 1024 || (block_threads % 32) != 0 || blocks_per_sm < 0 ||
-        blocks_per_sm > 64 || batch < 0 || (batch % 32) != 0 || batch > 4096)
+        blocks_per_sm > 64 || batch < 0 || batch > 32)
         return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_set_trace_config: out of range");
     ctx->trace_block = block_threads;
     ctx->trace_blocks_per_sm = blocks_per_sm;

@@ -26,6 +26,7 @@ namespace {
 // the push is checked (the ray is flagged instead of writing past the end).
 constexpr int kStack = 128;
 constexpr uint32_t kMaxSteps = 1u << 22;  // node+triangle visits per ray before the ray is flagged
+constexpr int kDefaultRefill = 8;         // idle lanes that trigger a warp's next claim
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ inline float imax_f(float a, float b) { return __int_as_float(max(__float_as_int(a), __float_as_int(b))); }
@@ -72,135 +73,205 @@ __device__ inline void load_tri(const TriRec* __restrict__ tris, int slot, f3& v
     e2 = mk(c.x, c.y, c.z);
 }
 
-template <bool kCullPop, bool kStats>
-__device__ void closest_one(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const float* root_box,
-                            const cav_ray* __restrict__ rays, int64_t i, int32_t* prim, float* tout, float* uv,
-                            int* flag, unsigned long long* stats) {
-    uint32_t n_nodes = 0, n_tris = 0;
-    const float4* rp = reinterpret_cast<const float4*>(rays + i);
-    float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
-    f3 o = mk(r0.x, r0.y, r0.z);
-    f3 d = mk(r1.x, r1.y, r1.z);
-    float tmax = r1.w;
-    f3 inv = mk(1.f / d.x, 1.f / d.y, 1.f / d.z);
-    bool hit = false;
-    float best = FLT_MAX, bu = 0.f, bv = 0.f;
-    int32_t bid = -1;
-    bool overflow = false;
-    if (slab(root_box[0], root_box[1], root_box[2], root_box[3], root_box[4], root_box[5], o, inv) >= 0.f) {
-        int32_t stack[kStack];
-        float sdist[kCullPop ? kStack : 1];
-        int top = -1;
-        int32_t ref = 0;
-        uint32_t steps = 0;
-        for (;;) {
-            if (++steps > kMaxSteps) {
-                overflow = true;
-                break;
-            }
-            if (ref >= 0) {
-                if (kStats) ++n_nodes;
-                const float4* np = reinterpret_cast<const float4*>(nodes + ref);
-                float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
-                int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
-                float ml = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv);
-                float mr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv);
-                bool okl = ml >= 0 && ml < best && !(ml > tmax);
-                bool okr = mr >= 0 && mr < best && !(mr > tmax);
-                if (okl && okr) {
-                    if (top + 1 >= kStack) {
-                        overflow = true;
-                        break;
-                    }
-                    // the reference pushes the farther child first and pops the nearer
-                    if (ml > mr) {
-                        stack[++top] = dd.x;
-                        if (kCullPop) sdist[top] = ml;
-                        ref = dd.y;
-                    } else {
-                        stack[++top] = dd.y;
-                        if (kCullPop) sdist[top] = mr;
-                        ref = dd.x;
-                    }
-                    continue;
-                } else if (okl) {
-                    ref = dd.x;
-                    continue;
-                } else if (okr) {
-                    ref = dd.y;
-                    continue;
-                }
-            } else {
-                if (kStats) ++n_tris;
-                f3 v0, e1, e2;
-                int id, mesh;
-                load_tri(tris, ~ref, v0, e1, e2, id, mesh);
-                float t, u, v;
-                if (tri_test(o, d, v0, e1, e2, t, u, v)) {
-                    if ((!hit || t < best) && !(t > tmax)) {
-                        hit = true;
-                        best = t;
-                        bid = id;
-                        bu = u;
-                        bv = v;
-                    }
-                }
-            }
-            // pop
-            if (kCullPop) {
-                while (top >= 0 && !(sdist[top] < best)) --top;
-            }
-            if (top < 0) break;
-            ref = stack[top--];
-        }
+// ---------------------------------------------------------------- kernels
+// Persistent warps with per-lane ray replacement: every lane owns one ray at a time and
+// advances it by one node or one triangle per iteration.  When at least `refill` lanes of a
+// warp are idle, the warp claims that many new ray indices from the device work counter
+// with one atomic, so lanes whose rays finish early do not wait for the warp's slowest ray.
+// Each ray is still traversed exactly as the reference does; only the assignment of rays
+// to lanes changes.
+struct TraceStats {
+    uint32_t nodes = 0, tris = 0;
+};
+
+template <bool kStats>
+__device__ inline void flush_stats(const TraceStats& st, unsigned long long* stats) {
+    if (!kStats) return;
+    unsigned long long a = st.nodes, b = st.tris;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        a += __shfl_down_sync(kFull, a, o);
+        b += __shfl_down_sync(kFull, b, o);
     }
-    if (overflow) {
-        bid = -2;
-        hit = false;
-        atomicOr(flag, 1);
-    }
-    prim[i] = hit ? bid : (overflow ? -2 : -1);
-    if (tout) tout[i] = hit ? best : __int_as_float(0x7f800000);
-    if (uv) {
-        reinterpret_cast<float2*>(uv)[i] = make_float2(bu, bv);
-    }
-    if (kStats) {
-        atomicAdd(stats, (unsigned long long)n_nodes);
-        atomicAdd(stats + 1, (unsigned long long)n_tris);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(stats, a);
+        atomicAdd(stats + 1, b);
     }
 }
 
+// Claims new rays for the idle lanes of the warp.  Returns the claimed index for this lane
+// (or -1) and clears `more` once the counter passed n.
+__device__ inline int64_t claim(unsigned idle, unsigned long long* counter, int64_t n, bool& more) {
+    const int lane = threadIdx.x & 31;
+    const int cnt = __popc(idle);
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, (unsigned long long)cnt);
+    base = __shfl_sync(kFull, base, 0);
+    if (base + (unsigned long long)cnt >= (unsigned long long)n) more = false;
+    if (!((idle >> lane) & 1u)) return -1;
+    int64_t my = (int64_t)base + __popc(idle & ((1u << lane) - 1u));
+    return my < n ? my : -1;
+}
+
 template <bool kCullPop, bool kStats>
-__device__ void any_one(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const cav_ray* __restrict__ rays,
-                        const float* __restrict__ limit, const int32_t* __restrict__ excl, int64_t i, uint8_t* occ,
-                        int* flag, unsigned long long* stats) {
-    uint32_t n_nodes = 0, n_tris = 0;
-    const float4* rp = reinterpret_cast<const float4*>(rays + i);
-    float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
-    f3 o = mk(r0.x, r0.y, r0.z);
-    f3 d = mk(r1.x, r1.y, r1.z);
-    f3 inv = mk(1.f / d.x, 1.f / d.y, 1.f / d.z);
-    const bool use_limit = limit != nullptr;
-    const float lim = use_limit ? __ldg(limit + i) : 0.f;
-    int32_t src = -1, dst = -1;
-    if (excl) {
-        int2 e = __ldg(reinterpret_cast<const int2*>(excl) + i);
-        src = e.x;
-        dst = e.y;
-    }
-    // The reference only reports a root-box miss (BVH/BVH.h:116-120) and traverses anyway.
-    int result = 0;
+__global__ void k_closest(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const float* root_box,
+                          const cav_ray* __restrict__ rays, int64_t n, int32_t* prim, float* tout, float* uv,
+                          unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
+    const float rb0 = root_box[0], rb1 = root_box[1], rb2 = root_box[2];
+    const float rb3 = root_box[3], rb4 = root_box[4], rb5 = root_box[5];
     int32_t stack[kStack];
+    float sdist[kCullPop ? kStack : 1];
+    TraceStats st;
+    bool more = true;
+    int64_t ray = -1;
+    f3 o = mk(0, 0, 0), d = mk(0, 0, 0), inv = mk(0, 0, 0);
+    float tmax = 0.f, best = 0.f, bu = 0.f, bv = 0.f;
+    int32_t bid = -1, ref = 0;
+    bool hit = false;
     int top = -1;
-    int32_t ref = 0;
     uint32_t steps = 0;
     for (;;) {
-        if (++steps > kMaxSteps) {
-            result = 2;
-            break;
+        const unsigned idle = __ballot_sync(kFull, ray < 0);
+        if (idle == kFull && !more) break;
+        if (more && idle != 0 && (__popc(idle) >= refill || idle == kFull)) {
+            int64_t r = claim(idle, counter, n, more);
+            if (r >= 0) {
+                const float4* rp = reinterpret_cast<const float4*>(rays + r);
+                float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+                o = mk(r0.x, r0.y, r0.z);
+                d = mk(r1.x, r1.y, r1.z);
+                tmax = r1.w;
+                inv = mk(1.f / d.x, 1.f / d.y, 1.f / d.z);
+                hit = false;
+                best = FLT_MAX;
+                bu = bv = 0.f;
+                bid = -1;
+                top = -1;
+                ref = 0;
+                steps = 0;
+                ray = r;
+                if (!(slab(rb0, rb1, rb2, rb3, rb4, rb5, o, inv) >= 0.f)) {
+                    prim[r] = -1;  // BVH::intersect returns early when the root box is missed
+                    if (tout) tout[r] = __int_as_float(0x7f800000);
+                    if (uv) reinterpret_cast<float2*>(uv)[r] = make_float2(0.f, 0.f);
+                    ray = -1;
+                }
+            }
         }
+        if (ray < 0) continue;
+        bool pop = false;
         if (ref >= 0) {
-            if (kStats) ++n_nodes;
+            if (kStats) ++st.nodes;
+            const float4* np = reinterpret_cast<const float4*>(nodes + ref);
+            float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+            int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
+            float ml = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv);
+            float mr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv);
+            bool okl = ml >= 0 && ml < best && !(ml > tmax);
+            bool okr = mr >= 0 && mr < best && !(mr > tmax);
+            if (okl && okr) {
+                if (top + 1 >= kStack) {
+                    steps = kMaxSteps;  // overflow: finish below with the flag
+                } else if (ml > mr) {  // the reference pushes the farther child, pops the nearer
+                    stack[++top] = dd.x;
+                    if (kCullPop) sdist[top] = ml;
+                    ref = dd.y;
+                } else {
+                    stack[++top] = dd.y;
+                    if (kCullPop) sdist[top] = mr;
+                    ref = dd.x;
+                }
+            } else if (okl) {
+                ref = dd.x;
+            } else if (okr) {
+                ref = dd.y;
+            } else {
+                pop = true;
+            }
+        } else {
+            if (kStats) ++st.tris;
+            f3 v0, e1, e2;
+            int id, mesh;
+            load_tri(tris, ~ref, v0, e1, e2, id, mesh);
+            float t, u, v;
+            if (tri_test(o, d, v0, e1, e2, t, u, v)) {
+                if ((!hit || t < best) && !(t > tmax)) {
+                    hit = true;
+                    best = t;
+                    bid = id;
+                    bu = u;
+                    bv = v;
+                }
+            }
+            pop = true;
+        }
+        bool finished = false;
+        if (++steps >= kMaxSteps) {
+            atomicOr(flag, 1);
+            hit = false;
+            bid = -2;
+            finished = true;
+        } else if (pop) {
+            if (kCullPop) {
+                while (top >= 0 && !(sdist[top] < best)) --top;
+            }
+            if (top < 0) finished = true;
+            else ref = stack[top--];
+        }
+        if (finished) {
+            prim[ray] = hit ? bid : (bid == -2 ? -2 : -1);
+            if (tout) tout[ray] = hit ? best : __int_as_float(0x7f800000);
+            if (uv) reinterpret_cast<float2*>(uv)[ray] = make_float2(bu, bv);
+            ray = -1;
+        }
+    }
+    flush_stats<kStats>(st, stats);
+}
+
+template <bool kCullPop, bool kStats>
+__global__ void k_any(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const cav_ray* __restrict__ rays,
+                      const float* __restrict__ limit, const int32_t* __restrict__ excl, int64_t n, uint8_t* occ,
+                      unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
+    int32_t stack[kStack];
+    TraceStats st;
+    bool more = true;
+    int64_t ray = -1;
+    f3 o = mk(0, 0, 0), d = mk(0, 0, 0), inv = mk(0, 0, 0);
+    float lim = 0.f;
+    int32_t src = -1, dst = -1, ref = 0;
+    int top = -1;
+    uint32_t steps = 0;
+    const bool use_limit = limit != nullptr;
+    for (;;) {
+        const unsigned idle = __ballot_sync(kFull, ray < 0);
+        if (idle == kFull && !more) break;
+        if (more && idle != 0 && (__popc(idle) >= refill || idle == kFull)) {
+            int64_t r = claim(idle, counter, n, more);
+            if (r >= 0) {
+                const float4* rp = reinterpret_cast<const float4*>(rays + r);
+                float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+                o = mk(r0.x, r0.y, r0.z);
+                d = mk(r1.x, r1.y, r1.z);
+                inv = mk(1.f / d.x, 1.f / d.y, 1.f / d.z);
+                lim = use_limit ? __ldg(limit + r) : 0.f;
+                src = dst = -1;
+                if (excl) {
+                    int2 e = __ldg(reinterpret_cast<const int2*>(excl) + r);
+                    src = e.x;
+                    dst = e.y;
+                }
+                // The reference only reports a root-box miss (BVH/BVH.h:116-120) and traverses anyway.
+                top = -1;
+                ref = 0;
+                steps = 0;
+                ray = r;
+            }
+        }
+        if (ray < 0) continue;
+        bool pop = false;
+        int result = -1;
+        if (ref >= 0) {
+            if (kStats) ++st.nodes;
             const float4* np = reinterpret_cast<const float4*>(nodes + ref);
             float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
             int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
@@ -215,81 +286,45 @@ __device__ void any_one(const TNode* __restrict__ nodes, const TriRec* __restric
             if (okl && okr) {
                 if (top + 1 >= kStack) {
                     result = 2;
-                    break;
-                }
-                if (ml > mr) {
+                } else if (ml > mr) {
                     stack[++top] = dd.x;
                     ref = dd.y;
                 } else {
                     stack[++top] = dd.y;
                     ref = dd.x;
                 }
-                continue;
             } else if (okl) {
                 ref = dd.x;
-                continue;
             } else if (okr) {
                 ref = dd.y;
-                continue;
+            } else {
+                pop = true;
             }
         } else {
-            if (kStats) ++n_tris;
+            if (kStats) ++st.tris;
             f3 v0, e1, e2;
             int id, mesh;
             load_tri(tris, ~ref, v0, e1, e2, id, mesh);
             if (mesh != src && mesh != dst) {
                 float t, u, v;
                 if (tri_test(o, d, v0, e1, e2, t, u, v)) {
-                    if (!use_limit || t < lim) {
-                        result = 1;
-                        break;
-                    }
+                    if (!use_limit || t < lim) result = 1;
                 }
             }
+            pop = true;
         }
-        if (top < 0) break;
-        ref = stack[top--];
-    }
-    if (result == 2) atomicOr(flag, 1);
-    occ[i] = (uint8_t)result;
-    if (kStats) {
-        atomicAdd(stats, (unsigned long long)n_nodes);
-        atomicAdd(stats + 1, (unsigned long long)n_tris);
-    }
-}
-
-template <bool kCullPop, bool kStats>
-__global__ void k_closest(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const float* root_box,
-                          const cav_ray* __restrict__ rays, int64_t n, int32_t* prim, float* tout, float* uv,
-                          unsigned long long* counter, int batch, int* flag, unsigned long long* stats) {
-    const int lane = threadIdx.x & 31;
-    for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(counter, (unsigned long long)batch);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= (unsigned long long)n) break;
-        for (int k = lane; k < batch; k += 32) {
-            int64_t i = (int64_t)base + k;
-            if (i < n) closest_one<kCullPop, kStats>(nodes, tris, root_box, rays, i, prim, tout, uv, flag, stats);
+        if (result < 0 && ++steps >= kMaxSteps) result = 2;
+        if (result < 0 && pop) {
+            if (top < 0) result = 0;
+            else ref = stack[top--];
+        }
+        if (result >= 0) {
+            if (result == 2) atomicOr(flag, 1);
+            occ[ray] = (uint8_t)result;
+            ray = -1;
         }
     }
-}
-
-template <bool kCullPop, bool kStats>
-__global__ void k_any(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const cav_ray* __restrict__ rays,
-                      const float* __restrict__ limit, const int32_t* __restrict__ excl, int64_t n, uint8_t* occ,
-                      unsigned long long* counter, int batch, int* flag, unsigned long long* stats) {
-    const int lane = threadIdx.x & 31;
-    for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(counter, (unsigned long long)batch);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= (unsigned long long)n) break;
-        for (int k = lane; k < batch; k += 32) {
-            int64_t i = (int64_t)base + k;
-            if (i < n) any_one<kCullPop, kStats>(nodes, tris, rays, limit, excl, i, occ, flag, stats);
-        }
-    }
+    flush_stats<kStats>(st, stats);
 }
 
 template <typename K>
@@ -307,7 +342,7 @@ cav_status launch_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays,
                           float* uv, uint32_t flags, cudaStream_t s, unsigned long long* counter,
                           unsigned long long* stats) {
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
-    const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : 32;
+    const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     if (flags & CAV_TRACE_CULL_ON_POP) {
         int grid = grid_for(ctx, k_closest<true, kStats>, block);
@@ -327,7 +362,7 @@ cav_status launch_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, con
                       int64_t n, uint8_t* occ, uint32_t flags, cudaStream_t s, unsigned long long* counter,
                       unsigned long long* stats) {
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
-    const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : 32;
+    const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     if (flags & CAV_TRACE_CULL_ON_POP) {
         int grid = grid_for(ctx, k_any<true, kStats>, block);

@@ -158,7 +158,8 @@ cav_status cav_trace_any_host(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* r
  * Launch-shape overrides used by the autotuner (0 = built-in default).
  *   block_threads : threads per traversal block (multiple of 32, <= 1024)
  *   blocks_per_sm : resident blocks requested per SM for the persistent grid
- *   batch         : rays a warp claims per fetch from the work counter (multiple of 32)
+ *   batch         : queue chunk: idle lanes (1..32) a warp accumulates before it claims
+ *                   that many new rays from the work counter with one atomic
  */
 cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_sm, int batch);
 
