@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "cav_internal.cuh"
@@ -748,3 +749,133 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
 }
 
 }  // namespace cav
+
+// ------------------------------------------------------- allocation-free entry point
+// Morton codes + stable sort (the first LBVH stages) for callers that cannot call
+// cudaMalloc: for example a renderer embedded in a host application that hands out all
+// device memory from its own pool fixed at start-up, or a per-frame loop that must not
+// block on cudaMalloc (which may synchronise the device) or risk an allocation failure
+// mid-frame.  Scratch lives in the file-scope array below, sized for at most
+// CAV_NOALLOC_MAX_TRIANGLES triangles (about 4.8 MB; every GPU that loads this library
+// keeps it until the process exits).  The sorted codes and the permutation are written
+// straight into the caller's output buffers, which double as the sort's ping-pong side A.
+namespace cav {
+namespace {
+
+constexpr int64_t kNoAllocMax = CAV_NOALLOC_MAX_TRIANGLES;
+constexpr int kNoAllocTiles = (int)((kNoAllocMax + kSortTile - 1) / kSortTile);
+constexpr size_t kAlign = 256;
+constexpr size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+constexpr size_t kOffBox = 0;
+constexpr size_t kOffKeys = kOffBox + align_up(sizeof(float) * 6 * kNoAllocMax);
+constexpr size_t kOffVals = kOffKeys + align_up(sizeof(uint64_t) * kNoAllocMax);
+constexpr size_t kOffHist = kOffVals + align_up(sizeof(uint32_t) * kNoAllocMax);
+constexpr size_t kOffStatus = kOffHist + align_up(sizeof(uint32_t) * 8 * 256);
+constexpr size_t kOffCounters = kOffStatus + align_up(sizeof(uint32_t) * 8 * (size_t)kNoAllocTiles * 256);
+constexpr size_t kOffErr = kOffCounters + align_up(sizeof(uint32_t) * 16);
+constexpr size_t kOffBounds = kOffErr + align_up(sizeof(int32_t) * 8);
+constexpr size_t kNoAllocBytes = kOffBounds + align_up(sizeof(float) * 8);
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// The host-side name g_noalloc_scratch is only a stand-in for the symbol; its device
+// address is looked up once per device (with that device current) and cached.
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+
+cav_status noalloc_scratch(unsigned char** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return CAV_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            return CAV_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return CAV_OK;
+}
+
+}  // namespace
+}  // namespace cav
+
+extern "C" cav_status cav_morton_sort_noalloc(const float* positions, int64_t num_vertices, const int32_t* indices,
+                                              int64_t num_triangles, const float* scene_bounds,
+                                              uint64_t* sorted_codes, int32_t* sorted_prims, void* stream) {
+    using namespace cav;
+    const int64_t n = num_triangles;
+    if (!positions || !indices || !sorted_codes || !sorted_prims || num_vertices < 1) return CAV_ERR_INVALID_ARGUMENT;
+    if (n < 2 || n > kNoAllocMax) return CAV_ERR_INVALID_ARGUMENT;  // outside [2, CAV_NOALLOC_MAX_TRIANGLES]
+    unsigned char* base = nullptr;
+    cav_status st = noalloc_scratch(&base);
+    if (st != CAV_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    float* leafbox = reinterpret_cast<float*>(base + kOffBox);
+    uint64_t* keys_b = reinterpret_cast<uint64_t*>(base + kOffKeys);
+    uint32_t* vals_b = reinterpret_cast<uint32_t*>(base + kOffVals);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(base + kOffHist);
+    uint32_t* status = reinterpret_cast<uint32_t*>(base + kOffStatus);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(base + kOffCounters);
+    int32_t* err = reinterpret_cast<int32_t*>(base + kOffErr);
+    float* dbounds = reinterpret_cast<float*>(base + kOffBounds);
+    const int tiles = div_up(n, kSortTile);
+    uint64_t* keys_a = sorted_codes;
+    uint32_t* vals_a = reinterpret_cast<uint32_t*>(sorted_prims);
+    // the array keeps the previous call's contents: clear everything that must start at zero
+    if (cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, s) != cudaSuccess ||
+        cudaMemsetAsync(status, 0, sizeof(uint32_t) * 8 * (size_t)tiles * 256, s) != cudaSuccess ||
+        cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 16, s) != cudaSuccess ||
+        cudaMemsetAsync(err, 0, sizeof(int32_t) * 8, s) != cudaSuccess) {
+        cudaGetLastError();
+        return CAV_ERR_CUDA;
+    }
+    const int gb = div_up(n, kThreads);
+    Bounds6 hb{};
+    int use_dev = scene_bounds ? 0 : 1;
+    int32_t* bounds_ord = reinterpret_cast<int32_t*>(counters + 8);
+    if (scene_bounds) {
+        for (int k = 0; k < 6; ++k) hb.v[k] = scene_bounds[k];
+        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, leafbox, nullptr);
+    } else {
+        k_bounds_init<<<1, 32, 0, s>>>(bounds_ord);
+        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, leafbox, bounds_ord);
+        k_bounds_decode<<<1, 32, 0, s>>>(bounds_ord, dbounds);
+    }
+    // keys_b receives the unsorted copy; the first sort pass overwrites it
+    k_morton<<<gb, kThreads, 0, s>>>(leafbox, n, dbounds, hb, use_dev, keys_a, keys_b, vals_a);
+    k_sort_hist<<<gb < 148 * 8 ? gb : 148 * 8, kSortThreads, 0, s>>>(keys_a, n, hist);
+    if (cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem)) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return CAV_ERR_CUDA;
+    }
+    uint64_t* kin = keys_a;
+    uint64_t* kout = keys_b;
+    uint32_t* vin = vals_a;
+    uint32_t* vout = vals_b;
+    for (int pass = 0; pass < 8; ++pass) {
+        k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, n, 8 * pass, hist + 256 * pass,
+                                                                  status + (size_t)pass * tiles * 256, counters + pass,
+                                                                  err);
+        uint64_t* tk = kin; kin = kout; kout = tk;
+        uint32_t* tv = vin; vin = vout; vout = tv;
+    }
+    // 8 passes: the result is back in side A, the caller's buffers
+    if (cudaGetLastError() != cudaSuccess) return CAV_ERR_CUDA;
+    int32_t herr = 0;
+    if (cudaMemcpyAsync(&herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        return CAV_ERR_CUDA;
+    }
+    return herr ? CAV_ERR_TIMEOUT : CAV_OK;
+}
+

@@ -163,6 +163,30 @@ cav_status cav_trace_any_host(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* r
  */
 cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_sm, int batch);
 
+/*
+ * Allocation-free Morton codes + stable sort (the first stages of BVH::build,
+ * BVH/BVH.cu:79-92 and :335) for callers that cannot call cudaMalloc: a renderer
+ * embedded in a host application that owns all device memory through a pool fixed at
+ * start-up, or a per-frame loop that must neither block on an allocation nor risk one
+ * failing mid-frame.  No counterpart in the reference (its build allocates every array
+ * it uses).
+ *
+ * Writes the sorted 63-bit codes to `sorted_codes` and the triangle of each sorted
+ * position to `sorted_prims` (device buffers of num_triangles entries, the values
+ * cav_bvh_export_stages reports).  positions / indices / scene_bounds as for
+ * cav_bvh_build; runs on the current CUDA device and synchronises `stream`.
+ * Scratch is a static device array sized for CAV_NOALLOC_MAX_TRIANGLES triangles,
+ * held by every GPU that loads this library until the process exits; sizes outside
+ * [2, CAV_NOALLOC_MAX_TRIANGLES] return CAV_ERR_INVALID_ARGUMENT.  The first call on a
+ * device looks up the array's device address; make that call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (on different
+ * streams or threads) race and must be serialised by the caller.
+ */
+#define CAV_NOALLOC_MAX_TRIANGLES 131072
+cav_status cav_morton_sort_noalloc(const float* positions, int64_t num_vertices, const int32_t* indices,
+                                   int64_t num_triangles, const float* scene_bounds, uint64_t* sorted_codes,
+                                   int32_t* sorted_prims, void* stream);
+
 /* Device-side event timing of the last build's stages (ms): leaf boxes + Morton,
  * sort, radix tree, refit, treelet rounds, layout.  Valid after the stream is synced. */
 cav_status cav_bvh_stage_times(cav_ctx* ctx, const cav_bvh* bvh, float* ms6);
