@@ -59,7 +59,7 @@ static_assert(sizeof(BNode) == 64, "BNode must be 64 bytes");
 
 // Traversal node (64 bytes): both children's boxes, fetched with four 16-byte loads.
 // child ref >= 0: internal node index; < 0: ~(triangle slot).
-struct __align__(16) TNode {
+struct __align__(64) TNode {
     float4 a;  // L.lo.x L.lo.y L.lo.z L.hi.x
     float4 b;  // L.hi.y L.hi.z R.lo.x R.lo.y
     float4 c;  // R.lo.z R.hi.x R.hi.y R.hi.z

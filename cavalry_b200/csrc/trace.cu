@@ -26,7 +26,7 @@ namespace {
 // the push is checked (the ray is flagged instead of writing past the end).
 constexpr int kStack = 128;
 constexpr uint32_t kMaxSteps = 1u << 22;  // node+triangle visits per ray before the ray is flagged
-constexpr int kDefaultRefill = 8;         // idle lanes that trigger a warp's next claim
+constexpr int kDefaultRefill = 4;         // idle lanes that trigger a warp's next claim
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ inline float imax_f(float a, float b) { return __int_as_float(max(__float_as_int(a), __float_as_int(b))); }
@@ -61,6 +61,25 @@ __device__ inline bool tri_test(const f3& o, const f3& d, const f3& v0, const f3
     t = dot3(e2, qvec) * det;
     if (t <= 0.f) return false;
     return true;
+}
+
+// One 64-byte node as two 256-bit read-only loads (sm_100 vector width): each load is one
+// 32-byte sector, half the L1 sector lookups of four 16-byte loads.
+__device__ __forceinline__ void ld_nc_v8(const void* p, float (&r)[8]) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7])
+                 : "l"(p));
+}
+
+struct NodeRegs {
+    float lo[8];  // L.lo.xyz L.hi.x L.hi.y L.hi.z R.lo.x R.lo.y
+    float hi[8];  // R.lo.z R.hi.xyz left right - -
+};
+
+__device__ __forceinline__ void load_node(const TNode* __restrict__ nodes, int32_t ref, NodeRegs& nr) {
+    const float* p = reinterpret_cast<const float*>(nodes + ref);
+    ld_nc_v8(p, nr.lo);
+    ld_nc_v8(p + 8, nr.hi);
 }
 
 __device__ inline void load_tri(const TriRec* __restrict__ tris, int slot, f3& v0, f3& e1, f3& e2, int& id, int& mesh) {
@@ -162,11 +181,11 @@ __global__ void k_closest(const TNode* __restrict__ nodes, const TriRec* __restr
         bool pop = false;
         if (ref >= 0) {
             if (kStats) ++st.nodes;
-            const float4* np = reinterpret_cast<const float4*>(nodes + ref);
-            float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
-            int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
-            float ml = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv);
-            float mr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv);
+            NodeRegs nr;
+            load_node(nodes, ref, nr);
+            const int2 dd = make_int2(__float_as_int(nr.hi[4]), __float_as_int(nr.hi[5]));
+            float ml = slab(nr.lo[0], nr.lo[1], nr.lo[2], nr.lo[3], nr.lo[4], nr.lo[5], o, inv);
+            float mr = slab(nr.lo[6], nr.lo[7], nr.hi[0], nr.hi[1], nr.hi[2], nr.hi[3], o, inv);
             bool okl = ml >= 0 && ml < best && !(ml > tmax);
             bool okr = mr >= 0 && mr < best && !(mr > tmax);
             if (okl && okr) {
@@ -272,11 +291,11 @@ __global__ void k_any(const TNode* __restrict__ nodes, const TriRec* __restrict_
         int result = -1;
         if (ref >= 0) {
             if (kStats) ++st.nodes;
-            const float4* np = reinterpret_cast<const float4*>(nodes + ref);
-            float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
-            int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
-            float ml = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv);
-            float mr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv);
+            NodeRegs nr;
+            load_node(nodes, ref, nr);
+            const int2 dd = make_int2(__float_as_int(nr.hi[4]), __float_as_int(nr.hi[5]));
+            float ml = slab(nr.lo[0], nr.lo[1], nr.lo[2], nr.lo[3], nr.lo[4], nr.lo[5], o, inv);
+            float mr = slab(nr.lo[6], nr.lo[7], nr.hi[0], nr.hi[1], nr.hi[2], nr.hi[3], o, inv);
             bool okl = ml >= 0;
             bool okr = mr >= 0;
             if (kCullPop && use_limit) {
