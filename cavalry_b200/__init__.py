@@ -19,7 +19,8 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ["CavError", "Context", "Bvh", "lib", "REF_NODE_DTYPE", "TRACE_EXACT", "TRACE_CULL_ON_POP"]
+__all__ = ["CavError", "Context", "Bvh", "Scene", "SceneInfo", "lib", "parse_pbrt", "film_to_rgb8", "REF_NODE_DTYPE",
+           "TRACE_EXACT", "TRACE_CULL_ON_POP"]
 
 _PKG = Path(__file__).resolve().parent
 _LIB_PATH = _PKG / "libcavalry_b200.so"
@@ -86,6 +87,15 @@ def lib() -> ctypes.CDLL:
         "cav_trace_any_host": ([P, P, P, P, P, I64, P, U32], ctypes.c_int),
         "cav_set_trace_config": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "cav_trace_stats": ([P, P, P, I64, ctypes.c_int, P, P, U32, P, P], ctypes.c_int),
+        "cav_scene_load_pbrt": ([P, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(P)],
+                                ctypes.c_int),
+        "cav_scene_free": ([P], ctypes.c_int),
+        "cav_scene_info": ([P, P], ctypes.c_int),
+        "cav_render_to_host": ([P, P, P, P, P, P], ctypes.c_int),
+        "cav_film_to_rgb8": ([P, P, ctypes.c_int, ctypes.c_int, P], ctypes.c_int),
+        "cav_write_png": ([ctypes.c_char_p, P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "cav_write_pfm": ([ctypes.c_char_p, P, P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "cav_pbrt_parse_info": ([ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, P, P, P, ctypes.c_int], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -145,6 +155,14 @@ class Context:
         self._check(lib().cav_set_trace_config(self.handle, block_threads, blocks_per_sm, batch),
                     "cav_set_trace_config")
 
+    def load_pbrt(self, path: str, spp: int = -1, integrator: str | None = None, bvh_rounds: int = -1) -> Scene:
+        """Load a .pbrt scene and build its BVH (the reference's --spp / --integrator / --bvh-opt-rounds)."""
+        h = ctypes.c_void_p()
+        st = lib().cav_scene_load_pbrt(self.handle, path.encode(), spp, integrator.encode() if integrator else None,
+                                       bvh_rounds, ctypes.byref(h))
+        self._check(st, "cav_scene_load_pbrt")
+        return Scene(self, h)
+
     def build(self, positions, indices, mesh_ids=None, scene_bounds=None, rounds: int = 0, stream=None) -> "Bvh":
         """LBVH + ``rounds`` treelet rounds over device tensors.
 
@@ -168,6 +186,74 @@ class Context:
         )
         self._check(st, "cav_bvh_build")
         return Bvh(self, h, indices.numel() // 3, keep=(positions, indices, mesh_ids))
+
+
+class SceneInfo(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("spp", ctypes.c_int), ("max_depth", ctypes.c_int),
+                ("triangles", ctypes.c_int64), ("meshes", ctypes.c_int), ("lights", ctypes.c_int),
+                ("bvh_rounds", ctypes.c_int), ("integrator", ctypes.c_int)]
+
+
+class RenderOpts(ctypes.Structure):
+    _fields_ = [("spp", ctypes.c_int), ("max_depth", ctypes.c_int), ("integrator", ctypes.c_int),
+                ("max_paths_in_flight", ctypes.c_int64)]
+
+
+def parse_pbrt(path: str, spp: int = -1, integrator: str | None = None) -> tuple[SceneInfo, np.ndarray]:
+    """Host-only parse of a .pbrt file (no GPU): scene counts and the camera-to-world matrix."""
+    info = SceneInfo()
+    c2w = np.zeros(16, np.float32)
+    err = ctypes.create_string_buffer(512)
+    st = lib().cav_pbrt_parse_info(path.encode(), spp, integrator.encode() if integrator else None,
+                                   ctypes.addressof(info), c2w.ctypes.data, ctypes.addressof(err), len(err))
+    if st != 0:
+        raise CavError(st, "cav_pbrt_parse_info: " + err.value.decode(errors="replace"))
+    return info, c2w.reshape(4, 4).T
+
+
+class Scene:
+    """A loaded .pbrt scene with its BVH (cav_scene)."""
+
+    def __init__(self, ctx: "Context", handle):
+        self.ctx = ctx
+        self.handle = handle
+
+    def info(self) -> SceneInfo:
+        out = SceneInfo()
+        self.ctx._check(lib().cav_scene_info(self.handle, ctypes.addressof(out)), "cav_scene_info")
+        return out
+
+    def render(self, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0):
+        """Render to host arrays; returns (film_sum [H,W,3], film_weight [H,W], ms)."""
+        inf = self.info()
+        s = np.zeros((inf.height, inf.width, 3), np.float32)
+        w = np.zeros((inf.height, inf.width), np.float32)
+        ms = np.zeros(1, np.float32)
+        opts = RenderOpts(spp, max_depth, 0, max_paths_in_flight)
+        st = lib().cav_render_to_host(self.ctx.handle, self.handle, ctypes.addressof(opts), s.ctypes.data,
+                                      w.ctypes.data, ms.ctypes.data)
+        self.ctx._check(st, "cav_render_to_host")
+        return s, w, float(ms[0])
+
+    def free(self):
+        if self.handle:
+            lib().cav_scene_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def film_to_rgb8(film_sum: np.ndarray, film_weight: np.ndarray) -> np.ndarray:
+    h, w = film_weight.shape
+    out = np.zeros((h, w, 3), np.uint8)
+    s = np.ascontiguousarray(film_sum, np.float32)
+    wt = np.ascontiguousarray(film_weight, np.float32)
+    lib().cav_film_to_rgb8(s.ctypes.data, wt.ctypes.data, w, h, out.ctypes.data)
+    return out
 
 
 class Bvh:

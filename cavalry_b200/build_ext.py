@@ -42,13 +42,15 @@ def nvcc() -> str:
 
 
 def _compile(src: Path, extra: list[str]) -> Path:
-    obj = BUILD / (src.stem + ".o")
-    if obj.exists() and obj.stat().st_mtime >= max(
-        src.stat().st_mtime, max(p.stat().st_mtime for p in CSRC.glob("*.cuh")),
-        (ROOT / "include" / "cavalry.h").stat().st_mtime,
-    ):
+    obj = BUILD / (src.stem + src.suffix.replace(".", "_") + ".o")
+    deps = [src, *CSRC.glob("*.cuh"), *CSRC.glob("*.h"), ROOT / "include" / "cavalry.h"]
+    if obj.exists() and obj.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
         return obj
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", str(src), "-o", str(obj)]
+    if src.suffix == ".cpp":  # host C++ (the .pbrt loader): plain g++ through nvcc
+        cmd = [nvcc(), "-std=c++17", "-O2", "-Xcompiler", "-fPIC,-O2", "-I", str(ROOT / "include"), "-x", "c++",
+               "-c", str(src), "-o", str(obj)]
+    else:
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", str(src), "-o", str(obj)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stdout}\n{r.stderr}")
@@ -57,7 +59,7 @@ def _compile(src: Path, extra: list[str]) -> Path:
 
 def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
     BUILD.mkdir(exist_ok=True)
-    srcs = sorted(CSRC.glob("*.cu"))
+    srcs = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
     with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, extra or []), srcs))
     if LIB.exists() and LIB.stat().st_mtime >= max(o.stat().st_mtime for o in objs):
@@ -71,6 +73,25 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
     if verbose:
         print(f"built {LIB}")
     return LIB
+
+
+CLI_SRC = PKG / "cli" / "cavalry_main.cpp"
+CLI = PKG / "cavalry"
+
+
+def build_cli(verbose: bool = False) -> Path:
+    """The `cavalry` command-line renderer, linked against the in-tree library."""
+    lib = build(verbose=verbose)
+    if CLI.exists() and CLI.stat().st_mtime >= max(CLI_SRC.stat().st_mtime, lib.stat().st_mtime):
+        return CLI
+    cmd = ["g++", "-std=c++17", "-O2", "-o", str(CLI), str(CLI_SRC), "-L", str(PKG), "-lcavalry_b200",
+           "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"CLI link failed:\n{r.stdout}\n{r.stderr}")
+    if verbose:
+        print(f"built {CLI}")
+    return CLI
 
 
 def ptxas_report() -> str:
@@ -88,3 +109,4 @@ if __name__ == "__main__":
         print(ptxas_report())
     else:
         build(verbose=True)
+        build_cli(verbose=True)

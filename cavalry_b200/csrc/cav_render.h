@@ -1,0 +1,27 @@
+// Device-side scene records of the wavefront renderer (render.cu).
+#pragma once
+
+#include <stdint.h>
+
+namespace cav {
+
+struct RMesh {
+    int32_t first_tri, tri_count;
+    int32_t has_normals, reverse;
+    int32_t material, light;
+    float area;  // TriangleMesh::surfaceArea
+    int32_t pad;
+};
+
+struct RMaterial {
+    int32_t type;
+    float kd[3], ks[3], kr[3], kt[3];
+    float alpha_u, alpha_v, eta, mirror_kr;
+};
+
+struct RLight {
+    float L[3];
+    int32_t mesh;
+};
+
+}  // namespace cav

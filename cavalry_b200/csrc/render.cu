@@ -1,0 +1,997 @@
+// Wavefront path tracer for sm_100a: the generate / extend / lighting (shadow) / material
+// evaluation / next-ray stages of the reference's PathTracingIntegrator
+// (Integrators/PathTracingIntegrator.cu:95-425), with queues compacted by warp-aggregated
+// atomics and every ray query going through the persistent traversal kernels of trace.cu.
+//
+// Sampling follows the reference exactly so that a render with the same sample count uses
+// the same random numbers per path: scrambled Halton (Samplers/HaltonSampler.h:13-76,
+// HaltonSampler.cu:14-67; the permutation tables are built on the host with the C
+// library's srand/rand, as the reference does), camera samples (Core/Sampler.cu:29-51),
+// and the per-bounce dimension budget of computeLighting / genNextRay (randInt for the
+// light, an unused rand4, the light-triangle sample, then Russian roulette after depth 3
+// and a BSDF rand2).  Shading is FP32 and restates the reference's BSDFs: Lambertian
+// (BSDFs/Lambertian.h), plastic = Lambertian + GGX microfacet reflection with Schlick
+// Fresnel (BSDFs/PlasticBSDF.h, Microfacet.h, MicrofacetDistribution.h, Fresnel.h),
+// specular glass (BSDFs/Specular.h) and mirror (BSDFs/MirrorBSDF.h); area lights are the
+// reference's DiffuseAreaLight (Lights/DiffuseAreaLight.h, Core/TriangleMesh.h:110-232).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cav_internal.cuh"
+#include "cav_render.h"
+#include "pbrt.h"
+
+namespace cav {
+namespace {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr int kThreads = 256;
+constexpr int kPrimes = 1024;
+
+// ------------------------------------------------------------------- vector helpers
+__device__ inline f3 operator*(float s, f3 a) { return a * s; }
+__device__ inline f3 operator/(f3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
+__device__ inline f3 neg(f3 a) { return mk(-a.x, -a.y, -a.z); }
+__device__ inline float length3(f3 a) { return sqrtf(dot3(a, a)); }
+__device__ inline f3 normalize3(f3 a) {
+    float inv = rsqrtf(dot3(a, a));
+    return a * inv;
+}
+__device__ inline bool all_zero(f3 a) { return a.x == 0 && a.y == 0 && a.z == 0; }
+__device__ inline bool finite3(f3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+__device__ inline f3 ld3(const float* p) { return mk(p[0], p[1], p[2]); }
+
+// ------------------------------------------------------------------------ Halton
+struct Halton {
+    const uint32_t* primes;
+    const uint32_t* perm_start;
+    const uint16_t* perms;
+};
+
+// runHalton + HaltonSampler::rand1 (Samplers/HaltonSampler.h:13-23, :59-66)
+__device__ inline float halton(const Halton& h, uint64_t index, int& dim) {
+    const int d = dim < kPrimes ? dim : kPrimes - 1;
+    dim += 1;
+    const uint32_t base = h.primes[d];
+    const uint16_t* perm = h.perms + h.perm_start[d];
+    float r = 0, f = 1;
+    uint64_t i = index;
+    while (i > 0) {
+        f = f / base;
+        r = r + f * (perm[i % base]);
+        i = i / base;
+    }
+    return r;
+}
+__device__ inline int halton_int(const Halton& h, uint64_t index, int& dim, int N) {
+    float f = halton(h, index, dim);
+    int r = f * N;
+    if (r >= N) r = N - 1;
+    return r;
+}
+
+// ------------------------------------------------------------------- local frame
+struct Frame {
+    f3 t0, t1, n;
+};
+// buildCoordinateSystem (Utils/MathsCommons.h:194-202)
+__device__ inline Frame make_frame(f3 n) {
+    f3 t0 = fabsf(n.x) < 0.5f ? cross3(mk(1, 0, 0), n) : cross3(mk(0, 1, 0), n);
+    t0 = normalize3(t0);
+    f3 t1 = normalize3(cross3(n, t0));
+    return Frame{t0, t1, n};
+}
+__device__ inline f3 to_local(const Frame& fr, f3 v) { return mk(dot3(fr.t0, v), dot3(fr.t1, v), dot3(fr.n, v)); }
+__device__ inline f3 to_world(const Frame& fr, f3 v) { return fr.t0 * v.x + fr.t1 * v.y + fr.n * v.z; }
+
+__device__ inline bool same_hemisphere(f3 a, f3 b) { return a.z * b.z > 0; }
+__device__ inline float pow5(float f) { return (f * f) * (f * f) * f; }
+__device__ inline float clampf(float x, float lo, float hi) { return fmaxf(lo, fminf(x, hi)); }
+__device__ inline float cos2_theta(f3 w) { return w.z * w.z; }
+__device__ inline float sin2_theta(f3 w) { return fmaxf(0.f, 1.f - cos2_theta(w)); }
+__device__ inline float sin_theta(f3 w) { return sqrtf(sin2_theta(w)); }
+__device__ inline float tan_theta(f3 w) { return sin_theta(w) / w.z; }
+__device__ inline float tan2_theta(f3 w) { return sin2_theta(w) / cos2_theta(w); }
+// The reference tests `sinZenith == 0` (a function name) and therefore never takes the
+// zero branch (Utils/MathsCommons.h:134-143); the division is always evaluated.
+__device__ inline float cos_phi(f3 w) { return clampf(w.x / sin_theta(w), -1.f, 1.f); }
+__device__ inline float sin_phi(f3 w) { return clampf(w.y / sin_theta(w), -1.f, 1.f); }
+
+// concentric disk + cosine hemisphere (Utils/RandomUtils.h:18-48)
+__device__ inline f3 cosine_hemisphere(float u0, float u1) {
+    float ox = 2.f * u0 - 1.f, oy = 2.f * u1 - 1.f;
+    float dx = 0.f, dy = 0.f;
+    if (!(ox == 0 && oy == 0)) {
+        float theta, r;
+        if (fabsf(ox) > fabsf(oy)) {
+            r = ox;
+            theta = (kPi / 4.f) * (oy / ox);
+        } else {
+            r = oy;
+            theta = (kPi / 2.f) - (kPi / 4.f) * (ox / oy);
+        }
+        dx = r * cosf(theta);
+        dy = r * sinf(theta);
+    }
+    float z = sqrtf(fmaxf(0.f, 1 - dx * dx - dy * dy));
+    return mk(dx, dy, z);
+}
+
+// ------------------------------------------------------------------------ GGX
+struct GGX {
+    float ax, ay;
+    __device__ float D(f3 h) const {
+        float t2 = tan2_theta(h);
+        if (isinf(t2)) return 0;
+        const float c4 = cos2_theta(h) * cos2_theta(h);
+        float cp = cos_phi(h), sp = sin_phi(h);
+        float e = (cp * cp / (ax * ax) + sp * sp / (ay * ay)) * t2;
+        return 1 / (kPi * ax * ay * c4 * (1 + e) * (1 + e));
+    }
+    __device__ float Lambda(f3 w) const {
+        if (w.z == 0) return 0;
+        float abs_tan = fabsf(tan_theta(w));
+        float cp = cos_phi(w), sp = sin_phi(w);
+        float alpha = sqrtf(cp * cp * ax * ax + sp * sp * ay * ay);
+        float a2t2 = (alpha * abs_tan) * (alpha * abs_tan);
+        return (-1 + sqrtf(1.f + a2t2)) / 2;
+    }
+    __device__ float G1(f3 w) const { return 1 / (1 + Lambda(w)); }
+    __device__ float G(f3 wi, f3 wo) const { return 1.f / (1.f + Lambda(wi) + Lambda(wo)); }
+    __device__ float pdf(f3 h, f3 wo) const { return D(h) * G1(wo) * fabsf(dot3(wo, h)) / fabsf(wo.z); }
+    // Heitz' visible-normal sampling as in MicrofacetDistribution.h sample/sampleGGX11
+    __device__ static void sample11(float cos_t, float U1, float U2, float& sx, float& sy) {
+        if (cos_t > .9999f) {
+            float r = sqrtf(U1 / (1 - U1));
+            float phi = 6.28318530718f * U2;
+            sx = r * cosf(phi);
+            sy = r * sinf(phi);
+            return;
+        }
+        float sin_t = sqrtf(fmaxf(0.f, 1.f - cos_t * cos_t));
+        float tan_t = sin_t / cos_t;
+        float a = 1 / tan_t;
+        float G1v = 2 / (1 + sqrtf(1.f + 1.f / (a * a)));
+        float A = 2 * U1 / G1v - 1;
+        float tmp = 1.f / (A * A - 1.f);
+        if (tmp > 1e10f) tmp = 1e10f;
+        float B = tan_t;
+        float Dd = sqrtf(fmaxf(B * B * tmp * tmp - (A * A - B * B) * tmp, 0.f));
+        float s1 = B * tmp - Dd, s2 = B * tmp + Dd;
+        sx = (A < 0 || s2 > 1.f / tan_t) ? s1 : s2;
+        float S;
+        if (U2 > 0.5f) {
+            S = 1.f;
+            U2 = 2.f * (U2 - .5f);
+        } else {
+            S = -1.f;
+            U2 = 2.f * (.5f - U2);
+        }
+        float z = (U2 * (U2 * (U2 * 0.27385f - 0.73369f) + 0.46341f)) /
+                  (U2 * (U2 * (U2 * 0.093073f + 0.309420f) - 1.000000f) + 0.597999f);
+        sy = S * z * sqrtf(1.f + sx * sx);
+    }
+    __device__ f3 sample(float u0, float u1, f3 wo) const {
+        bool flip = wo.z < 0;
+        if (flip) wo = neg(wo);
+        f3 ws = normalize3(mk(ax * wo.x, ay * wo.y, wo.z));
+        float sx, sy;
+        sample11(ws.z, u0, u1, sx, sy);
+        float cp = cos_phi(ws), sp = sin_phi(ws);
+        float t = cp * sx - sp * sy;
+        sy = sp * sx + cp * sy;
+        sx = t;
+        sx = ax * sx;
+        sy = ay * sy;
+        f3 r = normalize3(mk(-sx, -sy, 1.f));
+        if (flip) r = neg(r);
+        return r;
+    }
+};
+
+// Schlick Fresnel (BSDFs/Fresnel.h)
+__device__ inline f3 schlick(float cos_t, f3 f0) {
+    float t = pow5(1 - fabsf(cos_t));
+    return f0 + (mk(1, 1, 1) - f0) * t;
+}
+
+// ------------------------------------------------------------------------ BSDF
+struct Bsdf {
+    int type;       // pbrt material type
+    f3 kd, ks, kr, kt;
+    GGX ggx;
+    f3 f0;          // Fresnel f0
+    float eta;      // glass: aboveIOR = 1, belowIOR = eta
+    float mirror;   // mirror reflectivity
+    __device__ bool is_delta() const { return type == cavpbrt::kGlass || type == cavpbrt::kMirror; }
+
+    // ---- Lambertian
+    __device__ f3 lam_eval(f3 wi, f3 wo, f3 c) const { return same_hemisphere(wi, wo) ? c / kPi : mk(0, 0, 0); }
+    // ---- microfacet reflection (plastic specular)
+    __device__ f3 mf_eval(f3 wi, f3 wo) const {
+        if (!same_hemisphere(wi, wo)) return mk(0, 0, 0);
+        float co = fabsf(wo.z), ci = fabsf(wi.z);
+        f3 h = wi + wo;
+        if (ci == 0 || co == 0) return mk(0, 0, 0);
+        if (h.x == 0 && h.y == 0 && h.z == 0) return mk(0, 0, 0);
+        h = normalize3(h);
+        f3 F = schlick(dot3(wo, h), f0);
+        return ks * ggx.D(h) * ggx.G(wo, wi) * F / (4 * ci * co);
+    }
+    __device__ float mf_pdf(f3 wi, f3 wo) const {
+        f3 h = normalize3(wi + wo);
+        return ggx.pdf(h, wo) / (4.f * dot3(wo, h));
+    }
+    // ---- specular glass (Specular.h)
+    __device__ static bool refract(f3 in, f3 n, float eta, f3& out) {
+        float ci = dot3(n, in);
+        float s2i = fmaxf(0.f, 1.f - ci * ci);
+        float s2t = eta * eta * s2i;
+        if (s2t >= 1) return false;
+        float ct = sqrtf(1 - s2t);
+        out = eta * neg(in) + (eta * ci - ct) * n;
+        return true;
+    }
+    __device__ float glass_reflect_prob(f3 wo) const {
+        float p = schlick(fabsf(wo.z), f0).x;
+        if (all_zero(kr)) p = 0;
+        else if (all_zero(kt)) p = 1;
+        return p;
+    }
+
+    __device__ f3 eval(f3 wi, f3 wo) const {
+        switch (type) {
+            case cavpbrt::kMatte: return lam_eval(wi, wo, kd);
+            case cavpbrt::kPlastic: return lam_eval(wi, wo, kd) + mf_eval(wi, wo);
+            case cavpbrt::kMirror:
+                if (!(wi.x == -wo.x && wi.y == -wo.y && wi.z == wo.z)) return mk(0, 0, 0);
+                return mk(1, 1, 1) * mirror / fabsf(wi.z);
+            case cavpbrt::kGlass: {
+                if (same_hemisphere(wi, wo)) {
+                    if (!(wi.x == -wo.x && wi.y == -wo.y && wi.z == wo.z)) return mk(0, 0, 0);
+                    return kr * schlick(fabsf(wi.z), f0) / fabsf(wi.z);
+                }
+                float e = wo.z > 0 ? (1.f / eta) : (eta / 1.f);
+                f3 n = mk(0, 0, wo.z < 0 ? -1.f : 1.f);
+                f3 r;
+                if (!refract(wo, n, e, r)) return mk(0, 0, 0);
+                if (!(r.x == wi.x && r.y == wi.y && r.z == wi.z)) return mk(0, 0, 0);
+                return kt * (mk(1, 1, 1) - schlick(fabsf(wi.z), f0)) / fabsf(wi.z);
+            }
+        }
+        return mk(0, 0, 0);
+    }
+
+    __device__ float pdf(f3 wi, f3 wo) const {
+        switch (type) {
+            case cavpbrt::kMatte: return fabsf(wi.z / kPi);
+            case cavpbrt::kPlastic: return 0.5f * fabsf(wi.z / kPi) + 0.5f * mf_pdf(wi, wo);
+            case cavpbrt::kMirror: return (wi.x == -wo.x && wi.y == -wo.y && wi.z == wo.z) ? 1.f : 0.f;
+            case cavpbrt::kGlass: {
+                if (same_hemisphere(wi, wo)) {
+                    if (!(wi.x == -wo.x && wi.y == -wo.y && wi.z == wo.z)) return 0;
+                    return glass_reflect_prob(wo);
+                }
+                float e = wo.z > 0 ? (1.f / eta) : (eta / 1.f);
+                f3 n = mk(0, 0, wo.z < 0 ? -1.f : 1.f);
+                f3 r;
+                if (!refract(wo, n, e, r)) return 0;
+                if (!(r.x == wi.x && r.y == wi.y && r.z == wi.z)) return 0;
+                return 1.f - glass_reflect_prob(wo);
+            }
+        }
+        return 0;
+    }
+
+    // BSDF::sample: returns f, writes wi and pdf
+    __device__ f3 sample(float u0, float u1, f3 wo, f3& wi, float& pdf_out) const {
+        switch (type) {
+            case cavpbrt::kMatte: {
+                wi = cosine_hemisphere(u0, u1);
+                pdf_out = fabsf(wi.z / kPi);
+                if (wo.z < 0) wi.z *= -1;
+                return lam_eval(wi, wo, kd);
+            }
+            case cavpbrt::kPlastic: {
+                if (u0 < 0.5f) {
+                    u0 = u0 * (1.f / 0.5f);
+                    wi = cosine_hemisphere(u0, u1);
+                    if (wo.z < 0) wi.z *= -1;
+                } else {
+                    u0 = (u0 - 0.5f) * (1.f / (1.f - 0.5f));
+                    f3 h = ggx.sample(u0, u1, wo);
+                    wi = 2.0f * h * dot3(h, wo) - wo;  // reflectF
+                }
+                pdf_out = pdf(wi, wo);
+                return eval(wi, wo);
+            }
+            case cavpbrt::kMirror: {
+                wi = neg(wo);
+                wi.z = wo.z;
+                pdf_out = 1;
+                return eval(wi, wo);
+            }
+            case cavpbrt::kGlass: {
+                float p = glass_reflect_prob(wo);
+                if (u0 < p) {
+                    wi = mk(-wo.x, -wo.y, wo.z);
+                    pdf_out = 1 * p;
+                    return same_hemisphere(wi, wo) ? kr * schlick(fabsf(wi.z), f0) / fabsf(wi.z) : mk(0, 0, 0);
+                }
+                float e = wo.z > 0 ? (1.f / eta) : (eta / 1.f);
+                f3 n = mk(0, 0, wo.z < 0 ? -1.f : 1.f);
+                if (!refract(wo, n, e, wi)) {
+                    pdf_out = 0;  // left as set before the reference's early return
+                    return mk(0, 0, 0);
+                }
+                pdf_out = 1 * (1.f - p);
+                return same_hemisphere(wi, wo) ? mk(0, 0, 0) : kt * (mk(1, 1, 1) - schlick(fabsf(wi.z), f0)) / fabsf(wi.z);
+            }
+        }
+        pdf_out = 0;
+        return mk(0, 0, 0);
+    }
+};
+
+__device__ inline float mis_power(float a, float b) {
+    a *= a;
+    b *= b;
+    return a / (a + b);
+}
+
+// ------------------------------------------------------------------------ scene
+struct DevScene {
+    const float* pos;       // 3 per vertex (global)
+    const int32_t* idx;     // 3 per triangle (global vertex ids)
+    const float* nrm;       // 3 per vertex or nullptr
+    const int32_t* tri_mesh;
+    const RMesh* meshes;
+    const RMaterial* mats;
+    const RLight* lights;
+    int n_lights;
+    Halton halton;
+};
+
+__device__ inline Bsdf make_bsdf(const RMaterial& m) {
+    Bsdf b;
+    b.type = m.type;
+    b.kd = ld3(m.kd);
+    b.ks = ld3(m.ks);
+    b.kr = ld3(m.kr);
+    b.kt = ld3(m.kt);
+    b.ggx = GGX{m.alpha_u, m.alpha_v};
+    f3 e = mk(m.eta, m.eta, m.eta);
+    f3 tmp = (e - mk(1, 1, 1)) / (e + mk(1, 1, 1));
+    b.f0 = tmp * tmp;
+    b.eta = m.eta;
+    b.mirror = m.mirror_kr;
+    return b;
+}
+
+// Triangle normal at (u, v): Core/TriangleMesh.h getNormal / Triangle::fillIntersectionInformation
+__device__ inline f3 tri_normal(const DevScene& S, const RMesh& M, int t, float u, float v) {
+    int a = S.idx[3 * t], b = S.idx[3 * t + 1], c = S.idx[3 * t + 2];
+    f3 n;
+    if (M.has_normals) {
+        f3 n0 = ld3(S.nrm + 3 * a), n1 = ld3(S.nrm + 3 * b), n2 = ld3(S.nrm + 3 * c);
+        n = normalize3(n0 * (1.f - u - v) + u * n1 + v * n2);
+    } else {
+        f3 p0 = ld3(S.pos + 3 * a), p1 = ld3(S.pos + 3 * b), p2 = ld3(S.pos + 3 * c);
+        n = normalize3(cross3(p1 - p0, p2 - p0));
+    }
+    if (M.reverse) n = n * -1.f;
+    return n;
+}
+
+// ---------------------------------------------------------------- path state
+struct Paths {
+    uint64_t* sample_index;
+    float2* film_xy;
+    float* result;      // 3 per path
+    float* throughput;  // 3 per path
+    float* mat_pdf;
+    uint8_t* delta;
+};
+
+struct Queues {
+    int32_t* active;      // path ids of this bounce's rays (compacted)
+    cav_ray* rays;
+    int32_t* next_active;
+    cav_ray* next_rays;
+    int32_t* hit_prim;
+    float* hit_t;
+    float* hit_uv;
+    cav_ray* shadow_rays;
+    float* shadow_limit;
+    int32_t* shadow_excl;  // 2 per shadow ray
+    int32_t* shadow_path;
+    float* shadow_contrib; // 3 per shadow ray
+    uint8_t* shadow_occ;
+    uint32_t* counters;    // [0] next rays, [1] shadow rays
+};
+
+struct Camera {
+    float c2w[16];
+    float depth;
+    int width, height;
+};
+
+__device__ inline f3 apply_pt(const float* m, f3 v) {
+    float t0 = m[0] * v.x + m[4] * v.y + m[8] * v.z + m[12];
+    float t1 = m[1] * v.x + m[5] * v.y + m[9] * v.z + m[13];
+    float t2 = m[2] * v.x + m[6] * v.y + m[10] * v.z + m[14];
+    float t3 = m[3] * v.x + m[7] * v.y + m[11] * v.z + m[15];
+    return mk(t0 / t3, t1 / t3, t2 / t3);
+}
+
+// genCameraSampleSPPs (Core/Sampler.cu:29-51) + genInitialRays (PathTracingIntegrator.cu:252-266)
+__global__ void k_generate(Camera cam, Halton H, int spp, int64_t first, int64_t count, Paths P, Queues Q) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    int64_t s = first + i;  // global sample number, pixel-major
+    int64_t pixel = s / spp;
+    int x = (int)(pixel % cam.width), y = (int)(pixel / cam.width);
+    uint64_t index = (uint64_t)pixel * spp + (uint64_t)(s % spp);
+    int dim = 0;
+    float sx = x + halton(H, index, dim);
+    float sy = y + halton(H, index, dim);
+    f3 pl = mk(sx - cam.width / 2.f, cam.height / 2.f - sy, cam.depth);
+    f3 o = apply_pt(cam.c2w, mk(0, 0, 0));
+    f3 d = normalize3(apply_pt(cam.c2w, pl) - o);
+    P.sample_index[i] = index;
+    P.film_xy[i] = make_float2(sx, sy);
+    P.result[3 * i] = P.result[3 * i + 1] = P.result[3 * i + 2] = 0.f;
+    P.throughput[3 * i] = P.throughput[3 * i + 1] = P.throughput[3 * i + 2] = 1.f;
+    P.mat_pdf[i] = 1.f;
+    P.delta[i] = 1;
+    Q.active[i] = (int32_t)i;
+    Q.rays[i] = cav_ray{o.x, o.y, o.z, 0.f, d.x, d.y, d.z, INFINITY};
+}
+
+__device__ inline uint32_t warp_append(uint32_t* counter, bool pred) {
+    unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (m == 0) return 0;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+// intersectScene + computeLighting + genNextRay (PathTracingIntegrator.cu:95-225) for one
+// bounce; the shadow ray is traced in a separate any-hit launch and its contribution added
+// by k_add_direct (evalMaterial, :227-249, is folded in here).
+__global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Queues Q) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = j < n;
+    int path = valid ? Q.active[j] : 0;
+    int prim = valid ? Q.hit_prim[j] : -1;
+    bool hit = valid && prim >= 0;
+    bool emit_shadow = false, cont = false;
+    cav_ray shadow{}, next{};
+    float limit = 0.f;
+    int2 excl = make_int2(-1, -1);
+    f3 contrib = mk(0, 0, 0);
+    f3 thr = mk(0, 0, 0);
+    float next_pdf = 0.f;
+    bool next_delta = false;
+    if (hit) {
+        const cav_ray r = Q.rays[j];
+        f3 ro = mk(r.ox, r.oy, r.oz), rd = mk(r.dx, r.dy, r.dz);
+        float t = Q.hit_t[j];
+        float u = Q.hit_uv[2 * j], v = Q.hit_uv[2 * j + 1];
+        uint64_t index = P.sample_index[path];
+        thr = ld3(P.throughput + 3 * path);
+        f3 res = ld3(P.result + 3 * path);
+        const int mesh = S.tri_mesh[prim];
+        const RMesh& M = S.meshes[mesh];
+        f3 pos = ro + t * rd;  // Ray::positionAtDistance
+        f3 nrm = tri_normal(S, M, prim, u, v);
+        // ---- emission at the hit (computeLighting :190-205)
+        if (M.light >= 0) {
+            const RLight& L = S.lights[M.light];
+            f3 Le = dot3(rd, nrm) >= 0 ? mk(0, 0, 0) : ld3(L.L);
+            if (P.delta[path]) {
+                res = res + Le * thr;
+            } else if (depth > 0) {
+                f3 l2s = ro - pos;
+                float cosine = fabsf(dot3(nrm, normalize3(l2s)));
+                float light_pdf = dot3(l2s, l2s) / (cosine * S.meshes[L.mesh].area);
+                float w = mis_power(P.mat_pdf[path], light_pdf);
+                if (isfinite(w)) res = res + Le * thr * w;
+            }
+        }
+        P.result[3 * path] = res.x;
+        P.result[3 * path + 1] = res.y;
+        P.result[3 * path + 2] = res.z;
+        const Bsdf B = make_bsdf(S.mats[M.material]);
+        const Frame fr = make_frame(nrm);
+        const f3 wo_world = rd * -1.f;
+        const f3 wo = to_local(fr, wo_world);
+        // ---- light sample (computeLighting :207-224)
+        int dim = dim0;
+        int li = halton_int(S.halton, index, dim, S.n_lights);
+        dim += 4;  // rand4, drawn and unused by the reference
+        const RLight& L = S.lights[li];
+        const RMesh& LM = S.meshes[L.mesh];
+        int lt = LM.first_tri + halton_int(S.halton, index, dim, LM.tri_count);
+        float temp = sqrtf(halton(S.halton, index, dim));
+        float su = 1 - temp;
+        float sv = temp * halton(S.halton, index, dim);
+        int a = S.idx[3 * lt], b = S.idx[3 * lt + 1], c = S.idx[3 * lt + 2];
+        f3 lp = ld3(S.pos + 3 * a) * su + ld3(S.pos + 3 * b) * sv + ld3(S.pos + 3 * c) * (1.f - su - sv);
+        f3 ln = tri_normal(S, LM, lt, su, sv);
+        f3 l2s = pos - lp;
+        float lcos = fabsf(dot3(ln, normalize3(l2s)));
+        float light_pdf = dot3(l2s, l2s) / (lcos * LM.area);
+        f3 dir = normalize3(lp - pos);
+        f3 incident = dot3(dir, ln) >= 0 ? mk(0, 0, 0) : ld3(L.L);
+        if (isfinite(light_pdf)) {
+            f3 wi = to_local(fr, dir);
+            float bsdf_pdf = B.pdf(wi, wo);
+            float w = mis_power(light_pdf, bsdf_pdf);
+            float cosine = fabsf(dot3(dir, nrm));
+            f3 mult = thr * (float)S.n_lights / light_pdf;
+            contrib = incident * B.eval(wi, wo) * cosine * mult * w;
+            if (!all_zero(contrib)) {
+                emit_shadow = true;
+                shadow = cav_ray{pos.x, pos.y, pos.z, 0.f, dir.x, dir.y, dir.z, INFINITY};
+                limit = length3(lp - pos);
+                excl = make_int2(mesh, L.mesh);
+            }
+        }
+        // ---- continuation (genNextRay :124-171)
+        dim = dim0 + 8;
+        bool alive = true;
+        if (depth > 3) {
+            float q = 1;
+            q = fminf(q, 1 - thr.x);
+            q = fminf(q, 1 - thr.y);
+            q = fminf(q, 1 - thr.z);
+            q = fmaxf(q, 0.05f);
+            if (halton(S.halton, index, dim) < q) alive = false;
+            else thr = thr / (1.f - q);
+        }
+        if (alive) {
+            float u0 = halton(S.halton, index, dim);
+            float u1 = halton(S.halton, index, dim);
+            f3 wi;
+            float p = 0.f;
+            f3 f = B.sample(u0, u1, wo, wi, p);
+            f3 nd = to_world(fr, wi);
+            f3 no = pos + nd * 0.001f;
+            if (all_zero(f)) thr = mk(0, 0, 0);
+            else thr = thr * f * fabsf(dot3(nd, nrm)) / p;
+            next_pdf = p;
+            next_delta = B.is_delta();
+            // A path whose throughput is exactly zero adds nothing on later bounces; the
+            // reference traces it anyway, this queue drops it.
+            if (!all_zero(thr)) {
+                cont = true;
+                next = cav_ray{no.x, no.y, no.z, 0.f, nd.x, nd.y, nd.z, INFINITY};
+            }
+        }
+    }
+    uint32_t ks = warp_append(Q.counters + 1, emit_shadow);
+    if (emit_shadow) {
+        Q.shadow_rays[ks] = shadow;
+        Q.shadow_limit[ks] = limit;
+        reinterpret_cast<int2*>(Q.shadow_excl)[ks] = excl;
+        Q.shadow_path[ks] = path;
+        Q.shadow_contrib[3 * ks] = contrib.x;
+        Q.shadow_contrib[3 * ks + 1] = contrib.y;
+        Q.shadow_contrib[3 * ks + 2] = contrib.z;
+    }
+    uint32_t kn = warp_append(Q.counters + 0, cont);
+    if (cont) {
+        Q.next_active[kn] = path;
+        Q.next_rays[kn] = next;
+        P.throughput[3 * path] = thr.x;
+        P.throughput[3 * path + 1] = thr.y;
+        P.throughput[3 * path + 2] = thr.z;
+        P.mat_pdf[path] = next_pdf;
+        P.delta[path] = next_delta ? 1 : 0;
+    }
+}
+
+// evalMaterial's accumulation for unoccluded shadow rays.  The paths of one bounce are
+// distinct, so plain read-modify-write is race free.
+__global__ void k_add_direct(int64_t n, Paths P, Queues Q) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (Q.shadow_occ[k] != 0) return;
+    int path = Q.shadow_path[k];
+    P.result[3 * path] += Q.shadow_contrib[3 * k];
+    P.result[3 * path + 1] += Q.shadow_contrib[3 * k + 1];
+    P.result[3 * path + 2] += Q.shadow_contrib[3 * k + 2];
+}
+
+// addSamplesToFilm + Film::addSample (Core/Film.h:26-49) with the box filter of
+// Filters/BoxFilter.h ("triangle" maps to it, Filters/FilterObject.h:83-84).
+__global__ void k_film(int64_t n, Paths P, int width, int height, float xw, float yw, float* sum, float* wsum) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f3 s = ld3(P.result + 3 * i);
+    if (!finite3(s)) return;
+    float2 xy = P.film_xy[i];
+    int x0 = (int)floorf(xy.x - xw), x1 = (int)ceilf(xy.x + xw);
+    int y0 = (int)floorf(xy.y - yw), y1 = (int)ceilf(xy.y + yw);
+    for (int x = x0; x <= x1; ++x)
+        for (int y = y0; y <= y1; ++y) {
+            if (x >= width || y >= height || x < 0 || y < 0) continue;
+            float wgt = (fabsf(x - xy.x) > xw || fabsf(y - xy.y) > yw) ? 0.f : 1.f;
+            if (wgt > 0) {
+                int idx = y * width + x;
+                atomicAdd(sum + 3 * idx, s.x * wgt);
+                atomicAdd(sum + 3 * idx + 1, s.y * wgt);
+                atomicAdd(sum + 3 * idx + 2, s.z * wgt);
+                atomicAdd(wsum + idx, wgt);
+            }
+        }
+}
+
+template <typename T>
+T* carve(unsigned char*& p, size_t count) {
+    size_t off = ((uintptr_t)p + 255) & ~(uintptr_t)255;
+    T* r = reinterpret_cast<T*>(off);
+    p = reinterpret_cast<unsigned char*>(off + sizeof(T) * count);
+    return r;
+}
+
+// Permutation tables of HaltonSampler.cu:14-67: the first 1024 primes; one Fisher-Yates
+// shuffle per prime driven by the C library's rand() after srand(533799).
+void build_halton_tables(std::vector<uint32_t>& primes, std::vector<uint32_t>& start, std::vector<uint16_t>& perms) {
+    primes.clear();
+    primes.push_back(2);
+    for (uint32_t i = 3; primes.size() < (size_t)kPrimes; ++i) {
+        bool is_prime = true;
+        for (uint32_t p : primes) {
+            if (p * p > i) break;
+            if (i % p == 0) {
+                is_prime = false;
+                break;
+            }
+        }
+        if (is_prime) primes.push_back(i);
+    }
+    start.assign(primes.size(), 0);
+    size_t size = 0;
+    for (size_t k = 0; k < primes.size(); ++k) {
+        start[k] = (uint32_t)size;
+        size += primes[k];
+    }
+    perms.assign(size, 0);
+    std::srand(533799);
+    for (size_t k = 0; k < primes.size(); ++k) {
+        uint32_t p = primes[k];
+        std::vector<uint16_t> v(p);
+        for (uint32_t j = 0; j < p; ++j) v[j] = (uint16_t)j;
+        for (int m = (int)p - 1; m > 0; --m) std::swap(v[m], v[std::rand() % (m + 1)]);
+        std::memcpy(&perms[start[k]], v.data(), p * sizeof(uint16_t));
+    }
+}
+
+}  // namespace
+}  // namespace cav
+
+// =================================================================== host objects
+struct cav_scene {
+    int device = 0;
+    cavpbrt::Scene desc;
+    int64_t n_tri = 0, n_vert = 0;
+    float* d_pos = nullptr;
+    int32_t* d_idx = nullptr;
+    float* d_nrm = nullptr;
+    int32_t* d_tri_mesh = nullptr;
+    cav::RMesh* d_meshes = nullptr;
+    cav::RMaterial* d_mats = nullptr;
+    cav::RLight* d_lights = nullptr;
+    uint32_t* d_primes = nullptr;
+    uint32_t* d_perm_start = nullptr;
+    uint16_t* d_perms = nullptr;
+    cav_bvh* bvh = nullptr;
+    int bvh_rounds = 0;
+};
+
+namespace cav {
+
+static cav_status upload(cav_ctx* ctx, void** dst, const void* src, size_t bytes) {
+    CAV_CUDA(ctx, cudaMalloc(dst, bytes > 0 ? bytes : 16));
+    if (bytes) CAV_CUDA(ctx, cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    return CAV_OK;
+}
+
+cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, cav_scene** out) {
+    auto sc = new cav_scene();
+    sc->device = ctx->device;
+    sc->desc = std::move(desc);
+    const cavpbrt::Scene& D = sc->desc;
+    std::vector<float> pos, nrm;
+    std::vector<int32_t> idx, tri_mesh;
+    std::vector<RMesh> meshes;
+    bool any_normals = false;
+    for (const auto& m : D.meshes) any_normals |= !m.normals.empty();
+    for (size_t mi = 0; mi < D.meshes.size(); ++mi) {
+        const auto& m = D.meshes[mi];
+        RMesh rm{};
+        rm.first_tri = (int32_t)(idx.size() / 3);
+        rm.tri_count = (int32_t)(m.indices.size() / 3);
+        rm.has_normals = m.normals.empty() ? 0 : 1;
+        rm.reverse = m.reverse_orientation ? 1 : 0;
+        rm.material = m.material;
+        rm.light = m.light;
+        // TriangleMesh::computeArea (Core/TriangleMesh.cu:189-199): float sum of half cross lengths
+        float area = 0.f;
+        for (size_t t = 0; t < m.indices.size() / 3; ++t) {
+            const float* p0 = &m.positions[3 * m.indices[3 * t]];
+            const float* p1 = &m.positions[3 * m.indices[3 * t + 1]];
+            const float* p2 = &m.positions[3 * m.indices[3 * t + 2]];
+            float e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+            float e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+            float c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+            area += std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]) * 0.5f;
+        }
+        rm.area = area;
+        int32_t vbase = (int32_t)(pos.size() / 3);
+        pos.insert(pos.end(), m.positions.begin(), m.positions.end());
+        if (any_normals) {
+            if (m.normals.empty()) nrm.insert(nrm.end(), m.positions.size(), 0.f);
+            else nrm.insert(nrm.end(), m.normals.begin(), m.normals.end());
+        }
+        for (int v : m.indices) idx.push_back(v + vbase);
+        for (int t = 0; t < rm.tri_count; ++t) tri_mesh.push_back((int32_t)mi);
+        meshes.push_back(rm);
+    }
+    std::vector<RMaterial> mats;
+    for (const auto& m : D.materials) {
+        RMaterial r{};
+        r.type = m.type;
+        for (int k = 0; k < 3; ++k) {
+            r.kd[k] = m.kd[k];
+            r.ks[k] = m.ks[k];
+            r.kr[k] = m.kr[k];
+            r.kt[k] = m.kt[k];
+        }
+        r.alpha_u = m.alpha_u;
+        r.alpha_v = m.alpha_v;
+        r.eta = m.eta;
+        r.mirror_kr = m.mirror_kr;
+        mats.push_back(r);
+    }
+    std::vector<RLight> lights;
+    for (const auto& l : D.lights) lights.push_back(RLight{{l.L[0], l.L[1], l.L[2]}, l.mesh});
+    std::vector<uint32_t> primes, start;
+    std::vector<uint16_t> perms;
+    build_halton_tables(primes, start, perms);
+    sc->n_tri = (int64_t)idx.size() / 3;
+    sc->n_vert = (int64_t)pos.size() / 3;
+    cav_status st = CAV_OK;
+    if ((st = upload(ctx, (void**)&sc->d_pos, pos.data(), pos.size() * 4)) ||
+        (st = upload(ctx, (void**)&sc->d_idx, idx.data(), idx.size() * 4)) ||
+        (st = upload(ctx, (void**)&sc->d_tri_mesh, tri_mesh.data(), tri_mesh.size() * 4)) ||
+        (st = upload(ctx, (void**)&sc->d_meshes, meshes.data(), meshes.size() * sizeof(RMesh))) ||
+        (st = upload(ctx, (void**)&sc->d_mats, mats.data(), mats.size() * sizeof(RMaterial))) ||
+        (st = upload(ctx, (void**)&sc->d_lights, lights.data(), lights.size() * sizeof(RLight))) ||
+        (st = upload(ctx, (void**)&sc->d_primes, primes.data(), primes.size() * 4)) ||
+        (st = upload(ctx, (void**)&sc->d_perm_start, start.data(), start.size() * 4)) ||
+        (st = upload(ctx, (void**)&sc->d_perms, perms.data(), perms.size() * 2))) {
+        cav_scene_free(sc);
+        return st;
+    }
+    if (any_normals && (st = upload(ctx, (void**)&sc->d_nrm, nrm.data(), nrm.size() * 4))) {
+        cav_scene_free(sc);
+        return st;
+    }
+    // BVH over the global triangle list; rounds -1 = the reference's default
+    // (3, or 10 when spp >= 64; Core/Scene.cu:141-146)
+    if (bvh_rounds < 0) bvh_rounds = D.spp >= 64 ? 10 : 3;
+    sc->bvh_rounds = bvh_rounds;
+    st = build_bvh(ctx, sc->d_pos, sc->n_vert, sc->d_idx, sc->d_tri_mesh, sc->n_tri, nullptr, bvh_rounds, nullptr,
+                   &sc->bvh);
+    if (st != CAV_OK) {
+        cav_scene_free(sc);
+        return st;
+    }
+    CAV_CUDA(ctx, cudaDeviceSynchronize());
+    *out = sc;
+    return CAV_OK;
+}
+
+cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
+                       cudaStream_t s) {
+    const cavpbrt::Scene& D = sc->desc;
+    const int spp = opts && opts->spp > 0 ? opts->spp : D.spp;
+    const int max_depth = opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth;
+    const int64_t pixels = (int64_t)D.width * D.height;
+    const int64_t total = pixels * spp;
+    int64_t chunk = opts && opts->max_paths_in_flight > 0 ? opts->max_paths_in_flight : (int64_t)1 << 22;
+    chunk = std::min(chunk, total);
+    // path state + queues for `chunk` paths
+    size_t need = 0;
+    auto acc = [&](size_t bytes) { need += bytes + 256; };
+    acc(8 * chunk); acc(8 * chunk); acc(12 * chunk); acc(12 * chunk); acc(4 * chunk); acc(chunk);
+    acc(4 * chunk); acc(32 * chunk); acc(4 * chunk); acc(32 * chunk);
+    acc(4 * chunk); acc(4 * chunk); acc(8 * chunk);
+    acc(32 * chunk); acc(4 * chunk); acc(8 * chunk); acc(4 * chunk); acc(12 * chunk); acc(chunk); acc(64);
+    void* base = nullptr;
+    CAV_CUDA(ctx, cudaMallocAsync(&base, need, s));
+    unsigned char* p = (unsigned char*)base;
+    Paths P;
+    P.sample_index = carve<uint64_t>(p, chunk);
+    P.film_xy = carve<float2>(p, chunk);
+    P.result = carve<float>(p, 3 * chunk);
+    P.throughput = carve<float>(p, 3 * chunk);
+    P.mat_pdf = carve<float>(p, chunk);
+    P.delta = carve<uint8_t>(p, chunk);
+    Queues Q;
+    Q.active = carve<int32_t>(p, chunk);
+    Q.rays = carve<cav_ray>(p, chunk);
+    Q.next_active = carve<int32_t>(p, chunk);
+    Q.next_rays = carve<cav_ray>(p, chunk);
+    Q.hit_prim = carve<int32_t>(p, chunk);
+    Q.hit_t = carve<float>(p, chunk);
+    Q.hit_uv = carve<float>(p, 2 * chunk);
+    Q.shadow_rays = carve<cav_ray>(p, chunk);
+    Q.shadow_limit = carve<float>(p, chunk);
+    Q.shadow_excl = carve<int32_t>(p, 2 * chunk);
+    Q.shadow_path = carve<int32_t>(p, chunk);
+    Q.shadow_contrib = carve<float>(p, 3 * chunk);
+    Q.shadow_occ = carve<uint8_t>(p, chunk);
+    Q.counters = carve<uint32_t>(p, 16);
+
+    DevScene S;
+    S.pos = sc->d_pos;
+    S.idx = sc->d_idx;
+    S.nrm = sc->d_nrm;
+    S.tri_mesh = sc->d_tri_mesh;
+    S.meshes = sc->d_meshes;
+    S.mats = sc->d_mats;
+    S.lights = sc->d_lights;
+    S.n_lights = (int)D.lights.size();
+    S.halton = Halton{sc->d_primes, sc->d_perm_start, sc->d_perms};
+    Camera cam;
+    std::memcpy(cam.c2w, D.camera_to_world.data(), 64);
+    cam.width = D.width;
+    cam.height = D.height;
+    {  // PerspectiveCamera constructor (Cameras/PerspectiveCamera.cu:6-20)
+        float fov = D.fov_deg * 3.14159265358979323846f / 180.f;
+        if (D.height <= D.width) cam.depth = (D.height / 2.f) / std::tan(fov / 2.f);
+        else cam.depth = (D.width / 2.f) / std::tan(fov / 2.f);
+    }
+    uint32_t counts[2];
+    for (int64_t first = 0; first < total; first += chunk) {
+        const int64_t m = std::min(chunk, total - first);
+        k_generate<<<div_up(m, kThreads), kThreads, 0, s>>>(cam, S.halton, spp, first, m, P, Q);
+        int64_t n = m;
+        int dim0 = 2;
+        for (int depth = 0; n > 0 && depth < max_depth; ++depth) {
+            cav_status st = trace_closest(ctx, sc->bvh, Q.rays, n, Q.hit_prim, Q.hit_t, Q.hit_uv, CAV_TRACE_EXACT, s,
+                                          ctx->d_counters + 6);
+            if (st != CAV_OK) return st;
+            CAV_CUDA(ctx, cudaMemsetAsync(Q.counters, 0, 8, s));
+            k_shade<<<div_up(n, kThreads), kThreads, 0, s>>>(S, depth, dim0, n, P, Q);
+            CAV_CUDA(ctx, cudaMemcpyAsync(counts, Q.counters, 8, cudaMemcpyDeviceToHost, s));
+            CAV_CUDA(ctx, cudaStreamSynchronize(s));
+            if (counts[1] > 0) {
+                st = trace_any(ctx, sc->bvh, Q.shadow_rays, Q.shadow_limit, Q.shadow_excl, counts[1], Q.shadow_occ,
+                               CAV_TRACE_EXACT, s, ctx->d_counters + 7);
+                if (st != CAV_OK) return st;
+                k_add_direct<<<div_up(counts[1], kThreads), kThreads, 0, s>>>(counts[1], P, Q);
+            }
+            std::swap(Q.active, Q.next_active);
+            std::swap(Q.rays, Q.next_rays);
+            n = counts[0];
+            dim0 += 8 + 2 + (depth > 3 ? 1 : 0);
+        }
+        k_film<<<div_up(m, kThreads), kThreads, 0, s>>>(m, P, D.width, D.height, D.filter_xwidth, D.filter_ywidth,
+                                                         d_sum, d_wsum);
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    CAV_CUDA(ctx, cudaFreeAsync(base, s));
+    return CAV_OK;
+}
+
+}  // namespace cav
+
+// ======================================================================== C ABI
+extern "C" {
+
+cav_status cav_scene_load_pbrt(cav_ctx* ctx, const char* path, int spp_override, const char* integrator_override,
+                               int bvh_rounds, cav_scene** out) {
+    if (!ctx || !path || !out) return CAV_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return cav::cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
+    cavpbrt::Overrides ov;
+    ov.spp = spp_override;
+    if (integrator_override) ov.integrator = integrator_override;
+    cavpbrt::Scene desc;
+    try {
+        desc = cavpbrt::load_file(path, ov);
+    } catch (const std::exception& e) {
+        return cav::set_error(ctx, CAV_ERR_INVALID_ARGUMENT, std::string("pbrt: ") + e.what());
+    }
+    return cav::scene_from_desc(ctx, std::move(desc), bvh_rounds, out);
+}
+
+cav_status cav_scene_free(cav_scene* sc) {
+    if (!sc) return CAV_OK;
+    cudaSetDevice(sc->device);
+    cav_bvh_free(sc->bvh);
+    cudaFree(sc->d_pos);
+    cudaFree(sc->d_idx);
+    cudaFree(sc->d_nrm);
+    cudaFree(sc->d_tri_mesh);
+    cudaFree(sc->d_meshes);
+    cudaFree(sc->d_mats);
+    cudaFree(sc->d_lights);
+    cudaFree(sc->d_primes);
+    cudaFree(sc->d_perm_start);
+    cudaFree(sc->d_perms);
+    delete sc;
+    return CAV_OK;
+}
+
+cav_status cav_scene_info(const cav_scene* sc, cav_scene_info_t* info) {
+    if (!sc || !info) return CAV_ERR_INVALID_ARGUMENT;
+    info->width = sc->desc.width;
+    info->height = sc->desc.height;
+    info->spp = sc->desc.spp;
+    info->max_depth = sc->desc.max_depth;
+    info->triangles = sc->n_tri;
+    info->meshes = (int)sc->desc.meshes.size();
+    info->lights = (int)sc->desc.lights.size();
+    info->bvh_rounds = sc->bvh_rounds;
+    info->integrator = sc->desc.integrator == "rlpath" ? 1 : 0;
+    return CAV_OK;
+}
+
+const cav_bvh* cav_scene_bvh(const cav_scene* sc) { return sc ? sc->bvh : nullptr; }
+
+cav_status cav_render(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* film_sum, float* film_weight,
+                      void* stream) {
+    if (!ctx || !sc || !film_sum || !film_weight) return CAV_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return cav::cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t pixels = (int64_t)sc->desc.width * sc->desc.height;
+    CAV_CUDA(ctx, cudaMemsetAsync(film_sum, 0, sizeof(float) * 3 * pixels, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(film_weight, 0, sizeof(float) * pixels, s));
+    int integrator = opts ? opts->integrator : (sc->desc.integrator == "rlpath" ? 1 : 0);
+    if (integrator != 0) return cav::set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "only the path integrator is built");
+    return cav::render_path(ctx, sc, opts, film_sum, film_weight, s);
+}
+
+cav_status cav_render_to_host(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* host_sum,
+                              float* host_weight, float* ms_out) {
+    if (!ctx || !sc || !host_sum || !host_weight) return CAV_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return cav::cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
+    const int64_t pixels = (int64_t)sc->desc.width * sc->desc.height;
+    float* d = nullptr;
+    CAV_CUDA(ctx, cudaMalloc(&d, sizeof(float) * 4 * pixels));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, nullptr);
+    cav_status st = cav_render(ctx, sc, opts, d, d + 3 * pixels, nullptr);
+    cudaEventRecord(b, nullptr);
+    if (st == CAV_OK) {
+        cudaError_t e = cudaMemcpy(host_sum, d, sizeof(float) * 3 * pixels, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(host_weight, d + 3 * pixels, sizeof(float) * pixels, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = cav::cuda_error(ctx, e, "cudaMemcpy film");
+        if (ms_out) cudaEventElapsedTime(ms_out, a, b);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    return st;
+}
+
+}  // extern "C"

@@ -416,7 +416,7 @@ cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int
                           cudaStream_t s) {
     if (rounds <= 0) return CAV_OK;
     const int64_t count = 2 * n - 1;
-    uint32_t* counter = reinterpret_cast<uint32_t*>(ctx->d_counters) + 8;  // scratch word in the ctx block
+    uint32_t* counter = reinterpret_cast<uint32_t*>(ctx->d_counters + 20);  // ctx counter slot 20
     for (int r = 0; r < rounds; ++r) {
         CAV_CUDA(ctx, cudaMemsetAsync(visited, 0, sizeof(uint32_t) * count, s));
         CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), s));

@@ -116,7 +116,8 @@ def mini_room():
     v, t = _box_triangles((0.6, 1.2, 0.6), -18.0, (-0.35, -1.0, 0.3))
     add(v, t, "tall_box", grey)
     y = 0.999
-    add([[-0.25, y, -0.25], [0.25, y, -0.25], [0.25, y, 0.25], [-0.25, y, 0.25]], [(0, 2, 1), (0, 3, 2)], "light",
+    # wound so that the face normal points down into the room (the light emits on that side)
+    add([[-0.25, y, -0.25], [0.25, y, -0.25], [0.25, y, 0.25], [-0.25, y, 0.25]], [(0, 1, 2), (0, 2, 3)], "light",
         (0.0, 0.0, 0.0))
     return {
         "positions": np.ascontiguousarray(np.concatenate(verts).astype(np.float32)),
@@ -125,3 +126,50 @@ def mini_room():
         "meshes": meshes,
         "light_radiance": (17.0, 12.0, 4.0),
     }
+
+
+def _num(x: float) -> str:
+    """A number the reference's lexer accepts: characters [0-9.-e] only (no '+')."""
+    t = "%.9g" % float(x)
+    if "+" in t or "inf" in t or "nan" in t:
+        t = ("%.6f" % float(x)).rstrip("0").rstrip(".")
+    return t
+
+
+def _nums(v) -> str:
+    return " ".join(_num(x) for x in np.asarray(v).reshape(-1))
+
+
+def write_pbrt(path, room: dict, *, width=256, height=256, spp=16, max_depth=5, fov=40.0,
+               eye=(0.0, 0.0, -3.8), look=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), integrator="path"):
+    """Write a scene dict (as returned by mini_room) as a .pbrt file in the subset the
+    reference's loader reads (SceneLoading/Lexing.cu, Parsing.cu): one trianglemesh Shape per
+    mesh, matte materials, the light mesh as a diffuse AreaLightSource."""
+    pos, idx = room["positions"], room["indices"]
+    lines = [
+        f"LookAt {_nums(eye)}  {_nums(look)}  {_nums(up)}",
+        f'Camera "perspective" "float fov" [{_num(fov)}]',
+        f'Film "image" "integer xresolution" [{width}] "integer yresolution" [{height}] "string filename" "out.png"',
+        f'Sampler "halton" "integer pixelsamples" [{spp}]',
+        f'Integrator "{integrator}" "integer maxdepth" [{max_depth}]',
+        'PixelFilter "box"',
+        "WorldBegin",
+    ]
+    L = room.get("light_radiance", (17.0, 12.0, 4.0))
+    for name, first, count, mat in room["meshes"]:
+        tris = idx[first:first + count]
+        used = np.unique(tris)
+        remap = {int(v): k for k, v in enumerate(used)}
+        P = pos[used]
+        I = np.vectorize(remap.get)(tris)
+        lines.append("AttributeBegin")
+        if name == "light":
+            lines.append(f'AreaLightSource "diffuse" "rgb L" [{_nums(L)}]')
+            lines.append('Material "matte" "rgb Kd" [0 0 0]')
+        else:
+            lines.append(f'Material "matte" "rgb Kd" [{_nums(mat)}]')
+        lines.append(f'Shape "trianglemesh" "integer indices" [{_nums(I)}] "point P" [{_nums(P)}]')
+        lines.append("AttributeEnd")
+    lines.append("WorldEnd")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")

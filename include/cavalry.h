@@ -187,6 +187,57 @@ cav_status cav_morton_sort_noalloc(const float* positions, int64_t num_vertices,
                                    int64_t num_triangles, const float* scene_bounds, uint64_t* sorted_codes,
                                    int32_t* sorted_prims, void* stream);
 
+/*
+ * Scenes and rendering: the reference's Integrator::render (Integrators/PathTracingIntegrator.cu
+ * :318-425) over a scene loaded from a .pbrt file by the host parser (SceneLoading/Lexing.cu,
+ * SceneLoading/Parsing.cu), behind the CLI surface of main.cu:25-96.
+ */
+typedef struct cav_scene cav_scene;
+
+typedef struct cav_scene_info_t {
+    int width, height, spp, max_depth;
+    int64_t triangles;
+    int meshes, lights, bvh_rounds;
+    int integrator; /* 0 = path, 1 = rlpath */
+} cav_scene_info_t;
+
+typedef struct cav_render_opts {
+    int spp;                     /* <= 0: the scene's Sampler "pixelsamples" */
+    int max_depth;               /* <= 0: the scene's Integrator "maxdepth" */
+    int integrator;              /* 0 = path (rlpath is not built) */
+    int64_t max_paths_in_flight; /* <= 0: 4M; samples are rendered in chunks of this many paths */
+} cav_render_opts;
+
+/* Host-only .pbrt parse (no GPU): scene counts and the camera-to-world matrix (16 floats,
+ * column-major; may be NULL).  On a parse error returns CAV_ERR_INVALID_ARGUMENT and copies the
+ * message into err (may be NULL).  bvh_rounds in `info` is reported as -1. */
+cav_status cav_pbrt_parse_info(const char* path, int spp_override, const char* integrator_override,
+                               cav_scene_info_t* info, float* camera_to_world16, char* err, int err_len);
+/* Loads a .pbrt scene and builds its BVH.  spp_override > 0 replaces the sampler's
+ * pixelsamples (--spp), integrator_override (or NULL) the integrator name (--integrator),
+ * bvh_rounds the treelet rounds (--bvh-opt-rounds; -1 = 3, or 10 when spp >= 64, as
+ * Core/Scene.cu:141-146).  Parse errors: CAV_ERR_INVALID_ARGUMENT, message in cav_last_error.
+ * Synchronous. */
+cav_status cav_scene_load_pbrt(cav_ctx* ctx, const char* path, int spp_override, const char* integrator_override,
+                               int bvh_rounds, cav_scene** out);
+cav_status cav_scene_free(cav_scene* scene);
+cav_status cav_scene_info(const cav_scene* scene, cav_scene_info_t* info);
+const cav_bvh* cav_scene_bvh(const cav_scene* scene);
+/* Renders into a DEVICE film: film_sum (3 floats per pixel) and film_weight (1 per pixel),
+ * the reference's Film::samplesSum / samplesWeightSum (Core/Film.h:53-54); pixel = sum / weight.
+ * Stream-ordered, except that each bounce reads its queue sizes back to the host. */
+cav_status cav_render(cav_ctx* ctx, cav_scene* scene, const cav_render_opts* opts, float* film_sum,
+                      float* film_weight, void* stream);
+/* Host-film convenience: renders and copies the film to host arrays (3 + 1 floats per pixel);
+ * ms_out (or NULL) receives the render time measured with CUDA events. */
+cav_status cav_render_to_host(cav_ctx* ctx, cav_scene* scene, const cav_render_opts* opts, float* host_sum,
+                              float* host_weight, float* ms_out);
+/* Film -> 8-bit sRGB as the reference's Film::readCurrentResult (Core/Film.cu:20-46); HOST arrays. */
+cav_status cav_film_to_rgb8(const float* film_sum, const float* film_weight, int width, int height, uint8_t* rgb);
+/* Image writers: 8-bit RGB PNG (the reference's output format) and a float PFM of sum/weight. */
+cav_status cav_write_png(const char* path, const uint8_t* rgb, int width, int height);
+cav_status cav_write_pfm(const char* path, const float* film_sum, const float* film_weight, int width, int height);
+
 /* Device-side event timing of the last build's stages (ms): leaf boxes + Morton,
  * sort, radix tree, refit, treelet rounds, layout.  Valid after the stream is synced. */
 cav_status cav_bvh_stage_times(cav_ctx* ctx, const cav_bvh* bvh, float* ms6);
