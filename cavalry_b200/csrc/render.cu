@@ -872,7 +872,10 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
         const int64_t m = std::min(chunk, total - first);
         k_generate<<<div_up(m, kThreads), kThreads, 0, s>>>(cam, S.halton, spp, first, m, P, Q);
         int64_t n = m;
-        int dim0 = 2;
+        // genCameraSampleSPPs stores the sampling state in the CameraSample BEFORE drawing the
+        // two jitter dimensions from its local copy (Core/Sampler.cu:43-47), so a path's
+        // first bounce starts again at dimension 0.
+        int dim0 = 0;
         for (int depth = 0; n > 0 && depth < max_depth; ++depth) {
             cav_status st = trace_closest(ctx, sc->bvh, Q.rays, n, Q.hit_prim, Q.hit_t, Q.hit_uv, CAV_TRACE_EXACT, s,
                                           ctx->d_counters + 6);
