@@ -49,7 +49,15 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    return p.parse_args()
+    p.add_argument("--tris", type=int, default=None, help="soup size (default: the 1M-triangle workload)")
+    p.add_argument("--rays", type=int, default=None, help="rays per step (default: 4M)")
+    a = p.parse_args()
+    g = globals()
+    if a.tris or a.rays:  # a smaller case of the same kernels (profiling)
+        g["N_TRI"] = a.tris or N_TRI
+        g["N_RAYS"] = a.rays or N_RAYS
+        g["WORKLOAD"] = f"soup_{g['N_TRI']}_tris_3_treelet_rounds_{g['N_RAYS']}_closest_rays"
+    return a
 
 
 class ClockSampler:

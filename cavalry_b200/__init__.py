@@ -92,6 +92,7 @@ def lib() -> ctypes.CDLL:
         "cav_scene_free": ([P], ctypes.c_int),
         "cav_scene_info": ([P, P], ctypes.c_int),
         "cav_render_to_host": ([P, P, P, P, P, P], ctypes.c_int),
+        "cav_render": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_film_to_rgb8": ([P, P, ctypes.c_int, ctypes.c_int, P], ctypes.c_int),
         "cav_write_png": ([ctypes.c_char_p, P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "cav_write_pfm": ([ctypes.c_char_p, P, P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -234,6 +235,17 @@ class Scene:
                                       w.ctypes.data, ms.ctypes.data)
         self.ctx._check(st, "cav_render_to_host")
         return s, w, float(ms[0])
+
+    def render_into(self, film_sum, film_weight, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0,
+                    stream=None):
+        """Render into DEVICE films (pointers, or objects with data_ptr(): 3 + 1 floats per
+        pixel), stream-ordered on `stream` (a pointer, an object with cuda_stream, or None)."""
+        ptr = lambda x: x if isinstance(x, int) else x.data_ptr()  # noqa: E731
+        st_ptr = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
+        opts = RenderOpts(spp, max_depth, 0, max_paths_in_flight)
+        st = lib().cav_render(self.ctx.handle, self.handle, ctypes.addressof(opts), ptr(film_sum), ptr(film_weight),
+                              st_ptr)
+        self.ctx._check(st, "cav_render")
 
     def free(self):
         if self.handle:

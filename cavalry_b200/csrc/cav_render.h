@@ -17,6 +17,8 @@ struct RMaterial {
     int32_t type;
     float kd[3], ks[3], kr[3], kt[3];
     float alpha_u, alpha_v, eta, mirror_kr;
+    float f0[3];  // Schlick f0 of Fresnel::createFromIOR, computed on the host as the reference does
+    int32_t pad;
 };
 
 struct RLight {

@@ -33,6 +33,9 @@ namespace cav {
 namespace {
 
 constexpr float kPi = 3.14159265358979323846f;
+constexpr double kPiD = 3.14159265358979323846;
+// cosineSampleHemispherePdf: |z / M_PI| in double (Utils/RandomUtils.h:53-56)
+__device__ inline float cosine_pdf(float z) { return (float)fabs((double)z / kPiD); }
 constexpr int kThreads = 256;
 constexpr int kPrimes = 1024;
 
@@ -113,10 +116,10 @@ __device__ inline f3 cosine_hemisphere(float u0, float u1) {
         float theta, r;
         if (fabsf(ox) > fabsf(oy)) {
             r = ox;
-            theta = (kPi / 4.f) * (oy / ox);
+            theta = (float)((kPiD / 4.f) * (double)(oy / ox));  // the reference's M_PI expression is double
         } else {
             r = oy;
-            theta = (kPi / 2.f) - (kPi / 4.f) * (ox / oy);
+            theta = (float)((kPiD / 2.f) - (kPiD / 4.f) * (double)(ox / oy));
         }
         dx = r * cosf(theta);
         dy = r * sinf(theta);
@@ -134,7 +137,7 @@ struct GGX {
         const float c4 = cos2_theta(h) * cos2_theta(h);
         float cp = cos_phi(h), sp = sin_phi(h);
         float e = (cp * cp / (ax * ax) + sp * sp / (ay * ay)) * t2;
-        return 1 / (kPi * ax * ay * c4 * (1 + e) * (1 + e));
+        return (float)(1 / (kPiD * ax * ay * c4 * (1 + e) * (1 + e)));  // double, as M_PI makes it
     }
     __device__ float Lambda(f3 w) const {
         if (w.z == 0) return 0;
@@ -149,9 +152,9 @@ struct GGX {
     __device__ float pdf(f3 h, f3 wo) const { return D(h) * G1(wo) * fabsf(dot3(wo, h)) / fabsf(wo.z); }
     // Heitz' visible-normal sampling as in MicrofacetDistribution.h sample/sampleGGX11
     __device__ static void sample11(float cos_t, float U1, float U2, float& sx, float& sy) {
-        if (cos_t > .9999f) {
+        if (cos_t > .9999) {
             float r = sqrtf(U1 / (1 - U1));
-            float phi = 6.28318530718f * U2;
+            float phi = (float)(6.28318530718 * U2);
             sx = r * cosf(phi);
             sy = r * sinf(phi);
             return;
@@ -162,7 +165,7 @@ struct GGX {
         float G1v = 2 / (1 + sqrtf(1.f + 1.f / (a * a)));
         float A = 2 * U1 / G1v - 1;
         float tmp = 1.f / (A * A - 1.f);
-        if (tmp > 1e10f) tmp = 1e10f;
+        if (tmp > 1e10) tmp = 1e10f;
         float B = tan_t;
         float Dd = sqrtf(fmaxf(B * B * tmp * tmp - (A * A - B * B) * tmp, 0.f));
         float s1 = B * tmp - Dd, s2 = B * tmp + Dd;
@@ -272,8 +275,8 @@ struct Bsdf {
 
     __device__ float pdf(f3 wi, f3 wo) const {
         switch (type) {
-            case cavpbrt::kMatte: return fabsf(wi.z / kPi);
-            case cavpbrt::kPlastic: return 0.5f * fabsf(wi.z / kPi) + 0.5f * mf_pdf(wi, wo);
+            case cavpbrt::kMatte: return cosine_pdf(wi.z);
+            case cavpbrt::kPlastic: return 0.5f * cosine_pdf(wi.z) + (1.f - 0.5f) * mf_pdf(wi, wo);
             case cavpbrt::kMirror: return (wi.x == -wo.x && wi.y == -wo.y && wi.z == wo.z) ? 1.f : 0.f;
             case cavpbrt::kGlass: {
                 if (same_hemisphere(wi, wo)) {
@@ -296,7 +299,7 @@ struct Bsdf {
         switch (type) {
             case cavpbrt::kMatte: {
                 wi = cosine_hemisphere(u0, u1);
-                pdf_out = fabsf(wi.z / kPi);
+                pdf_out = cosine_pdf(wi.z);
                 if (wo.z < 0) wi.z *= -1;
                 return lam_eval(wi, wo, kd);
             }
@@ -368,9 +371,7 @@ __device__ inline Bsdf make_bsdf(const RMaterial& m) {
     b.kr = ld3(m.kr);
     b.kt = ld3(m.kt);
     b.ggx = GGX{m.alpha_u, m.alpha_v};
-    f3 e = mk(m.eta, m.eta, m.eta);
-    f3 tmp = (e - mk(1, 1, 1)) / (e + mk(1, 1, 1));
-    b.f0 = tmp * tmp;
+    b.f0 = ld3(m.f0);
     b.eta = m.eta;
     b.mirror = m.mirror_kr;
     return b;
@@ -765,6 +766,10 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
         r.alpha_v = m.alpha_v;
         r.eta = m.eta;
         r.mirror_kr = m.mirror_kr;
+        for (int k = 0; k < 3; ++k) {  // Fresnel::createFromIOR (BSDFs/Fresnel.h:27-31), host float
+            float t = (m.eta - 1.f) / (m.eta + 1.f);
+            r.f0[k] = t * t;
+        }
         mats.push_back(r);
     }
     std::vector<RLight> lights;

@@ -140,36 +140,180 @@ def _nums(v) -> str:
     return " ".join(_num(x) for x in np.asarray(v).reshape(-1))
 
 
-def write_pbrt(path, room: dict, *, width=256, height=256, spp=16, max_depth=5, fov=40.0,
-               eye=(0.0, 0.0, -3.8), look=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), integrator="path"):
-    """Write a scene dict (as returned by mini_room) as a .pbrt file in the subset the
+def _floats_text(a) -> str:
+    """Exact float32 text without '+' (the reference's lexer reads [0-9.-e] only)."""
+    a = np.asarray(a, np.float32).reshape(-1)
+    if a.size and np.abs(a[np.isfinite(a)]).max(initial=0) >= 1e9:
+        return _nums(a)
+    return " ".join(["%.9g"] * a.size) % tuple(a.tolist())
+
+
+def _material_line(mat) -> str:
+    """pbrt Material directive of a scene material: a tuple is a matte Kd, a dict names
+    "type" (matte, plastic, glass, mirror) and its parameters."""
+    if not isinstance(mat, dict):
+        return f'Material "matte" "rgb Kd" [{_nums(mat)}]'
+    t = mat["type"]
+    parts = [f'Material "{t}"']
+    for key, kind in (("Kd", "rgb"), ("Ks", "rgb"), ("Kr", "rgb"), ("Kt", "rgb"), ("roughness", "float"),
+                      ("eta", "float")):
+        if key in mat:
+            if t == "mirror" and key == "Kr":
+                parts.append(f'"float Kr" [{_num(mat[key])}]')
+            else:
+                parts.append(f'"{kind} {key}" [{_nums(mat[key])}]')
+    if "remaproughness" in mat:
+        parts.append(f'"string remaproughness" "{"true" if mat["remaproughness"] else "false"}"')
+    return " ".join(parts)
+
+
+def write_pbrt(path, room: dict, *, width=256, height=256, spp=16, max_depth=5, fov=None, eye=None, look=None,
+               up=None, integrator="path"):
+    """Write a scene dict (mini_room, sphere_scene) as a .pbrt file in the subset the
     reference's loader reads (SceneLoading/Lexing.cu, Parsing.cu): one trianglemesh Shape per
-    mesh, matte materials, the light mesh as a diffuse AreaLightSource."""
+    mesh with its Material; light meshes (``room["lights"]`` = [(mesh, L)], or a mesh named
+    "light" with ``room["light_radiance"]``) as diffuse AreaLightSources over a black matte.
+    Camera arguments default to ``room["camera"]``, else the config-1 view."""
+    cam = dict(eye=(0.0, 0.0, -3.8), look=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), fov=40.0)
+    cam.update(room.get("camera", {}))
+    for k, v in (("eye", eye), ("look", look), ("up", up), ("fov", fov)):
+        if v is not None:
+            cam[k] = v
     pos, idx = room["positions"], room["indices"]
     lines = [
-        f"LookAt {_nums(eye)}  {_nums(look)}  {_nums(up)}",
-        f'Camera "perspective" "float fov" [{_num(fov)}]',
+        f"LookAt {_nums(cam['eye'])}  {_nums(cam['look'])}  {_nums(cam['up'])}",
+        f'Camera "perspective" "float fov" [{_num(cam["fov"])}]',
         f'Film "image" "integer xresolution" [{width}] "integer yresolution" [{height}] "string filename" "out.png"',
         f'Sampler "halton" "integer pixelsamples" [{spp}]',
         f'Integrator "{integrator}" "integer maxdepth" [{max_depth}]',
         'PixelFilter "box"',
         "WorldBegin",
     ]
-    L = room.get("light_radiance", (17.0, 12.0, 4.0))
-    for name, first, count, mat in room["meshes"]:
-        tris = idx[first:first + count]
-        used = np.unique(tris)
-        remap = {int(v): k for k, v in enumerate(used)}
-        P = pos[used]
-        I = np.vectorize(remap.get)(tris)
-        lines.append("AttributeBegin")
-        if name == "light":
-            lines.append(f'AreaLightSource "diffuse" "rgb L" [{_nums(L)}]')
-            lines.append('Material "matte" "rgb Kd" [0 0 0]')
-        else:
-            lines.append(f'Material "matte" "rgb Kd" [{_nums(mat)}]')
-        lines.append(f'Shape "trianglemesh" "integer indices" [{_nums(I)}] "point P" [{_nums(P)}]')
-        lines.append("AttributeEnd")
-    lines.append("WorldEnd")
+    light_of = dict(room.get("lights", []))
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
+        for k, (name, first, count, mat) in enumerate(room["meshes"]):
+            tris = idx[first:first + count]
+            used, inv = np.unique(tris, return_inverse=True)
+            I = inv.reshape(-1)
+            P = pos[used]
+            L = light_of.get(k)
+            if L is None and name == "light":
+                L = room.get("light_radiance", (17.0, 12.0, 4.0))
+            out = ["AttributeBegin"]
+            if L is not None:
+                out.append(f'AreaLightSource "diffuse" "rgb L" [{_nums(L)}]')
+                out.append('Material "matte" "rgb Kd" [0 0 0]')
+            else:
+                out.append(_material_line(mat))
+            out.append('Shape "trianglemesh" "integer indices" [' + " ".join(map(str, I.tolist())) + '] "point P" ['
+                       + _floats_text(P) + "]")
+            out.append("AttributeEnd")
+            f.write("\n".join(out) + "\n")
+        f.write("WorldEnd\n")
+
+
+_ICO_CACHE: dict = {}
+
+
+def icosphere(level: int):
+    """Unit icosphere: the icosahedron with each triangle split into 4, `level` times, new
+    vertices pushed onto the sphere (20 * 4**level triangles).  Outward winding."""
+    if level in _ICO_CACHE:
+        return _ICO_CACHE[level]
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    for _ in range(level):
+        nv = len(v)
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        key = np.minimum(e[:, 0], e[:, 1]) * nv + np.maximum(e[:, 0], e[:, 1])
+        uk, inv = np.unique(key, return_inverse=True)
+        a, b = uk // nv, uk % nv
+        mid = v[a] + v[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        m = (inv + nv).reshape(3, -1)
+        m01, m12, m20 = m[0], m[1], m[2]
+        f = np.concatenate([np.stack([f[:, 0], m01, m20], 1), np.stack([f[:, 1], m12, m01], 1),
+                            np.stack([f[:, 2], m20, m12], 1), np.stack([m01, m12, m20], 1)])
+        v = np.concatenate([v, mid])
+    # outward winding: cross(e1, e2) along the centroid
+    c = v[f].mean(1)
+    n = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+    flip = (n * c).sum(1) < 0
+    f[flip] = f[flip][:, [0, 2, 1]]
+    _ICO_CACHE[level] = (v, f)
+    return v, f
+
+
+def sphere_scene(n_spheres: int = 64, level: int = 6, seed: int = 3, room=(20.0, 10.0, 20.0), n_lights: int = 3,
+                 materials=("matte", "plastic", "glass", "mirror")):
+    """Config-3 scene: `n_spheres` icospheres (20 * 4**level triangles each; 64 x level 6 =
+    5,242,880), radii log-uniform in [0.05, 0.5], centres from 4 Gaussian clusters (sigma 1.5)
+    clipped into a W x H x D room (floor y = 0, centred in x and z); each sphere's material
+    uniform over `materials` (matte; plastic roughness 0.1; glass eta 1.5; mirror) with albedo
+    uniform in [0.1, 0.9]; `n_lights` 2 x 2 emissive quads under the ceiling facing down with
+    radiance uniform in [10, 30].  Room walls are matte 0.73 grey, outward-facing normals in.
+    Returns the scene dict of mini_room plus "lights" and "camera"."""
+    rng = np.random.default_rng(seed)
+    W, H, D = room
+    verts, tris, mesh_ids, meshes, lights = [], [], [], [], []
+    nv = 0
+    nt = 0
+
+    def add(v, t, name, mat):
+        nonlocal nv, nt
+        mid = len(meshes)
+        verts.append(np.asarray(v, np.float32))
+        tris.append(np.asarray(t, np.int64) + nv)
+        mesh_ids.append(np.full(len(t), mid, np.int32))
+        meshes.append((name, nt, len(t), mat))
+        nv += len(v)
+        nt += len(t)
+        return mid
+
+    x0, x1, z0, z1 = -W / 2, W / 2, -D / 2, D / 2
+    grey = (0.73, 0.73, 0.73)
+    add([[x0, 0, z0], [x1, 0, z0], [x1, 0, z1], [x0, 0, z1]], [(0, 2, 1), (0, 3, 2)], "floor", grey)
+    add([[x0, H, z0], [x1, H, z0], [x1, H, z1], [x0, H, z1]], [(0, 1, 2), (0, 2, 3)], "ceiling", grey)
+    add([[x0, 0, z1], [x1, 0, z1], [x1, H, z1], [x0, H, z1]], [(0, 2, 1), (0, 3, 2)], "back", grey)
+    add([[x0, 0, z0], [x1, 0, z0], [x1, H, z0], [x0, H, z0]], [(0, 1, 2), (0, 2, 3)], "front", grey)
+    add([[x0, 0, z0], [x0, 0, z1], [x0, H, z1], [x0, H, z0]], [(0, 1, 2), (0, 2, 3)], "left", grey)
+    add([[x1, 0, z0], [x1, 0, z1], [x1, H, z1], [x1, H, z0]], [(0, 2, 1), (0, 3, 2)], "right", grey)
+    uv, uf = icosphere(level)
+    centres_c = np.stack([rng.uniform(x0 + 3, x1 - 3, 4), rng.uniform(2, H - 3, 4), rng.uniform(z0 + 3, z1 - 3, 4)], 1)
+    for k in range(n_spheres):
+        r = float(np.exp(rng.uniform(np.log(0.05), np.log(0.5))))
+        c = centres_c[rng.integers(0, 4)] + rng.normal(0, 1.5, 3)
+        c = np.clip(c, [x0 + r, r, z0 + r], [x1 - r, H - 1 - r, z1 - r])
+        kind = materials[rng.integers(0, len(materials))]
+        alb = tuple(float(a) for a in rng.uniform(0.1, 0.9, 3))
+        if kind == "matte":
+            mat = {"type": "matte", "Kd": alb}
+        elif kind == "plastic":
+            mat = {"type": "plastic", "Kd": alb, "roughness": 0.1}
+        elif kind == "glass":
+            mat = {"type": "glass", "eta": 1.5}
+        else:
+            mat = {"type": "mirror"}
+        add(uv * r + c, uf, f"sphere{k}", mat)
+    for k in range(n_lights):
+        cx, cz = rng.uniform(x0 + 2, x1 - 2), rng.uniform(z0 + 2, z1 - 2)
+        y = H - 0.01
+        L = tuple(float(a) for a in rng.uniform(10, 30, 3))
+        mid = add([[cx - 1, y, cz - 1], [cx + 1, y, cz - 1], [cx + 1, y, cz + 1], [cx - 1, y, cz + 1]],
+                  [(0, 1, 2), (0, 2, 3)], f"light{k}", (0.0, 0.0, 0.0))
+        lights.append((mid, L))
+    return {
+        "positions": np.ascontiguousarray(np.concatenate(verts)),
+        "indices": np.ascontiguousarray(np.concatenate(tris).astype(np.int32)),
+        "mesh_ids": np.concatenate(mesh_ids),
+        "meshes": meshes,
+        "lights": lights,
+        "camera": {"eye": (0.0, H * 0.45, z0 + 0.5), "look": (0.0, H * 0.35, 0.0), "up": (0.0, 1.0, 0.0),
+                   "fov": 60.0},
+    }

@@ -3,7 +3,7 @@ reference harness.
 
     python -m oracle.build
 
-* ``oracle/_build/libcavoracle.so`` from ``cav_oracle.c`` (gcc; -ffp-contract=off so
+* ``oracle/_build/libcavoracle.so`` from ``cav_oracle.c`` and ``pt_oracle.c`` (gcc; -ffp-contract=off so
   that only the explicit fmaf/fma calls contract, OpenMP for the timed CPU baseline).
 * ``oracle/_ref/libcavref.so`` from the reference's own BVH sources via
   ``build_ref.sh`` (nvcc, sm_100a).  Skipped when the reference tree is absent.
@@ -23,12 +23,12 @@ REFERENCE_ROOT = Path(os.environ.get("CAVALRY_REFERENCE", "/root/reference"))
 
 def build_oracle(force: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
-    src = HERE / "cav_oracle.c"
-    if not force and ORACLE_LIB.exists() and ORACLE_LIB.stat().st_mtime >= src.stat().st_mtime:
+    srcs = [HERE / "cav_oracle.c", HERE / "pt_oracle.c"]
+    if not force and ORACLE_LIB.exists() and ORACLE_LIB.stat().st_mtime >= max(p.stat().st_mtime for p in srcs):
         return ORACLE_LIB
     tmp = ORACLE_LIB.with_suffix(".tmp.so")
     cmd = ["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared",
-           "-o", str(tmp), str(src), "-lm"]
+           "-o", str(tmp), *map(str, srcs), "-lm"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, ORACLE_LIB)
     return ORACLE_LIB

@@ -711,6 +711,54 @@ static int tri_hit(const float* pos, const int32_t* idx, int32_t t, const float*
 
 /* BVH::intersect, BVH/BVH.h:23-107, over the final node array.  rays: 6 floats each.
  * prim_out: hit triangle (leaf primitiveIndexBegin) or -1.  Uses OpenMP when built with it. */
+/* One ray of BVH::intersect (BVH/BVH.h:23-107).  Returns the hit triangle or -1 (-2 on a
+ * traversal-stack overflow); writes t/u/v of the hit. */
+int32_t orc_closest_one(const ONode* nodes, const float* pos, const int32_t* idx, const float* o, const float* d,
+                        float* t_out, float* u_out, float* v_out) {
+    float inv[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
+    int hit = 0;
+    float best = 3.402823466e+38f;
+    int32_t best_t = -1;
+    float bu = 0, bv = 0, md;
+    if (box_hit(nodes[0].bmin, nodes[0].bmax, o, inv, &md)) {
+        int32_t stack[128];
+        int top = 0;
+        stack[0] = 0;
+        while (top >= 0) {
+            int32_t cur = stack[top--];
+            const ONode* nd = &nodes[cur];
+            if (nd->is_leaf) {
+                for (int32_t p = nd->begin; p <= nd->end; ++p) {
+                    float dist, u, v;
+                    if (tri_hit(pos, idx, p, o, d, &dist, &u, &v)) {
+                        if (!hit || dist < best) {
+                            hit = 1; best = dist; best_t = p; bu = u; bv = v;
+                        }
+                    }
+                }
+            } else {
+                float ml, mr;
+                box_hit(nodes[nd->left].bmin, nodes[nd->left].bmax, o, inv, &ml);
+                box_hit(nodes[nd->right].bmin, nodes[nd->right].bmax, o, inv, &mr);
+                int okl = ml >= 0 && ml < best;
+                int okr = mr >= 0 && mr < best;
+                if (top + 2 >= 128) { hit = 0; best_t = -2; break; } /* stack overflow: flag */
+                if (okl && okr) {
+                    if (ml > mr) { stack[++top] = nd->left; stack[++top] = nd->right; }
+                    else { stack[++top] = nd->right; stack[++top] = nd->left; }
+                } else if (okl) stack[++top] = nd->left;
+                else if (okr) stack[++top] = nd->right;
+            }
+        }
+    }
+    if (t_out) *t_out = best_t >= 0 ? best : INFINITY;
+    if (u_out) *u_out = bu;
+    if (v_out) *v_out = bv;
+    return best_t;
+}
+
+/* BVH::intersect over a batch.  rays: 6 floats each.  prim_out: hit triangle (leaf
+ * primitiveIndexBegin) or -1.  Uses OpenMP when built with it. */
 void orc_trace_closest(const ONode* nodes, const float* pos, const int32_t* idx, const float* rays, int64_t n,
                        int32_t* prim_out, float* t_out, float* u_out, float* v_out) {
     unsigned f = fp_enter();
@@ -719,48 +767,11 @@ void orc_trace_closest(const ONode* nodes, const float* pos, const int32_t* idx,
         unsigned ff = fp_enter();
 #pragma omp for schedule(dynamic, 256)
         for (int64_t r = 0; r < n; ++r) {
-            const float* o = rays + 6 * r;
-            const float* d = rays + 6 * r + 3;
-            float inv[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
-            int hit = 0;
-            float best = 3.402823466e+38f;
-            int32_t best_t = -1;
-            float bu = 0, bv = 0, md;
-            if (box_hit(nodes[0].bmin, nodes[0].bmax, o, inv, &md)) {
-                int32_t stack[128];
-                int top = 0;
-                stack[0] = 0;
-                while (top >= 0) {
-                    int32_t cur = stack[top--];
-                    const ONode* nd = &nodes[cur];
-                    if (nd->is_leaf) {
-                        for (int32_t p = nd->begin; p <= nd->end; ++p) {
-                            float dist, u, v;
-                            if (tri_hit(pos, idx, p, o, d, &dist, &u, &v)) {
-                                if (!hit || dist < best) {
-                                    hit = 1; best = dist; best_t = p; bu = u; bv = v;
-                                }
-                            }
-                        }
-                    } else {
-                        float ml, mr;
-                        box_hit(nodes[nd->left].bmin, nodes[nd->left].bmax, o, inv, &ml);
-                        box_hit(nodes[nd->right].bmin, nodes[nd->right].bmax, o, inv, &mr);
-                        int okl = ml >= 0 && ml < best;
-                        int okr = mr >= 0 && mr < best;
-                        if (top + 2 >= 128) { hit = 0; best_t = -2; break; } /* stack overflow: flag */
-                        if (okl && okr) {
-                            if (ml > mr) { stack[++top] = nd->left; stack[++top] = nd->right; }
-                            else { stack[++top] = nd->right; stack[++top] = nd->left; }
-                        } else if (okl) stack[++top] = nd->left;
-                        else if (okr) stack[++top] = nd->right;
-                    }
-                }
-            }
-            prim_out[r] = best_t;
-            if (t_out) t_out[r] = best_t >= 0 ? best : INFINITY;
-            if (u_out) u_out[r] = bu;
-            if (v_out) v_out[r] = bv;
+            float t, u, v;
+            prim_out[r] = orc_closest_one(nodes, pos, idx, rays + 6 * r, rays + 6 * r + 3, &t, &u, &v);
+            if (t_out) t_out[r] = t;
+            if (u_out) u_out[r] = u;
+            if (v_out) v_out[r] = v;
         }
         fp_leave(ff);
     }
@@ -770,6 +781,47 @@ void orc_trace_closest(const ONode* nodes, const float* pos, const int32_t* idx,
 /* BVH::testVisibility, BVH/BVH.h:109-189.  limit: per-ray distance limit or NULL;
  * excl: 2 mesh ids per ray (source, target) or NULL; mesh_of_tri: per-triangle mesh id.
  * occluded[r] = 1 when some non-excluded triangle is hit (closer than the limit). */
+/* One ray of BVH::testVisibility (BVH/BVH.h:109-189).  Returns 1 when a triangle outside
+ * meshes src/dst is hit closer than limit (limit < 0: no limit), 2 on stack overflow. */
+int orc_any_one(const ONode* nodes, const float* pos, const int32_t* idx, const int32_t* mesh_of_tri,
+                const float* o, const float* d, float limit, int32_t src, int32_t dst) {
+    float inv[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
+    int occ = 0;
+    float md;
+    box_hit(nodes[0].bmin, nodes[0].bmax, o, inv, &md); /* a miss is only reported */
+    int32_t stack[128];
+    int top = 0;
+    stack[0] = 0;
+    while (top >= 0 && !occ) {
+        int32_t cur = stack[top--];
+        const ONode* nd = &nodes[cur];
+        if (nd->is_leaf) {
+            for (int32_t p = nd->begin; p <= nd->end; ++p) {
+                int32_t mi = mesh_of_tri ? mesh_of_tri[p] : 0;
+                if (mi == src || mi == dst) continue;
+                float dist, u, v;
+                if (tri_hit(pos, idx, p, o, d, &dist, &u, &v)) {
+                    if (limit < 0 || dist < limit) { occ = 1; break; }
+                }
+            }
+        } else {
+            float ml, mr;
+            box_hit(nodes[nd->left].bmin, nodes[nd->left].bmax, o, inv, &ml);
+            box_hit(nodes[nd->right].bmin, nodes[nd->right].bmax, o, inv, &mr);
+            if (top + 2 >= 128) { occ = 2; break; }
+            if (ml >= 0 && mr >= 0) {
+                if (ml > mr) { stack[++top] = nd->left; stack[++top] = nd->right; }
+                else { stack[++top] = nd->right; stack[++top] = nd->left; }
+            } else if (ml >= 0) stack[++top] = nd->left;
+            else if (mr >= 0) stack[++top] = nd->right;
+        }
+    }
+    return occ;
+}
+
+/* BVH::testVisibility over a batch.  limit: per-ray distance limit or NULL; excl: 2 mesh
+ * ids per ray (source, target) or NULL; mesh_of_tri: per-triangle mesh id.  occluded[r] = 1
+ * when some non-excluded triangle is hit (closer than the limit). */
 void orc_trace_any(const ONode* nodes, const float* pos, const int32_t* idx, const int32_t* mesh_of_tri,
                    const float* rays, const float* limit, const int32_t* excl, int64_t n, uint8_t* occluded) {
     unsigned f = fp_enter();
@@ -778,41 +830,9 @@ void orc_trace_any(const ONode* nodes, const float* pos, const int32_t* idx, con
         unsigned ff = fp_enter();
 #pragma omp for schedule(dynamic, 256)
         for (int64_t r = 0; r < n; ++r) {
-            const float* o = rays + 6 * r;
-            const float* d = rays + 6 * r + 3;
-            float inv[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
             int32_t src = excl ? excl[2 * r] : -1, dst = excl ? excl[2 * r + 1] : -1;
-            int occ = 0;
-            float md;
-            box_hit(nodes[0].bmin, nodes[0].bmax, o, inv, &md); /* a miss is only reported */
-            int32_t stack[128];
-            int top = 0;
-            stack[0] = 0;
-            while (top >= 0 && !occ) {
-                int32_t cur = stack[top--];
-                const ONode* nd = &nodes[cur];
-                if (nd->is_leaf) {
-                    for (int32_t p = nd->begin; p <= nd->end; ++p) {
-                        int32_t mi = mesh_of_tri ? mesh_of_tri[p] : 0;
-                        if (mi == src || mi == dst) continue;
-                        float dist, u, v;
-                        if (tri_hit(pos, idx, p, o, d, &dist, &u, &v)) {
-                            if (!limit || dist < limit[r]) { occ = 1; break; }
-                        }
-                    }
-                } else {
-                    float ml, mr;
-                    box_hit(nodes[nd->left].bmin, nodes[nd->left].bmax, o, inv, &ml);
-                    box_hit(nodes[nd->right].bmin, nodes[nd->right].bmax, o, inv, &mr);
-                    if (top + 2 >= 128) { occ = 2; break; }
-                    if (ml >= 0 && mr >= 0) {
-                        if (ml > mr) { stack[++top] = nd->left; stack[++top] = nd->right; }
-                        else { stack[++top] = nd->right; stack[++top] = nd->left; }
-                    } else if (ml >= 0) stack[++top] = nd->left;
-                    else if (mr >= 0) stack[++top] = nd->right;
-                }
-            }
-            occluded[r] = (uint8_t)occ;
+            occluded[r] = (uint8_t)orc_any_one(nodes, pos, idx, mesh_of_tri, rays + 6 * r, rays + 6 * r + 3,
+                                               limit ? limit[r] : -1.0f, src, dst);
         }
         fp_leave(ff);
     }

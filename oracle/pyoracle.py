@@ -233,3 +233,116 @@ class RefScene:
             self.free()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- path-tracing oracle
+OMESH_DTYPE = np.dtype([("first_tri", "<i4"), ("tri_count", "<i4"), ("has_normals", "<i4"), ("reverse", "<i4"),
+                        ("material", "<i4"), ("light", "<i4"), ("area", "<f4"), ("pad", "<i4")])
+OMAT_DTYPE = np.dtype([("type", "<i4"), ("kd", "<f4", (3,)), ("ks", "<f4", (3,)), ("kr", "<f4", (3,)),
+                       ("kt", "<f4", (3,)), ("alpha_u", "<f4"), ("alpha_v", "<f4"), ("eta", "<f4"),
+                       ("mirror_kr", "<f4")])
+OLIGHT_DTYPE = np.dtype([("L", "<f4", (3,)), ("mesh", "<i4")])
+MATERIAL_TYPES = {"matte": 0, "mirror": 1, "glass": 4, "plastic": 5}
+
+
+def _pt_lib():
+    L = oracle_lib()
+    if not hasattr(L, "_pt_ready"):
+        P, I, I64, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float
+        L.orc_render_path.argtypes = [P, P, P, P, P, P, I, P, P, I, P, F, I, I, I, I, F, F, I64, I64, P, P]
+        L.orc_render_path.restype = I
+        L.orc_roughness_to_alpha.argtypes = [F]
+        L.orc_roughness_to_alpha.restype = F
+        L.orc_halton_tables.argtypes = [P, P, P]
+        L.orc_halton_tables.restype = I64
+        L._pt_ready = True
+    return L
+
+
+def roughness_to_alpha(r: float) -> float:
+    return float(_pt_lib().orc_roughness_to_alpha(float(r)))
+
+
+def material_record(mat) -> np.void:
+    """A material as the reference's parser builds it (Materials/*.h createFromParams):
+    a tuple is a matte Kd; a dict names "type" and the pbrt parameters."""
+    m = np.zeros((), OMAT_DTYPE)
+    if not isinstance(mat, dict):
+        mat = {"type": "matte", "Kd": mat}
+    t = mat["type"]
+    m["type"] = MATERIAL_TYPES[t]
+    m["eta"] = 1.5
+    m["mirror_kr"] = 0.9
+    if t == "matte":
+        m["kd"] = mat.get("Kd", (1, 1, 1))
+    elif t == "plastic":
+        m["kd"] = mat.get("Kd", (0.25, 0.25, 0.25))
+        m["ks"] = mat.get("Ks", (0.25, 0.25, 0.25))
+        r = float(mat.get("roughness", 0.1))
+        a = roughness_to_alpha(r) if mat.get("remaproughness", True) else r
+        m["alpha_u"] = m["alpha_v"] = a
+    elif t == "glass":
+        assert float(mat.get("roughness", 0.0)) == 0.0, "only specular glass is restated"
+        m["kr"] = mat.get("Kr", (1, 1, 1))
+        m["kt"] = mat.get("Kt", (1, 1, 1))
+        m["eta"] = mat.get("eta", 1.5)
+    elif t == "mirror":
+        m["mirror_kr"] = mat.get("Kr", 0.9)
+    return m
+
+
+def look_at_c2w(eye, look, up) -> np.ndarray:
+    """Camera-to-world of pbrt's LookAt as the reference builds it (glm::lookAtLH then
+    inverse, SceneLoading/Parsing.cu:196-204); column-major 16 floats."""
+    e, c, u = (np.asarray(x, np.float64) for x in (eye, look, up))
+    f = c - e
+    f /= np.linalg.norm(f)
+    s = np.cross(u, f)
+    s /= np.linalg.norm(s)
+    uu = np.cross(f, s)
+    V = np.eye(4)
+    V[0, :3], V[1, :3], V[2, :3] = s, uu, f
+    V[0, 3], V[1, 3], V[2, 3] = -s @ e, -uu @ e, -f @ e
+    return np.linalg.inv(V).astype(np.float32).T.reshape(-1).copy()
+
+
+def render_path(scene: dict, *, width: int, height: int, spp: int, max_depth: int, first: int = 0,
+                count: int | None = None, filter_width: float = 1.0):
+    """Oracle render of a scene dict (the format of cavalry_b200.scenes, camera from
+    scene["camera"] else the config-1 view): returns the float film (sum [H,W,3], weight
+    [H,W]) of camera samples [first, first + count)."""
+    cam = dict(eye=(0.0, 0.0, -3.8), look=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), fov=40.0)
+    cam.update(scene.get("camera", {}))
+    eye, look, up, fov = cam["eye"], cam["look"], cam["up"], cam["fov"]
+    pos = np.ascontiguousarray(scene["positions"], np.float32)
+    idx = np.ascontiguousarray(scene["indices"], np.int32)
+    tri_mesh = np.ascontiguousarray(scene["mesh_ids"], np.int32)
+    nodes = build(pos, idx, rounds=0)["merged"]
+    meshes = np.zeros(len(scene["meshes"]), OMESH_DTYPE)
+    mats = np.zeros(len(scene["meshes"]), OMAT_DTYPE)
+    lights = []
+    light_of = dict(scene.get("lights", []))
+    for k, (name, first_tri, n, mat) in enumerate(scene["meshes"]):
+        meshes[k]["first_tri"], meshes[k]["tri_count"] = first_tri, n
+        meshes[k]["material"] = k
+        mats[k] = material_record(mat)
+        L = light_of.get(k)
+        if L is None and name == "light":
+            L = scene.get("light_radiance", (17.0, 12.0, 4.0))
+        if L is not None:
+            meshes[k]["light"] = len(lights)
+            lights.append(((float(L[0]), float(L[1]), float(L[2])), k))
+        else:
+            meshes[k]["light"] = -1
+    light_arr = np.array(lights, OLIGHT_DTYPE)
+    c2w = look_at_c2w(eye, look, up)
+    total = width * height * spp
+    count = total - first if count is None else count
+    fsum = np.zeros((height, width, 3), np.float32)
+    fw = np.zeros((height, width), np.float32)
+    st = _pt_lib().orc_render_path(_c(nodes), _c(pos), _c(idx), None, _c(tri_mesh), _c(meshes), len(meshes),
+                                   _c(mats), _c(light_arr), len(light_arr), _c(c2w), float(fov), width, height, spp,
+                                   max_depth, filter_width, filter_width, int(first), int(count), _c(fsum), _c(fw))
+    if st != 0:
+        raise RuntimeError(f"orc_render_path failed ({st})")
+    return fsum, fw

@@ -1,0 +1,65 @@
+"""Generates tests/golden/render_ref.npz: 8-bit renders by the reference's own renderer.
+
+Runs on a machine with a GPU and the reference renderer built by oracle/build_ref_full.sh
+(oracle/_ref/cavalry_ref); writes the .pbrt scenes from the seeded generators of
+cavalry_b200.scenes, renders each with ``--bvh-opt-rounds 0`` and stores the PNG pixels
+with the case parameters.  The tests regenerate the same .pbrt text from the parameters.
+
+    python tests/golden/make_render_golden.py OUT.npz
+"""
+import json
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from cavalry_b200 import scenes  # noqa: E402
+from oracle import ref_cli  # noqa: E402
+
+# (name, generator kwargs, render kwargs)
+CASES = [
+    ("room_d1_s1", {"kind": "room"}, dict(width=256, height=256, spp=1, max_depth=1)),
+    ("room_d2_s16", {"kind": "room"}, dict(width=256, height=256, spp=16, max_depth=2)),
+    ("room_d5_s1", {"kind": "room"}, dict(width=256, height=256, spp=1, max_depth=5)),
+    ("room_d5_s16", {"kind": "room"}, dict(width=256, height=256, spp=16, max_depth=5)),
+    ("spheres_mixed", {"kind": "spheres", "n_spheres": 12, "level": 2, "seed": 5},
+     dict(width=128, height=96, spp=8, max_depth=8)),
+    ("spheres_glass", {"kind": "spheres", "n_spheres": 10, "level": 3, "seed": 6, "materials": ["glass"]},
+     dict(width=128, height=96, spp=8, max_depth=8)),
+    ("spheres_mirror", {"kind": "spheres", "n_spheres": 10, "level": 3, "seed": 7, "materials": ["mirror"]},
+     dict(width=128, height=96, spp=8, max_depth=8)),
+    ("spheres_plastic", {"kind": "spheres", "n_spheres": 10, "level": 3, "seed": 8, "materials": ["plastic"]},
+     dict(width=128, height=96, spp=8, max_depth=8)),
+]
+
+
+def make_scene(gen: dict) -> dict:
+    g = dict(gen)
+    kind = g.pop("kind")
+    if kind == "room":
+        return scenes.mini_room()
+    if "materials" in g:
+        g["materials"] = tuple(g["materials"])
+    return scenes.sphere_scene(**g)
+
+
+def main(out: str):
+    arrays = {}
+    meta = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, gen, rk in CASES:
+            pbrt = Path(tmp) / f"{name}.pbrt"
+            scenes.write_pbrt(pbrt, make_scene(gen), **rk)
+            img, _ = ref_cli.render(str(pbrt), str(Path(tmp) / f"{name}.png"), spp=rk["spp"])
+            arrays[name] = img
+            meta.append({"name": name, "gen": gen, "render": rk})
+            print(name, img.shape, float(img.mean()), flush=True)
+    np.savez_compressed(out, meta=json.dumps(meta), **arrays)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else str(ROOT / "tests" / "golden" / "render_ref.npz"))
