@@ -38,8 +38,10 @@ UNIT = "Mrays/s"
 WORKLOAD = "soup_1M_tris_3_treelet_rounds_4M_closest_rays"
 RAY_BYTES = 32
 HIT_BYTES = 16  # prim id 4 + t 4 + uv 8
+# algorithmic traversal bytes per ray: ray 32 B + hit 16 B, plus 64 B per node visited and
+# 36 B (three float3 vertices) per triangle tested, counted by the instrumented kernel
 NODE_BYTES = 64
-TRI_BYTES = 48
+TRI_BYTES = 36
 
 
 def parse():
