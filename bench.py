@@ -51,6 +51,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="soup", choices=["soup", "render"],
+                   help="soup: BVH + 4M closest-hit rays (default); render: the 5.24M-triangle path-traced scene")
+    p.add_argument("--render-steps", type=int, default=1, help="timed full renders (render workload)")
+    p.add_argument("--small", action="store_true", help="render workload at 1/16 size (smoke runs)")
     p.add_argument("--tris", type=int, default=None, help="soup size (default: the 1M-triangle workload)")
     p.add_argument("--rays", type=int, default=None, help="rays per step (default: 4M)")
     a = p.parse_args()
@@ -391,9 +395,152 @@ def run_reference(args):
     }))
 
 
+# ------------------------------------------------------------------------ render workload
+def run_render(args):
+    """The 5.24M-triangle path-traced scene: 64 icospheres (level 6) in a 20x10x20 room, 4
+    materials, 3 area lights, 1920x1080, 64 spp, max depth 8, path integrator, treelet
+    rounds 0 and 3.  Reports the extend stage's closest-hit Mrays/s (rays traced by the
+    closest-hit stage / that stage's device time) and samples/s of whole renders, beside the
+    reference's CUDA build on the same B200: its BVH::intersect on the renderer's own
+    bounce-0 and bounce-1 rays (same trees), and its CLI render of the same .pbrt."""
+    import tempfile
+
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+    from oracle import pyoracle as po
+    from oracle import ref_cli
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    if args.small:
+        n_sph, level, W, H, spp = 16, 5, 480, 270, 16
+    else:
+        n_sph, level, W, H, spp = 64, 6, 1920, 1080, 64
+    depth = 8
+    workload = f"spheres_{n_sph}x{20 * 4 ** level}_tris_{W}x{H}_{spp}spp_depth{depth}_path"
+    # seed 9: LBVH depth 44, inside the reference's fixed 64-entry traversal stack (seeds 3
+    # and 4 give depth 64 and 69, which the reference's unchecked stack could overrun)
+    scene = scenes.sphere_scene(n_sph, level, seed=9)
+    tmp = tempfile.mkdtemp()
+    pbrt = os.path.join(tmp, "spheres.pbrt")
+    scenes.write_pbrt(pbrt, scene, width=W, height=H, spp=spp, max_depth=depth)
+    ctx = cav.Context(0)
+    out = {"metric": "closest-hit Mrays/s (render extend stage)", "unit": "Mrays/s", "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded icosphere scene written as .pbrt)",
+           "config": {"workload": workload, "triangles": int(len(scene["indices"])), "width": W, "height": H,
+                      "spp": spp, "max_depth": depth}}
+    sampler = ClockSampler(0)
+    runs = {}
+    captured = {}
+    for rounds in (0, 3):
+        t0 = time.time()
+        sc = ctx.load_pbrt(pbrt, bvh_rounds=rounds)
+        load_s = time.time() - t0
+        for _ in range(max(args.warmup, 1)):  # warm-up: full-resolution 1-spp renders
+            sc.render(spp=1)
+        fs = torch.empty(H * W * 3, device="cuda")
+        fw = torch.empty(H * W, device="cuda")
+        if rounds == 3:
+            sampler.start()
+        totals = []
+        for _ in range(args.render_steps):
+            torch.cuda.synchronize()
+            sc.render_into(fs, fw)
+            st = sc.stats()
+            totals.append(st.as_dict())
+        if rounds == 3:
+            clocks = sampler.stop()
+        st = totals[-1]
+        samples = W * H * spp
+        runs[rounds] = {
+            "load_s": round(load_s, 2),
+            "ms_render": round(statistics.median(t["ms_total"] for t in totals), 2),
+            "samples_per_s": round(samples / (statistics.median(t["ms_total"] for t in totals) * 1e-3), 1),
+            "extend_mrays_s": round(st["closest_rays"] / (st["ms_closest"] * 1e-3) / 1e6, 2),
+            "shadow_mrays_s": round(st["shadow_rays"] / max(st["ms_any"], 1e-9) * 1e-3, 2),
+            "closest_rays": st["closest_rays"], "shadow_rays": st["shadow_rays"],
+            "ms_closest": round(st["ms_closest"], 2), "ms_any": round(st["ms_any"], 2),
+            "ms_shade": round(st["ms_shade"], 2), "bounces": st["bounces"],
+        }
+        # the renderer's own bounce-0 and bounce-1 rays, traced alone by ours (same tree)
+        bvh = sc.bvh()
+        caps = [sc.capture_rays(d, capacity=1 << 22) for d in (0, 1)]
+        ours = []
+        for r in caps:
+            for _ in range(3):
+                bvh.trace_closest(r)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(5):
+                bvh.trace_closest(r)
+            b.record()
+            torch.cuda.synchronize()
+            ours.append(len(r) * 5 / (a.elapsed_time(b) * 1e-3) / 1e6)
+        runs[rounds]["captured_rays"] = [int(len(r)) for r in caps]
+        runs[rounds]["ours_captured_mrays_s"] = [round(x, 2) for x in ours]
+        captured[rounds] = ([r.cpu().numpy() for r in caps], bvh.export_nodes())
+        if rounds == 0:
+            s_np, w_np = fs.view(H, W, 3).cpu().numpy(), fw.view(H, W).cpu().numpy()
+            ours_img = cav.film_to_rgb8(s_np, w_np)
+        sc.free()
+    out["value"] = runs[3]["extend_mrays_s"]
+    out["render"] = {f"rounds{k}": v for k, v in runs.items()}
+    out["clocks"] = clocks
+    # reference CUDA build on the same B200
+    ref = {}
+    if po.ref_available():
+        try:
+            R = po.RefScene(scene["positions"], scene["indices"], scene["mesh_ids"], rounds=0, dump=False)
+            for rounds in (0, 3):
+                rays, nodes = captured[rounds]
+                if rounds == 3:
+                    R.load_nodes(nodes)
+                mr = []
+                for r in rays:
+                    R.trace_closest(r, reps=1)
+                    _, _, ms = R.trace_closest(r, reps=3)
+                    mr.append(round(len(r) / (ms * 1e-3) / 1e6, 2))
+                ref[f"rounds{rounds}_bvh_intersect_mrays_s"] = mr
+                ref[f"rounds{rounds}_speedup"] = [round(a / b, 2) for a, b in
+                                                  zip(runs[rounds]["ours_captured_mrays_s"], mr)]
+            R.free()
+        except Exception as e:  # the harness is test infrastructure: report, do not fail the bench
+            ref["harness_error"] = str(e)[:300]
+    if ref_cli.available():
+        try:
+            t0 = time.time()
+            img, text = ref_cli.render(pbrt, os.path.join(tmp, "ref.png"), spp=spp, timeout=1500)
+            ref["cli_wall_s"] = round(time.time() - t0, 2)
+            for line in text.splitlines():
+                if line.startswith("Rendering took"):
+                    ms = float(line.split()[2].rstrip("ms"))
+                    ref["cli_rendering_ms"] = ms
+                    ref["cli_samples_per_s"] = round(W * H * spp / (ms * 1e-3), 1)
+            d = np.abs(img.astype(int) - ours_img.astype(int)).max(2)
+            ref["image_vs_ours_rounds0"] = {"exact": round(float((d == 0).mean()), 4),
+                                            "le2": round(float((d <= 2).mean()), 4), "max": int(d.max())}
+        except Exception as e:
+            ref["cli_error"] = str(e)[:300]
+    out["reference_cuda"] = ref or {"unavailable": "reference build not present (oracle/_ref)"}
+    # CPU baseline: the path-tracing oracle on a bounded sample of the same render
+    if not args.no_cpu_baseline:
+        n = 4096 if not args.small else 2048
+        t0 = time.time()
+        po.render_path(scene, width=W, height=H, spp=spp, max_depth=depth, first=0, count=n)
+        dt = time.time() - t0
+        out["cpu_baseline"] = {"value": round(n / dt, 1), "unit": "samples/s", "cores": po.num_threads(),
+                               "kind": "port", "sample": f"first {n} camera samples (pixel-major), OpenMP"}
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "render":
+        run_render(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -93,6 +93,9 @@ def lib() -> ctypes.CDLL:
         "cav_scene_info": ([P, P], ctypes.c_int),
         "cav_render_to_host": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render": ([P, P, P, P, P, P], ctypes.c_int),
+        "cav_render_stats": ([P, P], ctypes.c_int),
+        "cav_scene_bvh": ([P], P),
+        "cav_render_capture_rays": ([P, P, P, ctypes.c_int, P, ctypes.c_int64, P], ctypes.c_int),
         "cav_film_to_rgb8": ([P, P, ctypes.c_int, ctypes.c_int, P], ctypes.c_int),
         "cav_write_png": ([ctypes.c_char_p, P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "cav_write_pfm": ([ctypes.c_char_p, P, P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -212,6 +215,15 @@ def parse_pbrt(path: str, spp: int = -1, integrator: str | None = None) -> tuple
     return info, c2w.reshape(4, 4).T
 
 
+class RenderStats(ctypes.Structure):
+    _fields_ = [("paths", ctypes.c_int64), ("closest_rays", ctypes.c_int64), ("shadow_rays", ctypes.c_int64),
+                ("bounces", ctypes.c_int), ("ms_total", ctypes.c_float), ("ms_closest", ctypes.c_float),
+                ("ms_shade", ctypes.c_float), ("ms_any", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Scene:
     """A loaded .pbrt scene with its BVH (cav_scene)."""
 
@@ -247,6 +259,30 @@ class Scene:
                               st_ptr)
         self.ctx._check(st, "cav_render")
 
+    def bvh(self) -> "Bvh":
+        """The scene's BVH (owned by the scene; valid until the scene is freed)."""
+        h = lib().cav_scene_bvh(self.handle)
+        return Bvh(self.ctx, h, int(self.info().triangles), keep=(self,), owned=False)
+
+    def stats(self) -> RenderStats:
+        """Ray counts and device stage times of the last render (waits for it)."""
+        out = RenderStats()
+        self.ctx._check(lib().cav_render_stats(self.handle, ctypes.addressof(out)), "cav_render_stats")
+        return out
+
+    def capture_rays(self, depth: int, capacity: int = 1 << 22, spp: int = 0, max_depth: int = 0):
+        """Extend-stage rays of bounce `depth` of the first chunk of paths, as a [k, 8] float32
+        CUDA tensor (the 32-byte cav_ray records)."""
+        import torch
+
+        buf = torch.empty((capacity, 8), dtype=torch.float32, device=f"cuda:{self.ctx.device}")
+        n = ctypes.c_int64(0)
+        opts = RenderOpts(spp, max_depth, 0, capacity)
+        st = lib().cav_render_capture_rays(self.ctx.handle, self.handle, ctypes.addressof(opts), depth,
+                                           buf.data_ptr(), capacity, ctypes.byref(n))
+        self.ctx._check(st, "cav_render_capture_rays")
+        return buf[: n.value]
+
     def free(self):
         if self.handle:
             lib().cav_scene_free(self.handle)
@@ -271,16 +307,17 @@ def film_to_rgb8(film_sum: np.ndarray, film_weight: np.ndarray) -> np.ndarray:
 class Bvh:
     """A built BVH (cav_bvh).  Device memory is released by :meth:`free`."""
 
-    def __init__(self, ctx: Context, handle, n: int, keep=()):
+    def __init__(self, ctx: Context, handle, n: int, keep=(), owned: bool = True):
         self.ctx = ctx
         self.handle = handle
         self.n = n
         self._keep = keep
+        self._owned = owned
 
     def free(self):
-        if self.handle:
+        if self.handle and self._owned:
             lib().cav_bvh_free(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:

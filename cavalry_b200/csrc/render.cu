@@ -701,6 +701,31 @@ struct cav_scene {
     uint16_t* d_perms = nullptr;
     cav_bvh* bvh = nullptr;
     int bvh_rounds = 0;
+    // per-stage timing of the last render: event pairs on the render stream
+    struct Log {
+        std::vector<cudaEvent_t> pool;
+        size_t used = 0;
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> closest, shade, any;
+        cudaEvent_t start = nullptr, end = nullptr;
+        int64_t paths = 0, closest_rays = 0, shadow_rays = 0;
+        int bounces = 0;
+        cudaEvent_t next() {
+            if (used == pool.size()) {
+                cudaEvent_t e;
+                cudaEventCreate(&e);
+                pool.push_back(e);
+            }
+            return pool[used++];
+        }
+        void reset() {
+            used = 0;
+            closest.clear();
+            shade.clear();
+            any.clear();
+            paths = closest_rays = shadow_rays = 0;
+            bounces = 0;
+        }
+    } log;
 };
 
 namespace cav {
@@ -811,8 +836,17 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
     return CAV_OK;
 }
 
+// Optional capture of one bounce's extend-stage rays (first chunk only), for timing other
+// traversal implementations on exactly the rays the renderer traces.
+struct RayCapture {
+    int depth = -1;
+    cav_ray* out = nullptr;
+    int64_t capacity = 0;
+    int64_t* count = nullptr;
+};
+
 cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
-                       cudaStream_t s) {
+                       cudaStream_t s, const RayCapture* cap = nullptr) {
     const cavpbrt::Scene& D = sc->desc;
     const int spp = opts && opts->spp > 0 ? opts->spp : D.spp;
     const int max_depth = opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth;
@@ -829,6 +863,11 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
     acc(32 * chunk); acc(4 * chunk); acc(8 * chunk); acc(4 * chunk); acc(12 * chunk); acc(chunk); acc(64);
     void* base = nullptr;
     CAV_CUDA(ctx, cudaMallocAsync(&base, need, s));
+    struct FreeAsync {  // path state is released on every exit path, stream-ordered
+        void* p;
+        cudaStream_t s;
+        ~FreeAsync() { cudaFreeAsync(p, s); }
+    } free_base{base, s};
     unsigned char* p = (unsigned char*)base;
     Paths P;
     P.sample_index = carve<uint64_t>(p, chunk);
@@ -873,6 +912,12 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
         else cam.depth = (D.width / 2.f) / std::tan(fov / 2.f);
     }
     uint32_t counts[2];
+    auto& log = sc->log;
+    log.reset();
+    log.start = log.next();
+    CAV_CUDA(ctx, cudaEventRecord(log.start, s));
+    log.paths = total;
+    if (cap && cap->count) *cap->count = 0;
     for (int64_t first = 0; first < total; first += chunk) {
         const int64_t m = std::min(chunk, total - first);
         k_generate<<<div_up(m, kThreads), kThreads, 0, s>>>(cam, S.halton, spp, first, m, P, Q);
@@ -882,17 +927,35 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
         // first bounce starts again at dimension 0.
         int dim0 = 0;
         for (int depth = 0; n > 0 && depth < max_depth; ++depth) {
+            if (cap && first == 0 && depth == cap->depth && cap->out) {
+                const int64_t k = std::min(n, cap->capacity);
+                CAV_CUDA(ctx, cudaMemcpyAsync(cap->out, Q.rays, sizeof(cav_ray) * k, cudaMemcpyDeviceToDevice, s));
+                if (cap->count) *cap->count = k;
+            }
+            cudaEvent_t e0 = log.next(), e1 = log.next(), e2 = log.next();
+            CAV_CUDA(ctx, cudaEventRecord(e0, s));
             cav_status st = trace_closest(ctx, sc->bvh, Q.rays, n, Q.hit_prim, Q.hit_t, Q.hit_uv, CAV_TRACE_EXACT, s,
                                           ctx->d_counters + 6);
             if (st != CAV_OK) return st;
+            CAV_CUDA(ctx, cudaEventRecord(e1, s));
             CAV_CUDA(ctx, cudaMemsetAsync(Q.counters, 0, 8, s));
             k_shade<<<div_up(n, kThreads), kThreads, 0, s>>>(S, depth, dim0, n, P, Q);
+            CAV_CUDA(ctx, cudaEventRecord(e2, s));
             CAV_CUDA(ctx, cudaMemcpyAsync(counts, Q.counters, 8, cudaMemcpyDeviceToHost, s));
             CAV_CUDA(ctx, cudaStreamSynchronize(s));
+            log.closest.emplace_back(e0, e1);
+            log.shade.emplace_back(e1, e2);
+            log.closest_rays += n;
+            log.shadow_rays += counts[1];
+            log.bounces = std::max(log.bounces, depth + 1);
             if (counts[1] > 0) {
+                cudaEvent_t e3 = log.next(), e4 = log.next();
+                CAV_CUDA(ctx, cudaEventRecord(e3, s));
                 st = trace_any(ctx, sc->bvh, Q.shadow_rays, Q.shadow_limit, Q.shadow_excl, counts[1], Q.shadow_occ,
                                CAV_TRACE_EXACT, s, ctx->d_counters + 7);
                 if (st != CAV_OK) return st;
+                CAV_CUDA(ctx, cudaEventRecord(e4, s));
+                log.any.emplace_back(e3, e4);
                 k_add_direct<<<div_up(counts[1], kThreads), kThreads, 0, s>>>(counts[1], P, Q);
             }
             std::swap(Q.active, Q.next_active);
@@ -904,7 +967,8 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
                                                          d_sum, d_wsum);
     }
     CAV_CUDA(ctx, cudaGetLastError());
-    CAV_CUDA(ctx, cudaFreeAsync(base, s));
+    log.end = log.next();
+    CAV_CUDA(ctx, cudaEventRecord(log.end, s));
     return CAV_OK;
 }
 
@@ -944,6 +1008,7 @@ cav_status cav_scene_free(cav_scene* sc) {
     cudaFree(sc->d_primes);
     cudaFree(sc->d_perm_start);
     cudaFree(sc->d_perms);
+    for (cudaEvent_t e : sc->log.pool) cudaEventDestroy(e);
     delete sc;
     return CAV_OK;
 }
@@ -975,6 +1040,58 @@ cav_status cav_render(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, 
     int integrator = opts ? opts->integrator : (sc->desc.integrator == "rlpath" ? 1 : 0);
     if (integrator != 0) return cav::set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "only the path integrator is built");
     return cav::render_path(ctx, sc, opts, film_sum, film_weight, s);
+}
+
+cav_status cav_render_stats(const cav_scene* sc, cav_render_stats_t* out) {
+    if (!sc || !out) return CAV_ERR_INVALID_ARGUMENT;
+    const auto& L = sc->log;
+    *out = cav_render_stats_t{};
+    out->paths = L.paths;
+    out->closest_rays = L.closest_rays;
+    out->shadow_rays = L.shadow_rays;
+    out->bounces = L.bounces;
+    if (!L.start || !L.end) return CAV_OK;
+    if (cudaEventSynchronize(L.end) != cudaSuccess) return CAV_ERR_CUDA;
+    auto sum = [](const std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v) {
+        double t = 0;
+        for (const auto& p : v) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, p.first, p.second);
+            t += ms;
+        }
+        return (float)t;
+    };
+    out->ms_closest = sum(L.closest);
+    out->ms_shade = sum(L.shade);
+    out->ms_any = sum(L.any);
+    cudaEventElapsedTime(&out->ms_total, L.start, L.end);
+    return CAV_OK;
+}
+
+cav_status cav_render_capture_rays(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, int depth,
+                                   cav_ray* rays_out, int64_t capacity, int64_t* count) {
+    if (!ctx || !sc || !rays_out || !count || depth < 0 || capacity <= 0) return CAV_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return cav::cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
+    const int64_t pixels = (int64_t)sc->desc.width * sc->desc.height;
+    float* film = nullptr;
+    CAV_CUDA(ctx, cudaMalloc(&film, sizeof(float) * 4 * pixels));
+    cav_render_opts o = opts ? *opts : cav_render_opts{0, 0, 0, 0};
+    // one chunk is enough: the capture is taken from the first chunk
+    const int spp = o.spp > 0 ? o.spp : sc->desc.spp;
+    const int64_t total = pixels * spp;
+    if (o.max_paths_in_flight <= 0) o.max_paths_in_flight = (int64_t)1 << 22;
+    o.max_paths_in_flight = std::min(o.max_paths_in_flight, total);
+    cav::RayCapture cap;
+    cap.depth = depth;
+    cap.out = rays_out;
+    cap.capacity = capacity;
+    cap.count = count;
+    cudaMemset(film, 0, sizeof(float) * 4 * pixels);
+    cav_status st = cav::render_path(ctx, sc, &o, film, film + 3 * pixels, nullptr, &cap);
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaFree(film);
+    if (st == CAV_OK && e != cudaSuccess) st = cav::cuda_error(ctx, e, "render capture");
+    return st;
 }
 
 cav_status cav_render_to_host(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* host_sum,

@@ -232,6 +232,21 @@ cav_status cav_render(cav_ctx* ctx, cav_scene* scene, const cav_render_opts* opt
  * ms_out (or NULL) receives the render time measured with CUDA events. */
 cav_status cav_render_to_host(cav_ctx* ctx, cav_scene* scene, const cav_render_opts* opts, float* host_sum,
                               float* host_weight, float* ms_out);
+/* Statistics of the scene's last render: paths, closest-hit (extend) and shadow rays traced,
+ * bounces, and device time (CUDA events on the render stream) of the whole render and of
+ * the extend, shading and shadow stages.  Waits for the render to finish. */
+typedef struct cav_render_stats_t {
+    int64_t paths, closest_rays, shadow_rays;
+    int bounces;
+    float ms_total, ms_closest, ms_shade, ms_any;
+} cav_render_stats_t;
+cav_status cav_render_stats(const cav_scene* scene, cav_render_stats_t* out);
+/* Renders the first chunk of paths (opts->max_paths_in_flight, default 4M) and copies the
+ * extend-stage rays of bounce `depth` (at most `capacity`) into the DEVICE array rays_out;
+ * *count receives how many.  For timing other traversal code on the renderer's own rays.
+ * Synchronous. */
+cav_status cav_render_capture_rays(cav_ctx* ctx, cav_scene* scene, const cav_render_opts* opts, int depth,
+                                   cav_ray* rays_out, int64_t capacity, int64_t* count);
 /* Film -> 8-bit sRGB as the reference's Film::readCurrentResult (Core/Film.cu:20-46); HOST arrays. */
 cav_status cav_film_to_rgb8(const float* film_sum, const float* film_weight, int width, int height, uint8_t* rgb);
 /* Image writers: 8-bit RGB PNG (the reference's output format) and a float PFM of sum/weight. */
