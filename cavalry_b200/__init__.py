@@ -198,6 +198,9 @@ class SceneInfo(ctypes.Structure):
                 ("bvh_rounds", ctypes.c_int), ("integrator", ctypes.c_int)]
 
 
+_INTEGRATORS = {None: 0, "path": -1, "rlpath": 1}
+
+
 class RenderOpts(ctypes.Structure):
     _fields_ = [("spp", ctypes.c_int), ("max_depth", ctypes.c_int), ("integrator", ctypes.c_int),
                 ("max_paths_in_flight", ctypes.c_int64)]
@@ -236,25 +239,26 @@ class Scene:
         self.ctx._check(lib().cav_scene_info(self.handle, ctypes.addressof(out)), "cav_scene_info")
         return out
 
-    def render(self, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0):
-        """Render to host arrays; returns (film_sum [H,W,3], film_weight [H,W], ms)."""
+    def render(self, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0, integrator: str | None = None):
+        """Render to host arrays; returns (film_sum [H,W,3], film_weight [H,W], ms).  integrator:
+        None = the scene's, "path" or "rlpath"."""
         inf = self.info()
         s = np.zeros((inf.height, inf.width, 3), np.float32)
         w = np.zeros((inf.height, inf.width), np.float32)
         ms = np.zeros(1, np.float32)
-        opts = RenderOpts(spp, max_depth, 0, max_paths_in_flight)
+        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight)
         st = lib().cav_render_to_host(self.ctx.handle, self.handle, ctypes.addressof(opts), s.ctypes.data,
                                       w.ctypes.data, ms.ctypes.data)
         self.ctx._check(st, "cav_render_to_host")
         return s, w, float(ms[0])
 
     def render_into(self, film_sum, film_weight, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0,
-                    stream=None):
+                    stream=None, integrator: str | None = None):
         """Render into DEVICE films (pointers, or objects with data_ptr(): 3 + 1 floats per
         pixel), stream-ordered on `stream` (a pointer, an object with cuda_stream, or None)."""
         ptr = lambda x: x if isinstance(x, int) else x.data_ptr()  # noqa: E731
         st_ptr = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
-        opts = RenderOpts(spp, max_depth, 0, max_paths_in_flight)
+        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight)
         st = lib().cav_render(self.ctx.handle, self.handle, ctypes.addressof(opts), ptr(film_sum), ptr(film_weight),
                               st_ptr)
         self.ctx._check(st, "cav_render")

@@ -204,7 +204,7 @@ typedef struct cav_scene_info_t {
 typedef struct cav_render_opts {
     int spp;                     /* <= 0: the scene's Sampler "pixelsamples" */
     int max_depth;               /* <= 0: the scene's Integrator "maxdepth" */
-    int integrator;              /* 0 = path (rlpath is not built) */
+    int integrator;              /* 0: the scene's Integrator ("path" or "rlpath"); -1: path; 1: rlpath */
     int64_t max_paths_in_flight; /* <= 0: 4M; samples are rendered in chunks of this many paths */
 } cav_render_opts;
 

@@ -34,6 +34,10 @@ CASES = [
      dict(width=128, height=96, spp=8, max_depth=8)),
     ("spheres_plastic", {"kind": "spheres", "n_spheres": 10, "level": 3, "seed": 8, "materials": ["plastic"]},
      dict(width=128, height=96, spp=8, max_depth=8)),
+    # the learning integrator (the .pbrt names it; both renderers read the Integrator line)
+    ("room_rlpath_s16", {"kind": "room"}, dict(width=128, height=128, spp=16, max_depth=5, integrator="rlpath")),
+    ("spheres_rlpath_s16", {"kind": "spheres", "n_spheres": 12, "level": 3, "seed": 5},
+     dict(width=128, height=96, spp=16, max_depth=8, integrator="rlpath")),
 ]
 
 
@@ -54,7 +58,8 @@ def main(out: str):
         for name, gen, rk in CASES:
             pbrt = Path(tmp) / f"{name}.pbrt"
             scenes.write_pbrt(pbrt, make_scene(gen), **rk)
-            img, _ = ref_cli.render(str(pbrt), str(Path(tmp) / f"{name}.png"), spp=rk["spp"])
+            img, _ = ref_cli.render(str(pbrt), str(Path(tmp) / f"{name}.png"), spp=rk["spp"],
+                                    integrator=rk.get("integrator", "path"))
             arrays[name] = img
             meta.append({"name": name, "gen": gen, "render": rk})
             print(name, img.shape, float(img.mean()), flush=True)

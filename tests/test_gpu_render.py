@@ -51,7 +51,14 @@ def load(ctx, tmp_path, name, scene, render, rounds=0):
 # Device maths is the reference's (fast-math, same expression shapes), so the room agrees
 # to the 8-bit value almost everywhere; glass chains keep a few flipped lobe choices.
 TOL = {"room": dict(exact=0.999, le2=0.9998, gt8=0.0002),
-       "spheres": dict(exact=0.96, le2=0.99, gt8=0.003)}
+       "spheres": dict(exact=0.96, le2=0.99, gt8=0.003),
+       # rlpath learns its table with float atomics in both renderers, so the order of
+       # proposals (and with it a few samples) differs from run to run
+       "rlpath": dict(exact=0.95, le2=0.99, gt8=0.005)}
+
+
+def tol_of(case):
+    return TOL["rlpath"] if case["render"].get("integrator") == "rlpath" else TOL[case["gen"]["kind"]]
 
 
 @pytest.mark.parametrize("case", render_cases(), ids=[c["name"] for c in render_cases()])
@@ -63,7 +70,7 @@ def test_render_matches_reference_png(ctx, tmp_path, case):
     img = cav.film_to_rgb8(s, w)
     ref = np.load(GOLDEN)[case["name"]]
     d = np.abs(img.astype(int) - ref.astype(int)).max(2)
-    t = TOL[case["gen"]["kind"]]
+    t = tol_of(case)
     assert (d == 0).mean() >= t["exact"], (d == 0).mean()
     assert (d <= 2).mean() >= t["le2"], (d <= 2).mean()
     assert (d > 8).mean() <= t["gt8"], (d > 8).mean()
@@ -158,3 +165,24 @@ def test_cli_renders_png(tmp_path):
     img = cav.film_to_rgb8(*sc.render()[:2])
     d = np.abs(png.astype(int) - img.astype(int)).max(2)  # float atomics may round differently
     assert d.max() <= 1 and (d == 0).mean() >= 0.999
+
+
+def test_rlpath_converges_to_path(ctx, tmp_path):
+    """The learned proposal keeps the estimator unbiased: at 64 spp the rlpath image agrees
+    with a 1024-spp path render as closely as a 64-spp path render does."""
+    from cavalry_b200 import scenes
+
+    sc, _ = load(ctx, tmp_path, "conv", scenes.sphere_scene(12, 3, seed=5), dict(width=96, height=64, spp=16,
+                                                                                   max_depth=8))
+    s, w, _ = sc.render(spp=1024, integrator="path")
+    ref = s / w[..., None]
+
+    def relmse(x):
+        return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    s, w, _ = sc.render(spp=64, integrator="path")
+    e_path = relmse(s / w[..., None])
+    s, w, _ = sc.render(spp=64, integrator="rlpath")
+    e_rl = relmse(s / w[..., None])
+    assert e_rl <= 1.5 * e_path, (e_rl, e_path)
+    assert abs((s / w[..., None]).mean() - ref.mean()) <= 0.01 * ref.mean()

@@ -14,10 +14,11 @@ sys.path.insert(0, str(ROOT / "tests" / "golden"))
 
 
 def render_cases():
+    """Path-integrator cases (the oracle restates the path integrator only)."""
     if not GOLDEN.exists():
         return []
     g = np.load(GOLDEN)
-    return json.loads(str(g["meta"]))
+    return [c for c in json.loads(str(g["meta"])) if c["render"].get("integrator", "path") == "path"]
 
 
 def make_scene(gen):
