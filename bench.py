@@ -51,8 +51,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="soup", choices=["soup", "render"],
-                   help="soup: BVH + 4M closest-hit rays (default); render: the 5.24M-triangle path-traced scene")
+    p.add_argument("--workload", default="soup", choices=["soup", "render", "serve"],
+                   help="soup: BVH + 4M closest-hit rays (default); render: the 5.24M-triangle path-traced scene; "
+                        "serve: a Poisson stream of render and ray-query jobs, merged server vs sequential loop")
+    p.add_argument("--jobs", type=int, default=256, help="jobs in the served stream (serve workload)")
     p.add_argument("--render-steps", type=int, default=1, help="timed full renders (render workload)")
     p.add_argument("--small", action="store_true", help="render workload at 1/16 size (smoke runs)")
     p.add_argument("--tris", type=int, default=None, help="soup size (default: the 1M-triangle workload)")
@@ -536,9 +538,136 @@ def run_render(args):
     print(json.dumps(out))
 
 
+# ------------------------------------------------------------------------ serve workload
+def run_serve(args):
+    """Served stream: jobs arrive as a Poisson process (mean gap 20 ms, seed 4).  Scenes are
+    config-2-type soups (16 of them, triangle counts log-uniform in [1k, 2M], seeds 100+)
+    resident with their BVHs; 3 of 4 jobs render one (resolution uniform in {64^2, 256^2,
+    512^2, 1024^2}, spp uniform in {1, 4, 16, 64}, depth 6, path integrator), 1 of 4 is a
+    ray-query job of 256k-4M config-1-style rays (half closest hit, half any hit).  The same
+    stream is served by the merged server (continuous batching, shared traversal launches)
+    and by the plain sequential loop (one job at a time, same kernels); each job's result is
+    checked to be the same in both.  Latency = completion - arrival on the server clock."""
+    import tempfile
+    import threading
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    rng = np.random.default_rng(4)
+    n_scenes = 16
+    sizes = np.exp(rng.uniform(np.log(1e3), np.log(2e6), n_scenes)).astype(int)
+    resolutions = [64, 256, 512, 1024]
+    ctx = cav.Context(0)
+    tmp = tempfile.mkdtemp()
+    pool = {}
+    t0 = time.time()
+    soups = {}
+    for k, n in enumerate(sizes):
+        soups[k] = scenes.soup_scene(int(n), seed=100 + k)
+        path = os.path.join(tmp, f"soup{k}.pbrt")
+        scenes.write_pbrt(path, soups[k], width=64, height=64, spp=1, max_depth=6)
+        pool[k] = ctx.load_pbrt(path, bvh_rounds=3)  # resident scene + BVH; jobs pick the resolution
+    setup_s = time.time() - t0
+    # the job stream
+    jobs = []
+    t = 0.0
+    for i in range(args.jobs):
+        t += rng.exponential(0.020)
+        k = int(rng.integers(0, n_scenes))
+        if rng.random() < 0.25:
+            nr = int(np.exp(rng.uniform(np.log(2 ** 18), np.log(2 ** 22))))
+            kind = "any" if rng.random() < 0.5 else "closest"
+            jobs.append(dict(at=t, kind=kind, scene=k, rays=nr, seed=1000 + i))
+        else:
+            jobs.append(dict(at=t, kind="render", scene=k, res=resolutions[int(rng.integers(0, 4))],
+                             spp=[1, 4, 16, 64][int(rng.integers(0, 4))]))
+    ray_inputs = {}
+    for i, j in enumerate(jobs):
+        if j["kind"] == "closest":
+            ray_inputs[i] = (scenes.closest_rays(j["rays"], seed=j["seed"]), None)
+        elif j["kind"] == "any":
+            r, lim = scenes.shadow_rays(j["rays"], seed=j["seed"])
+            ray_inputs[i] = (r, lim)
+
+    def serve(mode):
+        sv = cav.Server(ctx, hbm_budget_bytes=80 << 30, mode=mode)
+        ids = [None] * len(jobs)
+        outs = [None] * len(jobs)
+        clock0 = sv.stats().now_s
+        wall0 = time.perf_counter()
+
+        def submitter():
+            for i, j in enumerate(jobs):
+                delay = j["at"] - (time.perf_counter() - wall0)
+                if delay > 0:
+                    time.sleep(delay)
+                if j["kind"] == "render":
+                    jid, fs, fw = sv.submit_render(pool[j["scene"]], spp=j["spp"], max_depth=6, width=j["res"],
+                                                   height=j["res"])
+                    outs[i] = (fs, fw)
+                else:
+                    bvh = pool[j["scene"]].bvh()
+                    r, lim = ray_inputs[i]
+                    res = sv.submit_rays(bvh, r, any_hit=j["kind"] == "any", limit=lim)
+                    jid = res[0]
+                    outs[i] = res[1:]
+                ids[i] = jid
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        stats = [sv.wait(jid, timeout_s=1800).as_dict() for jid in ids]
+        st = sv.stats().as_dict()
+        sv.close()
+        lat = np.array([s["t_done"] - s["t_submit"] for s in stats])
+        first = min(s["t_submit"] for s in stats)
+        last = max(s["t_done"] for s in stats)
+        return {"jobs_per_s": round(len(jobs) / (last - first), 2), "makespan_s": round(last - first, 3),
+                "p50_latency_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
+                "p99_latency_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
+                "mean_latency_ms": round(float(lat.mean()) * 1e3, 2),
+                "ticks": st["ticks"], "closest_launches": st["closest_launches"], "any_launches": st["any_launches"],
+                "max_segments_per_launch": st["max_segments"], "server_busy_s": round(st["busy_s"], 3)}, outs
+
+    merged, out_m = serve(cav.SERVE_MERGED)
+    seq, out_s = serve(cav.SERVE_SEQUENTIAL)
+    # the same result alone (sequential) and in the mix (merged)
+    worst = 0.0
+    for a, b in zip(out_m, out_s):
+        for x, y in zip(a, b):
+            if x.dtype == np.float32:
+                fin = np.isfinite(y)
+                if not np.array_equal(fin, np.isfinite(x)):
+                    worst = float("inf")
+                elif fin.any():
+                    worst = max(worst, float(np.max(np.abs(x[fin] - y[fin]) / (np.abs(y[fin]) + 1e-3))))
+            elif not np.array_equal(x, y):
+                worst = float("inf")
+    renders = sum(1 for j in jobs if j["kind"] == "render")
+    out = {
+        "metric": "served jobs/s (merged server vs sequential loop)", "value": merged["jobs_per_s"], "unit": "jobs/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded soups written as .pbrt; seeded Poisson job stream)",
+        "config": {"workload": f"served_stream_{len(jobs)}_jobs_poisson_20ms", "jobs": len(jobs), "render_jobs": renders,
+                   "ray_jobs": len(jobs) - renders, "scenes": n_scenes,
+                   "scene_triangles": [int(x) for x in sizes], "resolutions": resolutions, "spp": [1, 4, 16, 64],
+                   "depth": 6, "hbm_budget_gib": 80},
+        "merged": merged, "sequential": seq,
+        "speedup_jobs_per_s": round(merged["jobs_per_s"] / seq["jobs_per_s"], 3),
+        "max_rel_diff_merged_vs_sequential": worst, "setup_s": round(setup_s, 1),
+    }
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
-    if args.workload == "render":
+    if args.workload == "serve":
+        run_serve(args)
+    elif args.workload == "render":
         run_render(args)
     elif args.impl == "reference":
         run_reference(args)

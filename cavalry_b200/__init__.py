@@ -19,8 +19,8 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ["CavError", "Context", "Bvh", "Scene", "SceneInfo", "lib", "parse_pbrt", "film_to_rgb8", "REF_NODE_DTYPE",
-           "TRACE_EXACT", "TRACE_CULL_ON_POP"]
+__all__ = ["CavError", "Context", "Bvh", "Scene", "SceneInfo", "Server", "lib", "parse_pbrt", "film_to_rgb8",
+           "REF_NODE_DTYPE", "TRACE_EXACT", "TRACE_CULL_ON_POP", "SERVE_MERGED", "SERVE_SEQUENTIAL"]
 
 _PKG = Path(__file__).resolve().parent
 _LIB_PATH = _PKG / "libcavalry_b200.so"
@@ -94,6 +94,13 @@ def lib() -> ctypes.CDLL:
         "cav_render_to_host": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render_stats": ([P, P], ctypes.c_int),
+        "cav_server_create": ([P, P, ctypes.POINTER(P)], ctypes.c_int),
+        "cav_server_destroy": ([P], ctypes.c_int),
+        "cav_server_submit_render": ([P, P, P, P, P, P], ctypes.c_int),
+        "cav_server_submit_rays": ([P, P, ctypes.c_int, P, P, P, ctypes.c_int64, P, P, P, P, P], ctypes.c_int),
+        "cav_server_poll": ([P, ctypes.c_int64, P], ctypes.c_int),
+        "cav_server_wait": ([P, ctypes.c_int64, ctypes.c_double, P], ctypes.c_int),
+        "cav_server_stats": ([P, P], ctypes.c_int),
         "cav_scene_bvh": ([P], P),
         "cav_render_capture_rays": ([P, P, P, ctypes.c_int, P, ctypes.c_int64, P], ctypes.c_int),
         "cav_film_to_rgb8": ([P, P, ctypes.c_int, ctypes.c_int, P], ctypes.c_int),
@@ -203,7 +210,7 @@ _INTEGRATORS = {None: 0, "path": -1, "rlpath": 1}
 
 class RenderOpts(ctypes.Structure):
     _fields_ = [("spp", ctypes.c_int), ("max_depth", ctypes.c_int), ("integrator", ctypes.c_int),
-                ("max_paths_in_flight", ctypes.c_int64)]
+                ("max_paths_in_flight", ctypes.c_int64), ("width", ctypes.c_int), ("height", ctypes.c_int)]
 
 
 def parse_pbrt(path: str, spp: int = -1, integrator: str | None = None) -> tuple[SceneInfo, np.ndarray]:
@@ -239,26 +246,28 @@ class Scene:
         self.ctx._check(lib().cav_scene_info(self.handle, ctypes.addressof(out)), "cav_scene_info")
         return out
 
-    def render(self, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0, integrator: str | None = None):
+    def render(self, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0, integrator: str | None = None,
+               width: int = 0, height: int = 0):
         """Render to host arrays; returns (film_sum [H,W,3], film_weight [H,W], ms).  integrator:
-        None = the scene's, "path" or "rlpath"."""
+        None = the scene's, "path" or "rlpath"; width/height override the Film resolution."""
         inf = self.info()
-        s = np.zeros((inf.height, inf.width, 3), np.float32)
-        w = np.zeros((inf.height, inf.width), np.float32)
+        W, H = (width, height) if width > 0 and height > 0 else (inf.width, inf.height)
+        s = np.zeros((H, W, 3), np.float32)
+        w = np.zeros((H, W), np.float32)
         ms = np.zeros(1, np.float32)
-        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight)
+        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height)
         st = lib().cav_render_to_host(self.ctx.handle, self.handle, ctypes.addressof(opts), s.ctypes.data,
                                       w.ctypes.data, ms.ctypes.data)
         self.ctx._check(st, "cav_render_to_host")
         return s, w, float(ms[0])
 
     def render_into(self, film_sum, film_weight, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0,
-                    stream=None, integrator: str | None = None):
+                    stream=None, integrator: str | None = None, width: int = 0, height: int = 0):
         """Render into DEVICE films (pointers, or objects with data_ptr(): 3 + 1 floats per
         pixel), stream-ordered on `stream` (a pointer, an object with cuda_stream, or None)."""
         ptr = lambda x: x if isinstance(x, int) else x.data_ptr()  # noqa: E731
         st_ptr = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
-        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight)
+        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height)
         st = lib().cav_render(self.ctx.handle, self.handle, ctypes.addressof(opts), ptr(film_sum), ptr(film_weight),
                               st_ptr)
         self.ctx._check(st, "cav_render")
@@ -281,7 +290,7 @@ class Scene:
 
         buf = torch.empty((capacity, 8), dtype=torch.float32, device=f"cuda:{self.ctx.device}")
         n = ctypes.c_int64(0)
-        opts = RenderOpts(spp, max_depth, 0, capacity)
+        opts = RenderOpts(spp, max_depth, 0, capacity, 0, 0)
         st = lib().cav_render_capture_rays(self.ctx.handle, self.handle, ctypes.addressof(opts), depth,
                                            buf.data_ptr(), capacity, ctypes.byref(n))
         self.ctx._check(st, "cav_render_capture_rays")
@@ -297,6 +306,118 @@ class Scene:
             self.free()
         except Exception:
             pass
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("mode", ctypes.c_int), ("max_live_jobs", ctypes.c_int),
+                ("max_paths_per_job", ctypes.c_int64)]
+
+
+class JobStatus(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int), ("t_submit", ctypes.c_double),
+                ("t_start", ctypes.c_double), ("t_done", ctypes.c_double), ("bounces", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("ticks", ctypes.c_int64), ("closest_launches", ctypes.c_int64), ("any_launches", ctypes.c_int64),
+                ("max_segments", ctypes.c_int64), ("busy_s", ctypes.c_double), ("now_s", ctypes.c_double),
+                ("pending", ctypes.c_int64), ("live", ctypes.c_int64), ("hbm_in_use", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+JOB_PENDING, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+SERVE_MERGED, SERVE_SEQUENTIAL = 0, 1
+
+
+class Server:
+    """A serving loop (cav_server): render and ray-query jobs merged into shared traversal
+    launches.  Results land in the numpy arrays returned by the submit calls once
+    :meth:`wait` reports the job done."""
+
+    def __init__(self, ctx: "Context", hbm_budget_bytes: int = 80 << 30, mode: int = SERVE_MERGED,
+                 max_live_jobs: int = 64, max_paths_per_job: int = 0):
+        self.ctx = ctx
+        cfg = ServerConfig(hbm_budget_bytes, mode, max_live_jobs, max_paths_per_job)
+        h = ctypes.c_void_p()
+        ctx._check(lib().cav_server_create(ctx.handle, ctypes.addressof(cfg), ctypes.byref(h)), "cav_server_create")
+        self.handle = h
+        self._keep: dict[int, tuple] = {}
+
+    def submit_render(self, scene: "Scene", spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0,
+                      width: int = 0, height: int = 0):
+        inf = scene.info()
+        W, H = (width, height) if width > 0 and height > 0 else (inf.width, inf.height)
+        fs = np.zeros((H, W, 3), np.float32)
+        fw = np.zeros((H, W), np.float32)
+        opts = RenderOpts(spp, max_depth, -1, max_paths_in_flight, width, height)
+        job = ctypes.c_int64(0)
+        st = lib().cav_server_submit_render(self.handle, scene.handle, ctypes.addressof(opts), fs.ctypes.data,
+                                            fw.ctypes.data, ctypes.byref(job))
+        self.ctx._check(st, "cav_server_submit_render")
+        self._keep[job.value] = (scene, fs, fw, opts)
+        return job.value, fs, fw
+
+    def submit_rays(self, bvh: "Bvh", rays: np.ndarray, any_hit: bool = False, limit=None, excl=None):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        lim = None if limit is None else np.ascontiguousarray(limit, np.float32)
+        ex = None if excl is None else np.ascontiguousarray(excl, np.int32)
+        job = ctypes.c_int64(0)
+        if any_hit:
+            out = (np.zeros(n, np.uint8),)
+            st = lib().cav_server_submit_rays(self.handle, bvh.handle, 1, rays.ctypes.data, _np_ptr(lim), _np_ptr(ex),
+                                              n, None, None, None, out[0].ctypes.data, ctypes.byref(job))
+        else:
+            out = (np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros((n, 2), np.float32))
+            st = lib().cav_server_submit_rays(self.handle, bvh.handle, 0, rays.ctypes.data, None, None, n,
+                                              out[0].ctypes.data, out[1].ctypes.data, out[2].ctypes.data, None,
+                                              ctypes.byref(job))
+        self.ctx._check(st, "cav_server_submit_rays")
+        self._keep[job.value] = (bvh, rays, lim, ex, out)
+        return (job.value, *out)
+
+    def wait(self, job: int, timeout_s: float = -1.0) -> JobStatus:
+        out = JobStatus()
+        st = lib().cav_server_wait(self.handle, job, timeout_s, ctypes.addressof(out))
+        if st == 4:
+            raise TimeoutError(f"job {job} not done after {timeout_s} s")
+        self.ctx._check(st, f"job {job}")
+        return out
+
+    def poll(self, job: int) -> JobStatus:
+        out = JobStatus()
+        self.ctx._check(lib().cav_server_poll(self.handle, job, ctypes.addressof(out)), "cav_server_poll")
+        return out
+
+    def release(self, job: int):
+        """Drop the host arrays kept alive for a finished job."""
+        self._keep.pop(job, None)
+
+    def stats(self) -> ServerStats:
+        out = ServerStats()
+        self.ctx._check(lib().cav_server_stats(self.handle, ctypes.addressof(out)), "cav_server_stats")
+        return out
+
+    def close(self):
+        if self.handle:
+            lib().cav_server_destroy(self.handle)
+            self.handle = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _np_ptr(a):
+    return None if a is None else a.ctypes.data
 
 
 def film_to_rgb8(film_sum: np.ndarray, film_weight: np.ndarray) -> np.ndarray:

@@ -132,6 +132,37 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
 cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int32_t* leaf_list, uint32_t* visited,
                           cudaStream_t s);
 // trace.cu
+// A traversal segment: one job's rays against one tree, with its own outputs.  `begin` is
+// the segment's first index in the launch's global ray numbering.
+struct TraceSeg {
+    const TNode* nodes;
+    const TriRec* tris;
+    const float* root_box;
+    const cav_ray* rays;
+    int32_t* prim;     // closest hit
+    float* t;
+    float* uv;
+    const float* limit;  // any hit
+    const int32_t* excl;
+    uint8_t* occ;
+    int64_t begin;
+};
+cav_status trace_closest_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags,
+                                  cudaStream_t s, unsigned long long* counter);
+cav_status trace_any_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags, cudaStream_t s,
+                              unsigned long long* counter);
+int trace_max_segments();
+
+// Resumable path-integrator render (render.cu), advanced bounce by bounce by the server.
+struct PathJob;
+size_t path_job_bytes(const cav_scene* sc, const cav_render_opts* opts);
+cav_status path_job_create(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, cudaStream_t s, PathJob** out);
+int64_t path_job_extend(PathJob* J, TraceSeg* seg);
+cav_status path_job_shade(PathJob* J, cudaStream_t s);
+int64_t path_job_shadow(PathJob* J, TraceSeg* seg);
+cav_status path_job_advance(PathJob* J, cudaStream_t s, bool* finished);
+void path_job_film(PathJob* J, float** sum, float** wsum, int64_t* pixels);
+void path_job_destroy(PathJob* J, cudaStream_t s);
 cav_status trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int32_t* prim, float* t,
                          float* uv, uint32_t flags, cudaStream_t s, unsigned long long* counter);
 cav_status trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,

@@ -328,9 +328,11 @@ struct RayCapture {
 cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
                        cudaStream_t s, const RayCapture* cap = nullptr) {
     const cavpbrt::Scene& D = sc->desc;
+    int W, H;
+    film_size(sc, opts, W, H);
     const int spp = opts && opts->spp > 0 ? opts->spp : D.spp;
     const int max_depth = opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth;
-    const int64_t pixels = (int64_t)D.width * D.height;
+    const int64_t pixels = (int64_t)W * H;
     const int64_t total = pixels * spp;
     int64_t chunk = opts && opts->max_paths_in_flight > 0 ? opts->max_paths_in_flight : (int64_t)1 << 22;
     chunk = std::min(chunk, total);
@@ -373,7 +375,7 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
     Q.counters = carve<uint32_t>(p, 16);
 
     DevScene S = dev_scene_of(sc);
-    Camera cam = camera_of(sc);
+    Camera cam = camera_of(sc, W, H);
     uint32_t counts[2];
     auto& log = sc->log;
     log.reset();
@@ -426,13 +428,203 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
             n = counts[0];
             dim0 += 8 + 2 + (depth > 3 ? 1 : 0);
         }
-        k_film<<<div_up(m, kThreads), kThreads, 0, s>>>(m, P, D.width, D.height, D.filter_xwidth, D.filter_ywidth,
+        k_film<<<div_up(m, kThreads), kThreads, 0, s>>>(m, P, W, H, D.filter_xwidth, D.filter_ywidth,
                                                          d_sum, d_wsum);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     log.end = log.next();
     CAV_CUDA(ctx, cudaEventRecord(log.end, s));
     return CAV_OK;
+}
+
+// ------------------------------------------------------------------ resumable render job
+// The path integrator as a state machine advanced one bounce at a time by the serving loop
+// (serve.cu), whose traversal launches merge the wavefronts of every live job.  Per chunk
+// and bounce it launches exactly the kernels render_path launches, in the same order.
+struct PathJob {
+    cav_ctx* ctx = nullptr;
+    cav_scene* sc = nullptr;
+    int W = 0, H = 0;
+    int spp = 0, max_depth = 0;
+    int64_t total = 0, chunk = 0, first = 0, m = 0, n = 0;
+    int depth = 0, dim0 = 0;
+    void* base = nullptr;
+    float* d_sum = nullptr;
+    float* d_wsum = nullptr;
+    uint32_t* h_counts = nullptr;  // pinned: next rays, shadow rays
+    Paths P;
+    Queues Q;
+    DevScene S;
+    Camera cam;
+    bool done = false;
+};
+
+static size_t path_state_bytes(int64_t chunk) {
+    size_t need = 0;
+    auto acc = [&](size_t bytes) { need += bytes + 256; };
+    acc(8 * chunk); acc(8 * chunk); acc(12 * chunk); acc(12 * chunk); acc(4 * chunk); acc(chunk);
+    acc(4 * chunk); acc(32 * chunk); acc(4 * chunk); acc(32 * chunk);
+    acc(4 * chunk); acc(4 * chunk); acc(8 * chunk);
+    acc(32 * chunk); acc(4 * chunk); acc(8 * chunk); acc(4 * chunk); acc(12 * chunk); acc(chunk); acc(64);
+    return need;
+}
+
+static void job_chunk_sizes(const cav_scene* sc, const cav_render_opts* opts, int& spp, int& depth, int64_t& total,
+                            int64_t& chunk) {
+    const cavpbrt::Scene& D = sc->desc;
+    int W, H;
+    film_size(sc, opts, W, H);
+    spp = opts && opts->spp > 0 ? opts->spp : D.spp;
+    depth = opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth;
+    total = (int64_t)W * H * spp;
+    chunk = opts && opts->max_paths_in_flight > 0 ? opts->max_paths_in_flight : (int64_t)1 << 22;
+    chunk = std::min(chunk, total);
+}
+
+size_t path_job_bytes(const cav_scene* sc, const cav_render_opts* opts) {
+    int spp, depth;
+    int64_t total, chunk;
+    job_chunk_sizes(sc, opts, spp, depth, total, chunk);
+    int W, H;
+    film_size(sc, opts, W, H);
+    return path_state_bytes(chunk) + sizeof(float) * 4 * (int64_t)W * H + 512;
+}
+
+cav_status path_job_create(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, cudaStream_t s, PathJob** out) {
+    auto* J = new PathJob();
+    J->ctx = ctx;
+    J->sc = sc;
+    job_chunk_sizes(sc, opts, J->spp, J->max_depth, J->total, J->chunk);
+    film_size(sc, opts, J->W, J->H);
+    const int64_t pixels = (int64_t)J->W * J->H;
+    const size_t bytes = path_job_bytes(sc, opts);
+    if (cudaMallocAsync(&J->base, bytes, s) != cudaSuccess || cudaMallocHost(&J->h_counts, 16) != cudaSuccess) {
+        cudaGetLastError();
+        if (J->base) cudaFreeAsync(J->base, s);
+        delete J;
+        return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "render job: device allocation failed");
+    }
+    unsigned char* p = (unsigned char*)J->base;
+    J->d_sum = carve<float>(p, 3 * pixels);
+    J->d_wsum = carve<float>(p, pixels);
+    const int64_t c = J->chunk;
+    J->P.sample_index = carve<uint64_t>(p, c);
+    J->P.film_xy = carve<float2>(p, c);
+    J->P.result = carve<float>(p, 3 * c);
+    J->P.throughput = carve<float>(p, 3 * c);
+    J->P.mat_pdf = carve<float>(p, c);
+    J->P.delta = carve<uint8_t>(p, c);
+    J->Q.active = carve<int32_t>(p, c);
+    J->Q.rays = carve<cav_ray>(p, c);
+    J->Q.next_active = carve<int32_t>(p, c);
+    J->Q.next_rays = carve<cav_ray>(p, c);
+    J->Q.hit_prim = carve<int32_t>(p, c);
+    J->Q.hit_t = carve<float>(p, c);
+    J->Q.hit_uv = carve<float>(p, 2 * c);
+    J->Q.shadow_rays = carve<cav_ray>(p, c);
+    J->Q.shadow_limit = carve<float>(p, c);
+    J->Q.shadow_excl = carve<int32_t>(p, 2 * c);
+    J->Q.shadow_path = carve<int32_t>(p, c);
+    J->Q.shadow_contrib = carve<float>(p, 3 * c);
+    J->Q.shadow_occ = carve<uint8_t>(p, c);
+    J->Q.counters = carve<uint32_t>(p, 16);
+    J->S = dev_scene_of(sc);
+    J->cam = camera_of(sc, J->W, J->H);
+    CAV_CUDA(ctx, cudaMemsetAsync(J->d_sum, 0, sizeof(float) * 4 * pixels, s));
+    J->first = 0;
+    J->m = std::min(J->chunk, J->total);
+    k_generate<<<div_up(J->m, kThreads), kThreads, 0, s>>>(J->cam, J->S.halton, J->spp, 0, J->m, J->P, J->Q);
+    J->n = J->m;
+    J->depth = 0;
+    J->dim0 = 0;
+    CAV_CUDA(ctx, cudaGetLastError());
+    *out = J;
+    return CAV_OK;
+}
+
+// The extend segment of the current bounce (0 rays when the job has none this tick).
+int64_t path_job_extend(PathJob* J, TraceSeg* seg) {
+    if (J->done || J->n <= 0) return 0;
+    const cav_bvh* b = J->sc->bvh;
+    *seg = TraceSeg{};
+    seg->nodes = b->tnodes;
+    seg->tris = b->tris;
+    seg->root_box = b->d_root_box;
+    seg->rays = J->Q.rays;
+    seg->prim = J->Q.hit_prim;
+    seg->t = J->Q.hit_t;
+    seg->uv = J->Q.hit_uv;
+    return J->n;
+}
+
+cav_status path_job_shade(PathJob* J, cudaStream_t s) {
+    cav_ctx* ctx = J->ctx;
+    CAV_CUDA(ctx, cudaMemsetAsync(J->Q.counters, 0, 8, s));
+    k_shade<<<div_up(J->n, kThreads), kThreads, 0, s>>>(J->S, J->depth, J->dim0, J->n, J->P, J->Q);
+    CAV_CUDA(ctx, cudaMemcpyAsync(J->h_counts, J->Q.counters, 8, cudaMemcpyDeviceToHost, s));
+    return CAV_OK;
+}
+
+// After the stream has caught up with path_job_shade: the shadow segment.
+int64_t path_job_shadow(PathJob* J, TraceSeg* seg) {
+    const int64_t k = J->h_counts[1];
+    if (k <= 0) return 0;
+    const cav_bvh* b = J->sc->bvh;
+    *seg = TraceSeg{};
+    seg->nodes = b->tnodes;
+    seg->tris = b->tris;
+    seg->root_box = b->d_root_box;
+    seg->rays = J->Q.shadow_rays;
+    seg->limit = J->Q.shadow_limit;
+    seg->excl = J->Q.shadow_excl;
+    seg->occ = J->Q.shadow_occ;
+    return k;
+}
+
+// Adds the unoccluded light samples, advances to the next bounce or chunk; returns whether
+// the job has finished (its film complete on the stream).
+cav_status path_job_advance(PathJob* J, cudaStream_t s, bool* finished) {
+    cav_ctx* ctx = J->ctx;
+    const int64_t k = J->h_counts[1];
+    if (k > 0) k_add_direct<<<div_up(k, kThreads), kThreads, 0, s>>>(k, J->P, J->Q);
+    std::swap(J->Q.active, J->Q.next_active);
+    std::swap(J->Q.rays, J->Q.next_rays);
+    J->n = J->h_counts[0];
+    J->dim0 += 8 + 2 + (J->depth > 3 ? 1 : 0);
+    J->depth += 1;
+    if (J->n <= 0 || J->depth >= J->max_depth) {
+        const cavpbrt::Scene& D = J->sc->desc;
+        k_film<<<div_up(J->m, kThreads), kThreads, 0, s>>>(J->m, J->P, J->W, J->H, D.filter_xwidth,
+                                                            D.filter_ywidth, J->d_sum, J->d_wsum);
+        J->first += J->chunk;
+        if (J->first < J->total) {
+            J->m = std::min(J->chunk, J->total - J->first);
+            k_generate<<<div_up(J->m, kThreads), kThreads, 0, s>>>(J->cam, J->S.halton, J->spp, J->first, J->m, J->P,
+                                                                  J->Q);
+            J->n = J->m;
+            J->depth = 0;
+            J->dim0 = 0;
+        } else {
+            J->done = true;
+            J->n = 0;
+        }
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    *finished = J->done;
+    return CAV_OK;
+}
+
+void path_job_film(PathJob* J, float** sum, float** wsum, int64_t* pixels) {
+    *sum = J->d_sum;
+    *wsum = J->d_wsum;
+    *pixels = (int64_t)J->W * J->H;
+}
+
+void path_job_destroy(PathJob* J, cudaStream_t s) {
+    if (!J) return;
+    if (J->base) cudaFreeAsync(J->base, s);
+    if (J->h_counts) cudaFreeHost(J->h_counts);
+    delete J;
 }
 
 }  // namespace cav
@@ -497,7 +689,9 @@ cav_status cav_render(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, 
     if (!ctx || !sc || !film_sum || !film_weight) return CAV_ERR_INVALID_ARGUMENT;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return cav::cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
     cudaStream_t s = (cudaStream_t)stream;
-    const int64_t pixels = (int64_t)sc->desc.width * sc->desc.height;
+    int W, H;
+    cav::film_size(sc, opts, W, H);
+    const int64_t pixels = (int64_t)W * H;
     CAV_CUDA(ctx, cudaMemsetAsync(film_sum, 0, sizeof(float) * 3 * pixels, s));
     CAV_CUDA(ctx, cudaMemsetAsync(film_weight, 0, sizeof(float) * pixels, s));
     // integrator: the options' choice when given (> 0 selects rlpath), else the scene's
@@ -539,10 +733,12 @@ cav_status cav_render_capture_rays(cav_ctx* ctx, cav_scene* sc, const cav_render
                                    cav_ray* rays_out, int64_t capacity, int64_t* count) {
     if (!ctx || !sc || !rays_out || !count || depth < 0 || capacity <= 0) return CAV_ERR_INVALID_ARGUMENT;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return cav::cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
-    const int64_t pixels = (int64_t)sc->desc.width * sc->desc.height;
+    int W, H;
+    cav::film_size(sc, opts, W, H);
+    const int64_t pixels = (int64_t)W * H;
     float* film = nullptr;
     CAV_CUDA(ctx, cudaMalloc(&film, sizeof(float) * 4 * pixels));
-    cav_render_opts o = opts ? *opts : cav_render_opts{0, 0, 0, 0};
+    cav_render_opts o = opts ? *opts : cav_render_opts{0, 0, 0, 0, 0, 0};
     // one chunk is enough: the capture is taken from the first chunk
     const int spp = o.spp > 0 ? o.spp : sc->desc.spp;
     const int64_t total = pixels * spp;
@@ -565,7 +761,9 @@ cav_status cav_render_to_host(cav_ctx* ctx, cav_scene* sc, const cav_render_opts
                               float* host_weight, float* ms_out) {
     if (!ctx || !sc || !host_sum || !host_weight) return CAV_ERR_INVALID_ARGUMENT;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return cav::cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
-    const int64_t pixels = (int64_t)sc->desc.width * sc->desc.height;
+    int W, H;
+    cav::film_size(sc, opts, W, H);
+    const int64_t pixels = (int64_t)W * H;
     float* d = nullptr;
     CAV_CUDA(ctx, cudaMalloc(&d, sizeof(float) * 4 * pixels));
     cudaEvent_t a, b;

@@ -550,16 +550,25 @@ inline DevScene dev_scene_of(const cav_scene* sc) {
     S.halton = Halton{sc->d_primes, sc->d_perm_start, sc->d_perms};
     return S;
 }
-// PerspectiveCamera constructor (Cameras/PerspectiveCamera.cu:6-20)
-inline Camera camera_of(const cav_scene* sc) {
+// Film resolution of a render: the options' override, else the scene's Film.
+inline void film_size(const cav_scene* sc, const cav_render_opts* o, int& w, int& h) {
+    w = sc->desc.width;
+    h = sc->desc.height;
+    if (o && o->width > 0 && o->height > 0) {
+        w = o->width;
+        h = o->height;
+    }
+}
+// PerspectiveCamera constructor (Cameras/PerspectiveCamera.cu:6-20) for a W x H film
+inline Camera camera_of(const cav_scene* sc, int W, int H) {
     const cavpbrt::Scene& D = sc->desc;
     Camera cam;
     std::memcpy(cam.c2w, D.camera_to_world.data(), 64);
-    cam.width = D.width;
-    cam.height = D.height;
+    cam.width = W;
+    cam.height = H;
     float fov = D.fov_deg * 3.14159265358979323846f / 180.f;
-    if (D.height <= D.width) cam.depth = (D.height / 2.f) / std::tan(fov / 2.f);
-    else cam.depth = (D.width / 2.f) / std::tan(fov / 2.f);
+    if (H <= W) cam.depth = (H / 2.f) / std::tan(fov / 2.f);
+    else cam.depth = (W / 2.f) / std::tan(fov / 2.f);
     return cam;
 }
 }  // namespace

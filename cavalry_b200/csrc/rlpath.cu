@@ -531,7 +531,9 @@ cav_status render_rlpath(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opt
     const cavpbrt::Scene& D = sc->desc;
     const int spp = opts && opts->spp > 0 ? opts->spp : D.spp;
     const int max_depth = opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth;
-    const int64_t pixels = (int64_t)D.width * D.height;
+    int W, H;
+    film_size(sc, opts, W, H);
+    const int64_t pixels = (int64_t)W * H;
     const int64_t total = pixels * spp;
     int64_t chunk = opts && opts->max_paths_in_flight > 0 ? opts->max_paths_in_flight : (int64_t)1 << 22;
     chunk = std::min(chunk, total);
@@ -619,7 +621,7 @@ cav_status render_rlpath(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opt
     int32_t* dims = reinterpret_cast<int32_t*>(Q.counters + 4);  // [0] lighting base, [1] next-ray base
 
     DevScene S = dev_scene_of(sc);
-    Camera cam = camera_of(sc);
+    Camera cam = camera_of(sc, W, H);
     const float* box = sc->bvh->d_root_box;
     uint32_t counts[2];
     auto& log = sc->log;
@@ -675,7 +677,7 @@ cav_status render_rlpath(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opt
             std::swap(Q.rays, Q.next_rays);
             n = counts[0];
         }
-        k_film<<<div_up(m, kThreads), kThreads, 0, s>>>(m, P, D.width, D.height, D.filter_xwidth, D.filter_ywidth,
+        k_film<<<div_up(m, kThreads), kThreads, 0, s>>>(m, P, W, H, D.filter_xwidth, D.filter_ywidth,
                                                          d_sum, d_wsum);
     }
     CAV_CUDA(ctx, cudaGetLastError());

@@ -132,17 +132,42 @@ __device__ inline int64_t claim(unsigned idle, unsigned long long* counter, int6
     return my < n ? my : -1;
 }
 
-template <bool kCullPop, bool kStats>
-__global__ void k_closest(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const float* root_box,
-                          const cav_ray* __restrict__ rays, int64_t n, int32_t* prim, float* tout, float* uv,
+// Segments: one traversal launch over the rays of several jobs, each with its own BVH and
+// output arrays.  A lane that claims global ray g finds its segment by binary search over
+// the segment starts (staged in shared memory) and switches to that segment's tree.
+constexpr int kMaxSeg = 1024;
+
+__device__ inline int find_seg(const int64_t* sbeg, int nseg, int64_t g) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (sbeg[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <bool kCullPop, bool kStats, bool kSeg>
+__global__ void k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
                           unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
-    const float rb0 = root_box[0], rb1 = root_box[1], rb2 = root_box[2];
-    const float rb3 = root_box[3], rb4 = root_box[4], rb5 = root_box[5];
+    __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
+    if (kSeg) {
+        for (int i = threadIdx.x; i < nseg; i += blockDim.x) sbeg[i] = segs[i].begin;
+        __syncthreads();
+    }
+    const TNode* __restrict__ nodes = one.nodes;
+    const TriRec* __restrict__ tris = one.tris;
+    float rb0 = 0.f, rb1 = 0.f, rb2 = 0.f, rb3 = 0.f, rb4 = 0.f, rb5 = 0.f;
+    if (!kSeg) {
+        rb0 = one.root_box[0]; rb1 = one.root_box[1]; rb2 = one.root_box[2];
+        rb3 = one.root_box[3]; rb4 = one.root_box[4]; rb5 = one.root_box[5];
+    }
     int32_t stack[kStack];
     float sdist[kCullPop ? kStack : 1];
     TraceStats st;
     bool more = true;
-    int64_t ray = -1;
+    int64_t ray = -1;  // index within the lane's segment
+    int seg = 0;
     f3 o = mk(0, 0, 0), d = mk(0, 0, 0), inv = mk(0, 0, 0);
     float tmax = 0.f, best = 0.f, bu = 0.f, bv = 0.f;
     int32_t bid = -1, ref = 0;
@@ -155,6 +180,17 @@ __global__ void k_closest(const TNode* __restrict__ nodes, const TriRec* __restr
         if (more && idle != 0 && (__popc(idle) >= refill || idle == kFull)) {
             int64_t r = claim(idle, counter, n, more);
             if (r >= 0) {
+                const cav_ray* rays = one.rays;
+                if (kSeg) {
+                    seg = find_seg(sbeg, nseg, r);
+                    const TraceSeg& S = segs[seg];
+                    nodes = S.nodes;
+                    tris = S.tris;
+                    rays = S.rays;
+                    r -= S.begin;
+                    rb0 = S.root_box[0]; rb1 = S.root_box[1]; rb2 = S.root_box[2];
+                    rb3 = S.root_box[3]; rb4 = S.root_box[4]; rb5 = S.root_box[5];
+                }
                 const float4* rp = reinterpret_cast<const float4*>(rays + r);
                 float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
                 o = mk(r0.x, r0.y, r0.z);
@@ -170,9 +206,10 @@ __global__ void k_closest(const TNode* __restrict__ nodes, const TriRec* __restr
                 steps = 0;
                 ray = r;
                 if (!(slab(rb0, rb1, rb2, rb3, rb4, rb5, o, inv) >= 0.f)) {
-                    prim[r] = -1;  // BVH::intersect returns early when the root box is missed
-                    if (tout) tout[r] = __int_as_float(0x7f800000);
-                    if (uv) reinterpret_cast<float2*>(uv)[r] = make_float2(0.f, 0.f);
+                    const TraceSeg& S = kSeg ? segs[seg] : one;
+                    S.prim[r] = -1;  // BVH::intersect returns early when the root box is missed
+                    if (S.t) S.t[r] = __int_as_float(0x7f800000);
+                    if (S.uv) reinterpret_cast<float2*>(S.uv)[r] = make_float2(0.f, 0.f);
                     ray = -1;
                 }
             }
@@ -238,35 +275,57 @@ __global__ void k_closest(const TNode* __restrict__ nodes, const TriRec* __restr
             else ref = stack[top--];
         }
         if (finished) {
-            prim[ray] = hit ? bid : (bid == -2 ? -2 : -1);
-            if (tout) tout[ray] = hit ? best : __int_as_float(0x7f800000);
-            if (uv) reinterpret_cast<float2*>(uv)[ray] = make_float2(bu, bv);
+            const TraceSeg& S = kSeg ? segs[seg] : one;
+            S.prim[ray] = hit ? bid : (bid == -2 ? -2 : -1);
+            if (S.t) S.t[ray] = hit ? best : __int_as_float(0x7f800000);
+            if (S.uv) reinterpret_cast<float2*>(S.uv)[ray] = make_float2(bu, bv);
             ray = -1;
         }
     }
     flush_stats<kStats>(st, stats);
 }
 
-template <bool kCullPop, bool kStats>
-__global__ void k_any(const TNode* __restrict__ nodes, const TriRec* __restrict__ tris, const cav_ray* __restrict__ rays,
-                      const float* __restrict__ limit, const int32_t* __restrict__ excl, int64_t n, uint8_t* occ,
+template <bool kCullPop, bool kStats, bool kSeg>
+__global__ void k_any(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
                       unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
+    __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
+    if (kSeg) {
+        for (int i = threadIdx.x; i < nseg; i += blockDim.x) sbeg[i] = segs[i].begin;
+        __syncthreads();
+    }
+    const TNode* __restrict__ nodes = one.nodes;
+    const TriRec* __restrict__ tris = one.tris;
     int32_t stack[kStack];
     TraceStats st;
     bool more = true;
     int64_t ray = -1;
+    int seg = 0;
     f3 o = mk(0, 0, 0), d = mk(0, 0, 0), inv = mk(0, 0, 0);
     float lim = 0.f;
     int32_t src = -1, dst = -1, ref = 0;
     int top = -1;
     uint32_t steps = 0;
-    const bool use_limit = limit != nullptr;
+    bool use_limit = one.limit != nullptr;
     for (;;) {
         const unsigned idle = __ballot_sync(kFull, ray < 0);
         if (idle == kFull && !more) break;
         if (more && idle != 0 && (__popc(idle) >= refill || idle == kFull)) {
             int64_t r = claim(idle, counter, n, more);
             if (r >= 0) {
+                const cav_ray* rays = one.rays;
+                const float* limit = one.limit;
+                const int32_t* excl = one.excl;
+                if (kSeg) {
+                    seg = find_seg(sbeg, nseg, r);
+                    const TraceSeg& S = segs[seg];
+                    nodes = S.nodes;
+                    tris = S.tris;
+                    rays = S.rays;
+                    limit = S.limit;
+                    excl = S.excl;
+                    use_limit = limit != nullptr;
+                    r -= S.begin;
+                }
                 const float4* rp = reinterpret_cast<const float4*>(rays + r);
                 float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
                 o = mk(r0.x, r0.y, r0.z);
@@ -339,7 +398,7 @@ __global__ void k_any(const TNode* __restrict__ nodes, const TriRec* __restrict_
         }
         if (result >= 0) {
             if (result == 2) atomicOr(flag, 1);
-            occ[ray] = (uint8_t)result;
+            (kSeg ? segs[seg] : one).occ[ray] = (uint8_t)result;
             ray = -1;
         }
     }
@@ -356,41 +415,45 @@ int grid_for(cav_ctx* ctx, K kernel, int block) {
     return ctx->num_sms * per_sm;
 }
 
-template <bool kStats>
-cav_status launch_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int32_t* prim, float* t,
-                          float* uv, uint32_t flags, cudaStream_t s, unsigned long long* counter,
-                          unsigned long long* stats) {
+TraceSeg seg_of(const cav_bvh* bvh) {
+    TraceSeg g{};
+    g.nodes = bvh->tnodes;
+    g.tris = bvh->tris;
+    g.root_box = bvh->d_root_box;
+    return g;
+}
+
+template <bool kStats, bool kSeg>
+cav_status launch_closest(cav_ctx* ctx, const TraceSeg& one, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags,
+                          cudaStream_t s, unsigned long long* counter, unsigned long long* stats) {
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
     const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     if (flags & CAV_TRACE_CULL_ON_POP) {
-        int grid = grid_for(ctx, k_closest<true, kStats>, block);
-        k_closest<true, kStats><<<grid, block, 0, s>>>(bvh->tnodes, bvh->tris, bvh->d_root_box, rays, n, prim, t, uv,
-                                                       counter, batch, ctx->d_error + 2, stats);
+        int grid = grid_for(ctx, k_closest<true, kStats, kSeg>, block);
+        k_closest<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 2,
+                                                             stats);
     } else {
-        int grid = grid_for(ctx, k_closest<false, kStats>, block);
-        k_closest<false, kStats><<<grid, block, 0, s>>>(bvh->tnodes, bvh->tris, bvh->d_root_box, rays, n, prim, t, uv,
-                                                        counter, batch, ctx->d_error + 2, stats);
+        int grid = grid_for(ctx, k_closest<false, kStats, kSeg>, block);
+        k_closest<false, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 2,
+                                                              stats);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;
 }
 
-template <bool kStats>
-cav_status launch_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit, const int32_t* excl,
-                      int64_t n, uint8_t* occ, uint32_t flags, cudaStream_t s, unsigned long long* counter,
-                      unsigned long long* stats) {
+template <bool kStats, bool kSeg>
+cav_status launch_any(cav_ctx* ctx, const TraceSeg& one, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags,
+                      cudaStream_t s, unsigned long long* counter, unsigned long long* stats) {
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
     const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     if (flags & CAV_TRACE_CULL_ON_POP) {
-        int grid = grid_for(ctx, k_any<true, kStats>, block);
-        k_any<true, kStats><<<grid, block, 0, s>>>(bvh->tnodes, bvh->tris, rays, limit, excl, n, occ, counter, batch,
-                                                   ctx->d_error + 3, stats);
+        int grid = grid_for(ctx, k_any<true, kStats, kSeg>, block);
+        k_any<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 3, stats);
     } else {
-        int grid = grid_for(ctx, k_any<false, kStats>, block);
-        k_any<false, kStats><<<grid, block, 0, s>>>(bvh->tnodes, bvh->tris, rays, limit, excl, n, occ, counter, batch,
-                                                    ctx->d_error + 3, stats);
+        int grid = grid_for(ctx, k_any<false, kStats, kSeg>, block);
+        k_any<false, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 3, stats);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;
@@ -403,7 +466,12 @@ cav_status trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, 
     if (!bvh || !rays || !prim || n < 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_trace_closest: bad args");
     if (((uintptr_t)rays & 15) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
     if (n == 0) return CAV_OK;
-    return launch_closest<false>(ctx, bvh, rays, n, prim, t, uv, flags, s, counter, nullptr);
+    TraceSeg one = seg_of(bvh);
+    one.rays = rays;
+    one.prim = prim;
+    one.t = t;
+    one.uv = uv;
+    return launch_closest<false, false>(ctx, one, nullptr, 0, n, flags, s, counter, nullptr);
 }
 
 cav_status trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit, const int32_t* excl,
@@ -412,7 +480,12 @@ cav_status trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, cons
     if (((uintptr_t)rays & 15) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
     if (excl && ((uintptr_t)excl & 7) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "excl must be 8-byte aligned");
     if (n == 0) return CAV_OK;
-    return launch_any<false>(ctx, bvh, rays, limit, excl, n, occ, flags, s, counter, nullptr);
+    TraceSeg one = seg_of(bvh);
+    one.rays = rays;
+    one.limit = limit;
+    one.excl = excl;
+    one.occ = occ;
+    return launch_any<false, false>(ctx, one, nullptr, 0, n, flags, s, counter, nullptr);
 }
 
 cav_status trace_stats(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
@@ -426,11 +499,18 @@ cav_status trace_stats(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, in
     unsigned char* out = (unsigned char*)tmp + 64;
     CAV_CUDA(ctx, cudaMemsetAsync(stats, 0, 16, s));
     cav_status st;
-    if (any_hit)
-        st = launch_any<true>(ctx, bvh, rays, limit, excl, n, out, flags, s, ctx->d_counters + 4, stats);
-    else
-        st = launch_closest<true>(ctx, bvh, rays, n, (int32_t*)out, (float*)(out + 4 * n), nullptr, flags, s,
-                                  ctx->d_counters + 4, stats);
+    TraceSeg one = seg_of(bvh);
+    one.rays = rays;
+    if (any_hit) {
+        one.limit = limit;
+        one.excl = excl;
+        one.occ = out;
+        st = launch_any<true, false>(ctx, one, nullptr, 0, n, flags, s, ctx->d_counters + 4, stats);
+    } else {
+        one.prim = (int32_t*)out;
+        one.t = (float*)(out + 4 * n);
+        st = launch_closest<true, false>(ctx, one, nullptr, 0, n, flags, s, ctx->d_counters + 4, stats);
+    }
     if (st != CAV_OK) return st;
     unsigned long long h[2];
     CAV_CUDA(ctx, cudaMemcpyAsync(h, stats, 16, cudaMemcpyDeviceToHost, s));
@@ -440,5 +520,29 @@ cav_status trace_stats(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, in
     host2[1] = h[1];
     return CAV_OK;
 }
+
+}  // namespace cav
+
+namespace cav {
+
+// One launch over several segments (jobs): segs is a DEVICE array of nseg records whose
+// `begin` fields are the prefix sums of their ray counts; n = the total.
+cav_status trace_closest_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags,
+                                  cudaStream_t s, unsigned long long* counter) {
+    if (nseg <= 0 || n == 0) return CAV_OK;
+    if (nseg > kMaxSeg) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "too many trace segments in one launch");
+    TraceSeg none{};
+    return launch_closest<false, true>(ctx, none, segs, nseg, n, flags, s, counter, nullptr);
+}
+
+cav_status trace_any_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags, cudaStream_t s,
+                              unsigned long long* counter) {
+    if (nseg <= 0 || n == 0) return CAV_OK;
+    if (nseg > kMaxSeg) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "too many trace segments in one launch");
+    TraceSeg none{};
+    return launch_any<false, true>(ctx, none, segs, nseg, n, flags, s, counter, nullptr);
+}
+
+int trace_max_segments() { return kMaxSeg; }
 
 }  // namespace cav

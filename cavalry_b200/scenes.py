@@ -317,3 +317,24 @@ def sphere_scene(n_spheres: int = 64, level: int = 6, seed: int = 3, room=(20.0,
         "camera": {"eye": (0.0, H * 0.45, z0 + 0.5), "look": (0.0, H * 0.35, 0.0), "up": (0.0, 1.0, 0.0),
                    "fov": 60.0},
     }
+
+
+def soup_scene(n: int, seed: int):
+    """A config-2-type soup (`soup(n, seed)`, matte grey) under a 0.6 x 0.6 area light
+    (radiance 20) above the unit cube, seen from the front: the scenes of the served job
+    stream."""
+    pos, idx = soup(n, seed=seed)
+    light_v = np.array([[0.2, 1.5, 0.2], [0.8, 1.5, 0.2], [0.8, 1.5, 0.8], [0.2, 1.5, 0.8]], np.float32)
+    positions = np.concatenate([pos.astype(np.float32), light_v])
+    base = len(pos)
+    indices = np.concatenate([idx.astype(np.int32), np.array([[base, base + 1, base + 2], [base, base + 2, base + 3]],
+                                                               np.int32)])
+    mesh_ids = np.concatenate([np.zeros(len(idx), np.int32), np.ones(2, np.int32)])
+    return {
+        "positions": np.ascontiguousarray(positions),
+        "indices": np.ascontiguousarray(indices),
+        "mesh_ids": mesh_ids,
+        "meshes": [("soup", 0, len(idx), (0.6, 0.6, 0.6)), ("light0", len(idx), 2, (0.0, 0.0, 0.0))],
+        "lights": [(1, (20.0, 20.0, 20.0))],
+        "camera": {"eye": (0.5, 0.6, -1.6), "look": (0.5, 0.5, 0.5), "up": (0.0, 1.0, 0.0), "fov": 45.0},
+    }

@@ -206,6 +206,7 @@ typedef struct cav_render_opts {
     int max_depth;               /* <= 0: the scene's Integrator "maxdepth" */
     int integrator;              /* 0: the scene's Integrator ("path" or "rlpath"); -1: path; 1: rlpath */
     int64_t max_paths_in_flight; /* <= 0: 4M; samples are rendered in chunks of this many paths */
+    int width, height;           /* <= 0: the scene's Film resolution (the camera keeps its fov) */
 } cav_render_opts;
 
 /* Host-only .pbrt parse (no GPU): scene counts and the camera-to-world matrix (16 floats,
@@ -252,6 +253,51 @@ cav_status cav_film_to_rgb8(const float* film_sum, const float* film_weight, int
 /* Image writers: 8-bit RGB PNG (the reference's output format) and a float PFM of sum/weight. */
 cav_status cav_write_png(const char* path, const uint8_t* rgb, int width, int height);
 cav_status cav_write_pfm(const char* path, const float* film_sum, const float* film_weight, int width, int height);
+
+/*
+ * Serving with continuous batching (serve.cu).  A server owns a host thread and a stream;
+ * jobs are admitted FIFO as the HBM budget and the live-job limit allow, and every tick
+ * advances all live jobs by one bounce with one merged closest-hit and one merged any-hit
+ * traversal launch over all their rays (each job against its own resident BVH).
+ * CAV_SERVE_SEQUENTIAL runs one job at a time through the same kernels: the plain
+ * sequential loop.  Scenes, BVHs and host buffers must outlive their jobs.
+ */
+typedef struct cav_server cav_server;
+enum { CAV_SERVE_MERGED = 0, CAV_SERVE_SEQUENTIAL = 1 };
+enum { CAV_JOB_PENDING = 0, CAV_JOB_RUNNING = 1, CAV_JOB_DONE = 2, CAV_JOB_FAILED = 3 };
+typedef struct cav_server_config {
+    int64_t hbm_budget_bytes; /* <= 0: 80 GiB */
+    int mode;                 /* CAV_SERVE_MERGED or CAV_SERVE_SEQUENTIAL */
+    int max_live_jobs;        /* <= 0: 64 */
+    int64_t max_paths_per_job; /* paths a render job keeps in flight (its time slice per tick);
+                                  <= 0: 1M; a job's own max_paths_in_flight, when set, wins */
+} cav_server_config;
+typedef struct cav_job_status {
+    int state;         /* CAV_JOB_* */
+    cav_status status; /* final status of a finished job */
+    double t_submit, t_start, t_done; /* seconds on the server's clock (cav_server_stats.now_s) */
+    int64_t bounces;   /* ticks a render job took part in */
+} cav_job_status;
+typedef struct cav_server_stats_t {
+    int64_t ticks, closest_launches, any_launches, max_segments;
+    double busy_s, now_s;
+    int64_t pending, live, hbm_in_use;
+} cav_server_stats_t;
+cav_status cav_server_create(cav_ctx* ctx, const cav_server_config* cfg, cav_server** out);
+/* Finishes the live jobs, fails the pending ones (CAV_ERR_NOT_READY) and joins the thread. */
+cav_status cav_server_destroy(cav_server* server);
+/* A render (path integrator) of a loaded scene into HOST films (3 + 1 floats per pixel). */
+cav_status cav_server_submit_render(cav_server* server, cav_scene* scene, const cav_render_opts* opts,
+                                    float* host_sum, float* host_weight, int64_t* job_id);
+/* A ray-query job on HOST arrays: closest hit (prim, t, uv; t/uv may be NULL) or any hit
+ * (occ; limit / excl may be NULL), with the semantics of cav_trace_closest / cav_trace_any. */
+cav_status cav_server_submit_rays(cav_server* server, const cav_bvh* bvh, int any_hit, const cav_ray* host_rays,
+                                  const float* host_limit, const int32_t* host_excl, int64_t n, int32_t* host_prim,
+                                  float* host_t, float* host_uv, uint8_t* host_occ, int64_t* job_id);
+cav_status cav_server_poll(cav_server* server, int64_t job_id, cav_job_status* status);
+/* Waits for a job (timeout_s < 0: forever); returns the job's status or CAV_ERR_TIMEOUT. */
+cav_status cav_server_wait(cav_server* server, int64_t job_id, double timeout_s, cav_job_status* status);
+cav_status cav_server_stats(cav_server* server, cav_server_stats_t* out);
 
 /* Device-side event timing of the last build's stages (ms): leaf boxes + Morton,
  * sort, radix tree, refit, treelet rounds, layout.  Valid after the stream is synced. */

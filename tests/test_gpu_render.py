@@ -186,3 +186,17 @@ def test_rlpath_converges_to_path(ctx, tmp_path):
     e_rl = relmse(s / w[..., None])
     assert e_rl <= 1.5 * e_path, (e_rl, e_path)
     assert abs((s / w[..., None]).mean() - ref.mean()) <= 0.01 * ref.mean()
+
+
+def test_resolution_override_matches_scene_film(ctx, tmp_path):
+    """Render options' width/height give the image of a scene whose Film has that size."""
+    from cavalry_b200 import scenes
+
+    room = scenes.mini_room()
+    small, _ = load(ctx, tmp_path, "res_a", room, dict(width=32, height=24, spp=2, max_depth=3))
+    big, _ = load(ctx, tmp_path, "res_b", room, dict(width=80, height=60, spp=2, max_depth=3))
+    s1, w1, _ = small.render(width=80, height=60)
+    s2, w2, _ = big.render()
+    assert s1.shape == (60, 80, 3)
+    assert np.array_equal(w1, w2)
+    assert np.allclose(s1, s2, rtol=2e-5, atol=1e-6)

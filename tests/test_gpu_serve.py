@@ -1,0 +1,110 @@
+"""GPU tests of the serving loop (serve.cu): each job's result is the same through the
+server as through the direct entry points, alone and in a mix of concurrent jobs, in the
+merged (continuous batching) and sequential modes."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import cavalry_b200 as cav
+
+    return cav.Context(0)
+
+
+@pytest.fixture(scope="module")
+def pool(ctx, tmp_path_factory):
+    from cavalry_b200 import scenes
+
+    d = tmp_path_factory.mktemp("serve")
+    out = {}
+    for k, (n, res) in enumerate([(2000, 48), (30000, 64), (120000, 32)]):
+        p = str(d / f"s{k}.pbrt")
+        scenes.write_pbrt(p, scenes.soup_scene(n, seed=50 + k), width=res, height=res, spp=2, max_depth=4)
+        out[k] = ctx.load_pbrt(p, bvh_rounds=2)
+    return out
+
+
+def direct_render(sc, spp):
+    s, w, _ = sc.render(spp=spp, max_depth=4, integrator="path")
+    return s, w
+
+
+def test_ray_jobs_match_direct_queries(ctx, pool):
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    bvh = pool[1].bvh()
+    rays = scenes.closest_rays(50000, seed=3)
+    srays, lim = scenes.shadow_rays(40000, seed=4)
+    prim, t, uv = bvh.trace_closest(torch.from_numpy(rays).cuda())
+    occ = bvh.trace_any(torch.from_numpy(srays).cuda(), torch.from_numpy(lim).cuda())
+    sv = cav.Server(ctx)
+    j1, p1, t1, uv1 = sv.submit_rays(bvh, rays)
+    j2, o2 = sv.submit_rays(bvh, srays, any_hit=True, limit=lim)
+    assert sv.wait(j1, 60).state == cav.JOB_DONE and sv.wait(j2, 60).state == cav.JOB_DONE
+    sv.close()
+    assert np.array_equal(p1, prim.cpu().numpy())
+    assert np.array_equal(t1.view(np.uint32), t.cpu().numpy().view(np.uint32))
+    assert np.array_equal(o2, occ.cpu().numpy())
+
+
+@pytest.mark.parametrize("mode", ["merged", "sequential"])
+def test_mixed_jobs_same_as_alone(ctx, pool, mode):
+    """Renders of three scenes and two ray-query jobs submitted together: every result
+    equals the job run alone (films up to float atomic order)."""
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    alone = {k: direct_render(sc, 2) for k, sc in pool.items()}
+    sv = cav.Server(ctx, mode=cav.SERVE_MERGED if mode == "merged" else cav.SERVE_SEQUENTIAL)
+    subs = []
+    for k, sc in pool.items():
+        jid, fs, fw = sv.submit_render(sc, spp=2, max_depth=4)
+        subs.append((jid, k, fs, fw))
+    bvh = pool[2].bvh()
+    rays = scenes.closest_rays(30000, seed=9)
+    jr, pr, tr, _ = sv.submit_rays(bvh, rays)
+    for jid, k, fs, fw in subs:
+        st = sv.wait(jid, 120)
+        assert st.state == cav.JOB_DONE and st.t_done >= st.t_start >= st.t_submit
+        s, w = alone[k]
+        assert np.array_equal(fw, w)
+        assert np.allclose(fs, s, rtol=2e-5, atol=1e-6)
+    sv.wait(jr, 60)
+    stats = sv.stats()
+    sv.close()
+    import torch
+
+    p, _, _ = bvh.trace_closest(torch.from_numpy(rays).cuda())
+    assert np.array_equal(pr, p.cpu().numpy())
+    if mode == "merged":
+        # the five jobs shared traversal launches
+        assert stats.max_segments >= 2
+    else:
+        assert stats.max_segments == 1
+
+
+def test_small_hbm_budget_still_completes(ctx, pool):
+    """Jobs larger than the budget run one at a time instead of waiting forever."""
+    import cavalry_b200 as cav
+
+    sv = cav.Server(ctx, hbm_budget_bytes=1 << 20)
+    ids = [sv.submit_render(sc, spp=1, max_depth=2)[0] for sc in pool.values()]
+    for jid in ids:
+        assert sv.wait(jid, 120).state == cav.JOB_DONE
+    assert sv.stats().max_segments == 1
+    sv.close()
+
+
+def test_server_close_with_pending_jobs(ctx, pool):
+    import cavalry_b200 as cav
+
+    sv = cav.Server(ctx, max_live_jobs=1)
+    ids = [sv.submit_render(pool[1], spp=4, max_depth=4)[0] for _ in range(4)]
+    sv.wait(ids[0], 120)
+    sv.close()  # finishes the live job, fails the never-started ones
