@@ -183,6 +183,8 @@ def run_ours(args):
     tt = torch.empty(N_RAYS, dtype=torch.float32, device=dev)
     uv = torch.empty((N_RAYS, 2), dtype=torch.float32, device=dev)
     out = (prim, tt, uv)
+    # launch shape picked by the project's autotuner on a separate 1M-ray sample
+    tuned = bvh.autotune(torch.from_numpy(scenes.closest_rays(1 << 20, seed=90 + rank)).to(dev))
     nodes_v, tris_t = bvh.trace_stats(rays)
     nodes_per_ray = nodes_v / N_RAYS
     tris_per_ray = tris_t / N_RAYS
@@ -288,6 +290,8 @@ def run_ours(args):
             "rays_per_step": N_RAYS,
             "treelet_rounds": ROUNDS,
             "trace_mode": "exact (reference order and pruning)",
+            "launch_shape": {"block": tuned["block_threads"], "queue_chunk": tuned["batch"], "stack": tuned["stack"],
+                             "picked_by": "cav_trace_autotune on a separate 1M-ray sample"},
             "l2": "flushed between timed steps (256 MiB write); rays 128 MiB > L2",
             "parallelism": f"replicas x{world}",
         },
@@ -443,6 +447,11 @@ def run_render(args):
         load_s = time.time() - t0
         for _ in range(max(args.warmup, 1)):  # warm-up: full-resolution 1-spp renders
             sc.render(spp=1)
+        # the project's autotuner picks the traversal launch shape on the renderer's own
+        # bounce-0 and bounce-1 rays (a 1M-ray sample of each)
+        bvh = sc.bvh()
+        tune_rays = torch.cat([sc.capture_rays(d, capacity=1 << 20) for d in (0, 1)])
+        tuned = bvh.autotune(tune_rays)
         fs = torch.empty(H * W * 3, device="cuda")
         fw = torch.empty(H * W, device="cuda")
         if rounds == 3:
@@ -467,11 +476,15 @@ def run_render(args):
             "ms_closest": round(st["ms_closest"], 2), "ms_any": round(st["ms_any"], 2),
             "ms_shade": round(st["ms_shade"], 2), "bounces": st["bounces"],
         }
-        # the renderer's own bounce-0 and bounce-1 rays, traced alone by ours (same tree)
-        bvh = sc.bvh()
+        runs[rounds]["launch_shape"] = {k: tuned[k] for k in ("block_threads", "batch", "stack")}
+        # the renderer's own bounce-0 and bounce-1 rays, traced alone by ours (same tree),
+        # with the launch shape tuned for each bounce's rays
         caps = [sc.capture_rays(d, capacity=1 << 22) for d in (0, 1)]
         ours = []
+        shapes = []
         for r in caps:
+            t_b = bvh.autotune(r)
+            shapes.append({k: t_b[k] for k in ("block_threads", "batch", "stack")})
             for _ in range(3):
                 bvh.trace_closest(r)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -482,6 +495,7 @@ def run_render(args):
             torch.cuda.synchronize()
             ours.append(len(r) * 5 / (a.elapsed_time(b) * 1e-3) / 1e6)
         runs[rounds]["captured_rays"] = [int(len(r)) for r in caps]
+        runs[rounds]["captured_launch_shapes"] = shapes
         runs[rounds]["ours_captured_mrays_s"] = [round(x, 2) for x in ours]
         captured[rounds] = ([r.cpu().numpy() for r in caps], bvh.export_nodes())
         if rounds == 0:

@@ -94,6 +94,7 @@ def lib() -> ctypes.CDLL:
         "cav_render_to_host": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render_stats": ([P, P], ctypes.c_int),
+        "cav_trace_autotune": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, P, P], ctypes.c_int),
         "cav_server_create": ([P, P, ctypes.POINTER(P)], ctypes.c_int),
         "cav_server_destroy": ([P], ctypes.c_int),
         "cav_server_submit_render": ([P, P, P, P, P, P], ctypes.c_int),
@@ -206,11 +207,13 @@ class SceneInfo(ctypes.Structure):
 
 
 _INTEGRATORS = {None: 0, "path": -1, "rlpath": 1}
+RENDER_GRAPH = 1
 
 
 class RenderOpts(ctypes.Structure):
     _fields_ = [("spp", ctypes.c_int), ("max_depth", ctypes.c_int), ("integrator", ctypes.c_int),
-                ("max_paths_in_flight", ctypes.c_int64), ("width", ctypes.c_int), ("height", ctypes.c_int)]
+                ("max_paths_in_flight", ctypes.c_int64), ("width", ctypes.c_int), ("height", ctypes.c_int),
+                ("flags", ctypes.c_int)]
 
 
 def parse_pbrt(path: str, spp: int = -1, integrator: str | None = None) -> tuple[SceneInfo, np.ndarray]:
@@ -247,7 +250,7 @@ class Scene:
         return out
 
     def render(self, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0, integrator: str | None = None,
-               width: int = 0, height: int = 0):
+               width: int = 0, height: int = 0, graph: bool = False):
         """Render to host arrays; returns (film_sum [H,W,3], film_weight [H,W], ms).  integrator:
         None = the scene's, "path" or "rlpath"; width/height override the Film resolution."""
         inf = self.info()
@@ -255,19 +258,21 @@ class Scene:
         s = np.zeros((H, W, 3), np.float32)
         w = np.zeros((H, W), np.float32)
         ms = np.zeros(1, np.float32)
-        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height)
+        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height,
+                          RENDER_GRAPH if graph else 0)
         st = lib().cav_render_to_host(self.ctx.handle, self.handle, ctypes.addressof(opts), s.ctypes.data,
                                       w.ctypes.data, ms.ctypes.data)
         self.ctx._check(st, "cav_render_to_host")
         return s, w, float(ms[0])
 
     def render_into(self, film_sum, film_weight, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0,
-                    stream=None, integrator: str | None = None, width: int = 0, height: int = 0):
+                    stream=None, integrator: str | None = None, width: int = 0, height: int = 0, graph: bool = False):
         """Render into DEVICE films (pointers, or objects with data_ptr(): 3 + 1 floats per
         pixel), stream-ordered on `stream` (a pointer, an object with cuda_stream, or None)."""
         ptr = lambda x: x if isinstance(x, int) else x.data_ptr()  # noqa: E731
         st_ptr = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
-        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height)
+        opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height,
+                          RENDER_GRAPH if graph else 0)
         st = lib().cav_render(self.ctx.handle, self.handle, ctypes.addressof(opts), ptr(film_sum), ptr(film_weight),
                               st_ptr)
         self.ctx._check(st, "cav_render")
@@ -429,6 +434,14 @@ def film_to_rgb8(film_sum: np.ndarray, film_weight: np.ndarray) -> np.ndarray:
     return out
 
 
+class TraceConfig(ctypes.Structure):
+    _fields_ = [("block_threads", ctypes.c_int), ("blocks_per_sm", ctypes.c_int), ("batch", ctypes.c_int),
+                ("stack", ctypes.c_int), ("ms", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Bvh:
     """A built BVH (cav_bvh).  Device memory is released by :meth:`free`."""
 
@@ -474,6 +487,14 @@ class Bvh:
         ms = np.zeros(6, np.float32)
         self.ctx._check(lib().cav_bvh_stage_times(self.ctx.handle, self.handle, ms.ctypes.data), "cav_bvh_stage_times")
         return [float(x) for x in ms]
+
+    def autotune(self, rays, any_hit: bool = False, limit=None, excl=None, stream=None) -> dict:
+        """Pick and install the fastest traversal launch shape for this tree on a CUDA ray sample."""
+        out = TraceConfig()
+        st = lib().cav_trace_autotune(self.ctx.handle, self.handle, _ptr(rays), rays.shape[0], int(any_hit),
+                                      _ptr(limit), _ptr(excl), _stream_ptr(stream), ctypes.addressof(out))
+        self.ctx._check(st, "cav_trace_autotune")
+        return out.as_dict()
 
     def trace_closest(self, rays, flags: int = TRACE_EXACT, stream=None, out=None):
         """rays: float32 [n,8] CUDA (o.xyz, tmin, d.xyz, tmax).  Returns (prim int32, t float32, uv float32 [n,2])."""

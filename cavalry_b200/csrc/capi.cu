@@ -223,6 +223,7 @@ cav_status cav_bvh_depth(cav_ctx* ctx, const cav_bvh* bvh, void* stream, int32_t
         }
     }
     *depth = best;
+    bvh->depth = best;
     return CAV_OK;
 }
 

@@ -87,6 +87,7 @@ struct cav_ctx {
     int trace_block = 0;
     int trace_blocks_per_sm = 0;
     int trace_batch = 0;
+    int trace_stack = 0;  // 64 selects the short traversal stack for trees known to be shallow
     // persistent work counters (device), one per concurrent trace kind
     unsigned long long* d_counters = nullptr;
     int* d_error = nullptr;
@@ -101,6 +102,7 @@ struct cav_ctx {
 
 struct cav_bvh {
     int64_t n = 0;  // triangles
+    mutable int32_t depth = -1;  // tree depth once measured (cav_bvh_depth), else -1
     int device = 0;
     // build products
     cav::BNode* nodes = nullptr;       // 2N-1 restructure records (reference order)
@@ -146,12 +148,20 @@ struct TraceSeg {
     const int32_t* excl;
     uint8_t* occ;
     int64_t begin;
+    const uint32_t* n_dev;  // single-tree launches: ray count read from device memory (or null)
 };
 cav_status trace_closest_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags,
                                   cudaStream_t s, unsigned long long* counter);
 cav_status trace_any_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags, cudaStream_t s,
                               unsigned long long* counter);
 int trace_max_segments();
+// Single-tree traversal whose ray count is read from device memory at launch (n_dev),
+// n_max bounding it; for launch chains without host round trips (CUDA graphs).
+cav_status trace_closest_dev(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const uint32_t* n_dev,
+                             int32_t* prim, float* t, float* uv, cudaStream_t s, unsigned long long* counter);
+cav_status trace_any_dev(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,
+                         const int32_t* excl, const uint32_t* n_dev, uint8_t* occ, cudaStream_t s,
+                         unsigned long long* counter);
 
 // Resumable path-integrator render (render.cu), advanced bounce by bounce by the server.
 struct PathJob;

@@ -27,8 +27,11 @@ namespace {
 // intersectScene + computeLighting + genNextRay (PathTracingIntegrator.cu:95-225) for one
 // bounce; the shadow ray is traced in a separate any-hit launch and its contribution added
 // by k_add_direct (evalMaterial, :227-249, is folded in here).
-__global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Queues Q) {
+// n_dev (or null): the queue size read from device memory (graph-replayed bounces)
+__global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Queues Q,
+                        const uint32_t* n_dev = nullptr) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n_dev) n = *n_dev;
     bool valid = j < n;
     int path = valid ? Q.active[j] : 0;
     int prim = valid ? Q.hit_prim[j] : -1;
@@ -162,8 +165,9 @@ __global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Que
 
 // evalMaterial's accumulation for unoccluded shadow rays.  The paths of one bounce are
 // distinct, so plain read-modify-write is race free.
-__global__ void k_add_direct(int64_t n, Paths P, Queues Q) {
+__global__ void k_add_direct(int64_t n, Paths P, Queues Q, const uint32_t* n_dev = nullptr) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n_dev) n = *n_dev;
     if (k >= n) return;
     if (Q.shadow_occ[k] != 0) return;
     int path = Q.shadow_path[k];
@@ -437,6 +441,167 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
     return CAV_OK;
 }
 
+// ------------------------------------------------------------------ graph-replayed render
+// The path integrator with every queue size kept on the device: the traversal kernels read
+// their ray counts from the counters the previous kernel wrote, shading kernels run over the
+// chunk capacity and stop at the device count.  One chunk's whole chain (generate, max_depth
+// x (extend, shade, shadow, accumulate), film) is captured once as a CUDA graph and replayed
+// for every chunk; the chunk's sample range comes from a device table indexed by a device
+// counter that the graph's last node advances.  Bounces past the last live path launch
+// kernels that exit at once.
+namespace {
+__global__ void k_chunk_begin(const int64_t* table, const int32_t* idx, int64_t* fc, uint32_t* cnt, int nslots) {
+    const int i = *idx;
+    fc[0] = table[2 * i];
+    fc[1] = table[2 * i + 1];
+    for (int k = 0; k < nslots; ++k) cnt[k] = 0;
+    cnt[nslots] = (uint32_t)table[2 * i + 1];  // the extend queue size of bounce 0
+}
+
+__global__ void k_chunk_end(int32_t* idx, const uint32_t* cnt, int max_depth, unsigned long long* totals) {
+    *idx += 1;
+    unsigned long long closest = cnt[2 * max_depth], shadow = 0;
+    for (int d = 0; d < max_depth; ++d) {
+        if (d + 1 < max_depth) closest += cnt[2 * d];
+        shadow += cnt[2 * d + 1];
+    }
+    totals[0] += closest;
+    totals[1] += shadow;
+}
+
+}  // namespace
+
+cav_status render_path_graph(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
+                             cudaStream_t s) {
+    const cavpbrt::Scene& D = sc->desc;
+    int W, H;
+    film_size(sc, opts, W, H);
+    const int spp = opts && opts->spp > 0 ? opts->spp : D.spp;
+    const int max_depth = opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth;
+    const int64_t total = (int64_t)W * H * spp;
+    int64_t chunk = opts && opts->max_paths_in_flight > 0 ? opts->max_paths_in_flight : (int64_t)1 << 22;
+    chunk = std::min(chunk, total);
+    const int64_t nchunks = (total + chunk - 1) / chunk;
+    size_t need = 0;
+    {
+        auto acc = [&](size_t bytes) { need += bytes + 256; };
+        acc(8 * chunk); acc(8 * chunk); acc(12 * chunk); acc(12 * chunk); acc(4 * chunk); acc(chunk);
+        acc(4 * chunk); acc(32 * chunk); acc(4 * chunk); acc(32 * chunk);
+        acc(4 * chunk); acc(4 * chunk); acc(8 * chunk);
+        acc(32 * chunk); acc(4 * chunk); acc(8 * chunk); acc(4 * chunk); acc(12 * chunk); acc(chunk); acc(64);
+        acc(16 * nchunks); acc(16); acc(4); acc(4 * (2 * max_depth + 2)); acc(16);
+    }
+    void* base = nullptr;
+    CAV_CUDA(ctx, cudaMallocAsync(&base, need, s));
+    struct FreeAsync {
+        void* p;
+        cudaStream_t s;
+        ~FreeAsync() { cudaFreeAsync(p, s); }
+    } free_base{base, s};
+    unsigned char* p = (unsigned char*)base;
+    Paths P;
+    P.sample_index = carve<uint64_t>(p, chunk);
+    P.film_xy = carve<float2>(p, chunk);
+    P.result = carve<float>(p, 3 * chunk);
+    P.throughput = carve<float>(p, 3 * chunk);
+    P.mat_pdf = carve<float>(p, chunk);
+    P.delta = carve<uint8_t>(p, chunk);
+    Queues Q0;
+    Q0.active = carve<int32_t>(p, chunk);
+    Q0.rays = carve<cav_ray>(p, chunk);
+    Q0.next_active = carve<int32_t>(p, chunk);
+    Q0.next_rays = carve<cav_ray>(p, chunk);
+    Q0.hit_prim = carve<int32_t>(p, chunk);
+    Q0.hit_t = carve<float>(p, chunk);
+    Q0.hit_uv = carve<float>(p, 2 * chunk);
+    Q0.shadow_rays = carve<cav_ray>(p, chunk);
+    Q0.shadow_limit = carve<float>(p, chunk);
+    Q0.shadow_excl = carve<int32_t>(p, 2 * chunk);
+    Q0.shadow_path = carve<int32_t>(p, chunk);
+    Q0.shadow_contrib = carve<float>(p, 3 * chunk);
+    Q0.shadow_occ = carve<uint8_t>(p, chunk);
+    Q0.counters = carve<uint32_t>(p, 16);
+    int64_t* d_table = carve<int64_t>(p, 2 * nchunks);
+    int64_t* d_fc = carve<int64_t>(p, 2);
+    int32_t* d_idx = carve<int32_t>(p, 1);
+    uint32_t* cnt = carve<uint32_t>(p, 2 * max_depth + 2);  // [2d] next rays, [2d+1] shadow rays, [2D] bounce-0 size
+    unsigned long long* totals = carve<unsigned long long>(p, 2);
+    std::vector<int64_t> table(2 * nchunks);
+    for (int64_t c = 0; c < nchunks; ++c) {
+        table[2 * c] = c * chunk;
+        table[2 * c + 1] = std::min(chunk, total - c * chunk);
+    }
+    auto& log = sc->log;
+    log.reset();
+    log.start = log.next();
+    log.paths = total;
+    CAV_CUDA(ctx, cudaMemcpyAsync(d_table, table.data(), sizeof(int64_t) * 2 * nchunks, cudaMemcpyHostToDevice, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(d_idx, 0, 4, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(totals, 0, 16, s));
+    CAV_CUDA(ctx, cudaStreamSynchronize(s));  // the table copy reads pageable host memory
+    const DevScene S = dev_scene_of(sc);
+    const Camera cam = camera_of(sc, W, H);
+    const unsigned blocks = (unsigned)div_up(chunk, kThreads);
+    // capture and replay on the scene's own non-blocking stream (the legacy default stream
+    // cannot be captured), ordered after and before the caller's stream by events
+    const cudaStream_t caller = s;
+    if (!sc->graph_stream) CAV_CUDA(ctx, cudaStreamCreateWithFlags(&sc->graph_stream, cudaStreamNonBlocking));
+    s = sc->graph_stream;
+    {
+        cudaEvent_t fork = log.next();
+        CAV_CUDA(ctx, cudaEventRecord(fork, caller));
+        CAV_CUDA(ctx, cudaStreamWaitEvent(s, fork, 0));
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CAV_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cav_status st = CAV_OK;
+    {
+        k_chunk_begin<<<1, 1, 0, s>>>(d_table, d_idx, d_fc, cnt, 2 * max_depth);
+        k_generate<<<blocks, kThreads, 0, s>>>(cam, S.halton, spp, 0, 0, P, Q0, d_fc);
+        Queues Q = Q0;
+        int dim0 = 0;
+        for (int depth = 0; depth < max_depth && st == CAV_OK; ++depth) {
+            const uint32_t* n_dev = depth == 0 ? cnt + 2 * max_depth : cnt + 2 * (depth - 1);
+            Q.counters = cnt + 2 * depth;
+            st = trace_closest_dev(ctx, sc->bvh, Q.rays, n_dev, Q.hit_prim, Q.hit_t, Q.hit_uv, s, ctx->d_counters + 6);
+            if (st != CAV_OK) break;
+            k_shade<<<blocks, kThreads, 0, s>>>(S, depth, dim0, 0, P, Q, n_dev);
+            st = trace_any_dev(ctx, sc->bvh, Q.shadow_rays, Q.shadow_limit, Q.shadow_excl, cnt + 2 * depth + 1,
+                               Q.shadow_occ, s, ctx->d_counters + 7);
+            if (st != CAV_OK) break;
+            k_add_direct<<<blocks, kThreads, 0, s>>>(0, P, Q, cnt + 2 * depth + 1);
+            std::swap(Q.active, Q.next_active);
+            std::swap(Q.rays, Q.next_rays);
+            dim0 += 8 + 2 + (depth > 3 ? 1 : 0);
+        }
+        k_film<<<blocks, kThreads, 0, s>>>(0, P, W, H, D.filter_xwidth, D.filter_ywidth, d_sum, d_wsum, d_fc);
+        k_chunk_end<<<1, 1, 0, s>>>(d_idx, cnt, max_depth, totals);
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (st != CAV_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    CAV_CUDA(ctx, ce);
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CAV_CUDA(ctx, ce);
+    CAV_CUDA(ctx, cudaEventRecord(log.start, s));
+    for (int64_t c = 0; c < nchunks; ++c) {
+        ce = cudaGraphLaunch(exec, s);
+        if (ce != cudaSuccess) break;
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(sc->log_totals_host(), totals, 16, cudaMemcpyDeviceToHost, s);
+    cudaGraphExecDestroy(exec);  // released once the launches complete
+    CAV_CUDA(ctx, ce);
+    log.end = log.next();
+    CAV_CUDA(ctx, cudaEventRecord(log.end, s));
+    CAV_CUDA(ctx, cudaStreamWaitEvent(caller, log.end, 0));  // join: the film is ready on the caller's stream
+    log.graph = true;
+    return CAV_OK;
+}
+
 // ------------------------------------------------------------------ resumable render job
 // The path integrator as a state machine advanced one bounce at a time by the serving loop
 // (serve.cu), whose traversal launches merge the wavefronts of every live job.  Per chunk
@@ -663,7 +828,12 @@ cav_status cav_scene_free(cav_scene* sc) {
     cudaFree(sc->d_primes);
     cudaFree(sc->d_perm_start);
     cudaFree(sc->d_perms);
+    if (sc->graph_stream) {
+        cudaStreamSynchronize(sc->graph_stream);
+        cudaStreamDestroy(sc->graph_stream);
+    }
     for (cudaEvent_t e : sc->log.pool) cudaEventDestroy(e);
+    if (sc->log.totals_h) cudaFreeHost(sc->log.totals_h);
     delete sc;
     return CAV_OK;
 }
@@ -700,6 +870,7 @@ cav_status cav_render(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, 
     if (opts && opts->integrator < 0) integrator = 0;
     if (integrator == 1) return cav::render_rlpath(ctx, sc, opts, film_sum, film_weight, s);
     if (integrator != 0) return cav::set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "unknown integrator");
+    if (opts && (opts->flags & CAV_RENDER_GRAPH)) return cav::render_path_graph(ctx, sc, opts, film_sum, film_weight, s);
     return cav::render_path(ctx, sc, opts, film_sum, film_weight, s);
 }
 
@@ -713,6 +884,10 @@ cav_status cav_render_stats(const cav_scene* sc, cav_render_stats_t* out) {
     out->bounces = L.bounces;
     if (!L.start || !L.end) return CAV_OK;
     if (cudaEventSynchronize(L.end) != cudaSuccess) return CAV_ERR_CUDA;
+    if (L.graph && L.totals_h) {
+        out->closest_rays = (int64_t)L.totals_h[0];
+        out->shadow_rays = (int64_t)L.totals_h[1];
+    }
     auto sum = [](const std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v) {
         double t = 0;
         for (const auto& p : v) {
@@ -738,7 +913,7 @@ cav_status cav_render_capture_rays(cav_ctx* ctx, cav_scene* sc, const cav_render
     const int64_t pixels = (int64_t)W * H;
     float* film = nullptr;
     CAV_CUDA(ctx, cudaMalloc(&film, sizeof(float) * 4 * pixels));
-    cav_render_opts o = opts ? *opts : cav_render_opts{0, 0, 0, 0, 0, 0};
+    cav_render_opts o = opts ? *opts : cav_render_opts{0, 0, 0, 0, 0, 0, 0};
     // one chunk is enough: the capture is taken from the first chunk
     const int spp = o.spp > 0 ? o.spp : sc->desc.spp;
     const int64_t total = pixels * spp;

@@ -421,8 +421,14 @@ __device__ inline f3 apply_pt(const float* m, f3 v) {
 }
 
 // genCameraSampleSPPs (Core/Sampler.cu:29-51) + genInitialRays (PathTracingIntegrator.cu:252-266)
-__global__ void k_generate(Camera cam, Halton H, int spp, int64_t first, int64_t count, Paths P, Queues Q) {
+// dev_fc (or null): {first, count} read from device memory, for graph-replayed chunks
+__global__ void k_generate(Camera cam, Halton H, int spp, int64_t first, int64_t count, Paths P, Queues Q,
+                           const int64_t* dev_fc = nullptr) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (dev_fc) {
+        first = dev_fc[0];
+        count = dev_fc[1];
+    }
     if (i >= count) return;
     int64_t s = first + i;  // global sample number, pixel-major
     int64_t pixel = s / spp;
@@ -457,8 +463,10 @@ __device__ inline uint32_t warp_append(uint32_t* counter, bool pred) {
 
 // addSamplesToFilm + Film::addSample (Core/Film.h:26-49) with the box filter of
 // Filters/BoxFilter.h ("triangle" maps to it, Filters/FilterObject.h:83-84).
-__global__ void k_film(int64_t n, Paths P, int width, int height, float xw, float yw, float* sum, float* wsum) {
+__global__ void k_film(int64_t n, Paths P, int width, int height, float xw, float yw, float* sum, float* wsum,
+                       const int64_t* dev_fc = nullptr) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (dev_fc) n = dev_fc[1];
     if (i >= n) return;
     f3 s = ld3(P.result + 3 * i);
     if (!finite3(s)) return;
@@ -507,6 +515,7 @@ struct cav_scene {
     uint16_t* d_perms = nullptr;
     cav_bvh* bvh = nullptr;
     int bvh_rounds = 0;
+    cudaStream_t graph_stream = nullptr;  // private stream for graph capture and replay
     // per-stage timing of the last render: event pairs on the render stream
     struct Log {
         std::vector<cudaEvent_t> pool;
@@ -515,6 +524,8 @@ struct cav_scene {
         cudaEvent_t start = nullptr, end = nullptr;
         int64_t paths = 0, closest_rays = 0, shadow_rays = 0;
         int bounces = 0;
+        bool graph = false;                      // the last render was graph-replayed
+        unsigned long long* totals_h = nullptr;  // pinned: its closest / shadow ray totals
         cudaEvent_t next() {
             if (used == pool.size()) {
                 cudaEvent_t e;
@@ -525,6 +536,7 @@ struct cav_scene {
         }
         void reset() {
             used = 0;
+            graph = false;
             closest.clear();
             shade.clear();
             any.clear();
@@ -532,6 +544,10 @@ struct cav_scene {
             bounces = 0;
         }
     } log;
+    unsigned long long* log_totals_host() {
+        if (!log.totals_h) cudaMallocHost(&log.totals_h, 16);
+        return log.totals_h;
+    }
 };
 
 

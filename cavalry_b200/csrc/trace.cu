@@ -25,6 +25,9 @@ namespace {
 // 128 entries cover the deepest trees the treelet rounds produce on degenerate input, and
 // the push is checked (the ray is flagged instead of writing past the end).
 constexpr int kStack = 128;
+// The short stack is used only for trees whose depth is known to fit: a traversal holds at
+// most one deferred sibling per level, so depth + 1 entries always suffice.
+constexpr int kShortStack = 64;
 constexpr uint32_t kMaxSteps = 1u << 22;  // node+triangle visits per ray before the ray is flagged
 constexpr int kDefaultRefill = 4;         // idle lanes that trigger a warp's next claim
 constexpr unsigned kFull = 0xffffffffu;
@@ -147,7 +150,7 @@ __device__ inline int find_seg(const int64_t* sbeg, int nseg, int64_t g) {
     return lo;
 }
 
-template <bool kCullPop, bool kStats, bool kSeg>
+template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack>
 __global__ void k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
                           unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
     __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
@@ -155,6 +158,7 @@ __global__ void k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int n
         for (int i = threadIdx.x; i < nseg; i += blockDim.x) sbeg[i] = segs[i].begin;
         __syncthreads();
     }
+    if (!kSeg && one.n_dev) n = *one.n_dev;
     const TNode* __restrict__ nodes = one.nodes;
     const TriRec* __restrict__ tris = one.tris;
     float rb0 = 0.f, rb1 = 0.f, rb2 = 0.f, rb3 = 0.f, rb4 = 0.f, rb5 = 0.f;
@@ -162,8 +166,8 @@ __global__ void k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int n
         rb0 = one.root_box[0]; rb1 = one.root_box[1]; rb2 = one.root_box[2];
         rb3 = one.root_box[3]; rb4 = one.root_box[4]; rb5 = one.root_box[5];
     }
-    int32_t stack[kStack];
-    float sdist[kCullPop ? kStack : 1];
+    int32_t stack[kStackN];
+    float sdist[kCullPop ? kStackN : 1];
     TraceStats st;
     bool more = true;
     int64_t ray = -1;  // index within the lane's segment
@@ -226,7 +230,7 @@ __global__ void k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int n
             bool okl = ml >= 0 && ml < best && !(ml > tmax);
             bool okr = mr >= 0 && mr < best && !(mr > tmax);
             if (okl && okr) {
-                if (top + 1 >= kStack) {
+                if (top + 1 >= kStackN) {
                     steps = kMaxSteps;  // overflow: finish below with the flag
                 } else if (ml > mr) {  // the reference pushes the farther child, pops the nearer
                     stack[++top] = dd.x;
@@ -285,7 +289,7 @@ __global__ void k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int n
     flush_stats<kStats>(st, stats);
 }
 
-template <bool kCullPop, bool kStats, bool kSeg>
+template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack>
 __global__ void k_any(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
                       unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
     __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
@@ -293,9 +297,10 @@ __global__ void k_any(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg,
         for (int i = threadIdx.x; i < nseg; i += blockDim.x) sbeg[i] = segs[i].begin;
         __syncthreads();
     }
+    if (!kSeg && one.n_dev) n = *one.n_dev;
     const TNode* __restrict__ nodes = one.nodes;
     const TriRec* __restrict__ tris = one.tris;
-    int32_t stack[kStack];
+    int32_t stack[kStackN];
     TraceStats st;
     bool more = true;
     int64_t ray = -1;
@@ -362,7 +367,7 @@ __global__ void k_any(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg,
                 okr = okr && mr < lim;
             }
             if (okl && okr) {
-                if (top + 1 >= kStack) {
+                if (top + 1 >= kStackN) {
                     result = 2;
                 } else if (ml > mr) {
                     stack[++top] = dd.x;
@@ -415,6 +420,10 @@ int grid_for(cav_ctx* ctx, K kernel, int block) {
     return ctx->num_sms * per_sm;
 }
 
+bool use_short_stack(const cav_ctx* ctx, const cav_bvh* bvh) {
+    return ctx->trace_stack == kShortStack && bvh->depth >= 0 && bvh->depth + 1 < kShortStack;
+}
+
 TraceSeg seg_of(const cav_bvh* bvh) {
     TraceSeg g{};
     g.nodes = bvh->tnodes;
@@ -425,11 +434,15 @@ TraceSeg seg_of(const cav_bvh* bvh) {
 
 template <bool kStats, bool kSeg>
 cav_status launch_closest(cav_ctx* ctx, const TraceSeg& one, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags,
-                          cudaStream_t s, unsigned long long* counter, unsigned long long* stats) {
+                          cudaStream_t s, unsigned long long* counter, unsigned long long* stats, bool short_stack = false) {
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
     const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
-    if (flags & CAV_TRACE_CULL_ON_POP) {
+    if (!kStats && !kSeg && short_stack && !(flags & CAV_TRACE_CULL_ON_POP)) {
+        int grid = grid_for(ctx, k_closest<false, false, false, kShortStack>, block);
+        k_closest<false, false, false, kShortStack><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch,
+                                                                          ctx->d_error + 2, stats);
+    } else if (flags & CAV_TRACE_CULL_ON_POP) {
         int grid = grid_for(ctx, k_closest<true, kStats, kSeg>, block);
         k_closest<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 2,
                                                              stats);
@@ -444,11 +457,15 @@ cav_status launch_closest(cav_ctx* ctx, const TraceSeg& one, const TraceSeg* seg
 
 template <bool kStats, bool kSeg>
 cav_status launch_any(cav_ctx* ctx, const TraceSeg& one, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags,
-                      cudaStream_t s, unsigned long long* counter, unsigned long long* stats) {
+                      cudaStream_t s, unsigned long long* counter, unsigned long long* stats, bool short_stack = false) {
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
     const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
-    if (flags & CAV_TRACE_CULL_ON_POP) {
+    if (!kStats && !kSeg && short_stack && !(flags & CAV_TRACE_CULL_ON_POP)) {
+        int grid = grid_for(ctx, k_any<false, false, false, kShortStack>, block);
+        k_any<false, false, false, kShortStack><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch,
+                                                                      ctx->d_error + 3, stats);
+    } else if (flags & CAV_TRACE_CULL_ON_POP) {
         int grid = grid_for(ctx, k_any<true, kStats, kSeg>, block);
         k_any<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 3, stats);
     } else {
@@ -471,7 +488,7 @@ cav_status trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, 
     one.prim = prim;
     one.t = t;
     one.uv = uv;
-    return launch_closest<false, false>(ctx, one, nullptr, 0, n, flags, s, counter, nullptr);
+    return launch_closest<false, false>(ctx, one, nullptr, 0, n, flags, s, counter, nullptr, use_short_stack(ctx, bvh));
 }
 
 cav_status trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit, const int32_t* excl,
@@ -485,7 +502,7 @@ cav_status trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, cons
     one.limit = limit;
     one.excl = excl;
     one.occ = occ;
-    return launch_any<false, false>(ctx, one, nullptr, 0, n, flags, s, counter, nullptr);
+    return launch_any<false, false>(ctx, one, nullptr, 0, n, flags, s, counter, nullptr, use_short_stack(ctx, bvh));
 }
 
 cav_status trace_stats(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
@@ -545,4 +562,103 @@ cav_status trace_any_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, int6
 
 int trace_max_segments() { return kMaxSeg; }
 
+cav_status trace_closest_dev(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const uint32_t* n_dev,
+                             int32_t* prim, float* t, float* uv, cudaStream_t s, unsigned long long* counter) {
+    TraceSeg one = seg_of(bvh);
+    one.rays = rays;
+    one.prim = prim;
+    one.t = t;
+    one.uv = uv;
+    one.n_dev = n_dev;
+    return launch_closest<false, false>(ctx, one, nullptr, 0, INT64_MAX, CAV_TRACE_EXACT, s, counter, nullptr,
+                                        use_short_stack(ctx, bvh));
+}
+
+cav_status trace_any_dev(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,
+                         const int32_t* excl, const uint32_t* n_dev, uint8_t* occ, cudaStream_t s,
+                         unsigned long long* counter) {
+    TraceSeg one = seg_of(bvh);
+    one.rays = rays;
+    one.limit = limit;
+    one.excl = excl;
+    one.occ = occ;
+    one.n_dev = n_dev;
+    return launch_any<false, false>(ctx, one, nullptr, 0, INT64_MAX, CAV_TRACE_EXACT, s, counter, nullptr,
+                                    use_short_stack(ctx, bvh));
+}
+
 }  // namespace cav
+
+// ================================================================ launch-shape autotuner
+// Times the traversal of a ray sample over candidate launch shapes and installs the
+// fastest in the context: threads per block, queue chunk (idle lanes before a warp claims
+// new rays), and the traversal stack size (the short stack only when the tree's measured
+// depth guarantees it cannot overflow).  Blocks per SM stay at the occupancy maximum:
+// the kernels are persistent, so fewer resident blocks only idles SMs.
+extern "C" cav_status cav_trace_autotune(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
+                                         const float* limit, const int32_t* excl, void* stream,
+                                         cav_trace_config_t* best_out) {
+    using namespace cav;
+    if (!ctx || !bvh || !rays || n <= 0) return CAV_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (bvh->depth < 0) {
+        int32_t d = 0;
+        cav_status st = cav_bvh_depth(ctx, bvh, stream, &d);
+        if (st != CAV_OK) return st;
+    }
+    void* out = nullptr;
+    CAV_CUDA(ctx, cudaMallocAsync(&out, (size_t)n * 16 + 256, s));
+    int32_t* prim = (int32_t*)out;
+    float* t = (float*)((char*)out + 4 * n);
+    float* uv = (float*)((char*)out + 8 * n);
+    uint8_t* occ = (uint8_t*)out;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int saved[4] = {ctx->trace_block, ctx->trace_blocks_per_sm, ctx->trace_batch, ctx->trace_stack};
+    cav_trace_config_t best{0, 0, 0, 0, 1e30f};
+    const int blocks[] = {64, 128, 256};
+    const int batches[] = {1, 2, 4, 8, 16, 32};
+    const int stacks[] = {kStack, kShortStack};
+    cav_status st = CAV_OK;
+    for (int stk : stacks) {
+        if (stk == kShortStack && !(bvh->depth + 1 < kShortStack)) continue;
+        for (int blk : blocks)
+            for (int bat : batches) {
+                ctx->trace_block = blk;
+                ctx->trace_blocks_per_sm = 0;
+                ctx->trace_batch = bat;
+                ctx->trace_stack = stk;
+                float ms_best = 1e30f;
+                for (int rep = 0; rep < 3 && st == CAV_OK; ++rep) {  // first repetition warms up
+                    cudaEventRecord(a, s);
+                    st = any_hit ? trace_any(ctx, bvh, rays, limit, excl, n, occ, CAV_TRACE_EXACT, s, ctx->d_counters + 5)
+                                 : trace_closest(ctx, bvh, rays, n, prim, t, uv, CAV_TRACE_EXACT, s, ctx->d_counters + 5);
+                    cudaEventRecord(b, s);
+                    cudaEventSynchronize(b);
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, a, b);
+                    if (rep > 0) ms_best = std::min(ms_best, ms);
+                }
+                if (st != CAV_OK) break;
+                if (ms_best < best.ms) best = cav_trace_config_t{blk, 0, bat, stk, ms_best};
+            }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFreeAsync(out, s);
+    if (st != CAV_OK || best.block_threads == 0) {
+        ctx->trace_block = saved[0];
+        ctx->trace_blocks_per_sm = saved[1];
+        ctx->trace_batch = saved[2];
+        ctx->trace_stack = saved[3];
+        return st != CAV_OK ? st : set_error(ctx, CAV_ERR_CUDA, "cav_trace_autotune: no candidate ran");
+    }
+    ctx->trace_block = best.block_threads;
+    ctx->trace_blocks_per_sm = 0;
+    ctx->trace_batch = best.batch;
+    ctx->trace_stack = best.stack;
+    if (best_out) *best_out = best;
+    return CAV_OK;
+}

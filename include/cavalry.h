@@ -207,7 +207,11 @@ typedef struct cav_render_opts {
     int integrator;              /* 0: the scene's Integrator ("path" or "rlpath"); -1: path; 1: rlpath */
     int64_t max_paths_in_flight; /* <= 0: 4M; samples are rendered in chunks of this many paths */
     int width, height;           /* <= 0: the scene's Film resolution (the camera keeps its fov) */
+    int flags;                   /* CAV_RENDER_GRAPH: capture one chunk's bounce chain as a CUDA graph and
+                                    replay it per chunk, with queue sizes kept on the device (no host round
+                                    trip per bounce; path integrator; per-stage times not recorded) */
 } cav_render_opts;
+enum { CAV_RENDER_GRAPH = 1 };
 
 /* Host-only .pbrt parse (no GPU): scene counts and the camera-to-world matrix (16 floats,
  * column-major; may be NULL).  On a parse error returns CAV_ERR_INVALID_ARGUMENT and copies the
@@ -298,6 +302,18 @@ cav_status cav_server_poll(cav_server* server, int64_t job_id, cav_job_status* s
 /* Waits for a job (timeout_s < 0: forever); returns the job's status or CAV_ERR_TIMEOUT. */
 cav_status cav_server_wait(cav_server* server, int64_t job_id, double timeout_s, cav_job_status* status);
 cav_status cav_server_stats(cav_server* server, cav_server_stats_t* out);
+
+/* Launch-shape autotuner: times the closest-hit (any_hit = 0) or any-hit traversal of a
+ * DEVICE ray sample over candidate shapes (64/128/256 threads per block; queue chunk 1-32;
+ * a 64-entry traversal stack when the tree's depth allows it, else 128) and installs the
+ * fastest in ctx for later single-tree traversals (merged launches always use the full
+ * stack).  ms is the best launch time of the chosen shape on the sample. */
+typedef struct cav_trace_config_t {
+    int block_threads, blocks_per_sm, batch, stack;
+    float ms;
+} cav_trace_config_t;
+cav_status cav_trace_autotune(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
+                              const float* limit, const int32_t* excl, void* stream, cav_trace_config_t* best);
 
 /* Device-side event timing of the last build's stages (ms): leaf boxes + Morton,
  * sort, radix tree, refit, treelet rounds, layout.  Valid after the stream is synced. */

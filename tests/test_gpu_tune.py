@@ -1,0 +1,34 @@
+"""GPU tests of the launch-shape autotuner: the installed shape changes speed, never hits."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_autotune_keeps_results_and_picks_a_candidate():
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    ctx = cav.Context(0)
+    pos, idx = scenes.soup(200_000, seed=12)
+    bvh = ctx.build(torch.from_numpy(pos).cuda(), torch.from_numpy(idx).cuda(), rounds=2)
+    rays = torch.from_numpy(scenes.closest_rays(300_000, seed=13)).cuda()
+    srays, lim = scenes.shadow_rays(300_000, seed=14)
+    srays, lim = torch.from_numpy(srays).cuda(), torch.from_numpy(lim).cuda()
+    p0, t0, _ = bvh.trace_closest(rays)
+    o0 = bvh.trace_any(srays, lim)
+    best = bvh.autotune(rays)
+    assert best["block_threads"] in (64, 128, 256) and best["batch"] in (1, 2, 4, 8, 16, 32)
+    assert best["stack"] in (64, 128) and best["ms"] > 0
+    if best["stack"] == 64:
+        assert bvh.depth() + 1 < 64
+    p1, t1, _ = bvh.trace_closest(rays)
+    best_any = bvh.autotune(srays, any_hit=True, limit=lim)
+    o1 = bvh.trace_any(srays, lim)
+    assert best_any["ms"] > 0
+    assert np.array_equal(p0.cpu().numpy(), p1.cpu().numpy())
+    assert np.array_equal(t0.cpu().numpy().view(np.uint32), t1.cpu().numpy().view(np.uint32))
+    assert np.array_equal(o0.cpu().numpy(), o1.cpu().numpy())
+    ctx.sync_check()
