@@ -94,6 +94,16 @@ def lib() -> ctypes.CDLL:
         "cav_render_to_host": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render_stats": ([P, P], ctypes.c_int),
+        "cav_mlp_num_params": ([], ctypes.c_int),
+        "cav_mlp_create": ([P, ctypes.c_uint64, ctypes.POINTER(P)], ctypes.c_int),
+        "cav_mlp_free": ([P], ctypes.c_int),
+        "cav_mlp_get_params": ([P, P], ctypes.c_int),
+        "cav_mlp_set_params": ([P, P], ctypes.c_int),
+        "cav_mlp_forward": ([P, P, ctypes.c_int64, P, P], ctypes.c_int),
+        "cav_mlp_gradients": ([P, P, P, P, ctypes.c_int64, P, P], ctypes.c_int),
+        "cav_mlp_train_step": ([P, P, P, P, ctypes.c_int64, ctypes.c_float, P], ctypes.c_int),
+        "cav_mlp_last_loss": ([P, P], ctypes.c_int),
+        "cav_mlp_mixture": ([P, P, ctypes.c_int64, P, P, P, P, P], ctypes.c_int),
         "cav_trace_autotune": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, P, P], ctypes.c_int),
         "cav_server_create": ([P, P, ctypes.POINTER(P)], ctypes.c_int),
         "cav_server_destroy": ([P], ctypes.c_int),
@@ -417,6 +427,77 @@ class Server:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+class Mlp:
+    """The learned directional proposal (cav_mlp): 5 inputs in [0, 1] -> 8-lobe vMF mixture."""
+
+    def __init__(self, ctx: "Context", seed: int = 1):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        ctx._check(lib().cav_mlp_create(ctx.handle, seed, ctypes.byref(h)), "cav_mlp_create")
+        self.handle = h
+        self.n_params = lib().cav_mlp_num_params()
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, np.float32)
+        self.ctx._check(lib().cav_mlp_get_params(self.handle, p.ctypes.data), "cav_mlp_get_params")
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        self.ctx._check(lib().cav_mlp_set_params(self.handle, p.ctypes.data), "cav_mlp_set_params")
+
+    def forward(self, x):
+        import torch
+
+        out = torch.empty((x.shape[0], 32), dtype=torch.float32, device=x.device)
+        self.ctx._check(lib().cav_mlp_forward(self.handle, _ptr(x), x.shape[0], _ptr(out), None), "cav_mlp_forward")
+        return out
+
+    def gradients(self, x, dirs, w):
+        g = np.zeros(self.n_params, np.float32)
+        loss = np.zeros(1, np.float32)
+        st = lib().cav_mlp_gradients(self.handle, _ptr(x), _ptr(dirs), _ptr(w), x.shape[0], g.ctypes.data,
+                                     loss.ctypes.data)
+        self.ctx._check(st, "cav_mlp_gradients")
+        return g, float(loss[0])
+
+    def train_step(self, x, dirs, w, lr: float = 1e-3, stream=None):
+        st = lib().cav_mlp_train_step(self.handle, _ptr(x), _ptr(dirs), _ptr(w), x.shape[0], lr, _stream_ptr(stream))
+        self.ctx._check(st, "cav_mlp_train_step")
+
+    def last_loss(self) -> float:
+        v = np.zeros(1, np.float32)
+        self.ctx._check(lib().cav_mlp_last_loss(self.handle, v.ctypes.data), "cav_mlp_last_loss")
+        return float(v[0])
+
+    def pdf(self, out, dirs):
+        import torch
+
+        p = torch.empty(out.shape[0], dtype=torch.float32, device=out.device)
+        st = lib().cav_mlp_mixture(self.ctx.handle, _ptr(out), out.shape[0], _ptr(dirs), _ptr(p), None, None, None)
+        self.ctx._check(st, "cav_mlp_mixture")
+        return p
+
+    def sample(self, out, u):
+        import torch
+
+        d = torch.empty((out.shape[0], 3), dtype=torch.float32, device=out.device)
+        st = lib().cav_mlp_mixture(self.ctx.handle, _ptr(out), out.shape[0], None, None, _ptr(u), _ptr(d), None)
+        self.ctx._check(st, "cav_mlp_mixture")
+        return d
+
+    def free(self):
+        if self.handle:
+            lib().cav_mlp_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
         except Exception:
             pass
 

@@ -163,6 +163,9 @@ cav_status trace_any_dev(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, 
                          const int32_t* excl, const uint32_t* n_dev, uint8_t* occ, cudaStream_t s,
                          unsigned long long* counter);
 
+// MLP forward pass for the guided integrator (mlp.cu): in n x 5 -> out n x 32
+cav_status mlp_forward(cav_mlp* m, const float* in, int64_t n, float* out, cudaStream_t s);
+
 // Resumable path-integrator render (render.cu), advanced bounce by bounce by the server.
 struct PathJob;
 size_t path_job_bytes(const cav_scene* sc, const cav_render_opts* opts);

@@ -1,0 +1,755 @@
+// Learned directional proposal: a small MLP that maps a surface point to a mixture of 8
+// von Mises-Fisher lobes over the sphere of incident directions, trained online on the
+// radiance the path tracer itself measures (the learned counterpart of rlpath's Q-table,
+// Integrators/ReinforcementLearningPathTracing.cu:10-148).
+//
+// Network: 5 inputs (position in the scene box, 3; surface normal as two angles scaled to
+// [0, 1], 2), each one-blob encoded into 32 Gaussian bins (160 features) -> 64 ReLU -> 64
+// ReLU -> 64 ReLU -> 32 outputs = 8 lobes x (weight logit, theta, phi, kappa).
+// Forward and backward are fused per warp: a warp owns 16 samples, their activations stay
+// in registers as BF16 mma fragments (the m16n8k16 accumulator layout of two adjacent
+// 8-column tiles is exactly the A-operand layout of the next layer's 16-column k-tile), and
+// the weights of every layer sit in shared memory (rows padded by 8 elements against bank
+// conflicts).  Weight gradients are a separate reduction over samples with the same mma
+// instruction.  FP32 accumulation throughout; FP32 master weights and Adam moments.
+//
+// The tensor-core instruction here is the warp-level mma.sync (BF16 in, FP32 accumulate).
+// A 64-wide network evaluated per ray vertex is bound by instruction latency and memory,
+// not by tensor throughput (4M samples x 41 kFLOP = 0.17 TFLOP per bounce).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "cav_internal.cuh"
+
+namespace cav {
+namespace mlp {
+
+constexpr int kIn = 5;
+constexpr int kBins = 32;
+constexpr int kF0 = kIn * kBins;  // 160 one-blob features
+constexpr int kH = 64;
+constexpr int kOut = 32;
+constexpr int kLobes = 8;
+constexpr int kPad = 8;  // bf16 elements of row padding in shared memory
+// layer shapes: {in, out}
+constexpr int kLayers = 4;
+__host__ __device__ constexpr int layer_in(int l) { return l == 0 ? kF0 : kH; }
+__host__ __device__ constexpr int layer_out(int l) { return l == 3 ? kOut : kH; }
+// fp32 parameter layout: for each layer W[out][in] then b[out]
+__host__ __device__ constexpr int w_off(int l) {
+    int o = 0;
+    for (int i = 0; i < l; ++i) o += layer_in(i) * layer_out(i) + layer_out(i);
+    return o;
+}
+__host__ __device__ constexpr int b_off(int l) { return w_off(l) + layer_in(l) * layer_out(l); }
+constexpr int kParams = w_off(kLayers);  // 20,704
+// bf16 weight image: for each layer W[out][in + pad] (forward) then WT[in][out + pad] (backward)
+__host__ __device__ constexpr int wf_off(int l) {
+    int o = 0;
+    for (int i = 0; i < l; ++i) o += layer_out(i) * (layer_in(i) + kPad) + layer_in(i) * (layer_out(i) + kPad);
+    return o;
+}
+__host__ __device__ constexpr int wt_off(int l) { return wf_off(l) + layer_out(l) * (layer_in(l) + kPad); }
+constexpr int kWImage = wf_off(kLayers);  // bf16 elements
+constexpr int kSmemBytes = kWImage * 2 + (kH * 3 + kOut) * 4;
+
+constexpr float kPi = 3.14159265358979323846f;
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ float2 unpack_bf16(uint32_t u) {
+    __nv_bfloat162 v = *reinterpret_cast<__nv_bfloat162*>(&u);
+    return __bfloat1622float2(v);
+}
+
+// D += A(16x16, row) * B(16x8, col): BF16 inputs, FP32 accumulate
+__device__ __forceinline__ void mma(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// One-blob encoding: bin b of input x has value exp(-0.5 ((x - (b + 0.5) / 32) * 32)^2).
+__device__ __forceinline__ float blob(float x, int b) {
+    float z = (x - ((float)b + 0.5f) * (1.f / kBins)) * (float)kBins;
+    return __expf(-0.5f * z * z);
+}
+
+// ---------------------------------------------------------------- mixture of vMF lobes
+struct Lobe {
+    float w;      // mixture weight (softmax)
+    float mx, my, mz;
+    float kappa;
+    float norm;   // kappa / (2 pi (1 - exp(-2 kappa)))
+};
+
+__device__ inline float sigmoidf_(float x) { return 1.f / (1.f + __expf(-x)); }
+__device__ inline float softplusf_(float x) { return x > 15.f ? x : log1pf(__expf(x)); }
+
+// Decodes the 32 outputs: logit, theta = pi sigmoid(a), phi = 2 pi sigmoid(b),
+// kappa = softplus(c) + 0.01 (capped at 500).
+__device__ inline void decode(const float* o, Lobe (&L)[kLobes]) {
+    float mx = -INFINITY;
+    for (int k = 0; k < kLobes; ++k) mx = fmaxf(mx, o[4 * k]);
+    float s = 0.f;
+    for (int k = 0; k < kLobes; ++k) {
+        L[k].w = __expf(o[4 * k] - mx);
+        s += L[k].w;
+    }
+    for (int k = 0; k < kLobes; ++k) {
+        L[k].w /= s;
+        float th = kPi * sigmoidf_(o[4 * k + 1]);
+        float ph = 2.f * kPi * sigmoidf_(o[4 * k + 2]);
+        float st, ct, sp, cp;
+        __sincosf(th, &st, &ct);
+        __sincosf(ph, &sp, &cp);
+        L[k].mx = st * cp;
+        L[k].my = st * sp;
+        L[k].mz = ct;
+        float kap = fminf(softplusf_(o[4 * k + 3]) + 0.01f, 500.f);
+        L[k].kappa = kap;
+        L[k].norm = kap / (2.f * kPi * (1.f - __expf(-2.f * kap)));
+    }
+}
+
+__device__ inline float mixture_pdf(const Lobe (&L)[kLobes], float wx, float wy, float wz) {
+    float p = 0.f;
+    for (int k = 0; k < kLobes; ++k) {
+        float c = L[k].mx * wx + L[k].my * wy + L[k].mz * wz;
+        p += L[k].w * L[k].norm * __expf(L[k].kappa * (c - 1.f));
+    }
+    return p;
+}
+
+// Picks a lobe with u0, then samples it (the standard vMF inversion for the cosine,
+// uniform azimuth) with u1, u2.
+__device__ inline void mixture_sample(const Lobe (&L)[kLobes], float u0, float u1, float u2, float& wx, float& wy,
+                                      float& wz) {
+    int k = 0;
+    float acc = L[0].w;
+    while (k < kLobes - 1 && u0 >= acc) acc += L[++k].w;
+    const float kap = L[k].kappa;
+    float c = 1.f + logf(u1 + (1.f - u1) * __expf(-2.f * kap)) / kap;
+    c = fminf(1.f, fmaxf(-1.f, c));
+    float s = sqrtf(fmaxf(0.f, 1.f - c * c));
+    float sp, cp;
+    __sincosf(2.f * kPi * u2, &sp, &cp);
+    // frame around the lobe axis
+    float nx = L[k].mx, ny = L[k].my, nz = L[k].mz;
+    float tx, ty, tz;
+    if (fabsf(nx) < 0.5f) {
+        tx = 0.f; ty = -nz; tz = ny;
+    } else {
+        tx = nz; ty = 0.f; tz = -nx;
+    }
+    float tl = rsqrtf(tx * tx + ty * ty + tz * tz);
+    tx *= tl; ty *= tl; tz *= tl;
+    float bx = ny * tz - nz * ty, by = nz * tx - nx * tz, bz = nx * ty - ny * tx;
+    wx = s * cp * tx + s * sp * bx + c * nx;
+    wy = s * cp * ty + s * sp * by + c * ny;
+    wz = s * cp * tz + s * sp * bz + c * nz;
+}
+
+// d(-w log q(omega)) / d outputs for one sample (FP32).
+__device__ inline float loss_grad(const float* o, float wx, float wy, float wz, float weight, float* g) {
+    Lobe L[kLobes];
+    decode(o, L);
+    float v[kLobes];
+    float q = 0.f;
+    for (int k = 0; k < kLobes; ++k) {
+        float c = L[k].mx * wx + L[k].my * wy + L[k].mz * wz;
+        v[k] = L[k].norm * __expf(L[k].kappa * (c - 1.f));
+        q += L[k].w * v[k];
+    }
+    q = fmaxf(q, 1e-20f);
+    for (int k = 0; k < kLobes; ++k) {
+        const float r = L[k].w * v[k] / q;  // d log q / d log v_k
+        // logits: d log q / d logit_j = pi_j (v_j / q - 1)
+        g[4 * k] = -weight * (r - L[k].w);
+        // direction: d log v / d mu = kappa omega
+        float a = o[4 * k + 1], b = o[4 * k + 2], c = o[4 * k + 3];
+        float sa = sigmoidf_(a), sb = sigmoidf_(b);
+        float th = kPi * sa, ph = 2.f * kPi * sb;
+        float st, ct, sp, cp;
+        __sincosf(th, &st, &ct);
+        __sincosf(ph, &sp, &cp);
+        float dmu_dth = ct * cp * wx + ct * sp * wy - st * wz;    // omega . d mu / d theta
+        float dmu_dph = -st * sp * wx + st * cp * wy;             // omega . d mu / d phi
+        float kap = L[k].kappa;
+        g[4 * k + 1] = -weight * r * kap * dmu_dth * kPi * sa * (1.f - sa);
+        g[4 * k + 2] = -weight * r * kap * dmu_dph * 2.f * kPi * sb * (1.f - sb);
+        // concentration: d log v / d kappa = 1/kappa - 2 e^{-2k} / (1 - e^{-2k}) + (mu.omega - 1)
+        float cdot = L[k].mx * wx + L[k].my * wy + L[k].mz * wz;
+        float e2 = __expf(-2.f * kap);
+        float dlv = 1.f / kap - 2.f * e2 / (1.f - e2) + (cdot - 1.f);
+        float dk = (softplusf_(c) + 0.01f < 500.f) ? sigmoidf_(c) : 0.f;
+        g[4 * k + 3] = -weight * r * dlv * dk;
+    }
+    return -weight * logf(q);
+}
+
+// ---------------------------------------------------------------- fused forward
+// Shared-memory image: per layer the forward weights W[out][in + pad] and the transposed
+// WT[in][out + pad] (bf16), then the biases (fp32).
+__device__ __forceinline__ void load_image(const __nv_bfloat16* img, const float* params, unsigned char* smem) {
+    const uint4* src = reinterpret_cast<const uint4*>(img);
+    uint4* dst = reinterpret_cast<uint4*>(smem);
+    for (int i = threadIdx.x; i < kWImage * 2 / 16; i += blockDim.x) dst[i] = src[i];
+    float* bs = reinterpret_cast<float*>(smem + kWImage * 2);
+    int o = 0;
+    for (int l = 0; l < kLayers; ++l) {
+        for (int i = threadIdx.x; i < layer_out(l); i += blockDim.x) bs[o + i] = params[b_off(l) + i];
+        o += layer_out(l);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ const float* bias_smem(const unsigned char* smem, int l) {
+    const float* bs = reinterpret_cast<const float*>(smem + kWImage * 2);
+    int o = 0;
+    for (int i = 0; i < l; ++i) o += layer_out(i);
+    return bs + o;
+}
+
+// D[NT] = A[KT] * W^T for one layer: W is [out][in + pad] in shared memory.
+template <int KT, int NT>
+__device__ __forceinline__ void layer_mma(const uint32_t (&A)[KT][4], const __nv_bfloat16* W, int ld, float (&D)[NT][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) D[nt][0] = D[nt][1] = D[nt][2] = D[nt][3] = 0.f;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+            const __nv_bfloat16* row = W + (nt * 8 + g) * ld + kt * 16 + 2 * q;
+            uint32_t b0 = *reinterpret_cast<const uint32_t*>(row);
+            uint32_t b1 = *reinterpret_cast<const uint32_t*>(row + 8);
+            mma(D[nt], A[kt], b0, b1);
+        }
+    }
+}
+
+// bias + ReLU, then the accumulators of tiles (2kt, 2kt+1) become k-tile kt of the next A
+template <int NT>
+__device__ __forceinline__ void relu_to_a(float (&D)[NT][4], const float* bias, uint32_t (&A)[NT / 2][4]) {
+    const int lane = threadIdx.x & 31, q = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+        const float b0 = bias[nt * 8 + 2 * q], b1 = bias[nt * 8 + 2 * q + 1];
+        D[nt][0] = fmaxf(D[nt][0] + b0, 0.f);
+        D[nt][1] = fmaxf(D[nt][1] + b1, 0.f);
+        D[nt][2] = fmaxf(D[nt][2] + b0, 0.f);
+        D[nt][3] = fmaxf(D[nt][3] + b1, 0.f);
+    }
+#pragma unroll
+    for (int kt = 0; kt < NT / 2; ++kt) {
+        A[kt][0] = pack_bf16(D[2 * kt][0], D[2 * kt][1]);
+        A[kt][1] = pack_bf16(D[2 * kt][2], D[2 * kt][3]);
+        A[kt][2] = pack_bf16(D[2 * kt + 1][0], D[2 * kt + 1][1]);
+        A[kt][3] = pack_bf16(D[2 * kt + 1][2], D[2 * kt + 1][3]);
+    }
+}
+
+// Stores an A fragment set (16 rows x 16*KT columns, bf16) to a row-major [n][ld] array.
+template <int KT>
+__device__ __forceinline__ void store_a(const uint32_t (&A)[KT][4], __nv_bfloat16* dst, int ld, int64_t r0, int64_t n) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int64_t ra = r0 + g, rb = r0 + g + 8;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+        if (ra < n) {
+            *reinterpret_cast<uint32_t*>(dst + ra * ld + kt * 16 + 2 * q) = A[kt][0];
+            *reinterpret_cast<uint32_t*>(dst + ra * ld + kt * 16 + 8 + 2 * q) = A[kt][2];
+        }
+        if (rb < n) {
+            *reinterpret_cast<uint32_t*>(dst + rb * ld + kt * 16 + 2 * q) = A[kt][1];
+            *reinterpret_cast<uint32_t*>(dst + rb * ld + kt * 16 + 8 + 2 * q) = A[kt][3];
+        }
+    }
+}
+
+struct Acts {  // training only: each layer's input (bf16), [n][width]
+    __nv_bfloat16* x0;  // 160
+    __nv_bfloat16* x1;  // 64
+    __nv_bfloat16* x2;
+    __nv_bfloat16* x3;
+};
+
+template <bool kStore>
+__global__ void __launch_bounds__(128) k_forward(const float* __restrict__ in, int64_t n, const __nv_bfloat16* img,
+                                                 const float* params, float* __restrict__ out, Acts acts) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    load_image(img, params, smem);
+    const __nv_bfloat16* W = reinterpret_cast<const __nv_bfloat16*>(smem);
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    for (int64_t r0 = ((int64_t)blockIdx.x * warps + warp) * 16; r0 < n; r0 += (int64_t)gridDim.x * warps * 16) {
+        const int64_t ra = r0 + g, rb = r0 + g + 8;
+        float xa[kIn], xb[kIn];
+#pragma unroll
+        for (int i = 0; i < kIn; ++i) {
+            xa[i] = ra < n ? in[ra * kIn + i] : 0.f;
+            xb[i] = rb < n ? in[rb * kIn + i] : 0.f;
+        }
+        // layer 0: one-blob features built straight into A fragments (a k-tile = 16 bins of one input)
+        uint32_t A0[kF0 / 16][4];
+#pragma unroll
+        for (int t = 0; t < kF0 / 16; ++t) {
+            const int dim = t >> 1, b = (t & 1) * 16 + 2 * q;
+            A0[t][0] = pack_bf16(blob(xa[dim], b), blob(xa[dim], b + 1));
+            A0[t][1] = pack_bf16(blob(xb[dim], b), blob(xb[dim], b + 1));
+            A0[t][2] = pack_bf16(blob(xa[dim], b + 8), blob(xa[dim], b + 9));
+            A0[t][3] = pack_bf16(blob(xb[dim], b + 8), blob(xb[dim], b + 9));
+        }
+        if (kStore) store_a(A0, acts.x0, kF0, r0, n);
+        float D[8][4];
+        uint32_t A[4][4];
+        layer_mma(A0, W + wf_off(0), kF0 + kPad, D);
+        relu_to_a(D, bias_smem(smem, 0), A);
+        if (kStore) store_a(A, acts.x1, kH, r0, n);
+        layer_mma(A, W + wf_off(1), kH + kPad, D);
+        relu_to_a(D, bias_smem(smem, 1), A);
+        if (kStore) store_a(A, acts.x2, kH, r0, n);
+        layer_mma(A, W + wf_off(2), kH + kPad, D);
+        relu_to_a(D, bias_smem(smem, 2), A);
+        if (kStore) store_a(A, acts.x3, kH, r0, n);
+        float O[4][4];
+        layer_mma(A, W + wf_off(3), kH + kPad, O);
+        const float* b3 = bias_smem(smem, 3);
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int c = nt * 8 + 2 * q;
+            if (ra < n) {
+                out[ra * kOut + c] = O[nt][0] + b3[c];
+                out[ra * kOut + c + 1] = O[nt][1] + b3[c + 1];
+            }
+            if (rb < n) {
+                out[rb * kOut + c] = O[nt][2] + b3[c];
+                out[rb * kOut + c + 1] = O[nt][3] + b3[c + 1];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- loss and backward
+struct Grads {  // training only: each layer's output gradient (bf16), [n][width]
+    __nv_bfloat16* d3;  // d loss / d outputs, 32
+    __nv_bfloat16* d2;  // d loss / d pre-activation of layer 2, 64
+    __nv_bfloat16* d1;
+    __nv_bfloat16* d0;
+};
+
+// -w log q(omega) per sample and its gradient w.r.t. the 32 outputs, scaled by 1/n (mean).
+__global__ void k_loss(const float* __restrict__ out, const float* __restrict__ dirs, const float* __restrict__ w,
+                       int64_t n, float* __restrict__ dout, float* loss_sum) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (i < n) {
+        float o[kOut], g[kOut];
+#pragma unroll
+        for (int k = 0; k < kOut; ++k) o[k] = out[i * kOut + k];
+        const float inv = 1.f / (float)n;
+        l = loss_grad(o, dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2], w[i] * inv, g);
+#pragma unroll
+        for (int k = 0; k < kOut; ++k) dout[i * kOut + k] = g[k];
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss_sum, l);
+}
+
+// gradient w.r.t. a layer's pre-activation: dX masked by its ReLU (the stored input of the
+// next layer is the activation, > 0 where the unit was active)
+template <int NT>
+__device__ __forceinline__ void relu_mask(float (&D)[NT][4], const __nv_bfloat16* x, int ld, int64_t r0, int64_t n,
+                                          uint32_t (&A)[NT / 2][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int64_t ra = r0 + g, rb = r0 + g + 8;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+        const int c = nt * 8 + 2 * q;
+        float2 va = ra < n ? unpack_bf16(*reinterpret_cast<const uint32_t*>(x + ra * ld + c)) : make_float2(0.f, 0.f);
+        float2 vb = rb < n ? unpack_bf16(*reinterpret_cast<const uint32_t*>(x + rb * ld + c)) : make_float2(0.f, 0.f);
+        D[nt][0] = va.x > 0.f ? D[nt][0] : 0.f;
+        D[nt][1] = va.y > 0.f ? D[nt][1] : 0.f;
+        D[nt][2] = vb.x > 0.f ? D[nt][2] : 0.f;
+        D[nt][3] = vb.y > 0.f ? D[nt][3] : 0.f;
+    }
+#pragma unroll
+    for (int kt = 0; kt < NT / 2; ++kt) {
+        A[kt][0] = pack_bf16(D[2 * kt][0], D[2 * kt][1]);
+        A[kt][1] = pack_bf16(D[2 * kt][2], D[2 * kt][3]);
+        A[kt][2] = pack_bf16(D[2 * kt + 1][0], D[2 * kt + 1][1]);
+        A[kt][3] = pack_bf16(D[2 * kt + 1][2], D[2 * kt + 1][3]);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_backward(const float* __restrict__ dout, int64_t n, const __nv_bfloat16* img,
+                                                  const float* params, Acts acts, Grads grads) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    load_image(img, params, smem);
+    const __nv_bfloat16* W = reinterpret_cast<const __nv_bfloat16*>(smem);
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    for (int64_t r0 = ((int64_t)blockIdx.x * warps + warp) * 16; r0 < n; r0 += (int64_t)gridDim.x * warps * 16) {
+        const int64_t ra = r0 + g, rb = r0 + g + 8;
+        uint32_t A3[2][4];
+#pragma unroll
+        for (int kt = 0; kt < 2; ++kt) {
+            const int c = kt * 16 + 2 * q;
+            auto ld = [&](int64_t r, int cc) { return r < n ? dout[r * kOut + cc] : 0.f; };
+            A3[kt][0] = pack_bf16(ld(ra, c), ld(ra, c + 1));
+            A3[kt][1] = pack_bf16(ld(rb, c), ld(rb, c + 1));
+            A3[kt][2] = pack_bf16(ld(ra, c + 8), ld(ra, c + 9));
+            A3[kt][3] = pack_bf16(ld(rb, c + 8), ld(rb, c + 9));
+        }
+        store_a(A3, grads.d3, kOut, r0, n);
+        float D[8][4];
+        uint32_t A[4][4];
+        // through layer 3 (32 x 64): dX3 = dOut W3, then layer 2's ReLU
+        layer_mma(A3, W + wt_off(3), kOut + kPad, D);
+        relu_mask(D, acts.x3, kH, r0, n, A);
+        store_a(A, grads.d2, kH, r0, n);
+        layer_mma(A, W + wt_off(2), kH + kPad, D);
+        relu_mask(D, acts.x2, kH, r0, n, A);
+        store_a(A, grads.d1, kH, r0, n);
+        layer_mma(A, W + wt_off(1), kH + kPad, D);
+        relu_mask(D, acts.x1, kH, r0, n, A);
+        store_a(A, grads.d0, kH, r0, n);
+    }
+}
+
+// dW[m][k] += sum over samples s of dY[s][m] * X[s][k] (and db[m] += sum dY[s][m]), with the
+// samples as the mma reduction dimension; tiles of 64 samples are staged in shared memory.
+template <int M, int N>
+__global__ void __launch_bounds__(128) k_weight_grad(const __nv_bfloat16* __restrict__ dY,
+                                                     const __nv_bfloat16* __restrict__ X, int64_t n, float* dW,
+                                                     float* db) {
+    constexpr int S = 64;
+    constexpr int MT = M / 16, NTT = N / 8, TILES = MT * NTT, PER = (TILES + 3) / 4;
+    __shared__ __align__(16) __nv_bfloat16 ys[S][M + kPad];
+    __shared__ __align__(16) __nv_bfloat16 xs[S][N + kPad];
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int warp = threadIdx.x >> 5;
+    float acc[PER][4];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+    float bsum = 0.f;
+    auto raw = [](const __nv_bfloat16& v) { return (uint32_t)(*reinterpret_cast<const unsigned short*>(&v)); };
+    for (int64_t s0 = (int64_t)blockIdx.x * S; s0 < n; s0 += (int64_t)gridDim.x * S) {
+        for (int i = threadIdx.x; i < S * M; i += blockDim.x) {
+            const int s = i / M, m = i % M;
+            ys[s][m] = s0 + s < n ? dY[(s0 + s) * M + m] : __float2bfloat16(0.f);
+        }
+        for (int i = threadIdx.x; i < S * N; i += blockDim.x) {
+            const int s = i / N, k = i % N;
+            xs[s][k] = s0 + s < n ? X[(s0 + s) * N + k] : __float2bfloat16(0.f);
+        }
+        __syncthreads();
+        if (threadIdx.x < M)
+            for (int s = 0; s < S; ++s) bsum += __bfloat162float(ys[s][threadIdx.x]);
+#pragma unroll
+        for (int ks = 0; ks < S / 16; ++ks) {
+            const int sb = ks * 16 + 2 * q;
+#pragma unroll
+            for (int i = 0; i < PER; ++i) {
+                const int t = warp + 4 * i;
+                if (t >= TILES) break;
+                const int m0 = (t / NTT) * 16, n0 = (t % NTT) * 8;
+                uint32_t a[4];
+                a[0] = raw(ys[sb][m0 + g]) | raw(ys[sb + 1][m0 + g]) << 16;
+                a[1] = raw(ys[sb][m0 + g + 8]) | raw(ys[sb + 1][m0 + g + 8]) << 16;
+                a[2] = raw(ys[sb + 8][m0 + g]) | raw(ys[sb + 9][m0 + g]) << 16;
+                a[3] = raw(ys[sb + 8][m0 + g + 8]) | raw(ys[sb + 9][m0 + g + 8]) << 16;
+                const uint32_t b0 = raw(xs[sb][n0 + g]) | raw(xs[sb + 1][n0 + g]) << 16;
+                const uint32_t b1 = raw(xs[sb + 8][n0 + g]) | raw(xs[sb + 9][n0 + g]) << 16;
+                mma(acc[i], a, b0, b1);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int t = warp + 4 * i;
+        if (t >= TILES) break;
+        const int m0 = (t / NTT) * 16, n0 = (t % NTT) * 8;
+        atomicAdd(dW + (m0 + g) * N + n0 + 2 * q, acc[i][0]);
+        atomicAdd(dW + (m0 + g) * N + n0 + 2 * q + 1, acc[i][1]);
+        atomicAdd(dW + (m0 + g + 8) * N + n0 + 2 * q, acc[i][2]);
+        atomicAdd(dW + (m0 + g + 8) * N + n0 + 2 * q + 1, acc[i][3]);
+    }
+    if (threadIdx.x < M) atomicAdd(db + threadIdx.x, bsum);
+}
+
+__global__ void k_adam(float* p, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    if (!isfinite(gi)) return;  // a non-finite sample gradient leaves the parameter alone
+    m[i] = b1 * m[i] + (1.f - b1) * gi;
+    v[i] = b2 * v[i] + (1.f - b2) * gi * gi;
+    p[i] -= lr * (m[i] / c1) / (sqrtf(v[i] / c2) + eps);
+}
+
+// fp32 master parameters -> the bf16 shared-memory image (forward W and transposed WT)
+__global__ void k_pack(const float* p, __nv_bfloat16* img) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kWImage) return;
+    float v = 0.f;
+    for (int l = 0; l < kLayers; ++l) {
+        const int in = layer_in(l), out = layer_out(l);
+        if (i >= wf_off(l) && i < wt_off(l)) {
+            const int r = (i - wf_off(l)) / (in + kPad), c = (i - wf_off(l)) % (in + kPad);
+            if (c < in) v = p[w_off(l) + r * in + c];
+        } else if (i >= wt_off(l) && i < wf_off(l + 1)) {
+            const int r = (i - wt_off(l)) / (out + kPad), c = (i - wt_off(l)) % (out + kPad);
+            if (c < out) v = p[w_off(l) + c * in + r];
+        }
+    }
+    img[i] = __float2bfloat16(v);
+}
+
+}  // namespace mlp
+}  // namespace cav
+
+// ================================================================================ host
+struct cav_mlp {
+    cav_ctx* ctx = nullptr;
+    float* d_params = nullptr;  // fp32 master
+    float* d_grads = nullptr;
+    float* d_m = nullptr;
+    float* d_v = nullptr;
+    __nv_bfloat16* d_img = nullptr;
+    float* d_loss = nullptr;
+    int64_t step = 0;
+    // training scratch, sized to the largest batch seen
+    int64_t cap = 0;
+    void* scratch = nullptr;
+    float* out = nullptr;
+    float* dout = nullptr;
+    cav::mlp::Acts acts{};
+    cav::mlp::Grads grads{};
+};
+
+namespace {
+
+using namespace cav::mlp;
+
+int fwd_grid(cav_ctx* ctx, int64_t n) {
+    int64_t want = (n + 63) / 64;  // 4 warps x 16 samples per block and pass
+    return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->num_sms * 2));
+}
+
+cav_status ensure_scratch(cav_mlp* m, int64_t n, cudaStream_t s) {
+    if (n <= m->cap) return CAV_OK;
+    if (m->scratch) cudaFreeAsync(m->scratch, s);
+    m->scratch = nullptr;
+    const size_t bytes = (size_t)n * (4 * kOut * 2 + 2 * (kF0 + 3 * kH) + 2 * (kOut + 3 * kH)) + 8 * 256;
+    CAV_CUDA(m->ctx, cudaMallocAsync(&m->scratch, bytes, s));
+    unsigned char* p = (unsigned char*)m->scratch;
+    auto carve = [&](size_t b) {
+        unsigned char* r = (unsigned char*)(((uintptr_t)p + 255) & ~(uintptr_t)255);
+        p = r + b;
+        return (void*)r;
+    };
+    m->out = (float*)carve(4ull * kOut * n);
+    m->dout = (float*)carve(4ull * kOut * n);
+    m->acts.x0 = (__nv_bfloat16*)carve(2ull * kF0 * n);
+    m->acts.x1 = (__nv_bfloat16*)carve(2ull * kH * n);
+    m->acts.x2 = (__nv_bfloat16*)carve(2ull * kH * n);
+    m->acts.x3 = (__nv_bfloat16*)carve(2ull * kH * n);
+    m->grads.d3 = (__nv_bfloat16*)carve(2ull * kOut * n);
+    m->grads.d2 = (__nv_bfloat16*)carve(2ull * kH * n);
+    m->grads.d1 = (__nv_bfloat16*)carve(2ull * kH * n);
+    m->grads.d0 = (__nv_bfloat16*)carve(2ull * kH * n);
+    m->cap = n;
+    return CAV_OK;
+}
+
+cav_status pack(cav_mlp* m, cudaStream_t s) {
+    k_pack<<<(kWImage + 255) / 256, 256, 0, s>>>(m->d_params, m->d_img);
+    CAV_CUDA(m->ctx, cudaGetLastError());
+    return CAV_OK;
+}
+
+// forward (storing activations) + loss + backward + weight gradients into d_grads
+cav_status compute_grads(cav_mlp* m, const float* in, const float* dirs, const float* w, int64_t n, cudaStream_t s) {
+    cav_status st = ensure_scratch(m, n, s);
+    if (st != CAV_OK) return st;
+    cav_ctx* ctx = m->ctx;
+    CAV_CUDA(ctx, cudaMemsetAsync(m->d_grads, 0, sizeof(float) * kParams, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(m->d_loss, 0, sizeof(float), s));
+    const int grid = fwd_grid(ctx, n);
+    k_forward<true><<<grid, 128, kSmemBytes, s>>>(in, n, m->d_img, m->d_params, m->out, m->acts);
+    k_loss<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m->out, dirs, w, n, m->dout, m->d_loss);
+    k_backward<<<grid, 128, kSmemBytes, s>>>(m->dout, n, m->d_img, m->d_params, m->acts, m->grads);
+    const int wg = (int)std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, (int64_t)ctx->num_sms * 4));
+    float* G = m->d_grads;
+    k_weight_grad<kOut, kH><<<wg, 128, 0, s>>>(m->grads.d3, m->acts.x3, n, G + w_off(3), G + b_off(3));
+    k_weight_grad<kH, kH><<<wg, 128, 0, s>>>(m->grads.d2, m->acts.x2, n, G + w_off(2), G + b_off(2));
+    k_weight_grad<kH, kH><<<wg, 128, 0, s>>>(m->grads.d1, m->acts.x1, n, G + w_off(1), G + b_off(1));
+    k_weight_grad<kH, kF0><<<wg, 128, 0, s>>>(m->grads.d0, m->acts.x0, n, G + w_off(0), G + b_off(0));
+    CAV_CUDA(ctx, cudaGetLastError());
+    return CAV_OK;
+}
+
+}  // namespace
+
+namespace cav {
+// Device entry for the guided integrator: forward pass over n inputs into out (n x 32).
+cav_status mlp_forward(cav_mlp* m, const float* in, int64_t n, float* out, cudaStream_t s) {
+    if (n <= 0) return CAV_OK;
+    k_forward<false><<<fwd_grid(m->ctx, n), 128, kSmemBytes, s>>>(in, n, m->d_img, m->d_params, out,
+                                                                  cav::mlp::Acts{});
+    CAV_CUDA(m->ctx, cudaGetLastError());
+    return CAV_OK;
+}
+}  // namespace cav
+
+extern "C" {
+
+int cav_mlp_num_params(void) { return kParams; }
+
+cav_status cav_mlp_create(cav_ctx* ctx, uint64_t seed, cav_mlp** out) {
+    if (!ctx || !out) return CAV_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return cav::cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        cudaFuncSetAttribute(k_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        attr = true;
+    }
+    auto* m = new cav_mlp();
+    m->ctx = ctx;
+    cudaError_t e = cudaMalloc(&m->d_params, sizeof(float) * kParams * 4 + 256);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_img, sizeof(__nv_bfloat16) * kWImage);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_loss, sizeof(float) * 4);
+    if (e != cudaSuccess) {
+        cav_mlp_free(m);
+        return cav::cuda_error(ctx, e, "cav_mlp_create");
+    }
+    m->d_grads = m->d_params + kParams;
+    m->d_m = m->d_grads + kParams;
+    m->d_v = m->d_m + kParams;
+    // Xavier-uniform weights from a seeded host generator, zero biases, zero moments
+    std::vector<float> p(kParams, 0.f);
+    std::mt19937_64 rng(seed);
+    for (int l = 0; l < kLayers; ++l) {
+        const float a = std::sqrt(6.f / (float)(layer_in(l) + layer_out(l)));
+        std::uniform_real_distribution<float> U(-a, a);
+        for (int i = 0; i < layer_in(l) * layer_out(l); ++i) p[w_off(l) + i] = U(rng);
+    }
+    cudaMemcpy(m->d_params, p.data(), sizeof(float) * kParams, cudaMemcpyHostToDevice);
+    cudaMemset(m->d_m, 0, sizeof(float) * kParams * 2);
+    cav_status st = pack(m, nullptr);
+    if (st == CAV_OK && cudaDeviceSynchronize() != cudaSuccess) st = cav::cuda_error(ctx, cudaGetLastError(), "mlp init");
+    if (st != CAV_OK) {
+        cav_mlp_free(m);
+        return st;
+    }
+    *out = m;
+    return CAV_OK;
+}
+
+cav_status cav_mlp_free(cav_mlp* m) {
+    if (!m) return CAV_OK;
+    cudaDeviceSynchronize();
+    cudaFree(m->d_params);
+    cudaFree(m->d_img);
+    cudaFree(m->d_loss);
+    if (m->scratch) cudaFree(m->scratch);
+    delete m;
+    return CAV_OK;
+}
+
+cav_status cav_mlp_get_params(cav_mlp* m, float* host) {
+    if (!m || !host) return CAV_ERR_INVALID_ARGUMENT;
+    CAV_CUDA(m->ctx, cudaMemcpy(host, m->d_params, sizeof(float) * kParams, cudaMemcpyDeviceToHost));
+    return CAV_OK;
+}
+
+cav_status cav_mlp_set_params(cav_mlp* m, const float* host) {
+    if (!m || !host) return CAV_ERR_INVALID_ARGUMENT;
+    CAV_CUDA(m->ctx, cudaMemcpy(m->d_params, host, sizeof(float) * kParams, cudaMemcpyHostToDevice));
+    cav_status st = pack(m, nullptr);
+    if (st != CAV_OK) return st;
+    CAV_CUDA(m->ctx, cudaDeviceSynchronize());
+    return CAV_OK;
+}
+
+cav_status cav_mlp_forward(cav_mlp* m, const float* in, int64_t n, float* out, void* stream) {
+    if (!m || !in || !out || n < 0) return CAV_ERR_INVALID_ARGUMENT;
+    return cav::mlp_forward(m, in, n, out, (cudaStream_t)stream);
+}
+
+cav_status cav_mlp_gradients(cav_mlp* m, const float* in, const float* dirs, const float* w, int64_t n,
+                             float* host_grads, float* host_loss) {
+    if (!m || !in || !dirs || !w || n <= 0 || !host_grads) return CAV_ERR_INVALID_ARGUMENT;
+    cav_status st = compute_grads(m, in, dirs, w, n, nullptr);
+    if (st != CAV_OK) return st;
+    CAV_CUDA(m->ctx, cudaMemcpy(host_grads, m->d_grads, sizeof(float) * kParams, cudaMemcpyDeviceToHost));
+    if (host_loss) CAV_CUDA(m->ctx, cudaMemcpy(host_loss, m->d_loss, sizeof(float), cudaMemcpyDeviceToHost));
+    return CAV_OK;
+}
+
+cav_status cav_mlp_train_step(cav_mlp* m, const float* in, const float* dirs, const float* w, int64_t n, float lr,
+                              void* stream) {
+    if (!m || !in || !dirs || !w || n <= 0 || !(lr > 0)) return CAV_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    cav_status st = compute_grads(m, in, dirs, w, n, s);
+    if (st != CAV_OK) return st;
+    m->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)m->step), c2 = 1.f - std::pow(b2, (float)m->step);
+    k_adam<<<(kParams + 255) / 256, 256, 0, s>>>(m->d_params, m->d_grads, m->d_m, m->d_v, kParams, lr, b1, b2, 1e-8f,
+                                                 c1, c2);
+    return pack(m, s);
+}
+
+cav_status cav_mlp_last_loss(cav_mlp* m, float* loss) {
+    if (!m || !loss) return CAV_ERR_INVALID_ARGUMENT;
+    CAV_CUDA(m->ctx, cudaMemcpy(loss, m->d_loss, sizeof(float), cudaMemcpyDeviceToHost));
+    return CAV_OK;
+}
+
+}  // extern "C"
+
+// mixture evaluation for tests: pdf of dirs under the decoded outputs; samples from them
+namespace {
+__global__ void k_mix_pdf(const float* out, const float* dirs, int64_t n, float* pdf) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    cav::mlp::Lobe L[cav::mlp::kLobes];
+    cav::mlp::decode(out + i * cav::mlp::kOut, L);
+    pdf[i] = cav::mlp::mixture_pdf(L, dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]);
+}
+__global__ void k_mix_sample(const float* out, const float* u, int64_t n, float* dirs) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    cav::mlp::Lobe L[cav::mlp::kLobes];
+    cav::mlp::decode(out + i * cav::mlp::kOut, L);
+    cav::mlp::mixture_sample(L, u[3 * i], u[3 * i + 1], u[3 * i + 2], dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]);
+}
+}  // namespace
+
+extern "C" cav_status cav_mlp_mixture(cav_ctx* ctx, const float* out, int64_t n, const float* dirs, float* pdf,
+                                      const float* u, float* samples, void* stream) {
+    if (!ctx || !out || n <= 0) return CAV_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned g = (unsigned)((n + 255) / 256);
+    if (dirs && pdf) k_mix_pdf<<<g, 256, 0, s>>>(out, dirs, n, pdf);
+    if (u && samples) k_mix_sample<<<g, 256, 0, s>>>(out, u, n, samples);
+    CAV_CUDA(ctx, cudaGetLastError());
+    return CAV_OK;
+}

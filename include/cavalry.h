@@ -315,6 +315,36 @@ typedef struct cav_trace_config_t {
 cav_status cav_trace_autotune(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
                               const float* limit, const int32_t* excl, void* stream, cav_trace_config_t* best);
 
+/*
+ * Learned directional proposal (mlp.cu): an MLP from a surface point (position in the scene
+ * box and normal angles, 5 floats in [0, 1]) to a mixture of 8 von Mises-Fisher lobes (32
+ * outputs: per lobe a weight logit, theta = pi sigmoid, phi = 2 pi sigmoid, kappa =
+ * softplus + 0.01), trained on weighted directions with the loss mean(-w log q(omega)).
+ * Parameters are FP32 (cav_mlp_num_params of them: per layer W[out][in] then b[out], for
+ * 160->64, 64->64, 64->64, 64->32 with one-blob inputs); the kernels use BF16 copies with
+ * FP32 accumulation.  Arrays are DEVICE unless named host_.
+ */
+typedef struct cav_mlp cav_mlp;
+int cav_mlp_num_params(void);
+cav_status cav_mlp_create(cav_ctx* ctx, uint64_t seed, cav_mlp** out);
+cav_status cav_mlp_free(cav_mlp* mlp);
+cav_status cav_mlp_get_params(cav_mlp* mlp, float* host_params);
+cav_status cav_mlp_set_params(cav_mlp* mlp, const float* host_params);
+/* in: n x 5, out: n x 32 */
+cav_status cav_mlp_forward(cav_mlp* mlp, const float* in, int64_t n, float* out, void* stream);
+/* Loss gradient w.r.t. every parameter for one batch (in n x 5, dirs n x 3 unit, w n),
+ * copied to host_grads (num_params floats) with the batch loss; no update.  Synchronous. */
+cav_status cav_mlp_gradients(cav_mlp* mlp, const float* in, const float* dirs, const float* w, int64_t n,
+                             float* host_grads, float* host_loss);
+/* One Adam step (beta 0.9 / 0.999) on one batch; stream-ordered. */
+cav_status cav_mlp_train_step(cav_mlp* mlp, const float* in, const float* dirs, const float* w, int64_t n, float lr,
+                              void* stream);
+cav_status cav_mlp_last_loss(cav_mlp* mlp, float* loss);
+/* Mixture density of dirs (n x 3) under decoded outputs (n x 32) into pdf, and/or samples
+ * (n x 3) drawn with u (n x 3 uniforms); either pair may be NULL. */
+cav_status cav_mlp_mixture(cav_ctx* ctx, const float* out, int64_t n, const float* dirs, float* pdf, const float* u,
+                           float* samples, void* stream);
+
 /* Device-side event timing of the last build's stages (ms): leaf boxes + Morton,
  * sort, radix tree, refit, treelet rounds, layout.  Valid after the stream is synced. */
 cav_status cav_bvh_stage_times(cav_ctx* ctx, const cav_bvh* bvh, float* ms6);
