@@ -51,7 +51,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="soup", choices=["soup", "render", "serve"],
+    p.add_argument("--workload", default="soup", choices=["soup", "render", "serve", "guided"],
                    help="soup: BVH + 4M closest-hit rays (default); render: the 5.24M-triangle path-traced scene; "
                         "serve: a Poisson stream of render and ray-query jobs, merged server vs sequential loop")
     p.add_argument("--jobs", type=int, default=256, help="jobs in the served stream (serve workload)")
@@ -677,9 +677,69 @@ def run_serve(args):
     print(json.dumps(out))
 
 
+# ------------------------------------------------------------------------ guided workload
+def run_guided(args):
+    """Config-5 layout (scenes.aperture_scene: a room lit only through a 0.3 x 0.3 aperture,
+    80 % plastic spheres at roughness 0.05), 640 x 360 by default (1280 x 720 is the full
+    config; --small: 256 x 192), depth 10.  relMSE against a 4096-spp plain path render of
+    the same film for plain path, rlpath (Q-table) and the MLP-guided integrator at 16-256
+    spp, with device times; relMSE at equal time is interpolated (log-log) at the guided
+    render's time for each spp."""
+    import tempfile
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    W, H = (256, 192) if args.small else (640, 360)
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "aperture.pbrt")
+    scenes.write_pbrt(path, scenes.aperture_scene(), width=W, height=H, spp=4, max_depth=10)
+    ctx = cav.Context(0)
+    sc = ctx.load_pbrt(path, bvh_rounds=3)
+    s, w, ref_ms = sc.render(spp=4096, integrator="path")
+    ref = s / w[..., None]
+
+    def relmse(x):
+        return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    sc.render(spp=1, integrator="path")  # warm-up
+    rows = {"path": [], "rlpath": [], "guided": []}
+    # the baselines run to 1024 spp so that every guided time lies inside their sweep
+    for spp in (16, 32, 64, 128, 256, 512, 1024):
+        s, w, ms = sc.render(spp=spp, integrator="path")
+        rows["path"].append((spp, ms, relmse(s / w[..., None])))
+        s, w, ms = sc.render(spp=spp, integrator="rlpath")
+        rows["rlpath"].append((spp, ms, relmse(s / w[..., None])))
+        if spp <= 256:
+            s, w, ms, st = sc.render_guided(spp=spp, steps_per_pass=64, lr=5e-3)
+            rows["guided"].append((spp, ms, relmse(s / w[..., None])))
+
+    def at_time(rs, t):
+        ts = np.log([r[1] for r in rs])
+        es = np.log([r[2] for r in rs])
+        return float(np.exp(np.interp(np.log(t), ts, es)))
+
+    equal_time = [{"spp_guided": g[0], "ms": round(g[1], 2), "guided": round(g[2], 6),
+                   "path": round(at_time(rows["path"], g[1]), 6), "rlpath": round(at_time(rows["rlpath"], g[1]), 6)}
+                  for g in rows["guided"]]
+    out = {"metric": "relMSE at equal spp and equal time vs a 4096-spp path render", "unit": "relMSE",
+           "higher_is_better": False, "n_gpus": 1, "dtype": "f32 (network bf16, fp32 accumulate)",
+           "data": "synthetic (seeded aperture scene written as .pbrt)",
+           "config": {"workload": f"aperture_{W}x{H}_depth10", "triangles": int(sc.info().triangles),
+                      "reference_spp": 4096, "reference_ms": round(ref_ms, 1)},
+           "equal_spp": {k: [{"spp": r[0], "ms": round(r[1], 2), "relmse": round(r[2], 6)} for r in v]
+                         for k, v in rows.items()},
+           "equal_time": equal_time}
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
-    if args.workload == "serve":
+    if args.workload == "guided":
+        run_guided(args)
+    elif args.workload == "serve":
         run_serve(args)
     elif args.workload == "render":
         run_render(args)

@@ -94,6 +94,7 @@ def lib() -> ctypes.CDLL:
         "cav_render_to_host": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render_stats": ([P, P], ctypes.c_int),
+        "cav_render_guided": ([P, P, P, P, P, P, P, P, P], ctypes.c_int),
         "cav_mlp_num_params": ([], ctypes.c_int),
         "cav_mlp_create": ([P, ctypes.c_uint64, ctypes.POINTER(P)], ctypes.c_int),
         "cav_mlp_free": ([P], ctypes.c_int),
@@ -216,7 +217,7 @@ class SceneInfo(ctypes.Structure):
                 ("bvh_rounds", ctypes.c_int), ("integrator", ctypes.c_int)]
 
 
-_INTEGRATORS = {None: 0, "path": -1, "rlpath": 1}
+_INTEGRATORS = {None: 0, "path": -1, "rlpath": 1, "guided": 2}
 RENDER_GRAPH = 1
 
 
@@ -242,6 +243,20 @@ class RenderStats(ctypes.Structure):
     _fields_ = [("paths", ctypes.c_int64), ("closest_rays", ctypes.c_int64), ("shadow_rays", ctypes.c_int64),
                 ("bounces", ctypes.c_int), ("ms_total", ctypes.c_float), ("ms_closest", ctypes.c_float),
                 ("ms_shade", ctypes.c_float), ("ms_any", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GuideOpts(ctypes.Structure):
+    _fields_ = [("alpha", ctypes.c_float), ("train_samples_per_pass", ctypes.c_int64),
+                ("train_steps_per_pass", ctypes.c_int), ("train_batch", ctypes.c_int),
+                ("learning_rate", ctypes.c_float), ("freeze", ctypes.c_int), ("seed", ctypes.c_uint64)]
+
+
+class GuideStats(ctypes.Structure):
+    _fields_ = [("passes", ctypes.c_int), ("train_samples", ctypes.c_int64), ("train_steps", ctypes.c_int64),
+                ("last_loss", ctypes.c_float)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -286,6 +301,29 @@ class Scene:
         st = lib().cav_render(self.ctx.handle, self.handle, ctypes.addressof(opts), ptr(film_sum), ptr(film_weight),
                               st_ptr)
         self.ctx._check(st, "cav_render")
+
+    def render_guided(self, spp: int = 0, max_depth: int = 0, width: int = 0, height: int = 0, mlp=None,
+                      alpha: float = 0.5, freeze: bool = False, seed: int = 1, **train):
+        """MLP-guided render into host arrays: (film_sum, film_weight, ms, stats dict)."""
+        import torch
+
+        inf = self.info()
+        W, H = (width, height) if width > 0 and height > 0 else (inf.width, inf.height)
+        fs = torch.zeros(H * W * 3, device=f"cuda:{self.ctx.device}")
+        fw = torch.zeros(H * W, device=f"cuda:{self.ctx.device}")
+        opts = RenderOpts(spp, max_depth, -1, 0, width, height, 0)
+        g = GuideOpts(alpha, train.get("samples_per_pass", 0), train.get("steps_per_pass", 0), train.get("batch", 0),
+                      train.get("lr", 0.0), int(freeze), seed)
+        st_out = GuideStats()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        st = lib().cav_render_guided(self.ctx.handle, self.handle, ctypes.addressof(opts),
+                                     mlp.handle if mlp is not None else None, ctypes.addressof(g), fs.data_ptr(),
+                                     fw.data_ptr(), None, ctypes.addressof(st_out))
+        b.record()
+        self.ctx._check(st, "cav_render_guided")
+        torch.cuda.synchronize()
+        return (fs.view(H, W, 3).cpu().numpy(), fw.view(H, W).cpu().numpy(), a.elapsed_time(b), st_out.as_dict())
 
     def bvh(self) -> "Bvh":
         """The scene's BVH (owned by the scene; valid until the scene is freed)."""

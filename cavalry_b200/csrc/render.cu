@@ -869,6 +869,7 @@ cav_status cav_render(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, 
     if (opts && opts->integrator > 0) integrator = opts->integrator;
     if (opts && opts->integrator < 0) integrator = 0;
     if (integrator == 1) return cav::render_rlpath(ctx, sc, opts, film_sum, film_weight, s);
+    if (integrator == 2) return cav_render_guided(ctx, sc, opts, nullptr, nullptr, film_sum, film_weight, s, nullptr);
     if (integrator != 0) return cav::set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "unknown integrator");
     if (opts && (opts->flags & CAV_RENDER_GRAPH)) return cav::render_path_graph(ctx, sc, opts, film_sum, film_weight, s);
     return cav::render_path(ctx, sc, opts, film_sum, film_weight, s);

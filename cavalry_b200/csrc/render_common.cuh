@@ -588,6 +588,9 @@ inline Camera camera_of(const cav_scene* sc, int W, int H) {
     return cam;
 }
 }  // namespace
+// guided.cu: the MLP-guided path integrator
+cav_status render_guided(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
+                         cudaStream_t s, cav_mlp* net, const cav_guide_opts* gopt, cav_guide_stats* gstats);
 // rlpath.cu: the reinforcement-learning path integrator (Q-table guided directions)
 cav_status render_rlpath(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
                          cudaStream_t s);

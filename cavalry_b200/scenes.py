@@ -338,3 +338,66 @@ def soup_scene(n: int, seed: int):
         "lights": [(1, (20.0, 20.0, 20.0))],
         "camera": {"eye": (0.5, 0.6, -1.6), "look": (0.5, 0.5, 0.5), "up": (0.0, 1.0, 0.0), "fov": 45.0},
     }
+
+
+def aperture_scene(n_spheres: int = 24, level: int = 3, seed: int = 5, room=(8.0, 4.0, 8.0), aperture: float = 0.3):
+    """Config-5 layout: a closed room split by a wall with one square aperture (side
+    `aperture`, centred at mid height); the only light is a 2 x 2 quad under the ceiling of
+    the far side, so the near side, where the camera and the spheres are, is lit only
+    through the aperture (strong indirect light).  Spheres are 80 % plastic at roughness
+    0.05 (remapped) and 20 % matte."""
+    rng = np.random.default_rng(seed)
+    W, H, D = room
+    verts, tris, mesh_ids, meshes, lights = [], [], [], [], []
+    nv = nt = 0
+
+    def add(v, t, name, mat):
+        nonlocal nv, nt
+        mid = len(meshes)
+        verts.append(np.asarray(v, np.float32))
+        tris.append(np.asarray(t, np.int64) + nv)
+        mesh_ids.append(np.full(len(t), mid, np.int32))
+        meshes.append((name, nt, len(t), mat))
+        nv += len(v)
+        nt += len(t)
+        return mid
+
+    def rect_z(xa, xb, ya, yb, z):  # a rectangle in the plane z = const
+        return [[xa, ya, z], [xb, ya, z], [xb, yb, z], [xa, yb, z]], [(0, 1, 2), (0, 2, 3)]
+
+    x0, x1, z0, z1 = -W / 2, W / 2, -D / 2, D / 2
+    grey = (0.73, 0.73, 0.73)
+    add([[x0, 0, z0], [x1, 0, z0], [x1, 0, z1], [x0, 0, z1]], [(0, 2, 1), (0, 3, 2)], "floor", grey)
+    add([[x0, H, z0], [x1, H, z0], [x1, H, z1], [x0, H, z1]], [(0, 1, 2), (0, 2, 3)], "ceiling", grey)
+    add(*rect_z(x0, x1, 0, H, z1), "back", grey)
+    add(*rect_z(x0, x1, 0, H, z0), "front", grey)
+    add([[x0, 0, z0], [x0, 0, z1], [x0, H, z1], [x0, H, z0]], [(0, 1, 2), (0, 2, 3)], "left", (0.63, 0.06, 0.05))
+    add([[x1, 0, z0], [x1, 0, z1], [x1, H, z1], [x1, H, z0]], [(0, 2, 1), (0, 3, 2)], "right", (0.14, 0.45, 0.09))
+    # the dividing wall at z = zw with the aperture around (0, H/2)
+    zw, a, yc = z1 - 2.5, aperture / 2, H / 2
+    parts = [rect_z(x0, -a, 0, H, zw), rect_z(a, x1, 0, H, zw), rect_z(-a, a, 0, yc - a, zw), rect_z(-a, a, yc + a, H, zw)]
+    wv = np.concatenate([np.asarray(v) for v, _ in parts])
+    wt = np.concatenate([np.asarray(t) + 4 * k for k, (_, t) in enumerate(parts)])
+    add(wv, wt, "divider", (0.5, 0.5, 0.5))
+    uv, uf = icosphere(level)
+    for k in range(n_spheres):
+        r = float(rng.uniform(0.2, 0.6))
+        c = np.array([rng.uniform(x0 + r + 0.2, x1 - r - 0.2), r, rng.uniform(z0 + 2.0, zw - r - 0.3)])
+        alb = tuple(float(v) for v in rng.uniform(0.1, 0.9, 3))
+        if rng.random() < 0.8:
+            mat = {"type": "plastic", "Kd": alb, "roughness": 0.05, "remaproughness": True}
+        else:
+            mat = {"type": "matte", "Kd": alb}
+        add(uv * r + c, uf, f"sphere{k}", mat)
+    lz = (zw + z1) / 2
+    mid = add([[-1, H - 0.01, lz - 1], [1, H - 0.01, lz - 1], [1, H - 0.01, lz + 1], [-1, H - 0.01, lz + 1]],
+              [(0, 1, 2), (0, 2, 3)], "light0", (0.0, 0.0, 0.0))
+    lights.append((mid, (50.0, 50.0, 50.0)))
+    return {
+        "positions": np.ascontiguousarray(np.concatenate(verts)),
+        "indices": np.ascontiguousarray(np.concatenate(tris).astype(np.int32)),
+        "mesh_ids": np.concatenate(mesh_ids),
+        "meshes": meshes,
+        "lights": lights,
+        "camera": {"eye": (0.0, 1.8, z0 + 0.3), "look": (0.0, 1.2, zw), "up": (0.0, 1.0, 0.0), "fov": 70.0},
+    }

@@ -204,7 +204,8 @@ typedef struct cav_scene_info_t {
 typedef struct cav_render_opts {
     int spp;                     /* <= 0: the scene's Sampler "pixelsamples" */
     int max_depth;               /* <= 0: the scene's Integrator "maxdepth" */
-    int integrator;              /* 0: the scene's Integrator ("path" or "rlpath"); -1: path; 1: rlpath */
+    int integrator;              /* 0: the scene's Integrator ("path" or "rlpath"); -1: path; 1: rlpath;
+                                    2: MLP-guided path (cav_render_guided with defaults) */
     int64_t max_paths_in_flight; /* <= 0: 4M; samples are rendered in chunks of this many paths */
     int width, height;           /* <= 0: the scene's Film resolution (the camera keeps its fov) */
     int flags;                   /* CAV_RENDER_GRAPH: capture one chunk's bounce chain as a CUDA graph and
@@ -344,6 +345,31 @@ cav_status cav_mlp_last_loss(cav_mlp* mlp, float* loss);
  * (n x 3) drawn with u (n x 3 uniforms); either pair may be NULL. */
 cav_status cav_mlp_mixture(cav_ctx* ctx, const float* out, int64_t n, const float* dirs, float* pdf, const float* u,
                            float* samples, void* stream);
+
+/* MLP-guided path integrator (guided.cu): the path integrator whose continuation at
+ * non-delta surfaces draws, with probability alpha, from the network's mixture instead of
+ * the BSDF, weighted by the one-sample mixture density (unbiased for any network); rendered
+ * in passes of 1, 1, 2, 4, ... spp with the network trained after every pass but the last
+ * on up to train_samples_per_pass vertices (direction, luminance of returned radiance over
+ * throughput).  mlp: a network to use and keep training (NULL: a fresh one for this
+ * render).  Also reachable as cav_render with integrator 2 (fresh network, defaults). */
+typedef struct cav_guide_opts {
+    float alpha;                  /* <= 0: 0.5 */
+    int64_t train_samples_per_pass; /* <= 0: 2^18 */
+    int train_steps_per_pass;     /* <= 0: 32 */
+    int train_batch;              /* <= 0: 16384 */
+    float learning_rate;          /* <= 0: 3e-3 */
+    int freeze;                   /* 1: use the network as is, no training */
+    uint64_t seed;                /* network initialisation when mlp is NULL (0: 1) */
+} cav_guide_opts;
+typedef struct cav_guide_stats {
+    int passes;
+    int64_t train_samples, train_steps;
+    float last_loss;
+} cav_guide_stats;
+cav_status cav_render_guided(cav_ctx* ctx, cav_scene* scene, const cav_render_opts* opts, cav_mlp* mlp,
+                             const cav_guide_opts* gopts, float* film_sum, float* film_weight, void* stream,
+                             cav_guide_stats* stats);
 
 /* Device-side event timing of the last build's stages (ms): leaf boxes + Morton,
  * sort, radix tree, refit, treelet rounds, layout.  Valid after the stream is synced. */
