@@ -94,6 +94,7 @@ def lib() -> ctypes.CDLL:
         "cav_render_to_host": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_render_stats": ([P, P], ctypes.c_int),
+        "cav_bvh_build_batch": ([P, ctypes.c_int, P, P, P, P, P, P, ctypes.c_int, P, P], ctypes.c_int),
         "cav_render_guided": ([P, P, P, P, P, P, P, P, P], ctypes.c_int),
         "cav_mlp_num_params": ([], ctypes.c_int),
         "cav_mlp_create": ([P, ctypes.c_uint64, ctypes.POINTER(P)], ctypes.c_int),
@@ -177,6 +178,21 @@ class Context:
     def set_trace_config(self, block_threads: int = 0, blocks_per_sm: int = 0, batch: int = 0):
         self._check(lib().cav_set_trace_config(self.handle, block_threads, blocks_per_sm, batch),
                     "cav_set_trace_config")
+
+    def build_batch(self, scenes, rounds: int = 0, stream=None) -> list:
+        """Build many BVHs with one launch per LBVH stage: scenes = [(positions, indices) or
+        (positions, indices, mesh_ids)] of CUDA tensors.  Returns one Bvh per scene."""
+        K = len(scenes)
+        P = ctypes.c_void_p
+        pos = (P * K)(*[_ptr(sc[0]) for sc in scenes])
+        idx = (P * K)(*[_ptr(sc[1]) for sc in scenes])
+        mids = (P * K)(*[_ptr(sc[2]) if len(sc) > 2 else None for sc in scenes])
+        nv = (ctypes.c_int64 * K)(*[sc[0].shape[0] for sc in scenes])
+        nt = (ctypes.c_int64 * K)(*[sc[1].shape[0] for sc in scenes])
+        outs = (P * K)()
+        st = lib().cav_bvh_build_batch(self.handle, K, pos, nv, idx, mids, nt, None, rounds, _stream_ptr(stream), outs)
+        self._check(st, "cav_bvh_build_batch")
+        return [Bvh(self, outs[k], int(nt[k]), keep=tuple(scenes[k])) for k in range(K)]
 
     def load_pbrt(self, path: str, spp: int = -1, integrator: str | None = None, bvh_rounds: int = -1) -> Scene:
         """Load a .pbrt scene and build its BVH (the reference's --spp / --integrator / --bvh-opt-rounds)."""

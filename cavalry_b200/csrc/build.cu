@@ -355,10 +355,8 @@ __device__ inline int cpl(const uint64_t* __restrict__ m, uint64_t mi, uint32_t 
 // search, and the `rightChild == leavesCount - 1` leaf clause), writing straight into
 // the merged node layout of mergeNodesArray (BVH/BVH.cu:273-302): internal i at i,
 // leaf j at N-1+j.
-__global__ void __launch_bounds__(kThreads) k_radix_tree(const uint64_t* __restrict__ m, int32_t N,
-                                                         BNode* __restrict__ nodes, int* err) {
-    int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N - 1) return;
+__device__ inline void radix_node(const uint64_t* __restrict__ m, int32_t N, BNode* __restrict__ nodes, int32_t i,
+                                  int* err) {
     const uint64_t mi = __ldg(m + i);
     int d = 1;
     if (i > 0) d = (cpl(m, mi, i, i + 1) - cpl(m, mi, i, i - 1)) >= 0 ? 1 : -1;
@@ -408,16 +406,22 @@ __global__ void __launch_bounds__(kThreads) k_radix_tree(const uint64_t* __restr
     if (i == 0) nd.parent = 0;  // GpuArray zero fill: the root's parent field reads 0
 }
 
+__global__ void __launch_bounds__(kThreads) k_radix_tree(const uint64_t* __restrict__ m, int32_t N,
+                                                         BNode* __restrict__ nodes, int* err) {
+    int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N - 1) return;
+    radix_node(m, N, nodes, i, err);
+}
+
 // Leaf records (fillLeafBoundingBoxes + copyLeafNode, BVH/BVH.cu:46-56, 261-271) and
 // computeBounds (BVH/BVH.cu:217-259): the second arrival at a node unions its
 // children.  Child records written by other threads are read through L2 (ld.cg)
 // after an acquire fence; writes are published with a release fence before the
 // arrival counter is bumped (the reference has no fence here).
-__global__ void __launch_bounds__(kThreads) k_refit(const float* __restrict__ box, const uint32_t* __restrict__ perm,
-                                                    int32_t N, BNode* nodes, uint32_t* visited, int* err) {
-    int32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= N) return;
-    uint32_t t = perm[j];
+// box_index: the leaf's triangle in `box`; prim: the triangle id the leaf records
+__device__ inline void refit_leaf(const float* __restrict__ box, uint32_t box_index, int32_t prim, int32_t N,
+                                  BNode* nodes, uint32_t* visited, int32_t j, int* err) {
+    const uint32_t t = box_index;
     const float* b = box + 6 * (size_t)t;
     f3 lo = mk(b[0], b[1], b[2]), hi = mk(b[3], b[4], b[5]);
     BNode* L = nodes + (N - 1 + j);
@@ -425,7 +429,7 @@ __global__ void __launch_bounds__(kThreads) k_refit(const float* __restrict__ bo
     L->hi_x = hi.x; L->hi_y = hi.y; L->hi_z = hi.z;
     L->left = 0;
     L->right = 0;
-    L->prim = (int32_t)t;
+    L->prim = prim;
     L->is_leaf = 1;
     float area = surface_area(lo, hi);
     L->area = area;
@@ -463,6 +467,14 @@ __global__ void __launch_bounds__(kThreads) k_refit(const float* __restrict__ bo
         if (curr == 0) return;
         curr = __ldcg(&nd->parent);
     }
+}
+
+__global__ void __launch_bounds__(kThreads) k_refit(const float* __restrict__ box, const uint32_t* __restrict__ perm,
+                                                    int32_t N, BNode* nodes, uint32_t* visited, int* err) {
+    int32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    const uint32_t t = perm[j];
+    refit_leaf(box, t, (int32_t)t, N, nodes, visited, j, err);
 }
 
 // ---------------------------------------------------------------- layout
@@ -605,17 +617,12 @@ T* carve(unsigned char*& p, size_t count) {
 
 }  // namespace
 
-cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int32_t* indices,
-                     const int32_t* mesh_ids, int64_t n, const float* bounds, int rounds, cudaStream_t s,
-                     cav_bvh** out) {
-    if (!positions || !indices || !out || nv < 1 || n < 2 || n >= (1ll << 30) || rounds < 0)
-        return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build: invalid argument");
+// The persistent arena of one tree: build nodes, codes, permutation, traversal layout.
+cav_status alloc_bvh(cav_ctx* ctx, int64_t n, cav_bvh** out) {
     const int64_t count = 2 * n - 1;
     cav_bvh* bvh = new cav_bvh();
     bvh->n = n;
     bvh->device = ctx->device;
-
-    // persistent arena
     size_t need = 0;
     need += sizeof(BNode) * count + 256;
     need += 2 * (sizeof(uint64_t) * n + 256);
@@ -637,6 +644,19 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     bvh->tris = carve<TriRec>(p, n);
     bvh->d_root_box = carve<float>(p, 8);
     bvh->d_depth = carve<int32_t>(p, 8);
+    *out = bvh;
+    return CAV_OK;
+}
+
+cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int32_t* indices,
+                     const int32_t* mesh_ids, int64_t n, const float* bounds, int rounds, cudaStream_t s,
+                     cav_bvh** out) {
+    if (!positions || !indices || !out || nv < 1 || n < 2 || n >= (1ll << 30) || rounds < 0)
+        return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build: invalid argument");
+    const int64_t count = 2 * n - 1;
+    cav_bvh* bvh = nullptr;
+    cav_status ast = alloc_bvh(ctx, n, &bvh);
+    if (ast != CAV_OK) return ast;
 
     // scratch (stream ordered)
     const int tiles = div_up(n, kSortTile);
@@ -745,6 +765,331 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     k_merge_error<<<1, 32, 0, s>>>(err, ctx->d_error);
     CAV_CUDA(ctx, cudaFreeAsync(sbase, s));
     *out = bvh;
+    return CAV_OK;
+}
+
+// ------------------------------------------------------------ many scenes, one launch
+// A batch of scenes is built stage by stage with ONE launch per stage across all of them:
+// leaf boxes and per-scene bounds, Morton codes (each scene against its own bounds), one
+// stable sort of every code followed by one stable digit pass on the scene index (so each
+// scene's codes end up contiguous and in the order a build of that scene alone gives),
+// the radix trees of every scene, and the refits of every scene.  A thread finds its scene
+// by binary search over the scenes' prefix offsets.  The treelet rounds and the traversal
+// layout then run per scene.  Every scene gets its own cav_bvh, identical to cav_bvh_build's.
+namespace {
+
+struct BuildSeg {
+    const float* pos;
+    const int32_t* idx;
+    int64_t n;
+    BNode* nodes;
+    int32_t* perm;
+    uint64_t* codes_sorted;
+    uint64_t* codes_unsorted;
+    float bounds[6];
+    int use_dev;
+};
+
+__device__ inline int find_off(const int64_t* offs, int K, int64_t g) {
+    int lo = 0, hi = K - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (offs[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kThreads) k_leaf_boxes_batch(const BuildSeg* segs, const int64_t* leaf_offs, int K,
+                                                               int64_t total, float* __restrict__ box,
+                                                               int32_t* bounds_ord) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = g < total;
+    int sg = -1;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    bool dev = false;
+    if (valid) {
+        sg = find_off(leaf_offs, K, g);
+        const BuildSeg& S = segs[sg];
+        const int64_t t = g - leaf_offs[sg];
+        int32_t a = __ldg(S.idx + 3 * t), b = __ldg(S.idx + 3 * t + 1), c = __ldg(S.idx + 3 * t + 2);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float v0 = __ldg(S.pos + 3 * (int64_t)a + k), v1 = __ldg(S.pos + 3 * (int64_t)b + k),
+                  v2 = __ldg(S.pos + 3 * (int64_t)c + k);
+            lo[k] = fminf(v0, fminf(v1, v2));
+            hi[k] = fmaxf(v0, fmaxf(v1, v2));
+        }
+        float* o = box + 6 * g;
+        o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
+        o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
+        dev = S.use_dev != 0;
+    }
+    // bounds of the scenes without given bounds: a warp of one scene reduces first
+    const unsigned same = __match_any_sync(0xffffffffu, valid && dev ? sg : -1);
+    if (!(valid && dev)) return;
+    if (same == 0xffffffffu) {
+        int32_t v[6];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v[k] = __reduce_min_sync(0xffffffffu, f2ord(lo[k]));
+            v[3 + k] = __reduce_max_sync(0xffffffffu, f2ord(hi[k]));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            for (int k = 0; k < 3; ++k) atomicMin(bounds_ord + 6 * sg + k, v[k]);
+            for (int k = 0; k < 3; ++k) atomicMax(bounds_ord + 6 * sg + 3 + k, v[3 + k]);
+        }
+    } else {
+        for (int k = 0; k < 3; ++k) atomicMin(bounds_ord + 6 * sg + k, f2ord(lo[k]));
+        for (int k = 0; k < 3; ++k) atomicMax(bounds_ord + 6 * sg + 3 + k, f2ord(hi[k]));
+    }
+}
+
+__global__ void k_bounds_batch(int32_t* bounds_ord, int K, int init, float* bounds) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 6 * K) return;
+    if (init) bounds_ord[k] = (k % 6) < 3 ? INT32_MAX : INT32_MIN;
+    else bounds[k] = ord2f(bounds_ord[k]);
+}
+
+__global__ void __launch_bounds__(kThreads) k_morton_batch(const float* __restrict__ box, const BuildSeg* segs,
+                                                           const int64_t* leaf_offs, int K, int64_t total,
+                                                           const float* dev_bounds, uint64_t* __restrict__ codes,
+                                                           uint64_t* __restrict__ codes_copy, uint32_t* __restrict__ vals) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int sg = find_off(leaf_offs, K, g);
+    const BuildSeg& S = segs[sg];
+    const float* bb = S.use_dev ? dev_bounds + 6 * sg : S.bounds;
+    f3 slo = mk(bb[0], bb[1], bb[2]), shi = mk(bb[3], bb[4], bb[5]);
+    const float* b = box + 6 * g;
+    f3 lo = mk(b[0], b[1], b[2]), hi = mk(b[3], b[4], b[5]);
+    f3 centroid = ((lo + hi) * 0.5f - (slo + shi) * 0.5f) / (shi - slo);  // as k_morton
+    uint64_t factor = (uint64_t)(1L << 21);
+    uint64_t x = centroid.x * factor;
+    uint64_t y = centroid.y * factor;
+    uint64_t z = centroid.z * factor;
+    uint64_t code = (spread3(x) << 2) | (spread3(y) << 1) | spread3(z);
+    codes[g] = code;
+    codes_copy[g] = code;
+    vals[g] = (uint32_t)g;
+}
+
+__global__ void k_scene_keys(const uint32_t* vals, const int64_t* leaf_offs, int K, int64_t total, uint64_t* key) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    key[i] = (uint64_t)find_off(leaf_offs, K, vals[i]);
+}
+
+// per scene: codes in triangle order and in sorted order, and the scene-local permutation
+__global__ void k_scatter_batch(const uint64_t* codes_copy, const uint32_t* vals, const BuildSeg* segs,
+                                const int64_t* leaf_offs, int K, int64_t total) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int sg = find_off(leaf_offs, K, g);
+    const BuildSeg& S = segs[sg];
+    const int64_t j = g - leaf_offs[sg];
+    const uint32_t t = vals[g];
+    S.codes_unsorted[j] = codes_copy[g];
+    S.codes_sorted[j] = codes_copy[t];
+    S.perm[j] = (int32_t)((int64_t)t - leaf_offs[sg]);
+}
+
+__global__ void __launch_bounds__(kThreads) k_radix_batch(const BuildSeg* segs, const int64_t* int_offs, int K,
+                                                          int64_t total_internal, int* err) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total_internal) return;
+    const int sg = find_off(int_offs, K, g);
+    const BuildSeg& S = segs[sg];
+    radix_node(S.codes_sorted, (int32_t)S.n, S.nodes, (int32_t)(g - int_offs[sg]), err);
+}
+
+__global__ void __launch_bounds__(kThreads) k_refit_batch(const float* __restrict__ box, const uint32_t* vals,
+                                                          const BuildSeg* segs, const int64_t* leaf_offs,
+                                                          const int64_t* int_offs, int K, int64_t total,
+                                                          uint32_t* visited, int* err) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int sg = find_off(leaf_offs, K, g);
+    const BuildSeg& S = segs[sg];
+    const uint32_t t = vals[g];
+    refit_leaf(box, t, (int32_t)((int64_t)t - leaf_offs[sg]), (int32_t)S.n, S.nodes, visited + int_offs[sg],
+               (int32_t)(g - leaf_offs[sg]), err);
+}
+
+}  // namespace
+
+cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, const int64_t* num_vertices,
+                           const int32_t* const* indices, const int32_t* const* mesh_ids, const int64_t* num_triangles,
+                           const float* bounds, int rounds, cudaStream_t s, cav_bvh** out) {
+    if (K < 1 || K > 65536 || !positions || !indices || !num_triangles || !out || rounds < 0)
+        return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build_batch: invalid argument");
+    std::vector<int64_t> leaf_offs(K + 1, 0), int_offs(K + 1, 0);
+    int64_t nmax = 0;
+    for (int k = 0; k < K; ++k) {
+        const int64_t n = num_triangles[k];
+        if (!positions[k] || !indices[k] || n < 2 || n >= (1ll << 30) || (num_vertices && num_vertices[k] < 1))
+            return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build_batch: bad scene");
+        leaf_offs[k + 1] = leaf_offs[k] + n;
+        int_offs[k + 1] = int_offs[k] + n - 1;
+        nmax = std::max(nmax, n);
+    }
+    const int64_t total = leaf_offs[K], total_int = int_offs[K];
+    if (total >= (1ll << 32)) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build_batch: too many triangles");
+    for (int k = 0; k < K; ++k) out[k] = nullptr;
+    std::vector<cav_bvh*> bv(K, nullptr);
+    auto fail = [&](cav_status st) {
+        for (cav_bvh* b : bv)
+            if (b) {
+                cudaFree(b->arena);
+                delete b;
+            }
+        return st;
+    };
+    for (int k = 0; k < K; ++k) {
+        cav_status st = alloc_bvh(ctx, num_triangles[k], &bv[k]);
+        if (st != CAV_OK) return fail(st);
+    }
+    std::vector<BuildSeg> hs(K);
+    for (int k = 0; k < K; ++k) {
+        BuildSeg& g = hs[k];
+        g.pos = positions[k];
+        g.idx = indices[k];
+        g.n = num_triangles[k];
+        g.nodes = bv[k]->nodes;
+        g.perm = bv[k]->perm;
+        g.codes_sorted = bv[k]->codes_sorted;
+        g.codes_unsorted = bv[k]->codes_unsorted;
+        g.use_dev = bounds ? 0 : 1;
+        for (int c = 0; c < 6; ++c) g.bounds[c] = bounds ? bounds[6 * k + c] : 0.f;
+    }
+    const int tiles = div_up(total, kSortTile);
+    const int passes2 = K <= 256 ? 1 : 2;
+    const int64_t cmax = 2 * nmax - 1;
+    size_t scratch = 0;
+    auto acc = [&](size_t b) { scratch += b + 256; };
+    acc(sizeof(BuildSeg) * K);
+    acc(sizeof(int64_t) * (K + 1) * 2);
+    acc(sizeof(float) * 6 * total);                 // leaf boxes
+    acc(sizeof(uint64_t) * total * 3);              // codes, codes copy, ping-pong
+    acc(sizeof(uint32_t) * total * 2);              // values ping-pong
+    acc(sizeof(uint32_t) * 2 * 8 * 256);            // histograms (codes, scene keys)
+    acc(sizeof(uint32_t) * (8 + passes2) * (size_t)tiles * 256);  // look-back status
+    acc(sizeof(uint32_t) * 32);                     // tile counters
+    acc(sizeof(int32_t) * 6 * K * 2);               // bounds (ordered ints, floats)
+    acc(sizeof(int32_t) * 8);                       // error flag
+    acc(sizeof(uint32_t) * std::max<int64_t>(total_int, cmax));  // visited (refit, then treelets)
+    acc(sizeof(int32_t) * nmax);                    // leaf list
+    acc(sizeof(int32_t) * cmax);                    // compact index
+    acc(sizeof(int32_t) * nmax);                    // slot_of
+    acc(sizeof(uint32_t) * (div_up(cmax, kScanTile) + 1));
+    void* sbase = nullptr;
+    if (cudaMallocAsync(&sbase, scratch, s) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "cav_bvh_build_batch: scratch allocation failed"));
+    }
+    unsigned char* q = (unsigned char*)sbase;
+    BuildSeg* dsegs = carve<BuildSeg>(q, K);
+    int64_t* d_leaf = carve<int64_t>(q, K + 1);
+    int64_t* d_int = carve<int64_t>(q, K + 1);
+    float* leafbox = carve<float>(q, 6 * total);
+    uint64_t* codes = carve<uint64_t>(q, total);
+    uint64_t* codes_copy = carve<uint64_t>(q, total);
+    uint64_t* keys_b = carve<uint64_t>(q, total);
+    uint32_t* vals_a = carve<uint32_t>(q, total);
+    uint32_t* vals_b = carve<uint32_t>(q, total);
+    uint32_t* hist = carve<uint32_t>(q, 2 * 8 * 256);
+    uint32_t* status = carve<uint32_t>(q, (8 + passes2) * (size_t)tiles * 256);
+    uint32_t* counters = carve<uint32_t>(q, 32);
+    int32_t* bounds_ord = carve<int32_t>(q, 6 * K);
+    float* dbounds = carve<float>(q, 6 * K);
+    int32_t* err = carve<int32_t>(q, 8);
+    uint32_t* visited = carve<uint32_t>(q, std::max<int64_t>(total_int, cmax));
+    int32_t* leaf_list = carve<int32_t>(q, nmax);
+    int32_t* compact = carve<int32_t>(q, cmax);
+    int32_t* slot_of = carve<int32_t>(q, nmax);
+    uint32_t* blk = carve<uint32_t>(q, div_up(cmax, kScanTile) + 1);
+    // tables (synchronous copies from pageable host memory, before any launch reads them)
+    CAV_CUDA(ctx, cudaStreamSynchronize(s));
+    CAV_CUDA(ctx, cudaMemcpy(dsegs, hs.data(), sizeof(BuildSeg) * K, cudaMemcpyHostToDevice));
+    CAV_CUDA(ctx, cudaMemcpy(d_leaf, leaf_offs.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice));
+    CAV_CUDA(ctx, cudaMemcpy(d_int, int_offs.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice));
+    CAV_CUDA(ctx, cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 2 * 8 * 256, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(status, 0, sizeof(uint32_t) * (8 + passes2) * (size_t)tiles * 256, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 32, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(err, 0, sizeof(int32_t) * 8, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(visited, 0, sizeof(uint32_t) * total_int, s));
+    for (int k = 0; k < K; ++k) {
+        CAV_CUDA(ctx, cudaMemsetAsync(bv[k]->nodes, 0, sizeof(BNode) * (2 * num_triangles[k] - 1), s));
+        for (int e = 0; e < 7; ++e) cudaEventCreate(&bv[k]->ev[e]);
+        bv[k]->timed = true;
+        cudaEventRecord(bv[k]->ev[0], s);
+    }
+    const int gb = div_up(total, kThreads);
+    if (!bounds) k_bounds_batch<<<div_up(6 * K, 256), 256, 0, s>>>(bounds_ord, K, 1, dbounds);
+    k_leaf_boxes_batch<<<gb, kThreads, 0, s>>>(dsegs, d_leaf, K, total, leafbox, bounds_ord);
+    if (!bounds) k_bounds_batch<<<div_up(6 * K, 256), 256, 0, s>>>(bounds_ord, K, 0, dbounds);
+    k_morton_batch<<<gb, kThreads, 0, s>>>(leafbox, dsegs, d_leaf, K, total, dbounds, codes, codes_copy, vals_a);
+    for (int k = 0; k < K; ++k) cudaEventRecord(bv[k]->ev[1], s);
+    // sort by code (8 passes, stable), then by scene (1-2 passes, stable)
+    CAV_CUDA(ctx, cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem)));
+    k_sort_hist<<<std::min(gb, ctx->num_sms * 8), kSortThreads, 0, s>>>(codes, total, hist);
+    uint64_t* kin = codes;
+    uint64_t* kout = keys_b;
+    uint32_t* vin = vals_a;
+    uint32_t* vout = vals_b;
+    for (int pass = 0; pass < 8; ++pass) {
+        k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, total, 8 * pass,
+                                                                  hist + 256 * pass,
+                                                                  status + (size_t)pass * tiles * 256, counters + pass,
+                                                                  err);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    // kin/vin: codes in code order; now key by scene index
+    k_scene_keys<<<gb, kThreads, 0, s>>>(vin, d_leaf, K, total, kin);
+    k_sort_hist<<<std::min(gb, ctx->num_sms * 8), kSortThreads, 0, s>>>(kin, total, hist + 8 * 256);
+    for (int pass = 0; pass < passes2; ++pass) {
+        k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, total, 8 * pass,
+                                                                  hist + 8 * 256 + 256 * pass,
+                                                                  status + (size_t)(8 + pass) * tiles * 256,
+                                                                  counters + 8 + pass, err);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    k_scatter_batch<<<gb, kThreads, 0, s>>>(codes_copy, vin, dsegs, d_leaf, K, total);
+    for (int k = 0; k < K; ++k) cudaEventRecord(bv[k]->ev[2], s);
+    k_radix_batch<<<div_up(total_int, kThreads), kThreads, 0, s>>>(dsegs, d_int, K, total_int, err);
+    for (int k = 0; k < K; ++k) cudaEventRecord(bv[k]->ev[3], s);
+    k_refit_batch<<<gb, kThreads, 0, s>>>(leafbox, vin, dsegs, d_leaf, d_int, K, total, visited, err);
+    for (int k = 0; k < K; ++k) cudaEventRecord(bv[k]->ev[4], s);
+    CAV_CUDA(ctx, cudaGetLastError());
+    // per scene: treelet rounds and traversal layout
+    for (int k = 0; k < K; ++k) {
+        cav_bvh* b = bv[k];
+        const int64_t n = num_triangles[k], count = 2 * n - 1;
+        cav_status st = treelet_rounds(ctx, b->nodes, n, rounds, leaf_list, visited, s);
+        if (st != CAV_OK) {
+            cudaFreeAsync(sbase, s);
+            return fail(st);
+        }
+        cudaEventRecord(b->ev[5], s);
+        const int nblk = div_up(count, kScanTile);
+        k_count_internal<<<nblk, kScanThreads, 0, s>>>(b->nodes, count, blk);
+        k_scan_blocks<<<1, kScanThreads, 0, s>>>(blk, nblk);
+        k_compact_index<<<nblk, kScanThreads, 0, s>>>(b->nodes, count, blk, compact);
+        k_tri_layout<<<div_up(n, kThreads), kThreads, 0, s>>>(positions[k], indices[k], mesh_ids ? mesh_ids[k] : nullptr,
+                                                             reinterpret_cast<const uint32_t*>(b->perm), n, b->tris,
+                                                             slot_of);
+        k_tnode_layout<<<div_up(count, kThreads), kThreads, 0, s>>>(b->nodes, count, compact, slot_of, b->tnodes,
+                                                                    b->d_root_box);
+        cudaEventRecord(b->ev[6], s);
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    k_merge_error<<<1, 32, 0, s>>>(err, ctx->d_error);
+    CAV_CUDA(ctx, cudaFreeAsync(sbase, s));
+    for (int k = 0; k < K; ++k) out[k] = bv[k];
     return CAV_OK;
 }
 

@@ -128,6 +128,16 @@ cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_
     return CAV_OK;
 }
 
+cav_status cav_bvh_build_batch(cav_ctx* ctx, int num_scenes, const float* const* positions,
+                               const int64_t* num_vertices, const int32_t* const* indices,
+                               const int32_t* const* mesh_ids, const int64_t* num_triangles,
+                               const float* scene_bounds, int rounds, void* stream, cav_bvh** out) {
+    cav_status st = use_device(ctx);
+    if (st != CAV_OK) return st;
+    return build_bvh_batch(ctx, num_scenes, positions, num_vertices, indices, mesh_ids, num_triangles, scene_bounds,
+                           rounds, (cudaStream_t)stream, out);
+}
+
 cav_status cav_bvh_build(cav_ctx* ctx, const float* positions, int64_t num_vertices, const int32_t* indices,
                          const int32_t* mesh_ids, int64_t num_triangles, const float* scene_bounds, int rounds,
                          void* stream, cav_bvh** out) {

@@ -163,6 +163,11 @@ cav_status trace_any_dev(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, 
                          const int32_t* excl, const uint32_t* n_dev, uint8_t* occ, cudaStream_t s,
                          unsigned long long* counter);
 
+// Many scenes' BVHs, one launch per LBVH stage across all of them (build.cu)
+cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, const int64_t* num_vertices,
+                           const int32_t* const* indices, const int32_t* const* mesh_ids, const int64_t* num_triangles,
+                           const float* bounds, int rounds, cudaStream_t s, cav_bvh** out);
+
 // MLP forward pass for the guided integrator (mlp.cu): in n x 5 -> out n x 32
 cav_status mlp_forward(cav_mlp* m, const float* in, int64_t n, float* out, cudaStream_t s);
 

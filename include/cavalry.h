@@ -371,6 +371,18 @@ cav_status cav_render_guided(cav_ctx* ctx, cav_scene* scene, const cav_render_op
                              const cav_guide_opts* gopts, float* film_sum, float* film_weight, void* stream,
                              cav_guide_stats* stats);
 
+/* Builds the BVHs of num_scenes scenes with one launch per LBVH stage across all of them
+ * (leaf boxes and per-scene bounds, Morton codes, one stable sort of every code plus one
+ * stable pass on the scene index, the radix trees, the refits); treelet rounds and the
+ * traversal layout then run per scene.  out[k] is identical to cav_bvh_build of scene k
+ * alone.  positions[k], indices[k], mesh_ids[k] (mesh_ids may be NULL) are DEVICE arrays;
+ * num_vertices (may be NULL), num_triangles: host arrays; scene_bounds: NULL (computed) or
+ * num_scenes x 6 host floats.  At most 65,536 scenes and 2^32 triangles in total. */
+cav_status cav_bvh_build_batch(cav_ctx* ctx, int num_scenes, const float* const* positions,
+                               const int64_t* num_vertices, const int32_t* const* indices,
+                               const int32_t* const* mesh_ids, const int64_t* num_triangles,
+                               const float* scene_bounds, int rounds, void* stream, cav_bvh** out);
+
 /* Device-side event timing of the last build's stages (ms): leaf boxes + Morton,
  * sort, radix tree, refit, treelet rounds, layout.  Valid after the stream is synced. */
 cav_status cav_bvh_stage_times(cav_ctx* ctx, const cav_bvh* bvh, float* ms6);
