@@ -494,6 +494,27 @@ def run_render(args):
             b.record()
             torch.cuda.synchronize()
             ours.append(len(r) * 5 / (a.elapsed_time(b) * 1e-3) / 1e6)
+        # the same rays in the 4-wide fast mode (same hit distances; ties may pick another triangle)
+        fast = []
+        for r in caps:
+            for _ in range(3):
+                bvh.trace_closest(r, flags=cav.TRACE_FAST)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(5):
+                bvh.trace_closest(r, flags=cav.TRACE_FAST)
+            b.record()
+            torch.cuda.synchronize()
+            fast.append(len(r) * 5 / (a.elapsed_time(b) * 1e-3) / 1e6)
+        runs[rounds]["ours_fast_captured_mrays_s"] = [round(x, 2) for x in fast]
+        # a whole render with the fast traversal
+        torch.cuda.synchronize()
+        sc.render_into(fs, fw, fast_trace=True)
+        stf = sc.stats().as_dict()
+        runs[rounds]["fast_render"] = {
+            "ms_render": round(stf["ms_total"], 2),
+            "extend_mrays_s": round(stf["closest_rays"] / (stf["ms_closest"] * 1e-3) / 1e6, 2),
+            "shadow_mrays_s": round(stf["shadow_rays"] / max(stf["ms_any"], 1e-9) * 1e-3, 2)}
         runs[rounds]["captured_rays"] = [int(len(r)) for r in caps]
         runs[rounds]["captured_launch_shapes"] = shapes
         runs[rounds]["ours_captured_mrays_s"] = [round(x, 2) for x in ours]
@@ -522,6 +543,8 @@ def run_render(args):
                 ref[f"rounds{rounds}_bvh_intersect_mrays_s"] = mr
                 ref[f"rounds{rounds}_speedup"] = [round(a / b, 2) for a, b in
                                                   zip(runs[rounds]["ours_captured_mrays_s"], mr)]
+                ref[f"rounds{rounds}_speedup_fast"] = [round(a / b, 2) for a, b in
+                                                       zip(runs[rounds]["ours_fast_captured_mrays_s"], mr)]
             R.free()
         except Exception as e:  # the harness is test infrastructure: report, do not fail the bench
             ref["harness_error"] = str(e)[:300]

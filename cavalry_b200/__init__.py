@@ -27,6 +27,7 @@ _LIB_PATH = _PKG / "libcavalry_b200.so"
 
 TRACE_EXACT = 0
 TRACE_CULL_ON_POP = 1
+TRACE_FAST = 2
 
 STATUS = {
     0: "ok",
@@ -235,6 +236,7 @@ class SceneInfo(ctypes.Structure):
 
 _INTEGRATORS = {None: 0, "path": -1, "rlpath": 1, "guided": 2}
 RENDER_GRAPH = 1
+RENDER_FAST_TRACE = 2
 
 
 class RenderOpts(ctypes.Structure):
@@ -291,7 +293,7 @@ class Scene:
         return out
 
     def render(self, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0, integrator: str | None = None,
-               width: int = 0, height: int = 0, graph: bool = False):
+               width: int = 0, height: int = 0, graph: bool = False, fast_trace: bool = False):
         """Render to host arrays; returns (film_sum [H,W,3], film_weight [H,W], ms).  integrator:
         None = the scene's, "path" or "rlpath"; width/height override the Film resolution."""
         inf = self.info()
@@ -300,20 +302,21 @@ class Scene:
         w = np.zeros((H, W), np.float32)
         ms = np.zeros(1, np.float32)
         opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height,
-                          RENDER_GRAPH if graph else 0)
+                          (RENDER_GRAPH if graph else 0) | (RENDER_FAST_TRACE if fast_trace else 0))
         st = lib().cav_render_to_host(self.ctx.handle, self.handle, ctypes.addressof(opts), s.ctypes.data,
                                       w.ctypes.data, ms.ctypes.data)
         self.ctx._check(st, "cav_render_to_host")
         return s, w, float(ms[0])
 
     def render_into(self, film_sum, film_weight, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0,
-                    stream=None, integrator: str | None = None, width: int = 0, height: int = 0, graph: bool = False):
+                    stream=None, integrator: str | None = None, width: int = 0, height: int = 0, graph: bool = False,
+                    fast_trace: bool = False):
         """Render into DEVICE films (pointers, or objects with data_ptr(): 3 + 1 floats per
         pixel), stream-ordered on `stream` (a pointer, an object with cuda_stream, or None)."""
         ptr = lambda x: x if isinstance(x, int) else x.data_ptr()  # noqa: E731
         st_ptr = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
         opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height,
-                          RENDER_GRAPH if graph else 0)
+                          (RENDER_GRAPH if graph else 0) | (RENDER_FAST_TRACE if fast_trace else 0))
         st = lib().cav_render(self.ctx.handle, self.handle, ctypes.addressof(opts), ptr(film_sum), ptr(film_weight),
                               st_ptr)
         self.ctx._check(st, "cav_render")

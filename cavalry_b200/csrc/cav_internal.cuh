@@ -67,6 +67,21 @@ struct __align__(64) TNode {
 };
 static_assert(sizeof(TNode) == 64, "TNode must be 64 bytes");
 
+// 4-wide traversal node (128 bytes) of the fast mode: one per binary traversal node, whose
+// children are that node's grandchildren (a triangle child stays a direct child), so a
+// walk from the root visits every other binary level.  Child boxes are stored per axis for
+// 32-byte vector loads; ref >= 0 is another wide node (binary index), ~slot a triangle,
+// kWideEmpty an unused slot.
+constexpr int32_t kWideEmpty = INT32_MIN;
+struct __align__(128) WNode {
+    float lox[4], loy[4];
+    float loz[4], hix[4];
+    float hiy[4], hiz[4];
+    int32_t ref[4];
+    int32_t pad[4];
+};
+static_assert(sizeof(WNode) == 128, "WNode must be 128 bytes");
+
 // Triangle record (48 bytes) in sorted (Morton) order: v0, e1 = v1-v0, e2 = v2-v0
 // (the same subtractions as Core/Triangle.h:180-183), triangle id and mesh id.
 struct __align__(16) TriRec {
@@ -111,6 +126,7 @@ struct cav_bvh {
     int32_t* perm = nullptr;             // N: sorted position -> triangle id
     // traversal layout
     cav::TNode* tnodes = nullptr;  // N-1
+    cav::WNode* wnodes = nullptr;  // N-1: the 4-wide view for CAV_TRACE_FAST
     cav::TriRec* tris = nullptr;   // N
     float root_box[6];             // copied to the host at build time? no: device copy
     float* d_root_box = nullptr;   // 6 floats on device

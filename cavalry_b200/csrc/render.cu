@@ -380,6 +380,7 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
 
     DevScene S = dev_scene_of(sc);
     Camera cam = camera_of(sc, W, H);
+    const uint32_t tflags = opts && (opts->flags & CAV_RENDER_FAST_TRACE) ? CAV_TRACE_FAST : CAV_TRACE_EXACT;
     uint32_t counts[2];
     auto& log = sc->log;
     log.reset();
@@ -403,7 +404,7 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
             }
             cudaEvent_t e0 = log.next(), e1 = log.next(), e2 = log.next();
             CAV_CUDA(ctx, cudaEventRecord(e0, s));
-            cav_status st = trace_closest(ctx, sc->bvh, Q.rays, n, Q.hit_prim, Q.hit_t, Q.hit_uv, CAV_TRACE_EXACT, s,
+            cav_status st = trace_closest(ctx, sc->bvh, Q.rays, n, Q.hit_prim, Q.hit_t, Q.hit_uv, tflags, s,
                                           ctx->d_counters + 6);
             if (st != CAV_OK) return st;
             CAV_CUDA(ctx, cudaEventRecord(e1, s));
@@ -421,7 +422,7 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
                 cudaEvent_t e3 = log.next(), e4 = log.next();
                 CAV_CUDA(ctx, cudaEventRecord(e3, s));
                 st = trace_any(ctx, sc->bvh, Q.shadow_rays, Q.shadow_limit, Q.shadow_excl, counts[1], Q.shadow_occ,
-                               CAV_TRACE_EXACT, s, ctx->d_counters + 7);
+                               tflags, s, ctx->d_counters + 7);
                 if (st != CAV_OK) return st;
                 CAV_CUDA(ctx, cudaEventRecord(e4, s));
                 log.any.emplace_back(e3, e4);

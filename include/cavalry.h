@@ -106,6 +106,8 @@ typedef struct cav_ray {
 
 /* trace flags */
 #define CAV_TRACE_EXACT 0u        /* reference order and pruning (BVH/BVH.h); default */
+#define CAV_TRACE_FAST 2u         /* 4-wide traversal of the same tree: identical hit distances, equal-distance
+                                     ties may resolve to a different triangle than the reference order */
 #define CAV_TRACE_CULL_ON_POP 1u  /* also re-test a popped node against the current hit
                                      distance / distance limit (fewer visits; results can
                                      differ from the reference only at exact-t ties) */
@@ -212,7 +214,7 @@ typedef struct cav_render_opts {
                                     replay it per chunk, with queue sizes kept on the device (no host round
                                     trip per bounce; path integrator; per-stage times not recorded) */
 } cav_render_opts;
-enum { CAV_RENDER_GRAPH = 1 };
+enum { CAV_RENDER_GRAPH = 1, CAV_RENDER_FAST_TRACE = 2 /* trace with CAV_TRACE_FAST (path integrator) */ };
 
 /* Host-only .pbrt parse (no GPU): scene counts and the camera-to-world matrix (16 floats,
  * column-major; may be NULL).  On a parse error returns CAV_ERR_INVALID_ARGUMENT and copies the
