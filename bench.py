@@ -51,10 +51,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="soup", choices=["soup", "render", "serve", "guided"],
+    p.add_argument("--workload", default="soup", choices=["soup", "render", "serve", "guided", "mlp"],
                    help="soup: BVH + 4M closest-hit rays (default); render: the 5.24M-triangle path-traced scene; "
                         "serve: a Poisson stream of render and ray-query jobs, merged server vs sequential loop")
     p.add_argument("--jobs", type=int, default=256, help="jobs in the served stream (serve workload)")
+    p.add_argument("--no-reference", action="store_true", help="render workload: skip the reference's CUDA build")
     p.add_argument("--render-steps", type=int, default=1, help="timed full renders (render workload)")
     p.add_argument("--small", action="store_true", help="render workload at 1/16 size (smoke runs)")
     p.add_argument("--tris", type=int, default=None, help="soup size (default: the 1M-triangle workload)")
@@ -528,7 +529,7 @@ def run_render(args):
     out["clocks"] = clocks
     # reference CUDA build on the same B200
     ref = {}
-    if po.ref_available():
+    if po.ref_available() and not args.no_reference:
         try:
             R = po.RefScene(scene["positions"], scene["indices"], scene["mesh_ids"], rounds=0, dump=False)
             for rounds in (0, 3):
@@ -548,7 +549,7 @@ def run_render(args):
             R.free()
         except Exception as e:  # the harness is test infrastructure: report, do not fail the bench
             ref["harness_error"] = str(e)[:300]
-    if ref_cli.available():
+    if ref_cli.available() and not args.no_reference:
         try:
             t0 = time.time()
             img, text = ref_cli.render(pbrt, os.path.join(tmp, "ref.png"), spp=spp, timeout=1500)
@@ -758,9 +759,65 @@ def run_guided(args):
     print(json.dumps(out))
 
 
+# ------------------------------------------------------------------------ mlp workload
+def run_mlp(args):
+    """The learned proposal's kernels alone: forward passes over 4M vertices (--small: 1M)
+    and Adam steps at batch 16,384, device-timed; FLOP/s counts the 41 kFLOP of one
+    forward pass per vertex (160x64 + 2 x 64x64 + 64x32 multiply-adds x 2)."""
+    import torch
+
+    import cavalry_b200 as cav
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    ctx = cav.Context(0)
+    net = cav.Mlp(ctx, seed=1)
+    n = 1 << 20 if args.small else 1 << 22
+    g = torch.Generator("cuda").manual_seed(1)
+    x = torch.rand((n, 5), device="cuda", generator=g)
+    d = torch.nn.functional.normalize(torch.randn((n, 3), device="cuda", generator=g), dim=1).contiguous()
+    w = torch.rand(n, device="cuda", generator=g)
+    flop = 2 * (160 * 64 + 2 * 64 * 64 + 64 * 32)
+    for _ in range(max(args.warmup, 1)):
+        net.forward(x)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(args.steps, 1)
+    a.record()
+    for _ in range(steps):
+        net.forward(x)
+    b.record()
+    torch.cuda.synchronize()
+    fwd_ms = a.elapsed_time(b) / steps
+    bs = 16384
+    for _ in range(3):
+        net.train_step(x[:bs], d[:bs], w[:bs], lr=1e-3)
+    torch.cuda.synchronize()
+    a.record()
+    for k in range(steps):
+        o = (k * bs) % (n - bs)
+        net.train_step(x[o:o + bs], d[o:o + bs], w[o:o + bs], lr=1e-3)
+    b.record()
+    torch.cuda.synchronize()
+    train_ms = a.elapsed_time(b) / steps
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    ach = flop * n / (fwd_ms * 1e-3) / 1e12
+    print(json.dumps({"metric": "MLP forward samples/s", "value": round(n / (fwd_ms * 1e-3) / 1e9, 3),
+                      "unit": "G samples/s", "n_gpus": 1, "steps": steps, "higher_is_better": True,
+                      "dtype": "bf16 (fp32 accumulate)", "data": "synthetic",
+                      "config": {"workload": f"mlp_forward_{n}_vertices", "batch": n, "train_batch": bs},
+                      "forward_ms": round(fwd_ms, 4), "train_step_ms": round(train_ms, 4),
+                      "roofline": {"bound": "tensor", "achieved": round(ach, 1), "peak": peak, "unit": "TFLOP/s",
+                                   "frac": round(ach / peak, 4), "peak_kind": "measured" if peaks else "fallback",
+                                   "instruction": "mma.sync.m16n8k16 bf16"}}))
+
+
 def main():
     args = parse()
-    if args.workload == "guided":
+    if args.workload == "mlp":
+        run_mlp(args)
+    elif args.workload == "guided":
         run_guided(args)
     elif args.workload == "serve":
         run_serve(args)

@@ -284,8 +284,10 @@ struct Acts {  // training only: each layer's input (bf16), [n][width]
     __nv_bfloat16* x3;
 };
 
+constexpr int kFwdThreads = 256;  // 8 warps: two blocks per SM fit the 92 KB weight image each
+
 template <bool kStore>
-__global__ void __launch_bounds__(128) k_forward(const float* __restrict__ in, int64_t n, const __nv_bfloat16* img,
+__global__ void __launch_bounds__(kFwdThreads) k_forward(const float* __restrict__ in, int64_t n, const __nv_bfloat16* img,
                                                  const float* params, float* __restrict__ out, Acts acts) {
     extern __shared__ __align__(16) unsigned char smem[];
     load_image(img, params, smem);
@@ -544,8 +546,8 @@ namespace {
 
 using namespace cav::mlp;
 
-int fwd_grid(cav_ctx* ctx, int64_t n) {
-    int64_t want = (n + 63) / 64;  // 4 warps x 16 samples per block and pass
+int fwd_grid(cav_ctx* ctx, int64_t n, int threads) {
+    int64_t want = (n + (threads / 2) - 1) / (threads / 2);  // warps x 16 samples per block and pass
     return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->num_sms * 2));
 }
 
@@ -588,8 +590,9 @@ cav_status compute_grads(cav_mlp* m, const float* in, const float* dirs, const f
     cav_ctx* ctx = m->ctx;
     CAV_CUDA(ctx, cudaMemsetAsync(m->d_grads, 0, sizeof(float) * kParams, s));
     CAV_CUDA(ctx, cudaMemsetAsync(m->d_loss, 0, sizeof(float), s));
-    const int grid = fwd_grid(ctx, n);
-    k_forward<true><<<grid, 128, kSmemBytes, s>>>(in, n, m->d_img, m->d_params, m->out, m->acts);
+    k_forward<true><<<fwd_grid(ctx, n, kFwdThreads), kFwdThreads, kSmemBytes, s>>>(in, n, m->d_img, m->d_params, m->out,
+                                                                                  m->acts);
+    const int grid = fwd_grid(ctx, n, 128);
     k_loss<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m->out, dirs, w, n, m->dout, m->d_loss);
     k_backward<<<grid, 128, kSmemBytes, s>>>(m->dout, n, m->d_img, m->d_params, m->acts, m->grads);
     const int wg = (int)std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, (int64_t)ctx->num_sms * 4));
@@ -608,8 +611,8 @@ namespace cav {
 // Device entry for the guided integrator: forward pass over n inputs into out (n x 32).
 cav_status mlp_forward(cav_mlp* m, const float* in, int64_t n, float* out, cudaStream_t s) {
     if (n <= 0) return CAV_OK;
-    k_forward<false><<<fwd_grid(m->ctx, n), 128, kSmemBytes, s>>>(in, n, m->d_img, m->d_params, out,
-                                                                  cav::mlp::Acts{});
+    k_forward<false><<<fwd_grid(m->ctx, n, kFwdThreads), kFwdThreads, kSmemBytes, s>>>(in, n, m->d_img, m->d_params,
+                                                                                      out, cav::mlp::Acts{});
     CAV_CUDA(m->ctx, cudaGetLastError());
     return CAV_OK;
 }
