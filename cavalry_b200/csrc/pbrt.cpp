@@ -14,6 +14,8 @@
 //   materials Materials/{MatteMaterial,Plastic,Glass,Mirror}.h createFromParams defaults.
 #include "pbrt.h"
 
+#include <complex>
+
 #include "../../include/cavalry.h"
 
 #include <algorithm>
@@ -460,7 +462,7 @@ struct Parser {
             bool remap = p.has_string("remaproughness") ? p.str("remaproughness") == "true" : true;
             m.alpha_u = m.alpha_v = remap ? roughness_to_alpha(rough) : rough;
             m.eta = 1.5f;
-        } else if (type == "glass") {
+        } else if (type == "glass") {  // Materials/Glass.h: specular, or microfacet when rough
             m.type = kGlass;
             rgb(p, "Kr", m.kr);
             rgb(p, "Kt", m.kt);
@@ -468,12 +470,50 @@ struct Parser {
             float u = p.has_num("uroughness") ? p.num("uroughness") : 0.f;
             float v = p.has_num("vroughness") ? p.num("vroughness") : 0.f;
             if (p.has_num("roughness")) u = v = p.num("roughness");
-            if (u != 0.f || v != 0.f) throw ParseError("rough glass is not supported by this renderer (use roughness 0)");
+            bool remap = p.has_string("remaproughness") ? p.str("remaproughness") == "true" : true;
+            if (u != 0.f || v != 0.f) {  // perfectSpecular only when both are exactly 0
+                m.alpha_u = remap ? roughness_to_alpha(u) : u;
+                m.alpha_v = remap ? roughness_to_alpha(v) : v;
+            }
         } else if (type == "mirror") {
             m.type = kMirror;
             m.mirror_kr = p.has_num("Kr") ? p.num("Kr") : 0.9f;
+        } else if (type == "metal") {  // Materials/Metal.h
+            m.type = kMetal;
+            m.has_f0 = true;
+            m.f0[0] = 0.955f; m.f0[1] = 0.638f; m.f0[2] = 0.538f;  // the reference's copper f0
+            if (p.has_list("eta") && p.has_list("k")) {
+                const auto& e = p.list("eta");
+                const auto& k = p.list("k");
+                if (e.size() < 3 || k.size() < 3) throw ParseError("metal eta / k need 3 values");
+                for (int c = 0; c < 3; ++c) {  // |((eta - 1) + ik) / ((eta + 1) + ik)|^2
+                    std::complex<float> z((float)e[c], (float)k[c]), one(1.f, 0.f);
+                    m.f0[c] = (float)std::abs(std::pow((z - one) / (z + one), 2));
+                }
+            }
+            float u = p.has_num("uroughness") ? p.num("uroughness") : 0.1f;
+            float v = p.has_num("vroughness") ? p.num("vroughness") : 0.1f;
+            if (p.has_num("roughness")) u = v = p.num("roughness");
+            bool remap = p.has_string("remaproughness") ? p.str("remaproughness") == "true" : true;
+            m.alpha_u = remap ? roughness_to_alpha(u) : u;
+            m.alpha_v = remap ? roughness_to_alpha(v) : v;
+        } else if (type == "substrate") {  // Materials/Substrate.h: FresnelBlend
+            m.type = kSubstrate;
+            m.kd[0] = m.kd[1] = m.kd[2] = 0.5f;
+            m.ks[0] = m.ks[1] = m.ks[2] = 0.5f;
+            rgb(p, "Kd", m.kd);
+            rgb(p, "Ks", m.ks);
+            float u = p.has_num("uroughness") ? p.num("uroughness") : 0.1f;
+            float v = p.has_num("vroughness") ? p.num("vroughness") : 0.1f;
+            if (p.has_num("roughness")) u = v = p.num("roughness");
+            bool remap = p.has_string("remaproughness") ? p.str("remaproughness") == "true" : true;
+            m.alpha_u = remap ? roughness_to_alpha(u) : u;
+            m.alpha_v = remap ? roughness_to_alpha(v) : v;
         } else {
-            throw ParseError("unsupported material type: " + type);
+            // MaterialObject::createFromObjectDefinition falls back to matte for an unknown type
+            m.type = kMatte;
+            m.kd[0] = m.kd[1] = m.kd[2] = 1.f;
+            rgb(p, "Kd", m.kd);
         }
         return m;
     }

@@ -51,6 +51,8 @@ struct Material {
     float alpha_u = 0, alpha_v = 0;  // GGX alphas after the optional roughness remap
     float eta = 1.5f;
     float mirror_kr = 0.9f;
+    bool has_f0 = false;             // metal: Fresnel f0 from a complex IOR (or the copper default)
+    float f0[3] = {0, 0, 0};
 };
 
 struct Mesh {

@@ -277,7 +277,7 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
         r.mirror_kr = m.mirror_kr;
         for (int k = 0; k < 3; ++k) {  // Fresnel::createFromIOR (BSDFs/Fresnel.h:27-31), host float
             float t = (m.eta - 1.f) / (m.eta + 1.f);
-            r.f0[k] = t * t;
+            r.f0[k] = m.has_f0 ? m.f0[k] : t * t;  // metal: its complex-IOR (or copper) f0
         }
         mats.push_back(r);
     }

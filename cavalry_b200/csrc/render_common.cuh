@@ -201,7 +201,64 @@ struct Bsdf {
     f3 f0;          // Fresnel f0
     float eta;      // glass: aboveIOR = 1, belowIOR = eta
     float mirror;   // mirror reflectivity
-    __device__ bool is_delta() const { return type == cavpbrt::kGlass || type == cavpbrt::kMirror; }
+    __device__ bool is_delta() const {
+        return (type == cavpbrt::kGlass && !rough()) || type == cavpbrt::kMirror;
+    }
+    // Glass with a non-zero roughness uses MicrofacetBSDF with transmission (Materials/Glass.h)
+    __device__ bool rough() const { return ggx.ax != 0.f || ggx.ay != 0.f; }
+
+    // ---- FresnelBlend (substrate, BSDFs/Fresnel.h:65-150)
+    __device__ f3 fb_eval(f3 wi, f3 wo) const {
+        if (!same_hemisphere(wi, wo)) return mk(0, 0, 0);
+        const f3 one = mk(1, 1, 1);
+        f3 diffuse = (float)(28.f / (23.f * 3.14159265358979323846)) * kd * (one - ks) *
+                     (1 - pow5(1 - .5f * fabsf(wi.z))) * (1 - pow5(1 - .5f * fabsf(wo.z)));
+        f3 h = wi + wo;
+        if (h.x == 0 && h.y == 0 && h.z == 0) return mk(0, 0, 0);
+        h = normalize3(h);
+        f3 spec = ggx.D(h) * schlick(dot3(wi, h), ks) / (4 * fabsf(dot3(wi, h)) * fmaxf(fabsf(wi.z), fabsf(wo.z)));
+        return diffuse + spec;
+    }
+    __device__ float fb_pdf_h(f3 wi, f3 wo, f3 h) const {
+        return (1.f - 0.5f) * cosine_pdf(wi.z) + 0.5f * ggx.pdf(h, wo) / (4.f * dot3(wo, h));
+    }
+    __device__ float fb_pdf(f3 wi, f3 wo) const { return fb_pdf_h(wi, wo, normalize3(wi + wo)); }
+
+    // ---- microfacet transmission (rough glass, BSDFs/Microfacet.h:50-160); eta = above/below
+    __device__ float mt_eta(f3 wo) const { return wo.z > 0 ? (1.f / eta) : (eta / 1.f); }
+    __device__ f3 mt_eval(f3 wi, f3 wo) const {
+        if (same_hemisphere(wi, wo)) return mk(0, 0, 0);
+        float co = fabsf(wo.z), ci = fabsf(wi.z);
+        if (ci == 0 || co == 0) return mk(0, 0, 0);
+        float e = mt_eta(wo);
+        f3 h = normalize3(wo + wi * e);
+        if (h.z < 0) h = neg(h);
+        if (dot3(wo, h) * dot3(wi, h) > 0) return mk(0, 0, 0);
+        f3 F = schlick(dot3(wo, h), f0);
+        float sd = dot3(wo, h) + e * dot3(wi, h);
+        return (mk(1, 1, 1) - F) * kt *
+               fabsf(ggx.D(h) * ggx.G(wo, wi) * e * e * fabsf(dot3(wi, h)) * fabsf(dot3(wo, h)) / (ci * co * sd * sd));
+    }
+    __device__ float mt_pdf(f3 wi, f3 wo) const {
+        float e = mt_eta(wo);
+        f3 h = normalize3(wo + wi * e);
+        if (same_hemisphere(wi, wo)) return 0;
+        if (dot3(wo, h) * dot3(wi, h) > 0) return 0;
+        float sd = dot3(wo, h) + e * dot3(wi, h);
+        float dwh = fabsf((e * e * dot3(wi, h)) / (sd * sd));
+        return ggx.pdf(h, wo) * dwh;
+    }
+    // the reflection lobe of MicrofacetBSDF: reflectionColor kr (rough glass) or 1 (metal)
+    __device__ f3 mr_eval(f3 wi, f3 wo, f3 color) const {
+        if (!same_hemisphere(wi, wo)) return mk(0, 0, 0);
+        float co = fabsf(wo.z), ci = fabsf(wi.z);
+        f3 h = wi + wo;
+        if (ci == 0 || co == 0) return mk(0, 0, 0);
+        if (h.x == 0 && h.y == 0 && h.z == 0) return mk(0, 0, 0);
+        h = normalize3(h);
+        f3 F = schlick(dot3(wo, h), f0);
+        return color * ggx.D(h) * ggx.G(wo, wi) * F / (4 * ci * co);
+    }
 
     // ---- Lambertian
     __device__ f3 lam_eval(f3 wi, f3 wo, f3 c) const { return same_hemisphere(wi, wo) ? c / kPi : mk(0, 0, 0); }
@@ -244,7 +301,10 @@ struct Bsdf {
             case cavpbrt::kMirror:
                 if (!(wi.x == -wo.x && wi.y == -wo.y && wi.z == wo.z)) return mk(0, 0, 0);
                 return mk(1, 1, 1) * mirror / fabsf(wi.z);
+            case cavpbrt::kMetal: return mr_eval(wi, wo, mk(1, 1, 1));
+            case cavpbrt::kSubstrate: return fb_eval(wi, wo);
             case cavpbrt::kGlass: {
+                if (rough()) return same_hemisphere(wi, wo) ? mr_eval(wi, wo, kr) : mt_eval(wi, wo);
                 if (same_hemisphere(wi, wo)) {
                     if (!(wi.x == -wo.x && wi.y == -wo.y && wi.z == wo.z)) return mk(0, 0, 0);
                     return kr * schlick(fabsf(wi.z), f0) / fabsf(wi.z);
@@ -265,7 +325,13 @@ struct Bsdf {
             case cavpbrt::kMatte: return cosine_pdf(wi.z);
             case cavpbrt::kPlastic: return 0.5f * cosine_pdf(wi.z) + (1.f - 0.5f) * mf_pdf(wi, wo);
             case cavpbrt::kMirror: return (wi.x == -wo.x && wi.y == -wo.y && wi.z == wo.z) ? 1.f : 0.f;
+            case cavpbrt::kMetal: return mf_pdf(wi, wo);
+            case cavpbrt::kSubstrate: return fb_pdf(wi, wo);
             case cavpbrt::kGlass: {
+                if (rough()) {
+                    const float p = glass_reflect_prob(wo);
+                    return same_hemisphere(wi, wo) ? p * mf_pdf(wi, wo) : (1.f - p) * mt_pdf(wi, wo);
+                }
                 if (same_hemisphere(wi, wo)) {
                     if (!(wi.x == -wo.x && wi.y == -wo.y && wi.z == wo.z)) return 0;
                     return glass_reflect_prob(wo);
@@ -309,8 +375,50 @@ struct Bsdf {
                 pdf_out = 1;
                 return eval(wi, wo);
             }
+            case cavpbrt::kMetal: {  // MicrofacetBSDF::sampleReflection: pdf from the sampled half vector
+                f3 h = ggx.sample(u0, u1, wo);
+                wi = 2.0f * h * dot3(h, wo) - wo;
+                pdf_out = ggx.pdf(h, wo) / (4.f * dot3(wo, h));
+                return mr_eval(wi, wo, mk(1, 1, 1));
+            }
+            case cavpbrt::kSubstrate: {  // FresnelBlendBSDF::sample
+                f3 h;
+                if (u0 < 0.5f) {
+                    u0 = u0 * (1.f / 0.5f);
+                    h = ggx.sample(u0, u1, wo);
+                    wi = 2.0f * h * dot3(h, wo) - wo;
+                    if (!same_hemisphere(wi, wo)) {
+                        pdf_out = 0.f;  // the reference returns without setting the pdf
+                        return mk(0, 0, 0);
+                    }
+                } else {
+                    u0 = (u0 - 0.5f) * (1.f / (1.f - 0.5f));
+                    wi = cosine_hemisphere(u0, u1);
+                    if (wo.z < 0) wi.z *= -1;
+                    h = normalize3(wi + wo);
+                }
+                pdf_out = fb_pdf_h(wi, wo, h);
+                return fb_eval(wi, wo);
+            }
             case cavpbrt::kGlass: {
                 float p = glass_reflect_prob(wo);
+                if (rough()) {  // MicrofacetBSDF::sample with transmission
+                    if (u0 < p) {
+                        u0 = u0 * (1.f / p);
+                        f3 h = ggx.sample(u0, u1, wo);
+                        wi = 2.0f * h * dot3(h, wo) - wo;
+                        pdf_out = ggx.pdf(h, wo) / (4.f * dot3(wo, h)) * p;
+                        return mr_eval(wi, wo, kr);
+                    }
+                    u0 = (u0 - p) * (1.f / (1.f - p));
+                    f3 h = ggx.sample(u0, u1, wo);
+                    if (!refract(wo, h, mt_eta(wo), wi)) {
+                        pdf_out = 0.f;  // the reference returns without setting the pdf
+                        return mk(0, 0, 0);
+                    }
+                    pdf_out = mt_pdf(wi, wo) * (1.f - p);
+                    return mt_eval(wi, wo);
+                }
                 if (u0 < p) {
                     wi = mk(-wo.x, -wo.y, wo.z);
                     pdf_out = 1 * p;

@@ -141,11 +141,12 @@ __device__ inline int cdf_sample(const float* cdf, int n, float u, float& prob) 
 }
 __device__ inline float cdf_pdf(const float* cdf, int i) { return i == 0 ? cdf[0] : cdf[i] - cdf[i - 1]; }
 
+// isAlmostDelta (BSDFs/MicrofacetDistribution.h:157-159) is overridden by MicrofacetBSDF
+// (metal, rough glass) and FresnelBlend (substrate): alpha_x < 0.05 or alpha_y < 0.05.
 __device__ inline bool almost_delta(const Bsdf& B) {
-    // isAlmostDelta is overridden only by microfacet-based BSDFs with their own lobe
-    // (MicrofacetBSDF, FresnelBlend); none of the built materials has one, so it is false.
-    (void)B;
-    return false;
+    const bool microfacet = B.type == cavpbrt::kMetal || B.type == cavpbrt::kSubstrate ||
+                            (B.type == cavpbrt::kGlass && B.rough());
+    return microfacet && (B.ggx.ax < 0.05f || B.ggx.ay < 0.05f);
 }
 
 // Hit geometry of extend slot j, recomputed where needed (Triangle::fillIntersectionInformation).

@@ -150,15 +150,18 @@ def _floats_text(a) -> str:
 
 def _material_line(mat) -> str:
     """pbrt Material directive of a scene material: a tuple is a matte Kd, a dict names
-    "type" (matte, plastic, glass, mirror) and its parameters."""
+    "type" (matte, plastic, glass, mirror, metal, substrate) and its parameters; a metal's
+    "eta" and "k" are rgb triples (complex index of refraction)."""
     if not isinstance(mat, dict):
         return f'Material "matte" "rgb Kd" [{_nums(mat)}]'
     t = mat["type"]
     parts = [f'Material "{t}"']
     for key, kind in (("Kd", "rgb"), ("Ks", "rgb"), ("Kr", "rgb"), ("Kt", "rgb"), ("roughness", "float"),
-                      ("eta", "float")):
+                      ("eta", "float"), ("k", "rgb")):
         if key in mat:
-            if t == "mirror" and key == "Kr":
+            if t == "metal" and key == "eta":
+                parts.append(f'"rgb eta" [{_nums(mat[key])}]')
+            elif t == "mirror" and key == "Kr":
                 parts.append(f'"float Kr" [{_num(mat[key])}]')
             else:
                 parts.append(f'"{kind} {key}" [{_nums(mat[key])}]')
@@ -255,8 +258,9 @@ def sphere_scene(n_spheres: int = 64, level: int = 6, seed: int = 3, room=(20.0,
     """Config-3 scene: `n_spheres` icospheres (20 * 4**level triangles each; 64 x level 6 =
     5,242,880), radii log-uniform in [0.05, 0.5], centres from 4 Gaussian clusters (sigma 1.5)
     clipped into a W x H x D room (floor y = 0, centred in x and z); each sphere's material
-    uniform over `materials` (matte; plastic roughness 0.1; glass eta 1.5; mirror) with albedo
-    uniform in [0.1, 0.9]; `n_lights` 2 x 2 emissive quads under the ceiling facing down with
+    uniform over `materials` (matte; plastic roughness 0.1; glass eta 1.5; mirror; metal =
+    copper roughness 0.2; gold = metal with gold's complex index, roughness 0.05; substrate
+    Ks 0.3 roughness 0.15; roughglass = glass roughness 0.1) with albedo uniform in [0.1, 0.9]; `n_lights` 2 x 2 emissive quads under the ceiling facing down with
     radiance uniform in [10, 30].  Room walls are matte 0.73 grey, outward-facing normals in.
     Returns the scene dict of mini_room plus "lights" and "camera"."""
     rng = np.random.default_rng(seed)
@@ -298,6 +302,14 @@ def sphere_scene(n_spheres: int = 64, level: int = 6, seed: int = 3, room=(20.0,
             mat = {"type": "plastic", "Kd": alb, "roughness": 0.1}
         elif kind == "glass":
             mat = {"type": "glass", "eta": 1.5}
+        elif kind == "metal":
+            mat = {"type": "metal", "roughness": 0.2}
+        elif kind == "gold":
+            mat = {"type": "metal", "eta": (0.143, 0.374, 1.442), "k": (3.983, 2.385, 1.603), "roughness": 0.05}
+        elif kind == "substrate":
+            mat = {"type": "substrate", "Kd": alb, "Ks": (0.3, 0.3, 0.3), "roughness": 0.15}
+        elif kind == "roughglass":
+            mat = {"type": "glass", "eta": 1.5, "roughness": 0.1}
         else:
             mat = {"type": "mirror"}
         add(uv * r + c, uf, f"sphere{k}", mat)

@@ -60,16 +60,18 @@ typedef struct {
     int32_t pad;
 } OMesh;
 typedef struct {
-    int32_t type; /* 0 matte, 1 mirror, 4 glass (specular), 5 plastic */
+    int32_t type; /* 0 matte, 1 mirror, 2 substrate, 3 metal, 4 glass (specular or rough), 5 plastic */
     float kd[3], ks[3], kr[3], kt[3];
     float alpha_u, alpha_v, eta, mirror_kr;
+    float f0[3];     /* metal: Fresnel f0 (complex IOR or copper) */
+    int32_t has_f0;
 } OMaterial;
 typedef struct {
     float L[3];
     int32_t mesh;
 } OLight;
 
-enum { M_MATTE = 0, M_MIRROR = 1, M_GLASS = 4, M_PLASTIC = 5 };
+enum { M_MATTE = 0, M_MIRROR = 1, M_SUBSTRATE = 2, M_METAL = 3, M_GLASS = 4, M_PLASTIC = 5 };
 
 /* ------------------------------------------------------------------ vectors */
 typedef struct { float x, y, z; } V3;
@@ -285,7 +287,7 @@ static Bsdf make_bsdf(const OMaterial* m) {
     b.g.ay = m->alpha_v;
     V3 e = v3(m->eta, m->eta, m->eta);
     V3 t = v3((e.x - 1) / (e.x + 1), (e.y - 1) / (e.y + 1), (e.z - 1) / (e.z + 1));
-    b.f0 = vmul(t, t);
+    b.f0 = m->has_f0 ? ld3(m->f0) : vmul(t, t);
     b.eta = m->eta;
     b.mirror = m->mirror_kr;
     return b;
@@ -301,7 +303,7 @@ static V3 mf_eval(const Bsdf* b, V3 wi, V3 wo) {
     if (vzero(h)) return v3(0, 0, 0);
     h = vnorm(h);
     V3 F = schlick(vdot(wo, h), b->f0);
-    return vdivs(vmul(vs(b->ks, ggx_D(b->g, h) * ggx_G(b->g, wo, wi)), F), 4 * ci * co);
+    return vdivs(vmul(vs(vs(b->ks, ggx_D(b->g, h)), ggx_G(b->g, wo, wi)), F), 4 * ci * co);
 }
 static float mf_pdf(const Bsdf* b, V3 wi, V3 wo) {
     V3 h = vnorm(vadd(wi, wo));
@@ -322,6 +324,60 @@ static float glass_reflect_prob(const Bsdf* b, V3 wo) {
     else if (vzero(b->kt)) p = 1;
     return p;
 }
+static int rough(const Bsdf* b) { return b->g.ax != 0.f || b->g.ay != 0.f; }
+/* MicrofacetBSDF reflection lobe (BSDFs/Microfacet.h:25-40) with the given reflection colour */
+static V3 mr_eval(const Bsdf* b, V3 wi, V3 wo, V3 color) {
+    if (!same_hemi(wi, wo)) return v3(0, 0, 0);
+    float co = fabsf(wo.z), ci = fabsf(wi.z);
+    V3 h = vadd(wi, wo);
+    if (ci == 0 || co == 0) return v3(0, 0, 0);
+    if (vzero(h)) return v3(0, 0, 0);
+    h = vnorm(h);
+    V3 F = schlick(vdot(wo, h), b->f0);
+    return vdivs(vmul(vs(vs(color, ggx_D(b->g, h)), ggx_G(b->g, wo, wi)), F), 4 * ci * co);
+}
+static float mt_eta(const Bsdf* b, V3 wo) { return wo.z > 0 ? (1.f / b->eta) : (b->eta / 1.f); }
+/* MicrofacetBSDF transmission (BSDFs/Microfacet.h:42-62, :118-150) */
+static V3 mt_eval(const Bsdf* b, V3 wi, V3 wo) {
+    if (same_hemi(wi, wo)) return v3(0, 0, 0);
+    float co = fabsf(wo.z), ci = fabsf(wi.z);
+    if (ci == 0 || co == 0) return v3(0, 0, 0);
+    float e = mt_eta(b, wo);
+    V3 h = vnorm(vadd(wo, vs(wi, e)));
+    if (h.z < 0) h = vs(h, -1.f);
+    if (vdot(wo, h) * vdot(wi, h) > 0) return v3(0, 0, 0);
+    V3 F = schlick(vdot(wo, h), b->f0);
+    float sd = vdot(wo, h) + e * vdot(wi, h);
+    float m = fabsf(ggx_D(b->g, h) * ggx_G(b->g, wo, wi) * e * e * fabsf(vdot(wi, h)) * fabsf(vdot(wo, h)) /
+                    (ci * co * sd * sd));
+    return vs(vmul(vsub(v3(1, 1, 1), F), b->kt), m);
+}
+static float mt_pdf(const Bsdf* b, V3 wi, V3 wo) {
+    float e = mt_eta(b, wo);
+    V3 h = vnorm(vadd(wo, vs(wi, e)));
+    if (same_hemi(wi, wo)) return 0;
+    if (vdot(wo, h) * vdot(wi, h) > 0) return 0;
+    float sd = vdot(wo, h) + e * vdot(wi, h);
+    return ggx_pdf(b->g, h, wo) * fabsf((e * e * vdot(wi, h)) / (sd * sd));
+}
+/* FresnelBlendBSDF (BSDFs/Fresnel.h:65-150) */
+static V3 fb_eval(const Bsdf* b, V3 wi, V3 wo) {
+    if (!same_hemi(wi, wo)) return v3(0, 0, 0);
+    V3 one = v3(1, 1, 1);
+    V3 diffuse = vs(vs(vmul(vs(b->kd, (float)(28.f / (23.f * M_PI))), vsub(one, b->ks)),
+                       1 - pow5f(1 - .5f * fabsf(wi.z))),
+                    1 - pow5f(1 - .5f * fabsf(wo.z)));
+    V3 h = vadd(wi, wo);
+    if (vzero(h)) return v3(0, 0, 0);
+    h = vnorm(h);
+    V3 spec = vdivs(vs(schlick(vdot(wi, h), b->ks), ggx_D(b->g, h)),
+                    4 * fabsf(vdot(wi, h)) * fmaxf(fabsf(wi.z), fabsf(wo.z)));
+    return vadd(diffuse, spec);
+}
+static float fb_pdf_h(const Bsdf* b, V3 wi, V3 wo, V3 h) {
+    return (1.f - 0.5f) * cosine_pdf(wi) + 0.5f * ggx_pdf(b->g, h, wo) / (4.f * vdot(wo, h));
+}
+
 static V3 bsdf_eval(const Bsdf* b, V3 wi, V3 wo) {
     switch (b->type) {
         case M_MATTE: return lam_eval(wi, wo, b->kd);
@@ -329,7 +385,10 @@ static V3 bsdf_eval(const Bsdf* b, V3 wi, V3 wo) {
         case M_MIRROR:
             if (!is_mirror_dir(wi, wo)) return v3(0, 0, 0);
             return vdivs(vs(v3(1, 1, 1), b->mirror), fabsf(wi.z));
+        case M_METAL: return mr_eval(b, wi, wo, v3(1, 1, 1));
+        case M_SUBSTRATE: return fb_eval(b, wi, wo);
         case M_GLASS: {
+            if (rough(b)) return same_hemi(wi, wo) ? mr_eval(b, wi, wo, b->kr) : mt_eval(b, wi, wo);
             if (same_hemi(wi, wo)) {
                 if (!is_mirror_dir(wi, wo)) return v3(0, 0, 0);
                 return vdivs(vmul(b->kr, schlick(fabsf(wi.z), b->f0)), fabsf(wi.z));
@@ -348,7 +407,13 @@ static float bsdf_pdf(const Bsdf* b, V3 wi, V3 wo) {
         case M_MATTE: return cosine_pdf(wi);
         case M_PLASTIC: return 0.5f * cosine_pdf(wi) + (1.f - 0.5f) * mf_pdf(b, wi, wo);
         case M_MIRROR: return is_mirror_dir(wi, wo) ? 1.f : 0.f;
+        case M_METAL: return mf_pdf(b, wi, wo);
+        case M_SUBSTRATE: return fb_pdf_h(b, wi, wo, vnorm(vadd(wi, wo)));
         case M_GLASS: {
+            if (rough(b)) {
+                float p = glass_reflect_prob(b, wo);
+                return same_hemi(wi, wo) ? p * mf_pdf(b, wi, wo) : (1.f - p) * mt_pdf(b, wi, wo);
+            }
             if (same_hemi(wi, wo)) return is_mirror_dir(wi, wo) ? glass_reflect_prob(b, wo) : 0.f;
             float e = wo.z > 0 ? (1.f / b->eta) : (b->eta / 1.f);
             V3 n = v3(0, 0, wo.z < 0 ? -1.f : 1.f), r;
@@ -383,8 +448,50 @@ static V3 bsdf_sample(const Bsdf* b, float u0, float u1, V3 wo, V3* wi, float* p
             wi->z = wo.z;
             *pdf = 1;
             return bsdf_eval(b, *wi, wo);
+        case M_METAL: {
+            V3 h = ggx_sample(b->g, u0, u1, wo);
+            *wi = vsub(vs(vs(h, 2.0f), vdot(h, wo)), wo);
+            *pdf = ggx_pdf(b->g, h, wo) / (4.f * vdot(wo, h));
+            return mr_eval(b, *wi, wo, v3(1, 1, 1));
+        }
+        case M_SUBSTRATE: {
+            V3 h;
+            if (u0 < 0.5f) {
+                u0 = u0 * (1.f / 0.5f);
+                h = ggx_sample(b->g, u0, u1, wo);
+                *wi = vsub(vs(vs(h, 2.0f), vdot(h, wo)), wo);
+                if (!same_hemi(*wi, wo)) {
+                    *pdf = 0;
+                    return v3(0, 0, 0);
+                }
+            } else {
+                u0 = (u0 - 0.5f) * (1.f / (1.f - 0.5f));
+                *wi = cosine_hemisphere(u0, u1);
+                if (wo.z < 0) wi->z *= -1;
+                h = vnorm(vadd(*wi, wo));
+            }
+            *pdf = fb_pdf_h(b, *wi, wo, h);
+            return fb_eval(b, *wi, wo);
+        }
         case M_GLASS: {
             float p = glass_reflect_prob(b, wo);
+            if (rough(b)) {
+                if (u0 < p) {
+                    u0 = u0 * (1.f / p);
+                    V3 h = ggx_sample(b->g, u0, u1, wo);
+                    *wi = vsub(vs(vs(h, 2.0f), vdot(h, wo)), wo);
+                    *pdf = ggx_pdf(b->g, h, wo) / (4.f * vdot(wo, h)) * p;
+                    return mr_eval(b, *wi, wo, b->kr);
+                }
+                u0 = (u0 - p) * (1.f / (1.f - p));
+                V3 h = ggx_sample(b->g, u0, u1, wo);
+                if (!refract_dir(wo, h, mt_eta(b, wo), wi)) {
+                    *pdf = 0;
+                    return v3(0, 0, 0);
+                }
+                *pdf = mt_pdf(b, *wi, wo) * (1.f - p);
+                return mt_eval(b, *wi, wo);
+            }
             if (u0 < p) {
                 *wi = v3(-wo.x, -wo.y, wo.z);
                 *pdf = 1 * p;
@@ -405,7 +512,7 @@ static V3 bsdf_sample(const Bsdf* b, float u0, float u1, V3 wo, V3* wi, float* p
     *pdf = 0;
     return v3(0, 0, 0);
 }
-static int bsdf_delta(const Bsdf* b) { return b->type == M_GLASS || b->type == M_MIRROR; }
+static int bsdf_delta(const Bsdf* b) { return (b->type == M_GLASS && !rough(b)) || b->type == M_MIRROR; }
 static float mis_power(float a, float b) {
     a *= a;
     b *= b;

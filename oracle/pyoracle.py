@@ -240,9 +240,9 @@ OMESH_DTYPE = np.dtype([("first_tri", "<i4"), ("tri_count", "<i4"), ("has_normal
                         ("material", "<i4"), ("light", "<i4"), ("area", "<f4"), ("pad", "<i4")])
 OMAT_DTYPE = np.dtype([("type", "<i4"), ("kd", "<f4", (3,)), ("ks", "<f4", (3,)), ("kr", "<f4", (3,)),
                        ("kt", "<f4", (3,)), ("alpha_u", "<f4"), ("alpha_v", "<f4"), ("eta", "<f4"),
-                       ("mirror_kr", "<f4")])
+                       ("mirror_kr", "<f4"), ("f0", "<f4", (3,)), ("has_f0", "<i4")])
 OLIGHT_DTYPE = np.dtype([("L", "<f4", (3,)), ("mesh", "<i4")])
-MATERIAL_TYPES = {"matte": 0, "mirror": 1, "glass": 4, "plastic": 5}
+MATERIAL_TYPES = {"matte": 0, "mirror": 1, "substrate": 2, "metal": 3, "glass": 4, "plastic": 5}
 
 
 def _pt_lib():
@@ -282,10 +282,31 @@ def material_record(mat) -> np.void:
         a = roughness_to_alpha(r) if mat.get("remaproughness", True) else r
         m["alpha_u"] = m["alpha_v"] = a
     elif t == "glass":
-        assert float(mat.get("roughness", 0.0)) == 0.0, "only specular glass is restated"
         m["kr"] = mat.get("Kr", (1, 1, 1))
         m["kt"] = mat.get("Kt", (1, 1, 1))
         m["eta"] = mat.get("eta", 1.5)
+        r = float(mat.get("roughness", 0.0))
+        if r != 0.0:
+            a = roughness_to_alpha(r) if mat.get("remaproughness", True) else r
+            m["alpha_u"] = m["alpha_v"] = a
+    elif t == "metal":
+        m["has_f0"] = 1
+        f0 = np.array([0.955, 0.638, 0.538], np.float32)
+        if "eta" in mat and "k" in mat:  # |((eta - 1) + ik) / ((eta + 1) + ik)|^2, complex<float> as the parser
+            for c in range(3):
+                z = np.complex64(complex(mat["eta"][c], mat["k"][c]))
+                one = np.complex64(1)
+                f0[c] = np.float32(abs(((z - one) / (z + one)) ** 2))
+        m["f0"] = f0
+        r = float(mat.get("roughness", 0.1))
+        a = roughness_to_alpha(r) if mat.get("remaproughness", True) else r
+        m["alpha_u"] = m["alpha_v"] = a
+    elif t == "substrate":
+        m["kd"] = mat.get("Kd", (0.5, 0.5, 0.5))
+        m["ks"] = mat.get("Ks", (0.5, 0.5, 0.5))
+        r = float(mat.get("roughness", 0.1))
+        a = roughness_to_alpha(r) if mat.get("remaproughness", True) else r
+        m["alpha_u"] = m["alpha_v"] = a
     elif t == "mirror":
         m["mirror_kr"] = mat.get("Kr", 0.9)
     return m

@@ -34,9 +34,19 @@ CASES = [
      dict(width=128, height=96, spp=8, max_depth=8)),
     ("spheres_plastic", {"kind": "spheres", "n_spheres": 10, "level": 3, "seed": 8, "materials": ["plastic"]},
      dict(width=128, height=96, spp=8, max_depth=8)),
+    ("spheres_metal", {"kind": "spheres", "n_spheres": 10, "level": 3, "seed": 11, "materials": ["metal", "gold"]},
+     dict(width=128, height=96, spp=8, max_depth=8)),
+    ("spheres_substrate", {"kind": "spheres", "n_spheres": 10, "level": 3, "seed": 12, "materials": ["substrate"]},
+     dict(width=128, height=96, spp=8, max_depth=8)),
+    ("spheres_roughglass", {"kind": "spheres", "n_spheres": 10, "level": 3, "seed": 15,
+                            "materials": ["roughglass"]},
+     dict(width=128, height=96, spp=8, max_depth=8)),
     # the learning integrator (the .pbrt names it; both renderers read the Integrator line)
     ("room_rlpath_s16", {"kind": "room"}, dict(width=128, height=128, spp=16, max_depth=5, integrator="rlpath")),
     ("spheres_rlpath_s16", {"kind": "spheres", "n_spheres": 12, "level": 3, "seed": 5},
+     dict(width=128, height=96, spp=16, max_depth=8, integrator="rlpath")),
+    ("spheres_rough_rlpath_s16", {"kind": "spheres", "n_spheres": 12, "level": 3, "seed": 14,
+                                  "materials": ["metal", "gold", "substrate", "roughglass"]},
      dict(width=128, height=96, spp=16, max_depth=8, integrator="rlpath")),
 ]
 
@@ -52,10 +62,22 @@ def make_scene(gen: dict) -> dict:
 
 
 def main(out: str):
+    """Renders every case with the reference CLI; a case already in `out` with the same
+    scene and render settings keeps its image (the renders take minutes on a GPU)."""
     arrays = {}
     meta = []
+    old = {}
+    if Path(out).exists():
+        g = np.load(out)
+        old = {c["name"]: (c, g[c["name"]]) for c in json.loads(str(g["meta"]))}
     with tempfile.TemporaryDirectory() as tmp:
         for name, gen, rk in CASES:
+            entry = {"name": name, "gen": gen, "render": rk}
+            if name in old and json.dumps(old[name][0], sort_keys=True) == json.dumps(entry, sort_keys=True):
+                arrays[name] = old[name][1]
+                meta.append(entry)
+                print(name, "kept", flush=True)
+                continue
             pbrt = Path(tmp) / f"{name}.pbrt"
             scenes.write_pbrt(pbrt, make_scene(gen), **rk)
             img, _ = ref_cli.render(str(pbrt), str(Path(tmp) / f"{name}.png"), spp=rk["spp"],

@@ -185,3 +185,24 @@ def test_sphere_scene_sizes():
     sc = scenes.sphere_scene(4, 2, seed=1)
     assert len(sc["indices"]) == 12 + 4 * 320 + 3 * 2
     assert len(sc["lights"]) == 3
+
+
+def test_golden_sphere_scenes_have_disjoint_lights():
+    """The generator places light quads in one plane under the ceiling; two that overlap make
+    a shadow ray end inside both, so its visibility turns on the last bit of `t < limit` and
+    no two renderers agree there.  Every golden case keeps its quads apart."""
+    import make_render_golden
+
+    for name, gen, _ in make_render_golden.CASES:
+        if gen["kind"] != "spheres":
+            continue
+        sc = make_scene(gen)
+        boxes = []
+        for mid, _ in sc["lights"]:
+            _, first, n, _ = sc["meshes"][mid]
+            p = sc["positions"][np.unique(sc["indices"][first:first + n])]
+            boxes.append((p[:, 0].min(), p[:, 0].max(), p[:, 2].min(), p[:, 2].max()))
+        for i in range(len(boxes)):
+            for j in range(i + 1, len(boxes)):
+                a, b = boxes[i], boxes[j]
+                assert not (a[0] < b[1] and b[0] < a[1] and a[2] < b[3] and b[2] < a[3]), (name, i, j)
