@@ -603,56 +603,6 @@ __global__ void __launch_bounds__(kThreads) k_tnode_layout(const BNode* __restri
     out[c] = t;
 }
 
-// The 4-wide view: wide node x gathers the children of binary node x's internal children
-// (and its triangle children directly).
-__global__ void __launch_bounds__(kThreads) k_wide_layout(const TNode* __restrict__ tn, int64_t nt,
-                                                          WNode* __restrict__ out) {
-    const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= nt) return;
-    float box[4][6];
-    int32_t ref[4];
-    int k = 0;
-    auto child = [&](const TNode& t, int side, float (&b)[6], int32_t& r) {
-        if (side == 0) {
-            b[0] = t.a.x; b[1] = t.a.y; b[2] = t.a.z; b[3] = t.a.w; b[4] = t.b.x; b[5] = t.b.y;
-            r = t.d.x;
-        } else {
-            b[0] = t.b.z; b[1] = t.b.w; b[2] = t.c.x; b[3] = t.c.y; b[4] = t.c.z; b[5] = t.c.w;
-            r = t.d.y;
-        }
-    };
-    const TNode t = tn[x];
-    for (int side = 0; side < 2; ++side) {
-        float b[6];
-        int32_t r;
-        child(t, side, b, r);
-        if (r >= 0) {  // internal child: its two children join this wide node
-            const TNode c = tn[r];
-            for (int cs = 0; cs < 2; ++cs) {
-                child(c, cs, box[k], ref[k]);
-                ++k;
-            }
-        } else {
-            for (int q = 0; q < 6; ++q) box[k][q] = b[q];
-            ref[k] = r;
-            ++k;
-        }
-    }
-    WNode w;
-    for (int q = 0; q < 4; ++q) {
-        const bool used = q < k;
-        w.lox[q] = used ? box[q][0] : 0.f;
-        w.loy[q] = used ? box[q][1] : 0.f;
-        w.loz[q] = used ? box[q][2] : 0.f;
-        w.hix[q] = used ? box[q][3] : 0.f;
-        w.hiy[q] = used ? box[q][4] : 0.f;
-        w.hiz[q] = used ? box[q][5] : 0.f;
-        w.ref[q] = used ? ref[q] : kWideEmpty;
-        w.pad[q] = 0;
-    }
-    out[x] = w;
-}
-
 __global__ void k_merge_error(const int* src, int* dst) {
     if (threadIdx.x == 0 && src[0] != 0) atomicExch(dst, src[0]);
 }
@@ -678,7 +628,6 @@ cav_status alloc_bvh(cav_ctx* ctx, int64_t n, cav_bvh** out) {
     need += 2 * (sizeof(uint64_t) * n + 256);
     need += sizeof(int32_t) * n + 256;
     need += sizeof(TNode) * (n - 1) + 256;
-    need += sizeof(WNode) * (n - 1) + 256;
     need += sizeof(TriRec) * n + 256;
     need += 64 + 256;
     if (cudaMalloc(&bvh->arena, need) != cudaSuccess) {
@@ -692,7 +641,6 @@ cav_status alloc_bvh(cav_ctx* ctx, int64_t n, cav_bvh** out) {
     bvh->codes_sorted = carve<uint64_t>(p, n);
     bvh->perm = carve<int32_t>(p, n);
     bvh->tnodes = carve<TNode>(p, n - 1);
-    bvh->wnodes = carve<WNode>(p, n - 1);
     bvh->tris = carve<TriRec>(p, n);
     bvh->d_root_box = carve<float>(p, 8);
     bvh->d_depth = carve<int32_t>(p, 8);
@@ -812,7 +760,6 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     k_tri_layout<<<gb, kThreads, 0, s>>>(positions, indices, mesh_ids, vals_a, n, bvh->tris, slot_of);
     k_tnode_layout<<<div_up(count, kThreads), kThreads, 0, s>>>(bvh->nodes, count, compact, slot_of, bvh->tnodes,
                                                                 bvh->d_root_box);
-    k_wide_layout<<<div_up(n - 1, kThreads), kThreads, 0, s>>>(bvh->tnodes, n - 1, bvh->wnodes);
     cudaEventRecord(bvh->ev[6], s);
     CAV_CUDA(ctx, cudaGetLastError());
     k_merge_error<<<1, 32, 0, s>>>(err, ctx->d_error);
@@ -1137,7 +1084,6 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
                                                              slot_of);
         k_tnode_layout<<<div_up(count, kThreads), kThreads, 0, s>>>(b->nodes, count, compact, slot_of, b->tnodes,
                                                                     b->d_root_box);
-        k_wide_layout<<<div_up(n - 1, kThreads), kThreads, 0, s>>>(b->tnodes, n - 1, b->wnodes);
         cudaEventRecord(b->ev[6], s);
     }
     CAV_CUDA(ctx, cudaGetLastError());

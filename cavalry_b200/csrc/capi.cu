@@ -153,6 +153,7 @@ cav_status cav_bvh_free(cav_bvh* bvh) {
     cudaSetDevice(bvh->device);
     if (bvh->timed)
         for (int k = 0; k < 7; ++k) cudaEventDestroy(bvh->ev[k]);
+    cav::free_wide(bvh);
     cudaFree(bvh->arena);
     delete bvh;
     return CAV_OK;

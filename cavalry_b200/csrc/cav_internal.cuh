@@ -67,20 +67,25 @@ struct __align__(64) TNode {
 };
 static_assert(sizeof(TNode) == 64, "TNode must be 64 bytes");
 
-// 4-wide traversal node (128 bytes) of the fast mode: one per binary traversal node, whose
-// children are that node's grandchildren (a triangle child stays a direct child), so a
-// walk from the root visits every other binary level.  Child boxes are stored per axis for
-// 32-byte vector loads; ref >= 0 is another wide node (binary index), ~slot a triangle,
-// kWideEmpty an unused slot.
-constexpr int32_t kWideEmpty = INT32_MIN;
-struct __align__(128) WNode {
-    float lox[4], loy[4];
-    float loz[4], hix[4];
-    float hiy[4], hiz[4];
-    int32_t ref[4];
-    int32_t pad[4];
+// Compressed 8-wide traversal node (80 bytes) of the fast mode, after Ylitie, Karras and
+// Laine, "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs" (HPG
+// 2017).  Child boxes are 8-bit offsets on a per-node grid: plane = p + q * 2^(e - 127) per
+// axis, rounded outward when quantised.  Internal children are stored contiguously from
+// child_base in slot order (imask bit s = slot s holds an internal child); triangle children
+// contiguously from tri_base.  meta[s]: 0 = empty slot; 0x20 | (24 + s) = internal child;
+// 0x20 | k = triangle tri_base + k.  A child's slot is chosen so that the slot number's bits
+// give the side of the node's centre it lies on (bit 2: +x, bit 1: +y, bit 0: +z), which lets
+// a ray visit children near-first by its direction octant alone.
+struct __align__(16) CNode {
+    float px, py, pz;
+    uint32_t e_imask;  // biased exponents x | y << 8 | z << 16, imask << 24
+    uint32_t child_base, tri_base;
+    uint32_t meta[2];  // slots 0-3, 4-7 (one byte each)
+    uint32_t qlo_x[2], qlo_y[2];
+    uint32_t qlo_z[2], qhi_x[2];
+    uint32_t qhi_y[2], qhi_z[2];
 };
-static_assert(sizeof(WNode) == 128, "WNode must be 128 bytes");
+static_assert(sizeof(CNode) == 80, "CNode must be 80 bytes");
 
 // Triangle record (48 bytes) in sorted (Morton) order: v0, e1 = v1-v0, e2 = v2-v0
 // (the same subtractions as Core/Triangle.h:180-183), triangle id and mesh id.
@@ -126,7 +131,10 @@ struct cav_bvh {
     int32_t* perm = nullptr;             // N: sorted position -> triangle id
     // traversal layout
     cav::TNode* tnodes = nullptr;  // N-1
-    cav::WNode* wnodes = nullptr;  // N-1: the 4-wide view for CAV_TRACE_FAST
+    // compressed 8-wide view for CAV_TRACE_FAST, built on first use (wide.cu)
+    mutable cav::CNode* cnodes = nullptr;
+    mutable cav::TriRec* ctris = nullptr;  // triangles in wide-leaf order
+    mutable void* wide_arena = nullptr;
     cav::TriRec* tris = nullptr;   // N
     float root_box[6];             // copied to the host at build time? no: device copy
     float* d_root_box = nullptr;   // 6 floats on device
@@ -178,6 +186,17 @@ cav_status trace_closest_dev(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* ra
 cav_status trace_any_dev(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,
                          const int32_t* excl, const uint32_t* n_dev, uint8_t* occ, cudaStream_t s,
                          unsigned long long* counter);
+
+// Compressed 8-wide fast mode (wide.cu): the layout is built on the stream at first use.
+cav_status ensure_wide(cav_ctx* ctx, const cav_bvh* bvh, cudaStream_t s);
+// stats (2 counters: node visits, triangle tests), when given, selects the instrumented variant
+cav_status trace_wide_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n,
+                              const uint32_t* n_dev, int32_t* prim, float* t, float* uv, cudaStream_t s,
+                              unsigned long long* counter, unsigned long long* stats = nullptr);
+cav_status trace_wide_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,
+                          const int32_t* excl, int64_t n, const uint32_t* n_dev, uint8_t* occ, cudaStream_t s,
+                          unsigned long long* counter, unsigned long long* stats = nullptr);
+void free_wide(cav_bvh* bvh);
 
 // Many scenes' BVHs, one launch per LBVH stage across all of them (build.cu)
 cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, const int64_t* num_vertices,

@@ -14,7 +14,7 @@
 
 #include <cfloat>
 
-#include "cav_internal.cuh"
+#include "trace_common.cuh"
 
 namespace cav {
 
@@ -28,9 +28,6 @@ constexpr int kStack = 128;
 // The short stack is used only for trees whose depth is known to fit: a traversal holds at
 // most one deferred sibling per level, so depth + 1 entries always suffice.
 constexpr int kShortStack = 64;
-constexpr uint32_t kMaxSteps = 1u << 22;  // node+triangle visits per ray before the ray is flagged
-constexpr int kDefaultRefill = 4;         // idle lanes that trigger a warp's next claim
-constexpr unsigned kFull = 0xffffffffu;
 
 __device__ inline float imax_f(float a, float b) { return __int_as_float(max(__float_as_int(a), __float_as_int(b))); }
 __device__ inline float imin_f(float a, float b) { return __int_as_float(min(__float_as_int(a), __float_as_int(b))); }
@@ -46,24 +43,6 @@ __device__ inline float slab(float lx, float ly, float lz, float hx, float hy, f
         if (minmax > 0) return fmaxf(0.f, maxmin);
     }
     return -1.f;
-}
-
-// rayTriangleIntersection (Core/Triangle.h:7-57) on precomputed edges.
-__device__ inline bool tri_test(const f3& o, const f3& d, const f3& v0, const f3& e1, const f3& e2, float& t, float& u,
-                                float& v) {
-    f3 tvec = o - v0;
-    f3 pvec = cross3(d, e2);
-    float det = dot3(e1, pvec);
-    if (det == 0) return false;
-    det = 1.f / det;
-    u = dot3(tvec, pvec) * det;
-    if (u < 0.0f || u > 1.0f) return false;
-    f3 qvec = cross3(tvec, e1);
-    v = dot3(d, qvec) * det;
-    if (v < 0.0f || (u + v) > 1.0f) return false;
-    t = dot3(e2, qvec) * det;
-    if (t <= 0.f) return false;
-    return true;
 }
 
 // One 64-byte node as two 256-bit read-only loads (sm_100 vector width): each load is one
@@ -85,16 +64,6 @@ __device__ __forceinline__ void load_node(const TNode* __restrict__ nodes, int32
     ld_nc_v8(p + 8, nr.hi);
 }
 
-__device__ inline void load_tri(const TriRec* __restrict__ tris, int slot, f3& v0, f3& e1, f3& e2, int& id, int& mesh) {
-    const float4* p = reinterpret_cast<const float4*>(tris + slot);
-    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
-    v0 = mk(a.x, a.y, a.z);
-    id = __float_as_int(a.w);
-    e1 = mk(b.x, b.y, b.z);
-    mesh = __float_as_int(b.w);
-    e2 = mk(c.x, c.y, c.z);
-}
-
 // ---------------------------------------------------------------- kernels
 // Persistent warps with per-lane ray replacement: every lane owns one ray at a time and
 // advances it by one node or one triangle per iteration.  When at least `refill` lanes of a
@@ -102,39 +71,6 @@ __device__ inline void load_tri(const TriRec* __restrict__ tris, int slot, f3& v
 // with one atomic, so lanes whose rays finish early do not wait for the warp's slowest ray.
 // Each ray is still traversed exactly as the reference does; only the assignment of rays
 // to lanes changes.
-struct TraceStats {
-    uint32_t nodes = 0, tris = 0;
-};
-
-template <bool kStats>
-__device__ inline void flush_stats(const TraceStats& st, unsigned long long* stats) {
-    if (!kStats) return;
-    unsigned long long a = st.nodes, b = st.tris;
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) {
-        a += __shfl_down_sync(kFull, a, o);
-        b += __shfl_down_sync(kFull, b, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(stats, a);
-        atomicAdd(stats + 1, b);
-    }
-}
-
-// Claims new rays for the idle lanes of the warp.  Returns the claimed index for this lane
-// (or -1) and clears `more` once the counter passed n.
-__device__ inline int64_t claim(unsigned idle, unsigned long long* counter, int64_t n, bool& more) {
-    const int lane = threadIdx.x & 31;
-    const int cnt = __popc(idle);
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(counter, (unsigned long long)cnt);
-    base = __shfl_sync(kFull, base, 0);
-    if (base + (unsigned long long)cnt >= (unsigned long long)n) more = false;
-    if (!((idle >> lane) & 1u)) return -1;
-    int64_t my = (int64_t)base + __popc(idle & ((1u << lane) - 1u));
-    return my < n ? my : -1;
-}
-
 // Segments: one traversal launch over the rays of several jobs, each with its own BVH and
 // output arrays.  A lane that claims global ray g finds its segment by binary search over
 // the segment starts (staged in shared memory) and switches to that segment's tree.
@@ -411,193 +347,6 @@ __global__ void k_any(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg,
 }
 
 // ------------------------------------------------------------------ fast mode (4-wide)
-// The same persistent warps and lane refill, over the 4-wide view (WNode): a node visit
-// tests up to four child boxes, continues with the nearest hit and pushes the others far
-// to near with their entry distances; entries farther than the current hit are dropped when
-// popped.  Hit distances are exact (the same triangle test); only equal-distance ties may
-// resolve to a different triangle than the reference order.
-__device__ __forceinline__ void load_wide(const WNode* __restrict__ w, int32_t ref, float (&a)[8], float (&b)[8],
-                                          float (&c)[8], int4& r) {
-    const float* p = reinterpret_cast<const float*>(w + ref);
-    ld_nc_v8(p, a);       // lox, loy
-    ld_nc_v8(p + 8, b);   // loz, hix
-    ld_nc_v8(p + 16, c);  // hiy, hiz
-    r = __ldg(reinterpret_cast<const int4*>(p + 24));
-}
-
-// insertion of (ref, dist) into a small ascending list
-__device__ __forceinline__ void ins4(int32_t (&rr)[4], float (&dd)[4], int& m, int32_t r, float d) {
-    int k = m++;
-    while (k > 0 && dd[k - 1] > d) {
-        rr[k] = rr[k - 1];
-        dd[k] = dd[k - 1];
-        --k;
-    }
-    rr[k] = r;
-    dd[k] = d;
-}
-
-template <bool kAny>
-__global__ void k_trace_fast(const WNode* __restrict__ wn, const TriRec* __restrict__ tris, const float* root_box,
-                             const cav_ray* __restrict__ rays, int64_t n, const uint32_t* n_dev, int32_t* prim, float* tout,
-                             float* uv, const float* __restrict__ limit, const int32_t* __restrict__ excl, uint8_t* occ,
-                             unsigned long long* counter, int refill, int* flag) {
-    if (n_dev) n = *n_dev;
-    const float rb0 = root_box[0], rb1 = root_box[1], rb2 = root_box[2];
-    const float rb3 = root_box[3], rb4 = root_box[4], rb5 = root_box[5];
-    int32_t stack[kStack];
-    float sdist[kStack];
-    bool more = true;
-    int64_t ray = -1;
-    f3 o = mk(0, 0, 0), d = mk(0, 0, 0), inv = mk(0, 0, 0);
-    float tmax = 0.f, best = 0.f, bu = 0.f, bv = 0.f, lim = 0.f;
-    int32_t bid = -1, ref = 0, src = -1, dst = -1;
-    bool hit = false, use_limit = false;
-    int top = -1;
-    uint32_t steps = 0;
-    for (;;) {
-        const unsigned idle = __ballot_sync(kFull, ray < 0);
-        if (idle == kFull && !more) break;
-        if (more && idle != 0 && (__popc(idle) >= refill || idle == kFull)) {
-            int64_t r = claim(idle, counter, n, more);
-            if (r >= 0) {
-                const float4* rp = reinterpret_cast<const float4*>(rays + r);
-                float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
-                o = mk(r0.x, r0.y, r0.z);
-                d = mk(r1.x, r1.y, r1.z);
-                tmax = r1.w;
-                inv = mk(1.f / d.x, 1.f / d.y, 1.f / d.z);
-                hit = false;
-                best = FLT_MAX;
-                bu = bv = 0.f;
-                bid = -1;
-                top = -1;
-                ref = 0;
-                steps = 0;
-                ray = r;
-                if (kAny) {
-                    use_limit = limit != nullptr;
-                    lim = use_limit ? __ldg(limit + r) : 0.f;
-                    best = use_limit ? lim : FLT_MAX;
-                    src = dst = -1;
-                    if (excl) {
-                        int2 e = __ldg(reinterpret_cast<const int2*>(excl) + r);
-                        src = e.x;
-                        dst = e.y;
-                    }
-                } else if (!(slab(rb0, rb1, rb2, rb3, rb4, rb5, o, inv) >= 0.f)) {
-                    prim[r] = -1;
-                    if (tout) tout[r] = __int_as_float(0x7f800000);
-                    if (uv) reinterpret_cast<float2*>(uv)[r] = make_float2(0.f, 0.f);
-                    ray = -1;
-                }
-            }
-        }
-        if (ray < 0) continue;
-        bool pop = false;
-        int result = -1;  // any hit: 0 clear, 1 occluded, 2 overflow
-        if (ref >= 0) {
-            float a[8], b[8], c[8];
-            int4 rf;
-            load_wide(wn, ref, a, b, c, rf);
-            const int32_t rs[4] = {rf.x, rf.y, rf.z, rf.w};
-            int32_t hr[4];
-            float hd[4];
-            int m = 0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (rs[q] == kWideEmpty) continue;
-                float dq = slab(a[q], a[4 + q], b[q], b[4 + q], c[q], c[4 + q], o, inv);
-                bool ok = dq >= 0 && (kAny ? (!use_limit || dq < lim) : (dq < best && !(dq > tmax)));
-                if (ok) ins4(hr, hd, m, rs[q], dq);
-            }
-            if (m == 0) {
-                pop = true;
-            } else {
-                if (top + m >= kStack) {
-                    steps = kMaxSteps;
-                } else {
-                    for (int q = m - 1; q >= 1; --q) {  // far to near: the next nearest ends on top
-                        stack[++top] = hr[q];
-                        sdist[top] = hd[q];
-                    }
-                    ref = hr[0];
-                }
-            }
-        } else {
-            f3 v0, e1, e2;
-            int id, mesh;
-            load_tri(tris, ~ref, v0, e1, e2, id, mesh);
-            float t, u, v;
-            if (kAny) {
-                if (mesh != src && mesh != dst && tri_test(o, d, v0, e1, e2, t, u, v) && (!use_limit || t < lim))
-                    result = 1;
-            } else if (tri_test(o, d, v0, e1, e2, t, u, v)) {
-                if ((!hit || t < best) && !(t > tmax)) {
-                    hit = true;
-                    best = t;
-                    bid = id;
-                    bu = u;
-                    bv = v;
-                }
-            }
-            pop = true;
-        }
-        bool finished = false;
-        if (++steps >= kMaxSteps) {
-            atomicOr(flag, 1);
-            if (kAny) result = 2;
-            hit = false;
-            bid = -2;
-            finished = true;
-        } else if (kAny && result == 1) {
-            finished = true;
-        } else if (pop) {
-            while (top >= 0 && !(sdist[top] < best)) --top;  // farther than the current hit
-            if (top < 0) {
-                finished = true;
-                if (kAny) result = 0;
-            } else {
-                ref = stack[top--];
-            }
-        }
-        if (finished) {
-            if (kAny) {
-                occ[ray] = (uint8_t)result;
-            } else {
-                prim[ray] = hit ? bid : (bid == -2 ? -2 : -1);
-                if (tout) tout[ray] = hit ? best : __int_as_float(0x7f800000);
-                if (uv) reinterpret_cast<float2*>(uv)[ray] = make_float2(bu, bv);
-            }
-            ray = -1;
-        }
-    }
-}
-
-template <typename K>
-int grid_for(cav_ctx* ctx, K kernel, int block) {
-    int per_sm = ctx->trace_blocks_per_sm;
-    if (per_sm <= 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
-        if (per_sm < 1) per_sm = 1;
-    }
-    return ctx->num_sms * per_sm;
-}
-
-template <bool kAny>
-cav_status launch_fast(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, const uint32_t* n_dev,
-                       int32_t* prim, float* t, float* uv, const float* limit, const int32_t* excl, uint8_t* occ,
-                       cudaStream_t s, unsigned long long* counter) {
-    const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
-    const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
-    CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
-    const int grid = grid_for(ctx, k_trace_fast<kAny>, block);
-    k_trace_fast<kAny><<<grid, block, 0, s>>>(bvh->wnodes, bvh->tris, bvh->d_root_box, rays, n, n_dev, prim, t, uv, limit,
-                                              excl, occ, counter, batch, ctx->d_error + (kAny ? 3 : 2));
-    CAV_CUDA(ctx, cudaGetLastError());
-    return CAV_OK;
-}
-
 bool use_short_stack(const cav_ctx* ctx, const cav_bvh* bvh) {
     return ctx->trace_stack == kShortStack && bvh->depth >= 0 && bvh->depth + 1 < kShortStack;
 }
@@ -661,8 +410,7 @@ cav_status trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, 
     if (!bvh || !rays || !prim || n < 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_trace_closest: bad args");
     if (((uintptr_t)rays & 15) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
     if (n == 0) return CAV_OK;
-    if (flags & CAV_TRACE_FAST) return launch_fast<false>(ctx, bvh, rays, n, nullptr, prim, t, uv, nullptr, nullptr,
-                                                          nullptr, s, counter);
+    if (flags & CAV_TRACE_FAST) return trace_wide_closest(ctx, bvh, rays, n, nullptr, prim, t, uv, s, counter);
     TraceSeg one = seg_of(bvh);
     one.rays = rays;
     one.prim = prim;
@@ -677,8 +425,7 @@ cav_status trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, cons
     if (((uintptr_t)rays & 15) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
     if (excl && ((uintptr_t)excl & 7) != 0) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "excl must be 8-byte aligned");
     if (n == 0) return CAV_OK;
-    if (flags & CAV_TRACE_FAST) return launch_fast<true>(ctx, bvh, rays, n, nullptr, nullptr, nullptr, nullptr, limit,
-                                                         excl, occ, s, counter);
+    if (flags & CAV_TRACE_FAST) return trace_wide_any(ctx, bvh, rays, limit, excl, n, nullptr, occ, s, counter);
     TraceSeg one = seg_of(bvh);
     one.rays = rays;
     one.limit = limit;
@@ -700,7 +447,11 @@ cav_status trace_stats(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, in
     cav_status st;
     TraceSeg one = seg_of(bvh);
     one.rays = rays;
-    if (any_hit) {
+    if (flags & CAV_TRACE_FAST) {
+        st = any_hit ? trace_wide_any(ctx, bvh, rays, limit, excl, n, nullptr, out, s, ctx->d_counters + 4, stats)
+                     : trace_wide_closest(ctx, bvh, rays, n, nullptr, (int32_t*)out, (float*)(out + 4 * n), nullptr, s,
+                                          ctx->d_counters + 4, stats);
+    } else if (any_hit) {
         one.limit = limit;
         one.excl = excl;
         one.occ = out;
