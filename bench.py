@@ -42,6 +42,7 @@ HIT_BYTES = 16  # prim id 4 + t 4 + uv 8
 # 36 B (three float3 vertices) per triangle tested, counted by the instrumented kernel
 NODE_BYTES = 64
 TRI_BYTES = 36
+WIDE_NODE_BYTES = 80  # compressed 8-wide node of the fast mode
 
 
 def parse():
@@ -237,6 +238,38 @@ def run_ours(args):
         torch.cuda.synchronize()
         any_ms.append(a.elapsed_time(b))
 
+    # the compressed 8-wide fast mode on the same rays (secondary): same closest-hit
+    # distances, a different triangle only at an equal-distance tie
+    tuned_fast = bvh.autotune(torch.from_numpy(scenes.closest_rays(1 << 20, seed=90 + rank)).to(dev),
+                              flags=cav.TRACE_FAST)
+    fnodes, ftris = bvh.trace_stats(rays, flags=cav.TRACE_FAST)
+    fout = (torch.empty_like(prim), torch.empty_like(tt), torch.empty_like(uv))
+    for _ in range(2):
+        bvh.trace_closest(rays, flags=cav.TRACE_FAST, out=fout)
+    fast_ms = []
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        bvh.trace_closest(rays, flags=cav.TRACE_FAST, out=fout)
+        b.record()
+        torch.cuda.synchronize()
+        fast_ms.append(a.elapsed_time(b))
+    same_id = float((fout[0] == prim).float().mean().item())
+    same_t = bool(torch.equal(fout[1][prim >= 0], tt[prim >= 0]))
+    fany_ms = []
+    for k in range(max(3, args.steps // 2)):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        bvh.trace_any(srays, lim, flags=cav.TRACE_FAST, out=occ)
+        b.record()
+        torch.cuda.synchronize()
+        fany_ms.append(a.elapsed_time(b))
+    ctx.sync_check()
+    fast_ms_step = statistics.mean(fast_ms)
+    fast_bytes = RAY_BYTES + HIT_BYTES + WIDE_NODE_BYTES * fnodes / N_RAYS + TRI_BYTES * ftris / N_RAYS
+
     # e2e through the host-buffer C-ABI entry point (pinned host memory)
     h_rays = torch.from_numpy(rays_np).pin_memory()
     h_prim = torch.empty(N_RAYS, dtype=torch.int32).pin_memory()
@@ -314,6 +347,16 @@ def run_ours(args):
         },
         "clocks": clk,
         "anyhit_mrays_s": round(N_RAYS / (statistics.mean(any_ms) * 1e-3) / 1e6, 2),
+        "fast_mode": {
+            "closest_mrays_s": round(N_RAYS / (fast_ms_step * 1e-3) / 1e6, 2),
+            "anyhit_mrays_s": round(N_RAYS / (statistics.mean(fany_ms) * 1e-3) / 1e6, 2),
+            "same_prim_frac": round(same_id, 6), "same_t_on_hits": same_t,
+            "wide_nodes_per_ray": round(fnodes / N_RAYS, 3), "tris_per_ray": round(ftris / N_RAYS, 3),
+            "algorithmic_bytes_per_ray": round(fast_bytes, 2),
+            "achieved_gbs": round(fast_bytes * N_RAYS / (fast_ms_step * 1e-3) / 1e9, 1),
+            "launch_shape": {"block": tuned_fast["block_threads"], "queue_chunk": tuned_fast["batch"]},
+            "kernel": "k_trace_wide<false,false> (compressed 8-wide nodes, 80 B)",
+        },
         "build": {
             "ms": round(statistics.mean(builds_ms), 3),
             "builds_per_s": round(1000.0 / statistics.mean(builds_ms), 2),
@@ -453,16 +496,20 @@ def run_render(args):
         bvh = sc.bvh()
         tune_rays = torch.cat([sc.capture_rays(d, capacity=1 << 20) for d in (0, 1)])
         tuned = bvh.autotune(tune_rays)
+        tuned_fast = bvh.autotune(tune_rays, flags=cav.TRACE_FAST)
         fs = torch.empty(H * W * 3, device="cuda")
         fw = torch.empty(H * W, device="cuda")
+        sc.render_into(fs, fw, fast_trace=True)  # builds the fast mode's layout
         if rounds == 3:
             sampler.start()
-        totals = []
+        totals, totals_fast = [], []
         for _ in range(args.render_steps):
             torch.cuda.synchronize()
             sc.render_into(fs, fw)
-            st = sc.stats()
-            totals.append(st.as_dict())
+            totals.append(sc.stats().as_dict())
+            torch.cuda.synchronize()
+            sc.render_into(fs, fw, fast_trace=True)
+            totals_fast.append(sc.stats().as_dict())
         if rounds == 3:
             clocks = sampler.stop()
         st = totals[-1]
@@ -495,9 +542,11 @@ def run_render(args):
             b.record()
             torch.cuda.synchronize()
             ours.append(len(r) * 5 / (a.elapsed_time(b) * 1e-3) / 1e6)
-        # the same rays in the 4-wide fast mode (same hit distances; ties may pick another triangle)
+        # the same rays in the compressed 8-wide fast mode (same hit distances; ties may pick
+        # another triangle), its launch shape tuned for each bounce's rays
         fast = []
         for r in caps:
+            bvh.autotune(r, flags=cav.TRACE_FAST)
             for _ in range(3):
                 bvh.trace_closest(r, flags=cav.TRACE_FAST)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -508,14 +557,15 @@ def run_render(args):
             torch.cuda.synchronize()
             fast.append(len(r) * 5 / (a.elapsed_time(b) * 1e-3) / 1e6)
         runs[rounds]["ours_fast_captured_mrays_s"] = [round(x, 2) for x in fast]
-        # a whole render with the fast traversal
-        torch.cuda.synchronize()
-        sc.render_into(fs, fw, fast_trace=True)
-        stf = sc.stats().as_dict()
+        # whole renders with the fast traversal (timed beside the exact ones above)
+        stf = sorted(totals_fast, key=lambda t: t["ms_total"])[len(totals_fast) // 2]
         runs[rounds]["fast_render"] = {
             "ms_render": round(stf["ms_total"], 2),
+            "samples_per_s": round(samples / (stf["ms_total"] * 1e-3), 1),
             "extend_mrays_s": round(stf["closest_rays"] / (stf["ms_closest"] * 1e-3) / 1e6, 2),
-            "shadow_mrays_s": round(stf["shadow_rays"] / max(stf["ms_any"], 1e-9) * 1e-3, 2)}
+            "shadow_mrays_s": round(stf["shadow_rays"] / max(stf["ms_any"], 1e-9) * 1e-3, 2),
+            "ms_closest": round(stf["ms_closest"], 2), "ms_any": round(stf["ms_any"], 2),
+            "launch_shape": {k: tuned_fast[k] for k in ("block_threads", "batch")}}
         runs[rounds]["captured_rays"] = [int(len(r)) for r in caps]
         runs[rounds]["captured_launch_shapes"] = shapes
         runs[rounds]["ours_captured_mrays_s"] = [round(x, 2) for x in ours]
@@ -524,7 +574,9 @@ def run_render(args):
             s_np, w_np = fs.view(H, W, 3).cpu().numpy(), fw.view(H, W).cpu().numpy()
             ours_img = cav.film_to_rgb8(s_np, w_np)
         sc.free()
-    out["value"] = runs[3]["extend_mrays_s"]
+    out["value"] = runs[3]["fast_render"]["extend_mrays_s"]
+    out["config"]["trace_mode"] = ("fast: compressed 8-wide traversal (closest hits identical to the exact mode "
+                                   "except at equal-distance ties); exact-mode figures in render.roundsN")
     out["render"] = {f"rounds{k}": v for k, v in runs.items()}
     out["clocks"] = clocks
     # reference CUDA build on the same B200

@@ -108,6 +108,7 @@ def lib() -> ctypes.CDLL:
         "cav_mlp_last_loss": ([P, P], ctypes.c_int),
         "cav_mlp_mixture": ([P, P, ctypes.c_int64, P, P, P, P, P], ctypes.c_int),
         "cav_trace_autotune": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, P, P], ctypes.c_int),
+        "cav_trace_autotune_flags": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, U32, P, P], ctypes.c_int),
         "cav_server_create": ([P, P, ctypes.POINTER(P)], ctypes.c_int),
         "cav_server_destroy": ([P], ctypes.c_int),
         "cav_server_submit_render": ([P, P, P, P, P, P], ctypes.c_int),
@@ -626,12 +627,15 @@ class Bvh:
         self.ctx._check(lib().cav_bvh_stage_times(self.ctx.handle, self.handle, ms.ctypes.data), "cav_bvh_stage_times")
         return [float(x) for x in ms]
 
-    def autotune(self, rays, any_hit: bool = False, limit=None, excl=None, stream=None) -> dict:
-        """Pick and install the fastest traversal launch shape for this tree on a CUDA ray sample."""
+    def autotune(self, rays, any_hit: bool = False, limit=None, excl=None, flags: int = TRACE_EXACT,
+                 stream=None) -> dict:
+        """Pick and install the fastest traversal launch shape for this tree on a CUDA ray sample,
+        for the exact mode or (flags=TRACE_FAST) the compressed 8-wide mode."""
         out = TraceConfig()
-        st = lib().cav_trace_autotune(self.ctx.handle, self.handle, _ptr(rays), rays.shape[0], int(any_hit),
-                                      _ptr(limit), _ptr(excl), _stream_ptr(stream), ctypes.addressof(out))
-        self.ctx._check(st, "cav_trace_autotune")
+        st = lib().cav_trace_autotune_flags(self.ctx.handle, self.handle, _ptr(rays), rays.shape[0], int(any_hit),
+                                            _ptr(limit), _ptr(excl), flags, _stream_ptr(stream),
+                                            ctypes.addressof(out))
+        self.ctx._check(st, "cav_trace_autotune_flags")
         return out.as_dict()
 
     def trace_closest(self, rays, flags: int = TRACE_EXACT, stream=None, out=None):

@@ -108,6 +108,9 @@ struct cav_ctx {
     int trace_blocks_per_sm = 0;
     int trace_batch = 0;
     int trace_stack = 0;  // 64 selects the short traversal stack for trees known to be shallow
+    // launch configuration of the fast (compressed 8-wide) mode (0 = defaults)
+    int wide_block = 0;
+    int wide_batch = 0;
     // persistent work counters (device), one per concurrent trace kind
     unsigned long long* d_counters = nullptr;
     int* d_error = nullptr;

@@ -531,8 +531,18 @@ cav_status trace_any_dev(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, 
 extern "C" cav_status cav_trace_autotune(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
                                          const float* limit, const int32_t* excl, void* stream,
                                          cav_trace_config_t* best_out) {
+    return cav_trace_autotune_flags(ctx, bvh, rays, n, any_hit, limit, excl, CAV_TRACE_EXACT, stream, best_out);
+}
+
+// The same search for either traversal mode; the fast (compressed 8-wide) mode has its own
+// launch configuration in the context and no stack choice.
+extern "C" cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n,
+                                               int any_hit, const float* limit, const int32_t* excl, uint32_t flags,
+                                               void* stream, cav_trace_config_t* best_out) {
     using namespace cav;
     if (!ctx || !bvh || !rays || n <= 0) return CAV_ERR_INVALID_ARGUMENT;
+    if (flags & ~(uint32_t)CAV_TRACE_FAST) return CAV_ERR_INVALID_ARGUMENT;
+    const bool wide = (flags & CAV_TRACE_FAST) != 0;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
     cudaStream_t s = (cudaStream_t)stream;
     if (bvh->depth < 0) {
@@ -549,25 +559,31 @@ extern "C" cav_status cav_trace_autotune(cav_ctx* ctx, const cav_bvh* bvh, const
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    const int saved[4] = {ctx->trace_block, ctx->trace_blocks_per_sm, ctx->trace_batch, ctx->trace_stack};
+    const int saved[6] = {ctx->trace_block, ctx->trace_blocks_per_sm, ctx->trace_batch, ctx->trace_stack,
+                          ctx->wide_block, ctx->wide_batch};
     cav_trace_config_t best{0, 0, 0, 0, 1e30f};
     const int blocks[] = {64, 128, 256};
     const int batches[] = {1, 2, 4, 8, 16, 32};
     const int stacks[] = {kStack, kShortStack};
     cav_status st = CAV_OK;
     for (int stk : stacks) {
-        if (stk == kShortStack && !(bvh->depth + 1 < kShortStack)) continue;
+        if (stk == kShortStack && (wide || !(bvh->depth + 1 < kShortStack))) continue;
         for (int blk : blocks)
             for (int bat : batches) {
-                ctx->trace_block = blk;
-                ctx->trace_blocks_per_sm = 0;
-                ctx->trace_batch = bat;
-                ctx->trace_stack = stk;
+                if (wide) {
+                    ctx->wide_block = blk;
+                    ctx->wide_batch = bat;
+                } else {
+                    ctx->trace_block = blk;
+                    ctx->trace_blocks_per_sm = 0;
+                    ctx->trace_batch = bat;
+                    ctx->trace_stack = stk;
+                }
                 float ms_best = 1e30f;
                 for (int rep = 0; rep < 3 && st == CAV_OK; ++rep) {  // first repetition warms up
                     cudaEventRecord(a, s);
-                    st = any_hit ? trace_any(ctx, bvh, rays, limit, excl, n, occ, CAV_TRACE_EXACT, s, ctx->d_counters + 5)
-                                 : trace_closest(ctx, bvh, rays, n, prim, t, uv, CAV_TRACE_EXACT, s, ctx->d_counters + 5);
+                    st = any_hit ? trace_any(ctx, bvh, rays, limit, excl, n, occ, flags, s, ctx->d_counters + 5)
+                                 : trace_closest(ctx, bvh, rays, n, prim, t, uv, flags, s, ctx->d_counters + 5);
                     cudaEventRecord(b, s);
                     cudaEventSynchronize(b);
                     float ms = 0;
@@ -586,12 +602,26 @@ extern "C" cav_status cav_trace_autotune(cav_ctx* ctx, const cav_bvh* bvh, const
         ctx->trace_blocks_per_sm = saved[1];
         ctx->trace_batch = saved[2];
         ctx->trace_stack = saved[3];
+        ctx->wide_block = saved[4];
+        ctx->wide_batch = saved[5];
         return st != CAV_OK ? st : set_error(ctx, CAV_ERR_CUDA, "cav_trace_autotune: no candidate ran");
     }
-    ctx->trace_block = best.block_threads;
-    ctx->trace_blocks_per_sm = 0;
-    ctx->trace_batch = best.batch;
-    ctx->trace_stack = best.stack;
+    if (wide) {
+        ctx->trace_block = saved[0];  // the exact mode's shape stays as it was
+        ctx->trace_blocks_per_sm = saved[1];
+        ctx->trace_batch = saved[2];
+        ctx->trace_stack = saved[3];
+        ctx->wide_block = best.block_threads;
+        ctx->wide_batch = best.batch;
+        best.stack = 0;
+    } else {
+        ctx->trace_block = best.block_threads;
+        ctx->trace_blocks_per_sm = 0;
+        ctx->trace_batch = best.batch;
+        ctx->trace_stack = best.stack;
+        ctx->wide_block = saved[4];
+        ctx->wide_batch = saved[5];
+    }
     if (best_out) *best_out = best;
     return CAV_OK;
 }

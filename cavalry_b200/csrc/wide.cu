@@ -283,7 +283,7 @@ __device__ __forceinline__ uint32_t node_hits(const CNode* __restrict__ cn, uint
 }
 
 template <bool kAny, bool kStats>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256)
     k_trace_wide(const CNode* __restrict__ cn, const TriRec* __restrict__ tris, const cav_ray* __restrict__ rays,
                  int64_t n, const uint32_t* n_dev, int32_t* prim, float* tout, float* uv, const float* __restrict__ limit,
                  const int32_t* __restrict__ excl, uint8_t* occ, unsigned long long* counter, int refill, int* flag,
@@ -429,8 +429,8 @@ cav_status launch_wide(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, in
                        cudaStream_t s, unsigned long long* counter, unsigned long long* stats) {
     cav_status st = ensure_wide(ctx, bvh, s);
     if (st != CAV_OK) return st;
-    const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
-    const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
+    const int block = ctx->wide_block > 0 ? ctx->wide_block : 128;
+    const int batch = ctx->wide_batch > 0 ? ctx->wide_batch : kDefaultRefill;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     int* flag = ctx->d_error + (kAny ? 3 : 2);
     if (stats) {

@@ -32,3 +32,28 @@ def test_autotune_keeps_results_and_picks_a_candidate():
     assert np.array_equal(t0.cpu().numpy().view(np.uint32), t1.cpu().numpy().view(np.uint32))
     assert np.array_equal(o0.cpu().numpy(), o1.cpu().numpy())
     ctx.sync_check()
+
+
+def test_autotune_fast_mode_keeps_results_and_its_own_shape():
+    """Tuning the compressed 8-wide mode installs its shape without touching the exact mode's."""
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    ctx = cav.Context(0)
+    pos, idx = scenes.soup(200_000, seed=15)
+    bvh = ctx.build(torch.from_numpy(pos).cuda(), torch.from_numpy(idx).cuda(), rounds=2)
+    rays = torch.from_numpy(scenes.closest_rays(300_000, seed=16)).cuda()
+    exact = bvh.autotune(rays)
+    p0, t0, _ = bvh.trace_closest(rays, flags=cav.TRACE_FAST)
+    best = bvh.autotune(rays, flags=cav.TRACE_FAST)
+    assert best["block_threads"] in (64, 128, 256) and best["batch"] in (1, 2, 4, 8, 16, 32)
+    assert best["stack"] == 0 and best["ms"] > 0
+    p1, t1, _ = bvh.trace_closest(rays, flags=cav.TRACE_FAST)
+    assert np.array_equal(p0.cpu().numpy(), p1.cpu().numpy())
+    assert np.array_equal(t0.cpu().numpy().view(np.uint32), t1.cpu().numpy().view(np.uint32))
+    # the exact mode's tuned shape is still the one re-tuning picks as installed
+    pe, te, _ = bvh.trace_closest(rays)
+    assert exact["ms"] > 0 and (pe.cpu().numpy() >= -1).all()
+    ctx.sync_check()
