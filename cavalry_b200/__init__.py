@@ -108,6 +108,8 @@ def lib() -> ctypes.CDLL:
         "cav_mlp_last_loss": ([P, P], ctypes.c_int),
         "cav_mlp_mixture": ([P, P, ctypes.c_int64, P, P, P, P, P], ctypes.c_int),
         "cav_trace_autotune": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, P, P], ctypes.c_int),
+        "cav_pbrt_load_triangles": ([ctypes.c_char_p, P, ctypes.c_int64, P, P, ctypes.c_int64, P, P, P,
+                                     ctypes.c_int], ctypes.c_int),
         "cav_trace_autotune_flags": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, U32, P, P], ctypes.c_int),
         "cav_server_create": ([P, P, ctypes.POINTER(P)], ctypes.c_int),
         "cav_server_destroy": ([P], ctypes.c_int),
@@ -256,6 +258,25 @@ def parse_pbrt(path: str, spp: int = -1, integrator: str | None = None) -> tuple
     if st != 0:
         raise CavError(st, "cav_pbrt_parse_info: " + err.value.decode(errors="replace"))
     return info, c2w.reshape(4, 4).T
+
+
+def load_pbrt_triangles(path: str) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Host-only parse of a .pbrt file to (positions [V,3] f32, indices [T,3] i32, mesh ids [T] i32)."""
+    nv, nt = ctypes.c_int64(), ctypes.c_int64()
+    err = ctypes.create_string_buffer(512)
+    L = lib()
+    st = L.cav_pbrt_load_triangles(path.encode(), None, 0, None, None, 0, ctypes.byref(nv), ctypes.byref(nt),
+                                   ctypes.addressof(err), len(err))
+    if st != 0:
+        raise CavError(st, "cav_pbrt_load_triangles: " + err.value.decode(errors="replace"))
+    pos = np.zeros((nv.value, 3), np.float32)
+    idx = np.zeros((nt.value, 3), np.int32)
+    mid = np.zeros(nt.value, np.int32)
+    st = L.cav_pbrt_load_triangles(path.encode(), pos.ctypes.data, nv.value, idx.ctypes.data, mid.ctypes.data,
+                                   nt.value, ctypes.byref(nv), ctypes.byref(nt), ctypes.addressof(err), len(err))
+    if st != 0:
+        raise CavError(st, "cav_pbrt_load_triangles: " + err.value.decode(errors="replace"))
+    return pos, idx, mid
 
 
 class RenderStats(ctypes.Structure):

@@ -5,12 +5,17 @@
 
 namespace cav {
 
+// shape of a mesh (Core/TriangleMesh.h MeshShapeType): a tessellated sphere is sampled as a
+// light by the cone it subtends (TriangleMesh::sample :110-116)
+enum : int32_t { kShapeMesh = 0, kShapeSphere = 1, kShapeDisk = 2 };
+
 struct RMesh {
     int32_t first_tri, tri_count;
     int32_t has_normals, reverse;
     int32_t material, light;
     float area;  // TriangleMesh::surfaceArea
-    int32_t pad;
+    int32_t shape;
+    float sphere[4];  // kShapeSphere: world centre and radius (TriangleMesh::shapeParams)
 };
 
 struct RMaterial {

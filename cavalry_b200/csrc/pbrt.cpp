@@ -10,7 +10,8 @@
 //             :270-387 (AttributeBegin/End nesting, Material / MakeNamedMaterial /
 //             NamedMaterial, AreaLightSource bound to the next Shape, ReverseOrientation,
 //             Include spliced in place).
-//   shapes    Core/TriangleMesh.cu:119-186 ("P", "indices", optional "N").
+//   shapes    Core/TriangleMesh.cu:119-186 ("P", "indices", optional "N", or a PLY "filename"
+//             read by shapes.cu), ShapeMesh/ShapeMesh.h:8-24 (tessellated sphere and disk).
 //   materials Materials/{MatteMaterial,Plastic,Glass,Mirror}.h createFromParams defaults.
 #include "pbrt.h"
 
@@ -544,33 +545,78 @@ struct Parser {
                 world(xf, current_material, next_shape_light, false);
             } else if (w == "Shape") {
                 ObjectDef d = object();
-                if (d.name != "trianglemesh")
-                    throw ParseError("unsupported shape: " + d.name + " (only trianglemesh is supported)");
                 Mesh mesh;
-                const auto& P = d.params.list("P");
-                const auto& I = d.params.list("indices");
-                size_t nv = P.size() / 3, nt = I.size() / 3;
-                mesh.positions.resize(3 * nv);
-                for (size_t k = 0; k < nv; ++k) apply_point(xf, &P[3 * k], &mesh.positions[3 * k]);
-                mesh.indices.resize(3 * nt);
-                for (size_t k = 0; k < 3 * nt; ++k) {
-                    int v = (int)I[k];
-                    if (v < 0 || (size_t)v >= nv) throw ParseError("triangle index out of range");
-                    mesh.indices[k] = v;
-                }
-                if (d.params.has_list("N")) {
-                    const auto& N = d.params.list("N");
+                // positions through the CTM (apply), normals through transpose(inverse) of its
+                // upper 3x3 and normalised (getTransformForNormal, Utils/MathsCommons.h:80-82)
+                auto put_positions = [&](const std::vector<float>& P) {
+                    size_t nv = P.size() / 3;
+                    mesh.positions.resize(3 * nv);
+                    for (size_t k = 0; k < nv; ++k) apply_point(xf, &P[3 * k], &mesh.positions[3 * k]);
+                };
+                auto put_normals = [&](const std::vector<float>& N) {
+                    size_t nv = mesh.positions.size() / 3;
                     if (N.size() < 3 * nv) throw ParseError("N needs 3 values per vertex");
                     Mat4 inv = inverse(xf);
                     mesh.normals.resize(3 * nv);
                     for (size_t k = 0; k < nv; ++k) {
-                        // transpose(inverse(mat3(xf))) * n
                         float n[3];
                         for (int r = 0; r < 3; ++r)
                             n[r] = inv[r * 4 + 0] * N[3 * k] + inv[r * 4 + 1] * N[3 * k + 1] + inv[r * 4 + 2] * N[3 * k + 2];
                         float l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
                         for (int r = 0; r < 3; ++r) mesh.normals[3 * k + r] = n[r] / l;
                     }
+                };
+                auto put_indices = [&](const std::vector<int>& I) {
+                    const int nv = (int)(mesh.positions.size() / 3);
+                    for (int v : I)
+                        if (v < 0 || v >= nv) throw ParseError("triangle index out of range");
+                    mesh.indices = I;
+                };
+                if (d.name == "trianglemesh" || d.name == "plymesh") {  // Core/TriangleMesh.cu:119-186
+                    if (d.params.has_string("filename")) {
+                        PlyMesh pm = read_ply((base / d.params.str("filename")).string());
+                        put_positions(pm.positions);
+                        put_indices(pm.indices);
+                        if (!pm.normals.empty()) put_normals(pm.normals);
+                    } else if (d.params.has_list("P") && d.params.has_list("indices")) {
+                        put_positions(d.params.list("P"));
+                        const auto& I = d.params.list("indices");
+                        std::vector<int> ii(3 * (I.size() / 3));
+                        for (size_t k = 0; k < ii.size(); ++k) ii[k] = (int)I[k];
+                        put_indices(ii);
+                        if (d.params.has_list("N")) put_normals(d.params.list("N"));
+                    } else {
+                        throw ParseError("No valid inputs for triangle mesh");
+                    }
+                } else if (d.name == "sphere") {  // ShapeMesh/Sphere.cu:3-94
+                    const float radius = d.params.num("radius");
+                    std::vector<float> P, N;
+                    std::vector<int> I;
+                    sphere_mesh(radius, P, N, I);
+                    put_positions(P);
+                    put_indices(I);
+                    put_normals(N);
+                    mesh.shape = 1;
+                    const float o[3] = {0, 0, 0}, rx[3] = {radius, 0, 0};
+                    float c[3], e[3];
+                    apply_point(xf, o, c);
+                    apply_point(xf, rx, e);
+                    const float dx = c[0] - e[0], dy = c[1] - e[1], dz = c[2] - e[2];
+                    mesh.sphere[0] = c[0];
+                    mesh.sphere[1] = c[1];
+                    mesh.sphere[2] = c[2];
+                    mesh.sphere[3] = std::sqrt(dx * dx + dy * dy + dz * dz);
+                } else if (d.name == "disk") {  // ShapeMesh/Disk.cu:4-50
+                    const float radius = d.params.num("radius");
+                    const float height = d.params.has_num("height") ? d.params.num("height") : 0.f;
+                    std::vector<float> P;
+                    std::vector<int> I;
+                    disk_mesh(radius, height, P, I);
+                    put_positions(P);
+                    put_indices(I);
+                    mesh.shape = 2;
+                } else {
+                    throw ParseError("ShapeMesh type not supported: " + d.name);
                 }
                 mesh.reverse_orientation = reverse;
                 if (current_material < 0) {
@@ -652,6 +698,45 @@ Scene load_file(const std::string& path, const Overrides& ov) {
 // Host-only parse for tools and CPU tests: fills a cav_scene_info_t and the camera-to-world
 // matrix (16 floats, column-major) without touching the GPU.  `err` (or NULL) receives the
 // parser's message, truncated to err_len bytes.
+extern "C" cav_status cav_pbrt_load_triangles(const char* path, float* positions, int64_t max_vertices,
+                                              int32_t* indices, int32_t* mesh_ids, int64_t max_triangles,
+                                              int64_t* num_vertices, int64_t* num_triangles, char* err, int err_len) {
+    if (!path || !num_vertices || !num_triangles) return CAV_ERR_INVALID_ARGUMENT;
+    try {
+        cavpbrt::Scene s = cavpbrt::load_file(path, cavpbrt::Overrides{});
+        int64_t nv = 0, nt = 0;
+        for (const auto& m : s.meshes) {
+            nv += (int64_t)m.positions.size() / 3;
+            nt += (int64_t)m.indices.size() / 3;
+        }
+        *num_vertices = nv;
+        *num_triangles = nt;
+        if (!positions && !indices && !mesh_ids) return CAV_OK;
+        if ((positions && max_vertices < nv) || ((indices || mesh_ids) && max_triangles < nt))
+            return CAV_ERR_INVALID_ARGUMENT;
+        int64_t vb = 0, tb = 0;
+        for (size_t mi = 0; mi < s.meshes.size(); ++mi) {
+            const auto& m = s.meshes[mi];
+            if (positions) std::memcpy(positions + 3 * vb, m.positions.data(), m.positions.size() * sizeof(float));
+            const int64_t mt = (int64_t)m.indices.size() / 3;
+            for (int64_t t = 0; t < mt; ++t) {
+                if (indices)
+                    for (int k = 0; k < 3; ++k) indices[3 * (tb + t) + k] = (int32_t)(m.indices[3 * t + k] + vb);
+                if (mesh_ids) mesh_ids[tb + t] = (int32_t)mi;
+            }
+            vb += (int64_t)m.positions.size() / 3;
+            tb += mt;
+        }
+    } catch (const std::exception& e) {
+        if (err && err_len > 0) {
+            std::strncpy(err, e.what(), (size_t)err_len - 1);
+            err[err_len - 1] = 0;
+        }
+        return CAV_ERR_INVALID_ARGUMENT;
+    }
+    return CAV_OK;
+}
+
 extern "C" cav_status cav_pbrt_parse_info(const char* path, int spp_override, const char* integrator_override,
                                           cav_scene_info_t* info, float* camera_to_world16, char* err,
                                           int err_len) {

@@ -62,7 +62,23 @@ struct Mesh {
     bool reverse_orientation = false;
     int material = 0;
     int light = -1;  // index into Scene::lights when the mesh is an area light
+    int shape = 0;   // 0 triangle mesh, 1 tessellated sphere, 2 tessellated disk
+    float sphere[4] = {0, 0, 0, 0};  // sphere: world centre and radius (light sampling)
 };
+
+// A PLY file's triangle data as TriangleMesh::createFromPLY reads it (Core/TriangleMesh.cu:53-108):
+// float x/y/z (any numeric PLY type), optional nx/ny/nz and u/v, and the first three entries of
+// every face's "vertex_indices" list.  ASCII and binary (either byte order) formats.
+struct PlyMesh {
+    std::vector<float> positions, normals, uvs;
+    std::vector<int> indices;
+};
+PlyMesh read_ply(const std::string& path);
+
+// The reference's shape meshes (ShapeMesh/Sphere.cu:3-94, ShapeMesh/Disk.cu:4-50): positions
+// (and for the sphere unit normals before the normal transform) in object space.
+void sphere_mesh(float radius, std::vector<float>& pos, std::vector<float>& nrm, std::vector<int>& idx);
+void disk_mesh(float radius, float height, std::vector<float>& pos, std::vector<int>& idx);
 
 struct Light {
     float L[3] = {1, 1, 1};

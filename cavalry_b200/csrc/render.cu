@@ -63,9 +63,7 @@ __global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Que
             if (P.delta[path]) {
                 res = res + Le * thr;
             } else if (depth > 0) {
-                f3 l2s = ro - pos;
-                float cosine = fabsf(dot3(nrm, normalize3(l2s)));
-                float light_pdf = dot3(l2s, l2s) / (cosine * S.meshes[L.mesh].area);
+                float light_pdf = light_surface_pdf(S.meshes[L.mesh], ro, pos, nrm);
                 float w = mis_power(P.mat_pdf[path], light_pdf);
                 if (isfinite(w)) res = res + Le * thr * w;
             }
@@ -83,16 +81,9 @@ __global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Que
         dim += 4;  // rand4, drawn and unused by the reference
         const RLight& L = S.lights[li];
         const RMesh& LM = S.meshes[L.mesh];
-        int lt = LM.first_tri + halton_int(S.halton, index, dim, LM.tri_count);
-        float temp = sqrtf(halton(S.halton, index, dim));
-        float su = 1 - temp;
-        float sv = temp * halton(S.halton, index, dim);
-        int a = S.idx[3 * lt], b = S.idx[3 * lt + 1], c = S.idx[3 * lt + 2];
-        f3 lp = ld3(S.pos + 3 * a) * su + ld3(S.pos + 3 * b) * sv + ld3(S.pos + 3 * c) * (1.f - su - sv);
-        f3 ln = tri_normal(S, LM, lt, su, sv);
-        f3 l2s = pos - lp;
-        float lcos = fabsf(dot3(ln, normalize3(l2s)));
-        float light_pdf = dot3(l2s, l2s) / (lcos * LM.area);
+        const LightPoint lpt = sample_light_surface(S, LM, pos, index, dim);
+        const f3 lp = lpt.p, ln = lpt.n;
+        const float light_pdf = lpt.pdf;
         f3 dir = normalize3(lp - pos);
         f3 incident = dot3(dir, ln) >= 0 ? mk(0, 0, 0) : ld3(L.L);
         if (isfinite(light_pdf)) {
@@ -239,6 +230,8 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
         rm.reverse = m.reverse_orientation ? 1 : 0;
         rm.material = m.material;
         rm.light = m.light;
+        rm.shape = m.shape;
+        for (int k = 0; k < 4; ++k) rm.sphere[k] = m.sphere[k];
         // TriangleMesh::computeArea (Core/TriangleMesh.cu:189-199): float sum of half cross lengths
         float area = 0.f;
         for (size_t t = 0; t < m.indices.size() / 3; ++t) {

@@ -487,6 +487,93 @@ __device__ inline f3 tri_normal(const DevScene& S, const RMesh& M, int t, float 
     return n;
 }
 
+// --------------------------------------------------------------- light surfaces
+struct LightPoint {
+    f3 p, n;
+    float pdf;  // solid-angle pdf seen from the shading point
+};
+
+// TriangleMesh::sampleSphere (Core/TriangleMesh.h:154-210): a point of the sphere inside
+// the cone it subtends from `seen`, uniform in solid angle (pbrt-v3 Sphere::Sample).
+__device__ inline LightPoint sample_sphere_cone(const RMesh& M, f3 seen, float u0, float u1) {
+    const f3 c = mk(M.sphere[0], M.sphere[1], M.sphere[2]);
+    const float radius = M.sphere[3];
+    const float dc = length3(seen - c);
+    const float inv_dc = 1 / dc;
+    const f3 wc = (c - seen) * inv_dc;
+    const Frame fr = make_frame(wc);
+    const float sin_max = radius * inv_dc;
+    const float sin_max2 = sin_max * sin_max;
+    const float inv_sin_max = 1 / sin_max;
+    const float cos_max = sqrtf(fmaxf(0.f, 1 - sin_max2));
+    float cos_t = (cos_max - 1) * u0 + 1;
+    float sin_t2 = 1 - cos_t * cos_t;
+    if (sin_max2 < 0.00068523f) {  // sin^2(1.5 deg): series form for small cones
+        sin_t2 = sin_max2 * u0;
+        cos_t = sqrtf(1 - sin_t2);
+    }
+    const float cos_a = sin_t2 * inv_sin_max + cos_t * sqrtf(fmaxf(0.f, 1.f - sin_t2 * inv_sin_max * inv_sin_max));
+    const float sin_a = sqrtf(fmaxf(0.f, 1.f - cos_a * cos_a));
+    const float phi = (float)(u1 * 2 * 3.14159265358979323846);
+    f3 nw = (sin_a * cosf(phi) * fr.t0 + sin_a * sinf(phi) * fr.t1 + cos_t * wc) * -1.f;
+    LightPoint lp;
+    lp.p = c + radius * nw;
+    lp.n = M.reverse ? nw * -1.f : nw;
+    lp.pdf = (float)(1 / (2 * 3.14159265358979323846 * (1 - cos_max)));
+    return lp;
+}
+
+// TriangleMesh::sample (Core/TriangleMesh.h:110-152) for DiffuseAreaLight::sampleRayToPoint:
+// the cone of a sphere seen from outside (2 dimensions), else a triangle picked uniformly
+// and a uniform point on it (3 dimensions).  Advances `dim`.  The bounce's next draws start 8
+// dimensions after its first in every case: the reference synchronises dimensions to the
+// maximum over the bounce's paths, and a path that hits a tessellated light sphere shades
+// from inside the true sphere and takes the 3-dimension branch.  (Only a bounce in which no
+// path samples a light by triangles -- every light a sphere and no path inside one -- would
+// start one dimension earlier in the reference.)
+__device__ inline LightPoint sample_light_surface(const DevScene& S, const RMesh& LM, f3 seen, uint64_t index,
+                                                  int& dim) {
+    if (LM.shape == kShapeSphere) {
+        const f3 c = mk(LM.sphere[0], LM.sphere[1], LM.sphere[2]);
+        const f3 dv = seen - c;
+        if (dot3(dv, dv) > LM.sphere[3] * LM.sphere[3]) {
+            const float u0 = halton(S.halton, index, dim);
+            const float u1 = halton(S.halton, index, dim);
+            return sample_sphere_cone(LM, seen, u0, u1);
+        }
+    }
+    const int lt = LM.first_tri + halton_int(S.halton, index, dim, LM.tri_count);
+    const float temp = sqrtf(halton(S.halton, index, dim));
+    const float su = 1 - temp;
+    const float sv = temp * halton(S.halton, index, dim);
+    const int a = S.idx[3 * lt], b = S.idx[3 * lt + 1], c = S.idx[3 * lt + 2];
+    LightPoint lp;
+    lp.p = ld3(S.pos + 3 * a) * su + ld3(S.pos + 3 * b) * sv + ld3(S.pos + 3 * c) * (1.f - su - sv);
+    lp.n = tri_normal(S, LM, lt, su, sv);
+    const f3 l2s = seen - lp.p;
+    const float lcos = fabsf(dot3(lp.n, normalize3(l2s)));
+    lp.pdf = dot3(l2s, l2s) / (lcos * LM.area);
+    return lp;
+}
+
+// TriangleMesh::pdf (Core/TriangleMesh.h:213-232): the light pdf of a ray from `o` that
+// reached the light surface at p with normal n.
+__device__ inline float light_surface_pdf(const RMesh& LM, f3 o, f3 p, f3 n) {
+    if (LM.shape == kShapeSphere) {
+        const f3 c = mk(LM.sphere[0], LM.sphere[1], LM.sphere[2]);
+        const f3 dv = o - c;
+        const float d2 = dot3(dv, dv);
+        const float r2 = LM.sphere[3] * LM.sphere[3];
+        if (d2 > r2) {
+            const float cos_max = sqrtf(fmaxf(0.f, 1.f - r2 / d2));
+            return (float)(1.f / (2.f * 3.14159265358979323846 * (1 - cos_max)));
+        }
+    }
+    const f3 l2s = o - p;
+    const float cosine = fabsf(dot3(n, normalize3(l2s)));
+    return dot3(l2s, l2s) / (cosine * LM.area);
+}
+
 // ---------------------------------------------------------------- path state
 struct Paths {
     uint64_t* sample_index;

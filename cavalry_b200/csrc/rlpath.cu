@@ -208,9 +208,7 @@ __global__ void k_rl_light(DevScene S, const float* box, LightTable LT, int dept
             if (P.delta[path]) {
                 res = res + Le * thr;
             } else if (depth > 0) {
-                f3 l2s = h.ro - h.pos;
-                float cosine = fabsf(dot3(h.nrm, normalize3(l2s)));
-                float light_pdf = dot3(l2s, l2s) / (cosine * S.meshes[L.mesh].area);
+                float light_pdf = light_surface_pdf(S.meshes[L.mesh], h.ro, h.pos, h.nrm);
                 float w = mis_power(P.mat_pdf[path], light_pdf);
                 if (isfinite(w)) {
                     emis = luminance(Le);
@@ -228,16 +226,9 @@ __global__ void k_rl_light(DevScene S, const float* box, LightTable LT, int dept
         dim += 4;  // rand4, drawn and unused
         const RLight& L = S.lights[li];
         const RMesh& LM = S.meshes[L.mesh];
-        int lt = LM.first_tri + halton_int(S.halton, index, dim, LM.tri_count);
-        float temp = sqrtf(halton(S.halton, index, dim));
-        float su = 1 - temp;
-        float sv = temp * halton(S.halton, index, dim);
-        int a = S.idx[3 * lt], b = S.idx[3 * lt + 1], c = S.idx[3 * lt + 2];
-        f3 lp = ld3(S.pos + 3 * a) * su + ld3(S.pos + 3 * b) * sv + ld3(S.pos + 3 * c) * (1.f - su - sv);
-        f3 ln = tri_normal(S, LM, lt, su, sv);
-        f3 l2s = h.pos - lp;
-        float lcos = fabsf(dot3(ln, normalize3(l2s)));
-        float light_pdf = dot3(l2s, l2s) / (lcos * LM.area);
+        const LightPoint lpt = sample_light_surface(S, LM, h.pos, index, dim);
+        const f3 lp = lpt.p, ln = lpt.n;
+        const float light_pdf = lpt.pdf;
         f3 dir = normalize3(lp - h.pos);
         f3 incident = dot3(dir, ln) >= 0 ? mk(0, 0, 0) : ld3(L.L);
         T.light_dir[3 * j] = dir.x;

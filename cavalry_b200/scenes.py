@@ -15,6 +15,8 @@ configurations this project measures:
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 RAY_DTYPE = np.float32
@@ -171,12 +173,17 @@ def _material_line(mat) -> str:
 
 
 def write_pbrt(path, room: dict, *, width=256, height=256, spp=16, max_depth=5, fov=None, eye=None, look=None,
-               up=None, integrator="path"):
+               up=None, integrator="path", ply: bool | None = None):
     """Write a scene dict (mini_room, sphere_scene) as a .pbrt file in the subset the
     reference's loader reads (SceneLoading/Lexing.cu, Parsing.cu): one trianglemesh Shape per
     mesh with its Material; light meshes (``room["lights"]`` = [(mesh, L)], or a mesh named
     "light" with ``room["light_radiance"]``) as diffuse AreaLightSources over a black matte.
-    Camera arguments default to ``room["camera"]``, else the config-1 view."""
+    Camera arguments default to ``room["camera"]``, else the config-1 view.  Meshes listed in
+    ``room["shapes"]`` are written as pbrt ``sphere`` / ``disk`` Shapes under a Translate;
+    with `ply` (default ``room.get("write_ply")``), triangle meshes go to binary PLY files
+    beside the .pbrt ("plymesh")."""
+    if ply is None:
+        ply = bool(room.get("write_ply", False))
     cam = dict(eye=(0.0, 0.0, -3.8), look=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), fov=40.0)
     cam.update(room.get("camera", {}))
     for k, v in (("eye", eye), ("look", look), ("up", up), ("fov", fov)):
@@ -204,16 +211,149 @@ def write_pbrt(path, room: dict, *, width=256, height=256, spp=16, max_depth=5, 
             if L is None and name == "light":
                 L = room.get("light_radiance", (17.0, 12.0, 4.0))
             out = ["AttributeBegin"]
+            shape = room.get("shapes", {}).get(k)
+            if shape is not None:
+                out.append(f"Translate {_nums(shape['center'])}")
             if L is not None:
                 out.append(f'AreaLightSource "diffuse" "rgb L" [{_nums(L)}]')
                 out.append('Material "matte" "rgb Kd" [0 0 0]')
             else:
                 out.append(_material_line(mat))
-            out.append('Shape "trianglemesh" "integer indices" [' + " ".join(map(str, I.tolist())) + '] "point P" ['
-                       + _floats_text(P) + "]")
+            if shape is not None and shape["type"] == "sphere":
+                out.append(f'Shape "sphere" "float radius" [{_num(shape["radius"])}]')
+            elif shape is not None:
+                out.append(f'Shape "disk" "float radius" [{_num(shape["radius"])}] '
+                           f'"float height" [{_num(shape.get("height", 0.0))}]')
+            elif ply:
+                fn = f"{os.path.splitext(os.path.basename(str(path)))[0]}_{k}.ply"
+                _write_ply(os.path.join(os.path.dirname(os.path.abspath(str(path))), fn), P, I)
+                out.append(f'Shape "plymesh" "string filename" "{fn}"')
+            else:
+                out.append('Shape "trianglemesh" "integer indices" [' + " ".join(map(str, I.tolist())) + '] "point P" ['
+                           + _floats_text(P) + "]")
             out.append("AttributeEnd")
             f.write("\n".join(out) + "\n")
         f.write("WorldEnd\n")
+
+
+def _write_ply(path, P, I):
+    """Binary little-endian PLY: float x/y/z and a uchar/int "vertex_indices" list per face."""
+    P = np.ascontiguousarray(P, np.float32)
+    I = np.asarray(I, np.int32).reshape(-1, 3)
+    head = ("ply\nformat binary_little_endian 1.0\n"
+            f"element vertex {len(P)}\nproperty float x\nproperty float y\nproperty float z\n"
+            f"element face {len(I)}\nproperty list uchar int vertex_indices\nend_header\n")
+    face = np.zeros(len(I), np.dtype([("n", "u1"), ("i", "<i4", (3,))]))
+    face["n"] = 3
+    face["i"] = I
+    with open(path, "wb") as f:
+        f.write(head.encode())
+        f.write(P.tobytes())
+        f.write(face.tobytes())
+
+
+def sphere_shape_mesh(radius: float):
+    """The mesh the reference makes for a ``Shape "sphere"`` (ShapeMesh/Sphere.cu:3-94): an
+    octahedron split four times, every split pushing its three midpoints (normalised) as new
+    vertices, 2046 vertices and 2048 triangles.  Returns (unit positions = normals [V,3],
+    positions * radius [V,3], indices [T,3]) in object space, float32."""
+    p = [np.array(v, np.float32) for v in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1))]
+    cur = [(0, 2, 4), (0, 2, 5), (0, 3, 4), (0, 3, 5), (1, 2, 4), (1, 2, 5), (1, 3, 4), (1, 3, 5)]
+
+    def nrm(v):
+        inv = np.float32(1.0 / np.sqrt(np.float64(np.float32(v[0] * v[0] + v[1] * v[1]) + v[2] * v[2])))
+        return (v * inv).astype(np.float32)
+
+    for _ in range(4):
+        nxt = []
+        for i0, i1, i2 in cur:
+            p.append(nrm((p[i0] + p[i1]) * np.float32(0.5)))
+            i01 = len(p) - 1
+            p.append(nrm((p[i0] + p[i2]) * np.float32(0.5)))
+            i02 = len(p) - 1
+            p.append(nrm((p[i1] + p[i2]) * np.float32(0.5)))
+            i12 = len(p) - 1
+            nxt += [(i01, i02, i12), (i0, i01, i02), (i1, i01, i12), (i2, i02, i12)]
+        cur = nxt
+    unit = np.array(p, np.float32)
+    return unit, (unit * np.float32(radius)).astype(np.float32), np.array(cur, np.int32)
+
+
+def disk_shape_mesh(radius: float, height: float = 0.0):
+    """The mesh of a ``Shape "disk"`` (ShapeMesh/Disk.cu:4-50): 360 rim vertices at
+    (sin t r, cos t r, height), the centre last, triangles (s+1, s, centre)."""
+    th = (2.0 * np.pi * np.arange(360, dtype=np.float32).astype(np.float64) / 360.0).astype(np.float32)
+    rim = np.stack([np.sin(th) * np.float32(radius), np.cos(th) * np.float32(radius),
+                    np.full(360, height, np.float32)], 1).astype(np.float32)
+    P = np.concatenate([rim, np.array([[0, 0, height]], np.float32)])
+    s = np.arange(360)
+    return P, np.stack([(s + 1) % 360, s, np.full(360, 360)], 1).astype(np.int32)
+
+
+def shapes_scene(seed: int = 31, quad_light: bool = False):
+    """A 4 x 3 x 4 room (matte walls) holding tessellated ``sphere`` shapes of assorted
+    materials, a matte ``disk`` on the back wall and a sphere area light under the ceiling
+    (plus a 1 x 1 quad light when `quad_light`).  The scene dict carries
+    ``shapes = {mesh: {"type", "radius", "center", ("height")}}`` (written as pbrt Shapes with
+    Translate) and per-vertex ``normals`` (the spheres'; zero elsewhere)."""
+    rng = np.random.default_rng(seed)
+    verts, tris, mesh_ids, meshes, lights, nrms, shapes = [], [], [], [], [], [], {}
+    nv = nt = 0
+
+    def add(v, t, name, mat, n=None):
+        nonlocal nv, nt
+        mid = len(meshes)
+        verts.append(np.asarray(v, np.float32))
+        nrms.append(np.zeros_like(verts[-1]) if n is None else np.asarray(n, np.float32))
+        tris.append(np.asarray(t, np.int64) + nv)
+        mesh_ids.append(np.full(len(t), mid, np.int32))
+        meshes.append((name, nt, len(t), mat))
+        nv += len(v)
+        nt += len(t)
+        return mid
+
+    W, H, D = 4.0, 3.0, 4.0
+    x0, x1, z0, z1 = -W / 2, W / 2, -D / 2, D / 2
+    grey = (0.7, 0.7, 0.7)
+    add([[x0, 0, z0], [x1, 0, z0], [x1, 0, z1], [x0, 0, z1]], [(0, 2, 1), (0, 3, 2)], "floor", grey)
+    add([[x0, H, z0], [x1, H, z0], [x1, H, z1], [x0, H, z1]], [(0, 1, 2), (0, 2, 3)], "ceiling", grey)
+    add([[x0, 0, z1], [x1, 0, z1], [x1, H, z1], [x0, H, z1]], [(0, 2, 1), (0, 3, 2)], "back", grey)
+    add([[x0, 0, z0], [x0, 0, z1], [x0, H, z1], [x0, H, z0]], [(0, 1, 2), (0, 2, 3)], "left", (0.6, 0.15, 0.1))
+    add([[x1, 0, z0], [x1, 0, z1], [x1, H, z1], [x1, H, z0]], [(0, 2, 1), (0, 3, 2)], "right", (0.15, 0.5, 0.2))
+    kinds = [{"type": "matte", "Kd": (0.8, 0.5, 0.2)}, {"type": "plastic", "Kd": (0.2, 0.3, 0.7), "roughness": 0.1},
+             {"type": "glass", "eta": 1.5}, {"type": "metal", "roughness": 0.2},
+             {"type": "substrate", "Kd": (0.5, 0.6, 0.3), "Ks": (0.3, 0.3, 0.3), "roughness": 0.15}]
+    for k, mat in enumerate(kinds):
+        r = float(rng.uniform(0.25, 0.45))
+        c = (float(-1.4 + 0.7 * k), r, float(rng.uniform(-0.6, 0.8)))
+        unit, P, I = sphere_shape_mesh(r)
+        mid = add(P + np.array(c, np.float32), I, f"sphere{k}", mat, n=unit)
+        shapes[mid] = {"type": "sphere", "radius": r, "center": c}
+    dP, dI = disk_shape_mesh(0.6, 0.0)
+    dc = (0.8, 1.6, z1 - 0.01)
+    mid = add(dP + np.array(dc, np.float32), dI, "disk", (0.75, 0.75, 0.3))
+    shapes[mid] = {"type": "disk", "radius": 0.6, "height": 0.0, "center": dc}
+    lr = 0.25
+    lc = (-0.3, H - 0.6, 0.2)
+    unit, P, I = sphere_shape_mesh(lr)
+    mid = add(P + np.array(lc, np.float32), I, "light_sphere", (0.0, 0.0, 0.0), n=unit)
+    shapes[mid] = {"type": "sphere", "radius": lr, "center": lc}
+    lights.append((mid, (14.0, 12.0, 9.0)))
+    if quad_light:
+        y = H - 0.01
+        mid = add([[0.4, y, -0.9], [1.4, y, -0.9], [1.4, y, 0.1], [0.4, y, 0.1]], [(0, 1, 2), (0, 2, 3)],
+                  "light_quad", (0.0, 0.0, 0.0))
+        lights.append((mid, (4.0, 4.0, 6.0)))
+    return {
+        "positions": np.ascontiguousarray(np.concatenate(verts)),
+        "normals": np.ascontiguousarray(np.concatenate(nrms)),
+        "indices": np.ascontiguousarray(np.concatenate(tris).astype(np.int32)),
+        "mesh_ids": np.concatenate(mesh_ids),
+        "meshes": meshes,
+        "lights": lights,
+        "shapes": shapes,
+        "camera": {"eye": (0.0, 1.5, z0 + 0.1), "look": (0.0, 1.1, 0.0), "up": (0.0, 1.0, 0.0), "fov": 65.0},
+    }
 
 
 _ICO_CACHE: dict = {}

@@ -221,6 +221,15 @@ enum { CAV_RENDER_GRAPH = 1, CAV_RENDER_FAST_TRACE = 2 /* trace with CAV_TRACE_F
  * message into err (may be NULL).  bvh_rounds in `info` is reported as -1. */
 cav_status cav_pbrt_parse_info(const char* path, int spp_override, const char* integrator_override,
                                cav_scene_info_t* info, float* camera_to_world16, char* err, int err_len);
+/* Host-only .pbrt parse to flat triangle arrays (no GPU): world-space positions (3 floats per
+ * vertex, meshes concatenated in file order), triangle vertex indices (3 per triangle, global)
+ * and the mesh id of every triangle; trianglemesh / plymesh (PLY read from the file beside the
+ * .pbrt), sphere and disk shapes as the reference tessellates them.  Call with NULL arrays to
+ * get the counts; arrays smaller than the counts give CAV_ERR_INVALID_ARGUMENT.  Parse errors
+ * as cav_pbrt_parse_info. */
+cav_status cav_pbrt_load_triangles(const char* path, float* positions, int64_t max_vertices, int32_t* indices,
+                                   int32_t* mesh_ids, int64_t max_triangles, int64_t* num_vertices,
+                                   int64_t* num_triangles, char* err, int err_len);
 /* Loads a .pbrt scene and builds its BVH.  spp_override > 0 replaces the sampler's
  * pixelsamples (--spp), integrator_override (or NULL) the integrator name (--integrator),
  * bvh_rounds the treelet rounds (--bvh-opt-rounds; -1 = 3, or 10 when spp >= 64, as

@@ -57,7 +57,8 @@ int orc_any_one(const ONode* nodes, const float* pos, const int32_t* idx, const 
 typedef struct {
     int32_t first_tri, tri_count, has_normals, reverse, material, light;
     float area;
-    int32_t pad;
+    int32_t shape;    /* 0 triangle mesh, 1 tessellated sphere (cone-sampled as a light), 2 disk */
+    float sphere[4];  /* sphere: world centre and radius (TriangleMesh::shapeParams) */
 } OMesh;
 typedef struct {
     int32_t type; /* 0 matte, 1 mirror, 2 substrate, 3 metal, 4 glass (specular or rough), 5 plastic */
@@ -555,6 +556,75 @@ static V3 apply_pt(const float* m, V3 v) {
     return v3(t0 / t3, t1 / t3, t2 / t3);
 }
 
+/* TriangleMesh::sampleSphere (Core/TriangleMesh.h:154-210): uniform in the cone a sphere
+ * subtends from `seen` (pbrt-v3 Sphere::Sample), solid-angle pdf. */
+static void sphere_cone(const OMesh* M, V3 seen, float u0, float u1, V3* lp, V3* ln, float* pdf) {
+    V3 c = v3(M->sphere[0], M->sphere[1], M->sphere[2]);
+    float radius = M->sphere[3];
+    V3 dv = vsub(seen, c);
+    float dc = sqrtf(vdot(dv, dv));
+    float inv_dc = 1 / dc;
+    V3 wc = vs(vsub(c, seen), inv_dc);
+    Frame fr = make_frame(wc);
+    float sin_max = radius * inv_dc;
+    float sin_max2 = sin_max * sin_max;
+    float inv_sin_max = 1 / sin_max;
+    float cos_max = sqrtf(fmaxf(0.f, 1 - sin_max2));
+    float cos_t = (cos_max - 1) * u0 + 1;
+    float sin_t2 = 1 - cos_t * cos_t;
+    if (sin_max2 < 0.00068523f) {
+        sin_t2 = sin_max2 * u0;
+        cos_t = sqrtf(1 - sin_t2);
+    }
+    float cos_a = sin_t2 * inv_sin_max + cos_t * sqrtf(fmaxf(0.f, 1.f - sin_t2 * inv_sin_max * inv_sin_max));
+    float sin_a = sqrtf(fmaxf(0.f, 1.f - cos_a * cos_a));
+    float phi = (float)(u1 * 2 * M_PI);
+    V3 nw = vs(vadd(vadd(vs(fr.t0, sin_a * cosf(phi)), vs(fr.t1, sin_a * sinf(phi))), vs(wc, cos_t)), -1.f);
+    *lp = vadd(c, vs(nw, radius));
+    *ln = M->reverse ? vs(nw, -1.f) : nw;
+    *pdf = (float)(1 / (2 * M_PI * (1 - cos_max)));
+}
+
+/* TriangleMesh::sample (Core/TriangleMesh.h:110-152): the sphere cone seen from outside (2
+ * dimensions), else a uniform triangle and a uniform point on it (3 dimensions). */
+static void light_sample(const Scene* S, const OMesh* LM, V3 seen, uint64_t index, int* dim, V3* lp, V3* ln,
+                         float* pdf) {
+    if (LM->shape == 1) {
+        V3 dv = vsub(seen, v3(LM->sphere[0], LM->sphere[1], LM->sphere[2]));
+        if (vdot(dv, dv) > LM->sphere[3] * LM->sphere[3]) {
+            float u0 = halton(&S->h, index, dim);
+            float u1 = halton(&S->h, index, dim);
+            sphere_cone(LM, seen, u0, u1, lp, ln, pdf);
+            return;
+        }
+    }
+    int lt = LM->first_tri + halton_int(&S->h, index, dim, LM->tri_count);
+    float temp = sqrtf(halton(&S->h, index, dim));
+    float su = 1 - temp;
+    float sv = temp * halton(&S->h, index, dim);
+    int a = S->idx[3 * lt], b = S->idx[3 * lt + 1], c = S->idx[3 * lt + 2];
+    *lp = vadd(vadd(vs(ld3(S->pos + 3 * a), su), vs(ld3(S->pos + 3 * b), sv)), vs(ld3(S->pos + 3 * c), 1.f - su - sv));
+    *ln = tri_normal(S, LM, lt, su, sv);
+    V3 l2s = vsub(seen, *lp);
+    float lcos = fabsf(vdot(*ln, vnorm(l2s)));
+    *pdf = vdot(l2s, l2s) / (lcos * LM->area);
+}
+
+/* TriangleMesh::pdf (Core/TriangleMesh.h:213-232) of a ray from o reaching the light at p, n. */
+static float light_pdf_at(const OMesh* LM, V3 o, V3 p, V3 n) {
+    if (LM->shape == 1) {
+        V3 dv = vsub(o, v3(LM->sphere[0], LM->sphere[1], LM->sphere[2]));
+        float d2 = vdot(dv, dv), r2 = LM->sphere[3] * LM->sphere[3];
+        if (d2 > r2) {
+            float cos_max = sqrtf(fmaxf(0.f, 1.f - r2 / d2));
+            return (float)(1.f / (2.f * M_PI * (1 - cos_max)));
+        }
+    }
+    V3 l2s = vsub(o, p);
+    float c = fabsf(vdot(n, vnorm(l2s)));
+    return vdot(l2s, l2s) / (c * LM->area);
+}
+
 /* One camera sample through the integrator's bounce loop.  Returns the path's radiance. */
 static V3 trace_path(const Scene* S, uint64_t index, V3 ro, V3 rd, int max_depth) {
     V3 res = v3(0, 0, 0), thr = v3(1, 1, 1);
@@ -576,9 +646,7 @@ static V3 trace_path(const Scene* S, uint64_t index, V3 ro, V3 rd, int max_depth
             if (delta) {
                 res = vadd(res, vmul(Le, thr));
             } else if (depth > 0) {
-                V3 l2s = vsub(ro, pos);
-                float c = fabsf(vdot(nrm, vnorm(l2s)));
-                float lpdf = vdot(l2s, l2s) / (c * S->meshes[L->mesh].area);
+                float lpdf = light_pdf_at(&S->meshes[L->mesh], ro, pos, nrm);
                 float w = mis_power(mat_pdf, lpdf);
                 if (isfinite(w)) res = vadd(res, vs(vmul(Le, thr), w));
             }
@@ -592,16 +660,9 @@ static V3 trace_path(const Scene* S, uint64_t index, V3 ro, V3 rd, int max_depth
         dim += 4;
         const OLight* L = &S->lights[li];
         const OMesh* LM = &S->meshes[L->mesh];
-        int lt = LM->first_tri + halton_int(&S->h, index, &dim, LM->tri_count);
-        float temp = sqrtf(halton(&S->h, index, &dim));
-        float su = 1 - temp;
-        float sv = temp * halton(&S->h, index, &dim);
-        int a = S->idx[3 * lt], b = S->idx[3 * lt + 1], c = S->idx[3 * lt + 2];
-        V3 lp = vadd(vadd(vs(ld3(S->pos + 3 * a), su), vs(ld3(S->pos + 3 * b), sv)), vs(ld3(S->pos + 3 * c), 1.f - su - sv));
-        V3 ln = tri_normal(S, LM, lt, su, sv);
-        V3 l2s = vsub(pos, lp);
-        float lcos = fabsf(vdot(ln, vnorm(l2s)));
-        float lpdf = vdot(l2s, l2s) / (lcos * LM->area);
+        V3 lp, ln;
+        float lpdf;
+        light_sample(S, LM, pos, index, &dim, &lp, &ln, &lpdf);
         V3 dir = vnorm(vsub(lp, pos));
         V3 incident = vdot(dir, ln) >= 0 ? v3(0, 0, 0) : ld3(L->L);
         if (isfinite(lpdf)) {

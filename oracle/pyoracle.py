@@ -237,7 +237,8 @@ class RefScene:
 
 # ---------------------------------------------------------------- path-tracing oracle
 OMESH_DTYPE = np.dtype([("first_tri", "<i4"), ("tri_count", "<i4"), ("has_normals", "<i4"), ("reverse", "<i4"),
-                        ("material", "<i4"), ("light", "<i4"), ("area", "<f4"), ("pad", "<i4")])
+                        ("material", "<i4"), ("light", "<i4"), ("area", "<f4"), ("shape", "<i4"),
+                        ("sphere", "<f4", (4,))])
 OMAT_DTYPE = np.dtype([("type", "<i4"), ("kd", "<f4", (3,)), ("ks", "<f4", (3,)), ("kr", "<f4", (3,)),
                        ("kt", "<f4", (3,)), ("alpha_u", "<f4"), ("alpha_v", "<f4"), ("eta", "<f4"),
                        ("mirror_kr", "<f4"), ("f0", "<f4", (3,)), ("has_f0", "<i4")])
@@ -343,9 +344,22 @@ def render_path(scene: dict, *, width: int, height: int, spp: int, max_depth: in
     mats = np.zeros(len(scene["meshes"]), OMAT_DTYPE)
     lights = []
     light_of = dict(scene.get("lights", []))
+    shapes = scene.get("shapes", {})
+    nrm = scene.get("normals")
+    nrm = None if nrm is None else np.ascontiguousarray(nrm, np.float32)
     for k, (name, first_tri, n, mat) in enumerate(scene["meshes"]):
         meshes[k]["first_tri"], meshes[k]["tri_count"] = first_tri, n
         meshes[k]["material"] = k
+        sh = shapes.get(k)
+        if sh is not None and sh["type"] == "sphere":  # smooth normals; cone-sampled as a light
+            meshes[k]["has_normals"] = 1
+            meshes[k]["shape"] = 1
+            c = np.asarray(sh["center"], np.float32)
+            # TriangleMesh shapeParams: the transformed centre and |centre - transform(r, 0, 0)|
+            e = (np.array([sh["radius"], 0, 0], np.float32) + c).astype(np.float32)
+            meshes[k]["sphere"] = (c[0], c[1], c[2], np.float32(np.sqrt(np.float32(((c - e) ** 2).sum()))))
+        elif sh is not None:
+            meshes[k]["shape"] = 2
         mats[k] = material_record(mat)
         L = light_of.get(k)
         if L is None and name == "light":
@@ -361,7 +375,8 @@ def render_path(scene: dict, *, width: int, height: int, spp: int, max_depth: in
     count = total - first if count is None else count
     fsum = np.zeros((height, width, 3), np.float32)
     fw = np.zeros((height, width), np.float32)
-    st = _pt_lib().orc_render_path(_c(nodes), _c(pos), _c(idx), None, _c(tri_mesh), _c(meshes), len(meshes),
+    st = _pt_lib().orc_render_path(_c(nodes), _c(pos), _c(idx), None if nrm is None else _c(nrm), _c(tri_mesh),
+                                   _c(meshes), len(meshes),
                                    _c(mats), _c(light_arr), len(light_arr), _c(c2w), float(fov), width, height, spp,
                                    max_depth, filter_width, filter_width, int(first), int(count), _c(fsum), _c(fw))
     if st != 0:

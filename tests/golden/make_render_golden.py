@@ -41,6 +41,13 @@ CASES = [
     ("spheres_roughglass", {"kind": "spheres", "n_spheres": 10, "level": 3, "seed": 15,
                             "materials": ["roughglass"]},
      dict(width=128, height=96, spp=8, max_depth=8)),
+    # pbrt sphere / disk shapes (tessellated by both loaders) and a cone-sampled sphere light
+    ("shapes_sphere_light", {"kind": "shapes", "seed": 31}, dict(width=160, height=120, spp=8, max_depth=5)),
+    ("shapes_two_lights", {"kind": "shapes", "seed": 32, "quad_light": True},
+     dict(width=160, height=120, spp=8, max_depth=5)),
+    # the spheres_mixed scene with every triangle mesh in a binary PLY file ("plymesh")
+    ("spheres_mixed_ply", {"kind": "spheres", "n_spheres": 12, "level": 2, "seed": 5, "ply": True},
+     dict(width=128, height=96, spp=8, max_depth=8)),
     # the learning integrator (the .pbrt names it; both renderers read the Integrator line)
     ("room_rlpath_s16", {"kind": "room"}, dict(width=128, height=128, spp=16, max_depth=5, integrator="rlpath")),
     ("spheres_rlpath_s16", {"kind": "spheres", "n_spheres": 12, "level": 3, "seed": 5},
@@ -54,11 +61,18 @@ CASES = [
 def make_scene(gen: dict) -> dict:
     g = dict(gen)
     kind = g.pop("kind")
+    ply = g.pop("ply", False)
     if kind == "room":
-        return scenes.mini_room()
-    if "materials" in g:
-        g["materials"] = tuple(g["materials"])
-    return scenes.sphere_scene(**g)
+        sc = scenes.mini_room()
+    elif kind == "shapes":
+        sc = scenes.shapes_scene(**g)
+    else:
+        if "materials" in g:
+            g["materials"] = tuple(g["materials"])
+        sc = scenes.sphere_scene(**g)
+    if ply:
+        sc["write_ply"] = True
+    return sc
 
 
 def main(out: str):

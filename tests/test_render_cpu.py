@@ -31,7 +31,8 @@ def make_scene(gen):
 # agrees almost everywhere; glass and mirror chains amplify rounding (approximate device
 # maths vs IEEE host maths) into flipped lobe / roulette choices on a few percent of pixels.
 TOL = {"room": dict(exact=0.999, le2=0.9995, max_frac_gt8=0.0005),
-       "spheres": dict(exact=0.95, le2=0.985, max_frac_gt8=0.004)}
+       "spheres": dict(exact=0.95, le2=0.985, max_frac_gt8=0.004),
+       "shapes": dict(exact=0.95, le2=0.985, max_frac_gt8=0.004)}
 
 
 def check_against_png(img, ref, kind):
@@ -206,3 +207,103 @@ def test_golden_sphere_scenes_have_disjoint_lights():
             for j in range(i + 1, len(boxes)):
                 a, b = boxes[i], boxes[j]
                 assert not (a[0] < b[1] and b[0] < a[1] and a[2] < b[3] and b[2] < a[3]), (name, i, j)
+
+
+def _ply_text(P, faces, fmt, extra=True):
+    """A PLY of the given format with an extra vertex property and an extra element."""
+    import struct
+
+    head = ["ply", f"format {fmt} 1.0", "comment written by the test", f"element vertex {len(P)}",
+            "property float x", "property float y", "property float z"]
+    if extra:
+        head.append("property double confidence")
+    head += [f"element face {len(faces)}", "property list uchar int vertex_indices"]
+    if extra:
+        head += ["element edge 1", "property int vertex1", "property int vertex2"]
+    head.append("end_header")
+    out = ("\n".join(head) + "\n").encode()
+    if fmt == "ascii":
+        body = [" ".join(f"{c:.9g}" for c in p) + (" 0.5" if extra else "") for p in P]
+        body += [" ".join(map(str, [len(f)] + list(f))) for f in faces]
+        if extra:
+            body.append("0 1")
+        return out + ("\n".join(body) + "\n").encode()
+    e = "<" if fmt == "binary_little_endian" else ">"
+    for p in P:
+        out += struct.pack(e + "fff", *p) + (struct.pack(e + "d", 0.5) if extra else b"")
+    for f in faces:
+        out += struct.pack(e + "B" + "i" * len(f), len(f), *f)
+    if extra:
+        out += struct.pack(e + "ii", 0, 1)
+    return out
+
+
+def _scene_with_shape(tmp_path, shape_line, name="s.pbrt"):
+    text = ('LookAt 0 0 -3  0 0 0  0 1 0\nCamera "perspective" "float fov" [40]\n'
+            'Film "image" "integer xresolution" [32] "integer yresolution" [32]\n'
+            'Sampler "halton" "integer pixelsamples" [1]\nIntegrator "path" "integer maxdepth" [2]\nWorldBegin\n'
+            'AttributeBegin\nAreaLightSource "diffuse" "rgb L" [1 1 1]\n'
+            'Shape "trianglemesh" "integer indices" [0 1 2] "point P" [0 1 0 1 1 0 0 1 1]\nAttributeEnd\n'
+            f'AttributeBegin\nTranslate 0.25 -0.5 1\n{shape_line}\nAttributeEnd\nWorldEnd\n')
+    p = tmp_path / name
+    p.write_text(text)
+    return str(p)
+
+
+@pytest.mark.parametrize("fmt", ["ascii", "binary_little_endian", "binary_big_endian"])
+def test_ply_mesh_loads_like_the_inline_mesh(tmp_path, fmt):
+    """Core/TriangleMesh.cu:53-108: x/y/z of any PLY encoding, each face's first three indices
+    (a quad keeps one triangle), other properties and elements skipped; the CTM applies."""
+    import cavalry_b200 as cav
+
+    rng = np.random.default_rng(1)
+    P = rng.uniform(-1, 1, (7, 3)).astype(np.float32)
+    faces = [(0, 1, 2), (2, 3, 4, 5), (5, 6, 0)]
+    (tmp_path / "m.ply").write_bytes(_ply_text(P, faces, fmt))
+    a = cav.load_pbrt_triangles(_scene_with_shape(tmp_path, 'Shape "plymesh" "string filename" "m.ply"', "a.pbrt"))
+    flat = " ".join("%.9g" % c for c in P.reshape(-1))
+    b = cav.load_pbrt_triangles(_scene_with_shape(
+        tmp_path, f'Shape "trianglemesh" "integer indices" [0 1 2 2 3 4 5 6 0] "point P" [{flat}]', "b.pbrt"))
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert len(a[1]) == 1 + 3
+
+
+def test_ply_errors_are_reported(tmp_path):
+    import cavalry_b200 as cav
+
+    P = np.zeros((3, 3), np.float32)
+    (tmp_path / "short.ply").write_bytes(_ply_text(P, [(0, 1)], "ascii", extra=False))
+    with pytest.raises(cav.CavError, match="read ply file failed"):
+        cav.load_pbrt_triangles(_scene_with_shape(tmp_path, 'Shape "plymesh" "string filename" "short.ply"'))
+    with pytest.raises(cav.CavError, match="read ply file failed"):
+        cav.load_pbrt_triangles(_scene_with_shape(tmp_path, 'Shape "plymesh" "string filename" "missing.ply"'))
+    with pytest.raises(cav.CavError, match="ShapeMesh type not supported"):
+        cav.load_pbrt_triangles(_scene_with_shape(tmp_path, 'Shape "cylinder" "float radius" [1]'))
+
+
+def test_sphere_and_disk_shapes_follow_the_reference_tessellation(tmp_path):
+    """ShapeMesh/Sphere.cu:3-94 (2046 vertices, 2048 triangles) and ShapeMesh/Disk.cu:4-50
+    (361 vertices, 360 triangles), placed by the CTM; the scene generator's copies agree."""
+    import os
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    P, I, _ = cav.load_pbrt_triangles(_scene_with_shape(tmp_path, 'Shape "sphere" "float radius" [0.75]'))
+    assert len(I) == 1 + 2048 and len(P) == 3 + 2046
+    sp = P[3:] - np.array([0.25, -0.5, 1], np.float32)
+    assert np.allclose(np.linalg.norm(sp, axis=1), 0.75, atol=1e-6)
+    _, ref_p, ref_i = scenes.sphere_shape_mesh(0.75)
+    assert np.array_equal(I[1:] - 3, ref_i)
+    assert np.abs(sp - ref_p).max() < 1e-6
+    P, I, _ = cav.load_pbrt_triangles(_scene_with_shape(tmp_path, 'Shape "disk" "float radius" [0.5] "float height" [0.2]'))
+    assert len(I) == 1 + 360 and len(P) == 3 + 361
+    dp, di = scenes.disk_shape_mesh(0.5, 0.2)
+    assert np.array_equal(I[1:] - 3, di)
+    assert np.abs(P[3:] - np.array([0.25, -0.5, 1], np.float32) - dp).max() < 1e-6
+    sc = scenes.shapes_scene(31, quad_light=True)
+    path = str(tmp_path / "shapes.pbrt")
+    scenes.write_pbrt(path, sc, width=32, height=24, spp=1, max_depth=2)
+    P, I, _ = cav.load_pbrt_triangles(path)
+    assert os.path.exists(path) and np.abs(P[I] - sc["positions"][sc["indices"]]).max() < 1e-6
