@@ -237,7 +237,7 @@ class SceneInfo(ctypes.Structure):
                 ("bvh_rounds", ctypes.c_int), ("integrator", ctypes.c_int)]
 
 
-_INTEGRATORS = {None: 0, "path": -1, "rlpath": 1, "guided": 2}
+_INTEGRATORS = {None: 0, "path": -1, "rlpath": 1, "guided": 2, "directlighting": 3}
 RENDER_GRAPH = 1
 RENDER_FAST_TRACE = 2
 

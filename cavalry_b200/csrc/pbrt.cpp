@@ -428,6 +428,8 @@ struct Parser {
         scene.integrator = ov.integrator.empty() ? integrator.name : ov.integrator;
         if (scene.integrator == "path" || scene.integrator == "rlpath") {
             scene.max_depth = (int)integrator.params.num("maxdepth");
+        } else if (scene.integrator == "directlighting") {  // one bounce; maxdepth is not read
+            scene.max_depth = 1;
         } else {
             scene.integrator = "path";  // CreateIntegrator.cu:23-25
             scene.max_depth = 8;
@@ -756,7 +758,7 @@ extern "C" cav_status cav_pbrt_parse_info(const char* path, int spp_override, co
         info->meshes = (int)s.meshes.size();
         info->lights = (int)s.lights.size();
         info->bvh_rounds = -1;
-        info->integrator = s.integrator == "rlpath" ? 1 : 0;
+        info->integrator = s.integrator == "rlpath" ? 1 : (s.integrator == "directlighting" ? 3 : 0);
         if (camera_to_world16) std::memcpy(camera_to_world16, s.camera_to_world.data(), 64);
     } catch (const std::exception& e) {
         if (err && err_len > 0) {

@@ -88,8 +88,7 @@ __global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Que
         f3 incident = dot3(dir, ln) >= 0 ? mk(0, 0, 0) : ld3(L.L);
         if (isfinite(light_pdf)) {
             f3 wi = to_local(fr, dir);
-            float bsdf_pdf = B.pdf(wi, wo);
-            float w = mis_power(light_pdf, bsdf_pdf);
+            float w = S.direct ? 1.f : mis_power(light_pdf, B.pdf(wi, wo));
             float cosine = fabsf(dot3(dir, nrm));
             f3 mult = thr * (float)S.n_lights / light_pdf;
             contrib = incident * B.eval(wi, wo) * cosine * mult * w;
@@ -102,7 +101,7 @@ __global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Que
         }
         // ---- continuation (genNextRay :124-171)
         dim = dim0 + 8;
-        bool alive = true;
+        bool alive = !S.direct;
         if (depth > 3) {
             float q = 1;
             q = fminf(q, 1 - thr.x);
@@ -323,12 +322,12 @@ struct RayCapture {
 };
 
 cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
-                       cudaStream_t s, const RayCapture* cap = nullptr) {
+                       cudaStream_t s, const RayCapture* cap = nullptr, bool direct = false) {
     const cavpbrt::Scene& D = sc->desc;
     int W, H;
     film_size(sc, opts, W, H);
     const int spp = opts && opts->spp > 0 ? opts->spp : D.spp;
-    const int max_depth = opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth;
+    const int max_depth = direct ? 1 : (opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth);
     const int64_t pixels = (int64_t)W * H;
     const int64_t total = pixels * spp;
     int64_t chunk = opts && opts->max_paths_in_flight > 0 ? opts->max_paths_in_flight : (int64_t)1 << 22;
@@ -372,6 +371,7 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
     Q.counters = carve<uint32_t>(p, 16);
 
     DevScene S = dev_scene_of(sc);
+    S.direct = direct ? 1 : 0;
     Camera cam = camera_of(sc, W, H);
     const uint32_t tflags = opts && (opts->flags & CAV_RENDER_FAST_TRACE) ? CAV_TRACE_FAST : CAV_TRACE_EXACT;
     uint32_t counts[2];
@@ -842,7 +842,7 @@ cav_status cav_scene_info(const cav_scene* sc, cav_scene_info_t* info) {
     info->meshes = (int)sc->desc.meshes.size();
     info->lights = (int)sc->desc.lights.size();
     info->bvh_rounds = sc->bvh_rounds;
-    info->integrator = sc->desc.integrator == "rlpath" ? 1 : 0;
+    info->integrator = sc->desc.integrator == "rlpath" ? 1 : (sc->desc.integrator == "directlighting" ? 3 : 0);
     return CAV_OK;
 }
 
@@ -858,12 +858,13 @@ cav_status cav_render(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, 
     const int64_t pixels = (int64_t)W * H;
     CAV_CUDA(ctx, cudaMemsetAsync(film_sum, 0, sizeof(float) * 3 * pixels, s));
     CAV_CUDA(ctx, cudaMemsetAsync(film_weight, 0, sizeof(float) * pixels, s));
-    // integrator: the options' choice when given (> 0 selects rlpath), else the scene's
-    int integrator = sc->desc.integrator == "rlpath" ? 1 : 0;
+    // integrator: the options' choice when given (> 0 selects one), else the scene's
+    int integrator = sc->desc.integrator == "rlpath" ? 1 : (sc->desc.integrator == "directlighting" ? 3 : 0);
     if (opts && opts->integrator > 0) integrator = opts->integrator;
     if (opts && opts->integrator < 0) integrator = 0;
     if (integrator == 1) return cav::render_rlpath(ctx, sc, opts, film_sum, film_weight, s);
     if (integrator == 2) return cav_render_guided(ctx, sc, opts, nullptr, nullptr, film_sum, film_weight, s, nullptr);
+    if (integrator == 3) return cav::render_path(ctx, sc, opts, film_sum, film_weight, s, nullptr, true);
     if (integrator != 0) return cav::set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "unknown integrator");
     if (opts && (opts->flags & CAV_RENDER_GRAPH)) return cav::render_path_graph(ctx, sc, opts, film_sum, film_weight, s);
     return cav::render_path(ctx, sc, opts, film_sum, film_weight, s);

@@ -455,6 +455,9 @@ struct DevScene {
     const RMaterial* mats;
     const RLight* lights;
     int n_lights;
+    // DirectLightingIntegrator (Integrators/DirectLightingIntegrator.cu:22-89): emission plus
+    // one light sample per camera ray, without MIS weights and without a continuation
+    int direct;
     Halton halton;
 };
 
@@ -758,6 +761,7 @@ inline DevScene dev_scene_of(const cav_scene* sc) {
     S.mats = sc->d_mats;
     S.lights = sc->d_lights;
     S.n_lights = (int)sc->desc.lights.size();
+    S.direct = 0;
     S.halton = Halton{sc->d_primes, sc->d_perm_start, sc->d_perms};
     return S;
 }

@@ -200,14 +200,16 @@ typedef struct cav_scene_info_t {
     int width, height, spp, max_depth;
     int64_t triangles;
     int meshes, lights, bvh_rounds;
-    int integrator; /* 0 = path, 1 = rlpath */
+    int integrator; /* 0 = path, 1 = rlpath, 3 = directlighting */
 } cav_scene_info_t;
 
 typedef struct cav_render_opts {
     int spp;                     /* <= 0: the scene's Sampler "pixelsamples" */
     int max_depth;               /* <= 0: the scene's Integrator "maxdepth" */
-    int integrator;              /* 0: the scene's Integrator ("path" or "rlpath"); -1: path; 1: rlpath;
-                                    2: MLP-guided path (cav_render_guided with defaults) */
+    int integrator;              /* 0: the scene's Integrator ("path", "rlpath" or "directlighting");
+                                    -1: path; 1: rlpath; 2: MLP-guided path (cav_render_guided with
+                                    defaults); 3: direct lighting (emission + one light sample per
+                                    camera ray, no MIS, as DirectLightingIntegrator.cu) */
     int64_t max_paths_in_flight; /* <= 0: 4M; samples are rendered in chunks of this many paths */
     int width, height;           /* <= 0: the scene's Film resolution (the camera keeps its fov) */
     int flags;                   /* CAV_RENDER_GRAPH: capture one chunk's bounce chain as a CUDA graph and

@@ -531,6 +531,7 @@ typedef struct {
     const OMaterial* mats;
     const OLight* lights;
     int n_lights;
+    int direct; /* DirectLightingIntegrator.cu:22-89: one light sample, no MIS, no continuation */
     Halton h;
 } Scene;
 
@@ -667,8 +668,7 @@ static V3 trace_path(const Scene* S, uint64_t index, V3 ro, V3 rd, int max_depth
         V3 incident = vdot(dir, ln) >= 0 ? v3(0, 0, 0) : ld3(L->L);
         if (isfinite(lpdf)) {
             V3 wi = to_local(&fr, dir);
-            float bpdf = bsdf_pdf(&B, wi, wo);
-            float w = mis_power(lpdf, bpdf);
+            float w = S->direct ? 1.f : mis_power(lpdf, bsdf_pdf(&B, wi, wo));
             float cosine = fabsf(vdot(dir, nrm));
             V3 mult = vdivs(vs(thr, (float)S->n_lights), lpdf);
             V3 contrib = vs(vmul(vs(vmul(incident, bsdf_eval(&B, wi, wo)), cosine), mult), w);
@@ -728,7 +728,7 @@ int orc_render_path(const ONode* nodes, const float* pos, const int32_t* idx, co
                     const int32_t* tri_mesh, OMesh* meshes, int n_meshes, const OMaterial* mats,
                     const OLight* lights, int n_lights, const float* c2w, float fov_deg, int width, int height,
                     int spp, int max_depth, float xw, float yw, int64_t first, int64_t count, float* film_sum,
-                    float* film_w) {
+                    float* film_w, int direct) {
     if (n_lights <= 0 || width <= 0 || height <= 0 || spp <= 0) return -1;
     unsigned csr = _mm_getcsr();
     _mm_setcsr(csr | 0x8040); /* FTZ | DAZ, as the device build */
@@ -743,6 +743,8 @@ int orc_render_path(const ONode* nodes, const float* pos, const int32_t* idx, co
     S.mats = mats;
     S.lights = lights;
     S.n_lights = n_lights;
+    S.direct = direct;
+    if (direct) max_depth = 1;
     int64_t plen = orc_halton_tables(S.h.primes, S.h.start, NULL);
     S.h.perms = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)plen);
     orc_halton_tables(S.h.primes, S.h.start, S.h.perms);

@@ -250,7 +250,7 @@ def _pt_lib():
     L = oracle_lib()
     if not hasattr(L, "_pt_ready"):
         P, I, I64, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float
-        L.orc_render_path.argtypes = [P, P, P, P, P, P, I, P, P, I, P, F, I, I, I, I, F, F, I64, I64, P, P]
+        L.orc_render_path.argtypes = [P, P, P, P, P, P, I, P, P, I, P, F, I, I, I, I, F, F, I64, I64, P, P, I]
         L.orc_render_path.restype = I
         L.orc_roughness_to_alpha.argtypes = [F]
         L.orc_roughness_to_alpha.restype = F
@@ -329,10 +329,13 @@ def look_at_c2w(eye, look, up) -> np.ndarray:
 
 
 def render_path(scene: dict, *, width: int, height: int, spp: int, max_depth: int, first: int = 0,
-                count: int | None = None, filter_width: float = 1.0):
+                count: int | None = None, filter_width: float = 1.0, integrator: str = "path"):
     """Oracle render of a scene dict (the format of cavalry_b200.scenes, camera from
     scene["camera"] else the config-1 view): returns the float film (sum [H,W,3], weight
-    [H,W]) of camera samples [first, first + count)."""
+    [H,W]) of camera samples [first, first + count).  integrator "directlighting" restates
+    DirectLightingIntegrator.cu (one light sample per camera ray, no MIS)."""
+    if integrator not in ("path", "directlighting"):
+        raise ValueError(f"the oracle restates the path and direct-lighting integrators, not {integrator!r}")
     cam = dict(eye=(0.0, 0.0, -3.8), look=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), fov=40.0)
     cam.update(scene.get("camera", {}))
     eye, look, up, fov = cam["eye"], cam["look"], cam["up"], cam["fov"]
@@ -378,7 +381,8 @@ def render_path(scene: dict, *, width: int, height: int, spp: int, max_depth: in
     st = _pt_lib().orc_render_path(_c(nodes), _c(pos), _c(idx), None if nrm is None else _c(nrm), _c(tri_mesh),
                                    _c(meshes), len(meshes),
                                    _c(mats), _c(light_arr), len(light_arr), _c(c2w), float(fov), width, height, spp,
-                                   max_depth, filter_width, filter_width, int(first), int(count), _c(fsum), _c(fw))
+                                   max_depth, filter_width, filter_width, int(first), int(count), _c(fsum), _c(fw),
+                                   int(integrator == "directlighting"))
     if st != 0:
         raise RuntimeError(f"orc_render_path failed ({st})")
     return fsum, fw

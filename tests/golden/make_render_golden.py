@@ -48,6 +48,12 @@ CASES = [
     # the spheres_mixed scene with every triangle mesh in a binary PLY file ("plymesh")
     ("spheres_mixed_ply", {"kind": "spheres", "n_spheres": 12, "level": 2, "seed": 5, "ply": True},
      dict(width=128, height=96, spp=8, max_depth=8)),
+    # DirectLightingIntegrator: emission + one light sample per camera ray, no MIS
+    ("room_direct_s16", {"kind": "room"}, dict(width=256, height=256, spp=16, max_depth=5, integrator="directlighting")),
+    ("spheres_direct", {"kind": "spheres", "n_spheres": 12, "level": 2, "seed": 5},
+     dict(width=128, height=96, spp=8, max_depth=8, integrator="directlighting")),
+    ("shapes_direct", {"kind": "shapes", "seed": 32, "quad_light": True},
+     dict(width=160, height=120, spp=8, max_depth=5, integrator="directlighting")),
     # the learning integrator (the .pbrt names it; both renderers read the Integrator line)
     ("room_rlpath_s16", {"kind": "room"}, dict(width=128, height=128, spp=16, max_depth=5, integrator="rlpath")),
     ("spheres_rlpath_s16", {"kind": "spheres", "n_spheres": 12, "level": 3, "seed": 5},

@@ -14,11 +14,11 @@ sys.path.insert(0, str(ROOT / "tests" / "golden"))
 
 
 def render_cases():
-    """Path-integrator cases (the oracle restates the path integrator only)."""
+    """Path and direct-lighting cases (the oracle restates those two integrators)."""
     if not GOLDEN.exists():
         return []
     g = np.load(GOLDEN)
-    return [c for c in json.loads(str(g["meta"])) if c["render"].get("integrator", "path") == "path"]
+    return [c for c in json.loads(str(g["meta"])) if c["render"].get("integrator", "path") in ("path", "directlighting")]
 
 
 def make_scene(gen):
@@ -307,3 +307,16 @@ def test_sphere_and_disk_shapes_follow_the_reference_tessellation(tmp_path):
     scenes.write_pbrt(path, sc, width=32, height=24, spp=1, max_depth=2)
     P, I, _ = cav.load_pbrt_triangles(path)
     assert os.path.exists(path) and np.abs(P[I] - sc["positions"][sc["indices"]]).max() < 1e-6
+
+
+def test_parser_reads_the_direct_lighting_integrator(tmp_path):
+    """CreateIntegrator.cu:12-14: "directlighting" takes no maxdepth; the scene reports it as 3."""
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    path = str(tmp_path / "d.pbrt")
+    scenes.write_pbrt(path, scenes.mini_room(), width=32, height=32, spp=2, max_depth=7, integrator="directlighting")
+    info, _ = cav.parse_pbrt(path)
+    assert info.integrator == 3 and info.max_depth == 1
+    info, _ = cav.parse_pbrt(path, integrator="path")
+    assert info.integrator == 0 and info.max_depth == 7
