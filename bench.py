@@ -52,10 +52,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="soup", choices=["soup", "render", "serve", "guided", "mlp"],
+    p.add_argument("--workload", default="soup", choices=["soup", "render", "serve", "guided", "mlp", "capture"],
                    help="soup: BVH + 4M closest-hit rays (default); render: the 5.24M-triangle path-traced scene; "
                         "serve: a Poisson stream of render and ray-query jobs, merged server vs sequential loop")
     p.add_argument("--jobs", type=int, default=256, help="jobs in the served stream (serve workload)")
+    p.add_argument("--bounce", type=int, default=1, help="capture workload: which bounce's extend rays")
     p.add_argument("--no-reference", action="store_true", help="render workload: skip the reference's CUDA build")
     p.add_argument("--render-steps", type=int, default=1, help="timed full renders (render workload)")
     p.add_argument("--small", action="store_true", help="render workload at 1/16 size (smoke runs)")
@@ -628,6 +629,51 @@ def run_render(args):
     print(json.dumps(out))
 
 
+# ------------------------------------------------------------------------ captured-ray workload
+def run_capture(args):
+    """The renderer's own extend rays of one bounce on the icosphere scene (64 spheres,
+    level 6, or level 5 with --small; seed 9; 3 treelet rounds), traced alone by the exact
+    and the fast (compressed 8-wide) modes with default launch shapes: one warm-up and three
+    timed launches each (CUDA events), then the instrumented visit counts."""
+    import tempfile
+
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    level = 5 if args.small else 6
+    W, H = (640, 360) if args.small else (1920, 1080)
+    tmp = tempfile.mkdtemp()
+    pbrt = os.path.join(tmp, "spheres.pbrt")
+    scenes.write_pbrt(pbrt, scenes.sphere_scene(64, level, seed=9), width=W, height=H, spp=8, max_depth=8)
+    ctx = cav.Context(0)
+    sc = ctx.load_pbrt(pbrt, bvh_rounds=3)
+    sc.render(spp=1)
+    rays = sc.capture_rays(args.bounce, capacity=1 << 22)
+    bvh = sc.bvh()
+    out = {"metric": "closest-hit Mrays/s (captured extend rays)", "unit": "Mrays/s", "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded icosphere scene, renderer's rays)",
+           "config": {"workload": f"spheres_64x{20 * 4 ** level}_tris_bounce{args.bounce}_rays",
+                      "rays": int(len(rays)), "treelet_rounds": 3}}
+    for name, fl in (("fast", cav.TRACE_FAST), ("exact", cav.TRACE_EXACT)):
+        bvh.trace_closest(rays, flags=fl)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(3):
+            bvh.trace_closest(rays, flags=fl)
+        b.record()
+        torch.cuda.synchronize()
+        out[name] = {"mrays_s": round(3 * len(rays) / (a.elapsed_time(b) * 1e-3) / 1e6, 1)}
+    for name, fl in (("fast", cav.TRACE_FAST), ("exact", cav.TRACE_EXACT)):
+        nodes, tris = bvh.trace_stats(rays, flags=fl)
+        out[name]["nodes_per_ray"] = round(nodes / len(rays), 3)
+        out[name]["tris_per_ray"] = round(tris / len(rays), 3)
+    out["value"] = out["fast"]["mrays_s"]
+    ctx.sync_check()
+    print(json.dumps(out))
+
+
 # ------------------------------------------------------------------------ serve workload
 def run_serve(args):
     """Served stream: jobs arrive as a Poisson process (mean gap 20 ms, seed 4).  Scenes are
@@ -873,6 +919,8 @@ def main():
         run_guided(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "capture":
+        run_capture(args)
     elif args.workload == "render":
         run_render(args)
     elif args.impl == "reference":
