@@ -245,7 +245,7 @@ RENDER_FAST_TRACE = 2
 class RenderOpts(ctypes.Structure):
     _fields_ = [("spp", ctypes.c_int), ("max_depth", ctypes.c_int), ("integrator", ctypes.c_int),
                 ("max_paths_in_flight", ctypes.c_int64), ("width", ctypes.c_int), ("height", ctypes.c_int),
-                ("flags", ctypes.c_int)]
+                ("flags", ctypes.c_int), ("sample_begin", ctypes.c_int64), ("sample_end", ctypes.c_int64)]
 
 
 def parse_pbrt(path: str, spp: int = -1, integrator: str | None = None) -> tuple[SceneInfo, np.ndarray]:
@@ -315,16 +315,20 @@ class Scene:
         return out
 
     def render(self, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0, integrator: str | None = None,
-               width: int = 0, height: int = 0, graph: bool = False, fast_trace: bool = False):
+               width: int = 0, height: int = 0, graph: bool = False, fast_trace: bool = False,
+               sample_range: tuple[int, int] | None = None):
         """Render to host arrays; returns (film_sum [H,W,3], film_weight [H,W], ms).  integrator:
-        None = the scene's, "path" or "rlpath"; width/height override the Film resolution."""
+        None = the scene's, "path", "rlpath", "guided" or "directlighting"; width/height override
+        the Film resolution; sample_range = (begin, end) renders only those camera samples
+        (pixel-major numbering), whose films sum to the whole render's."""
         inf = self.info()
         W, H = (width, height) if width > 0 and height > 0 else (inf.width, inf.height)
         s = np.zeros((H, W, 3), np.float32)
         w = np.zeros((H, W), np.float32)
         ms = np.zeros(1, np.float32)
+        b, e = sample_range if sample_range is not None else (0, 0)
         opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height,
-                          (RENDER_GRAPH if graph else 0) | (RENDER_FAST_TRACE if fast_trace else 0))
+                          (RENDER_GRAPH if graph else 0) | (RENDER_FAST_TRACE if fast_trace else 0), b, e)
         st = lib().cav_render_to_host(self.ctx.handle, self.handle, ctypes.addressof(opts), s.ctypes.data,
                                       w.ctypes.data, ms.ctypes.data)
         self.ctx._check(st, "cav_render_to_host")
@@ -332,13 +336,14 @@ class Scene:
 
     def render_into(self, film_sum, film_weight, spp: int = 0, max_depth: int = 0, max_paths_in_flight: int = 0,
                     stream=None, integrator: str | None = None, width: int = 0, height: int = 0, graph: bool = False,
-                    fast_trace: bool = False):
+                    fast_trace: bool = False, sample_range: tuple[int, int] | None = None):
         """Render into DEVICE films (pointers, or objects with data_ptr(): 3 + 1 floats per
         pixel), stream-ordered on `stream` (a pointer, an object with cuda_stream, or None)."""
         ptr = lambda x: x if isinstance(x, int) else x.data_ptr()  # noqa: E731
         st_ptr = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
+        b, e = sample_range if sample_range is not None else (0, 0)
         opts = RenderOpts(spp, max_depth, _INTEGRATORS[integrator], max_paths_in_flight, width, height,
-                          (RENDER_GRAPH if graph else 0) | (RENDER_FAST_TRACE if fast_trace else 0))
+                          (RENDER_GRAPH if graph else 0) | (RENDER_FAST_TRACE if fast_trace else 0), b, e)
         st = lib().cav_render(self.ctx.handle, self.handle, ctypes.addressof(opts), ptr(film_sum), ptr(film_weight),
                               st_ptr)
         self.ctx._check(st, "cav_render")

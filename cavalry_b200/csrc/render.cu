@@ -330,8 +330,13 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
     const int max_depth = direct ? 1 : (opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth);
     const int64_t pixels = (int64_t)W * H;
     const int64_t total = pixels * spp;
+    // the camera samples of this render: all, or one shard [sample_begin, sample_end)
+    const int64_t s_begin = opts && opts->sample_begin > 0 ? opts->sample_begin : 0;
+    const int64_t s_end = opts && opts->sample_end > 0 ? std::min(opts->sample_end, total) : total;
+    if (s_begin > s_end) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "sample_begin after sample_end");
+    if (s_begin == s_end) return CAV_OK;
     int64_t chunk = opts && opts->max_paths_in_flight > 0 ? opts->max_paths_in_flight : (int64_t)1 << 22;
-    chunk = std::min(chunk, total);
+    chunk = std::min(chunk, s_end - s_begin);
     // path state + queues for `chunk` paths
     size_t need = 0;
     auto acc = [&](size_t bytes) { need += bytes + 256; };
@@ -379,10 +384,10 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
     log.reset();
     log.start = log.next();
     CAV_CUDA(ctx, cudaEventRecord(log.start, s));
-    log.paths = total;
+    log.paths = s_end - s_begin;
     if (cap && cap->count) *cap->count = 0;
-    for (int64_t first = 0; first < total; first += chunk) {
-        const int64_t m = std::min(chunk, total - first);
+    for (int64_t first = s_begin; first < s_end; first += chunk) {
+        const int64_t m = std::min(chunk, s_end - first);
         k_generate<<<div_up(m, kThreads), kThreads, 0, s>>>(cam, S.halton, spp, first, m, P, Q);
         int64_t n = m;
         // genCameraSampleSPPs stores the sampling state in the CameraSample BEFORE drawing the
@@ -390,7 +395,7 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
         // first bounce starts again at dimension 0.
         int dim0 = 0;
         for (int depth = 0; n > 0 && depth < max_depth; ++depth) {
-            if (cap && first == 0 && depth == cap->depth && cap->out) {
+            if (cap && first == s_begin && depth == cap->depth && cap->out) {
                 const int64_t k = std::min(n, cap->capacity);
                 CAV_CUDA(ctx, cudaMemcpyAsync(cap->out, Q.rays, sizeof(cav_ray) * k, cudaMemcpyDeviceToDevice, s));
                 if (cap->count) *cap->count = k;
@@ -862,11 +867,15 @@ cav_status cav_render(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, 
     int integrator = sc->desc.integrator == "rlpath" ? 1 : (sc->desc.integrator == "directlighting" ? 3 : 0);
     if (opts && opts->integrator > 0) integrator = opts->integrator;
     if (opts && opts->integrator < 0) integrator = 0;
+    const bool ranged = opts && (opts->sample_begin > 0 || opts->sample_end > 0);
+    if (ranged && (integrator == 1 || integrator == 2))
+        return cav::set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "sample ranges are for the path and direct integrators");
     if (integrator == 1) return cav::render_rlpath(ctx, sc, opts, film_sum, film_weight, s);
     if (integrator == 2) return cav_render_guided(ctx, sc, opts, nullptr, nullptr, film_sum, film_weight, s, nullptr);
     if (integrator == 3) return cav::render_path(ctx, sc, opts, film_sum, film_weight, s, nullptr, true);
     if (integrator != 0) return cav::set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "unknown integrator");
-    if (opts && (opts->flags & CAV_RENDER_GRAPH)) return cav::render_path_graph(ctx, sc, opts, film_sum, film_weight, s);
+    if (opts && (opts->flags & CAV_RENDER_GRAPH) && !ranged)
+        return cav::render_path_graph(ctx, sc, opts, film_sum, film_weight, s);
     return cav::render_path(ctx, sc, opts, film_sum, film_weight, s);
 }
 

@@ -215,6 +215,12 @@ typedef struct cav_render_opts {
     int flags;                   /* CAV_RENDER_GRAPH: capture one chunk's bounce chain as a CUDA graph and
                                     replay it per chunk, with queue sizes kept on the device (no host round
                                     trip per bounce; path integrator; per-stage times not recorded) */
+    int64_t sample_begin;        /* camera samples [sample_begin, sample_end) of the render, numbered
+                                    pixel-major (pixel * spp + s, the Halton index); sample_end <= 0: to the
+                                    last.  A sub-range renders exactly those samples' contributions, so
+                                    films of disjoint ranges sum to the whole render's (path and direct
+                                    integrators; a shard of a multi-GPU render) */
+    int64_t sample_end;
 } cav_render_opts;
 enum { CAV_RENDER_GRAPH = 1, CAV_RENDER_FAST_TRACE = 2 /* trace with CAV_TRACE_FAST (path integrator) */ };
 

@@ -235,3 +235,39 @@ def test_graph_replayed_render_matches(ctx, tmp_path, chunk):
     assert np.array_equal(w1, w2)
     assert np.allclose(s1, s2, rtol=2e-5, atol=1e-6)
     assert st2.closest_rays == st1.closest_rays and st2.shadow_rays == st1.shadow_rays
+
+
+def test_sample_ranges_sum_to_the_whole_render(ctx, tmp_path):
+    """Films of disjoint camera-sample ranges sum to the whole render's (the shard of a
+    multi-GPU render); one NCCL process group of one rank runs the sharded path end to end."""
+    import os
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from cavalry_b200 import distributed
+
+    case = next(c for c in render_cases() if c["name"] == "spheres_mixed")
+    sc, _ = load(ctx, tmp_path, "ranges", make_scene(case["gen"]), case["render"])
+    s, w, _ = sc.render()
+    info = sc.info()
+    total = info.width * info.height * info.spp
+    cut = total // 3 + 17
+    s1, w1, _ = sc.render(sample_range=(0, cut))
+    s2, w2, _ = sc.render(sample_range=(cut, total))
+    assert np.array_equal(w1 + w2, w)
+    assert np.allclose(s1 + s2, s, rtol=1e-5, atol=1e-5)
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        fs, fw = distributed.render_scene_sharded(sc)
+        assert np.array_equal(fw.view(info.height, info.width).cpu().numpy(), w)
+        assert np.allclose(fs.view(info.height, info.width, 3).cpu().numpy(), s, rtol=1e-5, atol=1e-5)
+    finally:
+        dist.destroy_process_group()
+    with pytest.raises(Exception, match="sample ranges"):
+        sc.render(integrator="rlpath", sample_range=(0, 10))
+    ctx.sync_check()
