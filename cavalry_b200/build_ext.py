@@ -65,7 +65,7 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
     if LIB.exists() and LIB.stat().st_mtime >= max(o.stat().st_mtime for o in objs):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs)]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lz"]  # zlib: PNG textures
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -182,7 +182,7 @@ __global__ void k_g_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Q
         P.result[3 * path] = res.x;
         P.result[3 * path + 1] = res.y;
         P.result[3 * path + 2] = res.z;
-        const Bsdf B = make_bsdf(S.mats[M.material]);
+        const Bsdf B = material_bsdf(S, S.mats[M.material], prim, u, v);
         const Frame fr = make_frame(nrm);
         const f3 wo = to_local(fr, rd * -1.f);
         const bool guided = alpha > 0.f && guidable(B);
@@ -197,13 +197,10 @@ __global__ void k_g_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Q
         int dim = dim0;
         int li = halton_int(S.halton, index, dim, S.n_lights);
         dim += 4;
-        const RLight& L = S.lights[li];
-        const RMesh& LM = S.meshes[L.mesh];
-        const LightPoint lpt = sample_light_surface(S, LM, pos, index, dim);  // 2 or 3 of the 3 reserved
-        const f3 lp = lpt.p, ln = lpt.n;
-        const float light_pdf = lpt.pdf;
-        f3 dir = normalize3(lp - pos);
-        f3 incident = dot3(dir, ln) >= 0 ? mk(0, 0, 0) : ld3(L.L);
+        const LightSample ls = sample_light(S, S.lights[li], pos, index, dim);  // 2 or 3 of the 3 reserved
+        const float light_pdf = ls.pdf;
+        const f3 dir = ls.dir;
+        const f3 incident = ls.incident;
         if (isfinite(light_pdf)) {
             f3 wi = to_local(fr, dir);
             float w = mis_power(light_pdf, cont_pdf(dir, wi));
@@ -213,8 +210,8 @@ __global__ void k_g_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Q
             if (!all_zero(contrib)) {
                 emit_shadow = true;
                 shadow = cav_ray{pos.x, pos.y, pos.z, 0.f, dir.x, dir.y, dir.z, INFINITY};
-                limit = length3(lp - pos);
-                excl = make_int2(mesh, L.mesh);
+                limit = ls.dist;
+                excl = make_int2(mesh, ls.target);
             }
         }
         // ---- continuation
@@ -273,6 +270,13 @@ __global__ void k_g_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Q
                 next = cav_ray{no.x, no.y, no.z, 0.f, nd.x, nd.y, nd.z, INFINITY};
             }
         }
+    }
+    if (valid && !hit && S.env >= 0) {  // rays leaving the scene see the environment
+        const cav_ray r = Q.rays[j];
+        const f3 e = env_eval(S, S.lights[S.env], mk(r.dx, r.dy, r.dz)) * ld3(P.throughput + 3 * path);
+        P.result[3 * path] += e.x;
+        P.result[3 * path + 1] += e.y;
+        P.result[3 * path + 2] += e.z;
     }
     uint32_t ks = warp_append(Q.counters + 1, emit_shadow);
     if (emit_shadow) {

@@ -25,6 +25,7 @@
 #include <filesystem>
 #include <fstream>
 #include <memory>
+#include <map>
 #include <set>
 #include <sstream>
 
@@ -518,8 +519,16 @@ struct Parser {
             m.kd[0] = m.kd[1] = m.kd[2] = 1.f;
             rgb(p, "Kd", m.kd);
         }
+        // "texture Kd": MatteMaterial multiplies its colour by the texel, Plastic and Substrate
+        // take the texel as their diffuse colour (Materials/*.h createFromParams)
+        if ((m.type == kMatte || m.type == kPlastic || m.type == kSubstrate) && p.has_string("Kd")) {
+            auto it = texture_names.find(p.str("Kd"));
+            if (it == texture_names.end()) throw ParseError("texture not found: " + p.str("Kd"));
+            m.kd_texture = it->second;
+        }
         return m;
     }
+    std::map<std::string, int> texture_names;
 
     int add_material(const Material& m) {
         scene.materials.push_back(m);
@@ -580,6 +589,7 @@ struct Parser {
                         put_positions(pm.positions);
                         put_indices(pm.indices);
                         if (!pm.normals.empty()) put_normals(pm.normals);
+                        mesh.uvs = pm.uvs;
                     } else if (d.params.has_list("P") && d.params.has_list("indices")) {
                         put_positions(d.params.list("P"));
                         const auto& I = d.params.list("indices");
@@ -587,6 +597,11 @@ struct Parser {
                         for (size_t k = 0; k < ii.size(); ++k) ii[k] = (int)I[k];
                         put_indices(ii);
                         if (d.params.has_list("N")) put_normals(d.params.list("N"));
+                        if (d.params.has_list("uv")) {
+                            const auto& uv = d.params.list("uv");
+                            if (uv.size() < mesh.positions.size() / 3 * 2) throw ParseError("uv needs 2 values per vertex");
+                            mesh.uvs.assign(uv.begin(), uv.begin() + (long)(mesh.positions.size() / 3 * 2));
+                        }
                     } else {
                         throw ParseError("No valid inputs for triangle mesh");
                     }
@@ -641,9 +656,24 @@ struct Parser {
                 else if (d.params.has_list("l")) rgb(d.params, "l", l.L);
                 scene.lights.push_back(l);
                 next_shape_light = true;
-            } else if (w == "LightSource") {
+            } else if (w == "LightSource") {  // Lights/LightObject.h:89-127, Parsing.cu:336-342
                 ObjectDef d = object();
-                throw ParseError("unsupported light source: " + d.name + " (only diffuse area lights)");
+                Light l;
+                l.kind = 1;
+                if (d.params.has_list("L")) rgb(d.params, "L", l.L);
+                else if (d.params.has_list("l")) rgb(d.params, "l", l.L);
+                l.world_to_light = inverse(xf);
+                if (d.name == "infinite") {
+                    if (d.params.has_list("scale")) rgb(d.params, "scale", l.L);
+                    if (d.params.has_string("mapname")) {
+                        scene.textures.push_back(load_texture_image((base / d.params.str("mapname")).string()));
+                        l.texture = (int)scene.textures.size() - 1;
+                    }
+                    scene.environment = (int)scene.lights.size();
+                } else {  // an unrecognised source stays in the light list as a black environment
+                    l.L[0] = l.L[1] = l.L[2] = 0.f;
+                }
+                scene.lights.push_back(l);
             } else if (transform(xf)) {
             } else if (w == "MakeNamedMaterial") {
                 ObjectDef d = object();
@@ -665,8 +695,13 @@ struct Parser {
             } else if (w == "ReverseOrientation") {
                 ++i;
                 reverse = true;
-            } else if (w == "Texture") {
-                throw ParseError("textures are not supported by this renderer");
+            } else if (w == "Texture") {  // Core/Texture.cu:12-25: an image, or one black texel
+                ObjectDef d = object();
+                TextureImage t;
+                if (d.params.has_string("filename"))
+                    t = load_texture_image((base / d.params.str("filename")).string());
+                scene.textures.push_back(std::move(t));
+                texture_names[d.name] = (int)scene.textures.size() - 1;
             } else {
                 skip_object();
             }
@@ -684,9 +719,9 @@ Scene load_string(const std::string& text, const std::string& base_dir, const Ov
     bool next_light = false;
     p.world(identity(), -1, next_light, true);
     if (scene.meshes.empty()) throw ParseError("the scene has no shapes");
-    if (scene.lights.empty()) throw ParseError("the scene has no area lights");
+    if (scene.lights.empty()) throw ParseError("the scene has no lights");
     for (const Light& l : scene.lights)
-        if (l.mesh < 0) throw ParseError("AreaLightSource without a following Shape");
+        if (l.kind == 0 && l.mesh < 0) throw ParseError("AreaLightSource without a following Shape");
     return scene;
 }
 

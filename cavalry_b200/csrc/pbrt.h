@@ -53,11 +53,21 @@ struct Material {
     float mirror_kr = 0.9f;
     bool has_f0 = false;             // metal: Fresnel f0 from a complex IOR (or the copper default)
     float f0[3] = {0, 0, 0};
+    int kd_texture = -1;             // matte / plastic / substrate "texture Kd": index into Scene::textures
 };
+
+// An 8-bit RGBA image texture as the reference holds it (Core/Texture.h: uchar4 texels,
+// bilinear filtering, wrapped normalized coordinates), rows bottom-up after the load flip.
+struct TextureImage {
+    int width = 1, height = 1;
+    std::vector<unsigned char> rgba{0, 0, 0, 0};
+};
+TextureImage load_texture_image(const std::string& path);
 
 struct Mesh {
     std::vector<float> positions;  // world space (transform applied), 3 per vertex
     std::vector<float> normals;    // 3 per vertex, or empty
+    std::vector<float> uvs;        // 2 per vertex ("uv" / PLY u v), or empty
     std::vector<int> indices;      // 3 per triangle
     bool reverse_orientation = false;
     int material = 0;
@@ -82,7 +92,11 @@ void disk_mesh(float radius, float height, std::vector<float>& pos, std::vector<
 
 struct Light {
     float L[3] = {1, 1, 1};
-    int mesh = -1;
+    int mesh = -1;     // diffuse area light: its mesh
+    int kind = 0;      // 0 diffuse area light; 1 environment (LightSource "infinite", or an
+                       // unrecognised LightSource, which the reference keeps as a black one)
+    int texture = -1;  // environment: "mapname" image, index into Scene::textures
+    Mat4 world_to_light{};
 };
 
 struct Scene {
@@ -100,6 +114,8 @@ struct Scene {
     std::vector<Material> materials;
     std::vector<Mesh> meshes;
     std::vector<Light> lights;
+    std::vector<TextureImage> textures;
+    int environment = -1;  // the light that rays leaving the scene see (the last "infinite")
 };
 
 struct Overrides {

@@ -71,7 +71,7 @@ __global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Que
         P.result[3 * path] = res.x;
         P.result[3 * path + 1] = res.y;
         P.result[3 * path + 2] = res.z;
-        const Bsdf B = make_bsdf(S.mats[M.material]);
+        const Bsdf B = material_bsdf(S, S.mats[M.material], prim, u, v);
         const Frame fr = make_frame(nrm);
         const f3 wo_world = rd * -1.f;
         const f3 wo = to_local(fr, wo_world);
@@ -79,28 +79,24 @@ __global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Que
         int dim = dim0;
         int li = halton_int(S.halton, index, dim, S.n_lights);
         dim += 4;  // rand4, drawn and unused by the reference
-        const RLight& L = S.lights[li];
-        const RMesh& LM = S.meshes[L.mesh];
-        const LightPoint lpt = sample_light_surface(S, LM, pos, index, dim);
-        const f3 lp = lpt.p, ln = lpt.n;
-        const float light_pdf = lpt.pdf;
-        f3 dir = normalize3(lp - pos);
-        f3 incident = dot3(dir, ln) >= 0 ? mk(0, 0, 0) : ld3(L.L);
+        const LightSample ls = sample_light(S, S.lights[li], pos, index, dim);
+        const float light_pdf = ls.pdf;
+        const f3 dir = ls.dir;
         if (isfinite(light_pdf)) {
             f3 wi = to_local(fr, dir);
             float w = S.direct ? 1.f : mis_power(light_pdf, B.pdf(wi, wo));
             float cosine = fabsf(dot3(dir, nrm));
             f3 mult = thr * (float)S.n_lights / light_pdf;
-            contrib = incident * B.eval(wi, wo) * cosine * mult * w;
+            contrib = ls.incident * B.eval(wi, wo) * cosine * mult * w;
             if (!all_zero(contrib)) {
                 emit_shadow = true;
                 shadow = cav_ray{pos.x, pos.y, pos.z, 0.f, dir.x, dir.y, dir.z, INFINITY};
-                limit = length3(lp - pos);
-                excl = make_int2(mesh, L.mesh);
+                limit = ls.dist;
+                excl = make_int2(mesh, ls.target);
             }
         }
         // ---- continuation (genNextRay :124-171)
-        dim = dim0 + 8;
+        dim = dim0 + S.cont_dim;
         bool alive = !S.direct;
         if (depth > 3) {
             float q = 1;
@@ -130,6 +126,13 @@ __global__ void k_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Que
                 next = cav_ray{no.x, no.y, no.z, 0.f, nd.x, nd.y, nd.z, INFINITY};
             }
         }
+    }
+    if (valid && !hit && S.env >= 0) {  // intersectScene :111-116: the environment, no MIS weight
+        const cav_ray r = Q.rays[j];
+        const f3 e = env_eval(S, S.lights[S.env], mk(r.dx, r.dy, r.dz)) * ld3(P.throughput + 3 * path);
+        P.result[3 * path] += e.x;
+        P.result[3 * path + 1] += e.y;
+        P.result[3 * path + 2] += e.z;
     }
     uint32_t ks = warp_append(Q.counters + 1, emit_shadow);
     if (emit_shadow) {
@@ -267,6 +270,7 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
         r.alpha_v = m.alpha_v;
         r.eta = m.eta;
         r.mirror_kr = m.mirror_kr;
+        r.kd_tex = m.kd_texture;
         for (int k = 0; k < 3; ++k) {  // Fresnel::createFromIOR (BSDFs/Fresnel.h:27-31), host float
             float t = (m.eta - 1.f) / (m.eta + 1.f);
             r.f0[k] = m.has_f0 ? m.f0[k] : t * t;  // metal: its complex-IOR (or copper) f0
@@ -274,7 +278,25 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
         mats.push_back(r);
     }
     std::vector<RLight> lights;
-    for (const auto& l : D.lights) lights.push_back(RLight{{l.L[0], l.L[1], l.L[2]}, l.mesh});
+    for (const auto& l : D.lights) {
+        RLight r{};
+        for (int k = 0; k < 3; ++k) r.L[k] = l.L[k];
+        r.mesh = l.mesh;
+        r.kind = l.kind == 1 ? kLightEnvironment : kLightArea;
+        r.tex = l.texture;
+        for (int row = 0; row < 3; ++row)  // glm::mat3(worldToLight): the upper-left 3x3
+            for (int c = 0; c < 3; ++c) r.w2l[row * 3 + c] = l.world_to_light[c * 4 + row];
+        lights.push_back(r);
+    }
+    // per-vertex texture coordinates, zero for meshes without them
+    std::vector<float> uv;
+    bool any_uv = false;
+    for (const auto& m : D.meshes) any_uv |= !m.uvs.empty();
+    if (any_uv)
+        for (const auto& m : D.meshes) {
+            if (m.uvs.empty()) uv.insert(uv.end(), m.positions.size() / 3 * 2, 0.f);
+            else uv.insert(uv.end(), m.uvs.begin(), m.uvs.end());
+        }
     std::vector<uint32_t> primes, start;
     std::vector<uint16_t> perms;
     build_halton_tables(primes, start, perms);
@@ -293,7 +315,43 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
         cav_scene_free(sc);
         return st;
     }
-    if (any_normals && (st = upload(ctx, (void**)&sc->d_nrm, nrm.data(), nrm.size() * 4))) {
+    if ((any_normals && (st = upload(ctx, (void**)&sc->d_nrm, nrm.data(), nrm.size() * 4))) ||
+        (any_uv && (st = upload(ctx, (void**)&sc->d_uv, uv.data(), uv.size() * 4)))) {
+        cav_scene_free(sc);
+        return st;
+    }
+    // image textures as the reference creates them (Core/Texture.h allocate): uchar4 texels
+    // read as normalized floats, bilinear filtering, wrapped normalized coordinates
+    for (const auto& t : D.textures) {
+        cudaChannelFormatDesc fmt = cudaCreateChannelDesc<uchar4>();
+        cudaArray_t arr = nullptr;
+        if (cudaMallocArray(&arr, &fmt, t.width, t.height) != cudaSuccess) {
+            cudaGetLastError();
+            cav_scene_free(sc);
+            return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "texture allocation failed");
+        }
+        sc->tex_arrays.push_back(arr);
+        cudaMemcpy2DToArray(arr, 0, 0, t.rgba.data(), (size_t)4 * t.width, (size_t)4 * t.width, t.height,
+                            cudaMemcpyHostToDevice);
+        cudaResourceDesc res{};
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = arr;
+        cudaTextureDesc td{};
+        td.addressMode[0] = cudaAddressModeWrap;
+        td.addressMode[1] = cudaAddressModeWrap;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeNormalizedFloat;
+        td.normalizedCoords = 1;
+        cudaTextureObject_t obj = 0;
+        if (cudaCreateTextureObject(&obj, &res, &td, nullptr) != cudaSuccess) {
+            cudaGetLastError();
+            cav_scene_free(sc);
+            return set_error(ctx, CAV_ERR_CUDA, "texture object creation failed");
+        }
+        sc->tex_objects.push_back(obj);
+    }
+    if (!sc->tex_objects.empty() &&
+        (st = upload(ctx, (void**)&sc->d_tex, sc->tex_objects.data(), sc->tex_objects.size() * sizeof(cudaTextureObject_t)))) {
         cav_scene_free(sc);
         return st;
     }
@@ -429,7 +487,7 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
             std::swap(Q.active, Q.next_active);
             std::swap(Q.rays, Q.next_rays);
             n = counts[0];
-            dim0 += 8 + 2 + (depth > 3 ? 1 : 0);
+            dim0 += S.cont_dim + 2 + (depth > 3 ? 1 : 0);
         }
         k_film<<<div_up(m, kThreads), kThreads, 0, s>>>(m, P, W, H, D.filter_xwidth, D.filter_ywidth,
                                                          d_sum, d_wsum);
@@ -572,7 +630,7 @@ cav_status render_path_graph(cav_ctx* ctx, cav_scene* sc, const cav_render_opts*
             k_add_direct<<<blocks, kThreads, 0, s>>>(0, P, Q, cnt + 2 * depth + 1);
             std::swap(Q.active, Q.next_active);
             std::swap(Q.rays, Q.next_rays);
-            dim0 += 8 + 2 + (depth > 3 ? 1 : 0);
+            dim0 += S.cont_dim + 2 + (depth > 3 ? 1 : 0);
         }
         k_film<<<blocks, kThreads, 0, s>>>(0, P, W, H, D.filter_xwidth, D.filter_ywidth, d_sum, d_wsum, d_fc);
         k_chunk_end<<<1, 1, 0, s>>>(d_idx, cnt, max_depth, totals);
@@ -754,7 +812,7 @@ cav_status path_job_advance(PathJob* J, cudaStream_t s, bool* finished) {
     std::swap(J->Q.active, J->Q.next_active);
     std::swap(J->Q.rays, J->Q.next_rays);
     J->n = J->h_counts[0];
-    J->dim0 += 8 + 2 + (J->depth > 3 ? 1 : 0);
+    J->dim0 += J->S.cont_dim + 2 + (J->depth > 3 ? 1 : 0);
     J->depth += 1;
     if (J->n <= 0 || J->depth >= J->max_depth) {
         const cavpbrt::Scene& D = J->sc->desc;
@@ -824,6 +882,10 @@ cav_status cav_scene_free(cav_scene* sc) {
     cudaFree(sc->d_meshes);
     cudaFree(sc->d_mats);
     cudaFree(sc->d_lights);
+    cudaFree(sc->d_uv);
+    for (cudaTextureObject_t t : sc->tex_objects) cudaDestroyTextureObject(t);
+    for (cudaArray_t a : sc->tex_arrays) cudaFreeArray(a);
+    cudaFree(sc->d_tex);
     cudaFree(sc->d_primes);
     cudaFree(sc->d_perm_start);
     cudaFree(sc->d_perms);

@@ -458,6 +458,14 @@ struct DevScene {
     // DirectLightingIntegrator (Integrators/DirectLightingIntegrator.cu:22-89): emission plus
     // one light sample per camera ray, without MIS weights and without a continuation
     int direct;
+    const float* uv;                  // 2 per vertex, or null
+    const cudaTextureObject_t* tex;   // image textures
+    int env;                          // the environment light rays leaving the scene see, or -1
+    // First dimension of a bounce's continuation, relative to the bounce's first: randInt +
+    // rand4 + the light sample, synchronised to the maximum over the bounce's paths.  An area
+    // light draws 3 (a triangle and a point; see sample_light_surface), an environment 2
+    // (rand2), so 8 whenever the scene has an area light and 7 with environments only.
+    int cont_dim;
     Halton halton;
 };
 
@@ -575,6 +583,84 @@ __device__ inline float light_surface_pdf(const RMesh& LM, f3 o, f3 p, f3 n) {
     const f3 l2s = o - p;
     const float cosine = fabsf(dot3(n, normalize3(l2s)));
     return dot3(l2s, l2s) / (cosine * LM.area);
+}
+
+// ------------------------------------------------------------ textures, environment
+// IntersectionResult::textureCoordinates (Core/Triangle.h:128-131)
+__device__ inline float2 hit_texcoord(const DevScene& S, int t, float u, float v) {
+    if (!S.uv) return make_float2(0.f, 0.f);
+    const int a = S.idx[3 * t], b = S.idx[3 * t + 1], c = S.idx[3 * t + 2];
+    const float w = 1.f - u - v;
+    return make_float2(S.uv[2 * a] * w + u * S.uv[2 * b] + v * S.uv[2 * c],
+                       S.uv[2 * a + 1] * w + u * S.uv[2 * b + 1] + v * S.uv[2 * c + 1]);
+}
+
+// Material::getBSDF with a "texture Kd": the matte colour times the texel, the plastic and
+// substrate diffuse colour replaced by it (Materials/{MatteMaterial,Plastic,Substrate}.h).
+__device__ inline Bsdf material_bsdf(const DevScene& S, const RMaterial& m, int prim, float u, float v) {
+    Bsdf b = make_bsdf(m);
+    if (m.kd_tex >= 0) {
+        const float2 tc = hit_texcoord(S, prim, u, v);
+        const float4 tx = tex2D<float4>(S.tex[m.kd_tex], tc.x, tc.y);
+        const f3 c = mk(tx.x, tx.y, tx.z);
+        b.kd = m.type == cavpbrt::kMatte ? b.kd * c : c;
+    }
+    return b;
+}
+
+// EnvironmentMap::evaluateRay (Core/Light.h:93-113): the colour, times the texel at the
+// direction's spherical coordinates in the light's frame when there is an image.
+__device__ inline f3 env_eval(const DevScene& S, const RLight& L, f3 d) {
+    f3 r = mk(L.L[0], L.L[1], L.L[2]);
+    if (L.tex >= 0) {
+        const f3 dl = mk(L.w2l[0] * d.x + L.w2l[1] * d.y + L.w2l[2] * d.z,
+                         L.w2l[3] * d.x + L.w2l[4] * d.y + L.w2l[5] * d.z,
+                         L.w2l[6] * d.x + L.w2l[7] * d.y + L.w2l[8] * d.z);
+        float phi = atan2f(dl.y, dl.x);
+        phi = (phi < 0) ? (float)(phi + 2 * 3.14159265358979323846) : phi;
+        const float theta = acosf(clampf(dl.z, -1.f, 1.f));
+        const float tu = (float)(phi / (2.f * 3.14159265358979323846));
+        const float tv = (float)(theta / 3.14159265358979323846);
+        const float4 tx = tex2D<float4>(S.tex[L.tex], tu, tv);
+        r = r * mk(tx.x, tx.y, tx.z);
+    }
+    return r;
+}
+
+// DiffuseAreaLight / EnvironmentMap::sampleRayToPoint: direction, solid-angle pdf, incident
+// radiance, and the shadow ray's length and target mesh (infinite and none for an
+// environment).  Advances `dim` by 2 (environment, sphere cone) or 3 (triangle).
+struct LightSample {
+    f3 dir;
+    float pdf;
+    f3 incident;
+    float dist;
+    int target;
+};
+__device__ inline LightSample sample_light(const DevScene& S, const RLight& L, f3 pos, uint64_t index, int& dim) {
+    LightSample ls;
+    if (L.kind == kLightEnvironment) {
+        // uniformSampleSphere (Utils/RandomUtils.h:70-78) as written: the latitude is drawn
+        // uniformly, with the uniform pdf 1 / (4 pi)
+        const float u0 = halton(S.halton, index, dim);
+        const float u1 = halton(S.halton, index, dim);
+        const float a = (float)(u0 * 2 * 3.14159265358979323846);
+        const float b = (float)((u1 - 0.5) * 3.14159265358979323846);
+        ls.dir = mk(cosf(b) * cosf(a), sinf(b), cosf(b) * sinf(a));
+        ls.pdf = (float)(1.f / (4.f * 3.14159265358979323846));
+        ls.incident = env_eval(S, L, ls.dir);
+        ls.dist = INFINITY;
+        ls.target = -1;
+        return ls;
+    }
+    const RMesh& LM = S.meshes[L.mesh];
+    const LightPoint lp = sample_light_surface(S, LM, pos, index, dim);
+    ls.pdf = lp.pdf;
+    ls.dir = normalize3(lp.p - pos);
+    ls.incident = dot3(ls.dir, lp.n) >= 0 ? mk(0, 0, 0) : mk(L.L[0], L.L[1], L.L[2]);
+    ls.dist = length3(lp.p - pos);
+    ls.target = L.mesh;
+    return ls;
 }
 
 // ---------------------------------------------------------------- path state
@@ -708,6 +794,10 @@ struct cav_scene {
     cav::RMesh* d_meshes = nullptr;
     cav::RMaterial* d_mats = nullptr;
     cav::RLight* d_lights = nullptr;
+    float* d_uv = nullptr;                        // 2 per vertex, or null when no mesh has uvs
+    std::vector<cudaArray_t> tex_arrays;          // image textures (uchar4, linear filter, wrap)
+    std::vector<cudaTextureObject_t> tex_objects;
+    cudaTextureObject_t* d_tex = nullptr;
     uint32_t* d_primes = nullptr;
     uint32_t* d_perm_start = nullptr;
     uint16_t* d_perms = nullptr;
@@ -762,6 +852,12 @@ inline DevScene dev_scene_of(const cav_scene* sc) {
     S.lights = sc->d_lights;
     S.n_lights = (int)sc->desc.lights.size();
     S.direct = 0;
+    S.uv = sc->d_uv;
+    S.tex = sc->d_tex;
+    S.env = sc->desc.environment;
+    S.cont_dim = 7;
+    for (const auto& l : sc->desc.lights)
+        if (l.kind == 0) S.cont_dim = 8;
     S.halton = Halton{sc->d_primes, sc->d_perm_start, sc->d_perms};
     return S;
 }

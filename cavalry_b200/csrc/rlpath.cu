@@ -153,6 +153,8 @@ __device__ inline bool almost_delta(const Bsdf& B) {
 struct Hit {
     f3 ro, rd, pos, nrm;
     int mesh;
+    int prim;
+    float u, v;
 };
 __device__ inline Hit hit_of(const DevScene& S, const Queues& Q, int64_t j, int prim) {
     const cav_ray r = Q.rays[j];
@@ -161,7 +163,10 @@ __device__ inline Hit hit_of(const DevScene& S, const Queues& Q, int64_t j, int 
     h.rd = mk(r.dx, r.dy, r.dz);
     h.pos = h.ro + Q.hit_t[j] * h.rd;
     h.mesh = S.tri_mesh[prim];
-    h.nrm = tri_normal(S, S.meshes[h.mesh], prim, Q.hit_uv[2 * j], Q.hit_uv[2 * j + 1]);
+    h.prim = prim;
+    h.u = Q.hit_uv[2 * j];
+    h.v = Q.hit_uv[2 * j + 1];
+    h.nrm = tri_normal(S, S.meshes[h.mesh], prim, h.u, h.v);
     return h;
 }
 
@@ -224,13 +229,14 @@ __global__ void k_rl_light(DevScene S, const float* box, LightTable LT, int dept
         float sel = 0.f;
         const int li = cdf_sample(LT.cdf + (int64_t)entry * LT.n_lights, LT.n_lights, halton(S.halton, index, dim), sel);
         dim += 4;  // rand4, drawn and unused
-        const RLight& L = S.lights[li];
-        const RMesh& LM = S.meshes[L.mesh];
-        const LightPoint lpt = sample_light_surface(S, LM, h.pos, index, dim);
-        const f3 lp = lpt.p, ln = lpt.n;
-        const float light_pdf = lpt.pdf;
-        f3 dir = normalize3(lp - h.pos);
-        f3 incident = dot3(dir, ln) >= 0 ? mk(0, 0, 0) : ld3(L.L);
+        const LightSample ls = sample_light(S, S.lights[li], h.pos, index, dim);
+        // computeQDistributions draws from this path's own state, which the reference does
+        // not synchronise after computeLighting: 2 (environment, sphere cone) or 3 (triangle)
+        // light-sample dimensions on from here
+        R.dim[path] = dim;
+        const float light_pdf = ls.pdf;
+        const f3 dir = ls.dir;
+        const f3 incident = ls.incident;
         T.light_dir[3 * j] = dir.x;
         T.light_dir[3 * j + 1] = dir.y;
         T.light_dir[3 * j + 2] = dir.z;
@@ -247,9 +253,16 @@ __global__ void k_rl_light(DevScene S, const float* box, LightTable LT, int dept
         T.shadowed[j] = emit ? 1 : 0;
         if (emit) {
             shadow = cav_ray{h.pos.x, h.pos.y, h.pos.z, 0.f, dir.x, dir.y, dir.z, INFINITY};
-            limit = length3(lp - h.pos);
-            excl = make_int2(h.mesh, L.mesh);
+            limit = ls.dist;
+            excl = make_int2(h.mesh, ls.target);
         }
+    } else if (j < n && S.env >= 0) {  // intersectScene :292-296: the environment, no MIS weight
+        const int path = Q.active[j];
+        const cav_ray r = Q.rays[j];
+        const f3 e = env_eval(S, S.lights[S.env], mk(r.dx, r.dy, r.dz)) * ld3(P.throughput + 3 * path);
+        P.result[3 * path] += e.x;
+        P.result[3 * path + 1] += e.y;
+        P.result[3 * path + 2] += e.z;
     }
     uint32_t k = warp_append(Q.counters + 1, emit);
     if (emit) {
@@ -278,7 +291,7 @@ __global__ void __launch_bounds__(128) k_rl_q(DevScene S, QTable QT, LightTable 
     const Hit h = hit_of(S, Q, j, prim);
     const uint64_t index = P.sample_index[path];
     const RMesh& M = S.meshes[h.mesh];
-    const Bsdf B = make_bsdf(S.mats[M.material]);
+    const Bsdf B = material_bsdf(S, S.mats[M.material], h.prim, h.u, h.v);
     const Frame fr = make_frame(h.nrm);
     const f3 wo = to_local(fr, h.rd * -1.f);
     // ---- light result: occluded (or non-finite pdf) samples carry zero radiance, pdf 1
@@ -298,7 +311,7 @@ __global__ void __launch_bounds__(128) k_rl_q(DevScene S, QTable QT, LightTable 
     atomicAdd(LT.new_res + ls, sampled);
     atomicAdd(LT.new_cnt + ls, 1);
     // ---- Q distribution over the 128 cells of this entry
-    int dim = *dim_in + 8;
+    int dim = R.dim[path];  // after this path's light sample (k_rl_light)
     const float r0 = halton(S.halton, index, dim);
     const float r1 = halton(S.halton, index, dim);
     const float* q = QT.Q + (int64_t)entry * kCells;
@@ -473,7 +486,7 @@ __global__ void k_rl_next(DevScene S, int depth, const int32_t* dim_in, int64_t 
             else thr = thr / (1.f - q);
         }
         if (alive) {
-            const Bsdf B = make_bsdf(S.mats[S.meshes[h.mesh].material]);
+            const Bsdf B = material_bsdf(S, S.mats[S.meshes[h.mesh].material], h.prim, h.u, h.v);
             const Frame fr = make_frame(h.nrm);
             const f3 wo = to_local(fr, h.rd * -1.f);
             entry = T.entry[j];

@@ -169,6 +169,8 @@ def _material_line(mat) -> str:
                 parts.append(f'"{kind} {key}" [{_nums(mat[key])}]')
     if "remaproughness" in mat:
         parts.append(f'"string remaproughness" "{"true" if mat["remaproughness"] else "false"}"')
+    if mat.get("Kd_texture"):
+        parts.append(f'"texture Kd" "{mat["Kd_texture"]}"')
     return " ".join(parts)
 
 
@@ -200,6 +202,19 @@ def write_pbrt(path, room: dict, *, width=256, height=256, spp=16, max_depth=5, 
         "WorldBegin",
     ]
     light_of = dict(room.get("lights", []))
+    here = os.path.dirname(os.path.abspath(str(path)))
+    stem = os.path.splitext(os.path.basename(str(path)))[0]
+    env = room.get("environment")
+    if env is not None:  # first, so it is light 0
+        line = f'LightSource "infinite" "rgb L" [{_nums(env["L"])}]'
+        if env.get("map") is not None:
+            write_png(os.path.join(here, f"{stem}_env.png"), env["map"])
+            line += f' "string mapname" "{stem}_env.png"'
+        lines.append(line)
+    for t in room.get("textures", []):
+        write_png(os.path.join(here, f"{stem}_{t['name']}.png"), t["rgba"])
+        lines.append(f'Texture "{t["name"]}" "spectrum" "imagemap" "string filename" "{stem}_{t["name"]}.png"')
+    uvs = room.get("uvs")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
         for k, (name, first, count, mat) in enumerate(room["meshes"]):
@@ -229,8 +244,9 @@ def write_pbrt(path, room: dict, *, width=256, height=256, spp=16, max_depth=5, 
                 _write_ply(os.path.join(os.path.dirname(os.path.abspath(str(path))), fn), P, I)
                 out.append(f'Shape "plymesh" "string filename" "{fn}"')
             else:
+                uv_text = "" if uvs is None else ' "float uv" [' + _floats_text(uvs[used]) + "]"
                 out.append('Shape "trianglemesh" "integer indices" [' + " ".join(map(str, I.tolist())) + '] "point P" ['
-                           + _floats_text(P) + "]")
+                           + _floats_text(P) + "]" + uv_text)
             out.append("AttributeEnd")
             f.write("\n".join(out) + "\n")
         f.write("WorldEnd\n")
@@ -250,6 +266,102 @@ def _write_ply(path, P, I):
         f.write(head.encode())
         f.write(P.tobytes())
         f.write(face.tobytes())
+
+
+def write_png(path, rgba) -> None:
+    """8-bit RGBA PNG (filter 0 on every row) of an [H, W, 4] uint8 array, top row first."""
+    import struct
+    import zlib
+
+    a = np.ascontiguousarray(rgba, np.uint8)
+    h, w = a.shape[:2]
+    raw = b"".join(b"\x00" + a[y].tobytes() for y in range(h))
+
+    def chunk(t, d):
+        return struct.pack(">I", len(d)) + t + d + struct.pack(">I", zlib.crc32(t + d) & 0xFFFFFFFF)
+
+    with open(path, "wb") as f:
+        f.write(b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 6, 0, 0, 0))
+                + chunk(b"IDAT", zlib.compress(raw, 6)) + chunk(b"IEND", b""))
+
+
+def courtyard_scene(seed: int = 41, area_light: bool = False):
+    """An open-topped courtyard under an environment map: a floor with a tiled checker
+    texture ("texture Kd" on matte, uv 0..4), two walls, a textured plastic box, and sphere
+    shapes of assorted materials; the environment ("infinite", a sky gradient with a bright
+    sun patch) is the only light unless `area_light` adds a 1 x 1 quad.  The dict carries
+    ``textures`` ([{"name", "rgba"}], PNG rows top-down), per-vertex ``uvs`` and
+    ``environment = {"L", "map"}``."""
+    rng = np.random.default_rng(seed)
+    verts, tris, mesh_ids, meshes, nrms, uvs, shapes, lights = [], [], [], [], [], [], {}, []
+    nv = nt = 0
+
+    def add(v, t, name, mat, n=None, uv=None):
+        nonlocal nv, nt
+        mid = len(meshes)
+        verts.append(np.asarray(v, np.float32))
+        nrms.append(np.zeros_like(verts[-1]) if n is None else np.asarray(n, np.float32))
+        uvs.append(np.zeros((len(v), 2), np.float32) if uv is None else np.asarray(uv, np.float32))
+        tris.append(np.asarray(t, np.int64) + nv)
+        mesh_ids.append(np.full(len(t), mid, np.int32))
+        meshes.append((name, nt, len(t), mat))
+        nv += len(v)
+        nt += len(t)
+        return mid
+
+    # textures: an 8 x 8-cell checker (64 x 64 texels) and a 32 x 32 stripe pattern
+    ij = np.add.outer(np.arange(64) // 8, np.arange(64) // 8) % 2
+    checker = np.zeros((64, 64, 4), np.uint8)
+    checker[..., :3] = np.where(ij[..., None] == 0, np.array([220, 210, 190]), np.array([60, 80, 120]))
+    checker[..., 3] = 255
+    stripes = np.zeros((32, 32, 4), np.uint8)
+    stripes[..., :3] = np.where((np.arange(32) // 4 % 2)[None, :, None] == 0, np.array([200, 60, 40]),
+                                np.array([240, 220, 120]))
+    stripes[..., 3] = 255
+    S = 3.0
+    add([[-S, 0, -S], [S, 0, -S], [S, 0, S], [-S, 0, S]], [(0, 2, 1), (0, 3, 2)], "floor",
+        {"type": "matte", "Kd": (0.9, 0.9, 0.9), "Kd_texture": "checker"},
+        uv=[[0, 0], [4, 0], [4, 4], [0, 4]])
+    add([[-S, 0, S], [S, 0, S], [S, 2, S], [-S, 2, S]], [(0, 2, 1), (0, 3, 2)], "back", (0.6, 0.6, 0.65))
+    add([[-S, 0, -S], [-S, 0, S], [-S, 2, S], [-S, 2, -S]], [(0, 1, 2), (0, 2, 3)], "left", (0.5, 0.3, 0.25))
+    bv, bt = _box_triangles((0.8, 0.8, 0.8), 20.0, (0.9, 0.0, 0.6))
+    buv = np.tile(np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32), (len(bv) // 4 + 1, 1))[:len(bv)]
+    add(bv, bt, "box", {"type": "plastic", "Kd": (0.5, 0.5, 0.5), "roughness": 0.1, "Kd_texture": "stripes"},
+        uv=buv)
+    kinds = [{"type": "glass", "eta": 1.5}, {"type": "metal", "roughness": 0.15}, (0.3, 0.7, 0.4)]
+    for k, mat in enumerate(kinds):
+        r = float(rng.uniform(0.3, 0.45))
+        c = (float(-1.4 + 1.0 * k), r, float(rng.uniform(-1.2, -0.2)))
+        unit, P, I = sphere_shape_mesh(r)
+        mid = add(P + np.array(c, np.float32), I, f"sphere{k}", mat, n=unit)
+        shapes[mid] = {"type": "sphere", "radius": r, "center": c}
+    if area_light:
+        y = 2.4
+        mid = add([[-1.5, y, 0.5], [-0.5, y, 0.5], [-0.5, y, 1.5], [-1.5, y, 1.5]], [(0, 1, 2), (0, 2, 3)],
+                  "light_quad", (0.0, 0.0, 0.0))
+        lights.append((mid, (6.0, 5.0, 4.0)))
+    # environment: sky gradient over the latitude (rows) with a warm sun patch
+    H_, W_ = 32, 64
+    sky = np.zeros((H_, W_, 4), np.uint8)
+    t = np.linspace(0, 1, H_)[:, None]
+    sky[..., 0] = (80 + 140 * t).astype(np.uint8)
+    sky[..., 1] = (120 + 110 * t).astype(np.uint8)
+    sky[..., 2] = (200 + 40 * t).astype(np.uint8)
+    sky[10:14, 20:26, :3] = (255, 240, 200)
+    sky[..., 3] = 255
+    return {
+        "positions": np.ascontiguousarray(np.concatenate(verts)),
+        "normals": np.ascontiguousarray(np.concatenate(nrms)),
+        "uvs": np.ascontiguousarray(np.concatenate(uvs)),
+        "indices": np.ascontiguousarray(np.concatenate(tris).astype(np.int32)),
+        "mesh_ids": np.concatenate(mesh_ids),
+        "meshes": meshes,
+        "lights": lights,
+        "shapes": shapes,
+        "textures": [{"name": "checker", "rgba": checker}, {"name": "stripes", "rgba": stripes}],
+        "environment": {"L": (1.5, 1.5, 1.5), "map": sky},
+        "camera": {"eye": (0.0, 1.6, -4.5), "look": (0.0, 0.5, 0.0), "up": (0.0, 1.0, 0.0), "fov": 55.0},
+    }
 
 
 def sphere_shape_mesh(radius: float):

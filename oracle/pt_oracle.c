@@ -66,11 +66,19 @@ typedef struct {
     float alpha_u, alpha_v, eta, mirror_kr;
     float f0[3];     /* metal: Fresnel f0 (complex IOR or copper) */
     int32_t has_f0;
+    int32_t kd_tex;  /* "texture Kd": texture index, or -1 */
 } OMaterial;
 typedef struct {
     float L[3];
-    int32_t mesh;
+    int32_t mesh;  /* area light: its mesh */
+    int32_t kind;  /* 0 area, 1 environment */
+    int32_t tex;   /* environment image, or -1 */
+    float w2l[9];  /* environment: mat3(worldToLight), row-major */
 } OLight;
+typedef struct {
+    int32_t width, height;
+    const uint8_t* rgba; /* rows bottom-up (after the load flip), before the inverse gamma */
+} OTexture;
 
 enum { M_MATTE = 0, M_MIRROR = 1, M_SUBSTRATE = 2, M_METAL = 3, M_GLASS = 4, M_PLASTIC = 5 };
 
@@ -532,6 +540,10 @@ typedef struct {
     const OLight* lights;
     int n_lights;
     int direct; /* DirectLightingIntegrator.cu:22-89: one light sample, no MIS, no continuation */
+    const float* uv;            /* 2 per vertex, or NULL */
+    const OTexture* textures;   /* texels after the reference's load-time inverse gamma */
+    int env;                    /* environment light index, or -1 */
+    int cont_dim;               /* 8 with an area light, 7 with environments only */
     Halton h;
 } Scene;
 
@@ -555,6 +567,64 @@ static V3 apply_pt(const float* m, V3 v) {
     float t2 = m[2] * v.x + m[6] * v.y + m[10] * v.z + m[14];
     float t3 = m[3] * v.x + m[7] * v.y + m[11] * v.z + m[15];
     return v3(t0 / t3, t1 / t3, t2 / t3);
+}
+
+/* ------------------------------------------------------------------ textures */
+/* Color.h inverseGammaCorrect, applied per channel at load and truncated to 8 bits
+ * (Core/Texture.cu:61-68, .png files) */
+static float inverse_gamma(float value) {
+    if (value <= 0.04045f) return value * 1.f / 12.92f;
+    return powf((value + 0.055f) * 1.f / 1.055f, (float)2.4f);
+}
+static uint8_t load_gamma(uint8_t c) { return (uint8_t)(255.f * inverse_gamma(c / 255.f)); }
+
+/* tex2D of a uchar4 texture read as normalized floats with bilinear filtering and wrapped
+ * normalized coordinates, restated from the CUDA programming guide's description of
+ * texture fetching: x = frac(u) * W - 0.5, texels i = floor(x) and i + 1 (wrapped), weight
+ * frac(x) held with 8 fractional bits; the same in y. */
+static V3 tex_read(const OTexture* t, float u, float v) {
+    float xs = (u - floorf(u)) * t->width - 0.5f, ys = (v - floorf(v)) * t->height - 0.5f;
+    float fx = floorf(xs), fy = floorf(ys);
+    float a = rintf((xs - fx) * 256.f) / 256.f, b = rintf((ys - fy) * 256.f) / 256.f;
+    int i0 = (int)fx, j0 = (int)fy;
+    V3 acc = v3(0, 0, 0);
+    for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+            int i = ((i0 + di) % t->width + t->width) % t->width;
+            int j = ((j0 + dj) % t->height + t->height) % t->height;
+            const uint8_t* p = t->rgba + 4 * ((size_t)j * t->width + i);
+            float w = (di ? a : 1.f - a) * (dj ? b : 1.f - b);
+            acc = vadd(acc, vs(v3(load_gamma(p[0]) / 255.f, load_gamma(p[1]) / 255.f, load_gamma(p[2]) / 255.f), w));
+        }
+    return acc;
+}
+
+/* IntersectionResult::textureCoordinates (Core/Triangle.h:128-131) */
+static void hit_texcoord(const Scene* S, int t, float u, float v, float* tu, float* tv) {
+    if (!S->uv) {
+        *tu = *tv = 0.f;
+        return;
+    }
+    int a = S->idx[3 * t], b = S->idx[3 * t + 1], c = S->idx[3 * t + 2];
+    float w = 1.f - u - v;
+    *tu = S->uv[2 * a] * w + u * S->uv[2 * b] + v * S->uv[2 * c];
+    *tv = S->uv[2 * a + 1] * w + u * S->uv[2 * b + 1] + v * S->uv[2 * c + 1];
+}
+
+/* EnvironmentMap::evaluateRay (Core/Light.h:93-113) */
+static V3 env_eval(const Scene* S, const OLight* L, V3 d) {
+    V3 r = ld3(L->L);
+    if (L->tex >= 0) {
+        const float* m = L->w2l;
+        V3 dl = v3(m[0] * d.x + m[1] * d.y + m[2] * d.z, m[3] * d.x + m[4] * d.y + m[5] * d.z,
+                   m[6] * d.x + m[7] * d.y + m[8] * d.z);
+        float phi = atan2f(dl.y, dl.x);
+        phi = (phi < 0) ? (float)(phi + 2 * M_PI) : phi;
+        float theta = acosf(fminf(fmaxf(dl.z, -1.f), 1.f));
+        V3 tx = tex_read(&S->textures[L->tex], (float)(phi / (2.f * M_PI)), (float)(theta / M_PI));
+        r = vmul(r, tx);
+    }
+    return r;
 }
 
 /* TriangleMesh::sampleSphere (Core/TriangleMesh.h:154-210): uniform in the cone a sphere
@@ -636,7 +706,10 @@ static V3 trace_path(const Scene* S, uint64_t index, V3 ro, V3 rd, int max_depth
         float o[3] = {ro.x, ro.y, ro.z}, d[3] = {rd.x, rd.y, rd.z};
         float t, u, v;
         int prim = orc_closest_one(S->nodes, S->pos, S->idx, o, d, &t, &u, &v);
-        if (prim < 0) break;
+        if (prim < 0) { /* intersectScene: the environment, without an MIS weight */
+            if (S->env >= 0) res = vadd(res, vmul(env_eval(S, &S->lights[S->env], rd), thr));
+            break;
+        }
         const int mesh = S->tri_mesh[prim];
         const OMesh* M = &S->meshes[mesh];
         V3 pos = vadd(ro, vs(rd, t));
@@ -652,20 +725,41 @@ static V3 trace_path(const Scene* S, uint64_t index, V3 ro, V3 rd, int max_depth
                 if (isfinite(w)) res = vadd(res, vs(vmul(Le, thr), w));
             }
         }
-        Bsdf B = make_bsdf(&S->mats[M->material]);
+        const OMaterial* mat = &S->mats[M->material];
+        Bsdf B = make_bsdf(mat);
+        if (mat->kd_tex >= 0 && (mat->type == M_MATTE || mat->type == M_PLASTIC || mat->type == M_SUBSTRATE)) {
+            float tu, tv;
+            hit_texcoord(S, prim, u, v, &tu, &tv);
+            V3 tx = tex_read(&S->textures[mat->kd_tex], tu, tv);
+            B.kd = mat->type == M_MATTE ? vmul(B.kd, tx) : tx;
+        }
         Frame fr = make_frame(nrm);
         V3 wo = to_local(&fr, vs(rd, -1.f));
-        /* light sample: randInt(lights), rand4 (unused), TriangleMesh::sample */
+        /* light sample: randInt(lights), rand4 (unused), then the light's own sample */
         int dim = dim0;
         int li = halton_int(&S->h, index, &dim, S->n_lights);
         dim += 4;
         const OLight* L = &S->lights[li];
-        const OMesh* LM = &S->meshes[L->mesh];
-        V3 lp, ln;
-        float lpdf;
-        light_sample(S, LM, pos, index, &dim, &lp, &ln, &lpdf);
-        V3 dir = vnorm(vsub(lp, pos));
-        V3 incident = vdot(dir, ln) >= 0 ? v3(0, 0, 0) : ld3(L->L);
+        V3 dir, incident;
+        float lpdf, limit;
+        int target;
+        if (L->kind == 1) { /* EnvironmentMap::sampleRayToPoint, uniformSampleSphere as written */
+            float a0 = halton(&S->h, index, &dim), a1 = halton(&S->h, index, &dim);
+            float a = (float)(a0 * 2 * M_PI), b = (float)((a1 - 0.5) * M_PI);
+            dir = v3(cosf(b) * cosf(a), sinf(b), cosf(b) * sinf(a));
+            lpdf = (float)(1.f / (4.f * M_PI));
+            incident = env_eval(S, L, dir);
+            limit = INFINITY;
+            target = -1;
+        } else {
+            V3 lp, ln;
+            light_sample(S, &S->meshes[L->mesh], pos, index, &dim, &lp, &ln, &lpdf);
+            dir = vnorm(vsub(lp, pos));
+            incident = vdot(dir, ln) >= 0 ? v3(0, 0, 0) : ld3(L->L);
+            V3 dl = vsub(lp, pos);
+            limit = sqrtf(vdot(dl, dl));
+            target = L->mesh;
+        }
         if (isfinite(lpdf)) {
             V3 wi = to_local(&fr, dir);
             float w = S->direct ? 1.f : mis_power(lpdf, bsdf_pdf(&B, wi, wo));
@@ -674,14 +768,12 @@ static V3 trace_path(const Scene* S, uint64_t index, V3 ro, V3 rd, int max_depth
             V3 contrib = vs(vmul(vs(vmul(incident, bsdf_eval(&B, wi, wo)), cosine), mult), w);
             if (!vzero(contrib)) {
                 float so[3] = {pos.x, pos.y, pos.z}, sd[3] = {dir.x, dir.y, dir.z};
-                V3 dl = vsub(lp, pos);
-                float limit = sqrtf(vdot(dl, dl));
-                if (orc_any_one(S->nodes, S->pos, S->idx, S->tri_mesh, so, sd, limit, mesh, L->mesh) == 0)
+                if (orc_any_one(S->nodes, S->pos, S->idx, S->tri_mesh, so, sd, limit, mesh, target) == 0)
                     res = vadd(res, contrib);
             }
         }
         /* continuation */
-        dim = dim0 + 8;
+        dim = dim0 + S->cont_dim;
         if (depth > 3) {
             float q = 1;
             q = fminf(q, 1 - thr.x);
@@ -704,7 +796,7 @@ static V3 trace_path(const Scene* S, uint64_t index, V3 ro, V3 rd, int max_depth
         delta = bsdf_delta(&B);
         ro = vadd(pos, vs(nd, 0.001f));
         rd = nd;
-        dim0 += 8 + 2 + (depth > 3 ? 1 : 0);
+        dim0 += S->cont_dim + 2 + (depth > 3 ? 1 : 0);
     }
     return res;
 }
@@ -728,7 +820,7 @@ int orc_render_path(const ONode* nodes, const float* pos, const int32_t* idx, co
                     const int32_t* tri_mesh, OMesh* meshes, int n_meshes, const OMaterial* mats,
                     const OLight* lights, int n_lights, const float* c2w, float fov_deg, int width, int height,
                     int spp, int max_depth, float xw, float yw, int64_t first, int64_t count, float* film_sum,
-                    float* film_w, int direct) {
+                    float* film_w, int direct, const float* uv, const OTexture* textures, int env) {
     if (n_lights <= 0 || width <= 0 || height <= 0 || spp <= 0) return -1;
     unsigned csr = _mm_getcsr();
     _mm_setcsr(csr | 0x8040); /* FTZ | DAZ, as the device build */
@@ -745,6 +837,12 @@ int orc_render_path(const ONode* nodes, const float* pos, const int32_t* idx, co
     S.n_lights = n_lights;
     S.direct = direct;
     if (direct) max_depth = 1;
+    S.uv = uv;
+    S.textures = textures;
+    S.env = env;
+    S.cont_dim = 7;
+    for (int l = 0; l < n_lights; ++l)
+        if (lights[l].kind == 0) S.cont_dim = 8;
     int64_t plen = orc_halton_tables(S.h.primes, S.h.start, NULL);
     S.h.perms = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)plen);
     orc_halton_tables(S.h.primes, S.h.start, S.h.perms);

@@ -241,8 +241,9 @@ OMESH_DTYPE = np.dtype([("first_tri", "<i4"), ("tri_count", "<i4"), ("has_normal
                         ("sphere", "<f4", (4,))])
 OMAT_DTYPE = np.dtype([("type", "<i4"), ("kd", "<f4", (3,)), ("ks", "<f4", (3,)), ("kr", "<f4", (3,)),
                        ("kt", "<f4", (3,)), ("alpha_u", "<f4"), ("alpha_v", "<f4"), ("eta", "<f4"),
-                       ("mirror_kr", "<f4"), ("f0", "<f4", (3,)), ("has_f0", "<i4")])
-OLIGHT_DTYPE = np.dtype([("L", "<f4", (3,)), ("mesh", "<i4")])
+                       ("mirror_kr", "<f4"), ("f0", "<f4", (3,)), ("has_f0", "<i4"), ("kd_tex", "<i4")])
+OLIGHT_DTYPE = np.dtype([("L", "<f4", (3,)), ("mesh", "<i4"), ("kind", "<i4"), ("tex", "<i4"), ("w2l", "<f4", (9,))])
+OTEX_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("rgba", "<u8")])
 MATERIAL_TYPES = {"matte": 0, "mirror": 1, "substrate": 2, "metal": 3, "glass": 4, "plastic": 5}
 
 
@@ -250,7 +251,7 @@ def _pt_lib():
     L = oracle_lib()
     if not hasattr(L, "_pt_ready"):
         P, I, I64, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float
-        L.orc_render_path.argtypes = [P, P, P, P, P, P, I, P, P, I, P, F, I, I, I, I, F, F, I64, I64, P, P, I]
+        L.orc_render_path.argtypes = [P, P, P, P, P, P, I, P, P, I, P, F, I, I, I, I, F, F, I64, I64, P, P, I, P, P, I]
         L.orc_render_path.restype = I
         L.orc_roughness_to_alpha.argtypes = [F]
         L.orc_roughness_to_alpha.restype = F
@@ -264,10 +265,14 @@ def roughness_to_alpha(r: float) -> float:
     return float(_pt_lib().orc_roughness_to_alpha(float(r)))
 
 
-def material_record(mat) -> np.void:
+def material_record(mat, texture_index: dict | None = None) -> np.void:
     """A material as the reference's parser builds it (Materials/*.h createFromParams):
-    a tuple is a matte Kd; a dict names "type" and the pbrt parameters."""
+    a tuple is a matte Kd; a dict names "type" and the pbrt parameters ("Kd_texture": the
+    name of a scene texture)."""
     m = np.zeros((), OMAT_DTYPE)
+    m["kd_tex"] = -1
+    if isinstance(mat, dict) and mat.get("Kd_texture") is not None:
+        m["kd_tex"] = (texture_index or {})[mat["Kd_texture"]]
     if not isinstance(mat, dict):
         mat = {"type": "matte", "Kd": mat}
     t = mat["type"]
@@ -345,7 +350,19 @@ def render_path(scene: dict, *, width: int, height: int, spp: int, max_depth: in
     nodes = build(pos, idx, rounds=0)["merged"]
     meshes = np.zeros(len(scene["meshes"]), OMESH_DTYPE)
     mats = np.zeros(len(scene["meshes"]), OMAT_DTYPE)
+    # image textures in declaration order (named ones, then the environment's map), rows
+    # flipped to the loader's bottom-up order
+    images = [t["rgba"] for t in scene.get("textures", [])]
+    tex_index = {t["name"]: k for k, t in enumerate(scene.get("textures", []))}
+    env = scene.get("environment")
     lights = []
+    w2l_id = (1, 0, 0, 0, 1, 0, 0, 0, 1)
+    if env is not None:  # written first in the .pbrt, so light 0
+        tex = -1
+        if env.get("map") is not None:
+            images.append(env["map"])
+            tex = len(images) - 1
+        lights.append((tuple(float(x) for x in env["L"]), -1, 1, tex, w2l_id))
     light_of = dict(scene.get("lights", []))
     shapes = scene.get("shapes", {})
     nrm = scene.get("normals")
@@ -363,16 +380,22 @@ def render_path(scene: dict, *, width: int, height: int, spp: int, max_depth: in
             meshes[k]["sphere"] = (c[0], c[1], c[2], np.float32(np.sqrt(np.float32(((c - e) ** 2).sum()))))
         elif sh is not None:
             meshes[k]["shape"] = 2
-        mats[k] = material_record(mat)
+        mats[k] = material_record(mat, tex_index)
         L = light_of.get(k)
         if L is None and name == "light":
             L = scene.get("light_radiance", (17.0, 12.0, 4.0))
         if L is not None:
             meshes[k]["light"] = len(lights)
-            lights.append(((float(L[0]), float(L[1]), float(L[2])), k))
+            lights.append(((float(L[0]), float(L[1]), float(L[2])), k, 0, -1, w2l_id))
         else:
             meshes[k]["light"] = -1
     light_arr = np.array(lights, OLIGHT_DTYPE)
+    flipped = [np.ascontiguousarray(np.asarray(im, np.uint8)[::-1]) for im in images]
+    texs = np.zeros(max(len(flipped), 1), OTEX_DTYPE)
+    for k, im in enumerate(flipped):
+        texs[k]["width"], texs[k]["height"], texs[k]["rgba"] = im.shape[1], im.shape[0], im.ctypes.data
+    uvs = scene.get("uvs")
+    uvs = None if uvs is None else np.ascontiguousarray(uvs, np.float32)
     c2w = look_at_c2w(eye, look, up)
     total = width * height * spp
     count = total - first if count is None else count
@@ -382,7 +405,9 @@ def render_path(scene: dict, *, width: int, height: int, spp: int, max_depth: in
                                    _c(meshes), len(meshes),
                                    _c(mats), _c(light_arr), len(light_arr), _c(c2w), float(fov), width, height, spp,
                                    max_depth, filter_width, filter_width, int(first), int(count), _c(fsum), _c(fw),
-                                   int(integrator == "directlighting"))
+                                   int(integrator == "directlighting"), None if uvs is None else _c(uvs), _c(texs),
+                                   0 if env is not None else -1)
+    del flipped
     if st != 0:
         raise RuntimeError(f"orc_render_path failed ({st})")
     return fsum, fw

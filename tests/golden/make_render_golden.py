@@ -54,6 +54,13 @@ CASES = [
      dict(width=128, height=96, spp=8, max_depth=8, integrator="directlighting")),
     ("shapes_direct", {"kind": "shapes", "seed": 32, "quad_light": True},
      dict(width=160, height=120, spp=8, max_depth=5, integrator="directlighting")),
+    # image textures ("texture Kd" on matte and plastic, uv coordinates) under an environment
+    # map ("infinite" with "mapname"): alone, with an area light, and with direct lighting
+    ("courtyard_env", {"kind": "courtyard", "seed": 41}, dict(width=160, height=120, spp=8, max_depth=5)),
+    ("courtyard_env_area", {"kind": "courtyard", "seed": 42, "area_light": True},
+     dict(width=160, height=120, spp=8, max_depth=5)),
+    ("courtyard_direct", {"kind": "courtyard", "seed": 41},
+     dict(width=160, height=120, spp=8, max_depth=5, integrator="directlighting")),
     # the learning integrator (the .pbrt names it; both renderers read the Integrator line)
     ("room_rlpath_s16", {"kind": "room"}, dict(width=128, height=128, spp=16, max_depth=5, integrator="rlpath")),
     ("spheres_rlpath_s16", {"kind": "spheres", "n_spheres": 12, "level": 3, "seed": 5},
@@ -61,6 +68,8 @@ CASES = [
     ("spheres_rough_rlpath_s16", {"kind": "spheres", "n_spheres": 12, "level": 3, "seed": 14,
                                   "materials": ["metal", "gold", "substrate", "roughglass"]},
      dict(width=128, height=96, spp=16, max_depth=8, integrator="rlpath")),
+    ("courtyard_rlpath_s16", {"kind": "courtyard", "seed": 42, "area_light": True},
+     dict(width=160, height=120, spp=16, max_depth=5, integrator="rlpath")),
 ]
 
 
@@ -72,6 +81,8 @@ def make_scene(gen: dict) -> dict:
         sc = scenes.mini_room()
     elif kind == "shapes":
         sc = scenes.shapes_scene(**g)
+    elif kind == "courtyard":
+        sc = scenes.courtyard_scene(**g)
     else:
         if "materials" in g:
             g["materials"] = tuple(g["materials"])
