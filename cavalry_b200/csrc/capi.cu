@@ -83,6 +83,15 @@ cav_status cav_ctx_create(int device, cav_ctx** out) {
         return CAV_ERR_CUDA;
     }
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    // Renders allocate their path state stream-ordered (cudaMallocAsync from the device's
+    // default pool); keep freed pool memory mapped instead of releasing it at every
+    // synchronisation, so repeated renders do not map gigabytes again each call.
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess && pool) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     if (cudaMalloc(&ctx->d_counters, sizeof(unsigned long long) * kCounterWords) != cudaSuccess ||
         cudaMalloc(&ctx->d_error, sizeof(int) * kErrorWords) != cudaSuccess) {
         cudaGetLastError();

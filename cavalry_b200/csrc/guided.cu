@@ -368,7 +368,14 @@ cav_status render_guided(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opt
     const int max_depth = opts && opts->max_depth > 0 ? opts->max_depth : D.max_depth;
     const int64_t pixels = (int64_t)W * H;
     int64_t chunk = opts && opts->max_paths_in_flight > 0 ? opts->max_paths_in_flight : (int64_t)1 << 22;
-    chunk = std::min(chunk, pixels * spp_total);
+    // passes render 1, 1, 2, 4, ... samples per pixel: the largest pass bounds the paths in flight
+    int max_pass = 1;
+    for (int done = 0, p = 0, ps = 1; done < spp_total; ++p) {
+        max_pass = std::max(max_pass, std::min(ps, spp_total - done));
+        done += std::min(ps, spp_total - done);
+        if (p >= 1) ps *= 2;
+    }
+    chunk = std::min(chunk, pixels * max_pass);
     const float alpha = gopt && gopt->alpha > 0.f ? gopt->alpha : 0.5f;
     const uint32_t cap = gopt && gopt->train_samples_per_pass > 0 ? (uint32_t)gopt->train_samples_per_pass : (1u << 18);
     const int steps_per_pass = gopt && gopt->train_steps_per_pass > 0 ? gopt->train_steps_per_pass : 32;
