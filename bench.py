@@ -729,8 +729,8 @@ def run_serve(args):
             r, lim = scenes.shadow_rays(j["rays"], seed=j["seed"])
             ray_inputs[i] = (r, lim)
 
-    def serve(mode):
-        sv = cav.Server(ctx, hbm_budget_bytes=80 << 30, mode=mode)
+    def serve(mode, flags=cav.TRACE_EXACT):
+        sv = cav.Server(ctx, hbm_budget_bytes=80 << 30, mode=mode, trace_flags=flags)
         ids = [None] * len(jobs)
         outs = [None] * len(jobs)
         clock0 = sv.stats().now_s
@@ -771,6 +771,9 @@ def run_serve(args):
 
     merged, out_m = serve(cav.SERVE_MERGED)
     seq, out_s = serve(cav.SERVE_SEQUENTIAL)
+    # both arms again with the compressed 8-wide traversal in the merged launches
+    merged_f, _ = serve(cav.SERVE_MERGED, cav.TRACE_FAST)
+    seq_f, _ = serve(cav.SERVE_SEQUENTIAL, cav.TRACE_FAST)
     # the same result alone (sequential) and in the mix (merged)
     worst = 0.0
     for a, b in zip(out_m, out_s):
@@ -785,13 +788,16 @@ def run_serve(args):
                 worst = float("inf")
     renders = sum(1 for j in jobs if j["kind"] == "render")
     out = {
-        "metric": "served jobs/s (merged server vs sequential loop)", "value": merged["jobs_per_s"], "unit": "jobs/s",
+        "metric": "served jobs/s (merged server vs sequential loop)", "value": merged_f["jobs_per_s"], "unit": "jobs/s",
         "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
         "data": "synthetic (seeded soups written as .pbrt; seeded Poisson job stream)",
         "config": {"workload": f"served_stream_{len(jobs)}_jobs_poisson_20ms", "jobs": len(jobs), "render_jobs": renders,
                    "ray_jobs": len(jobs) - renders, "scenes": n_scenes,
                    "scene_triangles": [int(x) for x in sizes], "resolutions": resolutions, "spp": [1, 4, 16, 64],
                    "depth": 6, "hbm_budget_gib": 80},
+        "trace_mode": "value: merged launches in the compressed 8-wide mode (fast_trace); exact-mode arms beside",
+        "fast_trace": {"merged": merged_f, "sequential": seq_f,
+                       "speedup_jobs_per_s": round(merged_f["jobs_per_s"] / seq_f["jobs_per_s"], 3)},
         "merged": merged, "sequential": seq,
         "speedup_jobs_per_s": round(merged["jobs_per_s"] / seq["jobs_per_s"], 3),
         "max_rel_diff_merged_vs_sequential": worst, "setup_s": round(setup_s, 1),

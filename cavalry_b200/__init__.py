@@ -108,6 +108,7 @@ def lib() -> ctypes.CDLL:
         "cav_mlp_last_loss": ([P, P], ctypes.c_int),
         "cav_mlp_mixture": ([P, P, ctypes.c_int64, P, P, P, P, P], ctypes.c_int),
         "cav_trace_autotune": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, P, P], ctypes.c_int),
+        "cav_bvh_has_fast_layout": ([P], ctypes.c_int),
         "cav_pbrt_load_triangles": ([ctypes.c_char_p, P, ctypes.c_int64, P, P, ctypes.c_int64, P, P, P,
                                      ctypes.c_int], ctypes.c_int),
         "cav_trace_autotune_flags": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, U32, P, P], ctypes.c_int),
@@ -409,7 +410,7 @@ class Scene:
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("mode", ctypes.c_int), ("max_live_jobs", ctypes.c_int),
-                ("max_paths_per_job", ctypes.c_int64)]
+                ("max_paths_per_job", ctypes.c_int64), ("trace_flags", ctypes.c_uint32)]
 
 
 class JobStatus(ctypes.Structure):
@@ -439,9 +440,9 @@ class Server:
     :meth:`wait` reports the job done."""
 
     def __init__(self, ctx: "Context", hbm_budget_bytes: int = 80 << 30, mode: int = SERVE_MERGED,
-                 max_live_jobs: int = 64, max_paths_per_job: int = 0):
+                 max_live_jobs: int = 64, max_paths_per_job: int = 0, trace_flags: int = TRACE_EXACT):
         self.ctx = ctx
-        cfg = ServerConfig(hbm_budget_bytes, mode, max_live_jobs, max_paths_per_job)
+        cfg = ServerConfig(hbm_budget_bytes, mode, max_live_jobs, max_paths_per_job, trace_flags)
         h = ctypes.c_void_p()
         ctx._check(lib().cav_server_create(ctx.handle, ctypes.addressof(cfg), ctypes.byref(h)), "cav_server_create")
         self.handle = h
@@ -663,6 +664,10 @@ class Bvh:
                                             ctypes.addressof(out))
         self.ctx._check(st, "cav_trace_autotune_flags")
         return out.as_dict()
+
+    def has_fast_layout(self) -> bool:
+        """Whether the compressed 8-wide view of TRACE_FAST has been built for this tree."""
+        return bool(lib().cav_bvh_has_fast_layout(self.handle))
 
     def trace_closest(self, rays, flags: int = TRACE_EXACT, stream=None, out=None):
         """rays: float32 [n,8] CUDA (o.xyz, tmin, d.xyz, tmax).  Returns (prim int32, t float32, uv float32 [n,2])."""

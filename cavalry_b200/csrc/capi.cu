@@ -170,6 +170,8 @@ cav_status cav_bvh_free(cav_bvh* bvh) {
 
 int64_t cav_bvh_num_triangles(const cav_bvh* bvh) { return bvh ? bvh->n : 0; }
 
+int cav_bvh_has_fast_layout(const cav_bvh* bvh) { return bvh && bvh->cnodes ? 1 : 0; }
+
 cav_status cav_bvh_stage_times(cav_ctx* ctx, const cav_bvh* bvh, float* ms6) {
     if (!ctx || !bvh || !ms6) return CAV_ERR_INVALID_ARGUMENT;
     if (!bvh->timed) return set_error(ctx, CAV_ERR_NOT_READY, "no timing recorded");

@@ -176,6 +176,8 @@ struct TraceSeg {
     uint8_t* occ;
     int64_t begin;
     const uint32_t* n_dev;  // single-tree launches: ray count read from device memory (or null)
+    const CNode* cnodes;    // the tree's compressed 8-wide view (fast-mode launches; ensure_wide)
+    const TriRec* ctris;
 };
 cav_status trace_closest_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags,
                                   cudaStream_t s, unsigned long long* counter);
@@ -200,6 +202,8 @@ cav_status trace_wide_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays,
                           const int32_t* excl, int64_t n, const uint32_t* n_dev, uint8_t* occ, cudaStream_t s,
                           unsigned long long* counter, unsigned long long* stats = nullptr);
 void free_wide(cav_bvh* bvh);
+cav_status trace_wide_segments(cav_ctx* ctx, bool any_hit, const TraceSeg* segs, int nseg, int64_t n, cudaStream_t s,
+                               unsigned long long* counter);
 
 // Many scenes' BVHs, one launch per LBVH stage across all of them (build.cu)
 cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, const int64_t* num_vertices,

@@ -771,6 +771,8 @@ int64_t path_job_extend(PathJob* J, TraceSeg* seg) {
     *seg = TraceSeg{};
     seg->nodes = b->tnodes;
     seg->tris = b->tris;
+    seg->cnodes = b->cnodes;  // set once the fast-mode view exists (ensure_wide)
+    seg->ctris = b->ctris;
     seg->root_box = b->d_root_box;
     seg->rays = J->Q.rays;
     seg->prim = J->Q.hit_prim;
@@ -795,6 +797,8 @@ int64_t path_job_shadow(PathJob* J, TraceSeg* seg) {
     *seg = TraceSeg{};
     seg->nodes = b->tnodes;
     seg->tris = b->tris;
+    seg->cnodes = b->cnodes;  // set once the fast-mode view exists (ensure_wide)
+    seg->ctris = b->ctris;
     seg->root_box = b->d_root_box;
     seg->rays = J->Q.shadow_rays;
     seg->limit = J->Q.shadow_limit;

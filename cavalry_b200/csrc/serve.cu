@@ -101,6 +101,7 @@ struct cav_server {
     double busy_s = 0;
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+    uint32_t trace_flags() const { return cfg.trace_flags & CAV_TRACE_FAST ? CAV_TRACE_FAST : CAV_TRACE_EXACT; }
     void run();
     void admit_locked(std::vector<Job*>& started);
     bool start(Job* j);
@@ -125,6 +126,12 @@ void cav_server::admit_locked(std::vector<Job*>& started) {
 bool cav_server::start(Job* j) {
     j->t_start = now();
     cav_status st = CAV_OK;
+    const cav_bvh* tree = j->kind == kRender ? cav_scene_bvh(j->scene) : j->bvh;
+    if (trace_flags() == CAV_TRACE_FAST) st = cav::ensure_wide(ctx, tree, stream);  // once per tree
+    if (st != CAV_OK) {
+        finish(j, st);
+        return false;
+    }
     if (j->kind == kRender) {
         st = cav::path_job_create(ctx, j->scene, &j->opts, stream, &j->pj);
     } else {
@@ -200,6 +207,8 @@ void cav_server::tick() {
             const cav_bvh* b = j->bvh;
             sg.nodes = b->tnodes;
             sg.tris = b->tris;
+            sg.cnodes = b->cnodes;
+            sg.ctris = b->ctris;
             sg.root_box = b->d_root_box;
             sg.rays = j->d_rays;
             sg.prim = j->d_prim;
@@ -217,7 +226,7 @@ void cav_server::tick() {
     if (nc > 0) {
         max_segments = std::max<int64_t>(max_segments, nc);
         cudaMemcpyAsync(d_seg_c, h_seg_c, sizeof(cav::TraceSeg) * nc, cudaMemcpyHostToDevice, stream);
-        err = cav::trace_closest_segments(ctx, d_seg_c, nc, total, CAV_TRACE_EXACT, stream, d_counter);
+        err = cav::trace_closest_segments(ctx, d_seg_c, nc, total, trace_flags(), stream, d_counter);
         ++closest_launches;
     }
     std::vector<Job*> shaded;
@@ -244,6 +253,8 @@ void cav_server::tick() {
             const cav_bvh* b = j->bvh;
             sg.nodes = b->tnodes;
             sg.tris = b->tris;
+            sg.cnodes = b->cnodes;
+            sg.ctris = b->ctris;
             sg.root_box = b->d_root_box;
             sg.rays = j->d_rays;
             sg.limit = j->d_limit;
@@ -260,7 +271,7 @@ void cav_server::tick() {
     }
     if (na > 0 && err == CAV_OK) {
         cudaMemcpyAsync(d_seg_a, h_seg_a, sizeof(cav::TraceSeg) * na, cudaMemcpyHostToDevice, stream);
-        err = cav::trace_any_segments(ctx, d_seg_a, na, total, CAV_TRACE_EXACT, stream, d_counter + 1);
+        err = cav::trace_any_segments(ctx, d_seg_a, na, total, trace_flags(), stream, d_counter + 1);
         ++any_launches;
     }
     for (Job* j : in_a)
@@ -358,6 +369,7 @@ cav_status cav_server_create(cav_ctx* ctx, const cav_server_config* cfg, cav_ser
         sv->cfg.mode = cfg->mode;
         if (cfg->max_live_jobs > 0) sv->cfg.max_live_jobs = cfg->max_live_jobs;
         if (cfg->max_paths_per_job > 0) sv->cfg.max_paths_per_job = cfg->max_paths_per_job;
+        sv->cfg.trace_flags = cfg->trace_flags;
     }
     const int ms = cav::trace_max_segments();
     cudaError_t e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);

@@ -74,18 +74,6 @@ __device__ __forceinline__ void load_node(const TNode* __restrict__ nodes, int32
 // Segments: one traversal launch over the rays of several jobs, each with its own BVH and
 // output arrays.  A lane that claims global ray g finds its segment by binary search over
 // the segment starts (staged in shared memory) and switches to that segment's tree.
-constexpr int kMaxSeg = 1024;
-
-__device__ inline int find_seg(const int64_t* sbeg, int nseg, int64_t g) {
-    int lo = 0, hi = nseg - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (sbeg[mid] <= g) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack>
 __global__ void k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
                           unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
@@ -481,6 +469,7 @@ cav_status trace_closest_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, 
                                   cudaStream_t s, unsigned long long* counter) {
     if (nseg <= 0 || n == 0) return CAV_OK;
     if (nseg > kMaxSeg) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "too many trace segments in one launch");
+    if (flags & CAV_TRACE_FAST) return trace_wide_segments(ctx, false, segs, nseg, n, s, counter);
     TraceSeg none{};
     return launch_closest<false, true>(ctx, none, segs, nseg, n, flags, s, counter, nullptr);
 }
@@ -489,6 +478,7 @@ cav_status trace_any_segments(cav_ctx* ctx, const TraceSeg* segs, int nseg, int6
                               unsigned long long* counter) {
     if (nseg <= 0 || n == 0) return CAV_OK;
     if (nseg > kMaxSeg) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "too many trace segments in one launch");
+    if (flags & CAV_TRACE_FAST) return trace_wide_segments(ctx, true, segs, nseg, n, s, counter);
     TraceSeg none{};
     return launch_any<false, true>(ctx, none, segs, nseg, n, flags, s, counter, nullptr);
 }

@@ -54,6 +54,21 @@ __device__ inline int64_t claim(unsigned idle, unsigned long long* counter, int6
     return my < n ? my : -1;
 }
 
+// Segments: one traversal launch over the rays of several jobs, each with its own tree and
+// outputs; a lane that claims global ray g finds its segment by binary search over the
+// segment starts (staged in shared memory).
+constexpr int kMaxSeg = 1024;
+
+__device__ inline int find_seg(const int64_t* sbeg, int nseg, int64_t g) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (sbeg[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 // Per-lane visit counters of the instrumented traversal variants, summed per warp.
 struct TraceStats {
     uint32_t nodes = 0, tris = 0;

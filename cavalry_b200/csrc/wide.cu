@@ -282,13 +282,24 @@ __device__ __forceinline__ uint32_t node_hits(const CNode* __restrict__ cn, uint
     return hits;
 }
 
-template <bool kAny, bool kStats>
+// kSeg: one launch over several jobs' rays (segs[k] = one tree and its outputs, ray indices
+// numbered across the launch); otherwise the pointer arguments describe the one tree.
+template <bool kAny, bool kStats, bool kSeg>
 __global__ void __launch_bounds__(256)
-    k_trace_wide(const CNode* __restrict__ cn, const TriRec* __restrict__ tris, const cav_ray* __restrict__ rays,
-                 int64_t n, const uint32_t* n_dev, int32_t* prim, float* tout, float* uv, const float* __restrict__ limit,
-                 const int32_t* __restrict__ excl, uint8_t* occ, unsigned long long* counter, int refill, int* flag,
-                 unsigned long long* stats) {
+    k_trace_wide(const CNode* __restrict__ cn0, const TriRec* __restrict__ tris0, const cav_ray* __restrict__ rays0,
+                 int64_t n, const uint32_t* n_dev, int32_t* prim0, float* tout0, float* uv0,
+                 const float* __restrict__ limit0, const int32_t* __restrict__ excl0, uint8_t* occ0,
+                 unsigned long long* counter, int refill, int* flag, unsigned long long* stats,
+                 const TraceSeg* __restrict__ segs, int nseg) {
+    __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
+    if (kSeg) {
+        for (int i = threadIdx.x; i < nseg; i += blockDim.x) sbeg[i] = segs[i].begin;
+        __syncthreads();
+    }
     if (n_dev) n = *n_dev;
+    const CNode* __restrict__ cn = cn0;
+    const TriRec* __restrict__ tris = tris0;
+    int seg = 0;
     TraceStats st;
     uint2 stack[kWideStack];
     bool more = true;
@@ -305,8 +316,21 @@ __global__ void __launch_bounds__(256)
         const unsigned idle = __ballot_sync(kFull, ray < 0);
         if (idle == kFull && !more) break;
         if (more && idle != 0 && (__popc(idle) >= refill || idle == kFull)) {
-            const int64_t r = claim(idle, counter, n, more);
+            int64_t r = claim(idle, counter, n, more);
             if (r >= 0) {
+                const cav_ray* rays = rays0;
+                const float* limit = limit0;
+                const int32_t* excl = excl0;
+                if (kSeg) {
+                    seg = find_seg(sbeg, nseg, r);
+                    const TraceSeg& G = segs[seg];
+                    cn = G.cnodes;
+                    tris = G.ctris;
+                    rays = G.rays;
+                    limit = G.limit;
+                    excl = G.excl;
+                    r -= G.begin;
+                }
                 const float4* rp = reinterpret_cast<const float4*>(rays + r);
                 const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
                 R.o = mk(r0.x, r0.y, r0.z);
@@ -411,8 +435,12 @@ __global__ void __launch_bounds__(256)
         }
         if (finished) {
             if (kAny) {
+                uint8_t* occ = kSeg ? segs[seg].occ : occ0;
                 occ[ray] = (uint8_t)result;
             } else {
+                int32_t* prim = kSeg ? segs[seg].prim : prim0;
+                float* tout = kSeg ? segs[seg].t : tout0;
+                float* uv = kSeg ? segs[seg].uv : uv0;
                 prim[ray] = hit ? bid : (bid == -2 ? -2 : -1);
                 if (tout) tout[ray] = hit ? best : __int_as_float(0x7f800000);
                 if (uv) reinterpret_cast<float2*>(uv)[ray] = make_float2(bu, bv);
@@ -434,19 +462,44 @@ cav_status launch_wide(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, in
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     int* flag = ctx->d_error + (kAny ? 3 : 2);
     if (stats) {
-        const int grid = grid_for(ctx, k_trace_wide<kAny, true>, block);
-        k_trace_wide<kAny, true><<<grid, block, 0, s>>>(bvh->cnodes, bvh->ctris, rays, n, n_dev, prim, t, uv, limit,
-                                                        excl, occ, counter, batch, flag, stats);
+        const int grid = grid_for(ctx, k_trace_wide<kAny, true, false>, block);
+        k_trace_wide<kAny, true, false><<<grid, block, 0, s>>>(bvh->cnodes, bvh->ctris, rays, n, n_dev, prim, t, uv,
+                                                               limit, excl, occ, counter, batch, flag, stats, nullptr, 0);
     } else {
-        const int grid = grid_for(ctx, k_trace_wide<kAny, false>, block);
-        k_trace_wide<kAny, false><<<grid, block, 0, s>>>(bvh->cnodes, bvh->ctris, rays, n, n_dev, prim, t, uv, limit,
-                                                         excl, occ, counter, batch, flag, nullptr);
+        const int grid = grid_for(ctx, k_trace_wide<kAny, false, false>, block);
+        k_trace_wide<kAny, false, false><<<grid, block, 0, s>>>(bvh->cnodes, bvh->ctris, rays, n, n_dev, prim, t, uv,
+                                                                limit, excl, occ, counter, batch, flag, nullptr, nullptr,
+                                                                0);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;
 }
 
 }  // namespace
+
+// Several jobs' rays, each against its own tree, in one fast-mode launch (the server's merged
+// wavefronts).  Every segment's cnodes / ctris must be set (ensure_wide on its tree).
+cav_status trace_wide_segments(cav_ctx* ctx, bool any_hit, const TraceSeg* segs, int nseg, int64_t n, cudaStream_t s,
+                               unsigned long long* counter) {
+    if (nseg <= 0 || n == 0) return CAV_OK;
+    if (nseg > kMaxSeg) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "too many trace segments in one launch");
+    const int block = ctx->wide_block > 0 ? ctx->wide_block : 128;
+    const int batch = ctx->wide_batch > 0 ? ctx->wide_batch : kDefaultRefill;
+    CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
+    if (any_hit) {
+        const int grid = grid_for(ctx, k_trace_wide<true, false, true>, block);
+        k_trace_wide<true, false, true><<<grid, block, 0, s>>>(nullptr, nullptr, nullptr, n, nullptr, nullptr, nullptr,
+                                                               nullptr, nullptr, nullptr, nullptr, counter, batch,
+                                                               ctx->d_error + 3, nullptr, segs, nseg);
+    } else {
+        const int grid = grid_for(ctx, k_trace_wide<false, false, true>, block);
+        k_trace_wide<false, false, true><<<grid, block, 0, s>>>(nullptr, nullptr, nullptr, n, nullptr, nullptr, nullptr,
+                                                                nullptr, nullptr, nullptr, nullptr, counter, batch,
+                                                                ctx->d_error + 2, nullptr, segs, nseg);
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    return CAV_OK;
+}
 
 cav_status ensure_wide(cav_ctx* ctx, const cav_bvh* bvh, cudaStream_t s) {
     if (bvh->cnodes) return CAV_OK;

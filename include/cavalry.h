@@ -75,6 +75,8 @@ cav_status cav_bvh_free(cav_bvh* bvh);
 int64_t cav_bvh_num_triangles(const cav_bvh* bvh);
 /* Tree depth (edges from the root to the deepest leaf); synchronises `stream`. */
 cav_status cav_bvh_depth(cav_ctx* ctx, const cav_bvh* bvh, void* stream, int32_t* depth);
+/* 1 once the tree's compressed 8-wide view (CAV_TRACE_FAST) has been built, else 0. */
+int cav_bvh_has_fast_layout(const cav_bvh* bvh);
 
 /*
  * Parity export of the final node array in the reference's BVHNode order
@@ -295,6 +297,7 @@ typedef struct cav_server_config {
     int max_live_jobs;        /* <= 0: 64 */
     int64_t max_paths_per_job; /* paths a render job keeps in flight (its time slice per tick);
                                   <= 0: 1M; a job's own max_paths_in_flight, when set, wins */
+    uint32_t trace_flags;      /* CAV_TRACE_EXACT (0) or CAV_TRACE_FAST: the merged launches' traversal */
 } cav_server_config;
 typedef struct cav_job_status {
     int state;         /* CAV_JOB_* */

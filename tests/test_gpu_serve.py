@@ -108,3 +108,33 @@ def test_server_close_with_pending_jobs(ctx, pool):
     ids = [sv.submit_render(pool[1], spp=4, max_depth=4)[0] for _ in range(4)]
     sv.wait(ids[0], 120)
     sv.close()  # finishes the live job, fails the never-started ones
+
+
+def test_fast_trace_server_matches_exact(ctx, pool):
+    """The server's merged launches in the compressed 8-wide mode: ray queries hit the same
+    distances as direct exact queries and renders agree with the exact renders (a closest
+    hit changes only at an equal-distance tie)."""
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    sv = cav.Server(ctx, mode=cav.SERVE_MERGED, trace_flags=cav.TRACE_FAST)
+    subs = [(k, *sv.submit_render(sc, spp=2, max_depth=4)) for k, sc in pool.items()]
+    bvh = pool[2].bvh()
+    rays = scenes.closest_rays(30000, seed=9)
+    jr, pr, tr, _ = sv.submit_rays(bvh, rays)
+    for k, jid, fs, fw in subs:
+        assert sv.wait(jid, 120).state == cav.JOB_DONE
+        s, w = direct_render(pool[k], 2)
+        assert np.array_equal(fw, w)
+        assert np.abs(fs - s).mean() <= 1e-3 * np.abs(s).mean() + 1e-6
+    assert sv.wait(jr, 60).state == cav.JOB_DONE
+    assert sv.stats().max_segments >= 2
+    sv.close()
+    assert pool[2].bvh().has_fast_layout()  # the server built the 8-wide view it traced
+    p, t, _ = bvh.trace_closest(torch.from_numpy(rays).cuda())
+    p, t = p.cpu().numpy(), t.cpu().numpy()
+    assert np.array_equal(pr >= 0, p >= 0)
+    both = p >= 0
+    assert np.all(np.abs(tr[both] - t[both]) <= 1e-6 * np.abs(t[both]))
