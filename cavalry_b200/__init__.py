@@ -410,7 +410,8 @@ class Scene:
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("mode", ctypes.c_int), ("max_live_jobs", ctypes.c_int),
-                ("max_paths_per_job", ctypes.c_int64), ("trace_flags", ctypes.c_uint32)]
+                ("max_paths_per_job", ctypes.c_int64), ("trace_flags", ctypes.c_uint32), ("lanes", ctypes.c_int),
+                ("min_paths_per_slice", ctypes.c_int64)]
 
 
 class JobStatus(ctypes.Structure):
@@ -440,9 +441,11 @@ class Server:
     :meth:`wait` reports the job done."""
 
     def __init__(self, ctx: "Context", hbm_budget_bytes: int = 80 << 30, mode: int = SERVE_MERGED,
-                 max_live_jobs: int = 64, max_paths_per_job: int = 0, trace_flags: int = TRACE_EXACT):
+                 max_live_jobs: int = 64, max_paths_per_job: int = 0, trace_flags: int = TRACE_EXACT, lanes: int = 0,
+                 min_paths_per_slice: int = 0):
         self.ctx = ctx
-        cfg = ServerConfig(hbm_budget_bytes, mode, max_live_jobs, max_paths_per_job, trace_flags)
+        cfg = ServerConfig(hbm_budget_bytes, mode, max_live_jobs, max_paths_per_job, trace_flags, lanes,
+                           min_paths_per_slice)
         h = ctypes.c_void_p()
         ctx._check(lib().cav_server_create(ctx.handle, ctypes.addressof(cfg), ctypes.byref(h)), "cav_server_create")
         self.handle = h

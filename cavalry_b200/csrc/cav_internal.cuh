@@ -216,7 +216,10 @@ cav_status mlp_forward(cav_mlp* m, const float* in, int64_t n, float* out, cudaS
 // Resumable path-integrator render (render.cu), advanced bounce by bounce by the server.
 struct PathJob;
 size_t path_job_bytes(const cav_scene* sc, const cav_render_opts* opts);
-cav_status path_job_create(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, cudaStream_t s, PathJob** out);
+cav_status path_job_create(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, int64_t slice, cudaStream_t s,
+                           PathJob** out);
+void path_job_set_slice(PathJob* J, int64_t slice);
+int64_t path_job_capacity(const PathJob* J);
 int64_t path_job_extend(PathJob* J, TraceSeg* seg);
 cav_status path_job_shade(PathJob* J, cudaStream_t s);
 int64_t path_job_shadow(PathJob* J, TraceSeg* seg);

@@ -599,6 +599,11 @@ cav_status render_path_graph(cav_ctx* ctx, cav_scene* sc, const cav_render_opts*
     const DevScene S = dev_scene_of(sc);
     const Camera cam = camera_of(sc, W, H);
     const unsigned blocks = (unsigned)div_up(chunk, kThreads);
+    const bool fast = opts && (opts->flags & CAV_RENDER_FAST_TRACE);
+    if (fast) {  // the 8-wide view is built (with host checks) before the capture begins
+        cav_status wst = ensure_wide(ctx, sc->bvh, s);
+        if (wst != CAV_OK) return wst;
+    }
     // capture and replay on the scene's own non-blocking stream (the legacy default stream
     // cannot be captured), ordered after and before the caller's stream by events
     const cudaStream_t caller = s;
@@ -621,11 +626,16 @@ cav_status render_path_graph(cav_ctx* ctx, cav_scene* sc, const cav_render_opts*
         for (int depth = 0; depth < max_depth && st == CAV_OK; ++depth) {
             const uint32_t* n_dev = depth == 0 ? cnt + 2 * max_depth : cnt + 2 * (depth - 1);
             Q.counters = cnt + 2 * depth;
-            st = trace_closest_dev(ctx, sc->bvh, Q.rays, n_dev, Q.hit_prim, Q.hit_t, Q.hit_uv, s, ctx->d_counters + 6);
+            st = fast ? trace_wide_closest(ctx, sc->bvh, Q.rays, INT64_MAX, n_dev, Q.hit_prim, Q.hit_t, Q.hit_uv, s,
+                                           ctx->d_counters + 6)
+                      : trace_closest_dev(ctx, sc->bvh, Q.rays, n_dev, Q.hit_prim, Q.hit_t, Q.hit_uv, s,
+                                          ctx->d_counters + 6);
             if (st != CAV_OK) break;
             k_shade<<<blocks, kThreads, 0, s>>>(S, depth, dim0, 0, P, Q, n_dev);
-            st = trace_any_dev(ctx, sc->bvh, Q.shadow_rays, Q.shadow_limit, Q.shadow_excl, cnt + 2 * depth + 1,
-                               Q.shadow_occ, s, ctx->d_counters + 7);
+            st = fast ? trace_wide_any(ctx, sc->bvh, Q.shadow_rays, Q.shadow_limit, Q.shadow_excl, INT64_MAX,
+                                       cnt + 2 * depth + 1, Q.shadow_occ, s, ctx->d_counters + 7)
+                      : trace_any_dev(ctx, sc->bvh, Q.shadow_rays, Q.shadow_limit, Q.shadow_excl, cnt + 2 * depth + 1,
+                                      Q.shadow_occ, s, ctx->d_counters + 7);
             if (st != CAV_OK) break;
             k_add_direct<<<blocks, kThreads, 0, s>>>(0, P, Q, cnt + 2 * depth + 1);
             std::swap(Q.active, Q.next_active);
@@ -669,6 +679,7 @@ struct PathJob {
     int W = 0, H = 0;
     int spp = 0, max_depth = 0;
     int64_t total = 0, chunk = 0, first = 0, m = 0, n = 0;
+    int64_t slice = 0;  // paths started per chunk (<= chunk, the state's capacity); 0: chunk
     int depth = 0, dim0 = 0;
     void* base = nullptr;
     float* d_sum = nullptr;
@@ -712,7 +723,8 @@ size_t path_job_bytes(const cav_scene* sc, const cav_render_opts* opts) {
     return path_state_bytes(chunk) + sizeof(float) * 4 * (int64_t)W * H + 512;
 }
 
-cav_status path_job_create(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, cudaStream_t s, PathJob** out) {
+cav_status path_job_create(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, int64_t slice, cudaStream_t s,
+                           PathJob** out) {
     auto* J = new PathJob();
     J->ctx = ctx;
     J->sc = sc;
@@ -754,7 +766,8 @@ cav_status path_job_create(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* o
     J->cam = camera_of(sc, J->W, J->H);
     CAV_CUDA(ctx, cudaMemsetAsync(J->d_sum, 0, sizeof(float) * 4 * pixels, s));
     J->first = 0;
-    J->m = std::min(J->chunk, J->total);
+    J->slice = slice > 0 ? std::min(slice, J->chunk) : J->chunk;
+    J->m = std::min(J->slice, J->total);
     k_generate<<<div_up(J->m, kThreads), kThreads, 0, s>>>(J->cam, J->S.halton, J->spp, 0, J->m, J->P, J->Q);
     J->n = J->m;
     J->depth = 0;
@@ -822,9 +835,9 @@ cav_status path_job_advance(PathJob* J, cudaStream_t s, bool* finished) {
         const cavpbrt::Scene& D = J->sc->desc;
         k_film<<<div_up(J->m, kThreads), kThreads, 0, s>>>(J->m, J->P, J->W, J->H, D.filter_xwidth,
                                                             D.filter_ywidth, J->d_sum, J->d_wsum);
-        J->first += J->chunk;
+        J->first += J->m;
         if (J->first < J->total) {
-            J->m = std::min(J->chunk, J->total - J->first);
+            J->m = std::min(J->slice, J->total - J->first);
             k_generate<<<div_up(J->m, kThreads), kThreads, 0, s>>>(J->cam, J->S.halton, J->spp, J->first, J->m, J->P,
                                                                   J->Q);
             J->n = J->m;
@@ -839,6 +852,11 @@ cav_status path_job_advance(PathJob* J, cudaStream_t s, bool* finished) {
     *finished = J->done;
     return CAV_OK;
 }
+
+// The paths the job's next chunk starts (clamped to the state's capacity).
+void path_job_set_slice(PathJob* J, int64_t slice) { J->slice = slice > 0 ? std::min(slice, J->chunk) : J->chunk; }
+
+int64_t path_job_capacity(const PathJob* J) { return J->chunk; }
 
 void path_job_film(PathJob* J, float** sum, float** wsum, int64_t* pixels) {
     *sum = J->d_sum;

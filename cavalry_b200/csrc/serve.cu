@@ -1,17 +1,21 @@
 // Serving loop with continuous batching: render jobs and ray-query jobs of uneven size are
 // admitted as they arrive (FIFO, under an HBM budget and a live-job limit), and every tick
-// advances all live jobs by one bounce with ONE closest-hit and ONE any-hit traversal
-// launch over the merged wavefronts of all of them (trace_*_segments: each segment is one
-// job's rays against its own resident BVH).  Shading stays per job (its own kernels on the
-// same stream).  Scenes and their BVHs are resident (cav_scene / cav_bvh handles owned by
-// the caller); path state lives on the device for the job's lifetime.
+// advances all live jobs of a lane by one bounce with ONE closest-hit and ONE any-hit
+// traversal launch over the merged wavefronts of all of them (trace_*_segments: each
+// segment is one job's rays against its own resident BVH).  Shading stays per job (its own
+// kernels on the lane's stream).  Scenes and their BVHs are resident (cav_scene / cav_bvh
+// handles owned by the caller); path state lives on the device for the job's lifetime.
+//
+// Lanes: a few host threads, each with its own stream and share of the live jobs, tick
+// independently, so the GPU runs one lane's traversal while the other lane's launches
+// drain their tails, its per-job kernels run and its host waits for queue counts.
 //
 // The reference renders one scene per process (main.cu:25-96) and has no request loop; the
-// baseline for this component is the same loop with one live job at a time
-// (CAV_SERVE_SEQUENTIAL), i.e. the plain sequential render loop over the same kernels.
+// baseline for this component is the plain sequential loop of cav_render calls (and
+// CAV_SERVE_SEQUENTIAL, one live job at a time, the same loop inside the server).
 //
-// A dedicated host thread runs the loop; submissions and polls from other threads take a
-// mutex.  Host buffers handed to a job must stay valid until the job is done.
+// Submissions and polls from other threads take a mutex.  Host buffers handed to a job
+// must stay valid until the job is done.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -75,46 +79,84 @@ size_t ray_job_bytes(int kind, int64_t n) {
 
 }  // namespace
 
-struct cav_server {
-    cav_ctx* ctx = nullptr;
-    cav_server_config cfg{};
+// One lane: a host thread with its own stream, live jobs and segment tables.  Lanes tick
+// independently and share the GPU, so one lane's launch tails and small per-job kernels
+// overlap the other lane's traversal.
+struct Lane {
+    int index = 0;
     cudaStream_t stream = nullptr;
     std::thread worker;
-    std::mutex mu;
-    std::condition_variable cv;       // work arrived / stop
-    std::condition_variable done_cv;  // a job finished
-    bool stop = false;
-    std::deque<Job*> pending;
-    std::vector<Job*> live;
-    std::unordered_map<int64_t, Job*> jobs;
-    int64_t next_id = 1;
-    size_t used = 0;
-    Clock::time_point t0;
+    std::vector<Job*> live;  // changed by the lane's own thread, under the server mutex
     // segment tables: pinned host staging + device copies, one pair per traversal kind
     cav::TraceSeg* h_seg_c = nullptr;
     cav::TraceSeg* h_seg_a = nullptr;
     cav::TraceSeg* d_seg_c = nullptr;
     cav::TraceSeg* d_seg_a = nullptr;
     unsigned long long* d_counter = nullptr;  // traversal work counters (2)
-    // statistics
+};
+
+struct cav_server {
+    cav_ctx* ctx = nullptr;
+    cav_server_config cfg{};
+    std::vector<Lane*> lanes;
+    std::mutex mu;
+    std::condition_variable cv;       // work arrived / memory freed / stop
+    std::condition_variable done_cv;  // a job finished
+    bool stop = false;
+    std::deque<Job*> pending;
+    std::unordered_map<int64_t, Job*> jobs;
+    int64_t next_id = 1;
+    size_t used = 0;
+    Clock::time_point t0;
+    // statistics (under mu)
     int64_t ticks = 0, closest_launches = 0, any_launches = 0, max_segments = 0;
     double busy_s = 0;
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
     uint32_t trace_flags() const { return cfg.trace_flags & CAV_TRACE_FAST ? CAV_TRACE_FAST : CAV_TRACE_EXACT; }
-    void run();
-    void admit_locked(std::vector<Job*>& started);
-    bool start(Job* j);
-    void tick();
-    void finish(Job* j, cav_status st);
+    int lane_limit() const {  // live jobs a lane keeps
+        if (cfg.mode == CAV_SERVE_SEQUENTIAL) return 1;
+        const int total = cfg.max_live_jobs > 0 ? cfg.max_live_jobs : 64;
+        const int nl = (int)lanes.size();
+        return std::max(1, (total + nl - 1) / nl);
+    }
+    int64_t live_count_locked() const {
+        int64_t k = 0;
+        for (const Lane* l : lanes) k += (int64_t)l->live.size();
+        return k;
+    }
+    int live_renders_locked() const {
+        int k = 0;
+        for (const Lane* l : lanes)
+            for (const Job* j : l->live) k += j->kind == kRender;
+        return k;
+    }
+    // Paths a render job's next chunk starts: the live render jobs share one job's capacity,
+    // but no slice drops below the configured floor (or the capacity, when that is smaller).
+    // A job alone runs chunks as large as cav_render's; many jobs advance in shorter ticks.
+    int64_t slice_for(int64_t capacity, int renders) const {
+        const int64_t floor_paths = std::min<int64_t>(capacity, cfg.min_paths_per_slice);
+        return std::max(floor_paths, capacity / std::max(renders, 1));
+    }
+    bool can_admit_locked(const Lane* l) const;
+    void run(Lane* l);
+    void admit_locked(Lane* l, std::vector<Job*>& started);
+    bool start(Lane* l, Job* j);
+    void tick(Lane* l);
+    void finish(Lane* l, Job* j, cav_status st);
 };
 
-void cav_server::admit_locked(std::vector<Job*>& started) {
-    const int max_live = cfg.mode == CAV_SERVE_SEQUENTIAL ? 1 : (cfg.max_live_jobs > 0 ? cfg.max_live_jobs : 64);
-    while (!pending.empty() && (int)live.size() + (int)started.size() < max_live) {
+bool cav_server::can_admit_locked(const Lane* l) const {
+    if (pending.empty() || (int)l->live.size() >= lane_limit()) return false;
+    // FIFO under the HBM budget; a job larger than the whole budget runs alone
+    return live_count_locked() == 0 || used + pending.front()->bytes <= (size_t)cfg.hbm_budget_bytes;
+}
+
+void cav_server::admit_locked(Lane* l, std::vector<Job*>& started) {
+    const int limit = lane_limit();
+    while (!pending.empty() && (int)l->live.size() + (int)started.size() < limit) {
         Job* j = pending.front();
-        const bool alone = live.empty() && started.empty();
-        // FIFO under the HBM budget; a job larger than the whole budget runs alone
+        const bool alone = live_count_locked() == 0 && started.empty();
         if (!alone && used + j->bytes > (size_t)cfg.hbm_budget_bytes) break;
         pending.pop_front();
         used += j->bytes;
@@ -123,17 +165,24 @@ void cav_server::admit_locked(std::vector<Job*>& started) {
     }
 }
 
-bool cav_server::start(Job* j) {
+bool cav_server::start(Lane* l, Job* j) {
     j->t_start = now();
     cav_status st = CAV_OK;
+    const cudaStream_t stream = l->stream;
     const cav_bvh* tree = j->kind == kRender ? cav_scene_bvh(j->scene) : j->bvh;
     if (trace_flags() == CAV_TRACE_FAST) st = cav::ensure_wide(ctx, tree, stream);  // once per tree
     if (st != CAV_OK) {
-        finish(j, st);
+        finish(l, j, st);
         return false;
     }
     if (j->kind == kRender) {
-        st = cav::path_job_create(ctx, j->scene, &j->opts, stream, &j->pj);
+        int renders;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            renders = 1 + live_renders_locked();
+        }
+        st = cav::path_job_create(ctx, j->scene, &j->opts, slice_for(j->opts.max_paths_in_flight, renders), stream,
+                                  &j->pj);
     } else {
         if (cudaMallocAsync(&j->dbuf, j->bytes, stream) != cudaSuccess) {
             cudaGetLastError();
@@ -165,19 +214,19 @@ bool cav_server::start(Job* j) {
         }
     }
     if (st != CAV_OK) {
-        finish(j, st);
+        finish(l, j, st);
         return false;
     }
     return true;
 }
 
-void cav_server::finish(Job* j, cav_status st) {
+void cav_server::finish(Lane* l, Job* j, cav_status st) {
     if (j->pj) {
-        cav::path_job_destroy(j->pj, stream);
+        cav::path_job_destroy(j->pj, l->stream);
         j->pj = nullptr;
     }
     if (j->dbuf) {
-        cudaFreeAsync(j->dbuf, stream);
+        cudaFreeAsync(j->dbuf, l->stream);
         j->dbuf = nullptr;
     }
     std::lock_guard<std::mutex> lk(mu);
@@ -186,14 +235,17 @@ void cav_server::finish(Job* j, cav_status st) {
     j->state = st == CAV_OK ? CAV_JOB_DONE : CAV_JOB_FAILED;
     j->t_done = now();
     done_cv.notify_all();
+    cv.notify_all();  // memory came free: another lane may admit
 }
 
-// One bounce of every live job: merged extend traversal, per-job shading, merged shadow
-// traversal, per-job accumulation; finished jobs copy their results out.
-void cav_server::tick() {
+// One bounce of every live job of the lane: merged extend traversal, per-job shading,
+// merged shadow traversal, per-job accumulation; finished jobs copy their results out.
+void cav_server::tick(Lane* l) {
     const auto t_begin = Clock::now();
-    ++ticks;
+    const cudaStream_t stream = l->stream;
+    std::vector<Job*>& live = l->live;
     cav_status err = CAV_OK;
+    int64_t segs_c = 0, launches_c = 0, launches_a = 0;
     // ---- extend (closest hit): render jobs' current rays + closest-hit query jobs
     int nc = 0;
     int64_t total = 0;
@@ -219,15 +271,15 @@ void cav_server::tick() {
         if (k <= 0) continue;
         if (nc == cav::trace_max_segments()) break;  // the rest waits for the next tick
         sg.begin = total;
-        h_seg_c[nc++] = sg;
+        l->h_seg_c[nc++] = sg;
         total += k;
         in_c.push_back(j);
     }
     if (nc > 0) {
-        max_segments = std::max<int64_t>(max_segments, nc);
-        cudaMemcpyAsync(d_seg_c, h_seg_c, sizeof(cav::TraceSeg) * nc, cudaMemcpyHostToDevice, stream);
-        err = cav::trace_closest_segments(ctx, d_seg_c, nc, total, trace_flags(), stream, d_counter);
-        ++closest_launches;
+        segs_c = nc;
+        cudaMemcpyAsync(l->d_seg_c, l->h_seg_c, sizeof(cav::TraceSeg) * nc, cudaMemcpyHostToDevice, stream);
+        err = cav::trace_closest_segments(ctx, l->d_seg_c, nc, total, trace_flags(), stream, l->d_counter);
+        ++launches_c;
     }
     std::vector<Job*> shaded;
     for (Job* j : in_c) {
@@ -265,21 +317,27 @@ void cav_server::tick() {
         if (k <= 0) continue;
         if (na == cav::trace_max_segments()) break;
         sg.begin = total;
-        h_seg_a[na++] = sg;
+        l->h_seg_a[na++] = sg;
         total += k;
         in_a.push_back(j);
     }
     if (na > 0 && err == CAV_OK) {
-        cudaMemcpyAsync(d_seg_a, h_seg_a, sizeof(cav::TraceSeg) * na, cudaMemcpyHostToDevice, stream);
-        err = cav::trace_any_segments(ctx, d_seg_a, na, total, trace_flags(), stream, d_counter + 1);
-        ++any_launches;
+        cudaMemcpyAsync(l->d_seg_a, l->h_seg_a, sizeof(cav::TraceSeg) * na, cudaMemcpyHostToDevice, stream);
+        err = cav::trace_any_segments(ctx, l->d_seg_a, na, total, trace_flags(), stream, l->d_counter + 1);
+        ++launches_a;
     }
     for (Job* j : in_a)
         if (j->kind == kAny) j->traced = true;
     // ---- advance render jobs; results of finished jobs
     std::vector<Job*> done;
+    int renders;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        renders = live_renders_locked();
+    }
     for (Job* j : shaded) {
         bool fin = false;
+        cav::path_job_set_slice(j->pj, slice_for(cav::path_job_capacity(j->pj), renders));
         cav::path_job_advance(j->pj, stream, &fin);
         ++j->bounces;
         if (fin) {
@@ -304,13 +362,20 @@ void cav_server::tick() {
     }
     cudaError_t ce = cudaStreamSynchronize(stream);
     if (ce != cudaSuccess && err == CAV_OK) err = cav::cuda_error(ctx, ce, "serve tick");
-    if (err != CAV_OK) {  // a failed launch fails every live job
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        ++ticks;
+        closest_launches += launches_c;
+        any_launches += launches_a;
+        max_segments = std::max(max_segments, segs_c);
+    }
+    if (err != CAV_OK) {  // a failed launch fails every live job of the lane
         std::vector<Job*> all;
         {
             std::lock_guard<std::mutex> lk(mu);
             all.swap(live);
         }
-        for (Job* j : all) finish(j, err);
+        for (Job* j : all) finish(l, j, err);
         return;
     }
     for (Job* j : done) {
@@ -318,19 +383,21 @@ void cav_server::tick() {
             std::lock_guard<std::mutex> lk(mu);
             live.erase(std::find(live.begin(), live.end(), j));
         }
-        finish(j, CAV_OK);
+        finish(l, j, CAV_OK);
     }
-    busy_s += std::chrono::duration<double>(Clock::now() - t_begin).count();
+    const double dt = std::chrono::duration<double>(Clock::now() - t_begin).count();
+    std::lock_guard<std::mutex> lk(mu);
+    busy_s += dt;
 }
 
-void cav_server::run() {
+void cav_server::run(Lane* l) {
     cudaSetDevice(ctx->device);
     for (;;) {
         std::vector<Job*> started;
         {
             std::unique_lock<std::mutex> lk(mu);
-            cv.wait(lk, [&] { return stop || !pending.empty() || !live.empty(); });
-            if (stop && live.empty()) {
+            cv.wait(lk, [&] { return stop || !l->live.empty() || can_admit_locked(l); });
+            if (stop && l->live.empty()) {
                 for (Job* j : pending) {  // never started
                     j->state = CAV_JOB_FAILED;
                     j->status = CAV_ERR_NOT_READY;
@@ -340,14 +407,14 @@ void cav_server::run() {
                 done_cv.notify_all();
                 return;
             }
-            if (!stop) admit_locked(started);
+            if (!stop) admit_locked(l, started);
         }
         for (Job* j : started)
-            if (start(j)) {
+            if (start(l, j)) {
                 std::lock_guard<std::mutex> lk(mu);
-                live.push_back(j);
+                l->live.push_back(j);
             }
-        if (!live.empty()) tick();
+        if (!l->live.empty()) tick(l);
     }
 }
 
@@ -363,7 +430,7 @@ cav_status cav_server_create(cav_ctx* ctx, const cav_server_config* cfg, cav_ser
     sv->cfg.hbm_budget_bytes = (int64_t)80 << 30;
     sv->cfg.mode = CAV_SERVE_MERGED;
     sv->cfg.max_live_jobs = 64;
-    sv->cfg.max_paths_per_job = (int64_t)1 << 20;
+    sv->cfg.max_paths_per_job = (int64_t)1 << 22;
     if (cfg) {
         if (cfg->hbm_budget_bytes > 0) sv->cfg.hbm_budget_bytes = cfg->hbm_budget_bytes;
         sv->cfg.mode = cfg->mode;
@@ -371,41 +438,54 @@ cav_status cav_server_create(cav_ctx* ctx, const cav_server_config* cfg, cav_ser
         if (cfg->max_paths_per_job > 0) sv->cfg.max_paths_per_job = cfg->max_paths_per_job;
         sv->cfg.trace_flags = cfg->trace_flags;
     }
+    sv->cfg.min_paths_per_slice = cfg && cfg->min_paths_per_slice > 0 ? cfg->min_paths_per_slice : (int64_t)1 << 22;
+    int nl = cfg && cfg->lanes > 0 ? std::min(cfg->lanes, 8) : 1;
+    if (sv->cfg.mode == CAV_SERVE_SEQUENTIAL) nl = 1;
+    sv->cfg.lanes = nl;
     const int ms = cav::trace_max_segments();
-    cudaError_t e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMallocHost(&sv->h_seg_c, sizeof(cav::TraceSeg) * ms);
-    if (e == cudaSuccess) e = cudaMallocHost(&sv->h_seg_a, sizeof(cav::TraceSeg) * ms);
-    if (e == cudaSuccess) e = cudaMalloc(&sv->d_seg_c, sizeof(cav::TraceSeg) * ms);
-    if (e == cudaSuccess) e = cudaMalloc(&sv->d_seg_a, sizeof(cav::TraceSeg) * ms);
-    if (e == cudaSuccess) e = cudaMalloc(&sv->d_counter, 64);
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < nl && e == cudaSuccess; ++k) {
+        auto* l = new Lane();
+        l->index = k;
+        sv->lanes.push_back(l);
+        e = cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaMallocHost(&l->h_seg_c, sizeof(cav::TraceSeg) * ms);
+        if (e == cudaSuccess) e = cudaMallocHost(&l->h_seg_a, sizeof(cav::TraceSeg) * ms);
+        if (e == cudaSuccess) e = cudaMalloc(&l->d_seg_c, sizeof(cav::TraceSeg) * ms);
+        if (e == cudaSuccess) e = cudaMalloc(&l->d_seg_a, sizeof(cav::TraceSeg) * ms);
+        if (e == cudaSuccess) e = cudaMalloc(&l->d_counter, 64);
+    }
     if (e != cudaSuccess) {
         cav_server_destroy(sv);
         return cav::cuda_error(ctx, e, "cav_server_create");
     }
     sv->t0 = Clock::now();
-    sv->worker = std::thread([sv] { sv->run(); });
+    for (Lane* l : sv->lanes) l->worker = std::thread([sv, l] { sv->run(l); });
     *out = sv;
     return CAV_OK;
 }
 
 cav_status cav_server_destroy(cav_server* sv) {
     if (!sv) return CAV_OK;
-    if (sv->worker.joinable()) {
-        {
-            std::lock_guard<std::mutex> lk(sv->mu);
-            sv->stop = true;
-        }
-        sv->cv.notify_all();
-        sv->worker.join();
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
     }
-    if (sv->stream) cudaStreamSynchronize(sv->stream);
+    sv->cv.notify_all();
+    for (Lane* l : sv->lanes)
+        if (l->worker.joinable()) l->worker.join();
+    for (Lane* l : sv->lanes)
+        if (l->stream) cudaStreamSynchronize(l->stream);
     for (auto& kv : sv->jobs) delete kv.second;
-    cudaFreeHost(sv->h_seg_c);
-    cudaFreeHost(sv->h_seg_a);
-    cudaFree(sv->d_seg_c);
-    cudaFree(sv->d_seg_a);
-    cudaFree(sv->d_counter);
-    if (sv->stream) cudaStreamDestroy(sv->stream);
+    for (Lane* l : sv->lanes) {
+        cudaFreeHost(l->h_seg_c);
+        cudaFreeHost(l->h_seg_a);
+        cudaFree(l->d_seg_c);
+        cudaFree(l->d_seg_a);
+        cudaFree(l->d_counter);
+        if (l->stream) cudaStreamDestroy(l->stream);
+        delete l;
+    }
     delete sv;
     return CAV_OK;
 }
@@ -504,7 +584,7 @@ cav_status cav_server_stats(cav_server* sv, cav_server_stats_t* out) {
     out->busy_s = sv->busy_s;
     out->now_s = sv->now();
     out->pending = (int64_t)sv->pending.size();
-    out->live = (int64_t)sv->live.size();
+    out->live = sv->live_count_locked();
     out->hbm_in_use = (int64_t)sv->used;
     return CAV_OK;
 }

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <mutex>
 
 #include "trace_common.cuh"
 
@@ -502,6 +503,10 @@ cav_status trace_wide_segments(cav_ctx* ctx, bool any_hit, const TraceSeg* segs,
 }
 
 cav_status ensure_wide(cav_ctx* ctx, const cav_bvh* bvh, cudaStream_t s) {
+    // serialised: several host threads (the server's lanes) may reach one tree at once; the
+    // view is published only once its build has completed on the device
+    static std::mutex build_mu;
+    std::lock_guard<std::mutex> lk(build_mu);
     if (bvh->cnodes) return CAV_OK;
     const int64_t n = bvh->n;
     const int64_t nw = n - 1;  // each wide node but the root stands for a distinct binary internal node

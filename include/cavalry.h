@@ -295,9 +295,15 @@ typedef struct cav_server_config {
     int64_t hbm_budget_bytes; /* <= 0: 80 GiB */
     int mode;                 /* CAV_SERVE_MERGED or CAV_SERVE_SEQUENTIAL */
     int max_live_jobs;        /* <= 0: 64 */
-    int64_t max_paths_per_job; /* paths a render job keeps in flight (its time slice per tick);
-                                  <= 0: 1M; a job's own max_paths_in_flight, when set, wins */
+    int64_t max_paths_per_job; /* path state a render job holds (<= 0: 4M; a job's own
+                                  max_paths_in_flight, when set, wins).  Each chunk starts
+                                  max(this / live render jobs, min_paths_per_slice) paths */
     uint32_t trace_flags;      /* CAV_TRACE_EXACT (0) or CAV_TRACE_FAST: the merged launches' traversal */
+    int lanes;                 /* host threads, each with its own stream and live jobs, ticking
+                                  independently on the one GPU (<= 0: 1; sequential mode: 1) */
+    int64_t min_paths_per_slice; /* floor of a render job's chunk while others are live (<= 0:
+                                  4M, i.e. every chunk as large as the job's state allows);
+                                  smaller floors shorten ticks (latency) at some throughput */
 } cav_server_config;
 typedef struct cav_job_status {
     int state;         /* CAV_JOB_* */

@@ -221,17 +221,18 @@ def test_resolution_override_matches_scene_film(ctx, tmp_path):
     assert np.allclose(s1, s2, rtol=2e-5, atol=1e-6)
 
 
+@pytest.mark.parametrize("fast", [False, True])
 @pytest.mark.parametrize("chunk", [0, 3000])
-def test_graph_replayed_render_matches(ctx, tmp_path, chunk):
+def test_graph_replayed_render_matches(ctx, tmp_path, chunk, fast):
     """The CUDA-graph render (queue sizes on the device, one graph per chunk) gives the
-    stream-ordered render's film and ray counts."""
+    stream-ordered render's film and ray counts, in both traversal modes."""
     from cavalry_b200 import scenes
 
-    sc, _ = load(ctx, tmp_path, f"graph{chunk}", scenes.sphere_scene(8, 2, seed=5),
+    sc, _ = load(ctx, tmp_path, f"graph{chunk}{fast}", scenes.sphere_scene(8, 2, seed=5),
                  dict(width=64, height=48, spp=4, max_depth=6))
-    s1, w1, _ = sc.render(max_paths_in_flight=chunk)
+    s1, w1, _ = sc.render(max_paths_in_flight=chunk, fast_trace=fast)
     st1 = sc.stats()
-    s2, w2, _ = sc.render(max_paths_in_flight=chunk, graph=True)
+    s2, w2, _ = sc.render(max_paths_in_flight=chunk, graph=True, fast_trace=fast)
     st2 = sc.stats()
     assert np.array_equal(w1, w2)
     assert np.allclose(s1, s2, rtol=2e-5, atol=1e-6)

@@ -56,12 +56,13 @@ def test_ray_jobs_match_direct_queries(ctx, pool):
 @pytest.mark.parametrize("mode", ["merged", "sequential"])
 def test_mixed_jobs_same_as_alone(ctx, pool, mode):
     """Renders of three scenes and two ray-query jobs submitted together: every result
-    equals the job run alone (films up to float atomic order)."""
+    equals the job run alone (films up to float atomic order).  One lane, so the merged
+    server puts every live job in the same launches."""
     import cavalry_b200 as cav
     from cavalry_b200 import scenes
 
     alone = {k: direct_render(sc, 2) for k, sc in pool.items()}
-    sv = cav.Server(ctx, mode=cav.SERVE_MERGED if mode == "merged" else cav.SERVE_SEQUENTIAL)
+    sv = cav.Server(ctx, mode=cav.SERVE_MERGED if mode == "merged" else cav.SERVE_SEQUENTIAL, lanes=1)
     subs = []
     for k, sc in pool.items():
         jid, fs, fw = sv.submit_render(sc, spp=2, max_depth=4)
@@ -87,6 +88,46 @@ def test_mixed_jobs_same_as_alone(ctx, pool, mode):
         assert stats.max_segments >= 2
     else:
         assert stats.max_segments == 1
+
+
+@pytest.mark.parametrize("lanes", [2, 3])
+def test_lanes_many_jobs_same_as_alone(ctx, pool, lanes):
+    """Several lanes (host threads with their own streams) serving a burst of renders and
+    ray queries over the same resident scenes, in both traversal modes: every job finishes
+    with the result it has alone."""
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    alone = {k: direct_render(sc, 2) for k, sc in pool.items()}
+    rays = scenes.closest_rays(20000, seed=11)
+    p_ref, _, _ = pool[0].bvh().trace_closest(torch.from_numpy(rays).cuda())
+    p_ref = p_ref.cpu().numpy()
+    for flags in (cav.TRACE_EXACT, cav.TRACE_FAST):
+        sv = cav.Server(ctx, mode=cav.SERVE_MERGED, trace_flags=flags, lanes=lanes, max_paths_per_job=4096)
+        subs, rq = [], []
+        for rep in range(4):
+            for k, sc in pool.items():
+                subs.append((k, *sv.submit_render(sc, spp=2, max_depth=4)))
+            rq.append(sv.submit_rays(pool[0].bvh(), rays))
+        for k, jid, fs, fw in subs:
+            assert sv.wait(jid, 120).state == cav.JOB_DONE
+            s, w = alone[k]
+            assert np.array_equal(fw, w)
+            if flags == cav.TRACE_EXACT:
+                assert np.allclose(fs, s, rtol=2e-5, atol=1e-6)
+            else:
+                assert np.abs(fs - s).mean() <= 1e-3 * np.abs(s).mean() + 1e-6
+        for jid, pr, _, _ in rq:
+            assert sv.wait(jid, 60).state == cav.JOB_DONE
+            if flags == cav.TRACE_EXACT:
+                assert np.array_equal(pr, p_ref)
+            else:
+                assert np.array_equal(pr >= 0, p_ref >= 0)
+        st = sv.stats()
+        assert st.live == 0 and st.pending == 0 and st.hbm_in_use == 0
+        sv.close()
 
 
 def test_small_hbm_budget_still_completes(ctx, pool):
@@ -119,7 +160,7 @@ def test_fast_trace_server_matches_exact(ctx, pool):
     import cavalry_b200 as cav
     from cavalry_b200 import scenes
 
-    sv = cav.Server(ctx, mode=cav.SERVE_MERGED, trace_flags=cav.TRACE_FAST)
+    sv = cav.Server(ctx, mode=cav.SERVE_MERGED, trace_flags=cav.TRACE_FAST, lanes=1)
     subs = [(k, *sv.submit_render(sc, spp=2, max_depth=4)) for k, sc in pool.items()]
     bvh = pool[2].bvh()
     rays = scenes.closest_rays(30000, seed=9)
