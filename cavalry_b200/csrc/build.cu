@@ -978,8 +978,10 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     acc(sizeof(uint32_t) * 32);                     // tile counters
     acc(sizeof(int32_t) * 6 * K * 2);               // bounds (ordered ints, floats)
     acc(sizeof(int32_t) * 8);                       // error flag
-    acc(sizeof(uint32_t) * std::max<int64_t>(total_int, cmax));  // visited (refit, then treelets)
-    acc(sizeof(int32_t) * nmax);                    // leaf list
+    acc(sizeof(uint32_t) * std::max<int64_t>(total_int, 2 * total - K));  // visited (refit, then treelets)
+    acc(sizeof(int32_t) * total);                   // leaf lists of all trees
+    acc(sizeof(uint32_t) * K);                      // leaf-list counters
+    acc(sizeof(TreeletSeg) * K);                    // treelet table
     acc(sizeof(int32_t) * cmax);                    // compact index
     acc(sizeof(int32_t) * nmax);                    // slot_of
     acc(sizeof(uint32_t) * (div_up(cmax, kScanTile) + 1));
@@ -1004,8 +1006,10 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     int32_t* bounds_ord = carve<int32_t>(q, 6 * K);
     float* dbounds = carve<float>(q, 6 * K);
     int32_t* err = carve<int32_t>(q, 8);
-    uint32_t* visited = carve<uint32_t>(q, std::max<int64_t>(total_int, cmax));
-    int32_t* leaf_list = carve<int32_t>(q, nmax);
+    uint32_t* visited = carve<uint32_t>(q, std::max<int64_t>(total_int, 2 * total - K));
+    int32_t* leaf_list = carve<int32_t>(q, total);
+    uint32_t* leaf_ctr = carve<uint32_t>(q, K);
+    TreeletSeg* tsegs = carve<TreeletSeg>(q, K);
     int32_t* compact = carve<int32_t>(q, cmax);
     int32_t* slot_of = carve<int32_t>(q, nmax);
     uint32_t* blk = carve<uint32_t>(q, div_up(cmax, kScanTile) + 1);
@@ -1014,6 +1018,9 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     CAV_CUDA(ctx, cudaMemcpy(dsegs, hs.data(), sizeof(BuildSeg) * K, cudaMemcpyHostToDevice));
     CAV_CUDA(ctx, cudaMemcpy(d_leaf, leaf_offs.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice));
     CAV_CUDA(ctx, cudaMemcpy(d_int, int_offs.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice));
+    std::vector<TreeletSeg> tsegs_host(K);
+    for (int k = 0; k < K; ++k) tsegs_host[k] = TreeletSeg{bv[k]->nodes, num_triangles[k]};
+    CAV_CUDA(ctx, cudaMemcpy(tsegs, tsegs_host.data(), sizeof(TreeletSeg) * K, cudaMemcpyHostToDevice));
     CAV_CUDA(ctx, cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 2 * 8 * 256, s));
     CAV_CUDA(ctx, cudaMemsetAsync(status, 0, sizeof(uint32_t) * (8 + passes2) * (size_t)tiles * 256, s));
     CAV_CUDA(ctx, cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 32, s));
@@ -1065,16 +1072,20 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     k_refit_batch<<<gb, kThreads, 0, s>>>(leafbox, vin, dsegs, d_leaf, d_int, K, total, visited, err);
     for (int k = 0; k < K; ++k) cudaEventRecord(bv[k]->ev[4], s);
     CAV_CUDA(ctx, cudaGetLastError());
-    // per scene: treelet rounds and traversal layout
-    for (int k = 0; k < K; ++k) {
-        cav_bvh* b = bv[k];
-        const int64_t n = num_triangles[k], count = 2 * n - 1;
-        cav_status st = treelet_rounds(ctx, b->nodes, n, rounds, leaf_list, visited, s);
+    // treelet rounds of all scenes (two launches per round and group of scenes), then the
+    // traversal layout per scene
+    {
+        cav_status st = treelet_rounds_batch(ctx, tsegs, tsegs_host.data(), d_leaf, leaf_offs.data(), K, rounds,
+                                             leaf_list, leaf_ctr, visited, s);
         if (st != CAV_OK) {
             cudaFreeAsync(sbase, s);
             return fail(st);
         }
-        cudaEventRecord(b->ev[5], s);
+    }
+    for (int k = 0; k < K; ++k) cudaEventRecord(bv[k]->ev[5], s);
+    for (int k = 0; k < K; ++k) {
+        cav_bvh* b = bv[k];
+        const int64_t n = num_triangles[k], count = 2 * n - 1;
         const int nblk = div_up(count, kScanTile);
         k_count_internal<<<nblk, kScanThreads, 0, s>>>(b->nodes, count, blk);
         k_scan_blocks<<<1, kScanThreads, 0, s>>>(blk, nblk);

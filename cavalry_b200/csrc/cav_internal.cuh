@@ -160,6 +160,13 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
 // treelet.cu
 cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int32_t* leaf_list, uint32_t* visited,
                           cudaStream_t s);
+struct TreeletSeg {  // one tree of a batched treelet pass
+    BNode* nodes;
+    int64_t n;  // leaves (triangles)
+};
+cav_status treelet_rounds_batch(cav_ctx* ctx, const TreeletSeg* segs, const TreeletSeg* segs_host,
+                                const int64_t* leaf_off, const int64_t* leaf_off_host, int K, int rounds,
+                                int32_t* leaf_list, uint32_t* counters, uint32_t* visited, cudaStream_t s);
 // trace.cu
 // A traversal segment: one job's rays against one tree, with its own outputs.  `begin` is
 // the segment's first index in the launch's global ray numbering.
