@@ -25,7 +25,7 @@ namespace cav {
 
 namespace {
 
-constexpr int kWarpsPerBlock = 8;
+constexpr int kWarpsPerBlock = 1;  // see k_treelet
 constexpr unsigned kFull = 0xffffffffu;
 
 struct SubsetTable {
@@ -404,10 +404,13 @@ __device__ void treelet_walk(BNode* nodes, int32_t curr, int32_t count, uint32_t
     }
 }
 
-// 4 blocks per SM (64 registers, about 200 bytes spilled to local memory): the walk waits
-// on atomics and dependent loads, so resident warps matter more than registers.  Measured on
-// 3 rounds over a 1M-triangle soup: 17.4 ms at 2 blocks (98 registers), 15.0 at 3, 11.4 at 4.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_treelet(BNode* nodes, const int32_t* __restrict__ list,
+// One warp per block, 32 blocks per SM (64 registers): the walk waits on atomics and
+// dependent loads, so resident warps matter more than registers, and most warps exit after
+// one step (first arrivals), which frees a one-warp block's slot at once, where a larger
+// block holds its slots until its last warp reaches the top.  Measured on 3 rounds over a
+// 1M-triangle soup: 8 warps per block at 98 registers 17.4 ms, at 80 15.0, at 64 11.4;
+// 2 warps per block 9.2; 1 warp 8.3.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 32) k_treelet(BNode* nodes, const int32_t* __restrict__ list,
                                                                  int64_t n, uint32_t* visited, int* err) {
     __shared__ WarpSmem smem[kWarpsPerBlock];
     const int w = threadIdx.x >> 5;
@@ -455,7 +458,7 @@ __global__ void k_leaf_list_batch(const TreeletSeg* __restrict__ segs, const int
     if (pos < (uint32_t)n) list[leaf_off[k] + pos] = (int32_t)local;
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 32)
     k_treelet_batch(const TreeletSeg* __restrict__ segs, const int64_t* __restrict__ leaf_off, int k0, int k1,
                     const int32_t* __restrict__ list, uint32_t* visited, int* err) {
     __shared__ WarpSmem smem[kWarpsPerBlock];
