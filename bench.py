@@ -361,6 +361,12 @@ def run_ours(args):
         "build": {
             "ms": round(statistics.mean(builds_ms), 3),
             "builds_per_s": round(1000.0 / statistics.mean(builds_ms), 2),
+            # algorithmic bytes: ~390 B per triangle for the LBVH stages (vertices in, codes,
+            # 6 sort passes, radix tree, refit, node write) plus, per treelet round, every
+            # node read and written once (2N-1 x 128 B); latency-bound, so far below HBM
+            "algorithmic_bytes": int(390 * N_TRI + ROUNDS * (2 * N_TRI - 1) * 128),
+            "achieved_gbs": round((390 * N_TRI + ROUNDS * (2 * N_TRI - 1) * 128)
+                                  / (statistics.mean(builds_ms) * 1e-3) / 1e9, 1),
             "stage_ms": {k: round(v, 4) for k, v in zip(
                 ["boxes_morton", "sort", "radix_tree", "refit", "treelet_rounds", "layout"], stage)},
         },
