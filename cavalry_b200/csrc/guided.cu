@@ -141,7 +141,10 @@ __global__ void k_g_features(DevScene S, const float* box, int64_t n, Queues Q, 
 }
 
 // k_shade of the path integrator with the guided continuation and its MIS density.
-__global__ void k_g_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Queues Q, const float* feat,
+// 2 blocks per SM (128 registers, about 200 bytes spilled) instead of 1 at 146 registers:
+// the 640x360 64-spp guided render of the aperture scene took 163 ms at 1 block, 153 at 2
+// and 152 at 3 (80 registers, about 1 KB spilled).
+__global__ void __launch_bounds__(kThreads, 2) k_g_shade(DevScene S, int depth, int dim0, int64_t n, Paths P, Queues Q, const float* feat,
                           const float* mout, float alpha, Records R, int record) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = j < n;
