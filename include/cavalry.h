@@ -281,12 +281,12 @@ cav_status cav_write_png(const char* path, const uint8_t* rgb, int width, int he
 cav_status cav_write_pfm(const char* path, const float* film_sum, const float* film_weight, int width, int height);
 
 /*
- * Serving with continuous batching (serve.cu).  A server owns a host thread and a stream;
- * jobs are admitted FIFO as the HBM budget and the live-job limit allow, and every tick
- * advances all live jobs by one bounce with one merged closest-hit and one merged any-hit
- * traversal launch over all their rays (each job against its own resident BVH).
- * CAV_SERVE_SEQUENTIAL runs one job at a time through the same kernels: the plain
- * sequential loop.  Scenes, BVHs and host buffers must outlive their jobs.
+ * Serving with continuous batching (serve.cu).  A server owns host threads ("lanes", one by
+ * default), each with a stream; jobs are admitted FIFO as the HBM budget and the live-job
+ * limit allow, and every tick advances all live jobs of a lane by one bounce with one
+ * merged closest-hit and one merged any-hit traversal launch over all their rays (each job
+ * against its own resident BVH).  CAV_SERVE_SEQUENTIAL runs one job at a time through the
+ * same kernels.  Scenes, BVHs and host buffers must outlive their jobs.
  */
 typedef struct cav_server cav_server;
 enum { CAV_SERVE_MERGED = 0, CAV_SERVE_SEQUENTIAL = 1 };
