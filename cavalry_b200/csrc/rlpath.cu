@@ -282,7 +282,10 @@ __global__ void k_rl_occlusion(int64_t m, Queues Q, RLTask T) {
 // The end of computeLighting (light statistics), computeQDistributions and
 // accumulateLightingContribs for one hit.  dim_out receives the maximum dimension reached
 // (syncDimension before genNextRay).
-__global__ void __launch_bounds__(128) k_rl_q(DevScene S, QTable QT, LightTable LT, const int32_t* dim_in, int64_t n,
+// 6 blocks of 128 per SM (80 registers, a few bytes spilled) rather than 4 at 117: more
+// resident warps for a kernel that waits on the Q-table and light-table loads (with the
+// k_rl_next bound below: 640x360 64-spp rlpath render of the aperture scene 179 -> 172 ms)
+__global__ void __launch_bounds__(128, 6) k_rl_q(DevScene S, QTable QT, LightTable LT, const int32_t* dim_in, int64_t n,
                                               Paths P, Queues Q, RLTask T, RLPath R, int32_t* dim_out) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int prim = j < n ? Q.hit_prim[j] : -1;
@@ -458,7 +461,8 @@ __global__ void k_rl_init_tables(QTable QT, LightTable LT) {
 
 // genNextRay (:304-375): Russian roulette, then the table's direction (with its pdf) or,
 // for delta BSDFs and hits without a table product, a BSDF sample.
-__global__ void k_rl_next(DevScene S, int depth, const int32_t* dim_in, int64_t n, Paths P, Queues Q, RLTask T,
+// 4 blocks per SM (64 registers, a few bytes spilled) rather than 3 at 76
+__global__ void __launch_bounds__(kThreads, 4) k_rl_next(DevScene S, int depth, const int32_t* dim_in, int64_t n, Paths P, Queues Q, RLTask T,
                           RLPath R) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int prim = j < n ? Q.hit_prim[j] : -1;
