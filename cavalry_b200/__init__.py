@@ -112,6 +112,7 @@ def lib() -> ctypes.CDLL:
         "cav_pbrt_load_triangles": ([ctypes.c_char_p, P, ctypes.c_int64, P, P, ctypes.c_int64, P, P, P,
                                      ctypes.c_int], ctypes.c_int),
         "cav_trace_autotune_flags": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, U32, P, P], ctypes.c_int),
+        "cav_load_texture_png": ([ctypes.c_char_p, P, ctypes.c_int64, P, P, P, ctypes.c_int], ctypes.c_int),
         "cav_server_create": ([P, P, ctypes.POINTER(P)], ctypes.c_int),
         "cav_server_destroy": ([P], ctypes.c_int),
         "cav_server_submit_render": ([P, P, P, P, P, P], ctypes.c_int),
@@ -259,6 +260,24 @@ def parse_pbrt(path: str, spp: int = -1, integrator: str | None = None) -> tuple
     if st != 0:
         raise CavError(st, "cav_pbrt_parse_info: " + err.value.decode(errors="replace"))
     return info, c2w.reshape(4, 4).T
+
+
+def load_texture_png(path: str) -> np.ndarray:
+    """Host-only: a texture image as scene loading decodes it, [H, W, 4] uint8 with rows
+    bottom-up and the colour channels through the inverse sRGB curve (no GPU)."""
+    w, h = ctypes.c_int(), ctypes.c_int()
+    err = ctypes.create_string_buffer(512)
+    L = lib()
+    st = L.cav_load_texture_png(path.encode(), None, 0, ctypes.byref(w), ctypes.byref(h), ctypes.addressof(err),
+                                len(err))
+    if st != 0:
+        raise CavError(st, "cav_load_texture_png: " + err.value.decode(errors="replace"))
+    out = np.zeros((h.value, w.value, 4), np.uint8)
+    st = L.cav_load_texture_png(path.encode(), out.ctypes.data, out.nbytes, ctypes.byref(w), ctypes.byref(h),
+                                ctypes.addressof(err), len(err))
+    if st != 0:
+        raise CavError(st, "cav_load_texture_png: " + err.value.decode(errors="replace"))
+    return out
 
 
 def load_pbrt_triangles(path: str) -> tuple[np.ndarray, np.ndarray, np.ndarray]:

@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/cavalry.h"
 #include "pbrt.h"
 
 namespace cavpbrt {
@@ -144,3 +145,30 @@ TextureImage load_texture_image(const std::string& path) {
 }
 
 }  // namespace cavpbrt
+
+// Host-only: the texture loader's output for one image (no GPU).
+extern "C" cav_status cav_load_texture_png(const char* path, uint8_t* rgba, int64_t capacity_bytes, int* width,
+                                           int* height, char* err, int err_len) {
+    if (!path || !width || !height) return CAV_ERR_INVALID_ARGUMENT;
+    try {
+        const cavpbrt::TextureImage t = cavpbrt::load_texture_image(path);
+        *width = t.width;
+        *height = t.height;
+        if (!rgba) return CAV_OK;  // size query
+        if (capacity_bytes < (int64_t)t.rgba.size()) {
+            if (err && err_len > 0) {
+                std::strncpy(err, "cav_load_texture_png: output buffer too small", (size_t)err_len - 1);
+                err[err_len - 1] = 0;
+            }
+            return CAV_ERR_INVALID_ARGUMENT;
+        }
+        std::memcpy(rgba, t.rgba.data(), t.rgba.size());
+    } catch (const std::exception& e) {
+        if (err && err_len > 0) {
+            std::strncpy(err, e.what(), (size_t)err_len - 1);
+            err[err_len - 1] = 0;
+        }
+        return CAV_ERR_INVALID_ARGUMENT;
+    }
+    return CAV_OK;
+}

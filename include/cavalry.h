@@ -237,6 +237,13 @@ cav_status cav_pbrt_parse_info(const char* path, int spp_override, const char* i
  * .pbrt), sphere and disk shapes as the reference tessellates them.  Call with NULL arrays to
  * get the counts; arrays smaller than the counts give CAV_ERR_INVALID_ARGUMENT.  Parse errors
  * as cav_pbrt_parse_info. */
+/* Host-only: decode a texture image exactly as scene loading does (Core/Texture.cu:27-83):
+ * 8-bit RGBA, rows bottom-up (flipped on load), colour channels of a .png through the inverse
+ * sRGB curve and truncated to 8 bits, alpha unchanged.  PNG only (greyscale, grey + alpha,
+ * RGB, RGBA, palette; 8 or 16 bits; not interlaced).  With rgba null only width and height
+ * are returned; otherwise capacity_bytes must hold 4 * width * height bytes. */
+cav_status cav_load_texture_png(const char* path, uint8_t* rgba, int64_t capacity_bytes, int* width, int* height,
+                                char* err, int err_len);
 cav_status cav_pbrt_load_triangles(const char* path, float* positions, int64_t max_vertices, int32_t* indices,
                                    int32_t* mesh_ids, int64_t max_triangles, int64_t* num_vertices,
                                    int64_t* num_triangles, char* err, int err_len);

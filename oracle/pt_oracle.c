@@ -578,6 +578,11 @@ static float inverse_gamma(float value) {
 }
 static uint8_t load_gamma(uint8_t c) { return (uint8_t)(255.f * inverse_gamma(c / 255.f)); }
 
+/* The 256-entry table of load_gamma (Core/Texture.cu:19, :64-71: .png channels at load time). */
+void orc_load_gamma_table(uint8_t* out) {
+    for (int c = 0; c < 256; ++c) out[c] = load_gamma((uint8_t)c);
+}
+
 /* tex2D of a uchar4 texture read as normalized floats with bilinear filtering and wrapped
  * normalized coordinates, restated from the CUDA programming guide's description of
  * texture fetching: x = frac(u) * W - 0.5, texels i = floor(x) and i + 1 (wrapped), weight

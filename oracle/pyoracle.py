@@ -257,12 +257,21 @@ def _pt_lib():
         L.orc_roughness_to_alpha.restype = F
         L.orc_halton_tables.argtypes = [P, P, P]
         L.orc_halton_tables.restype = I64
+        L.orc_load_gamma_table.argtypes = [P]
+        L.orc_load_gamma_table.restype = None
         L._pt_ready = True
     return L
 
 
 def roughness_to_alpha(r: float) -> float:
     return float(_pt_lib().orc_roughness_to_alpha(float(r)))
+
+
+def load_gamma_table() -> np.ndarray:
+    """uint8 [256]: a .png colour byte after the load-time inverse sRGB curve."""
+    out = np.zeros(256, np.uint8)
+    _pt_lib().orc_load_gamma_table(out.ctypes.data)
+    return out
 
 
 def material_record(mat, texture_index: dict | None = None) -> np.void:
