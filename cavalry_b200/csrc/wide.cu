@@ -285,6 +285,9 @@ __device__ __forceinline__ uint32_t node_hits(const CNode* __restrict__ cn, uint
 
 // kSeg: one launch over several jobs' rays (segs[k] = one tree and its outputs, ray indices
 // numbered across the launch); otherwise the pointer arguments describe the one tree.
+// 64 registers, unconstrained: the kernel is ALU-bound, and capping it for more resident
+// warps made the 5.24M-triangle render's extend stage slower (231 ms at 64 registers, 263 at
+// 48, 302 at 40).
 template <bool kAny, bool kStats, bool kSeg>
 __global__ void __launch_bounds__(256)
     k_trace_wide(const CNode* __restrict__ cn0, const TriRec* __restrict__ tris0, const cav_ray* __restrict__ rays0,
