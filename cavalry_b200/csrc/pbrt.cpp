@@ -22,6 +22,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cfloat>
+#include <charconv>
+#include <cstdlib>
+#include <cerrno>
 #include <filesystem>
 #include <fstream>
 #include <memory>
@@ -225,8 +229,41 @@ std::vector<std::string> split_spaces(const std::string& s) {
     return out;
 }
 
+// NumToken::read (SceneLoading/Lexing.cu:88-103) converts the token's characters with
+// std::stof after prefixing "0" to a leading '.'.  This gives std::stof's result and failures
+// (no conversion, or ERANGE, which the reference leaves uncaught) on those characters:
+// the characters are copied into a terminated buffer so that strtof cannot read past the
+// token (it would accept "e+5" or "x1p3" that the lexer leaves for the next token).
+float token_number(const char* p, size_t n) {
+    char small[64];
+    std::string big;
+    char* buf = small;
+    const bool dot = p[0] == '.';  // the lexer reads ".5" as "0.5"
+    const size_t len = n + (dot ? 1 : 0);
+    if (len + 1 > sizeof(small)) {
+        big.resize(len + 1);
+        buf = &big[0];
+    }
+    size_t k = 0;
+    if (dot) buf[k++] = '0';
+    std::memcpy(buf + k, p, n);
+    buf[len] = 0;
+    // std::from_chars and strtof both round correctly, so they agree on every normal result;
+    // zero, subnormal, infinite or failed conversions take strtof's path, whose ERANGE rules
+    // std::stof follows
+    float v = 0.f;
+    const std::from_chars_result r = std::from_chars(buf, buf + len, v);
+    if (r.ec == std::errc() && r.ptr != buf && std::fabs(v) >= FLT_MIN && std::fabs(v) <= FLT_MAX) return v;
+    char* end = nullptr;
+    errno = 0;
+    v = std::strtof(buf, &end);
+    if (end == buf || errno == ERANGE) throw ParseError("Lexing Error: bad number '" + std::string(buf) + "'");
+    return v;
+}
+
 std::vector<Token> lex(const std::string& input) {
     std::vector<Token> toks;
+    toks.reserve(input.size() / 10 + 16);  // a mesh number with its separator is about 10 characters
     size_t pos = 0;
     while (pos < input.size()) {
         char c = input[pos];
@@ -242,30 +279,29 @@ std::vector<Token> lex(const std::string& input) {
             toks.push_back({Tok::RBracket, "]", {}, 0.f});
             ++pos;
         } else if (is_letter(c)) {
-            std::string w;
-            while (pos < input.size() && is_letter(input[pos])) w += input[pos++];
+            const size_t start = pos;
+            while (pos < input.size() && is_letter(input[pos])) ++pos;
+            std::string w = input.substr(start, pos - start);
             if (!keywords().count(w)) throw ParseError("Unrecognized Keyword: " + w);
-            toks.push_back({Tok::Keyword, w, {}, 0.f});
+            toks.push_back({Tok::Keyword, std::move(w), {}, 0.f});
         } else if (c == '"') {
             ++pos;
-            std::string raw;
-            while (pos < input.size() && input[pos] != '"') raw += input[pos++];
+            const size_t start = pos;
+            while (pos < input.size() && input[pos] != '"') ++pos;
             if (pos == input.size()) throw ParseError("Lexing Error: Didn't find ending quotation");
+            std::string raw = input.substr(start, pos - start);
             ++pos;
-            toks.push_back({Tok::String, raw, split_spaces(raw), 0.f});
+            std::vector<std::string> words = split_spaces(raw);
+            toks.push_back({Tok::String, std::move(raw), std::move(words), 0.f});
         } else if (is_digit(c) || c == '-' || c == '.') {
-            std::string raw;
+            const size_t start = pos;
             while (pos < input.size() &&
                    (is_digit(input[pos]) || input[pos] == '-' || input[pos] == '.' || input[pos] == 'e'))
-                raw += input[pos++];
-            if (raw[0] == '.') raw = "0" + raw;
-            float v;
-            try {
-                v = std::stof(raw);
-            } catch (const std::exception&) {
-                throw ParseError("Lexing Error: bad number '" + raw + "'");
-            }
-            toks.push_back({Tok::Num, raw, {}, v});
+                ++pos;
+            const float v = token_number(input.data() + start, pos - start);
+            std::string raw = input.substr(start, pos - start);
+            if (raw[0] == '.') raw.insert(raw.begin(), '0');
+            toks.push_back({Tok::Num, std::move(raw), {}, v});
         } else {
             throw ParseError(std::string("unrecognized character ") + c);
         }

@@ -352,3 +352,36 @@ def test_textures_and_light_sources_parse_like_the_reference(tmp_path):
         parse('LightSource "infinite"\nTexture "a" "spectrum" "imagemap" "string filename" "t.jpg"\n' + tri)
     with pytest.raises(cav.CavError, match="no lights"):
         parse(tri)
+
+
+@pytest.mark.parametrize("text,value", [(".5", 0.5), ("-.5", -0.5), ("1e", 1.0), ("2.5e1", 25.0), ("1-2", 1.0),
+                                        ("0.1", float(np.float32(0.1))), ("3.4028235e38", float(np.finfo(np.float32).max)),
+                                        ("1.17549435e-38", float(np.finfo(np.float32).tiny))])
+def test_lexer_numbers_read_like_stof(tmp_path, text, value):
+    """Numbers are read as the reference's lexer reads them with std::stof (Lexing.cu:88-103): the
+    longest prefix of the token that is a number, a leading '.' read as "0.", correctly
+    rounded to float."""
+    import cavalry_b200 as cav
+
+    p = tmp_path / "n.pbrt"
+    p.write_text('LookAt 0 0 -3  0 0 0  0 1 0\nCamera "perspective" "float fov" [40]\n'
+                 'Film "image" "integer xresolution" [16] "integer yresolution" [16]\n'
+                 'Sampler "halton" "integer pixelsamples" [1]\nIntegrator "path" "integer maxdepth" [2]\nWorldBegin\n'
+                 'AttributeBegin\nAreaLightSource "diffuse" "rgb L" [1 1 1]\n'
+                 'Shape "trianglemesh" "integer indices" [0 1 2] "point P" [0 0 5 1 0 5 0 1 5]\nAttributeEnd\n'
+                 f'AttributeBegin\nScale {text} 1 1\n'
+                 'Shape "trianglemesh" "integer indices" [0 1 2] "point P" [1 0 0 0 1 0 0 0 1]\nAttributeEnd\nWorldEnd\n')
+    pos, _, _ = cav.load_pbrt_triangles(str(p))
+    assert pos[3, 0] == np.float32(value)
+
+
+@pytest.mark.parametrize("text", ["1e-40", "1e39", "-"])
+def test_lexer_rejects_numbers_stof_rejects(tmp_path, text):
+    """Out-of-range (std::stof's ERANGE: overflow, or underflow into the subnormals) and
+    non-numbers are lexing errors, as in the reference."""
+    import cavalry_b200 as cav
+
+    p = tmp_path / "n.pbrt"
+    p.write_text(f'LookAt 0 0 -3  0 0 0  0 1 0\nCamera "perspective" "float fov" [{text}]\nWorldBegin\nWorldEnd\n')
+    with pytest.raises(cav.CavError, match="bad number"):
+        cav.parse_pbrt(str(p))
