@@ -24,6 +24,7 @@
 #include <cstring>
 #include <cfloat>
 #include <charconv>
+#include <deque>
 #include <cstdlib>
 #include <cerrno>
 #include <filesystem>
@@ -198,12 +199,37 @@ namespace {
 
 enum class Tok { Keyword, String, Num, LBracket, RBracket };
 
+struct StrRec {
+    std::string text;                // keyword word / full string
+    std::vector<std::string> words;  // string split on spaces
+};
+
+// 16 bytes: a mesh's numbers are most of a large file's tokens.  Keyword and string tokens
+// point into the parser's arena (a deque, so the records never move).
 struct Token {
     Tok type;
-    std::string text;                 // keyword word / full string
-    std::vector<std::string> words;   // string split on spaces
     float num = 0.f;
+    const StrRec* s = nullptr;
+    const std::string& text() const {
+        static const std::string empty;
+        return s ? s->text : empty;
+    }
+    const std::vector<std::string>& words() const {
+        static const std::vector<std::string> none;
+        return s ? s->words : none;
+    }
 };
+
+std::string describe(const Token& t) {  // for messages
+    if (t.type == Tok::LBracket) return "[";
+    if (t.type == Tok::RBracket) return "]";
+    if (t.type == Tok::Num) {
+        char b[32];
+        const auto r = std::to_chars(b, b + sizeof(b), t.num);
+        return std::string(b, r.ptr);
+    }
+    return t.text();
+}
 
 const std::set<std::string>& keywords() {
     static const std::set<std::string> k = {
@@ -261,7 +287,7 @@ float token_number(const char* p, size_t n) {
     return v;
 }
 
-std::vector<Token> lex(const std::string& input) {
+std::vector<Token> lex(const std::string& input, std::deque<StrRec>& arena) {
     std::vector<Token> toks;
     toks.reserve(input.size() / 10 + 16);  // a mesh number with its separator is about 10 characters
     size_t pos = 0;
@@ -273,17 +299,18 @@ std::vector<Token> lex(const std::string& input) {
             while (pos < input.size() && input[pos] != '\n') ++pos;
             ++pos;
         } else if (c == '[') {
-            toks.push_back({Tok::LBracket, "[", {}, 0.f});
+            toks.push_back({Tok::LBracket, 0.f, nullptr});
             ++pos;
         } else if (c == ']') {
-            toks.push_back({Tok::RBracket, "]", {}, 0.f});
+            toks.push_back({Tok::RBracket, 0.f, nullptr});
             ++pos;
         } else if (is_letter(c)) {
             const size_t start = pos;
             while (pos < input.size() && is_letter(input[pos])) ++pos;
             std::string w = input.substr(start, pos - start);
             if (!keywords().count(w)) throw ParseError("Unrecognized Keyword: " + w);
-            toks.push_back({Tok::Keyword, std::move(w), {}, 0.f});
+            arena.push_back(StrRec{std::move(w), {}});
+            toks.push_back({Tok::Keyword, 0.f, &arena.back()});
         } else if (c == '"') {
             ++pos;
             const size_t start = pos;
@@ -292,16 +319,14 @@ std::vector<Token> lex(const std::string& input) {
             std::string raw = input.substr(start, pos - start);
             ++pos;
             std::vector<std::string> words = split_spaces(raw);
-            toks.push_back({Tok::String, std::move(raw), std::move(words), 0.f});
+            arena.push_back(StrRec{std::move(raw), std::move(words)});
+            toks.push_back({Tok::String, 0.f, &arena.back()});
         } else if (is_digit(c) || c == '-' || c == '.') {
             const size_t start = pos;
             while (pos < input.size() &&
                    (is_digit(input[pos]) || input[pos] == '-' || input[pos] == '.' || input[pos] == 'e'))
                 ++pos;
-            const float v = token_number(input.data() + start, pos - start);
-            std::string raw = input.substr(start, pos - start);
-            if (raw[0] == '.') raw.insert(raw.begin(), '0');
-            toks.push_back({Tok::Num, std::move(raw), {}, v});
+            toks.push_back({Tok::Num, token_number(input.data() + start, pos - start), nullptr});
         } else {
             throw ParseError(std::string("unrecognized character ") + c);
         }
@@ -319,13 +344,16 @@ std::string read_text(const std::filesystem::path& p) {
 
 // ------------------------------------------------------------------- parser
 struct Parser {
+    std::deque<StrRec> arena;  // keyword and string tokens' text (stable addresses)
     std::vector<Token> toks;
     size_t i = 0;
     std::filesystem::path base;
     Scene& scene;
     std::map<std::string, Material> named;
 
-    Parser(std::vector<Token> t, std::filesystem::path b, Scene& s) : toks(std::move(t)), base(std::move(b)), scene(s) {}
+    Parser(const std::string& text, std::filesystem::path b, Scene& s) : base(std::move(b)), scene(s) {
+        toks = lex(text, arena);
+    }
 
     const Token& peek(size_t k = 0) {
         if (i + k >= toks.size()) throw ParseError("unexpected end of input");
@@ -335,7 +363,7 @@ struct Parser {
         const Token& t = peek();
         if (t.type != want)
             throw ParseError(std::string("Parsing Error: ") + what + " expected at token " + std::to_string(i) + ": " +
-                             t.text);
+                             describe(t));
         ++i;
         return t;
     }
@@ -350,21 +378,21 @@ struct Parser {
     std::vector<std::string> string_list() {
         pop(Tok::LBracket, "[");
         std::vector<std::string> r;
-        while (peek().type == Tok::String) r.push_back(pop(Tok::String, "string").text);
+        while (peek().type == Tok::String) r.push_back(pop(Tok::String, "string").text());
         pop(Tok::RBracket, "]");
         return r;
     }
 
     ObjectDef object() {
         ObjectDef d;
-        d.keyword = pop(Tok::Keyword, "keyword").text;
-        d.name = pop(Tok::String, "object name").words[0];
+        d.keyword = pop(Tok::Keyword, "keyword").text();
+        d.name = pop(Tok::String, "object name").words()[0];
         while (i < toks.size() && peek().type == Tok::String) {
             const Token& key = pop(Tok::String, "parameter name");
-            std::string field = key.words.back();
+            std::string field = key.words().back();
             const Token& nx = peek();
             if (nx.type == Tok::String) {
-                d.params.strings[field] = pop(Tok::String, "string").text;
+                d.params.strings[field] = pop(Tok::String, "string").text();
             } else if (nx.type == Tok::Num) {
                 d.params.nums[field] = pop(Tok::Num, "number").num;
             } else if (nx.type == Tok::LBracket) {
@@ -388,21 +416,21 @@ struct Parser {
     bool transform(Mat4& m) {
         const Token& t = peek();
         if (t.type != Tok::Keyword) throw ParseError("Keyword expected at token " + std::to_string(i));
-        if (t.text == "Translate" || t.text == "Scale") {
-            bool tr = t.text == "Translate";
+        if (t.text() == "Translate" || t.text() == "Scale") {
+            bool tr = t.text() == "Translate";
             ++i;
             float x = pop(Tok::Num, "number").num, y = pop(Tok::Num, "number").num, z = pop(Tok::Num, "number").num;
             m = tr ? translate(m, x, y, z) : scale(m, x, y, z);
             return true;
         }
-        if (t.text == "Rotate") {
+        if (t.text() == "Rotate") {
             ++i;
             float a = pop(Tok::Num, "number").num;
             float x = pop(Tok::Num, "number").num, y = pop(Tok::Num, "number").num, z = pop(Tok::Num, "number").num;
             m = rotate(m, a, x, y, z);
             return true;
         }
-        if (t.text == "Transform") {
+        if (t.text() == "Transform") {
             ++i;
             std::vector<float> v = num_list();
             if (v.size() != 16) throw ParseError("Transform needs 16 numbers");
@@ -422,8 +450,8 @@ struct Parser {
         for (;;) {
             const Token& t = peek();
             if (t.type != Tok::Keyword) throw ParseError("Keyword expected at token " + std::to_string(i));
-            if (t.text == "WorldBegin") break;
-            if (t.text == "LookAt") {
+            if (t.text() == "WorldBegin") break;
+            if (t.text() == "LookAt") {
                 ++i;
                 float e[3], c[3], u[3];
                 for (float& v : e) v = pop(Tok::Num, "number").num;
@@ -434,16 +462,16 @@ struct Parser {
                 apply_point(xf, c, c2);
                 apply_vector3(xf, u, u2);
                 xf = mul(look_at_lh(e2, c2, u2), xf);
-            } else if (t.text == "Camera") {
+            } else if (t.text() == "Camera") {
                 camera = object();
-            } else if (t.text == "Film") {
+            } else if (t.text() == "Film") {
                 film = object();
-            } else if (t.text == "Sampler") {
+            } else if (t.text() == "Sampler") {
                 sampler = object();
             } else if (transform(xf)) {
-            } else if (t.text == "Integrator") {
+            } else if (t.text() == "Integrator") {
                 integrator = object();
-            } else if (t.text == "PixelFilter") {
+            } else if (t.text() == "PixelFilter") {
                 filter = object();
             } else {
                 skip_object();
@@ -573,7 +601,7 @@ struct Parser {
 
     void world(Mat4 xf, int current_material, bool& next_shape_light, bool top) {
         const Token& begin = pop(Tok::Keyword, "XXXBegin");
-        const std::string bw = begin.text;
+        const std::string bw = begin.text();
         if (bw.size() < 5 || bw.compare(bw.size() - 5, 5, "Begin") != 0) throw ParseError("XXXBegin expected");
         std::string name = bw.substr(0, bw.size() - 5);
         bool reverse = false;
@@ -584,7 +612,7 @@ struct Parser {
             }
             const Token& t = peek();
             if (t.type != Tok::Keyword) throw ParseError("Keyword expected at token " + std::to_string(i));
-            const std::string w = t.text;
+            const std::string w = t.text();
             if (w.size() > 3 && w.compare(w.size() - 3, 3, "End") == 0) {
                 if (w.substr(0, w.size() - 3) != name) throw ParseError("Mismatching subsection names: " + w);
                 break;
@@ -719,14 +747,14 @@ struct Parser {
                 current_material = add_material(material(d, d.name));
             } else if (w == "NamedMaterial") {
                 ++i;
-                std::string n = pop(Tok::String, "material name").text;
+                std::string n = pop(Tok::String, "material name").text();
                 auto it = named.find(n);
                 if (it == named.end()) throw ParseError("Named material not found: " + n);
                 current_material = add_material(it->second);
             } else if (w == "Include") {
                 ++i;
-                std::string file = pop(Tok::String, "file name").text;
-                std::vector<Token> inc = lex(read_text(base / file));
+                std::string file = pop(Tok::String, "file name").text();
+                std::vector<Token> inc = lex(read_text(base / file), arena);
                 toks.insert(toks.begin() + (long)i, inc.begin(), inc.end());
             } else if (w == "ReverseOrientation") {
                 ++i;
@@ -750,7 +778,7 @@ struct Parser {
 
 Scene load_string(const std::string& text, const std::string& base_dir, const Overrides& ov) {
     Scene scene;
-    Parser p(lex(text), std::filesystem::path(base_dir), scene);
+    Parser p(text, std::filesystem::path(base_dir), scene);
     p.scene_wide(ov);
     bool next_light = false;
     p.world(identity(), -1, next_light, true);
