@@ -192,6 +192,35 @@ PlyMesh read_ply(const std::string& path) {
             m.positions.resize(3 * (size_t)e.count);
             if (normals) m.normals.resize(3 * (size_t)e.count);
             if (uvs) m.uvs.resize(2 * (size_t)e.count);
+            bool all_f32 = fmt == 1;  // binary little endian with float properties only: one block
+            for (const PlyProp& p : e.props) all_f32 = all_f32 && !p.list && p.type == kF32;
+            if (all_f32) {
+                const size_t np = e.props.size(), bytes = 4 * np * (size_t)e.count;
+                if (body.pos + bytes > data.size())
+                    throw ParseError("read ply file failed, unexpected end of data in " + path);
+                const char* base = data.data() + body.pos;
+                auto col = [&](int64_t r, int k) {
+                    float v;
+                    std::memcpy(&v, base + 4 * (np * (size_t)r + (size_t)k), 4);
+                    return v;
+                };
+                for (int64_t r = 0; r < e.count; ++r) {
+                    m.positions[3 * r] = col(r, ix);
+                    m.positions[3 * r + 1] = col(r, iy);
+                    m.positions[3 * r + 2] = col(r, iz);
+                    if (normals) {
+                        m.normals[3 * r] = col(r, inx);
+                        m.normals[3 * r + 1] = col(r, iny);
+                        m.normals[3 * r + 2] = col(r, inz);
+                    }
+                    if (uvs) {
+                        m.uvs[2 * r] = col(r, iu);
+                        m.uvs[2 * r + 1] = col(r, iv);
+                    }
+                }
+                body.pos += bytes;
+                continue;
+            }
             std::vector<double> rec(e.props.size());
             for (int64_t r = 0; r < e.count; ++r) {
                 for (size_t k = 0; k < e.props.size(); ++k) {
@@ -224,6 +253,28 @@ PlyMesh read_ply(const std::string& path) {
                 if (e.props[k].list && e.props[k].name == "vertex_indices") il = (int)k;
             if (il < 0) throw ParseError("read ply file failed, face list 'vertex_indices' missing in " + path);
             m.indices.reserve(3 * (size_t)e.count);
+            const PlyProp& lp = e.props[il];
+            if (fmt == 1 && e.props.size() == 1 && lp.count_type == kU8 && (lp.type == kI32 || lp.type == kU32)) {
+                // binary little endian, the index list alone: read each face's count byte and
+                // indices straight from the buffer (the same values the generic path reads)
+                size_t pos = body.pos;
+                for (int64_t r = 0; r < e.count; ++r) {
+                    if (pos + 1 > data.size())
+                        throw ParseError("read ply file failed, unexpected end of data in " + path);
+                    const int c = (unsigned char)data[pos];
+                    if (c < 3) throw ParseError("read ply file failed, a face with fewer than 3 vertices in " + path);
+                    if (pos + 1 + 4 * (size_t)c > data.size())
+                        throw ParseError("read ply file failed, unexpected end of data in " + path);
+                    for (int q = 0; q < 3; ++q) {  // TriangleMesh::createFromPLY keeps the first three
+                        int32_t v;
+                        std::memcpy(&v, data.data() + pos + 1 + 4 * q, 4);
+                        m.indices.push_back(lp.type == kI32 ? (int)v : (int)(double)(uint32_t)v);
+                    }
+                    pos += 1 + 4 * (size_t)c;
+                }
+                body.pos = pos;
+                continue;
+            }
             for (int64_t r = 0; r < e.count; ++r) {
                 for (size_t k = 0; k < e.props.size(); ++k) {
                     const PlyProp& p = e.props[k];

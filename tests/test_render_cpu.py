@@ -251,16 +251,19 @@ def _scene_with_shape(tmp_path, shape_line, name="s.pbrt"):
     return str(p)
 
 
+@pytest.mark.parametrize("extra", [True, False])
 @pytest.mark.parametrize("fmt", ["ascii", "binary_little_endian", "binary_big_endian"])
-def test_ply_mesh_loads_like_the_inline_mesh(tmp_path, fmt):
+def test_ply_mesh_loads_like_the_inline_mesh(tmp_path, fmt, extra):
     """Core/TriangleMesh.cu:53-108: x/y/z of any PLY encoding, each face's first three indices
-    (a quad keeps one triangle), other properties and elements skipped; the CTM applies."""
+    (a quad keeps one triangle), other properties and elements skipped; the CTM applies.
+    Without the extra property and element, a little-endian file takes the block-read path
+    (float vertices only, faces holding only their index list)."""
     import cavalry_b200 as cav
 
     rng = np.random.default_rng(1)
     P = rng.uniform(-1, 1, (7, 3)).astype(np.float32)
     faces = [(0, 1, 2), (2, 3, 4, 5), (5, 6, 0)]
-    (tmp_path / "m.ply").write_bytes(_ply_text(P, faces, fmt))
+    (tmp_path / "m.ply").write_bytes(_ply_text(P, faces, fmt, extra=extra))
     a = cav.load_pbrt_triangles(_scene_with_shape(tmp_path, 'Shape "plymesh" "string filename" "m.ply"', "a.pbrt"))
     flat = " ".join("%.9g" % c for c in P.reshape(-1))
     b = cav.load_pbrt_triangles(_scene_with_shape(
