@@ -335,11 +335,13 @@ std::vector<Token> lex(const std::string& input, std::deque<StrRec>& arena) {
 }
 
 std::string read_text(const std::filesystem::path& p) {
-    std::ifstream f(p, std::ios::binary);
+    std::ifstream f(p, std::ios::binary | std::ios::ate);
     if (!f) throw ParseError("fileNotFound: " + p.string());
-    std::stringstream ss;
-    ss << f.rdbuf();
-    return ss.str();
+    const std::streamoff n = f.tellg();
+    std::string text(n > 0 ? (size_t)n : 0, '\0');
+    f.seekg(0);
+    if (n > 0 && !f.read(&text[0], n)) throw ParseError("cannot read " + p.string());
+    return text;
 }
 
 // ------------------------------------------------------------------- parser
