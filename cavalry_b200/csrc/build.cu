@@ -40,16 +40,33 @@ struct Bounds6 {
     float v[6];
 };
 
+// A triangle's three vertex indices, checked against the vertex count.  An index outside
+// [0, nv) sets kErrBadIndex and the triangle reads vertex 0 instead, so no load leaves the
+// caller's position array (the reference reads whatever the pointer gives).
+__device__ inline bool load_tri_idx(const int32_t* __restrict__ idx, int64_t t, int64_t nv, int32_t& a, int32_t& b,
+                                    int32_t& c, int* err) {
+    a = __ldg(idx + 3 * t);
+    b = __ldg(idx + 3 * t + 1);
+    c = __ldg(idx + 3 * t + 2);
+    if ((uint32_t)a < (uint64_t)nv && (uint32_t)b < (uint64_t)nv && (uint32_t)c < (uint64_t)nv) return true;
+    if (err) atomicExch(err, kErrBadIndex);
+    a = b = c = 0;
+    return false;
+}
+
 // Leaf boxes, Core/Triangle.h:242-268 (min/max of the three vertices), written as
 // 6 floats per triangle in triangle order, plus an optional scene-bounds reduction
-// (the union that Core/Scene.cu:131-135 folds on the host).
+// (the union that Core/Scene.cu:131-135 folds on the host).  A triangle with an index out
+// of range gets vertex 0's point box and stays out of the bounds reduction.
 __global__ void __launch_bounds__(kThreads) k_leaf_boxes(const float* __restrict__ pos, const int32_t* __restrict__ idx,
-                                                         int64_t n, float* __restrict__ box, int32_t* bounds_ord) {
+                                                         int64_t n, int64_t nv, float* __restrict__ box,
+                                                         int32_t* bounds_ord, int* err) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     bool valid = i < n;
     if (valid) {
-        int32_t a = __ldg(idx + 3 * i), b = __ldg(idx + 3 * i + 1), c = __ldg(idx + 3 * i + 2);
+        int32_t a, b, c;
+        valid = load_tri_idx(idx, i, nv, a, b, c, err);
         float v0[3], v1[3], v2[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -273,7 +290,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
             if ((s & ~kCountMask) == 0) {
                 if (t0 == 0) t0 = globaltimer_ns();
                 else if (globaltimer_ns() - t0 > 2000000000ull) {  // 2 s: give up, flag the error
-                    atomicExch(err, 1);
+                    atomicExch(err, kErrLookback);
                     break;
                 }
                 continue;
@@ -321,7 +338,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
                 S.keys[pos] = key[k];
                 S.vals[pos] = val[k];
             } else {
-                atomicExch(err, 3);
+                atomicExch(err, kErrSortScatter);
             }
         }
     }
@@ -335,7 +352,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
             kout[o] = k;
             vout[o] = S.vals[i];
         } else {
-            atomicExch(err, 3);
+            atomicExch(err, kErrSortScatter);
         }
     }
 }
@@ -389,7 +406,7 @@ __device__ inline void radix_node(const uint64_t* __restrict__ m, int32_t N, BNo
     int32_t split = (int32_t)((uint32_t)i + dist * (uint32_t)d) + min(0, d);
     int32_t lc = split, rc = split + 1;
     if (lc < 0 || rc > N - 1) {
-        atomicExch(err, 4);
+        atomicExch(err, kErrRadixSplit);
         return;
     }
     bool lleaf = min(i, j) == lc;
@@ -438,7 +455,7 @@ __device__ inline void refit_leaf(const float* __restrict__ box, uint32_t box_in
     int32_t curr = L->parent;
     for (;;) {
         if (curr < 0 || curr >= N - 1) {
-            atomicExch(err, 5);
+            atomicExch(err, kErrRefitLink);
             return;
         }
         uint32_t old = atomicAdd(visited + curr, 1u);
@@ -447,7 +464,7 @@ __device__ inline void refit_leaf(const float* __restrict__ box, uint32_t box_in
         BNode* nd = nodes + curr;
         int32_t l = __ldcg(&nd->left), r = __ldcg(&nd->right);
         if (l < 0 || r < 0 || l >= 2 * N - 1 || r >= 2 * N - 1) {
-            atomicExch(err, 5);
+            atomicExch(err, kErrRefitLink);
             return;
         }
         const BNode* A = nodes + l;
@@ -557,13 +574,15 @@ __global__ void __launch_bounds__(kScanThreads) k_compact_index(const BNode* __r
 }
 
 // Triangle records in sorted (Morton) order; slot_of[t] = sorted position of triangle t.
-__global__ void __launch_bounds__(kThreads) k_tri_layout(const float* __restrict__ pos, const int32_t* __restrict__ idx,
+__global__ void __launch_bounds__(kThreads) k_tri_layout(const float* __restrict__ pos, int64_t nv,
+                                                         const int32_t* __restrict__ idx,
                                                          const int32_t* __restrict__ mesh, const uint32_t* __restrict__ perm,
                                                          int64_t n, TriRec* __restrict__ tris, int32_t* __restrict__ slot_of) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t t = perm[j];
-    int32_t a = idx[3 * (size_t)t], b = idx[3 * (size_t)t + 1], c = idx[3 * (size_t)t + 2];
+    int32_t a, b, c;
+    load_tri_idx(idx, t, nv, a, b, c, nullptr);  // already flagged by the leaf-box pass
     f3 v0 = mk(pos[3 * (size_t)a], pos[3 * (size_t)a + 1], pos[3 * (size_t)a + 2]);
     f3 v1 = mk(pos[3 * (size_t)b], pos[3 * (size_t)b + 1], pos[3 * (size_t)b + 2]);
     f3 v2 = mk(pos[3 * (size_t)c], pos[3 * (size_t)c + 1], pos[3 * (size_t)c + 2]);
@@ -716,10 +735,10 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     int use_dev = bounds ? 0 : 1;
     if (bounds) {
         for (int k = 0; k < 6; ++k) hb.v[k] = bounds[k];
-        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, leafbox, nullptr);
+        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, nv, leafbox, nullptr, err);
     } else {
         k_bounds_init<<<1, 32, 0, s>>>(bounds_ord);
-        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, leafbox, bounds_ord);
+        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, nv, leafbox, bounds_ord, err);
         k_bounds_decode<<<1, 32, 0, s>>>(bounds_ord, dbounds);
     }
     k_morton<<<gb, kThreads, 0, s>>>(leafbox, n, dbounds, hb, use_dev, bvh->codes_sorted, bvh->codes_unsorted, vals_a);
@@ -757,7 +776,7 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     k_count_internal<<<nblk, kScanThreads, 0, s>>>(bvh->nodes, count, blk);
     k_scan_blocks<<<1, kScanThreads, 0, s>>>(blk, nblk);
     k_compact_index<<<nblk, kScanThreads, 0, s>>>(bvh->nodes, count, blk, compact);
-    k_tri_layout<<<gb, kThreads, 0, s>>>(positions, indices, mesh_ids, vals_a, n, bvh->tris, slot_of);
+    k_tri_layout<<<gb, kThreads, 0, s>>>(positions, nv, indices, mesh_ids, vals_a, n, bvh->tris, slot_of);
     k_tnode_layout<<<div_up(count, kThreads), kThreads, 0, s>>>(bvh->nodes, count, compact, slot_of, bvh->tnodes,
                                                                 bvh->d_root_box);
     cudaEventRecord(bvh->ev[6], s);
@@ -782,6 +801,7 @@ struct BuildSeg {
     const float* pos;
     const int32_t* idx;
     int64_t n;
+    int64_t nv;
     BNode* nodes;
     int32_t* perm;
     uint64_t* codes_sorted;
@@ -802,7 +822,7 @@ __device__ inline int find_off(const int64_t* offs, int K, int64_t g) {
 
 __global__ void __launch_bounds__(kThreads) k_leaf_boxes_batch(const BuildSeg* segs, const int64_t* leaf_offs, int K,
                                                                int64_t total, float* __restrict__ box,
-                                                               int32_t* bounds_ord) {
+                                                               int32_t* bounds_ord, int* err) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = g < total;
     int sg = -1;
@@ -812,7 +832,8 @@ __global__ void __launch_bounds__(kThreads) k_leaf_boxes_batch(const BuildSeg* s
         sg = find_off(leaf_offs, K, g);
         const BuildSeg& S = segs[sg];
         const int64_t t = g - leaf_offs[sg];
-        int32_t a = __ldg(S.idx + 3 * t), b = __ldg(S.idx + 3 * t + 1), c = __ldg(S.idx + 3 * t + 2);
+        int32_t a, b, c;
+        const bool ok = load_tri_idx(S.idx, t, S.nv, a, b, c, err);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             float v0 = __ldg(S.pos + 3 * (int64_t)a + k), v1 = __ldg(S.pos + 3 * (int64_t)b + k),
@@ -823,7 +844,7 @@ __global__ void __launch_bounds__(kThreads) k_leaf_boxes_batch(const BuildSeg* s
         float* o = box + 6 * g;
         o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
         o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
-        dev = S.use_dev != 0;
+        dev = S.use_dev != 0 && ok;
     }
     // bounds of the scenes without given bounds: a warp of one scene reduces first
     const unsigned same = __match_any_sync(0xffffffffu, valid && dev ? sg : -1);
@@ -922,13 +943,13 @@ __global__ void __launch_bounds__(kThreads) k_refit_batch(const float* __restric
 cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, const int64_t* num_vertices,
                            const int32_t* const* indices, const int32_t* const* mesh_ids, const int64_t* num_triangles,
                            const float* bounds, int rounds, cudaStream_t s, cav_bvh** out) {
-    if (K < 1 || K > 65536 || !positions || !indices || !num_triangles || !out || rounds < 0)
+    if (K < 1 || K > 65536 || !positions || !num_vertices || !indices || !num_triangles || !out || rounds < 0)
         return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build_batch: invalid argument");
     std::vector<int64_t> leaf_offs(K + 1, 0), int_offs(K + 1, 0);
     int64_t nmax = 0;
     for (int k = 0; k < K; ++k) {
         const int64_t n = num_triangles[k];
-        if (!positions[k] || !indices[k] || n < 2 || n >= (1ll << 30) || (num_vertices && num_vertices[k] < 1))
+        if (!positions[k] || !indices[k] || n < 2 || n >= (1ll << 30) || num_vertices[k] < 1)
             return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build_batch: bad scene");
         leaf_offs[k + 1] = leaf_offs[k] + n;
         int_offs[k + 1] = int_offs[k] + n - 1;
@@ -956,6 +977,7 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
         g.pos = positions[k];
         g.idx = indices[k];
         g.n = num_triangles[k];
+        g.nv = num_vertices[k];
         g.nodes = bv[k]->nodes;
         g.perm = bv[k]->perm;
         g.codes_sorted = bv[k]->codes_sorted;
@@ -1034,7 +1056,7 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     }
     const int gb = div_up(total, kThreads);
     if (!bounds) k_bounds_batch<<<div_up(6 * K, 256), 256, 0, s>>>(bounds_ord, K, 1, dbounds);
-    k_leaf_boxes_batch<<<gb, kThreads, 0, s>>>(dsegs, d_leaf, K, total, leafbox, bounds_ord);
+    k_leaf_boxes_batch<<<gb, kThreads, 0, s>>>(dsegs, d_leaf, K, total, leafbox, bounds_ord, err);
     if (!bounds) k_bounds_batch<<<div_up(6 * K, 256), 256, 0, s>>>(bounds_ord, K, 0, dbounds);
     k_morton_batch<<<gb, kThreads, 0, s>>>(leafbox, dsegs, d_leaf, K, total, dbounds, codes, codes_copy, vals_a);
     for (int k = 0; k < K; ++k) cudaEventRecord(bv[k]->ev[1], s);
@@ -1090,7 +1112,8 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
         k_count_internal<<<nblk, kScanThreads, 0, s>>>(b->nodes, count, blk);
         k_scan_blocks<<<1, kScanThreads, 0, s>>>(blk, nblk);
         k_compact_index<<<nblk, kScanThreads, 0, s>>>(b->nodes, count, blk, compact);
-        k_tri_layout<<<div_up(n, kThreads), kThreads, 0, s>>>(positions[k], indices[k], mesh_ids ? mesh_ids[k] : nullptr,
+        k_tri_layout<<<div_up(n, kThreads), kThreads, 0, s>>>(positions[k], num_vertices[k], indices[k],
+                                                             mesh_ids ? mesh_ids[k] : nullptr,
                                                              reinterpret_cast<const uint32_t*>(b->perm), n, b->tris,
                                                              slot_of);
         k_tnode_layout<<<div_up(count, kThreads), kThreads, 0, s>>>(b->nodes, count, compact, slot_of, b->tnodes,
@@ -1136,11 +1159,13 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // The host-side name g_noalloc_scratch is only a stand-in for the symbol; its device
 // address is looked up once per device (with that device current) and cached.
+// The device's SM count, read at the same time, sizes the histogram grid.
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+int g_noalloc_sms[kMaxDevices] = {};
 
-cav_status noalloc_scratch(unsigned char** out) {
+cav_status noalloc_scratch(unsigned char** out, int* num_sms) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();
@@ -1149,14 +1174,18 @@ cav_status noalloc_scratch(unsigned char** out) {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_ptr[dev]) {
         void* p = nullptr;
+        int sms = 0;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr) {
+        if (e != cudaSuccess || p == nullptr ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
             cudaGetLastError();
             return CAV_ERR_CUDA;
         }
         g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+        g_noalloc_sms[dev] = sms;
     }
     *out = g_noalloc_ptr[dev];
+    *num_sms = g_noalloc_sms[dev];
     return CAV_OK;
 }
 
@@ -1170,8 +1199,10 @@ extern "C" cav_status cav_morton_sort_noalloc(const float* positions, int64_t nu
     const int64_t n = num_triangles;
     if (!positions || !indices || !sorted_codes || !sorted_prims || num_vertices < 1) return CAV_ERR_INVALID_ARGUMENT;
     if (n < 2 || n > kNoAllocMax) return CAV_ERR_INVALID_ARGUMENT;  // outside [2, CAV_NOALLOC_MAX_TRIANGLES]
+    const int64_t nv = num_vertices;
     unsigned char* base = nullptr;
-    cav_status st = noalloc_scratch(&base);
+    int num_sms = 0;
+    cav_status st = noalloc_scratch(&base, &num_sms);
     if (st != CAV_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     float* leafbox = reinterpret_cast<float*>(base + kOffBox);
@@ -1199,15 +1230,15 @@ extern "C" cav_status cav_morton_sort_noalloc(const float* positions, int64_t nu
     int32_t* bounds_ord = reinterpret_cast<int32_t*>(counters + 8);
     if (scene_bounds) {
         for (int k = 0; k < 6; ++k) hb.v[k] = scene_bounds[k];
-        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, leafbox, nullptr);
+        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, nv, leafbox, nullptr, err);
     } else {
         k_bounds_init<<<1, 32, 0, s>>>(bounds_ord);
-        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, leafbox, bounds_ord);
+        k_leaf_boxes<<<gb, kThreads, 0, s>>>(positions, indices, n, nv, leafbox, bounds_ord, err);
         k_bounds_decode<<<1, 32, 0, s>>>(bounds_ord, dbounds);
     }
     // keys_b receives the unsorted copy; the first sort pass overwrites it
     k_morton<<<gb, kThreads, 0, s>>>(leafbox, n, dbounds, hb, use_dev, keys_a, keys_b, vals_a);
-    k_sort_hist<<<gb < 148 * 8 ? gb : 148 * 8, kSortThreads, 0, s>>>(keys_a, n, hist);
+    k_sort_hist<<<std::min(gb, num_sms * 8), kSortThreads, 0, s>>>(keys_a, n, hist);
     if (cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem)) !=
         cudaSuccess) {
         cudaGetLastError();
@@ -1232,6 +1263,9 @@ extern "C" cav_status cav_morton_sort_noalloc(const float* positions, int64_t nu
         cudaGetLastError();
         return CAV_ERR_CUDA;
     }
-    return herr ? CAV_ERR_TIMEOUT : CAV_OK;
+    if (herr == 0) return CAV_OK;
+    if (herr == kErrLookback) return CAV_ERR_TIMEOUT;
+    if (herr == kErrBadIndex) return CAV_ERR_INVALID_ARGUMENT;
+    return CAV_ERR_CUDA;  // a sort invariant broke (kErrSortScatter)
 }
 

@@ -258,7 +258,10 @@ cav_status cav_sync_check(cav_ctx* ctx, void* stream) {
     CAV_CUDA(ctx, cudaStreamSynchronize((cudaStream_t)stream));
     CAV_CUDA(ctx, cudaMemcpy(flags, ctx->d_error, sizeof(flags), cudaMemcpyDeviceToHost));
     CAV_CUDA(ctx, cudaMemset(ctx->d_error, 0, sizeof(flags)));
-    if (flags[0]) return set_error(ctx, CAV_ERR_TIMEOUT, "radix sort look-back wait gave up");
+    if (flags[0] == kErrLookback) return set_error(ctx, CAV_ERR_TIMEOUT, "radix sort look-back wait gave up");
+    if (flags[0] == kErrBadIndex)
+        return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build: a vertex index is outside [0, num_vertices)");
+    if (flags[0]) return set_error(ctx, CAV_ERR_CUDA, "BVH build: a sort or radix-tree invariant broke");
     if (flags[1]) return set_error(ctx, CAV_ERR_CUDA, "treelet reconstruction found an inconsistent partition");
     if (flags[2] || flags[3]) return set_error(ctx, CAV_ERR_STACK_OVERFLOW, "traversal stack overflow");
     return CAV_OK;

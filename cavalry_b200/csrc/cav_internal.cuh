@@ -43,6 +43,14 @@ __device__ inline float leaf_cost(float area, int n) { return area * 1.0 * n; }
 __device__ inline float internal_cost(float area, float l, float r) { return area * 1.2 + l + r; }
 __device__ inline float internal_cost(float area, float c) { return area * 1.2 + c; }
 
+// Build error codes, written to the context's first error word by a build and mapped to a
+// cav_status by cav_sync_check.
+constexpr int kErrLookback = 1;    // sort look-back wait gave up
+constexpr int kErrSortScatter = 3; // a sort scatter position broke an invariant
+constexpr int kErrRadixSplit = 4;  // a radix-tree split fell outside its range
+constexpr int kErrBadIndex = 5;    // a triangle's vertex index is outside [0, num_vertices)
+constexpr int kErrRefitLink = 6;   // the refit met a parent or child link outside the tree
+
 // ------------------------------------------------------------ node records
 // Build/restructure node (64 bytes).  Internal nodes at [0, N-2] after the build,
 // leaf j (sorted position) at N-1+j; treelet rounds permute roles among ids.

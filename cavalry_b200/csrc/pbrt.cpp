@@ -335,10 +335,19 @@ std::vector<Token> lex(const std::string& input, std::deque<StrRec>& arena) {
 }
 
 std::string read_text(const std::filesystem::path& p) {
-    std::ifstream f(p, std::ios::binary | std::ios::ate);
+    std::ifstream f(p, std::ios::binary);
     if (!f) throw ParseError("fileNotFound: " + p.string());
-    const std::streamoff n = f.tellg();
-    std::string text(n > 0 ? (size_t)n : 0, '\0');
+    f.seekg(0, std::ios::end);
+    const std::streamoff n = f ? (std::streamoff)f.tellg() : (std::streamoff)-1;
+    if (n < 0) {
+        // not seekable (a FIFO, /dev/stdin, process substitution): read the stream to its end
+        f.clear();
+        std::ostringstream all;
+        all << f.rdbuf();
+        if (f.bad()) throw ParseError("cannot read " + p.string());
+        return all.str();
+    }
+    std::string text((size_t)n, '\0');
     f.seekg(0);
     if (n > 0 && !f.read(&text[0], n)) throw ParseError("cannot read " + p.string());
     return text;

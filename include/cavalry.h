@@ -66,7 +66,10 @@ cav_status cav_sync_check(cav_ctx* ctx, void* stream);
  * rounds    : treelet restructuring rounds (>= 0; the reference's
  *             --bvh-opt-rounds, Core/Scene.cu:141-146 picks 3 or 10 when it is -1).
  * The call is stream-ordered; the returned handle may be used on `stream` at once.
- * num_triangles must be in [2, 2^30).
+ * num_triangles must be in [2, 2^30).  Every vertex index must lie in [0, num_vertices):
+ * the kernels check each one, read vertex 0 in place of an index out of range (no load
+ * leaves `positions`) and flag it, and the next cav_sync_check returns
+ * CAV_ERR_INVALID_ARGUMENT; the tree built from such input is not meaningful.
  */
 cav_status cav_bvh_build(cav_ctx* ctx, const float* positions, int64_t num_vertices, const int32_t* indices,
                          const int32_t* mesh_ids, int64_t num_triangles, const float* scene_bounds, int rounds,
@@ -178,13 +181,16 @@ cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_
  * Writes the sorted 63-bit codes to `sorted_codes` and the triangle of each sorted
  * position to `sorted_prims` (device buffers of num_triangles entries, the values
  * cav_bvh_export_stages reports).  positions / indices / scene_bounds as for
- * cav_bvh_build; runs on the current CUDA device and synchronises `stream`.
- * Scratch is a static device array sized for CAV_NOALLOC_MAX_TRIANGLES triangles,
- * held by every GPU that loads this library until the process exits; sizes outside
- * [2, CAV_NOALLOC_MAX_TRIANGLES] return CAV_ERR_INVALID_ARGUMENT.  The first call on a
- * device looks up the array's device address; make that call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (on different
- * streams or threads) race and must be serialised by the caller.
+ * cav_bvh_build; runs on the current CUDA device and synchronises `stream` before it
+ * returns.  Scratch is a static device array sized for CAV_NOALLOC_MAX_TRIANGLES
+ * triangles, held by every GPU that loads this library until the process exits; sizes
+ * outside [2, CAV_NOALLOC_MAX_TRIANGLES] return CAV_ERR_INVALID_ARGUMENT.  The first call
+ * on a device looks up the array's device address and the device's SM count; make that
+ * call before any stream capture.  All calls share the array: calls that overlap on the
+ * GPU (on different streams or threads) race and must be serialised by the caller.
+ * Returns CAV_ERR_INVALID_ARGUMENT for a vertex index outside [0, num_vertices) (the
+ * outputs are then not meaningful), CAV_ERR_TIMEOUT when the sort's look-back wait gave
+ * up, and CAV_ERR_CUDA for a failed CUDA call or a broken sort invariant.
  */
 #define CAV_NOALLOC_MAX_TRIANGLES 131072
 cav_status cav_morton_sort_noalloc(const float* positions, int64_t num_vertices, const int32_t* indices,
@@ -416,8 +422,9 @@ cav_status cav_render_guided(cav_ctx* ctx, cav_scene* scene, const cav_render_op
  * stable pass on the scene index, the radix trees, the refits); treelet rounds and the
  * traversal layout then run per scene.  out[k] is identical to cav_bvh_build of scene k
  * alone.  positions[k], indices[k], mesh_ids[k] (mesh_ids may be NULL) are DEVICE arrays;
- * num_vertices (may be NULL), num_triangles: host arrays; scene_bounds: NULL (computed) or
- * num_scenes x 6 host floats.  At most 65,536 scenes and 2^32 triangles in total. */
+ * num_vertices, num_triangles: host arrays (vertex indices are checked against num_vertices
+ * as in cav_bvh_build); scene_bounds: NULL (computed) or num_scenes x 6 host floats.  At
+ * most 65,536 scenes and 2^32 triangles in total. */
 cav_status cav_bvh_build_batch(cav_ctx* ctx, int num_scenes, const float* const* positions,
                                const int64_t* num_vertices, const int32_t* const* indices,
                                const int32_t* const* mesh_ids, const int64_t* num_triangles,

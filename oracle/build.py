@@ -1,12 +1,14 @@
 """Test infrastructure: builds the C oracle and (when the reference sources exist) the
 reference harness.
 
-    python -m oracle.build
+    python -m oracle.build [REFERENCE_ROOT]
 
 * ``oracle/_build/libcavoracle.so`` from ``cav_oracle.c`` and ``pt_oracle.c`` (gcc; -ffp-contract=off so
   that only the explicit fmaf/fma calls contract, OpenMP for the timed CPU baseline).
 * ``oracle/_ref/libcavref.so`` from the reference's own BVH sources via
-  ``build_ref.sh`` (nvcc, sm_100a).  Skipped when the reference tree is absent.
+  ``build_ref.sh`` (nvcc, sm_100a).  The reference tree is given as an argument or by the
+  ``CAVALRY_REFERENCE`` environment variable; without one (or when it is absent) the step
+  is skipped and an earlier build, if any, is kept.
 """
 from __future__ import annotations
 
@@ -18,7 +20,6 @@ HERE = Path(__file__).resolve().parent
 BUILD = HERE / "_build"
 ORACLE_LIB = BUILD / "libcavoracle.so"
 REF_LIB = HERE / "_ref" / "libcavref.so"
-REFERENCE_ROOT = Path(os.environ.get("CAVALRY_REFERENCE", "/root/reference"))
 
 
 def build_oracle(force: bool = False) -> Path:
@@ -34,16 +35,19 @@ def build_oracle(force: bool = False) -> Path:
     return ORACLE_LIB
 
 
-def build_ref(force: bool = False) -> Path | None:
-    if not (REFERENCE_ROOT / "BVH" / "BVH.cu").exists():
+def build_ref(reference_root: str | os.PathLike | None = None, force: bool = False) -> Path | None:
+    root = reference_root or os.environ.get("CAVALRY_REFERENCE")
+    if not root or not (Path(root) / "BVH" / "BVH.cu").exists():
         return REF_LIB if REF_LIB.exists() else None
     deps = [HERE / "ref_harness.cu", HERE / "build_ref.sh", *sorted((HERE / "ref_shim").rglob("*.h"))]
     if not force and REF_LIB.exists() and REF_LIB.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
         return REF_LIB
-    subprocess.run(["bash", str(HERE / "build_ref.sh"), str(REFERENCE_ROOT)], check=True)
+    subprocess.run(["bash", str(HERE / "build_ref.sh"), str(root)], check=True)
     return REF_LIB
 
 
 if __name__ == "__main__":
+    import sys
+
     print(build_oracle())
-    print(build_ref())
+    print(build_ref(sys.argv[1] if len(sys.argv) > 1 else None))

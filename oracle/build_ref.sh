@@ -8,9 +8,9 @@
 # touches).  BVH/BVH.cu and BVH/Optimization.cu are compiled verbatim, with the
 # reference's numerics flags (CMakeLists.txt:5: -use_fast_math), for sm_100a.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:?usage: oracle/build_ref.sh REFERENCE_ROOT}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 SRC="$OUT/src"

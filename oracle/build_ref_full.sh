@@ -17,12 +17,16 @@
 # sm_100a.  The renderer must always be run with --bvh-opt-rounds 0: its treelet kernel
 # faulted on the B200 (see oracle/ref_harness.cu).
 #
-# Usage: oracle/build_ref_full.sh [REFERENCE_ROOT]
+# Usage: CAV_REF_WORK=SCRATCH_DIR oracle/build_ref_full.sh REFERENCE_ROOT
+# SCRATCH_DIR receives the patched copy and the objects; it must lie outside this repository.
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:?usage: CAV_REF_WORK=SCRATCH_DIR oracle/build_ref_full.sh REFERENCE_ROOT}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
-WORK="${CAV_REF_WORK:-/tmp/cav_ref_full}"
+WORK="${CAV_REF_WORK:?set CAV_REF_WORK to a scratch directory outside the repository}"
+case "$(cd "$(dirname "$WORK")" && pwd)/" in
+    "$(cd "$HERE/.." && pwd)/"*) echo "build_ref_full: CAV_REF_WORK must lie outside the repository" >&2; exit 2 ;;
+esac
 if [ ! -f "$REF/main.cu" ]; then
     echo "build_ref_full: reference not found at $REF; skipping" >&2
     exit 0

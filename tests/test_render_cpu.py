@@ -133,6 +133,29 @@ def test_parser_overrides(tmp_path):
     assert info.spp == 8 and info.integrator == 0 and info.triangles == 2
 
 
+def test_parser_reads_a_stream_that_cannot_seek(tmp_path):
+    """A .pbrt given as a FIFO (tellg fails) parses like the same text in a regular file."""
+    import os
+    import threading
+
+    import cavalry_b200 as cav
+
+    text = HEADER + 'WorldBegin\nAreaLightSource "diffuse" "rgb L" [1 1 1]\n' + QUAD + "WorldEnd\n"
+    fifo = tmp_path / "scene.fifo"
+    os.mkfifo(fifo)
+
+    def feed():
+        with open(fifo, "w") as f:
+            f.write(text)
+
+    th = threading.Thread(target=feed)
+    th.start()
+    info, _ = cav.parse_pbrt(str(fifo))
+    th.join(timeout=10)
+    want, _ = cav.parse_pbrt(write(tmp_path, "same.pbrt", text))
+    assert (info.spp, info.triangles, info.lights) == (want.spp, want.triangles, want.lights) == (8, 2, 1)
+
+
 def test_parser_rejects_scene_without_lights(tmp_path):
     """The reference's light pick randInt(0) yields index -1 (HaltonSampler.h:41-47); the
     loader refuses such a scene instead."""

@@ -82,3 +82,29 @@ def test_noalloc_host_bounds_and_size_limit():
     pos_b, idx_b = scenes.soup(big, seed=64)
     st, _, _ = _noalloc(f, torch.from_numpy(pos_b).cuda(), torch.from_numpy(idx_b).cuda(), big)
     assert st == 1  # CAV_ERR_INVALID_ARGUMENT: above the static scratch's maximum
+
+
+def test_noalloc_rejects_an_out_of_range_vertex_index():
+    """A vertex index outside [0, num_vertices) is reported as CAV_ERR_INVALID_ARGUMENT (the
+    kernel reads no position outside the array); the next call on valid input is exact."""
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    f = _bind()
+    pos, idx = scenes.soup(2000, seed=65)
+    bad = idx.copy()
+    bad[100, 0] = pos.shape[0]
+    d_pos = torch.from_numpy(pos).cuda()
+    st, _, _ = _noalloc(f, d_pos, torch.from_numpy(bad).cuda(), 2000)
+    assert st == 1
+    d_idx = torch.from_numpy(idx).cuda()
+    st, codes, prims = _noalloc(f, d_pos, d_idx, 2000)
+    assert st == 0
+    ctx = cav.Context(0)
+    bvh = ctx.build(d_pos, d_idx, rounds=0)
+    _, want_codes, want_prims = bvh.export_stages()
+    assert np.array_equal(codes, want_codes) and np.array_equal(prims, want_prims)
+    bvh.free()
+    ctx.close()
