@@ -52,6 +52,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--launch-shape", default=None,
+                   help="soup workload: BLOCK,CHUNK for the exact traversal instead of the autotuner's pick")
+    p.add_argument("--no-reference-cuda", action="store_true",
+                   help="soup workload: skip the reference CUDA timings and the config-1 block")
     p.add_argument("--workload", default="soup", choices=["soup", "render", "serve", "guided", "mlp", "capture"],
                    help="soup: BVH + 4M closest-hit rays (default); render: the 5.24M-triangle path-traced scene; "
                         "serve: a Poisson stream of render and ray-query jobs, merged server vs sequential loop")
@@ -125,13 +129,10 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """DRAM bytes per launch of the closest-hit kernel from the committed ncu summary, or None."""
+def committed_profile():
+    """The committed ncu summary of the closest-hit kernel on this workload ({} if absent)."""
     p = ROOT / "profiles" / "trace_closest_soup1m.json"
-    if p.exists():
-        d = json.loads(p.read_text())
-        return d.get("dram_bytes_per_launch")
-    return None
+    return json.loads(p.read_text()) if p.exists() else {}
 
 
 # ------------------------------------------------------------------------- ours
@@ -187,7 +188,12 @@ def run_ours(args):
     uv = torch.empty((N_RAYS, 2), dtype=torch.float32, device=dev)
     out = (prim, tt, uv)
     # launch shape picked by the project's autotuner on a separate 1M-ray sample
-    tuned = bvh.autotune(torch.from_numpy(scenes.closest_rays(1 << 20, seed=90 + rank)).to(dev))
+    if args.launch_shape:
+        blk, chunk = (int(x) for x in args.launch_shape.split(","))
+        ctx.set_trace_config(blk, 0, chunk)
+        tuned = {"block_threads": blk, "batch": chunk, "stack": 128, "picked_by": "--launch-shape"}
+    else:
+        tuned = bvh.autotune(torch.from_numpy(scenes.closest_rays(1 << 20, seed=90 + rank)).to(dev))
     nodes_v, tris_t = bvh.trace_stats(rays)
     nodes_per_ray = nodes_v / N_RAYS
     tris_per_ray = tris_t / N_RAYS
@@ -300,11 +306,19 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     bytes_per_ray = RAY_BYTES + HIT_BYTES + NODE_BYTES * nodes_per_ray + TRI_BYTES * tris_per_ray
     achieved = bytes_per_ray * N_RAYS / (ms_per_step * 1e-3) / 1e9
-    traffic = committed_traffic()
+    prof = committed_profile()
+    traffic = prof.get("dram_bytes_per_launch")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(bvh, pos, idx, rays_np)
+    ref_cuda = cfg1 = None
+    if rank == 0 and world == 1 and not args.no_reference_cuda:
+        try:
+            ref_cuda = reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, round(value, 2), tuned)
+        except Exception as e:  # a reported baseline: note the failure, keep the bench line
+            ref_cuda = {"error": str(e)[:300]}
+        cfg1 = config1_block(ctx)
 
     result = {
         "metric": METRIC,
@@ -326,7 +340,7 @@ def run_ours(args):
             "treelet_rounds": ROUNDS,
             "trace_mode": "exact (reference order and pruning)",
             "launch_shape": {"block": tuned["block_threads"], "queue_chunk": tuned["batch"], "stack": tuned["stack"],
-                             "picked_by": "cav_trace_autotune on a separate 1M-ray sample"},
+                             "picked_by": tuned.get("picked_by", "cav_trace_autotune on a separate 1M-ray sample")},
             "l2": "flushed between timed steps (256 MiB write); rays 128 MiB > L2",
             "parallelism": f"replicas x{world}",
         },
@@ -334,13 +348,22 @@ def run_ours(args):
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * RAY_BYTES,
                 "d2h_bytes_per_step": N_RAYS * HIT_BYTES},
         "roofline": {
-            "bound": "hbm",
+            # The node-fetch stream is measured against the HBM copy peak (the algorithmic
+            # bytes of the scope table), but 83 % of it is served by L2 and DRAM carries a
+            # twentieth of the peak: the kernel is bound by the L1 data pipe's wavefronts
+            # (one per lane per 32-byte node half, ncu) and L2 latency, not by HBM.
+            "bound": "l1/l2",
             "achieved": round(achieved, 1),
             "peak": peak,
             "unit": "GB/s",
             "frac": round(achieved / peak, 4),
             "traffic": traffic,
             "peak_kind": peak_kind,
+            "dram_frac": (round(traffic / (ms_per_step * 1e-3) / 1e9 / peak, 4) if traffic else None),
+            "l1_data_pipe_wavefronts_pct": prof.get("l1_data_pipe_lsu_wavefronts_pct"),
+            "l1tex_throughput_pct": prof.get("l1tex_throughput_pct"),
+            "lts_throughput_pct": prof.get("lts_throughput_pct"),
+            "l2_hit_rate_pct": prof.get("l2_hit_rate_pct"),
             "algorithmic_bytes_per_ray": round(bytes_per_ray, 2),
             "nodes_per_ray": round(nodes_per_ray, 3),
             "tris_per_ray": round(tris_per_ray, 3),
@@ -374,6 +397,10 @@ def run_ours(args):
     }
     if cpu is not None:
         result["cpu_baseline"] = cpu
+    if ref_cuda is not None:
+        result["reference_cuda"] = ref_cuda
+    if cfg1 is not None:
+        result["config1_mini_room"] = cfg1
     if rank == 0:
         print(json.dumps(result))
     bvh.free()
@@ -409,6 +436,151 @@ def cpu_baseline(bvh, pos, idx, rays_np, target_s: float = 10.0):
     return {"value": round(m2 / dt / 1e6, 3), "unit": UNIT, "cores": po.num_threads(), "kind": "port",
             "sample": f"{m2} of the step's {len(rays_np)} closest-hit rays on the same tree, "
                       f"{dt:.1f} s wall, OpenMP"}
+
+
+# ------------------------------------------------------- reference CUDA build, config 1
+def _median(xs):
+    return float(statistics.median(xs))
+
+
+def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, closest_shape):
+    """The reference's own CUDA code on this B200 beside ours (a reported baseline, like
+    cpu_baseline): its BVH::build (BVH/BVH.cu:317-370, replayed stage by stage with CUDA events
+    by oracle/ref_harness.cu, 0 treelet rounds: its treelet kernel faults on the B200) against
+    our LBVH build of the same 1M soup; its BVH::intersect (BVH/BVH.h:23-107) on this step's
+    rays over our 3-round tree; and, on the 5.24M-triangle icosphere scene at 0 rounds (its
+    own LBVH, bit-exact topology with ours), its BVH::intersect against ours on the renderer's
+    bounce-0 and bounce-1 extend rays."""
+    import os as _os
+    import tempfile
+
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+    from oracle import pyoracle as po
+
+    if not po.ref_available():
+        return {"unavailable": "reference harness not built (oracle/_ref/libcavref.so)"}
+    out = {}
+    # (1) LBVH build of the 1M soup
+    ref_ms, ours_ms = [], []
+    for k in range(4):
+        R = po.RefScene(pos, idx, rounds=0, id_mode=0, dump=False)
+        if k > 0:
+            ref_ms.append(float(np.sum(R.stage_ms)))
+        R.free()
+        b = ctx.build(d_pos, d_idx, rounds=0)
+        torch.cuda.synchronize()
+        if k > 0:
+            ours_ms.append(float(np.sum(b.stage_times())))
+        b.free()
+    out["soup_1M_lbvh_build"] = {
+        "ref_ms": round(_median(ref_ms), 3), "ours_ms": round(_median(ours_ms), 3),
+        "ref_builds_per_s": round(1e3 / _median(ref_ms), 1), "ours_builds_per_s": round(1e3 / _median(ours_ms), 1),
+        "speedup": round(_median(ref_ms) / _median(ours_ms), 2),
+        "timing": "device stage times (CUDA events), median of 3; 0 treelet rounds"}
+    # (2) closest hit on this step's rays over the 3-round tree, ours loaded into the reference
+    R = po.RefScene(pos, idx, rounds=0, id_mode=0, dump=False)
+    R.load_nodes(bvh.export_nodes())
+    R.trace_closest(rays_np[: 1 << 20], reps=1)
+    _, _, ms = R.trace_closest(rays_np, reps=2)
+    ref_mrays = len(rays_np) / (ms * 1e-3) / 1e6
+    R.free()
+    out["soup_1M_closest_3_rounds"] = {"ref_mrays_s": round(ref_mrays, 2), "ours_mrays_s": value,
+                                       "speedup": round(value / ref_mrays, 2), "rays": len(rays_np)}
+    # (3) the 5.24M-triangle scene at 0 rounds: the north-star comparison
+    sc_np = scenes.sphere_scene(64, 6, seed=9)
+    tmp = tempfile.mkdtemp()
+    path = _os.path.join(tmp, "spheres.pbrt")
+    scenes.write_pbrt(path, sc_np, width=1920, height=1080, spp=64, max_depth=8)
+    sc = ctx.load_pbrt(path, bvh_rounds=0)
+    _os.remove(path)
+    sb = sc.bvh()
+    R = po.RefScene(sc_np["positions"], sc_np["indices"], sc_np["mesh_ids"], rounds=0, id_mode=0, dump=False)
+    ref_nodes = R.nodes()
+    ours_nodes = sb.export_nodes()
+    topo = bool(np.array_equal(ref_nodes["left"], ours_nodes["left"]) and
+                np.array_equal(ref_nodes["right"], ours_nodes["right"]) and
+                np.array_equal(ref_nodes["is_leaf"], ours_nodes["is_leaf"]))
+    leaves = ours_nodes["is_leaf"] == 1
+    topo = topo and bool(np.array_equal(ref_nodes["begin"][leaves], ours_nodes["prim_begin"][leaves]))
+    del ref_nodes, ours_nodes
+    rows = {}
+    for depth in (0, 1):
+        r = sc.capture_rays(depth, capacity=1 << 22)
+        r_np = r.cpu().numpy()
+        R.trace_closest(r_np[: 1 << 18], reps=1)
+        _, _, rms = R.trace_closest(r_np, reps=2)
+        ref_v = len(r_np) / (rms * 1e-3) / 1e6
+        mine = {}
+        for name, fl in (("exact", cav.TRACE_EXACT), ("fast", cav.TRACE_FAST)):
+            sb.autotune(r[: 1 << 20].contiguous(), flags=fl)
+            for _ in range(2):
+                sb.trace_closest(r, flags=fl)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(3):
+                sb.trace_closest(r, flags=fl)
+            b.record()
+            torch.cuda.synchronize()
+            mine[name] = 3 * len(r_np) / (a.elapsed_time(b) * 1e-3) / 1e6
+        rows[f"bounce{depth}"] = {"rays": len(r_np), "ref_mrays_s": round(ref_v, 2),
+                                  "ours_exact_mrays_s": round(mine["exact"], 2),
+                                  "ours_fast_mrays_s": round(mine["fast"], 2),
+                                  "speedup_exact": round(mine["exact"] / ref_v, 2),
+                                  "speedup_fast": round(mine["fast"] / ref_v, 2)}
+    R.free()
+    sc.free()
+    # the soup bench's own launch shape is restored for anything measured after this block
+    ctx.set_trace_config(closest_shape["block_threads"], 0, closest_shape["batch"])
+    out["spheres_5M_closest_0_rounds"] = {"triangles": int(len(sc_np["indices"])), "topology_bit_exact": topo, **rows}
+    return out
+
+
+def config1_block(ctx):
+    """Config 1: the mini room (36 triangles with the light quad), 256x256, 16 spp, depth 5,
+    path integrator, 0 treelet rounds: paths/s of whole renders (device time, median of 5);
+    and the LBVH build + 2 treelet rounds of its 34 non-light triangles alone (device stage
+    times, median of 20 builds)."""
+    import os as _os
+    import tempfile
+
+    import torch
+
+    from cavalry_b200 import scenes
+
+    room = scenes.mini_room()
+    tmp = tempfile.mkdtemp()
+    path = _os.path.join(tmp, "room.pbrt")
+    scenes.write_pbrt(path, room, width=256, height=256, spp=16, max_depth=5)
+    sc = ctx.load_pbrt(path, bvh_rounds=0)
+    ms = []
+    for k in range(6):
+        _, _, m = sc.render()
+        if k > 0:
+            ms.append(m)
+    st = sc.stats().as_dict()
+    sc.free()
+    paths = 256 * 256 * 16
+    light = {i for i, m in enumerate(room["meshes"]) if m[0].startswith("light")}
+    keep = np.array([int(m) not in light for m in room["mesh_ids"]])
+    idx34 = np.ascontiguousarray(room["indices"][keep])
+    d_pos = torch.from_numpy(np.ascontiguousarray(room["positions"])).cuda()
+    d_idx = torch.from_numpy(idx34).cuda()
+    bms = []
+    for k in range(21):
+        b = ctx.build(d_pos, d_idx, rounds=2)
+        torch.cuda.synchronize()
+        if k > 0:
+            bms.append(float(np.sum(b.stage_times())))
+        b.free()
+    return {"render": {"workload": "mini_room_256x256_16spp_depth5_path", "ms": round(_median(ms), 3),
+                       "paths_per_s": round(paths / (_median(ms) * 1e-3), 1), "closest_rays": st["closest_rays"],
+                       "shadow_rays": st["shadow_rays"], "timing": "cav_render_to_host device time, median of 5"},
+            "build_34_tris_2_rounds": {"triangles": int(len(idx34)), "ms": round(_median(bms), 4),
+                                       "builds_per_s": round(1e3 / _median(bms), 1),
+                                       "timing": "device stage times (CUDA events), median of 20"}}
 
 
 # -------------------------------------------------------------------- reference

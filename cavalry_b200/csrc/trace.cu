@@ -64,6 +64,15 @@ __device__ __forceinline__ void load_node(const TNode* __restrict__ nodes, int32
     ld_nc_v8(p + 8, nr.hi);
 }
 
+// Register cap of the single-tree traversal kernels: 48 fit the walk without spills and
+// give 42 resident warps per SM where the compiler's own choice (53) gives 36 (measured
+// +2.6 % closest-hit rays/s on the 1M soup).  The segmented and instrumented variants
+// carry more state and keep 56.  ncu on the soup shows the kernel limited by the L1 data
+// pipe's wavefronts (76 % of peak): each lane's node fetch is its own 32-byte wavefront,
+// so resident warps matter little and a register-cached stack top or batched triangle
+// tests (both tried, both slower) do not pay.
+constexpr int kTraceRegs = 48;
+
 // ---------------------------------------------------------------- kernels
 // Persistent warps with per-lane ray replacement: every lane owns one ray at a time and
 // advances it by one node or one triangle per iteration.  When at least `refill` lanes of a
@@ -75,7 +84,7 @@ __device__ __forceinline__ void load_node(const TNode* __restrict__ nodes, int32
 // output arrays.  A lane that claims global ray g finds its segment by binary search over
 // the segment starts (staged in shared memory) and switches to that segment's tree.
 template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack>
-__global__ void k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
+__global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
                           unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
     __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
     if (kSeg) {
@@ -214,7 +223,7 @@ __global__ void k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int n
 }
 
 template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack>
-__global__ void k_any(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
+__global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_any(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
                       unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
     __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
     if (kSeg) {
