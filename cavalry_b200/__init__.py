@@ -37,6 +37,7 @@ STATUS = {
     4: "device-side wait timed out",
     5: "traversal stack overflow",
     6: "not ready",
+    7: "cancelled",
 }
 
 # cav_ref_node (include/cavalry.h), the reference's BVHNode fields (BVH/BVHNode.h:8-21)
@@ -87,6 +88,9 @@ def lib() -> ctypes.CDLL:
         "cav_trace_closest_host": ([P, P, P, I64, P, P, P, U32], ctypes.c_int),
         "cav_trace_any_host": ([P, P, P, P, P, I64, P, U32], ctypes.c_int),
         "cav_set_trace_config": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "cav_ctx_set_limits": ([P, ctypes.c_double, I64], ctypes.c_int),
+        "cav_ctx_inject": ([P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "cav_server_cancel": ([P, I64], ctypes.c_int),
         "cav_trace_stats": ([P, P, P, I64, ctypes.c_int, P, P, U32, P, P], ctypes.c_int),
         "cav_scene_load_pbrt": ([P, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(P)],
                                 ctypes.c_int),
@@ -180,6 +184,14 @@ class Context:
 
     def sync_check(self, stream=None):
         self._check(lib().cav_sync_check(self.handle, _stream_ptr(stream)), "cav_sync_check")
+
+    def set_limits(self, sort_wait_s: float = 0.0, max_trace_steps: int = 0):
+        """Bounds of the device-side waits (0: defaults, 2 s and 2^22 visits per ray)."""
+        self._check(lib().cav_ctx_set_limits(self.handle, sort_wait_s, max_trace_steps), "cav_ctx_set_limits")
+
+    def inject(self, what: int, count: int = 1):
+        """Failure injection for tests (INJECT_SORT_STALL, INJECT_ALLOC_FAIL, INJECT_NONE)."""
+        self._check(lib().cav_ctx_inject(self.handle, what, count), "cav_ctx_inject")
 
     def set_trace_config(self, block_threads: int = 0, blocks_per_sm: int = 0, batch: int = 0):
         self._check(lib().cav_set_trace_config(self.handle, block_threads, blocks_per_sm, batch),
@@ -430,7 +442,7 @@ class Scene:
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("mode", ctypes.c_int), ("max_live_jobs", ctypes.c_int),
                 ("max_paths_per_job", ctypes.c_int64), ("trace_flags", ctypes.c_uint32), ("lanes", ctypes.c_int),
-                ("min_paths_per_slice", ctypes.c_int64)]
+                ("min_paths_per_slice", ctypes.c_int64), ("reject_over_budget", ctypes.c_int)]
 
 
 class JobStatus(ctypes.Structure):
@@ -450,7 +462,8 @@ class ServerStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-JOB_PENDING, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+JOB_PENDING, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
+INJECT_NONE, INJECT_SORT_STALL, INJECT_ALLOC_FAIL = 0, 1, 2
 SERVE_MERGED, SERVE_SEQUENTIAL = 0, 1
 
 
@@ -461,10 +474,10 @@ class Server:
 
     def __init__(self, ctx: "Context", hbm_budget_bytes: int = 80 << 30, mode: int = SERVE_MERGED,
                  max_live_jobs: int = 64, max_paths_per_job: int = 0, trace_flags: int = TRACE_EXACT, lanes: int = 0,
-                 min_paths_per_slice: int = 0):
+                 min_paths_per_slice: int = 0, reject_over_budget: bool = False):
         self.ctx = ctx
         cfg = ServerConfig(hbm_budget_bytes, mode, max_live_jobs, max_paths_per_job, trace_flags, lanes,
-                           min_paths_per_slice)
+                           min_paths_per_slice, int(reject_over_budget))
         h = ctypes.c_void_p()
         ctx._check(lib().cav_server_create(ctx.handle, ctypes.addressof(cfg), ctypes.byref(h)), "cav_server_create")
         self.handle = h
@@ -504,12 +517,19 @@ class Server:
         return (job.value, *out)
 
     def wait(self, job: int, timeout_s: float = -1.0) -> JobStatus:
+        """Waits for a job; returns its status (state JOB_DONE or JOB_CANCELLED), raises
+        TimeoutError when it is still running after timeout_s and CavError when it failed."""
         out = JobStatus()
         st = lib().cav_server_wait(self.handle, job, timeout_s, ctypes.addressof(out))
-        if st == 4:
+        if st == 4 and out.state not in (JOB_DONE, JOB_FAILED, JOB_CANCELLED):
             raise TimeoutError(f"job {job} not done after {timeout_s} s")
-        self.ctx._check(st, f"job {job}")
+        if st != 7:  # CAV_ERR_CANCELLED: the status says so
+            self.ctx._check(st, f"job {job}")
         return out
+
+    def cancel(self, job: int):
+        """Cancel a pending or running job (cav_server_cancel); wait() then reports JOB_CANCELLED."""
+        self.ctx._check(lib().cav_server_cancel(self.handle, job), "cav_server_cancel")
 
     def poll(self, job: int) -> JobStatus:
         out = JobStatus()

@@ -49,7 +49,7 @@ __device__ inline bool load_tri_idx(const int32_t* __restrict__ idx, int64_t t, 
     b = __ldg(idx + 3 * t + 1);
     c = __ldg(idx + 3 * t + 2);
     if ((uint32_t)a < (uint64_t)nv && (uint32_t)b < (uint64_t)nv && (uint32_t)c < (uint64_t)nv) return true;
-    if (err) atomicExch(err, kErrBadIndex);
+    if (err) atomicOr(err, kErrBadIndex);
     a = b = c = 0;
     return false;
 }
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
                                                            uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                            int64_t n, int shift, const uint32_t* __restrict__ hist,
                                                            uint32_t* status /*tiles x 256*/, uint32_t* tile_counter,
-                                                           int* err) {
+                                                           int* err, uint64_t wait_ns, int stall_first_tile) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -277,7 +277,9 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
     // publish this tile's aggregate, then look back for the exclusive prefix
     uint32_t* my_status = status + (size_t)tile * 256 + digit;
     if (tile == 0) {
-        atomicExch(my_status, kFlagInc | total);
+        // failure injection (tests): the first tile withholds its counts, so every later
+        // tile's bounded look-back wait runs out
+        if (!stall_first_tile) atomicExch(my_status, kFlagInc | total);
     } else {
         atomicExch(my_status, kFlagAgg | total);
     }
@@ -289,8 +291,8 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
             uint32_t s = *((volatile uint32_t*)(status + (size_t)p * 256 + digit));
             if ((s & ~kCountMask) == 0) {
                 if (t0 == 0) t0 = globaltimer_ns();
-                else if (globaltimer_ns() - t0 > 2000000000ull) {  // 2 s: give up, flag the error
-                    atomicExch(err, kErrLookback);
+                else if (globaltimer_ns() - t0 > wait_ns) {  // give up and flag the error
+                    atomicOr(err, kErrLookback);
                     break;
                 }
                 continue;
@@ -338,7 +340,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
                 S.keys[pos] = key[k];
                 S.vals[pos] = val[k];
             } else {
-                atomicExch(err, kErrSortScatter);
+                atomicOr(err, kErrSortScatter);
             }
         }
     }
@@ -352,7 +354,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
             kout[o] = k;
             vout[o] = S.vals[i];
         } else {
-            atomicExch(err, kErrSortScatter);
+            atomicOr(err, kErrSortScatter);
         }
     }
 }
@@ -406,7 +408,7 @@ __device__ inline void radix_node(const uint64_t* __restrict__ m, int32_t N, BNo
     int32_t split = (int32_t)((uint32_t)i + dist * (uint32_t)d) + min(0, d);
     int32_t lc = split, rc = split + 1;
     if (lc < 0 || rc > N - 1) {
-        atomicExch(err, kErrRadixSplit);
+        atomicOr(err, kErrRadixSplit);
         return;
     }
     bool lleaf = min(i, j) == lc;
@@ -455,7 +457,7 @@ __device__ inline void refit_leaf(const float* __restrict__ box, uint32_t box_in
     int32_t curr = L->parent;
     for (;;) {
         if (curr < 0 || curr >= N - 1) {
-            atomicExch(err, kErrRefitLink);
+            atomicOr(err, kErrRefitLink);
             return;
         }
         uint32_t old = atomicAdd(visited + curr, 1u);
@@ -464,7 +466,7 @@ __device__ inline void refit_leaf(const float* __restrict__ box, uint32_t box_in
         BNode* nd = nodes + curr;
         int32_t l = __ldcg(&nd->left), r = __ldcg(&nd->right);
         if (l < 0 || r < 0 || l >= 2 * N - 1 || r >= 2 * N - 1) {
-            atomicExch(err, kErrRefitLink);
+            atomicOr(err, kErrRefitLink);
             return;
         }
         const BNode* A = nodes + l;
@@ -491,6 +493,10 @@ __global__ void __launch_bounds__(kThreads) k_refit(const float* __restrict__ bo
     int32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= N) return;
     const uint32_t t = perm[j];
+    if (t >= (uint32_t)N) {  // a permutation entry out of range (after a failed sort)
+        atomicOr(err, kErrRefitLink);
+        return;
+    }
     refit_leaf(box, t, (int32_t)t, N, nodes, visited, j, err);
 }
 
@@ -581,6 +587,7 @@ __global__ void __launch_bounds__(kThreads) k_tri_layout(const float* __restrict
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t t = perm[j];
+    if (t >= (uint64_t)n) t = 0;  // a permutation entry out of range (a failed sort, flagged there)
     int32_t a, b, c;
     load_tri_idx(idx, t, nv, a, b, c, nullptr);  // already flagged by the leaf-box pass
     f3 v0 = mk(pos[3 * (size_t)a], pos[3 * (size_t)a + 1], pos[3 * (size_t)a + 2]);
@@ -608,10 +615,13 @@ __global__ void __launch_bounds__(kThreads) k_tnode_layout(const BNode* __restri
         root_box[3] = nd.hi_x; root_box[4] = nd.hi_y; root_box[5] = nd.hi_z;
     }
     if (nd.is_leaf) return;
+    if (nd.left < 0 || nd.left >= count || nd.right < 0 || nd.right >= count) return;  // a failed build
     const BNode& A = nodes[nd.left];
     const BNode& B = nodes[nd.right];
-    int32_t lref = A.is_leaf ? ~slot_of[A.prim] : compact[nd.left];
-    int32_t rref = B.is_leaf ? ~slot_of[B.prim] : compact[nd.right];
+    const int64_t n = (count + 1) / 2;
+    const bool lp = A.prim >= 0 && A.prim < n, rp = B.prim >= 0 && B.prim < n;
+    int32_t lref = A.is_leaf ? ~(lp ? slot_of[A.prim] : 0) : compact[nd.left];
+    int32_t rref = B.is_leaf ? ~(rp ? slot_of[B.prim] : 0) : compact[nd.right];
     int32_t c = compact[x];
     if (c < 0 || c >= count / 2) return;  // N-1 internal slots
     TNode t;
@@ -623,7 +633,22 @@ __global__ void __launch_bounds__(kThreads) k_tnode_layout(const BNode* __restri
 }
 
 __global__ void k_merge_error(const int* src, int* dst) {
-    if (threadIdx.x == 0 && src[0] != 0) atomicExch(dst, src[0]);
+    if (threadIdx.x == 0 && src[0] != 0) atomicOr(dst, src[0]);
+}
+
+// After a structural build error (kErrStructural): node 0 of the traversal layout points
+// both children at triangle slot 0, which becomes an all-zero record that every triangle test
+// rejects (zero determinant), so a tree whose build failed is still safe to trace and
+// reports no hits; cav_sync_check reports the error.
+__global__ void k_poison_tree(const int* err, TNode* tnodes, TriRec* tris) {
+    if (threadIdx.x != 0 || !(*err & kErrStructural)) return;
+    TNode t;
+    t.a = t.b = t.c = make_float4(0.f, 0.f, 0.f, 0.f);
+    t.d = make_int4(~0, ~0, 0, 0);
+    tnodes[0] = t;
+    TriRec r;
+    r.v0 = r.e1 = r.e2 = make_float4(0.f, 0.f, 0.f, 0.f);
+    tris[0] = r;
 }
 
 template <typename T>
@@ -649,7 +674,7 @@ cav_status alloc_bvh(cav_ctx* ctx, int64_t n, cav_bvh** out) {
     need += sizeof(TNode) * (n - 1) + 256;
     need += sizeof(TriRec) * n + 256;
     need += 64 + 256;
-    if (cudaMalloc(&bvh->arena, need) != cudaSuccess) {
+    if (dev_alloc(ctx, &bvh->arena, need, nullptr, false) != cudaSuccess) {
         cudaGetLastError();
         delete bvh;
         return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "cav_bvh_build: device allocation failed");
@@ -695,7 +720,7 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     scratch += sizeof(int32_t) * n + 256;             // slot_of
     scratch += sizeof(uint32_t) * (div_up(count, kScanTile) + 1) + 256;
     void* sbase = nullptr;
-    cudaError_t e = cudaMallocAsync(&sbase, scratch, s);
+    cudaError_t e = dev_alloc(ctx, &sbase, scratch, s, true);
     if (e != cudaSuccess) {
         cudaGetLastError();
         cudaFree(bvh->arena);
@@ -753,7 +778,8 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     uint32_t* vout = vals_b;
     for (int pass = 0; pass < 8; ++pass) {
         k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, n, 8 * pass, hist + 256 * pass,
-                                                                  status + (size_t)pass * tiles * 256, counters + pass, err);
+                                                                  status + (size_t)pass * tiles * 256, counters + pass, err,
+                                                                  ctx->sort_wait_ns, ctx->inject_sort_stall.load());
         std::swap(kin, kout);
         std::swap(vin, vout);
     }
@@ -779,6 +805,7 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     k_tri_layout<<<gb, kThreads, 0, s>>>(positions, nv, indices, mesh_ids, vals_a, n, bvh->tris, slot_of);
     k_tnode_layout<<<div_up(count, kThreads), kThreads, 0, s>>>(bvh->nodes, count, compact, slot_of, bvh->tnodes,
                                                                 bvh->d_root_box);
+    k_poison_tree<<<1, 32, 0, s>>>(err, bvh->tnodes, bvh->tris);
     cudaEventRecord(bvh->ev[6], s);
     CAV_CUDA(ctx, cudaGetLastError());
     k_merge_error<<<1, 32, 0, s>>>(err, ctx->d_error);
@@ -910,7 +937,8 @@ __global__ void k_scatter_batch(const uint64_t* codes_copy, const uint32_t* vals
     const int sg = find_off(leaf_offs, K, g);
     const BuildSeg& S = segs[sg];
     const int64_t j = g - leaf_offs[sg];
-    const uint32_t t = vals[g];
+    uint32_t t = vals[g];
+    if ((int64_t)t < leaf_offs[sg] || (int64_t)t >= leaf_offs[sg + 1]) t = (uint32_t)leaf_offs[sg];  // failed sort
     S.codes_unsorted[j] = codes_copy[g];
     S.codes_sorted[j] = codes_copy[t];
     S.perm[j] = (int32_t)((int64_t)t - leaf_offs[sg]);
@@ -934,6 +962,10 @@ __global__ void __launch_bounds__(kThreads) k_refit_batch(const float* __restric
     const int sg = find_off(leaf_offs, K, g);
     const BuildSeg& S = segs[sg];
     const uint32_t t = vals[g];
+    if ((int64_t)t < leaf_offs[sg] || (int64_t)t >= leaf_offs[sg + 1]) {  // outside its scene (a failed sort)
+        atomicOr(err, kErrRefitLink);
+        return;
+    }
     refit_leaf(box, t, (int32_t)((int64_t)t - leaf_offs[sg]), (int32_t)S.n, S.nodes, visited + int_offs[sg],
                (int32_t)(g - leaf_offs[sg]), err);
 }
@@ -1008,7 +1040,7 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     acc(sizeof(int32_t) * nmax);                    // slot_of
     acc(sizeof(uint32_t) * (div_up(cmax, kScanTile) + 1));
     void* sbase = nullptr;
-    if (cudaMallocAsync(&sbase, scratch, s) != cudaSuccess) {
+    if (dev_alloc(ctx, &sbase, scratch, s, true) != cudaSuccess) {
         cudaGetLastError();
         return fail(set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "cav_bvh_build_batch: scratch allocation failed"));
     }
@@ -1071,7 +1103,7 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
         k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, total, 8 * pass,
                                                                   hist + 256 * pass,
                                                                   status + (size_t)pass * tiles * 256, counters + pass,
-                                                                  err);
+                                                                  err, ctx->sort_wait_ns, ctx->inject_sort_stall.load());
         std::swap(kin, kout);
         std::swap(vin, vout);
     }
@@ -1082,7 +1114,8 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
         k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, total, 8 * pass,
                                                                   hist + 8 * 256 + 256 * pass,
                                                                   status + (size_t)(8 + pass) * tiles * 256,
-                                                                  counters + 8 + pass, err);
+                                                                  counters + 8 + pass, err, ctx->sort_wait_ns,
+                                                                  ctx->inject_sort_stall.load());
         std::swap(kin, kout);
         std::swap(vin, vout);
     }
@@ -1118,6 +1151,7 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
                                                              slot_of);
         k_tnode_layout<<<div_up(count, kThreads), kThreads, 0, s>>>(b->nodes, count, compact, slot_of, b->tnodes,
                                                                     b->d_root_box);
+        k_poison_tree<<<1, 32, 0, s>>>(err, b->tnodes, b->tris);
         cudaEventRecord(b->ev[6], s);
     }
     CAV_CUDA(ctx, cudaGetLastError());
@@ -1142,6 +1176,7 @@ namespace cav {
 namespace {
 
 constexpr int64_t kNoAllocMax = CAV_NOALLOC_MAX_TRIANGLES;
+constexpr uint64_t kNoAllocSortWaitNs = 2000000000ull;  // the sort's look-back gives up after 2 s
 constexpr int kNoAllocTiles = (int)((kNoAllocMax + kSortTile - 1) / kSortTile);
 constexpr size_t kAlign = 256;
 constexpr size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
@@ -1251,7 +1286,7 @@ extern "C" cav_status cav_morton_sort_noalloc(const float* positions, int64_t nu
     for (int pass = 0; pass < 8; ++pass) {
         k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, n, 8 * pass, hist + 256 * pass,
                                                                   status + (size_t)pass * tiles * 256, counters + pass,
-                                                                  err);
+                                                                  err, kNoAllocSortWaitNs, 0);
         uint64_t* tk = kin; kin = kout; kout = tk;
         uint32_t* tv = vin; vin = vout; vout = tv;
     }
@@ -1264,8 +1299,8 @@ extern "C" cav_status cav_morton_sort_noalloc(const float* positions, int64_t nu
         return CAV_ERR_CUDA;
     }
     if (herr == 0) return CAV_OK;
-    if (herr == kErrLookback) return CAV_ERR_TIMEOUT;
-    if (herr == kErrBadIndex) return CAV_ERR_INVALID_ARGUMENT;
+    if (herr & kErrLookback) return CAV_ERR_TIMEOUT;
+    if (herr & kErrBadIndex) return CAV_ERR_INVALID_ARGUMENT;
     return CAV_ERR_CUDA;  // a sort invariant broke (kErrSortScatter)
 }
 

@@ -7,12 +7,24 @@
 #include <vector>
 
 #include "cav_internal.cuh"
+#include "trace_common.cuh"
 
 namespace cav {
 
 cav_status set_error(cav_ctx* ctx, cav_status s, const std::string& msg) {
     if (ctx) ctx->last_error = msg;
     return s;
+}
+
+cudaError_t dev_alloc(cav_ctx* ctx, void** p, size_t bytes, cudaStream_t s, bool async) {
+    int left = ctx->inject_alloc_fail.load();
+    while (left > 0) {  // count down to the injected failure
+        if (ctx->inject_alloc_fail.compare_exchange_weak(left, left - 1)) {
+            if (left == 1) return cudaErrorMemoryAllocation;
+            break;
+        }
+    }
+    return async ? cudaMallocAsync(p, bytes, s) : cudaMalloc(p, bytes);
 }
 
 cav_status cuda_error(cav_ctx* ctx, cudaError_t e, const char* what) {
@@ -63,6 +75,7 @@ const char* cav_status_string(cav_status s) {
         case CAV_ERR_TIMEOUT: return "device-side wait timed out";
         case CAV_ERR_STACK_OVERFLOW: return "traversal stack overflow";
         case CAV_ERR_NOT_READY: return "not ready";
+        case CAV_ERR_CANCELLED: return "cancelled";
     }
     return "unknown status";
 }
@@ -258,13 +271,46 @@ cav_status cav_sync_check(cav_ctx* ctx, void* stream) {
     CAV_CUDA(ctx, cudaStreamSynchronize((cudaStream_t)stream));
     CAV_CUDA(ctx, cudaMemcpy(flags, ctx->d_error, sizeof(flags), cudaMemcpyDeviceToHost));
     CAV_CUDA(ctx, cudaMemset(ctx->d_error, 0, sizeof(flags)));
-    if (flags[0] == kErrLookback) return set_error(ctx, CAV_ERR_TIMEOUT, "radix sort look-back wait gave up");
-    if (flags[0] == kErrBadIndex)
+    if (flags[0] & kErrLookback)
+        return set_error(ctx, CAV_ERR_TIMEOUT, "radix sort look-back wait gave up (the tree reports no hits)");
+    if (flags[0] & kErrBadIndex)
         return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build: a vertex index is outside [0, num_vertices)");
-    if (flags[0]) return set_error(ctx, CAV_ERR_CUDA, "BVH build: a sort or radix-tree invariant broke");
+    if (flags[0])
+        return set_error(ctx, CAV_ERR_CUDA, "BVH build: a sort, radix-tree or refit invariant broke (the tree reports "
+                                            "no hits)");
     if (flags[1]) return set_error(ctx, CAV_ERR_CUDA, "treelet reconstruction found an inconsistent partition");
-    if (flags[2] || flags[3]) return set_error(ctx, CAV_ERR_STACK_OVERFLOW, "traversal stack overflow");
+    if ((flags[2] | flags[3]) & kFlagStackOverflow)
+        return set_error(ctx, CAV_ERR_STACK_OVERFLOW, "traversal stack overflow");
+    if ((flags[2] | flags[3]) & kFlagStepLimit)
+        return set_error(ctx, CAV_ERR_TIMEOUT, "traversal step limit reached (rays stopped)");
     return CAV_OK;
+}
+
+cav_status cav_ctx_set_limits(cav_ctx* ctx, double sort_wait_s, int64_t max_trace_steps) {
+    if (!ctx) return CAV_ERR_INVALID_ARGUMENT;
+    if (sort_wait_s > 60.0 || max_trace_steps > (int64_t)UINT32_MAX)
+        return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_ctx_set_limits: out of range");
+    ctx->sort_wait_ns = sort_wait_s > 0 ? (uint64_t)(sort_wait_s * 1e9) : 2000000000ull;
+    ctx->max_trace_steps = max_trace_steps > 0 ? (uint32_t)max_trace_steps : kMaxSteps;
+    return CAV_OK;
+}
+
+cav_status cav_ctx_inject(cav_ctx* ctx, int what, int count) {
+    if (!ctx || count < 0) return CAV_ERR_INVALID_ARGUMENT;
+    switch (what) {
+        case CAV_INJECT_NONE:
+            ctx->inject_sort_stall = 0;
+            ctx->inject_alloc_fail = 0;
+            return CAV_OK;
+        case CAV_INJECT_SORT_STALL:
+            ctx->inject_sort_stall = count > 0 ? 1 : 0;
+            return CAV_OK;
+        case CAV_INJECT_ALLOC_FAIL:
+            ctx->inject_alloc_fail = count;
+            return CAV_OK;
+        default:
+            return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_ctx_inject: unknown failure");
+    }
 }
 
 cav_status cav_trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int32_t* prim_id,

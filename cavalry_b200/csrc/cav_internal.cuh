@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 
 #include "../../include/cavalry.h"
@@ -43,13 +44,17 @@ __device__ inline float leaf_cost(float area, int n) { return area * 1.0 * n; }
 __device__ inline float internal_cost(float area, float l, float r) { return area * 1.2 + l + r; }
 __device__ inline float internal_cost(float area, float c) { return area * 1.2 + c; }
 
-// Build error codes, written to the context's first error word by a build and mapped to a
-// cav_status by cav_sync_check.
-constexpr int kErrLookback = 1;    // sort look-back wait gave up
-constexpr int kErrSortScatter = 3; // a sort scatter position broke an invariant
-constexpr int kErrRadixSplit = 4;  // a radix-tree split fell outside its range
-constexpr int kErrBadIndex = 5;    // a triangle's vertex index is outside [0, num_vertices)
-constexpr int kErrRefitLink = 6;   // the refit met a parent or child link outside the tree
+// Build error bits, or-ed into the context's first error word by a build and mapped to a
+// cav_status by cav_sync_check.  Every bit but kErrBadIndex means the tree's structure is not
+// to be trusted (the sort's permutation, the radix tree or the refit broke): the build's
+// later kernels then check every index they take from it, and its last kernel replaces the
+// traversal root with one that no ray hits, so a failed tree is still safe to trace.
+constexpr int kErrLookback = 1;     // sort look-back wait gave up
+constexpr int kErrSortScatter = 2;  // a sort scatter position broke an invariant
+constexpr int kErrRadixSplit = 4;   // a radix-tree split fell outside its range
+constexpr int kErrBadIndex = 8;     // a triangle's vertex index is outside [0, num_vertices)
+constexpr int kErrRefitLink = 16;   // the refit met a parent, child or leaf index outside the tree
+constexpr int kErrStructural = kErrLookback | kErrSortScatter | kErrRadixSplit | kErrRefitLink;
 
 // ------------------------------------------------------------ node records
 // Build/restructure node (64 bytes).  Internal nodes at [0, N-2] after the build,
@@ -116,6 +121,12 @@ struct cav_ctx {
     int trace_blocks_per_sm = 0;
     int trace_batch = 0;
     int trace_stack = 0;  // 64 selects the short traversal stack for trees known to be shallow
+    // bounded device-side waits (cav_ctx_set_limits)
+    uint32_t max_trace_steps = 1u << 22;     // node + triangle visits allowed one ray
+    uint64_t sort_wait_ns = 2000000000ull;  // a sort tile's look-back wait before it gives up
+    // failure injection for tests (cav_ctx_inject); lanes of a server read them concurrently
+    std::atomic<int> inject_sort_stall{0};
+    std::atomic<int> inject_alloc_fail{0};  // k > 0: the k-th next device allocation fails
     // launch configuration of the fast (compressed 8-wide) mode (0 = defaults)
     int wide_block = 0;
     int wide_batch = 0;
@@ -160,6 +171,10 @@ namespace cav {
 
 cav_status set_error(cav_ctx* ctx, cav_status s, const std::string& msg);
 cav_status cuda_error(cav_ctx* ctx, cudaError_t e, const char* what);
+// A device allocation made for a context: stream-ordered on `s` when `async`, else plain.
+// Fails with cudaErrorMemoryAllocation while the context's injected allocation failures last
+// (cav_ctx_inject), so the error paths of every caller can be tested without exhausting HBM.
+cudaError_t dev_alloc(cav_ctx* ctx, void** p, size_t bytes, cudaStream_t s, bool async);
 
 // build.cu
 cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int32_t* indices,

@@ -212,7 +212,7 @@ void build_halton_tables(std::vector<uint32_t>& primes, std::vector<uint32_t>& s
 namespace cav {
 
 static cav_status upload(cav_ctx* ctx, void** dst, const void* src, size_t bytes) {
-    CAV_CUDA(ctx, cudaMalloc(dst, bytes > 0 ? bytes : 16));
+    CAV_CUDA(ctx, dev_alloc(ctx, dst, bytes > 0 ? bytes : 16, nullptr, false));
     if (bytes) CAV_CUDA(ctx, cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
     return CAV_OK;
 }
@@ -407,7 +407,7 @@ cav_status render_path(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts,
     acc(4 * chunk); acc(4 * chunk); acc(8 * chunk);
     acc(32 * chunk); acc(4 * chunk); acc(8 * chunk); acc(4 * chunk); acc(12 * chunk); acc(chunk); acc(64);
     void* base = nullptr;
-    CAV_CUDA(ctx, cudaMallocAsync(&base, need, s));
+    CAV_CUDA(ctx, dev_alloc(ctx, &base, need, s, true));
     struct FreeAsync {  // path state is released on every exit path, stream-ordered
         void* p;
         cudaStream_t s;
@@ -553,7 +553,7 @@ cav_status render_path_graph(cav_ctx* ctx, cav_scene* sc, const cav_render_opts*
         acc(16 * nchunks); acc(16); acc(4); acc(4 * (2 * max_depth + 2)); acc(16);
     }
     void* base = nullptr;
-    CAV_CUDA(ctx, cudaMallocAsync(&base, need, s));
+    CAV_CUDA(ctx, dev_alloc(ctx, &base, need, s, true));
     struct FreeAsync {
         void* p;
         cudaStream_t s;
@@ -736,7 +736,7 @@ cav_status path_job_create(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* o
     film_size(sc, opts, J->W, J->H);
     const int64_t pixels = (int64_t)J->W * J->H;
     const size_t bytes = path_job_bytes(sc, opts);
-    if (cudaMallocAsync(&J->base, bytes, s) != cudaSuccess || cudaMallocHost(&J->h_counts, 16) != cudaSuccess) {
+    if (dev_alloc(ctx, &J->base, bytes, s, true) != cudaSuccess || cudaMallocHost(&J->h_counts, 16) != cudaSuccess) {
         cudaGetLastError();
         if (J->base) cudaFreeAsync(J->base, s);
         delete J;

@@ -17,6 +17,7 @@
 // Submissions and polls from other threads take a mutex.  Host buffers handed to a job
 // must stay valid until the job is done.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -64,6 +65,7 @@ struct Job {
     bool traced = false;
     // bookkeeping
     size_t bytes = 0;
+    std::atomic<bool> cancel{false};  // set by cav_server_cancel while the job runs
     int state = CAV_JOB_PENDING;
     cav_status status = CAV_OK;
     double t_submit = 0, t_start = 0, t_done = 0;
@@ -184,7 +186,7 @@ bool cav_server::start(Lane* l, Job* j) {
         st = cav::path_job_create(ctx, j->scene, &j->opts, slice_for(j->opts.max_paths_in_flight, renders), stream,
                                   &j->pj);
     } else {
-        if (cudaMallocAsync(&j->dbuf, j->bytes, stream) != cudaSuccess) {
+        if (cav::dev_alloc(ctx, &j->dbuf, j->bytes, stream, true) != cudaSuccess) {
             cudaGetLastError();
             st = CAV_ERR_OUT_OF_MEMORY;
         } else {
@@ -232,7 +234,7 @@ void cav_server::finish(Lane* l, Job* j, cav_status st) {
     std::lock_guard<std::mutex> lk(mu);
     used -= j->bytes;
     j->status = st;
-    j->state = st == CAV_OK ? CAV_JOB_DONE : CAV_JOB_FAILED;
+    j->state = st == CAV_OK ? CAV_JOB_DONE : st == CAV_ERR_CANCELLED ? CAV_JOB_CANCELLED : CAV_JOB_FAILED;
     j->t_done = now();
     done_cv.notify_all();
     cv.notify_all();  // memory came free: another lane may admit
@@ -244,6 +246,17 @@ void cav_server::tick(Lane* l) {
     const auto t_begin = Clock::now();
     const cudaStream_t stream = l->stream;
     std::vector<Job*>& live = l->live;
+    // cancelled jobs leave before the tick: their last work on this stream has completed
+    // (every tick ends with a stream synchronisation), so their state is freed in order
+    std::vector<Job*> cancelled;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (Job* j : live)
+            if (j->cancel.load()) cancelled.push_back(j);
+        for (Job* j : cancelled) live.erase(std::find(live.begin(), live.end(), j));
+    }
+    for (Job* j : cancelled) finish(l, j, CAV_ERR_CANCELLED);
+    if (live.empty()) return;
     cav_status err = CAV_OK;
     int64_t segs_c = 0, launches_c = 0, launches_a = 0;
     // ---- extend (closest hit): render jobs' current rays + closest-hit query jobs
@@ -437,6 +450,7 @@ cav_status cav_server_create(cav_ctx* ctx, const cav_server_config* cfg, cav_ser
         if (cfg->max_live_jobs > 0) sv->cfg.max_live_jobs = cfg->max_live_jobs;
         if (cfg->max_paths_per_job > 0) sv->cfg.max_paths_per_job = cfg->max_paths_per_job;
         sv->cfg.trace_flags = cfg->trace_flags;
+        sv->cfg.reject_over_budget = cfg->reject_over_budget;
     }
     sv->cfg.min_paths_per_slice = cfg && cfg->min_paths_per_slice > 0 ? cfg->min_paths_per_slice : (int64_t)1 << 22;
     int nl = cfg && cfg->lanes > 0 ? std::min(cfg->lanes, 8) : 1;
@@ -496,6 +510,13 @@ static cav_status enqueue(cav_server* sv, Job* j, int64_t* id) {
         delete j;
         return CAV_ERR_NOT_READY;
     }
+    if (sv->cfg.reject_over_budget && j->bytes > (size_t)sv->cfg.hbm_budget_bytes) {
+        const size_t need = j->bytes;
+        delete j;
+        return cav::set_error(sv->ctx, CAV_ERR_OUT_OF_MEMORY,
+                              "job rejected: it needs " + std::to_string(need) + " bytes of device memory, more than "
+                              "the server's whole HBM budget");
+    }
     j->id = sv->next_id++;
     j->t_submit = sv->now();
     sv->jobs[j->id] = j;
@@ -552,6 +573,26 @@ static void fill_status(const Job* j, cav_job_status* st) {
     st->bounces = j->bounces;
 }
 
+cav_status cav_server_cancel(cav_server* sv, int64_t job_id) {
+    if (!sv) return CAV_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(job_id);
+    if (it == sv->jobs.end()) return CAV_ERR_INVALID_ARGUMENT;
+    Job* j = it->second;
+    if (j->state == CAV_JOB_PENDING) {  // never admitted: it leaves the queue now
+        auto q = std::find(sv->pending.begin(), sv->pending.end(), j);
+        if (q != sv->pending.end()) sv->pending.erase(q);
+        j->state = CAV_JOB_CANCELLED;
+        j->status = CAV_ERR_CANCELLED;
+        j->t_done = sv->now();
+        sv->done_cv.notify_all();
+    } else if (j->state == CAV_JOB_RUNNING) {  // its lane frees it before its next bounce
+        j->cancel = true;
+        sv->cv.notify_all();
+    }
+    return CAV_OK;  // a finished job stays finished
+}
+
 cav_status cav_server_poll(cav_server* sv, int64_t job_id, cav_job_status* st) {
     if (!sv || !st) return CAV_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -567,7 +608,9 @@ cav_status cav_server_wait(cav_server* sv, int64_t job_id, double timeout_s, cav
     auto it = sv->jobs.find(job_id);
     if (it == sv->jobs.end()) return CAV_ERR_INVALID_ARGUMENT;
     Job* j = it->second;
-    auto pred = [&] { return j->state == CAV_JOB_DONE || j->state == CAV_JOB_FAILED; };
+    auto pred = [&] {
+        return j->state == CAV_JOB_DONE || j->state == CAV_JOB_FAILED || j->state == CAV_JOB_CANCELLED;
+    };
     if (timeout_s < 0) sv->done_cv.wait(lk, pred);
     else if (!sv->done_cv.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) return CAV_ERR_TIMEOUT;
     if (st) fill_status(j, st);

@@ -85,7 +85,8 @@ constexpr int kTraceRegs = 48;
 // the segment starts (staged in shared memory) and switches to that segment's tree.
 template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack>
 __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
-                          unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
+                          unsigned long long* counter, int refill, uint32_t max_steps, int* flag,
+                          unsigned long long* stats) {
     __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
     if (kSeg) {
         for (int i = threadIdx.x; i < nseg; i += blockDim.x) sbeg[i] = segs[i].begin;
@@ -152,7 +153,7 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg
             }
         }
         if (ray < 0) continue;
-        bool pop = false;
+        bool pop = false, overflow = false;
         if (ref >= 0) {
             if (kStats) ++st.nodes;
             NodeRegs nr;
@@ -164,7 +165,7 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg
             bool okr = mr >= 0 && mr < best && !(mr > tmax);
             if (okl && okr) {
                 if (top + 1 >= kStackN) {
-                    steps = kMaxSteps;  // overflow: finish below with the flag
+                    overflow = true;  // finish below with the flag
                 } else if (ml > mr) {  // the reference pushes the farther child, pops the nearer
                     stack[++top] = dd.x;
                     if (kCullPop) sdist[top] = ml;
@@ -199,8 +200,8 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg
             pop = true;
         }
         bool finished = false;
-        if (++steps >= kMaxSteps) {
-            atomicOr(flag, 1);
+        if (overflow || ++steps >= max_steps) {
+            atomicOr(flag, overflow ? kFlagStackOverflow : kFlagStepLimit);
             hit = false;
             bid = -2;
             finished = true;
@@ -224,7 +225,8 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg
 
 template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack>
 __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_any(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
-                      unsigned long long* counter, int refill, int* flag, unsigned long long* stats) {
+                      unsigned long long* counter, int refill, uint32_t max_steps, int* flag,
+                      unsigned long long* stats) {
     __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
     if (kSeg) {
         for (int i = threadIdx.x; i < nseg; i += blockDim.x) sbeg[i] = segs[i].begin;
@@ -302,6 +304,7 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_any(TraceSeg one
             if (okl && okr) {
                 if (top + 1 >= kStackN) {
                     result = 2;
+                    atomicOr(flag, kFlagStackOverflow);
                 } else if (ml > mr) {
                     stack[++top] = dd.x;
                     ref = dd.y;
@@ -329,13 +332,15 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_any(TraceSeg one
             }
             pop = true;
         }
-        if (result < 0 && ++steps >= kMaxSteps) result = 2;
+        if (result < 0 && ++steps >= max_steps) {
+            result = 2;
+            atomicOr(flag, kFlagStepLimit);
+        }
         if (result < 0 && pop) {
             if (top < 0) result = 0;
             else ref = stack[top--];
         }
         if (result >= 0) {
-            if (result == 2) atomicOr(flag, 1);
             (kSeg ? segs[seg] : one).occ[ray] = (uint8_t)result;
             ray = -1;
         }
@@ -361,18 +366,19 @@ cav_status launch_closest(cav_ctx* ctx, const TraceSeg& one, const TraceSeg* seg
                           cudaStream_t s, unsigned long long* counter, unsigned long long* stats, bool short_stack = false) {
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
     const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
+    const uint32_t ms = ctx->max_trace_steps;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     if (!kStats && !kSeg && short_stack && !(flags & CAV_TRACE_CULL_ON_POP)) {
         int grid = grid_for(ctx, k_closest<false, false, false, kShortStack>, block);
-        k_closest<false, false, false, kShortStack><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch,
+        k_closest<false, false, false, kShortStack><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms,
                                                                           ctx->d_error + 2, stats);
     } else if (flags & CAV_TRACE_CULL_ON_POP) {
         int grid = grid_for(ctx, k_closest<true, kStats, kSeg>, block);
-        k_closest<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 2,
+        k_closest<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms, ctx->d_error + 2,
                                                              stats);
     } else {
         int grid = grid_for(ctx, k_closest<false, kStats, kSeg>, block);
-        k_closest<false, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 2,
+        k_closest<false, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms, ctx->d_error + 2,
                                                               stats);
     }
     CAV_CUDA(ctx, cudaGetLastError());
@@ -384,17 +390,18 @@ cav_status launch_any(cav_ctx* ctx, const TraceSeg& one, const TraceSeg* segs, i
                       cudaStream_t s, unsigned long long* counter, unsigned long long* stats, bool short_stack = false) {
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
     const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
+    const uint32_t ms = ctx->max_trace_steps;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     if (!kStats && !kSeg && short_stack && !(flags & CAV_TRACE_CULL_ON_POP)) {
         int grid = grid_for(ctx, k_any<false, false, false, kShortStack>, block);
-        k_any<false, false, false, kShortStack><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch,
+        k_any<false, false, false, kShortStack><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms,
                                                                       ctx->d_error + 3, stats);
     } else if (flags & CAV_TRACE_CULL_ON_POP) {
         int grid = grid_for(ctx, k_any<true, kStats, kSeg>, block);
-        k_any<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 3, stats);
+        k_any<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms, ctx->d_error + 3, stats);
     } else {
         int grid = grid_for(ctx, k_any<false, kStats, kSeg>, block);
-        k_any<false, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ctx->d_error + 3, stats);
+        k_any<false, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms, ctx->d_error + 3, stats);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;

@@ -7,7 +7,10 @@
 
 namespace cav {
 
-constexpr uint32_t kMaxSteps = 1u << 22;  // node+triangle visits per ray before the ray is flagged
+constexpr uint32_t kMaxSteps = 1u << 22;  // default node+triangle visits per ray before the ray is stopped
+// Bits of a traversal kind's error word (cav_sync_check maps them to a cav_status).
+constexpr int kFlagStackOverflow = 1;  // a push found the traversal stack full
+constexpr int kFlagStepLimit = 2;      // a ray reached the context's step limit
 constexpr int kDefaultRefill = 4;         // idle lanes that trigger a warp's next claim
 constexpr unsigned kFull = 0xffffffffu;
 

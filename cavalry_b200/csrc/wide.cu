@@ -293,7 +293,8 @@ __global__ void __launch_bounds__(256)
     k_trace_wide(const CNode* __restrict__ cn0, const TriRec* __restrict__ tris0, const cav_ray* __restrict__ rays0,
                  int64_t n, const uint32_t* n_dev, int32_t* prim0, float* tout0, float* uv0,
                  const float* __restrict__ limit0, const int32_t* __restrict__ excl0, uint8_t* occ0,
-                 unsigned long long* counter, int refill, int* flag, unsigned long long* stats,
+                 unsigned long long* counter, int refill, uint32_t max_steps, int* flag,
+                 unsigned long long* stats,
                  const TraceSeg* __restrict__ segs, int nseg) {
     __shared__ int64_t sbeg[kSeg ? kMaxSeg : 1];
     if (kSeg) {
@@ -378,7 +379,7 @@ __global__ void __launch_bounds__(256)
         }
         if (ray < 0) continue;
         int result = -1;  // any hit: 0 clear, 1 occluded
-        bool finished = false;
+        bool finished = false, overflow = false;
         // node phase: a lane without pending triangles takes its next internal child
         if (tgrp.y == 0u) {
             if ((grp.y & 0xFF000000u) == 0u) {
@@ -395,7 +396,7 @@ __global__ void __launch_bounds__(256)
                 const uint32_t slot = (bit - 24u) ^ (R.octinv4 & 7u);
                 const uint32_t idx = grp.x + __popc(grp.y & 0xFFu & ((1u << slot) - 1u));
                 if (grp.y & 0xFF000000u) {
-                    if (top + 1 >= kWideStack) steps = kMaxSteps;  // overflow: flagged below
+                    if (top + 1 >= kWideStack) overflow = true;  // flagged below
                     else stack[++top] = grp;
                 }
                 uint32_t cbase, tbase, imask;
@@ -430,8 +431,8 @@ __global__ void __launch_bounds__(256)
                 }
             }
         }
-        if (!finished && ++steps >= kMaxSteps) {
-            atomicOr(flag, 1);
+        if (!finished && (overflow || ++steps >= max_steps)) {
+            atomicOr(flag, overflow ? kFlagStackOverflow : kFlagStepLimit);
             result = 2;
             hit = false;
             bid = -2;
@@ -468,12 +469,13 @@ cav_status launch_wide(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, in
     if (stats) {
         const int grid = grid_for(ctx, k_trace_wide<kAny, true, false>, block);
         k_trace_wide<kAny, true, false><<<grid, block, 0, s>>>(bvh->cnodes, bvh->ctris, rays, n, n_dev, prim, t, uv,
-                                                               limit, excl, occ, counter, batch, flag, stats, nullptr, 0);
+                                                               limit, excl, occ, counter, batch, ctx->max_trace_steps, flag, stats,
+                                                               nullptr, 0);
     } else {
         const int grid = grid_for(ctx, k_trace_wide<kAny, false, false>, block);
         k_trace_wide<kAny, false, false><<<grid, block, 0, s>>>(bvh->cnodes, bvh->ctris, rays, n, n_dev, prim, t, uv,
-                                                                limit, excl, occ, counter, batch, flag, nullptr, nullptr,
-                                                                0);
+                                                                limit, excl, occ, counter, batch, ctx->max_trace_steps,
+                                                                flag, nullptr, nullptr, 0);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;
@@ -494,12 +496,14 @@ cav_status trace_wide_segments(cav_ctx* ctx, bool any_hit, const TraceSeg* segs,
         const int grid = grid_for(ctx, k_trace_wide<true, false, true>, block);
         k_trace_wide<true, false, true><<<grid, block, 0, s>>>(nullptr, nullptr, nullptr, n, nullptr, nullptr, nullptr,
                                                                nullptr, nullptr, nullptr, nullptr, counter, batch,
-                                                               ctx->d_error + 3, nullptr, segs, nseg);
+                                                               ctx->max_trace_steps, ctx->d_error + 3, nullptr, segs,
+                                                               nseg);
     } else {
         const int grid = grid_for(ctx, k_trace_wide<false, false, true>, block);
         k_trace_wide<false, false, true><<<grid, block, 0, s>>>(nullptr, nullptr, nullptr, n, nullptr, nullptr, nullptr,
                                                                 nullptr, nullptr, nullptr, nullptr, counter, batch,
-                                                                ctx->d_error + 2, nullptr, segs, nseg);
+                                                                ctx->max_trace_steps, ctx->d_error + 2, nullptr, segs,
+                                                                nseg);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;

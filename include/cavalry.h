@@ -30,7 +30,8 @@ typedef enum cav_status {
     CAV_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed */
     CAV_ERR_TIMEOUT = 4,          /* a bounded device-side wait gave up */
     CAV_ERR_STACK_OVERFLOW = 5,   /* traversal stack depth exceeded (rays flagged) */
-    CAV_ERR_NOT_READY = 6
+    CAV_ERR_NOT_READY = 6,
+    CAV_ERR_CANCELLED = 7         /* the job was cancelled (cav_server_cancel) */
 } cav_status;
 
 typedef struct cav_ctx cav_ctx;
@@ -45,10 +46,31 @@ const char* cav_status_string(cav_status s);
 /* ABI version: major*10000 + minor*100 + patch. */
 int cav_version(void);
 /* Synchronises `stream` and reports the device-side error flags raised since the last
- * check (sort look-back timeout, treelet inconsistency, traversal stack overflow),
- * clearing them.  The reference reports such conditions with device printf only
- * (Utils/GpuCommons.h:13-20). */
+ * check, clearing them: CAV_ERR_TIMEOUT for a radix-sort look-back wait that gave up or a
+ * ray stopped at the traversal step limit, CAV_ERR_STACK_OVERFLOW for a full traversal
+ * stack, CAV_ERR_INVALID_ARGUMENT for a vertex index out of range in a build, CAV_ERR_CUDA
+ * for a broken build or treelet invariant.  The reference reports such conditions with
+ * device printf only (Utils/GpuCommons.h:13-20). */
 cav_status cav_sync_check(cav_ctx* ctx, void* stream);
+
+/* Bounds of the device-side waits of this context (no wait in any kernel is unbounded):
+ *   sort_wait_s     : how long a radix-sort tile waits for its predecessors' published
+ *                     digit counts before it gives up (<= 0: 2 s);
+ *   max_trace_steps : node + triangle visits one ray may take before the traversal stops it
+ *                     (prim_id -2 / occluded 2) (<= 0: 2^22).
+ * Either ends in CAV_ERR_TIMEOUT from cav_sync_check; the context stays usable. */
+cav_status cav_ctx_set_limits(cav_ctx* ctx, double sort_wait_s, int64_t max_trace_steps);
+/* Failure injection, for testing the error paths without a device fault:
+ *   CAV_INJECT_SORT_STALL (count > 0 on, 0 off): the first tile of every radix-sort pass
+ *     withholds its digit counts, so the later tiles' bounded look-back waits run out; the
+ *     build completes with CAV_ERR_TIMEOUT from cav_sync_check and a tree that is not
+ *     meaningful;
+ *   CAV_INJECT_ALLOC_FAIL: the count-th next device allocation made for this context (build
+ *     arenas and scratch, scene uploads, render path state, server job buffers) fails once,
+ *     and the call that made it returns CAV_ERR_OUT_OF_MEMORY (the others succeed);
+ *   CAV_INJECT_NONE clears both.  Nothing here faults, traps or hangs the device. */
+enum { CAV_INJECT_NONE = 0, CAV_INJECT_SORT_STALL = 1, CAV_INJECT_ALLOC_FAIL = 2 };
+cav_status cav_ctx_inject(cav_ctx* ctx, int what, int count);
 
 /*
  * LBVH build + treelet restructuring.  Replaces BVH::build (BVH/BVH.cu:317-370).
@@ -125,7 +147,8 @@ typedef struct cav_ray {
  * has no tmax).  Outputs (device, any may be NULL except prim_id):
  *   prim_id[i] : hit triangle (reference triangle index) or -1; -2 if the traversal
  *                stack (128 entries, i.e. trees up to 128 deep) overflowed for that
- *                ray; cav_sync_check then reports CAV_ERR_STACK_OVERFLOW.
+ *                ray or the ray reached the step limit (cav_ctx_set_limits);
+ *                cav_sync_check then reports CAV_ERR_STACK_OVERFLOW / CAV_ERR_TIMEOUT.
  *   t[i], uv[2i..2i+1] : hit distance and barycentrics (u, v) of that triangle.
  */
 cav_status cav_trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int32_t* prim_id,
@@ -136,7 +159,7 @@ cav_status cav_trace_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* ra
  * id equals the ray's source or target mesh are skipped; with a limit a hit counts
  * only if its distance is < limit.  limit: n floats or NULL (no limit);
  * excl_mesh: 2n int32 (source, target; -1 = none) or NULL.  occluded[i] = 1 if
- * blocked, 0 if visible, 2 if the stack overflowed.
+ * blocked, 0 if visible, 2 if the stack overflowed or the step limit was reached.
  */
 cav_status cav_trace_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,
                          const int32_t* excl_mesh, int64_t n, uint8_t* occluded, uint32_t flags, void* stream);
@@ -303,7 +326,7 @@ cav_status cav_write_pfm(const char* path, const float* film_sum, const float* f
  */
 typedef struct cav_server cav_server;
 enum { CAV_SERVE_MERGED = 0, CAV_SERVE_SEQUENTIAL = 1 };
-enum { CAV_JOB_PENDING = 0, CAV_JOB_RUNNING = 1, CAV_JOB_DONE = 2, CAV_JOB_FAILED = 3 };
+enum { CAV_JOB_PENDING = 0, CAV_JOB_RUNNING = 1, CAV_JOB_DONE = 2, CAV_JOB_FAILED = 3, CAV_JOB_CANCELLED = 4 };
 typedef struct cav_server_config {
     int64_t hbm_budget_bytes; /* <= 0: 80 GiB */
     int mode;                 /* CAV_SERVE_MERGED or CAV_SERVE_SEQUENTIAL */
@@ -317,6 +340,8 @@ typedef struct cav_server_config {
     int64_t min_paths_per_slice; /* floor of a render job's chunk while others are live (<= 0:
                                   4M, i.e. every chunk as large as the job's state allows);
                                   smaller floors shorten ticks (latency) at some throughput */
+    int reject_over_budget;    /* 1: a job whose device memory exceeds the whole budget is refused at
+                                  submission (CAV_ERR_OUT_OF_MEMORY); 0: it runs when it is alone */
 } cav_server_config;
 typedef struct cav_job_status {
     int state;         /* CAV_JOB_* */
@@ -340,6 +365,11 @@ cav_status cav_server_submit_render(cav_server* server, cav_scene* scene, const 
 cav_status cav_server_submit_rays(cav_server* server, const cav_bvh* bvh, int any_hit, const cav_ray* host_rays,
                                   const float* host_limit, const int32_t* host_excl, int64_t n, int32_t* host_prim,
                                   float* host_t, float* host_uv, uint8_t* host_occ, int64_t* job_id);
+/* Cancels a job.  A pending job leaves the queue at once; a running job is stopped by its
+ * lane before its next bounce, its device state freed, and its host outputs are left as they
+ * are (partial).  Either way the job ends in CAV_JOB_CANCELLED and cav_server_wait returns
+ * CAV_ERR_CANCELLED; a job that already finished is not changed.  Other jobs are unaffected. */
+cav_status cav_server_cancel(cav_server* server, int64_t job_id);
 cav_status cav_server_poll(cav_server* server, int64_t job_id, cav_job_status* status);
 /* Waits for a job (timeout_s < 0: forever); returns the job's status or CAV_ERR_TIMEOUT. */
 cav_status cav_server_wait(cav_server* server, int64_t job_id, double timeout_s, cav_job_status* status);

@@ -179,3 +179,80 @@ def test_fast_trace_server_matches_exact(ctx, pool):
     assert np.array_equal(pr >= 0, p >= 0)
     both = p >= 0
     assert np.all(np.abs(tr[both] - t[both]) <= 1e-6 * np.abs(t[both]))
+
+
+def _wait_running(sv, jid, timeout=60.0):
+    import time
+
+    import cavalry_b200 as cav
+
+    t0 = time.time()
+    while sv.poll(jid).state == cav.JOB_PENDING:
+        assert time.time() - t0 < timeout
+        time.sleep(0.001)
+
+
+def test_cancel_pending_and_running_jobs(ctx, pool):
+    """A job cancelled while pending leaves the queue at once; a job cancelled while running
+    stops before its next bounce and frees its state; the job between them finishes with the
+    result it has alone, and the server ends with nothing live and no memory in use."""
+    import cavalry_b200 as cav
+
+    sv = cav.Server(ctx, max_live_jobs=1, max_paths_per_job=4096)
+    long_id, _, _ = sv.submit_render(pool[1], spp=256, max_depth=4, width=64, height=64)  # 256 chunks x 4 bounces
+    mid_id, fs, fw = sv.submit_render(pool[0], spp=2, max_depth=4)
+    late_id, _, _ = sv.submit_render(pool[2], spp=2, max_depth=4)
+    sv.cancel(late_id)
+    st = sv.poll(late_id)
+    assert st.state == cav.JOB_CANCELLED and st.status == 7
+    _wait_running(sv, long_id)
+    sv.cancel(long_id)
+    assert sv.wait(long_id, 120).state == cav.JOB_CANCELLED
+    assert sv.wait(mid_id, 120).state == cav.JOB_DONE
+    s, w = direct_render(pool[0], 2)
+    assert np.array_equal(fw, w) and np.allclose(fs, s, rtol=2e-5, atol=1e-6)
+    sv.cancel(mid_id)  # finished: unchanged
+    assert sv.poll(mid_id).state == cav.JOB_DONE
+    st = sv.stats()
+    assert st.live == 0 and st.pending == 0 and st.hbm_in_use == 0
+    sv.close()
+
+
+def test_admission_rejects_jobs_over_the_budget(ctx, pool):
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    sv = cav.Server(ctx, hbm_budget_bytes=1 << 20, reject_over_budget=True)
+    with pytest.raises(cav.CavError) as e:
+        sv.submit_render(pool[1], spp=2, max_depth=4)
+    assert e.value.status == 3  # CAV_ERR_OUT_OF_MEMORY, and no job was created
+    rays = scenes.closest_rays(1000, seed=12)  # ~50 KB: admitted
+    jid, p, _, _ = sv.submit_rays(pool[1].bvh(), rays)
+    assert sv.wait(jid, 60).state == cav.JOB_DONE and (p >= -1).all()
+    sv.close()
+
+
+def test_injected_allocation_failure_fails_only_that_job(ctx, pool):
+    """While a long render runs, the next device allocation is made to fail: the job that
+    makes it (a render submitted then) fails with CAV_ERR_OUT_OF_MEMORY, the running job and
+    a job submitted afterwards finish with the results they have alone."""
+    import cavalry_b200 as cav
+
+    sv = cav.Server(ctx, max_paths_per_job=4096)
+    long_id, fs_l, fw_l = sv.submit_render(pool[1], spp=16, max_depth=4, width=64, height=64)
+    _wait_running(sv, long_id)
+    ctx.inject(cav.INJECT_ALLOC_FAIL, 1)
+    bad_id, _, _ = sv.submit_render(pool[0], spp=2, max_depth=4)
+    with pytest.raises(cav.CavError) as e:
+        sv.wait(bad_id, 120)
+    assert e.value.status == 3 and sv.poll(bad_id).state == cav.JOB_FAILED
+    ctx.inject(cav.INJECT_NONE)
+    ok_id, fs, fw = sv.submit_render(pool[0], spp=2, max_depth=4)
+    assert sv.wait(ok_id, 120).state == cav.JOB_DONE
+    assert sv.wait(long_id, 120).state == cav.JOB_DONE
+    s, w = direct_render(pool[0], 2)
+    assert np.array_equal(fw, w) and np.allclose(fs, s, rtol=2e-5, atol=1e-6)
+    s, w, _ = pool[1].render(spp=16, max_depth=4, width=64, height=64, integrator="path",
+                             max_paths_in_flight=4096)
+    assert np.array_equal(fw_l, w) and np.allclose(fs_l, s, rtol=2e-5, atol=1e-6)
+    sv.close()
