@@ -60,6 +60,8 @@ def parse():
                    help="soup: BVH + 4M closest-hit rays (default); render: the 5.24M-triangle path-traced scene; "
                         "serve: a Poisson stream of render and ray-query jobs, merged server vs sequential loop")
     p.add_argument("--jobs", type=int, default=256, help="jobs in the served stream (serve workload)")
+    p.add_argument("--serve-trace", default="fast", choices=["fast", "exact"], help="serve workload: traversal mode")
+    p.add_argument("--serve-loaders", type=int, default=8, help="serve workload: the server's scene loader threads")
     p.add_argument("--bounce", type=int, default=1, help="capture workload: which bounce's extend rays")
     p.add_argument("--no-reference", action="store_true", help="render workload: skip the reference's CUDA build")
     p.add_argument("--render-steps", type=int, default=1, help="timed full renders (render workload)")
@@ -854,15 +856,25 @@ def run_capture(args):
 
 # ------------------------------------------------------------------------ serve workload
 def run_serve(args):
-    """Served stream: jobs arrive as a Poisson process (mean gap 20 ms, seed 4).  Scenes are
-    config-2-type soups (16 of them, triangle counts log-uniform in [1k, 2M], seeds 100+)
-    resident with their BVHs; 3 of 4 jobs render one (resolution uniform in {64^2, 256^2,
-    512^2, 1024^2}, spp uniform in {1, 4, 16, 64}, depth 6, path integrator), 1 of 4 is a
-    ray-query job of 256k-4M config-1-style rays (half closest hit, half any hit).  The same
-    stream is served by the merged server (continuous batching, shared traversal launches)
-    and by the plain sequential loop (each job through cav_render or the host-buffer trace
-    calls in arrival order, same kernels); each job's result is checked to be the same in
-    both.  Latency = completion - arrival."""
+    """Served stream (config 4): `--jobs` jobs (256) arriving as a Poisson process (mean gap
+    20 ms, seed 4), each with its OWN seeded scene of the soup type (scenes.soup_scene: a
+    config-2-type soup, triangle counts log-uniform in [1k, 2M], seed 1000 + job) written
+    before the stream starts as a .pbrt file with its mesh in binary PLY.  3 of 4 jobs render
+    their scene (resolution uniform in {64^2, 256^2, 512^2, 1024^2}, spp uniform in {1, 4, 16,
+    64}, depth 6, path integrator); 1 of 4 are ray queries of 256k-4M rays (log-uniform; half
+    closest hit, half any hit with limits) against their scene's tree.  Treelet rounds follow
+    the reference's default (3, or 10 when spp >= 64) in both arms.
+
+    Server arm: cav_server_submit_scene per job at its arrival: loader threads parse, the
+    job is admitted under an 80 GB HBM budget, the trees of scenes admitted together are
+    built in one batched build on the lane's stream, renders join the merged traversal
+    launches (or, for small ones, are replayed as one CUDA graph), the scene is freed at the
+    end.  Plain loop: per job in arrival order, what a user writes with the public calls:
+    cav_scene_load_pbrt (parse, upload, build), cav_render_to_host or the host-buffer trace
+    calls, cav_scene_free.  Both arms trace in the same mode (`--serve-trace`, default fast)
+    and render the same samples, so every job's result is compared between them (relMSE of
+    films, equality of hits).  Latency = completion - arrival."""
+    import shutil
     import tempfile
     import threading
 
@@ -872,48 +884,51 @@ def run_serve(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    flags = cav.TRACE_FAST if args.serve_trace == "fast" else cav.TRACE_EXACT
     rng = np.random.default_rng(4)
-    n_scenes = 16
-    sizes = np.exp(rng.uniform(np.log(1e3), np.log(2e6), n_scenes)).astype(int)
     resolutions = [64, 256, 512, 1024]
-    ctx = cav.Context(0)
-    tmp = tempfile.mkdtemp()
-    pool = {}
-    t0 = time.time()
-    soups = {}
-    for k, n in enumerate(sizes):
-        soups[k] = scenes.soup_scene(int(n), seed=100 + k)
-        path = os.path.join(tmp, f"soup{k}.pbrt")
-        scenes.write_pbrt(path, soups[k], width=64, height=64, spp=1, max_depth=6)
-        pool[k] = ctx.load_pbrt(path, bvh_rounds=3)  # resident scene + BVH; jobs pick the resolution
-    setup_s = time.time() - t0
-    # the job stream
     jobs = []
     t = 0.0
     for i in range(args.jobs):
         t += rng.exponential(0.020)
-        k = int(rng.integers(0, n_scenes))
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(2e6))))
         if rng.random() < 0.25:
             nr = int(np.exp(rng.uniform(np.log(2 ** 18), np.log(2 ** 22))))
             kind = "any" if rng.random() < 0.5 else "closest"
-            jobs.append(dict(at=t, kind=kind, scene=k, rays=nr, seed=1000 + i))
+            jobs.append(dict(at=t, kind=kind, tris=n, rays=nr, seed=1000 + i))
         else:
-            jobs.append(dict(at=t, kind="render", scene=k, res=resolutions[int(rng.integers(0, 4))],
-                             spp=[1, 4, 16, 64][int(rng.integers(0, 4))]))
+            jobs.append(dict(at=t, kind="render", tris=n, res=resolutions[int(rng.integers(0, 4))],
+                             spp=[1, 4, 16, 64][int(rng.integers(0, 4))], seed=1000 + i))
+    tmp = tempfile.mkdtemp(prefix="cav_serve_")
+    t0 = time.time()
     ray_inputs = {}
     for i, j in enumerate(jobs):
+        j["path"] = os.path.join(tmp, f"job{i}.pbrt")
+        res = j.get("res", 64)
+        scenes.write_pbrt(j["path"], scenes.soup_scene(j["tris"], seed=j["seed"]), width=res, height=res,
+                          spp=j.get("spp", 1), max_depth=6, ply=True)
         if j["kind"] == "closest":
             ray_inputs[i] = (scenes.closest_rays(j["rays"], seed=j["seed"]), None)
         elif j["kind"] == "any":
-            r, lim = scenes.shadow_rays(j["rays"], seed=j["seed"])
-            ray_inputs[i] = (r, lim)
+            ray_inputs[i] = scenes.shadow_rays(j["rays"], seed=j["seed"])
+    setup_s = time.time() - t0
+    ctx = cav.Context(0)
 
-    def serve(mode, flags=cav.TRACE_EXACT, floor=0):
-        sv = cav.Server(ctx, hbm_budget_bytes=80 << 30, mode=mode, trace_flags=flags, min_paths_per_slice=floor)
+    def summarize(lat, makespan, service):
+        lat = np.array(lat)
+        return {"jobs_per_s": round(len(jobs) / makespan, 3), "makespan_s": round(makespan, 3),
+                "p50_latency_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
+                "p99_latency_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
+                "mean_latency_ms": round(float(lat.mean()) * 1e3, 2),
+                "service_s_by_class": dict(sorted((k, round(v, 3)) for k, v in service.items()))}
+
+    def serve():
+        sv = cav.Server(ctx, hbm_budget_bytes=80 << 30, mode=cav.SERVE_MERGED, trace_flags=flags,
+                        loaders=args.serve_loaders)
         ids = [None] * len(jobs)
         outs = [None] * len(jobs)
-        clock0 = sv.stats().now_s
         wall0 = time.perf_counter()
+        clock0 = sv.stats().now_s
 
         def submitter():
             for i, j in enumerate(jobs):
@@ -921,13 +936,11 @@ def run_serve(args):
                 if delay > 0:
                     time.sleep(delay)
                 if j["kind"] == "render":
-                    jid, fs, fw = sv.submit_render(pool[j["scene"]], spp=j["spp"], max_depth=6, width=j["res"],
-                                                   height=j["res"])
+                    jid, fs, fw = sv.submit_scene_render(j["path"], j["res"], j["res"], spp=j["spp"], max_depth=6)
                     outs[i] = (fs, fw)
                 else:
-                    bvh = pool[j["scene"]].bvh()
                     r, lim = ray_inputs[i]
-                    res = sv.submit_rays(bvh, r, any_hit=j["kind"] == "any", limit=lim)
+                    res = sv.submit_scene_rays(j["path"], r, any_hit=j["kind"] == "any", limit=lim)
                     jid = res[0]
                     outs[i] = res[1:]
                 ids[i] = jid
@@ -935,30 +948,25 @@ def run_serve(args):
         th = threading.Thread(target=submitter)
         th.start()
         th.join()
-        stats = [sv.wait(jid, timeout_s=1800).as_dict() for jid in ids]
+        stats = [sv.wait(jid, timeout_s=3600).as_dict() for jid in ids]
         st = sv.stats().as_dict()
         sv.close()
-        lat = np.array([s["t_done"] - s["t_submit"] for s in stats])
-        first = min(s["t_submit"] for s in stats)
-        last = max(s["t_done"] for s in stats)
-        # start-to-done time summed per job class (in the sequential loop these add up to
-        # the makespan, so they show which jobs the stream's time goes to)
+        # arrival = submission on the server's clock (the submitter keeps the schedule)
+        lat = [s["t_done"] - (clock0 + j["at"]) for s, j in zip(stats, jobs)]
+        makespan = max(s["t_done"] for s in stats) - (clock0 + jobs[0]["at"])
         service = {}
         for j, s in zip(jobs, stats):
             cls = f"render_{j['res']}" if j["kind"] == "render" else f"rays_{j['kind']}"
-            service[cls] = round(service.get(cls, 0.0) + s["t_done"] - s["t_start"], 3)
-        return {"jobs_per_s": round(len(jobs) / (last - first), 2), "makespan_s": round(last - first, 3),
-                "service_s_by_class": dict(sorted(service.items())),
-                "p50_latency_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
-                "p99_latency_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
-                "mean_latency_ms": round(float(lat.mean()) * 1e3, 2),
-                "ticks": st["ticks"], "closest_launches": st["closest_launches"], "any_launches": st["any_launches"],
-                "max_segments_per_launch": st["max_segments"], "server_busy_s": round(st["busy_s"], 3)}, outs
+            service[cls] = service.get(cls, 0.0) + s["t_done"] - s["t_start"]
+        out = summarize(lat, makespan, service)
+        out.update({"ticks": st["ticks"], "closest_launches": st["closest_launches"],
+                    "any_launches": st["any_launches"], "max_segments_per_launch": st["max_segments"],
+                    "server_busy_s": round(st["busy_s"], 3)})
+        return out, outs
 
-    def plain_loop(flags=cav.TRACE_EXACT):
-        """The plain sequential loop a user writes without the server: each job, in arrival
-        order, through the public one-shot calls (cav_render with its default 4M-path chunks;
-        the host-buffer trace calls), results back in host memory."""
+    def plain_loop():
+        """The plain sequential loop: each job, in arrival order, through the public one-shot
+        calls; results back in host memory."""
         fast = flags == cav.TRACE_FAST
         outs = [None] * len(jobs)
         lat, service = [], {}
@@ -968,68 +976,61 @@ def run_serve(args):
             if delay > 0:
                 time.sleep(delay)
             t0 = time.perf_counter()
+            sc = ctx.load_pbrt(j["path"])
             if j["kind"] == "render":
-                fs, fw, _ = pool[j["scene"]].render(spp=j["spp"], max_depth=6, width=j["res"], height=j["res"],
-                                                    fast_trace=fast)
+                fs, fw, _ = sc.render(spp=j["spp"], max_depth=6, width=j["res"], height=j["res"], integrator="path",
+                                      fast_trace=fast)
                 outs[i] = (fs, fw)
                 cls = f"render_{j['res']}"
             else:
-                bvh = pool[j["scene"]].bvh()
+                bvh = sc.bvh()
                 r, lim = ray_inputs[i]
                 if j["kind"] == "closest":
                     outs[i] = tuple(bvh.trace_closest_host(r, flags=flags))
                 else:
                     outs[i] = (bvh.trace_any_host(r, limit=lim, flags=flags),)
                 cls = f"rays_{j['kind']}"
+            sc.free()
             t1 = time.perf_counter()
-            service[cls] = round(service.get(cls, 0.0) + t1 - t0, 3)
+            service[cls] = service.get(cls, 0.0) + t1 - t0
             lat.append(t1 - wall0 - j["at"])
         makespan = time.perf_counter() - wall0 - jobs[0]["at"]
-        lat = np.array(lat)
-        return {"jobs_per_s": round(len(jobs) / makespan, 2), "makespan_s": round(makespan, 3),
-                "service_s_by_class": dict(sorted(service.items())),
-                "p50_latency_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
-                "p99_latency_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
-                "mean_latency_ms": round(float(lat.mean()) * 1e3, 2)}, outs
+        return summarize(lat, makespan, service), outs
 
-    for sc in pool.values():  # the 8-wide views exist before any timed arm
-        sc.render(spp=1, max_depth=1, width=8, height=8, fast_trace=True)
-    merged_f, out_mf = serve(cav.SERVE_MERGED, cav.TRACE_FAST)
-    merged_fl, _ = serve(cav.SERVE_MERGED, cav.TRACE_FAST, floor=1 << 20)  # 1M-path slices: shorter ticks
-    plain_f, out_pf = plain_loop(cav.TRACE_FAST)
-    seq_f, _ = serve(cav.SERVE_SEQUENTIAL, cav.TRACE_FAST)
-    merged, out_m = serve(cav.SERVE_MERGED)
+    # warm-up: one small job through each arm (first-use costs: module load, Halton tables)
+    sc = ctx.load_pbrt(jobs[0]["path"])
+    sc.render(spp=1, max_depth=2, width=16, height=16, fast_trace=flags == cav.TRACE_FAST)
+    sc.free()
     plain, out_p = plain_loop()
-    # the same result alone (the plain loop) and in the mix (merged server)
-    worst = 0.0
-    for a, b in list(zip(out_m, out_p)) + list(zip(out_mf, out_pf)):
-        for x, y in zip(a, b):
-            if x.dtype == np.float32:
-                fin = np.isfinite(y)
-                if not np.array_equal(fin, np.isfinite(x)):
-                    worst = float("inf")
-                elif fin.any():
-                    worst = max(worst, float(np.max(np.abs(x[fin] - y[fin]) / (np.abs(y[fin]) + 1e-3))))
-            elif not np.array_equal(x, y):
-                worst = float("inf")
+    merged, out_m = serve()
+    # each job's result alone (plain loop) against the same job in the mix (server)
+    rel, ray_same = [], []
+    for i, j in enumerate(jobs):
+        a, b = out_m[i], out_p[i]
+        if j["kind"] == "render":
+            ra = a[0] / np.maximum(a[1], 1e-30)[..., None]
+            rb = b[0] / np.maximum(b[1], 1e-30)[..., None]
+            rel.append(float(np.mean((ra - rb) ** 2 / (rb ** 2 + 1e-2))))
+        else:
+            ray_same.append(all(np.array_equal(x, y) for x, y in zip(a, b)))
+    shutil.rmtree(tmp, ignore_errors=True)
     renders = sum(1 for j in jobs if j["kind"] == "render")
     out = {
-        "metric": "served jobs/s (merged server vs plain sequential render loop)", "value": merged_f["jobs_per_s"],
-        "unit": "jobs/s",
-        "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
-        "data": "synthetic (seeded soups written as .pbrt; seeded Poisson job stream)",
-        "config": {"workload": f"served_stream_{len(jobs)}_jobs_poisson_20ms", "jobs": len(jobs), "render_jobs": renders,
-                   "ray_jobs": len(jobs) - renders, "scenes": n_scenes,
-                   "scene_triangles": [int(x) for x in sizes], "resolutions": resolutions, "spp": [1, 4, 16, 64],
-                   "depth": 6, "hbm_budget_gib": 80},
-        "trace_mode": "value: merged launches in the compressed 8-wide mode (fast_trace); exact-mode arms beside",
-        "baseline": "plain loop: cav_render / host-buffer trace calls per job in arrival order, same trace mode",
-        "fast_trace": {"merged": merged_f, "merged_1M_slices": merged_fl, "plain_loop": plain_f,
-                       "server_one_job_at_a_time": seq_f,
-                       "speedup_vs_plain_loop": round(merged_f["jobs_per_s"] / plain_f["jobs_per_s"], 3)},
-        "merged": merged, "plain_loop": plain,
+        "metric": "served jobs/s (server vs plain sequential loop, jobs bring their own scenes)",
+        "value": merged["jobs_per_s"], "unit": "jobs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded soups written as .pbrt + binary PLY per job; seeded Poisson job stream)",
+        "config": {"workload": f"served_stream_{len(jobs)}_jobs_own_scenes_poisson_20ms", "jobs": len(jobs),
+                   "render_jobs": renders, "ray_jobs": len(jobs) - renders,
+                   "triangles_total": int(sum(j["tris"] for j in jobs)),
+                   "triangles_range": [int(min(j["tris"] for j in jobs)), int(max(j["tris"] for j in jobs))],
+                   "resolutions": resolutions, "spp": [1, 4, 16, 64], "depth": 6, "hbm_budget_gib": 80,
+                   "trace_mode": args.serve_trace, "loaders": args.serve_loaders},
+        "server": merged, "plain_loop": plain,
         "speedup_vs_plain_loop": round(merged["jobs_per_s"] / plain["jobs_per_s"], 3),
-        "max_rel_diff_merged_vs_plain_loop": worst, "setup_s": round(setup_s, 1),
+        "p99_latency_ratio_plain_over_server": round(plain["p99_latency_ms"] / merged["p99_latency_ms"], 3),
+        "relmse_server_vs_alone": {"max": max(rel) if rel else None, "mean": float(np.mean(rel)) if rel else None,
+                                   "renders": len(rel)},
+        "ray_jobs_identical": int(sum(ray_same)), "setup_s": round(setup_s, 1),
     }
     print(json.dumps(out))
 

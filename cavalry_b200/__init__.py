@@ -121,6 +121,7 @@ def lib() -> ctypes.CDLL:
         "cav_server_destroy": ([P], ctypes.c_int),
         "cav_server_submit_render": ([P, P, P, P, P, P], ctypes.c_int),
         "cav_server_submit_rays": ([P, P, ctypes.c_int, P, P, P, ctypes.c_int64, P, P, P, P, P], ctypes.c_int),
+        "cav_server_submit_scene": ([P, P, P], ctypes.c_int),
         "cav_server_poll": ([P, ctypes.c_int64, P], ctypes.c_int),
         "cav_server_wait": ([P, ctypes.c_int64, ctypes.c_double, P], ctypes.c_int),
         "cav_server_stats": ([P, P], ctypes.c_int),
@@ -439,10 +440,22 @@ class Scene:
             pass
 
 
+SCENE_RENDER, SCENE_CLOSEST, SCENE_ANY = 0, 1, 2
+
+
+class SceneJob(ctypes.Structure):
+    _fields_ = [("pbrt_path", ctypes.c_char_p), ("kind", ctypes.c_int), ("bvh_rounds", ctypes.c_int),
+                ("render", RenderOpts), ("host_sum", ctypes.c_void_p), ("host_weight", ctypes.c_void_p),
+                ("host_rays", ctypes.c_void_p), ("host_limit", ctypes.c_void_p), ("host_excl", ctypes.c_void_p),
+                ("n_rays", ctypes.c_int64), ("host_prim", ctypes.c_void_p), ("host_t", ctypes.c_void_p),
+                ("host_uv", ctypes.c_void_p), ("host_occ", ctypes.c_void_p)]
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("mode", ctypes.c_int), ("max_live_jobs", ctypes.c_int),
                 ("max_paths_per_job", ctypes.c_int64), ("trace_flags", ctypes.c_uint32), ("lanes", ctypes.c_int),
-                ("min_paths_per_slice", ctypes.c_int64), ("reject_over_budget", ctypes.c_int)]
+                ("min_paths_per_slice", ctypes.c_int64), ("reject_over_budget", ctypes.c_int),
+                ("loaders", ctypes.c_int), ("graph_max_paths", ctypes.c_int64)]
 
 
 class JobStatus(ctypes.Structure):
@@ -474,10 +487,11 @@ class Server:
 
     def __init__(self, ctx: "Context", hbm_budget_bytes: int = 80 << 30, mode: int = SERVE_MERGED,
                  max_live_jobs: int = 64, max_paths_per_job: int = 0, trace_flags: int = TRACE_EXACT, lanes: int = 0,
-                 min_paths_per_slice: int = 0, reject_over_budget: bool = False):
+                 min_paths_per_slice: int = 0, reject_over_budget: bool = False, loaders: int = 0,
+                 graph_max_paths: int = 0):
         self.ctx = ctx
         cfg = ServerConfig(hbm_budget_bytes, mode, max_live_jobs, max_paths_per_job, trace_flags, lanes,
-                           min_paths_per_slice, int(reject_over_budget))
+                           min_paths_per_slice, int(reject_over_budget), loaders, graph_max_paths)
         h = ctypes.c_void_p()
         ctx._check(lib().cav_server_create(ctx.handle, ctypes.addressof(cfg), ctypes.byref(h)), "cav_server_create")
         self.handle = h
@@ -514,6 +528,42 @@ class Server:
                                               ctypes.byref(job))
         self.ctx._check(st, "cav_server_submit_rays")
         self._keep[job.value] = (bvh, rays, lim, ex, out)
+        return (job.value, *out)
+
+    def submit_scene_render(self, pbrt_path: str, width: int, height: int, spp: int = 0, max_depth: int = 0,
+                            bvh_rounds: int = -1, max_paths_in_flight: int = 0):
+        """A render job that brings its own scene (cav_server_submit_scene): returns (job id,
+        film_sum [H,W,3], film_weight [H,W]), filled once the job is done."""
+        fs = np.zeros((height, width, 3), np.float32)
+        fw = np.zeros((height, width), np.float32)
+        spec = SceneJob(pbrt_path.encode(), SCENE_RENDER, bvh_rounds,
+                        RenderOpts(spp, max_depth, -1, max_paths_in_flight, width, height), fs.ctypes.data,
+                        fw.ctypes.data)
+        job = ctypes.c_int64(0)
+        st = lib().cav_server_submit_scene(self.handle, ctypes.addressof(spec), ctypes.byref(job))
+        self.ctx._check(st, "cav_server_submit_scene")
+        self._keep[job.value] = (spec, fs, fw)
+        return job.value, fs, fw
+
+    def submit_scene_rays(self, pbrt_path: str, rays: np.ndarray, any_hit: bool = False, limit=None, excl=None,
+                          bvh_rounds: int = -1):
+        """A ray-query job against its own scene's tree: returns (job id, *outputs) as submit_rays."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        lim = None if limit is None else np.ascontiguousarray(limit, np.float32)
+        ex = None if excl is None else np.ascontiguousarray(excl, np.int32)
+        if any_hit:
+            out = (np.zeros(n, np.uint8),)
+            spec = SceneJob(pbrt_path.encode(), SCENE_ANY, bvh_rounds, RenderOpts(), None, None, rays.ctypes.data,
+                            _np_ptr(lim), _np_ptr(ex), n, None, None, None, out[0].ctypes.data)
+        else:
+            out = (np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros((n, 2), np.float32))
+            spec = SceneJob(pbrt_path.encode(), SCENE_CLOSEST, bvh_rounds, RenderOpts(), None, None, rays.ctypes.data,
+                            None, None, n, out[0].ctypes.data, out[1].ctypes.data, out[2].ctypes.data, None)
+        job = ctypes.c_int64(0)
+        st = lib().cav_server_submit_scene(self.handle, ctypes.addressof(spec), ctypes.byref(job))
+        self.ctx._check(st, "cav_server_submit_scene")
+        self._keep[job.value] = (spec, rays, lim, ex, out)
         return (job.value, *out)
 
     def wait(self, job: int, timeout_s: float = -1.0) -> JobStatus:

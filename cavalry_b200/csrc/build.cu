@@ -661,12 +661,10 @@ T* carve(unsigned char*& p, size_t count) {
 
 }  // namespace
 
-// The persistent arena of one tree: build nodes, codes, permutation, traversal layout.
-cav_status alloc_bvh(cav_ctx* ctx, int64_t n, cav_bvh** out) {
+// The persistent arrays of one tree (build nodes, codes, permutation, traversal layout),
+// carved from `base`, which must hold bvh_arena_bytes(n).
+size_t bvh_arena_bytes(int64_t n) {
     const int64_t count = 2 * n - 1;
-    cav_bvh* bvh = new cav_bvh();
-    bvh->n = n;
-    bvh->device = ctx->device;
     size_t need = 0;
     need += sizeof(BNode) * count + 256;
     need += 2 * (sizeof(uint64_t) * n + 256);
@@ -674,12 +672,15 @@ cav_status alloc_bvh(cav_ctx* ctx, int64_t n, cav_bvh** out) {
     need += sizeof(TNode) * (n - 1) + 256;
     need += sizeof(TriRec) * n + 256;
     need += 64 + 256;
-    if (dev_alloc(ctx, &bvh->arena, need, nullptr, false) != cudaSuccess) {
-        cudaGetLastError();
-        delete bvh;
-        return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "cav_bvh_build: device allocation failed");
-    }
-    unsigned char* p = (unsigned char*)bvh->arena;
+    return need;
+}
+
+static cav_bvh* carve_bvh(cav_ctx* ctx, int64_t n, unsigned char* base) {
+    const int64_t count = 2 * n - 1;
+    cav_bvh* bvh = new cav_bvh();
+    bvh->n = n;
+    bvh->device = ctx->device;
+    unsigned char* p = base;
     bvh->nodes = carve<BNode>(p, count);
     bvh->codes_unsorted = carve<uint64_t>(p, n);
     bvh->codes_sorted = carve<uint64_t>(p, n);
@@ -688,8 +689,42 @@ cav_status alloc_bvh(cav_ctx* ctx, int64_t n, cav_bvh** out) {
     bvh->tris = carve<TriRec>(p, n);
     bvh->d_root_box = carve<float>(p, 8);
     bvh->d_depth = carve<int32_t>(p, 8);
+    return bvh;
+}
+
+// One tree's arena, stream-ordered on the build's stream (the tree is used there first).
+cav_status alloc_bvh(cav_ctx* ctx, int64_t n, cudaStream_t s, cav_bvh** out) {
+    void* arena = nullptr;
+    if (dev_alloc(ctx, &arena, bvh_arena_bytes(n), s, true) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "cav_bvh_build: device allocation failed");
+    }
+    cav_bvh* bvh = carve_bvh(ctx, n, (unsigned char*)arena);
+    bvh->arena = arena;
     *out = bvh;
     return CAV_OK;
+}
+
+// Releases a tree: its events, its fast-mode view and its arena (or its share of a batch's
+// arena, freed with the last tree of the batch).  async: stream-ordered frees on `s`.
+void bvh_release(cav_bvh* bvh, cudaStream_t s, bool async) {
+    if (!bvh) return;
+    if (bvh->timed)
+        for (int k = 0; k < 7; ++k) cudaEventDestroy(bvh->ev[k]);
+    free_wide(bvh, s, async);
+    void* mem = bvh->arena;
+    if (bvh->shared) {
+        mem = nullptr;
+        if (bvh->shared->refs.fetch_sub(1) == 1) {
+            mem = bvh->shared->p;
+            delete bvh->shared;
+        }
+    }
+    if (mem) {
+        if (async) cudaFreeAsync(mem, s);
+        else cudaFree(mem);
+    }
+    delete bvh;
 }
 
 cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int32_t* indices,
@@ -699,7 +734,7 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
         return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build: invalid argument");
     const int64_t count = 2 * n - 1;
     cav_bvh* bvh = nullptr;
-    cav_status ast = alloc_bvh(ctx, n, &bvh);
+    cav_status ast = alloc_bvh(ctx, n, s, &bvh);
     if (ast != CAV_OK) return ast;
 
     // scratch (stream ordered)
@@ -723,8 +758,7 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     cudaError_t e = dev_alloc(ctx, &sbase, scratch, s, true);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(bvh->arena);
-        delete bvh;
+        bvh_release(bvh, s, true);
         return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "cav_bvh_build: scratch allocation failed");
     }
     unsigned char* q = (unsigned char*)sbase;
@@ -990,19 +1024,32 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     const int64_t total = leaf_offs[K], total_int = int_offs[K];
     if (total >= (1ll << 32)) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_bvh_build_batch: too many triangles");
     for (int k = 0; k < K; ++k) out[k] = nullptr;
+    // one arena for every tree of the batch (one allocation, not K), stream-ordered; the trees
+    // share it and the last one released frees it
+    size_t arena_bytes = 0;
+    for (int k = 0; k < K; ++k) arena_bytes += bvh_arena_bytes(num_triangles[k]) + 256;
+    void* arena = nullptr;
+    if (dev_alloc(ctx, &arena, arena_bytes, s, true) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "cav_bvh_build_batch: device allocation failed");
+    }
+    auto* shared = new SharedArena();
+    shared->p = arena;
+    shared->refs = K;
     std::vector<cav_bvh*> bv(K, nullptr);
+    {
+        unsigned char* p = (unsigned char*)arena;
+        for (int k = 0; k < K; ++k) {
+            p = (unsigned char*)(((uintptr_t)p + 255) & ~(uintptr_t)255);
+            bv[k] = carve_bvh(ctx, num_triangles[k], p);
+            bv[k]->shared = shared;
+            p += bvh_arena_bytes(num_triangles[k]);
+        }
+    }
     auto fail = [&](cav_status st) {
-        for (cav_bvh* b : bv)
-            if (b) {
-                cudaFree(b->arena);
-                delete b;
-            }
+        for (cav_bvh* b : bv) bvh_release(b, s, true);
         return st;
     };
-    for (int k = 0; k < K; ++k) {
-        cav_status st = alloc_bvh(ctx, num_triangles[k], &bv[k]);
-        if (st != CAV_OK) return fail(st);
-    }
     std::vector<BuildSeg> hs(K);
     for (int k = 0; k < K; ++k) {
         BuildSeg& g = hs[k];
@@ -1067,14 +1114,14 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     int32_t* compact = carve<int32_t>(q, cmax);
     int32_t* slot_of = carve<int32_t>(q, nmax);
     uint32_t* blk = carve<uint32_t>(q, div_up(cmax, kScanTile) + 1);
-    // tables (synchronous copies from pageable host memory, before any launch reads them)
-    CAV_CUDA(ctx, cudaStreamSynchronize(s));
-    CAV_CUDA(ctx, cudaMemcpy(dsegs, hs.data(), sizeof(BuildSeg) * K, cudaMemcpyHostToDevice));
-    CAV_CUDA(ctx, cudaMemcpy(d_leaf, leaf_offs.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice));
-    CAV_CUDA(ctx, cudaMemcpy(d_int, int_offs.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice));
+    // tables: stream-ordered copies from pageable host memory (staged before each call returns,
+    // so the host vectors may go once the calls are made)
+    CAV_CUDA(ctx, cudaMemcpyAsync(dsegs, hs.data(), sizeof(BuildSeg) * K, cudaMemcpyHostToDevice, s));
+    CAV_CUDA(ctx, cudaMemcpyAsync(d_leaf, leaf_offs.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice, s));
+    CAV_CUDA(ctx, cudaMemcpyAsync(d_int, int_offs.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice, s));
     std::vector<TreeletSeg> tsegs_host(K);
     for (int k = 0; k < K; ++k) tsegs_host[k] = TreeletSeg{bv[k]->nodes, num_triangles[k]};
-    CAV_CUDA(ctx, cudaMemcpy(tsegs, tsegs_host.data(), sizeof(TreeletSeg) * K, cudaMemcpyHostToDevice));
+    CAV_CUDA(ctx, cudaMemcpyAsync(tsegs, tsegs_host.data(), sizeof(TreeletSeg) * K, cudaMemcpyHostToDevice, s));
     CAV_CUDA(ctx, cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 2 * 8 * 256, s));
     CAV_CUDA(ctx, cudaMemsetAsync(status, 0, sizeof(uint32_t) * (8 + passes2) * (size_t)tiles * 256, s));
     CAV_CUDA(ctx, cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 32, s));

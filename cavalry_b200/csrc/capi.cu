@@ -133,6 +133,9 @@ cav_status cav_ctx_destroy(cav_ctx* ctx) {
     if (ctx->dev_stage) cudaFree(ctx->dev_stage);
     cudaFree(ctx->d_counters);
     cudaFree(ctx->d_error);
+    cudaFree(ctx->d_halton_primes);
+    cudaFree(ctx->d_halton_start);
+    cudaFree(ctx->d_halton_perms);
     delete ctx;
     return CAV_OK;
 }
@@ -173,11 +176,7 @@ cav_status cav_bvh_build(cav_ctx* ctx, const float* positions, int64_t num_verti
 cav_status cav_bvh_free(cav_bvh* bvh) {
     if (!bvh) return CAV_OK;
     cudaSetDevice(bvh->device);
-    if (bvh->timed)
-        for (int k = 0; k < 7; ++k) cudaEventDestroy(bvh->ev[k]);
-    cav::free_wide(bvh);
-    cudaFree(bvh->arena);
-    delete bvh;
+    cav::bvh_release(bvh, nullptr, false);
     return CAV_OK;
 }
 

@@ -10,6 +10,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <mutex>
 #include <string>
 
 #include "../../include/cavalry.h"
@@ -140,7 +141,20 @@ struct cav_ctx {
     size_t dev_stage_bytes = 0;
     cudaStream_t hstream[2] = {nullptr, nullptr};
     cudaEvent_t hevent[2] = {nullptr, nullptr};
+    // Halton tables on the device, uploaded by the first scene and shared by all
+    std::mutex halton_mu;
+    uint32_t* d_halton_primes = nullptr;
+    uint32_t* d_halton_start = nullptr;
+    uint16_t* d_halton_perms = nullptr;
 };
+
+namespace cav {
+// A device allocation shared by the trees of one batched build; the last tree released frees it.
+struct SharedArena {
+    void* p = nullptr;
+    std::atomic<int> refs{0};
+};
+}  // namespace cav
 
 struct cav_bvh {
     int64_t n = 0;  // triangles
@@ -164,7 +178,8 @@ struct cav_bvh {
     float stage_ms[6] = {0, 0, 0, 0, 0, 0};
     cudaEvent_t ev[7] = {};
     bool timed = false;
-    void* arena = nullptr;  // one allocation holding the arrays above
+    void* arena = nullptr;  // one allocation holding the arrays above (null when shared)
+    cav::SharedArena* shared = nullptr;  // the batch's arena the arrays live in, or null
 };
 
 namespace cav {
@@ -177,6 +192,10 @@ cav_status cuda_error(cav_ctx* ctx, cudaError_t e, const char* what);
 cudaError_t dev_alloc(cav_ctx* ctx, void** p, size_t bytes, cudaStream_t s, bool async);
 
 // build.cu
+// Releases a tree (cav_bvh_free); async: stream-ordered frees on `s`, for callers (the
+// server) that must not wait for the device.
+void bvh_release(cav_bvh* bvh, cudaStream_t s, bool async);
+size_t bvh_arena_bytes(int64_t n);
 cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int32_t* indices,
                      const int32_t* mesh_ids, int64_t n, const float* bounds, int rounds, cudaStream_t s,
                      cav_bvh** out);
@@ -231,9 +250,27 @@ cav_status trace_wide_closest(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* r
 cav_status trace_wide_any(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, const float* limit,
                           const int32_t* excl, int64_t n, const uint32_t* n_dev, uint8_t* occ, cudaStream_t s,
                           unsigned long long* counter, unsigned long long* stats = nullptr);
-void free_wide(cav_bvh* bvh);
+void free_wide(cav_bvh* bvh, cudaStream_t s, bool async);
 cav_status trace_wide_segments(cav_ctx* ctx, bool any_hit, const TraceSeg* segs, int nseg, int64_t n, cudaStream_t s,
                                unsigned long long* counter);
+
+// render.cu: scenes that a job brings (the server uploads, builds and releases them on its
+// stream), and the graph-replayed render
+}  // namespace cav
+namespace cavpbrt {
+struct Scene;
+}
+namespace cav {
+cav_status scene_upload(cav_ctx* ctx, cavpbrt::Scene&& desc, cudaStream_t s, bool async, cav_scene** out);
+void scene_release(cav_scene* sc, cudaStream_t s, bool async);
+size_t scene_device_bytes(const cavpbrt::Scene& desc);
+// The scene's device geometry (the inputs of its BVH build) and the tree it traverses.
+void scene_geometry(const cav_scene* sc, const float** pos, int64_t* nv, const int32_t** idx, const int32_t** mesh,
+                    int64_t* nt);
+void scene_set_bvh(cav_scene* sc, cav_bvh* bvh, int rounds);
+int scene_spp(const cav_scene* sc);
+cav_status render_path_graph(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
+                             cudaStream_t s);
 
 // Many scenes' BVHs, one launch per LBVH stage across all of them (build.cu)
 cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, const int64_t* num_vertices,
@@ -246,6 +283,8 @@ cav_status mlp_forward(cav_mlp* m, const float* in, int64_t n, float* out, cudaS
 // Resumable path-integrator render (render.cu), advanced bounce by bounce by the server.
 struct PathJob;
 size_t path_job_bytes(const cav_scene* sc, const cav_render_opts* opts);
+// Path state + film of a W x H x spp render in chunks of max_paths (<= 0: 4M) paths.
+size_t render_state_bytes(int W, int H, int spp, int64_t max_paths);
 cav_status path_job_create(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, int64_t slice, cudaStream_t s,
                            PathJob** out);
 void path_job_set_slice(PathJob* J, int64_t slice);

@@ -211,16 +211,77 @@ void build_halton_tables(std::vector<uint32_t>& primes, std::vector<uint32_t>& s
 
 namespace cav {
 
-static cav_status upload(cav_ctx* ctx, void** dst, const void* src, size_t bytes) {
-    CAV_CUDA(ctx, dev_alloc(ctx, dst, bytes > 0 ? bytes : 16, nullptr, false));
-    if (bytes) CAV_CUDA(ctx, cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+// The Halton tables depend only on the reference's fixed srand(533799): the host tables are
+// computed once per process (std::rand is process-wide state, so never from two threads at
+// once) and copied to the device once per context; every scene of the context shares them.
+struct HaltonTables {
+    std::vector<uint32_t> primes, start;
+    std::vector<uint16_t> perms;
+};
+static const HaltonTables& halton_tables() {
+    static std::once_flag once;
+    static HaltonTables t;
+    std::call_once(once, [] { build_halton_tables(t.primes, t.start, t.perms); });
+    return t;
+}
+
+static cav_status ctx_halton(cav_ctx* ctx, cav_scene* sc) {
+    std::lock_guard<std::mutex> lk(ctx->halton_mu);
+    if (!ctx->d_halton_perms) {
+        const HaltonTables& t = halton_tables();
+        void *a = nullptr, *b = nullptr, *c = nullptr;
+        if (cudaMalloc(&a, t.primes.size() * 4) != cudaSuccess || cudaMalloc(&b, t.start.size() * 4) != cudaSuccess ||
+            cudaMalloc(&c, t.perms.size() * 2) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(a);
+            cudaFree(b);
+            return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "Halton tables: device allocation failed");
+        }
+        CAV_CUDA(ctx, cudaMemcpy(a, t.primes.data(), t.primes.size() * 4, cudaMemcpyHostToDevice));
+        CAV_CUDA(ctx, cudaMemcpy(b, t.start.data(), t.start.size() * 4, cudaMemcpyHostToDevice));
+        CAV_CUDA(ctx, cudaMemcpy(c, t.perms.data(), t.perms.size() * 2, cudaMemcpyHostToDevice));
+        ctx->d_halton_primes = (uint32_t*)a;
+        ctx->d_halton_start = (uint32_t*)b;
+        ctx->d_halton_perms = (uint16_t*)c;
+    }
+    sc->d_primes = ctx->d_halton_primes;
+    sc->d_perm_start = ctx->d_halton_start;
+    sc->d_perms = ctx->d_halton_perms;
     return CAV_OK;
 }
 
-cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, cav_scene** out) {
+// Device bytes a scene takes once uploaded and built (geometry, the tree, the build's peak
+// scratch): the server's admission estimate for jobs that bring their own scene.
+size_t scene_device_bytes(const cavpbrt::Scene& D) {
+    size_t v = 0, t = 0, uv = 0, nrm = 0;
+    for (const auto& m : D.meshes) {
+        v += m.positions.size() / 3;
+        t += m.indices.size() / 3;
+        uv += m.uvs.size() / 2;
+        nrm += m.normals.size() / 3;
+    }
+    size_t b = 12 * v + 16 * t + (nrm ? 12 * v : 0) + (uv ? 8 * v : 0) + 4096 * 4;
+    for (const auto& tx : D.textures) b += (size_t)4 * tx.width * tx.height;
+    b += bvh_arena_bytes((int64_t)std::max<size_t>(t, 2)) + 96 * t;  // tree + build scratch
+    return b;
+}
+
+// Uploads a parsed scene (geometry, materials, lights, textures) without building its BVH.
+// async: device arrays are stream-ordered allocations and copies on `s` (the caller builds
+// and renders on `s` and releases with scene_release_async); else plain, synchronous ones.
+cav_status scene_upload(cav_ctx* ctx, cavpbrt::Scene&& desc, cudaStream_t stream, bool async, cav_scene** out) {
     auto sc = new cav_scene();
     sc->device = ctx->device;
+    sc->async_mem = async;
     sc->desc = std::move(desc);
+    auto upload = [&](void** dst, const void* src, size_t bytes) -> cav_status {
+        CAV_CUDA(ctx, dev_alloc(ctx, dst, bytes > 0 ? bytes : 16, stream, async));
+        if (bytes) {
+            if (async) CAV_CUDA(ctx, cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream));
+            else CAV_CUDA(ctx, cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        }
+        return CAV_OK;
+    };
     const cavpbrt::Scene& D = sc->desc;
     std::vector<float> pos, nrm;
     std::vector<int32_t> idx, tri_mesh;
@@ -301,27 +362,22 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
             if (m.uvs.empty()) uv.insert(uv.end(), m.positions.size() / 3 * 2, 0.f);
             else uv.insert(uv.end(), m.uvs.begin(), m.uvs.end());
         }
-    std::vector<uint32_t> primes, start;
-    std::vector<uint16_t> perms;
-    build_halton_tables(primes, start, perms);
     sc->n_tri = (int64_t)idx.size() / 3;
     sc->n_vert = (int64_t)pos.size() / 3;
     cav_status st = CAV_OK;
-    if ((st = upload(ctx, (void**)&sc->d_pos, pos.data(), pos.size() * 4)) ||
-        (st = upload(ctx, (void**)&sc->d_idx, idx.data(), idx.size() * 4)) ||
-        (st = upload(ctx, (void**)&sc->d_tri_mesh, tri_mesh.data(), tri_mesh.size() * 4)) ||
-        (st = upload(ctx, (void**)&sc->d_meshes, meshes.data(), meshes.size() * sizeof(RMesh))) ||
-        (st = upload(ctx, (void**)&sc->d_mats, mats.data(), mats.size() * sizeof(RMaterial))) ||
-        (st = upload(ctx, (void**)&sc->d_lights, lights.data(), lights.size() * sizeof(RLight))) ||
-        (st = upload(ctx, (void**)&sc->d_primes, primes.data(), primes.size() * 4)) ||
-        (st = upload(ctx, (void**)&sc->d_perm_start, start.data(), start.size() * 4)) ||
-        (st = upload(ctx, (void**)&sc->d_perms, perms.data(), perms.size() * 2))) {
-        cav_scene_free(sc);
+    if ((st = upload((void**)&sc->d_pos, pos.data(), pos.size() * 4)) ||
+        (st = upload((void**)&sc->d_idx, idx.data(), idx.size() * 4)) ||
+        (st = upload((void**)&sc->d_tri_mesh, tri_mesh.data(), tri_mesh.size() * 4)) ||
+        (st = upload((void**)&sc->d_meshes, meshes.data(), meshes.size() * sizeof(RMesh))) ||
+        (st = upload((void**)&sc->d_mats, mats.data(), mats.size() * sizeof(RMaterial))) ||
+        (st = upload((void**)&sc->d_lights, lights.data(), lights.size() * sizeof(RLight))) ||
+        (st = ctx_halton(ctx, sc))) {
+        scene_release(sc, stream, async);
         return st;
     }
-    if ((any_normals && (st = upload(ctx, (void**)&sc->d_nrm, nrm.data(), nrm.size() * 4))) ||
-        (any_uv && (st = upload(ctx, (void**)&sc->d_uv, uv.data(), uv.size() * 4)))) {
-        cav_scene_free(sc);
+    if ((any_normals && (st = upload((void**)&sc->d_nrm, nrm.data(), nrm.size() * 4))) ||
+        (any_uv && (st = upload((void**)&sc->d_uv, uv.data(), uv.size() * 4)))) {
+        scene_release(sc, stream, async);
         return st;
     }
     // image textures as the reference creates them (Core/Texture.h allocate): uchar4 texels
@@ -331,7 +387,7 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
         cudaArray_t arr = nullptr;
         if (cudaMallocArray(&arr, &fmt, t.width, t.height) != cudaSuccess) {
             cudaGetLastError();
-            cav_scene_free(sc);
+            scene_release(sc, stream, async);
             return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "texture allocation failed");
         }
         sc->tex_arrays.push_back(arr);
@@ -349,16 +405,65 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
         cudaTextureObject_t obj = 0;
         if (cudaCreateTextureObject(&obj, &res, &td, nullptr) != cudaSuccess) {
             cudaGetLastError();
-            cav_scene_free(sc);
+            scene_release(sc, stream, async);
             return set_error(ctx, CAV_ERR_CUDA, "texture object creation failed");
         }
         sc->tex_objects.push_back(obj);
     }
     if (!sc->tex_objects.empty() &&
-        (st = upload(ctx, (void**)&sc->d_tex, sc->tex_objects.data(), sc->tex_objects.size() * sizeof(cudaTextureObject_t)))) {
-        cav_scene_free(sc);
+        (st = upload((void**)&sc->d_tex, sc->tex_objects.data(), sc->tex_objects.size() * sizeof(cudaTextureObject_t)))) {
+        scene_release(sc, stream, async);
         return st;
     }
+    *out = sc;
+    return CAV_OK;
+}
+
+// Releases a scene and its tree.  async: stream-ordered frees on `s` (scenes uploaded with
+// async = true); the Halton tables belong to the context.
+void scene_release(cav_scene* sc, cudaStream_t s, bool async) {
+    if (!sc) return;
+    bvh_release(sc->bvh, s, async);
+    void* arrays[] = {sc->d_pos, sc->d_idx, sc->d_nrm, sc->d_tri_mesh, sc->d_meshes, sc->d_mats,
+                      sc->d_lights, sc->d_uv, sc->d_tex};
+    for (void* p : arrays) {
+        if (!p) continue;
+        if (async) cudaFreeAsync(p, s);
+        else cudaFree(p);
+    }
+    for (cudaTextureObject_t t : sc->tex_objects) cudaDestroyTextureObject(t);
+    for (cudaArray_t a : sc->tex_arrays) cudaFreeArray(a);
+    if (sc->graph_stream) {
+        cudaStreamSynchronize(sc->graph_stream);
+        cudaStreamDestroy(sc->graph_stream);
+    }
+    for (cudaEvent_t e : sc->log.pool) cudaEventDestroy(e);
+    if (sc->log.totals_h) cudaFreeHost(sc->log.totals_h);
+    delete sc;
+}
+
+void scene_geometry(const cav_scene* sc, const float** pos, int64_t* nv, const int32_t** idx, const int32_t** mesh,
+                    int64_t* nt) {
+    *pos = sc->d_pos;
+    *nv = sc->n_vert;
+    *idx = sc->d_idx;
+    *mesh = sc->d_tri_mesh;
+    *nt = sc->n_tri;
+}
+
+void scene_set_bvh(cav_scene* sc, cav_bvh* bvh, int rounds) {
+    sc->bvh = bvh;
+    sc->bvh_rounds = rounds;
+}
+
+int scene_spp(const cav_scene* sc) { return sc->desc.spp; }
+
+// Parse result -> uploaded scene with its BVH, synchronously (cav_scene_load_pbrt).
+cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, cav_scene** out) {
+    cav_scene* sc = nullptr;
+    cav_status st = scene_upload(ctx, std::move(desc), nullptr, false, &sc);
+    if (st != CAV_OK) return st;
+    const cavpbrt::Scene& D = sc->desc;
     // BVH over the global triangle list; rounds -1 = the reference's default
     // (3, or 10 when spp >= 64; Core/Scene.cu:141-146)
     if (bvh_rounds < 0) bvh_rounds = D.spp >= 64 ? 10 : 3;
@@ -366,7 +471,7 @@ cav_status scene_from_desc(cav_ctx* ctx, cavpbrt::Scene&& desc, int bvh_rounds, 
     st = build_bvh(ctx, sc->d_pos, sc->n_vert, sc->d_idx, sc->d_tri_mesh, sc->n_tri, nullptr, bvh_rounds, nullptr,
                    &sc->bvh);
     if (st != CAV_OK) {
-        cav_scene_free(sc);
+        scene_release(sc, nullptr, false);
         return st;
     }
     CAV_CUDA(ctx, cudaDeviceSynchronize());
@@ -718,6 +823,12 @@ static void job_chunk_sizes(const cav_scene* sc, const cav_render_opts* opts, in
     chunk = std::min(chunk, total);
 }
 
+size_t render_state_bytes(int W, int H, int spp, int64_t max_paths) {
+    const int64_t total = (int64_t)W * H * spp;
+    const int64_t chunk = std::min<int64_t>(max_paths > 0 ? max_paths : (int64_t)1 << 22, total);
+    return path_state_bytes(chunk) + sizeof(float) * 4 * (int64_t)W * H + 512;
+}
+
 size_t path_job_bytes(const cav_scene* sc, const cav_render_opts* opts) {
     int spp, depth;
     int64_t total, chunk;
@@ -900,28 +1011,7 @@ cav_status cav_scene_load_pbrt(cav_ctx* ctx, const char* path, int spp_override,
 cav_status cav_scene_free(cav_scene* sc) {
     if (!sc) return CAV_OK;
     cudaSetDevice(sc->device);
-    cav_bvh_free(sc->bvh);
-    cudaFree(sc->d_pos);
-    cudaFree(sc->d_idx);
-    cudaFree(sc->d_nrm);
-    cudaFree(sc->d_tri_mesh);
-    cudaFree(sc->d_meshes);
-    cudaFree(sc->d_mats);
-    cudaFree(sc->d_lights);
-    cudaFree(sc->d_uv);
-    for (cudaTextureObject_t t : sc->tex_objects) cudaDestroyTextureObject(t);
-    for (cudaArray_t a : sc->tex_arrays) cudaFreeArray(a);
-    cudaFree(sc->d_tex);
-    cudaFree(sc->d_primes);
-    cudaFree(sc->d_perm_start);
-    cudaFree(sc->d_perms);
-    if (sc->graph_stream) {
-        cudaStreamSynchronize(sc->graph_stream);
-        cudaStreamDestroy(sc->graph_stream);
-    }
-    for (cudaEvent_t e : sc->log.pool) cudaEventDestroy(e);
-    if (sc->log.totals_h) cudaFreeHost(sc->log.totals_h);
-    delete sc;
+    cav::scene_release(sc, nullptr, false);
     return CAV_OK;
 }
 

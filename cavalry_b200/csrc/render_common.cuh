@@ -798,11 +798,12 @@ struct cav_scene {
     std::vector<cudaArray_t> tex_arrays;          // image textures (uchar4, linear filter, wrap)
     std::vector<cudaTextureObject_t> tex_objects;
     cudaTextureObject_t* d_tex = nullptr;
-    uint32_t* d_primes = nullptr;
+    uint32_t* d_primes = nullptr;  // Halton tables: the context's (shared by its scenes)
     uint32_t* d_perm_start = nullptr;
     uint16_t* d_perms = nullptr;
     cav_bvh* bvh = nullptr;
     int bvh_rounds = 0;
+    bool async_mem = false;  // arrays are stream-ordered allocations (scene_upload with async)
     cudaStream_t graph_stream = nullptr;  // private stream for graph capture and replay
     // per-stage timing of the last render: event pairs on the render stream
     struct Log {

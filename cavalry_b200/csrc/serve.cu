@@ -22,12 +22,14 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
 #include <vector>
 
 #include "cav_internal.cuh"
+#include "pbrt.h"
 
 namespace {
 
@@ -38,6 +40,15 @@ enum JobKind { kRender = 0, kClosest = 1, kAny = 2 };
 struct Job {
     int64_t id = 0;
     int kind = kRender;
+    // a scene the job brings (cav_server_submit_scene): parsed by a loader thread, uploaded
+    // and built by the lane that admits the job, released when the job ends
+    bool owns_scene = false;
+    std::string path;
+    int rounds = -1;
+    std::unique_ptr<cavpbrt::Scene> desc;
+    bool graph = false;            // render replayed as one CUDA graph instead of per-tick bounces
+    bool graph_launched = false;
+    float* d_film = nullptr;       // the graph render's device film
     // render
     cav_scene* scene = nullptr;
     cav_render_opts opts{};
@@ -106,6 +117,9 @@ struct cav_server {
     std::condition_variable done_cv;  // a job finished
     bool stop = false;
     std::deque<Job*> pending;
+    std::deque<Job*> to_parse;          // scene jobs waiting for a loader thread
+    std::vector<std::thread> loaders;   // host threads parsing the scenes jobs bring
+    std::condition_variable loader_cv;
     std::unordered_map<int64_t, Job*> jobs;
     int64_t next_id = 1;
     size_t used = 0;
@@ -142,7 +156,10 @@ struct cav_server {
     }
     bool can_admit_locked(const Lane* l) const;
     void run(Lane* l);
+    void load();
     void admit_locked(Lane* l, std::vector<Job*>& started);
+    bool upload(Lane* l, Job* j);
+    void build_trees(Lane* l, std::vector<Job*>& jobs);
     bool start(Lane* l, Job* j);
     void tick(Lane* l);
     void finish(Lane* l, Job* j, cav_status st);
@@ -167,13 +184,140 @@ void cav_server::admit_locked(Lane* l, std::vector<Job*>& started) {
     }
 }
 
-bool cav_server::start(Lane* l, Job* j) {
+// Loader thread: parses the scenes that jobs bring (host work that overlaps the device work
+// of the jobs already running), sizes each job's device memory and queues it for admission.
+void cav_server::load() {
+    for (;;) {
+        Job* j = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            loader_cv.wait(lk, [&] { return stop || !to_parse.empty(); });
+            if (stop) return;  // cav_server_destroy fails what is still queued
+            j = to_parse.front();
+            to_parse.pop_front();
+        }
+        auto d = std::make_unique<cavpbrt::Scene>();
+        cav_status st = CAV_OK;
+        try {
+            *d = cavpbrt::load_file(j->path, cavpbrt::Overrides{});
+        } catch (const std::exception&) {
+            st = CAV_ERR_INVALID_ARGUMENT;
+        }
+        size_t bytes = 0;
+        if (st == CAV_OK) {
+            bytes = cav::scene_device_bytes(*d);
+            if (j->kind == kRender) {
+                const int spp = j->opts.spp > 0 ? j->opts.spp : d->spp;
+                const int64_t total = (int64_t)j->opts.width * j->opts.height * spp;
+                j->graph = cfg.graph_max_paths > 0 && total <= cfg.graph_max_paths;
+                bytes += cav::render_state_bytes(j->opts.width, j->opts.height, spp,
+                                                 j->graph ? 0 : j->opts.max_paths_in_flight);
+            } else {
+                bytes += ray_job_bytes(j->kind, j->n);
+            }
+            if (cfg.reject_over_budget && bytes > (size_t)cfg.hbm_budget_bytes) st = CAV_ERR_OUT_OF_MEMORY;
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        if (j->state == CAV_JOB_CANCELLED) continue;  // cancelled while it was parsed
+        if (st != CAV_OK) {
+            j->state = CAV_JOB_FAILED;
+            j->status = st;
+            j->t_done = now();
+            done_cv.notify_all();
+            continue;
+        }
+        j->desc = std::move(d);
+        j->bytes = bytes;
+        pending.push_back(j);
+        cv.notify_all();
+    }
+}
+
+// A scene job's scene: uploaded on the lane's stream (stream-ordered allocations and copies).
+bool cav_server::upload(Lane* l, Job* j) {
     j->t_start = now();
+    cav_scene* sc = nullptr;
+    cav_status st = cav::scene_upload(ctx, std::move(*j->desc), l->stream, true, &sc);
+    j->desc.reset();
+    if (st != CAV_OK) {
+        finish(l, j, st);
+        return false;
+    }
+    j->scene = sc;
+    if (j->rounds < 0) {  // the reference's default (Core/Scene.cu:141-146)
+        const int spp = j->kind == kRender && j->opts.spp > 0 ? j->opts.spp : cav::scene_spp(sc);
+        j->rounds = spp >= 64 ? 10 : 3;
+    }
+    return true;
+}
+
+// The trees of the scenes admitted together: one batched build (one launch per LBVH stage
+// over all of them) per treelet-round count.  Jobs whose build fails are finished here.
+void cav_server::build_trees(Lane* l, std::vector<Job*>& js) {
+    std::vector<Job*> ok;
+    std::vector<int> rounds_seen;
+    for (Job* j : js)
+        if (std::find(rounds_seen.begin(), rounds_seen.end(), j->rounds) == rounds_seen.end())
+            rounds_seen.push_back(j->rounds);
+    for (int rounds : rounds_seen) {
+        std::vector<Job*> g;
+        for (Job* j : js)
+            if (j->rounds == rounds) g.push_back(j);
+        const int K = (int)g.size();
+        std::vector<const float*> pos(K);
+        std::vector<const int32_t*> idx(K), mesh(K);
+        std::vector<int64_t> nv(K), nt(K);
+        std::vector<cav_bvh*> out(K, nullptr);
+        for (int k = 0; k < K; ++k) cav::scene_geometry(g[k]->scene, &pos[k], &nv[k], &idx[k], &mesh[k], &nt[k]);
+        const cav_status st =
+            K == 1 ? cav::build_bvh(ctx, pos[0], nv[0], idx[0], mesh[0], nt[0], nullptr, rounds, l->stream, &out[0])
+                   : cav::build_bvh_batch(ctx, K, pos.data(), nv.data(), idx.data(), mesh.data(), nt.data(), nullptr,
+                                          rounds, l->stream, out.data());
+        for (int k = 0; k < K; ++k) {
+            if (st == CAV_OK) {
+                cav::scene_set_bvh(g[k]->scene, out[k], rounds);
+                ok.push_back(g[k]);
+            } else {
+                finish(l, g[k], st);
+            }
+        }
+    }
+    js.swap(ok);
+}
+
+bool cav_server::start(Lane* l, Job* j) {
+    if (!j->owns_scene) j->t_start = now();
     cav_status st = CAV_OK;
     const cudaStream_t stream = l->stream;
+    if (j->owns_scene && j->kind != kRender) j->bvh = cav_scene_bvh(j->scene);
     const cav_bvh* tree = j->kind == kRender ? cav_scene_bvh(j->scene) : j->bvh;
     if (trace_flags() == CAV_TRACE_FAST) st = cav::ensure_wide(ctx, tree, stream);  // once per tree
     if (st != CAV_OK) {
+        finish(l, j, st);
+        return false;
+    }
+    if (j->graph) {
+        // a small render: its whole bounce chain replayed as one CUDA graph on the lane's
+        // stream (no per-bounce host round trip); the copies to pageable host memory return
+        // once the film is on the host, so the job ends here
+        const int64_t px = (int64_t)j->opts.width * j->opts.height;
+        cav_render_opts o = j->opts;
+        if (trace_flags() == CAV_TRACE_FAST) o.flags |= CAV_RENDER_FAST_TRACE;
+        if (cav::dev_alloc(ctx, (void**)&j->d_film, sizeof(float) * 4 * px, stream, true) != cudaSuccess) {
+            cudaGetLastError();
+            finish(l, j, CAV_ERR_OUT_OF_MEMORY);
+            return false;
+        }
+        cudaMemsetAsync(j->d_film, 0, sizeof(float) * 4 * px, stream);
+        st = cav::render_path_graph(ctx, j->scene, &o, j->d_film, j->d_film + 3 * px, stream);
+        if (st == CAV_OK) {
+            cudaError_t e = cudaMemcpyAsync(j->host_sum, j->d_film, sizeof(float) * 3 * px, cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(j->host_weight, j->d_film + 3 * px, sizeof(float) * px, cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) st = cav::cuda_error(ctx, e, "graph render job");
+        }
+        ++j->bounces;
         finish(l, j, st);
         return false;
     }
@@ -231,6 +375,16 @@ void cav_server::finish(Lane* l, Job* j, cav_status st) {
         cudaFreeAsync(j->dbuf, l->stream);
         j->dbuf = nullptr;
     }
+    if (j->d_film) {
+        cudaFreeAsync(j->d_film, l->stream);
+        j->d_film = nullptr;
+    }
+    if (j->owns_scene && j->scene) {  // the scene (and its tree) the job brought
+        cav::scene_release(j->scene, l->stream, true);
+        j->scene = nullptr;
+        j->bvh = nullptr;
+    }
+    j->desc.reset();
     std::lock_guard<std::mutex> lk(mu);
     used -= j->bytes;
     j->status = st;
@@ -422,7 +576,15 @@ void cav_server::run(Lane* l) {
             }
             if (!stop) admit_locked(l, started);
         }
-        for (Job* j : started)
+        // jobs that bring a scene: upload each, then build all their trees together
+        std::vector<Job*> owned, ready;
+        for (Job* j : started) {
+            if (!j->owns_scene) ready.push_back(j);
+            else if (upload(l, j)) owned.push_back(j);
+        }
+        if (!owned.empty()) build_trees(l, owned);
+        ready.insert(ready.end(), owned.begin(), owned.end());
+        for (Job* j : ready)
             if (start(l, j)) {
                 std::lock_guard<std::mutex> lk(mu);
                 l->live.push_back(j);
@@ -452,6 +614,10 @@ cav_status cav_server_create(cav_ctx* ctx, const cav_server_config* cfg, cav_ser
         sv->cfg.trace_flags = cfg->trace_flags;
         sv->cfg.reject_over_budget = cfg->reject_over_budget;
     }
+    sv->cfg.loaders = cfg && cfg->loaders > 0 ? std::min(cfg->loaders, 64) : 4;
+    sv->cfg.graph_max_paths = !cfg || cfg->graph_max_paths == 0 ? (int64_t)1 << 18
+                              : cfg->graph_max_paths < 0   ? 0
+                                                           : cfg->graph_max_paths;
     sv->cfg.min_paths_per_slice = cfg && cfg->min_paths_per_slice > 0 ? cfg->min_paths_per_slice : (int64_t)1 << 22;
     int nl = cfg && cfg->lanes > 0 ? std::min(cfg->lanes, 8) : 1;
     if (sv->cfg.mode == CAV_SERVE_SEQUENTIAL) nl = 1;
@@ -475,6 +641,7 @@ cav_status cav_server_create(cav_ctx* ctx, const cav_server_config* cfg, cav_ser
     }
     sv->t0 = Clock::now();
     for (Lane* l : sv->lanes) l->worker = std::thread([sv, l] { sv->run(l); });
+    for (int k = 0; k < sv->cfg.loaders; ++k) sv->loaders.emplace_back([sv] { sv->load(); });
     *out = sv;
     return CAV_OK;
 }
@@ -486,8 +653,23 @@ cav_status cav_server_destroy(cav_server* sv) {
         sv->stop = true;
     }
     sv->cv.notify_all();
+    sv->loader_cv.notify_all();
     for (Lane* l : sv->lanes)
         if (l->worker.joinable()) l->worker.join();
+    for (std::thread& t : sv->loaders)
+        if (t.joinable()) t.join();
+    {  // jobs still being parsed or queued when the server stopped never ran
+        std::lock_guard<std::mutex> lk(sv->mu);
+        for (auto& kv : sv->jobs) {
+            Job* j = kv.second;
+            if (j->state == CAV_JOB_PENDING) {
+                j->state = CAV_JOB_FAILED;
+                j->status = CAV_ERR_NOT_READY;
+                j->t_done = sv->now();
+            }
+        }
+        sv->done_cv.notify_all();
+    }
     for (Lane* l : sv->lanes)
         if (l->stream) cudaStreamSynchronize(l->stream);
     for (auto& kv : sv->jobs) delete kv.second;
@@ -564,6 +746,57 @@ cav_status cav_server_submit_rays(cav_server* sv, const cav_bvh* bvh, int any_hi
     return enqueue(sv, j, job_id);
 }
 
+cav_status cav_server_submit_scene(cav_server* sv, const cav_scene_job* spec, int64_t* job_id) {
+    if (!sv || !spec || !spec->pbrt_path || !job_id) return CAV_ERR_INVALID_ARGUMENT;
+    auto* j = new Job();
+    j->owns_scene = true;
+    j->path = spec->pbrt_path;
+    j->rounds = spec->bvh_rounds;
+    if (spec->kind == CAV_SCENE_RENDER) {
+        if (!spec->host_sum || !spec->host_weight || spec->render.width <= 0 || spec->render.height <= 0 ||
+            spec->render.integrator > 0) {
+            delete j;
+            return cav::set_error(sv->ctx, CAV_ERR_INVALID_ARGUMENT,
+                                  "scene render job: films, width and height are required (path integrator)");
+        }
+        j->kind = kRender;
+        j->opts = spec->render;
+        j->host_sum = spec->host_sum;
+        j->host_weight = spec->host_weight;
+        if (j->opts.max_paths_in_flight <= 0) j->opts.max_paths_in_flight = sv->cfg.max_paths_per_job;
+    } else if (spec->kind == CAV_SCENE_CLOSEST || spec->kind == CAV_SCENE_ANY) {
+        const bool any = spec->kind == CAV_SCENE_ANY;
+        if (!spec->host_rays || spec->n_rays <= 0 || (any ? !spec->host_occ : !spec->host_prim)) {
+            delete j;
+            return cav::set_error(sv->ctx, CAV_ERR_INVALID_ARGUMENT, "scene ray job: rays and outputs are required");
+        }
+        j->kind = any ? kAny : kClosest;
+        j->h_rays = spec->host_rays;
+        j->h_limit = spec->host_limit;
+        j->h_excl = spec->host_excl;
+        j->n = spec->n_rays;
+        j->h_prim = spec->host_prim;
+        j->h_t = spec->host_t;
+        j->h_uv = spec->host_uv;
+        j->h_occ = spec->host_occ;
+    } else {
+        delete j;
+        return cav::set_error(sv->ctx, CAV_ERR_INVALID_ARGUMENT, "scene job: unknown kind");
+    }
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (sv->stop) {
+        delete j;
+        return CAV_ERR_NOT_READY;
+    }
+    j->id = sv->next_id++;
+    j->t_submit = sv->now();
+    sv->jobs[j->id] = j;
+    sv->to_parse.push_back(j);
+    *job_id = j->id;
+    sv->loader_cv.notify_one();
+    return CAV_OK;
+}
+
 static void fill_status(const Job* j, cav_job_status* st) {
     st->state = j->state;
     st->status = j->status;
@@ -582,6 +815,9 @@ cav_status cav_server_cancel(cav_server* sv, int64_t job_id) {
     if (j->state == CAV_JOB_PENDING) {  // never admitted: it leaves the queue now
         auto q = std::find(sv->pending.begin(), sv->pending.end(), j);
         if (q != sv->pending.end()) sv->pending.erase(q);
+        auto r = std::find(sv->to_parse.begin(), sv->to_parse.end(), j);
+        if (r != sv->to_parse.end()) sv->to_parse.erase(r);
+        j->desc.reset();  // a loader that is parsing it drops it when done
         j->state = CAV_JOB_CANCELLED;
         j->status = CAV_ERR_CANCELLED;
         j->t_done = sv->now();

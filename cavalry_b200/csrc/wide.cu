@@ -521,8 +521,8 @@ cav_status ensure_wide(cav_ctx* ctx, const cav_bvh* bvh, cudaStream_t s) {
     need += sizeof(TriRec) * (size_t)n + 256;
     need += sizeof(int32_t) * (size_t)nw + 256;
     need += 64 + 256;
-    void* arena = nullptr;
-    if (cudaMalloc(&arena, need) != cudaSuccess) {
+    void* arena = nullptr;  // stream-ordered: complete before the view is published below
+    if (dev_alloc(ctx, &arena, need, s, true) != cudaSuccess) {
         cudaGetLastError();
         return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "fast traversal layout: device allocation failed");
     }
@@ -577,8 +577,11 @@ cav_status ensure_wide(cav_ctx* ctx, const cav_bvh* bvh, cudaStream_t s) {
     return CAV_OK;
 }
 
-void free_wide(cav_bvh* bvh) {
-    if (bvh->wide_arena) cudaFree(bvh->wide_arena);
+void free_wide(cav_bvh* bvh, cudaStream_t s, bool async) {
+    if (bvh->wide_arena) {
+        if (async) cudaFreeAsync(bvh->wide_arena, s);
+        else cudaFree(bvh->wide_arena);
+    }
     bvh->wide_arena = nullptr;
     bvh->cnodes = nullptr;
     bvh->ctris = nullptr;

@@ -342,6 +342,10 @@ typedef struct cav_server_config {
                                   smaller floors shorten ticks (latency) at some throughput */
     int reject_over_budget;    /* 1: a job whose device memory exceeds the whole budget is refused at
                                   submission (CAV_ERR_OUT_OF_MEMORY); 0: it runs when it is alone */
+    int loaders;               /* host threads parsing the scenes of cav_server_submit_scene jobs (<= 0: 4) */
+    int64_t graph_max_paths;   /* scene render jobs of at most this many paths run as one graph-replayed
+                                  render (every bounce captured, no per-bounce host round trip) instead of
+                                  joining the merged ticks (0: 262,144; < 0: never) */
 } cav_server_config;
 typedef struct cav_job_status {
     int state;         /* CAV_JOB_* */
@@ -360,6 +364,37 @@ cav_status cav_server_destroy(cav_server* server);
 /* A render (path integrator) of a loaded scene into HOST films (3 + 1 floats per pixel). */
 cav_status cav_server_submit_render(cav_server* server, cav_scene* scene, const cav_render_opts* opts,
                                     float* host_sum, float* host_weight, int64_t* job_id);
+/* A job that brings its own scene (a .pbrt file): one of the server's loader threads parses it
+ * while the GPU works on other jobs; the job is admitted when its device memory (scene, tree,
+ * path state or ray buffers) fits the HBM budget; the admitting lane uploads the scene on its
+ * stream and builds its BVH together with those of the other scenes admitted in the same
+ * round (one launch per LBVH stage, as cav_bvh_build_batch); the job runs; its scene is
+ * released when it ends.  kind CAV_SCENE_RENDER: path integrator into host_sum (3 floats per
+ * pixel) and host_weight of render.width x render.height pixels (both required; render.spp and
+ * render.max_depth <= 0 take the file's); small renders (config graph_max_paths) are replayed
+ * as one CUDA graph.  CAV_SCENE_CLOSEST / CAV_SCENE_ANY: ray queries against the scene's tree,
+ * with the arguments and semantics of cav_server_submit_rays.  bvh_rounds: treelet rounds (-1:
+ * the reference's default, 3, or 10 when the render's spp >= 64; Core/Scene.cu:141-146).
+ * A file that does not parse fails the job with CAV_ERR_INVALID_ARGUMENT.  Host buffers must
+ * stay valid until the job is done. */
+enum { CAV_SCENE_RENDER = 0, CAV_SCENE_CLOSEST = 1, CAV_SCENE_ANY = 2 };
+typedef struct cav_scene_job {
+    const char* pbrt_path;
+    int kind;
+    int bvh_rounds;
+    cav_render_opts render;
+    float* host_sum;
+    float* host_weight;
+    const cav_ray* host_rays;
+    const float* host_limit;
+    const int32_t* host_excl;
+    int64_t n_rays;
+    int32_t* host_prim;
+    float* host_t;
+    float* host_uv;
+    uint8_t* host_occ;
+} cav_scene_job;
+cav_status cav_server_submit_scene(cav_server* server, const cav_scene_job* job, int64_t* job_id);
 /* A ray-query job on HOST arrays: closest hit (prim, t, uv; t/uv may be NULL) or any hit
  * (occ; limit / excl may be NULL), with the semantics of cav_trace_closest / cav_trace_any. */
 cav_status cav_server_submit_rays(cav_server* server, const cav_bvh* bvh, int any_hit, const cav_ray* host_rays,

@@ -20,6 +20,7 @@ PAIRS = {  # C struct -> ctypes class name in cavalry_b200
     "cav_job_status": "JobStatus",
     "cav_server_stats_t": "ServerStats",
     "cav_trace_config_t": "TraceConfig",
+    "cav_scene_job": "SceneJob",
 }
 
 

@@ -256,3 +256,74 @@ def test_injected_allocation_failure_fails_only_that_job(ctx, pool):
                              max_paths_in_flight=4096)
     assert np.array_equal(fw_l, w) and np.allclose(fs_l, s, rtol=2e-5, atol=1e-6)
     sv.close()
+
+
+@pytest.mark.parametrize("flags", ["exact", "fast"])
+def test_scene_jobs_same_as_load_and_render(ctx, tmp_path, flags):
+    """Jobs that bring their own scene file: a small render (replayed as one CUDA graph), a
+    larger render (merged ticks), a closest-hit and an any-hit ray job, submitted together.
+    The server parses the files on its loader threads, builds the trees of the scenes admitted
+    together in one batched build, runs the jobs and frees the scenes; every result equals
+    loading the same file (cav_scene_load_pbrt) and rendering or tracing it alone."""
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    tf = cav.TRACE_FAST if flags == "fast" else cav.TRACE_EXACT
+    paths = []
+    for k, n in enumerate([2000, 30000, 8000, 60000]):
+        p = str(tmp_path / f"job{k}.pbrt")
+        scenes.write_pbrt(p, scenes.soup_scene(n, seed=70 + k), width=32, height=32, spp=2, max_depth=4)
+        paths.append(p)
+    rays = scenes.closest_rays(20000, seed=13)
+    srays, lim = scenes.shadow_rays(20000, seed=14)
+    sv = cav.Server(ctx, trace_flags=tf, graph_max_paths=64 * 64 * 2, lanes=1)
+    j0, fs0, fw0 = sv.submit_scene_render(paths[0], 64, 64, spp=2, max_depth=4)
+    j1, fs1, fw1 = sv.submit_scene_render(paths[1], 96, 96, spp=4, max_depth=4)
+    j2, p2, t2, _ = sv.submit_scene_rays(paths[2], rays)
+    j3, o3 = sv.submit_scene_rays(paths[3], srays, any_hit=True, limit=lim)
+    jbad, _, _ = sv.submit_scene_render(str(tmp_path / "missing.pbrt"), 16, 16)
+    for j in (j0, j1, j2, j3):
+        assert sv.wait(j, 120).state == cav.JOB_DONE
+    with pytest.raises(cav.CavError) as e:
+        sv.wait(jbad, 60)
+    assert e.value.status == 1 and sv.poll(jbad).state == cav.JOB_FAILED
+    st = sv.stats()
+    assert st.live == 0 and st.pending == 0 and st.hbm_in_use == 0
+    sv.close()
+    fast = flags == "fast"
+    for p, (w_, h_, spp), fs, fw in ((paths[0], (64, 64, 2), fs0, fw0), (paths[1], (96, 96, 4), fs1, fw1)):
+        sc = ctx.load_pbrt(p)
+        s, w, _ = sc.render(spp=spp, max_depth=4, width=w_, height=h_, integrator="path", fast_trace=fast)
+        sc.free()
+        assert np.array_equal(fw, w)
+        if fast:
+            assert np.abs(fs - s).mean() <= 1e-3 * np.abs(s).mean() + 1e-6
+        else:
+            assert np.allclose(fs, s, rtol=2e-5, atol=1e-6)
+    sc = ctx.load_pbrt(paths[2])
+    p, t, _ = sc.bvh().trace_closest(torch.from_numpy(rays).cuda(), flags=tf)
+    assert np.array_equal(p2, p.cpu().numpy()) and np.array_equal(t2.view(np.uint32), t.cpu().numpy().view(np.uint32))
+    sc.free()
+    sc = ctx.load_pbrt(paths[3])
+    o = sc.bvh().trace_any(torch.from_numpy(srays).cuda(), torch.from_numpy(lim).cuda(), flags=tf)
+    assert np.array_equal(o3, o.cpu().numpy())
+    sc.free()
+
+
+def test_scene_job_cancelled_before_it_runs(ctx, tmp_path):
+    """A scene job cancelled while it waits to be parsed or admitted never runs; the others do."""
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    p = str(tmp_path / "s.pbrt")
+    scenes.write_pbrt(p, scenes.soup_scene(20000, seed=80), width=32, height=32, spp=1, max_depth=3)
+    sv = cav.Server(ctx, max_live_jobs=1, loaders=1)
+    ids = [sv.submit_scene_render(p, 32, 32)[0] for _ in range(6)]
+    sv.cancel(ids[-1])
+    assert sv.wait(ids[-1], 60).state == cav.JOB_CANCELLED
+    for j in ids[:-1]:
+        assert sv.wait(j, 120).state == cav.JOB_DONE
+    assert sv.stats().hbm_in_use == 0
+    sv.close()
