@@ -62,7 +62,11 @@ def parse():
     p.add_argument("--jobs", type=int, default=256, help="jobs in the served stream (serve workload)")
     p.add_argument("--serve-trace", default="fast", choices=["fast", "exact"], help="serve workload: traversal mode")
     p.add_argument("--serve-loaders", type=int, default=8, help="serve workload: the server's scene loader threads")
+    p.add_argument("--serve-lanes", default="2",
+                   help="serve workload: the server's lanes; a comma list runs the server arm once per value "
+                        "(the first value is the bench's `value`)")
     p.add_argument("--bounce", type=int, default=1, help="capture workload: which bounce's extend rays")
+    p.add_argument("--ref-spp", type=int, default=16384, help="guided workload: spp of the reference render")
     p.add_argument("--no-reference", action="store_true", help="render workload: skip the reference's CUDA build")
     p.add_argument("--render-steps", type=int, default=1, help="timed full renders (render workload)")
     p.add_argument("--small", action="store_true", help="render workload at 1/16 size (smoke runs)")
@@ -922,9 +926,9 @@ def run_serve(args):
                 "mean_latency_ms": round(float(lat.mean()) * 1e3, 2),
                 "service_s_by_class": dict(sorted((k, round(v, 3)) for k, v in service.items()))}
 
-    def serve():
+    def serve(lanes):
         sv = cav.Server(ctx, hbm_budget_bytes=80 << 30, mode=cav.SERVE_MERGED, trace_flags=flags,
-                        loaders=args.serve_loaders)
+                        loaders=args.serve_loaders, lanes=lanes)
         ids = [None] * len(jobs)
         outs = [None] * len(jobs)
         wall0 = time.perf_counter()
@@ -1002,7 +1006,13 @@ def run_serve(args):
     sc.render(spp=1, max_depth=2, width=16, height=16, fast_trace=flags == cav.TRACE_FAST)
     sc.free()
     plain, out_p = plain_loop()
-    merged, out_m = serve()
+    lane_list = [int(x) for x in str(args.serve_lanes).split(",")]
+    sweep = {}
+    for k, lanes in enumerate(lane_list):
+        res, outs = serve(lanes)
+        sweep[f"lanes{lanes}"] = res
+        if k == 0:
+            merged, out_m = res, outs
     # each job's result alone (plain loop) against the same job in the mix (server)
     rel, ray_same = [], []
     for i, j in enumerate(jobs):
@@ -1024,8 +1034,10 @@ def run_serve(args):
                    "triangles_total": int(sum(j["tris"] for j in jobs)),
                    "triangles_range": [int(min(j["tris"] for j in jobs)), int(max(j["tris"] for j in jobs))],
                    "resolutions": resolutions, "spp": [1, 4, 16, 64], "depth": 6, "hbm_budget_gib": 80,
-                   "trace_mode": args.serve_trace, "loaders": args.serve_loaders},
+                   "trace_mode": args.serve_trace, "loaders": args.serve_loaders, "lanes": lane_list[0]},
         "server": merged, "plain_loop": plain,
+        "server_by_lanes": {k: {"jobs_per_s": v["jobs_per_s"], "p50_latency_ms": v["p50_latency_ms"],
+                                "p99_latency_ms": v["p99_latency_ms"]} for k, v in sweep.items()},
         "speedup_vs_plain_loop": round(merged["jobs_per_s"] / plain["jobs_per_s"], 3),
         "p99_latency_ratio_plain_over_server": round(plain["p99_latency_ms"] / merged["p99_latency_ms"], 3),
         "relmse_server_vs_alone": {"max": max(rel) if rel else None, "mean": float(np.mean(rel)) if rel else None,
@@ -1037,12 +1049,11 @@ def run_serve(args):
 
 # ------------------------------------------------------------------------ guided workload
 def run_guided(args):
-    """Config-5 layout (scenes.aperture_scene: a room lit only through a 0.3 x 0.3 aperture,
-    80 % plastic spheres at roughness 0.05), 640 x 360 by default (1280 x 720 is the full
-    config; --small: 256 x 192), depth 10.  relMSE against a 4096-spp plain path render of
-    the same film for plain path, rlpath (Q-table) and the MLP-guided integrator at 16-256
-    spp, with device times; relMSE at equal time is interpolated (log-log) at the guided
-    render's time for each spp."""
+    """Config 5 (scenes.aperture_scene: a room lit only through a 0.3 x 0.3 aperture, 80 %
+    plastic spheres at roughness 0.05), 1280 x 720 (--small: 256 x 192), depth 10.  relMSE
+    against a 16384-spp plain path render of the same film (`--ref-spp`) for plain path,
+    rlpath (Q-table) and the MLP-guided integrator at 16-256 spp, with device times; relMSE
+    at equal time is interpolated (log-log) at the guided render's time for each spp."""
     import tempfile
 
     import cavalry_b200 as cav
@@ -1050,13 +1061,13 @@ def run_guided(args):
 
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    W, H = (256, 192) if args.small else (640, 360)
+    W, H = (256, 192) if args.small else (1280, 720)
     tmp = tempfile.mkdtemp()
     path = os.path.join(tmp, "aperture.pbrt")
     scenes.write_pbrt(path, scenes.aperture_scene(), width=W, height=H, spp=4, max_depth=10)
     ctx = cav.Context(0)
     sc = ctx.load_pbrt(path, bvh_rounds=3)
-    s, w, ref_ms = sc.render(spp=4096, integrator="path")
+    s, w, ref_ms = sc.render(spp=args.ref_spp, integrator="path", fast_trace=True)
     ref = s / w[..., None]
 
     def relmse(x):
@@ -1082,11 +1093,13 @@ def run_guided(args):
     equal_time = [{"spp_guided": g[0], "ms": round(g[1], 2), "guided": round(g[2], 6),
                    "path": round(at_time(rows["path"], g[1]), 6), "rlpath": round(at_time(rows["rlpath"], g[1]), 6)}
                   for g in rows["guided"]]
-    out = {"metric": "relMSE at equal spp and equal time vs a 4096-spp path render", "unit": "relMSE",
+    out = {"metric": f"relMSE at equal spp and equal time vs a {args.ref_spp}-spp path render", "unit": "relMSE",
            "higher_is_better": False, "n_gpus": 1, "dtype": "f32 (network bf16, fp32 accumulate)",
            "data": "synthetic (seeded aperture scene written as .pbrt)",
            "config": {"workload": f"aperture_{W}x{H}_depth10", "triangles": int(sc.info().triangles),
-                      "reference_spp": 4096, "reference_ms": round(ref_ms, 1)},
+                      "reference_spp": args.ref_spp, "reference_ms": round(ref_ms, 1),
+                      "reference_trace": "fast (same hit distances; an equal-distance tie may pick another "
+                                         "triangle)"},
            "equal_spp": {k: [{"spp": r[0], "ms": round(r[1], 2), "relmse": round(r[2], 6)} for r in v]
                          for k, v in rows.items()},
            "equal_time": equal_time}

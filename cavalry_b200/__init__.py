@@ -117,6 +117,7 @@ def lib() -> ctypes.CDLL:
                                      ctypes.c_int], ctypes.c_int),
         "cav_trace_autotune_flags": ([P, P, P, ctypes.c_int64, ctypes.c_int, P, P, U32, P, P], ctypes.c_int),
         "cav_load_texture_png": ([ctypes.c_char_p, P, ctypes.c_int64, P, P, P, ctypes.c_int], ctypes.c_int),
+        "cav_load_texture_exr": ([ctypes.c_char_p, P, ctypes.c_int64, P, P, P, ctypes.c_int], ctypes.c_int),
         "cav_server_create": ([P, P, ctypes.POINTER(P)], ctypes.c_int),
         "cav_server_destroy": ([P], ctypes.c_int),
         "cav_server_submit_render": ([P, P, P, P, P, P], ctypes.c_int),
@@ -273,6 +274,24 @@ def parse_pbrt(path: str, spp: int = -1, integrator: str | None = None) -> tuple
     if st != 0:
         raise CavError(st, "cav_pbrt_parse_info: " + err.value.decode(errors="replace"))
     return info, c2w.reshape(4, 4).T
+
+
+def load_texture_exr(path: str) -> np.ndarray:
+    """Host-only: an OpenEXR texture as scene loading decodes it, [H, W, 4] float32 RGBA with
+    rows in the file's order (no flip, no gamma) (no GPU)."""
+    w, h = ctypes.c_int(), ctypes.c_int()
+    err = ctypes.create_string_buffer(512)
+    L = lib()
+    st = L.cav_load_texture_exr(path.encode(), None, 0, ctypes.byref(w), ctypes.byref(h), ctypes.addressof(err),
+                                len(err))
+    if st != 0:
+        raise CavError(st, "cav_load_texture_exr: " + err.value.decode(errors="replace"))
+    out = np.zeros((h.value, w.value, 4), np.float32)
+    st = L.cav_load_texture_exr(path.encode(), out.ctypes.data, out.size, ctypes.byref(w), ctypes.byref(h),
+                                ctypes.addressof(err), len(err))
+    if st != 0:
+        raise CavError(st, "cav_load_texture_exr: " + err.value.decode(errors="replace"))
+    return out
 
 
 def load_texture_png(path: str) -> np.ndarray:

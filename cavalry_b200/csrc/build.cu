@@ -768,7 +768,7 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     uint32_t* vals_b = carve<uint32_t>(q, n);
     uint32_t* hist = carve<uint32_t>(q, 8 * 256);
     uint32_t* status = carve<uint32_t>(q, 8 * (size_t)tiles * 256);
-    uint32_t* counters = carve<uint32_t>(q, 16);  // [0..7] tile counters, [8..13] bounds ords
+    uint32_t* counters = carve<uint32_t>(q, 16);  // [0..7] tile counters, [8..13] bounds ords, [14..15] treelets
     int32_t* err = carve<int32_t>(q, 8);
     float* dbounds = carve<float>(q, 8);
     uint32_t* visited = carve<uint32_t>(q, count);
@@ -827,7 +827,7 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     CAV_CUDA(ctx, cudaMemcpyAsync(bvh->perm, vals_a, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
     CAV_CUDA(ctx, cudaGetLastError());
 
-    cav_status st = treelet_rounds(ctx, bvh->nodes, n, rounds, leaf_list, visited, s);
+    cav_status st = treelet_rounds(ctx, bvh->nodes, n, rounds, leaf_list, visited, counters + 14, s);
     if (st != CAV_OK) return st;
     cudaEventRecord(bvh->ev[5], s);
 
@@ -1081,7 +1081,7 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     acc(sizeof(int32_t) * 8);                       // error flag
     acc(sizeof(uint32_t) * std::max<int64_t>(total_int, 2 * total - K));  // visited (refit, then treelets)
     acc(sizeof(int32_t) * total);                   // leaf lists of all trees
-    acc(sizeof(uint32_t) * K);                      // leaf-list counters
+    acc(sizeof(uint32_t) * (K + 2));                // leaf-list counters + treelet claim counters
     acc(sizeof(TreeletSeg) * K);                    // treelet table
     acc(sizeof(int32_t) * cmax);                    // compact index
     acc(sizeof(int32_t) * nmax);                    // slot_of
@@ -1109,7 +1109,7 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     int32_t* err = carve<int32_t>(q, 8);
     uint32_t* visited = carve<uint32_t>(q, std::max<int64_t>(total_int, 2 * total - K));
     int32_t* leaf_list = carve<int32_t>(q, total);
-    uint32_t* leaf_ctr = carve<uint32_t>(q, K);
+    uint32_t* leaf_ctr = carve<uint32_t>(q, K + 2);
     TreeletSeg* tsegs = carve<TreeletSeg>(q, K);
     int32_t* compact = carve<int32_t>(q, cmax);
     int32_t* slot_of = carve<int32_t>(q, nmax);

@@ -200,8 +200,9 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
                      const int32_t* mesh_ids, int64_t n, const float* bounds, int rounds, cudaStream_t s,
                      cav_bvh** out);
 // treelet.cu
+// counters: device words of the caller's scratch ([0]: leaf-list positions)
 cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int32_t* leaf_list, uint32_t* visited,
-                          cudaStream_t s);
+                          uint32_t* counters, cudaStream_t s);
 struct TreeletSeg {  // one tree of a batched treelet pass
     BNode* nodes;
     int64_t n;  // leaves (triangles)
@@ -269,8 +270,9 @@ void scene_geometry(const cav_scene* sc, const float** pos, int64_t* nv, const i
                     int64_t* nt);
 void scene_set_bvh(cav_scene* sc, cav_bvh* bvh, int rounds);
 int scene_spp(const cav_scene* sc);
+// counters: two device words for the traversals' work counters (null: the context's)
 cav_status render_path_graph(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
-                             cudaStream_t s);
+                             cudaStream_t s, unsigned long long* counters = nullptr);
 
 // Many scenes' BVHs, one launch per LBVH stage across all of them (build.cu)
 cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, const int64_t* num_vertices,

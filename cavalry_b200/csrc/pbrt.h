@@ -56,13 +56,20 @@ struct Material {
     int kd_texture = -1;             // matte / plastic / substrate "texture Kd": index into Scene::textures
 };
 
-// An 8-bit RGBA image texture as the reference holds it (Core/Texture.h: uchar4 texels,
-// bilinear filtering, wrapped normalized coordinates), rows bottom-up after the load flip.
+// An image texture as the reference holds it (Core/Texture.h): 8-bit RGBA texels read as
+// normalized floats, rows bottom-up after stb_image's load flip (PNG), or FLOAT RGBA texels
+// read as they are, rows in the file's order (OpenEXR through tinyexr's LoadEXR, no flip);
+// bilinear filtering, wrapped normalized coordinates either way.
 struct TextureImage {
     int width = 1, height = 1;
-    std::vector<unsigned char> rgba{0, 0, 0, 0};
+    std::vector<unsigned char> rgba{0, 0, 0, 0};  // 8-bit texels (is_float false)
+    bool is_float = false;
+    std::vector<float> rgbaf;                     // float texels (is_float true)
 };
 TextureImage load_texture_image(const std::string& path);
+// OpenEXR (scanline, single part; NONE, RLE, ZIPS and ZIP compression; HALF and FLOAT
+// channels) to RGBA floats as tinyexr's LoadEXR returns them.
+TextureImage load_exr(const std::string& path);
 
 struct Mesh {
     std::vector<float> positions;  // world space (transform applied), 3 per vertex

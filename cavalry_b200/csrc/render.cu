@@ -261,7 +261,7 @@ size_t scene_device_bytes(const cavpbrt::Scene& D) {
         nrm += m.normals.size() / 3;
     }
     size_t b = 12 * v + 16 * t + (nrm ? 12 * v : 0) + (uv ? 8 * v : 0) + 4096 * 4;
-    for (const auto& tx : D.textures) b += (size_t)4 * tx.width * tx.height;
+    for (const auto& tx : D.textures) b += (size_t)(tx.is_float ? 16 : 4) * tx.width * tx.height;
     b += bvh_arena_bytes((int64_t)std::max<size_t>(t, 2)) + 96 * t;  // tree + build scratch
     return b;
 }
@@ -381,9 +381,10 @@ cav_status scene_upload(cav_ctx* ctx, cavpbrt::Scene&& desc, cudaStream_t stream
         return st;
     }
     // image textures as the reference creates them (Core/Texture.h allocate): uchar4 texels
-    // read as normalized floats, bilinear filtering, wrapped normalized coordinates
+    // read as normalized floats (8-bit images) or float4 texels read as they are (OpenEXR),
+    // bilinear filtering, wrapped normalized coordinates
     for (const auto& t : D.textures) {
-        cudaChannelFormatDesc fmt = cudaCreateChannelDesc<uchar4>();
+        cudaChannelFormatDesc fmt = t.is_float ? cudaCreateChannelDesc<float4>() : cudaCreateChannelDesc<uchar4>();
         cudaArray_t arr = nullptr;
         if (cudaMallocArray(&arr, &fmt, t.width, t.height) != cudaSuccess) {
             cudaGetLastError();
@@ -391,8 +392,9 @@ cav_status scene_upload(cav_ctx* ctx, cavpbrt::Scene&& desc, cudaStream_t stream
             return set_error(ctx, CAV_ERR_OUT_OF_MEMORY, "texture allocation failed");
         }
         sc->tex_arrays.push_back(arr);
-        cudaMemcpy2DToArray(arr, 0, 0, t.rgba.data(), (size_t)4 * t.width, (size_t)4 * t.width, t.height,
-                            cudaMemcpyHostToDevice);
+        const size_t texel = t.is_float ? sizeof(float4) : 4;
+        cudaMemcpy2DToArray(arr, 0, 0, t.is_float ? (const void*)t.rgbaf.data() : (const void*)t.rgba.data(),
+                            texel * t.width, texel * t.width, t.height, cudaMemcpyHostToDevice);
         cudaResourceDesc res{};
         res.resType = cudaResourceTypeArray;
         res.res.array.array = arr;
@@ -400,7 +402,7 @@ cav_status scene_upload(cav_ctx* ctx, cavpbrt::Scene&& desc, cudaStream_t stream
         td.addressMode[0] = cudaAddressModeWrap;
         td.addressMode[1] = cudaAddressModeWrap;
         td.filterMode = cudaFilterModeLinear;
-        td.readMode = cudaReadModeNormalizedFloat;
+        td.readMode = t.is_float ? cudaReadModeElementType : cudaReadModeNormalizedFloat;
         td.normalizedCoords = 1;
         cudaTextureObject_t obj = 0;
         if (cudaCreateTextureObject(&obj, &res, &td, nullptr) != cudaSuccess) {
@@ -638,7 +640,9 @@ __global__ void k_chunk_end(int32_t* idx, const uint32_t* cnt, int max_depth, un
 }  // namespace
 
 cav_status render_path_graph(cav_ctx* ctx, cav_scene* sc, const cav_render_opts* opts, float* d_sum, float* d_wsum,
-                             cudaStream_t s) {
+                             cudaStream_t s, unsigned long long* counters) {
+    // the traversals' work counters: the caller's (two words), else the context's
+    if (!counters) counters = ctx->d_counters + 6;
     const cavpbrt::Scene& D = sc->desc;
     int W, H;
     film_size(sc, opts, W, H);
@@ -736,15 +740,15 @@ cav_status render_path_graph(cav_ctx* ctx, cav_scene* sc, const cav_render_opts*
             const uint32_t* n_dev = depth == 0 ? cnt + 2 * max_depth : cnt + 2 * (depth - 1);
             Q.counters = cnt + 2 * depth;
             st = fast ? trace_wide_closest(ctx, sc->bvh, Q.rays, INT64_MAX, n_dev, Q.hit_prim, Q.hit_t, Q.hit_uv, s,
-                                           ctx->d_counters + 6)
+                                           counters)
                       : trace_closest_dev(ctx, sc->bvh, Q.rays, n_dev, Q.hit_prim, Q.hit_t, Q.hit_uv, s,
-                                          ctx->d_counters + 6);
+                                          counters);
             if (st != CAV_OK) break;
             k_shade<<<blocks, kThreads, 0, s>>>(S, depth, dim0, 0, P, Q, n_dev);
             st = fast ? trace_wide_any(ctx, sc->bvh, Q.shadow_rays, Q.shadow_limit, Q.shadow_excl, INT64_MAX,
-                                       cnt + 2 * depth + 1, Q.shadow_occ, s, ctx->d_counters + 7)
+                                       cnt + 2 * depth + 1, Q.shadow_occ, s, counters + 1)
                       : trace_any_dev(ctx, sc->bvh, Q.shadow_rays, Q.shadow_limit, Q.shadow_excl, cnt + 2 * depth + 1,
-                                      Q.shadow_occ, s, ctx->d_counters + 7);
+                                      Q.shadow_occ, s, counters + 1);
             if (st != CAV_OK) break;
             k_add_direct<<<blocks, kThreads, 0, s>>>(0, P, Q, cnt + 2 * depth + 1);
             std::swap(Q.active, Q.next_active);

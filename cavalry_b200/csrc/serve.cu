@@ -309,7 +309,7 @@ bool cav_server::start(Lane* l, Job* j) {
             return false;
         }
         cudaMemsetAsync(j->d_film, 0, sizeof(float) * 4 * px, stream);
-        st = cav::render_path_graph(ctx, j->scene, &o, j->d_film, j->d_film + 3 * px, stream);
+        st = cav::render_path_graph(ctx, j->scene, &o, j->d_film, j->d_film + 3 * px, stream, l->d_counter + 2);
         if (st == CAV_OK) {
             cudaError_t e = cudaMemcpyAsync(j->host_sum, j->d_film, sizeof(float) * 3 * px, cudaMemcpyDeviceToHost, stream);
             if (e == cudaSuccess)

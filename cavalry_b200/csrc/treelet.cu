@@ -478,10 +478,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 32)
 }  // namespace
 
 cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int32_t* leaf_list, uint32_t* visited,
-                          cudaStream_t s) {
+                          uint32_t* counter, cudaStream_t s) {
     if (rounds <= 0) return CAV_OK;
     const int64_t count = 2 * n - 1;
-    uint32_t* counter = reinterpret_cast<uint32_t*>(ctx->d_counters + 20);  // ctx counter slot 20
+    // counter: the leaf list's positions, in the build's own scratch (builds on different
+    // streams, such as a server's lanes, never share it)
     for (int r = 0; r < rounds; ++r) {
         CAV_CUDA(ctx, cudaMemsetAsync(visited, 0, sizeof(uint32_t) * count, s));
         CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), s));
@@ -500,7 +501,8 @@ cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int
 // 0.5-2M triangles, and launch overhead does not matter there).  Each tree's result is the
 // single-tree one: within a tree the walk is the same, and trees share no nodes.  segs /
 // leaf_off: device tables (K trees, K + 1 leaf offsets), segs_host / leaf_off_host the same
-// on the host; leaf_list holds leaf_off[K] entries, visited 2 leaf_off[K] - K, counters K.
+// on the host; leaf_list holds leaf_off[K] entries, visited 2 leaf_off[K] - K, counters K + 1
+// (per tree leaf-list positions, then one for a tree that runs the single-tree pass).
 cav_status treelet_rounds_batch(cav_ctx* ctx, const TreeletSeg* segs, const TreeletSeg* segs_host,
                                 const int64_t* leaf_off, const int64_t* leaf_off_host, int K, int rounds,
                                 int32_t* leaf_list, uint32_t* counters, uint32_t* visited, cudaStream_t s) {
@@ -514,7 +516,7 @@ cav_status treelet_rounds_batch(cav_ctx* ctx, const TreeletSeg* segs, const Tree
         const int64_t nodes = node_off_h(k1) - node_off_h(k0);
         if (k1 == k0 + 1 && leaves >= kGroupLeaves / 2) {
             cav_status st = treelet_rounds(ctx, segs_host[k0].nodes, segs_host[k0].n, rounds,
-                                           leaf_list + leaf_off_host[k0], visited + node_off_h(k0), s);
+                                           leaf_list + leaf_off_host[k0], visited + node_off_h(k0), counters + K, s);
             if (st != CAV_OK) return st;
             k0 = k1;
             continue;

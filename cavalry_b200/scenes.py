@@ -205,15 +205,24 @@ def write_pbrt(path, room: dict, *, width=256, height=256, spp=16, max_depth=5, 
     here = os.path.dirname(os.path.abspath(str(path)))
     stem = os.path.splitext(os.path.basename(str(path)))[0]
     env = room.get("environment")
+
+    def image_file(name, img):  # 8-bit arrays as PNG, float arrays as OpenEXR (ZIP)
+        if np.asarray(img).dtype.kind == "f":
+            fn = f"{stem}_{name}.exr"
+            write_exr(os.path.join(here, fn), img, compression=room.get("exr_compression", "zip"))
+        else:
+            fn = f"{stem}_{name}.png"
+            write_png(os.path.join(here, fn), img)
+        return fn
+
     if env is not None:  # first, so it is light 0
         line = f'LightSource "infinite" "rgb L" [{_nums(env["L"])}]'
         if env.get("map") is not None:
-            write_png(os.path.join(here, f"{stem}_env.png"), env["map"])
-            line += f' "string mapname" "{stem}_env.png"'
+            line += f' "string mapname" "{image_file("env", env["map"])}"'
         lines.append(line)
     for t in room.get("textures", []):
-        write_png(os.path.join(here, f"{stem}_{t['name']}.png"), t["rgba"])
-        lines.append(f'Texture "{t["name"]}" "spectrum" "imagemap" "string filename" "{stem}_{t["name"]}.png"')
+        fn = image_file(t["name"], t["rgba"])
+        lines.append(f'Texture "{t["name"]}" "spectrum" "imagemap" "string filename" "{fn}"')
     uvs = room.get("uvs")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
@@ -285,7 +294,91 @@ def write_png(path, rgba) -> None:
                 + chunk(b"IDAT", zlib.compress(raw, 6)) + chunk(b"IEND", b""))
 
 
-def courtyard_scene(seed: int = 41, area_light: bool = False):
+EXR_COMPRESSION = {"none": 0, "rle": 1, "zips": 2, "zip": 3}
+
+
+def _exr_pack(raw: bytes) -> bytes:
+    """The OpenEXR ZIP/RLE pre-pass: bytes split into even and odd halves, then each byte
+    stored as its difference to the previous one plus 128."""
+    a = np.frombuffer(raw, np.uint8)
+    t = np.concatenate([a[0::2], a[1::2]]).astype(np.int16)
+    d = t.copy()
+    d[1:] = (t[1:] - t[:-1] + 128) & 255
+    return d.astype(np.uint8).tobytes()
+
+
+def _exr_rle(data: bytes) -> bytes:
+    out = bytearray()
+    i, n = 0, len(data)
+    while i < n:
+        j = i
+        while j + 1 < n and data[j + 1] == data[i] and j - i < 127:
+            j += 1
+        if j - i >= 2:  # a run of 3..128 equal bytes
+            out += bytes([j - i]) + data[i:i + 1]
+            i = j + 1
+        else:  # literals up to the next run of 3 (at most 127)
+            k = i
+            while k < n and k - i < 127 and not (k + 2 < n and data[k] == data[k + 1] == data[k + 2]):
+                k += 1
+            out += bytes([(256 - (k - i)) & 255]) + data[i:k]
+            i = k
+    return bytes(out)
+
+
+def write_exr(path, img, compression: str = "zip", channels: list[str] | None = None) -> None:
+    """A single-part scanline OpenEXR file of an [H, W, C] (or [H, W]) float array, top row first
+    (data window from (0, 0)): float16 arrays as HALF channels, float32 as FLOAT.  C = 1, 3 or
+    4 with default names Y / R G B / R G B A; channels are stored in name order, as the format
+    requires.  compression: "none", "rle", "zips" (one line per block) or "zip" (16 lines)."""
+    import struct
+    import zlib
+
+    a = np.asarray(img)
+    if a.ndim == 2:
+        a = a[..., None]
+    h, w, c = a.shape
+    names = channels or {1: ["Y"], 3: ["R", "G", "B"], 4: ["R", "G", "B", "A"]}[c]
+    half = a.dtype == np.float16
+    a = a.astype(np.float16 if half else np.float32)
+    order = sorted(range(c), key=lambda k: names[k])
+    ptype = 1 if half else 2
+
+    def attr(name, typ, value):
+        return name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(value)) + value
+
+    chl = b"".join(names[k].encode() + b"\0" + struct.pack("<iB3xii", ptype, 0, 1, 1) for k in order) + b"\0"
+    head = struct.pack("<ii", 20000630, 2)
+    head += attr("channels", "chlist", chl)
+    head += attr("compression", "compression", bytes([EXR_COMPRESSION[compression]]))
+    head += attr("dataWindow", "box2i", struct.pack("<iiii", 0, 0, w - 1, h - 1))
+    head += attr("displayWindow", "box2i", struct.pack("<iiii", 0, 0, w - 1, h - 1))
+    head += attr("lineOrder", "lineOrder", b"\0")
+    head += attr("pixelAspectRatio", "float", struct.pack("<f", 1.0))
+    head += attr("screenWindowCenter", "v2f", struct.pack("<ff", 0.0, 0.0))
+    head += attr("screenWindowWidth", "float", struct.pack("<f", 1.0)) + b"\0"
+    lines = 16 if compression == "zip" else 1
+    blocks = []
+    for y0 in range(0, h, lines):
+        raw = b"".join(a[y, :, k].tobytes() for y in range(y0, min(y0 + lines, h)) for k in order)
+        if compression in ("zip", "zips"):
+            packed = zlib.compress(_exr_pack(raw), 6)
+        elif compression == "rle":
+            packed = _exr_rle(_exr_pack(raw))
+        else:
+            packed = raw
+        if len(packed) >= len(raw):  # stored as is when the codec does not pay
+            packed = raw
+        blocks.append(struct.pack("<ii", y0, len(packed)) + packed)
+    offsets, off = [], len(head) + 8 * len(blocks)
+    for b in blocks:
+        offsets.append(off)
+        off += len(b)
+    with open(path, "wb") as f:
+        f.write(head + struct.pack(f"<{len(offsets)}Q", *offsets) + b"".join(blocks))
+
+
+def courtyard_scene(seed: int = 41, area_light: bool = False, hdr_sky: bool = False):
     """An open-topped courtyard under an environment map: a floor with a tiled checker
     texture ("texture Kd" on matte, uv 0..4), two walls, a textured plastic box, and sphere
     shapes of assorted materials; the environment ("infinite", a sky gradient with a bright
@@ -349,6 +442,13 @@ def courtyard_scene(seed: int = 41, area_light: bool = False):
     sky[..., 2] = (200 + 40 * t).astype(np.uint8)
     sky[10:14, 20:26, :3] = (255, 240, 200)
     sky[..., 3] = 255
+    if hdr_sky:  # the same sky as an HDR map (HALF floats, written as OpenEXR), the sun 6x brighter
+        hdr = np.zeros((H_, W_, 3), np.float32)
+        hdr[..., 0] = 0.3 + 0.5 * t
+        hdr[..., 1] = 0.45 + 0.4 * t
+        hdr[..., 2] = 0.8 + 0.15 * t
+        hdr[10:14, 20:26] = (6.0, 5.6, 4.7)
+        sky = hdr.astype(np.float16)
     return {
         "positions": np.ascontiguousarray(np.concatenate(verts)),
         "normals": np.ascontiguousarray(np.concatenate(nrms)),

@@ -273,6 +273,16 @@ cav_status cav_pbrt_parse_info(const char* path, int spp_override, const char* i
  * are returned; otherwise capacity_bytes must hold 4 * width * height bytes. */
 cav_status cav_load_texture_png(const char* path, uint8_t* rgba, int64_t capacity_bytes, int* width, int* height,
                                 char* err, int err_len);
+/* Host-only: decode an OpenEXR texture exactly as scene loading does for a file name ending in
+ * "exr" (Core/Texture.cu:34-57, tinyexr's LoadEXR): RGBA floats, rows in the file's order (no
+ * flip, no gamma); R, G, B and A looked up among the first four channels (layer prefixes
+ * dropped), a missing A reads 1, a single channel fills all four.  Scanline images with NONE,
+ * RLE, ZIPS or ZIP compression and HALF or FLOAT channels; tiled and multi-part files, UINT
+ * channels and the PIZ / PXR24 / B44 / DWA codecs are refused (CAV_ERR_INVALID_ARGUMENT, the
+ * reason in err).  With rgba null only width and height are returned; otherwise
+ * capacity_floats must hold 4 * width * height floats. */
+cav_status cav_load_texture_exr(const char* path, float* rgba, int64_t capacity_floats, int* width, int* height,
+                                char* err, int err_len);
 cav_status cav_pbrt_load_triangles(const char* path, float* positions, int64_t max_vertices, int32_t* indices,
                                    int32_t* mesh_ids, int64_t max_triangles, int64_t* num_vertices,
                                    int64_t* num_triangles, char* err, int err_len);

@@ -77,7 +77,8 @@ typedef struct {
 } OLight;
 typedef struct {
     int32_t width, height;
-    const uint8_t* rgba; /* rows bottom-up (after the load flip), before the inverse gamma */
+    const uint8_t* rgba; /* 8-bit images: rows bottom-up (after the load flip), before the inverse gamma */
+    const float* rgbaf;  /* OpenEXR images (when not NULL): RGBA floats, rows as stored (no flip, no gamma) */
 } OTexture;
 
 enum { M_MATTE = 0, M_MIRROR = 1, M_SUBSTRATE = 2, M_METAL = 3, M_GLASS = 4, M_PLASTIC = 5 };
@@ -583,10 +584,11 @@ void orc_load_gamma_table(uint8_t* out) {
     for (int c = 0; c < 256; ++c) out[c] = load_gamma((uint8_t)c);
 }
 
-/* tex2D of a uchar4 texture read as normalized floats with bilinear filtering and wrapped
- * normalized coordinates, restated from the CUDA programming guide's description of
- * texture fetching: x = frac(u) * W - 0.5, texels i = floor(x) and i + 1 (wrapped), weight
- * frac(x) held with 8 fractional bits; the same in y. */
+/* tex2D of a uchar4 texture read as normalized floats (or of a float4 texture read as it
+ * is) with bilinear filtering and wrapped normalized coordinates, restated from the CUDA
+ * programming guide's description of texture fetching: x = frac(u) * W - 0.5, texels
+ * i = floor(x) and i + 1 (wrapped), weight frac(x) held with 8 fractional bits; the same
+ * in y. */
 static V3 tex_read(const OTexture* t, float u, float v) {
     float xs = (u - floorf(u)) * t->width - 0.5f, ys = (v - floorf(v)) * t->height - 0.5f;
     float fx = floorf(xs), fy = floorf(ys);
@@ -597,9 +599,14 @@ static V3 tex_read(const OTexture* t, float u, float v) {
         for (int di = 0; di < 2; ++di) {
             int i = ((i0 + di) % t->width + t->width) % t->width;
             int j = ((j0 + dj) % t->height + t->height) % t->height;
-            const uint8_t* p = t->rgba + 4 * ((size_t)j * t->width + i);
             float w = (di ? a : 1.f - a) * (dj ? b : 1.f - b);
-            acc = vadd(acc, vs(v3(load_gamma(p[0]) / 255.f, load_gamma(p[1]) / 255.f, load_gamma(p[2]) / 255.f), w));
+            if (t->rgbaf) {
+                const float* q = t->rgbaf + 4 * ((size_t)j * t->width + i);
+                acc = vadd(acc, vs(v3(q[0], q[1], q[2]), w));
+            } else {
+                const uint8_t* p = t->rgba + 4 * ((size_t)j * t->width + i);
+                acc = vadd(acc, vs(v3(load_gamma(p[0]) / 255.f, load_gamma(p[1]) / 255.f, load_gamma(p[2]) / 255.f), w));
+            }
         }
     return acc;
 }

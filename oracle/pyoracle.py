@@ -243,7 +243,7 @@ OMAT_DTYPE = np.dtype([("type", "<i4"), ("kd", "<f4", (3,)), ("ks", "<f4", (3,))
                        ("kt", "<f4", (3,)), ("alpha_u", "<f4"), ("alpha_v", "<f4"), ("eta", "<f4"),
                        ("mirror_kr", "<f4"), ("f0", "<f4", (3,)), ("has_f0", "<i4"), ("kd_tex", "<i4")])
 OLIGHT_DTYPE = np.dtype([("L", "<f4", (3,)), ("mesh", "<i4"), ("kind", "<i4"), ("tex", "<i4"), ("w2l", "<f4", (9,))])
-OTEX_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("rgba", "<u8")])
+OTEX_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("rgba", "<u8"), ("rgbaf", "<u8")])
 MATERIAL_TYPES = {"matte": 0, "mirror": 1, "substrate": 2, "metal": 3, "glass": 4, "plastic": 5}
 
 
@@ -399,10 +399,24 @@ def render_path(scene: dict, *, width: int, height: int, spp: int, max_depth: in
         else:
             meshes[k]["light"] = -1
     light_arr = np.array(lights, OLIGHT_DTYPE)
-    flipped = [np.ascontiguousarray(np.asarray(im, np.uint8)[::-1]) for im in images]
+    # 8-bit images flipped to the PNG loader's bottom-up rows; float (OpenEXR) images as stored,
+    # RGBA as the EXR loader returns them (A = 1 when absent, one channel in all four)
+    def float_rgba(im):
+        f = np.asarray(im).astype(np.float32)
+        if f.ndim == 2:
+            f = f[..., None]
+        if f.shape[2] == 1:
+            f = np.repeat(f, 4, axis=2)
+        elif f.shape[2] == 3:
+            f = np.concatenate([f, np.ones(f.shape[:2] + (1,), np.float32)], axis=2)
+        return np.ascontiguousarray(f)
+
+    flipped = [float_rgba(im) if np.asarray(im).dtype.kind == "f" else np.ascontiguousarray(np.asarray(im, np.uint8)[::-1])
+               for im in images]
     texs = np.zeros(max(len(flipped), 1), OTEX_DTYPE)
     for k, im in enumerate(flipped):
-        texs[k]["width"], texs[k]["height"], texs[k]["rgba"] = im.shape[1], im.shape[0], im.ctypes.data
+        texs[k]["width"], texs[k]["height"] = im.shape[1], im.shape[0]
+        texs[k]["rgbaf" if im.dtype == np.float32 else "rgba"] = im.ctypes.data
     uvs = scene.get("uvs")
     uvs = None if uvs is None else np.ascontiguousarray(uvs, np.float32)
     c2w = look_at_c2w(eye, look, up)

@@ -61,6 +61,12 @@ CASES = [
      dict(width=160, height=120, spp=8, max_depth=5)),
     ("courtyard_direct", {"kind": "courtyard", "seed": 41},
      dict(width=160, height=120, spp=8, max_depth=5, integrator="directlighting")),
+    # the environment as an HDR OpenEXR map (HALF channels, ZIP compression; tinyexr in the
+    # reference, this project's EXR loader here): alone and with an area light
+    ("courtyard_env_exr", {"kind": "courtyard", "seed": 41, "hdr_sky": True},
+     dict(width=160, height=120, spp=8, max_depth=5)),
+    ("courtyard_env_exr_area", {"kind": "courtyard", "seed": 42, "area_light": True, "hdr_sky": True},
+     dict(width=160, height=120, spp=8, max_depth=5)),
     # the learning integrator (the .pbrt names it; both renderers read the Integrator line)
     ("room_rlpath_s16", {"kind": "room"}, dict(width=128, height=128, spp=16, max_depth=5, integrator="rlpath")),
     ("spheres_rlpath_s16", {"kind": "spheres", "n_spheres": 12, "level": 3, "seed": 5},
