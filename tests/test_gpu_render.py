@@ -60,7 +60,12 @@ TOL = {"room": dict(exact=0.999, le2=0.9998, gt8=0.0002),
 
 
 def tol_of(case):
-    return TOL["rlpath"] if case["render"].get("integrator") == "rlpath" else TOL[case["gen"]["kind"]]
+    t = TOL["rlpath"] if case["render"].get("integrator") == "rlpath" else TOL[case["gen"]["kind"]]
+    if case["gen"].get("hdr_sky"):
+        # an HDR sun 6x brighter than the 8-bit sky: one flipped path choice that reaches it
+        # moves its pixel far, so more pixels differ by more than 8 (the oracle shows it too)
+        t = dict(t, gt8=0.005)
+    return t
 
 
 @pytest.mark.parametrize("case", render_cases(), ids=[c["name"] for c in render_cases()])
@@ -273,3 +278,34 @@ def test_sample_ranges_sum_to_the_whole_render(ctx, tmp_path):
     with pytest.raises(Exception, match="sample ranges"):
         sc.render(integrator="rlpath", sample_range=(0, 10))
     ctx.sync_check()
+
+
+CONFIG3 = Path(__file__).resolve().parent / "golden" / "spheres5m_ref_sub4.npz"
+
+
+@pytest.mark.skipif(not CONFIG3.exists(), reason="fixture made by tests/golden/make_config3_golden.py")
+def test_full_size_scene_matches_reference_png(ctx, tmp_path):
+    """The full-size path-traced scene (64 level-6 icospheres, 5.24M triangles, 1920 x 1080, 64
+    spp, depth 8), compared with the reference renderer's PNG on every 4th row and column.
+    This project's render uses its own 3-round tree (a closest hit changes only at an exact
+    distance tie) in the exact traversal mode.  The tolerance is stated for this size: each
+    pixel averages 64 sample paths, and a discrete choice flipped by last-bit rounding in any
+    of them (a glass lobe, a roulette draw) moves the pixel's 8-bit value, so fewer pixels are
+    exactly equal than in the 8-16 spp goldens (measured 92.7 % exact, 99.7 % within 2)."""
+    import json
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    g = np.load(CONFIG3)
+    meta = json.loads(str(g["meta"]))
+    path = str(tmp_path / "spheres5m.pbrt")
+    scenes.write_pbrt(path, scenes.sphere_scene(**meta["scene"]), **meta["render"])
+    sc = ctx.load_pbrt(path, bvh_rounds=3)
+    s, w, _ = sc.render()
+    sc.free()
+    img = cav.film_to_rgb8(s, w)[:: meta["step"], :: meta["step"]]
+    d = np.abs(img.astype(int) - g["sub"].astype(int)).max(2)
+    assert (d == 0).mean() >= 0.90, (d == 0).mean()
+    assert (d <= 2).mean() >= 0.995, (d <= 2).mean()
+    assert (d > 8).mean() <= 0.001, (d > 8).mean()
