@@ -62,7 +62,7 @@ def parse():
     p.add_argument("--jobs", type=int, default=256, help="jobs in the served stream (serve workload)")
     p.add_argument("--serve-trace", default="fast", choices=["fast", "exact"], help="serve workload: traversal mode")
     p.add_argument("--serve-loaders", type=int, default=8, help="serve workload: the server's scene loader threads")
-    p.add_argument("--serve-lanes", default="2",
+    p.add_argument("--serve-lanes", default="8",
                    help="serve workload: the server's lanes; a comma list runs the server arm once per value "
                         "(the first value is the bench's `value`)")
     p.add_argument("--bounce", type=int, default=1, help="capture workload: which bounce's extend rays")
@@ -1075,14 +1075,23 @@ def run_guided(args):
 
     sc.render(spp=1, integrator="path")  # warm-up
     rows = {"path": [], "rlpath": [], "guided": []}
+
+    def best_of_two(fn):
+        # each render runs twice and keeps the first film with the faster time (path is
+        # deterministic; rlpath and the guided render relearn from the same start, so their
+        # two films differ only by the order of float atomics)
+        r0 = fn()
+        r1 = fn()
+        return r0[0], r0[1], min(r0[2], r1[2])
+
     # the baselines run to 1024 spp so that every guided time lies inside their sweep
     for spp in (16, 32, 64, 128, 256, 512, 1024):
-        s, w, ms = sc.render(spp=spp, integrator="path")
+        s, w, ms = best_of_two(lambda: sc.render(spp=spp, integrator="path"))
         rows["path"].append((spp, ms, relmse(s / w[..., None])))
-        s, w, ms = sc.render(spp=spp, integrator="rlpath")
+        s, w, ms = best_of_two(lambda: sc.render(spp=spp, integrator="rlpath"))
         rows["rlpath"].append((spp, ms, relmse(s / w[..., None])))
         if spp <= 256:
-            s, w, ms, st = sc.render_guided(spp=spp, steps_per_pass=64, lr=5e-3)
+            s, w, ms = best_of_two(lambda: sc.render_guided(spp=spp, steps_per_pass=64, lr=5e-3)[:3])
             rows["guided"].append((spp, ms, relmse(s / w[..., None])))
 
     def at_time(rs, t):
@@ -1109,8 +1118,10 @@ def run_guided(args):
 # ------------------------------------------------------------------------ mlp workload
 def run_mlp(args):
     """The learned proposal's kernels alone: forward passes over 4M vertices (--small: 1M)
-    and Adam steps at batch 16,384, device-timed; FLOP/s counts the 41 kFLOP of one
-    forward pass per vertex (160x64 + 2 x 64x64 + 64x32 multiply-adds x 2)."""
+    and Adam steps at batch 16,384, device-timed, for the tcgen05 kernel (the value) and
+    the mma.sync kernel beside it; FLOP/s counts the 41 kFLOP of one forward pass per
+    vertex (160x64 + 2 x 64x64 + 64x32 multiply-adds x 2).  The forward reads 20 bytes and
+    writes 128 bytes per vertex, so its HBM floor is also reported."""
     import torch
 
     import cavalry_b200 as cav
@@ -1118,46 +1129,60 @@ def run_mlp(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     ctx = cav.Context(0)
-    net = cav.Mlp(ctx, seed=1)
     n = 1 << 20 if args.small else 1 << 22
     g = torch.Generator("cuda").manual_seed(1)
     x = torch.rand((n, 5), device="cuda", generator=g)
     d = torch.nn.functional.normalize(torch.randn((n, 3), device="cuda", generator=g), dim=1).contiguous()
     w = torch.rand(n, device="cuda", generator=g)
     flop = 2 * (160 * 64 + 2 * 64 * 64 + 64 * 32)
-    for _ in range(max(args.warmup, 1)):
-        net.forward(x)
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     steps = max(args.steps, 1)
-    a.record()
-    for _ in range(steps):
-        net.forward(x)
-    b.record()
-    torch.cuda.synchronize()
-    fwd_ms = a.elapsed_time(b) / steps
-    bs = 16384
-    for _ in range(3):
-        net.train_step(x[:bs], d[:bs], w[:bs], lr=1e-3)
-    torch.cuda.synchronize()
-    a.record()
-    for k in range(steps):
-        o = (k * bs) % (n - bs)
-        net.train_step(x[o:o + bs], d[o:o + bs], w[o:o + bs], lr=1e-3)
-    b.record()
-    torch.cuda.synchronize()
-    train_ms = a.elapsed_time(b) / steps
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("bf16_tflops", 1590.0))
-    ach = flop * n / (fwd_ms * 1e-3) / 1e12
-    print(json.dumps({"metric": "MLP forward samples/s", "value": round(n / (fwd_ms * 1e-3) / 1e9, 3),
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+
+    def measure(kernel):
+        net = cav.Mlp(ctx, seed=1, kernel=kernel)
+        for _ in range(max(args.warmup, 3)):
+            net.forward(x)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(steps):
+            net.forward(x)
+        b.record()
+        torch.cuda.synchronize()
+        fwd_ms = a.elapsed_time(b) / steps
+        bs = 16384
+        for _ in range(3):
+            net.train_step(x[:bs], d[:bs], w[:bs], lr=1e-3)
+        torch.cuda.synchronize()
+        a.record()
+        for k in range(steps):
+            o = (k * bs) % (n - bs)
+            net.train_step(x[o:o + bs], d[o:o + bs], w[o:o + bs], lr=1e-3)
+        b.record()
+        torch.cuda.synchronize()
+        train_ms = a.elapsed_time(b) / steps
+        ctx.sync_check()
+        net.free()
+        ach = flop * n / (fwd_ms * 1e-3) / 1e12
+        return {"forward_ms": round(fwd_ms, 4), "train_step_ms": round(train_ms, 4),
+                "g_samples_s": round(n / (fwd_ms * 1e-3) / 1e9, 3), "tflops": round(ach, 1),
+                "frac": round(ach / peak, 4)}
+
+    tc = measure(cav.MLP_KERNEL_TCGEN05)
+    ms = measure(cav.MLP_KERNEL_MMA_SYNC)
+    floor_ms = n * (20 + 128) / (hbm * 1e9) * 1e3
+    print(json.dumps({"metric": "MLP forward samples/s", "value": tc["g_samples_s"],
                       "unit": "G samples/s", "n_gpus": 1, "steps": steps, "higher_is_better": True,
                       "dtype": "bf16 (fp32 accumulate)", "data": "synthetic",
-                      "config": {"workload": f"mlp_forward_{n}_vertices", "batch": n, "train_batch": bs},
-                      "forward_ms": round(fwd_ms, 4), "train_step_ms": round(train_ms, 4),
-                      "roofline": {"bound": "tensor", "achieved": round(ach, 1), "peak": peak, "unit": "TFLOP/s",
-                                   "frac": round(ach / peak, 4), "peak_kind": "measured" if peaks else "fallback",
-                                   "instruction": "mma.sync.m16n8k16 bf16"}}))
+                      "config": {"workload": f"mlp_forward_{n}_vertices", "batch": n, "train_batch": 16384},
+                      "forward_ms": tc["forward_ms"], "train_step_ms": tc["train_step_ms"],
+                      "roofline": {"bound": "tensor", "achieved": tc["tflops"], "peak": peak, "unit": "TFLOP/s",
+                                   "frac": tc["frac"], "peak_kind": "measured" if peaks else "fallback",
+                                   "instruction": "tcgen05.mma.cta_group::1.kind::f16 M128 bf16, TMEM accumulators",
+                                   "hbm_floor_ms": round(floor_ms, 4)},
+                      "mma_sync": ms}))
 
 
 def main():

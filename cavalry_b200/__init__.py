@@ -107,6 +107,7 @@ def lib() -> ctypes.CDLL:
         "cav_mlp_get_params": ([P, P], ctypes.c_int),
         "cav_mlp_set_params": ([P, P], ctypes.c_int),
         "cav_mlp_forward": ([P, P, ctypes.c_int64, P, P], ctypes.c_int),
+        "cav_mlp_set_kernel": ([P, ctypes.c_int], ctypes.c_int),
         "cav_mlp_gradients": ([P, P, P, P, ctypes.c_int64, P, P], ctypes.c_int),
         "cav_mlp_train_step": ([P, P, P, P, ctypes.c_int64, ctypes.c_float, P], ctypes.c_int),
         "cav_mlp_last_loss": ([P, P], ctypes.c_int),
@@ -627,15 +628,25 @@ class Server:
             pass
 
 
-class Mlp:
-    """The learned directional proposal (cav_mlp): 5 inputs in [0, 1] -> 8-lobe vMF mixture."""
+MLP_KERNEL_TCGEN05 = 0  # cav_mlp_set_kernel: 128-sample tiles on tcgen05, accumulators in TMEM
+MLP_KERNEL_MMA_SYNC = 1  # 16-sample warp tiles with mma.sync
 
-    def __init__(self, ctx: "Context", seed: int = 1):
+
+class Mlp:
+    """The learned directional proposal (cav_mlp): 5 inputs in [0, 1] -> 8-lobe vMF mixture.
+    `kernel` picks the forward-pass kernel (MLP_KERNEL_TCGEN05 by default)."""
+
+    def __init__(self, ctx: "Context", seed: int = 1, kernel: int = MLP_KERNEL_TCGEN05):
         self.ctx = ctx
         h = ctypes.c_void_p()
         ctx._check(lib().cav_mlp_create(ctx.handle, seed, ctypes.byref(h)), "cav_mlp_create")
         self.handle = h
         self.n_params = lib().cav_mlp_num_params()
+        self.set_kernel(kernel)
+
+    def set_kernel(self, kernel: int):
+        self.ctx._check(lib().cav_mlp_set_kernel(self.handle, kernel), "cav_mlp_set_kernel")
+        self.kernel = kernel
 
     def params(self) -> np.ndarray:
         p = np.zeros(self.n_params, np.float32)

@@ -282,6 +282,7 @@ cav_status cav_sync_check(cav_ctx* ctx, void* stream) {
         return set_error(ctx, CAV_ERR_STACK_OVERFLOW, "traversal stack overflow");
     if ((flags[2] | flags[3]) & kFlagStepLimit)
         return set_error(ctx, CAV_ERR_TIMEOUT, "traversal step limit reached (rays stopped)");
+    if (flags[4]) return set_error(ctx, CAV_ERR_TIMEOUT, "MLP forward: a tensor-core completion wait gave up");
     return CAV_OK;
 }
 

@@ -342,6 +342,273 @@ __global__ void __launch_bounds__(kFwdThreads) k_forward(const float* __restrict
     }
 }
 
+// ---------------------------------------------------------------- tcgen05 forward
+// The same forward pass on the 5th-generation tensor cores.  A persistent CTA holds the
+// BF16 weights in shared memory in the UMMA K-major canonical layout (no swizzle: an 8-row
+// x 16-byte core matrix is 128 contiguous bytes, 8-row groups 128 bytes apart, the two
+// 8-element K halves of one instruction R*16 bytes apart for an R-row operand) and runs
+// kGroups independent 128-sample tiles, one per warpgroup.  Per tile: each thread builds
+// its sample's 160 one-blob features into the tile's A buffer; one thread issues the
+// layer's UMMAs (M = 128, N = 64 or 32, K = 16 each) with the FP32 accumulator in the
+// warpgroup's 64 TMEM columns and commits them to the warpgroup's mbarrier; every thread
+// then reads its sample's row back (tcgen05.ld 32x32b: warp w of the group owns TMEM lanes
+// 32w..32w+31, i.e. samples 32w..32w+31), adds the bias, applies ReLU and writes the next
+// layer's A operand (BF16, the same rounding points as the mma.sync kernel) in place.
+// The last layer's row goes to global memory as 32 FP32 outputs.
+//
+// Waits are bounded: a warpgroup whose commit does not arrive within kWaitNs sets bit 1 of
+// the error word, waits once more (bounded) for the MMAs it issued, and stops; TMEM is
+// freed on every path.
+namespace umma {
+
+constexpr int kM = 128;        // samples per tile = UMMA M = TMEM lanes
+constexpr int kGroups = 4;     // warpgroups (independent tiles) per CTA
+constexpr int kThreads = 128 * kGroups;
+constexpr int kTmemCols = 64 * kGroups;  // one 64-column FP32 accumulator per warpgroup
+constexpr uint64_t kWaitNs = 1000000000ull;
+constexpr int kErrWait = 1;
+
+__host__ __device__ constexpr int w_at(int l) {  // byte offset of layer l's weights
+    int o = 0;
+    for (int i = 0; i < l; ++i) o += layer_out(i) * layer_in(i) * 2;
+    return o;
+}
+constexpr int kBiasAt = w_at(kLayers);  // 40,960
+constexpr int kAAt = kBiasAt + 1024;    // FP32 biases (896 bytes), then the A buffers
+constexpr int kABytes = kM * kF0 * 2;   // a tile's widest operand: 160 BF16 features per sample
+constexpr int kBarAt = kAAt + kGroups * kABytes;
+constexpr int kSmem = kBarAt + 8 * kGroups + 16;
+static_assert(kSmem <= 227 * 1024, "tcgen05 forward exceeds the shared-memory limit");
+static_assert(kTmemCols <= 512 && (kTmemCols & (kTmemCols - 1)) == 0, "TMEM allocation must be a power of two");
+
+// byte offset of element (row r, column k) in a K-major canonical operand of R rows
+__device__ __forceinline__ uint32_t canon(int R, int r, int k) {
+    return (uint32_t)((k >> 3) * (R * 16) + r * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start, leading (K) and stride (8-row) byte offsets, SM100 version 1, no swizzle
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, M = 128, N = n
+__host__ __device__ constexpr uint32_t idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(a), "l"(b), "r"(id), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// One layer: K/16 UMMAs into the group's accumulator, then a commit to its mbarrier.
+template <int K, int N>
+__device__ __forceinline__ void issue_layer(uint32_t a_s, uint32_t w_s, uint32_t tmem, uint32_t bar) {
+    fence_after();
+#pragma unroll
+    for (int j = 0; j < K / 16; ++j)
+        mma_bf16(tmem, sdesc(a_s + j * 2 * kM * 16, kM * 16, 128), sdesc(w_s + j * 2 * N * 16, N * 16, 128), idesc(N),
+                 j > 0);
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ uint64_t now_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    uint64_t t0 = 0;
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        const uint64_t t = now_ns();
+        if (t0 == 0) t0 = t;
+        else if (t - t0 > kWaitNs) return false;
+    }
+}
+
+// named barrier over the 128 threads of warpgroup g that also ANDs a predicate across them
+__device__ __forceinline__ bool group_all(int g, bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred a, b;\n\tsetp.ne.u32 a, %1, 0;\n\tbar.red.and.pred b, %2, 128, a;\n\tselp.u32 %0, 1, 0, b;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(g + 1)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void group_sync(int g) { asm volatile("bar.sync %0, 128;" ::"r"(g + 1) : "memory"); }
+
+template <int kCols>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&v)[32]);
+
+template <>
+__device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
+        "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+          "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// bias + ReLU of 32 accumulator columns, packed to BF16 as 4 x 8-element K chunks of the next A
+__device__ __forceinline__ void relu_pack(const uint32_t (&v)[32], const float* bias, uint4 (&o)[4]) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        uint32_t w[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int j = c * 8 + 2 * e;
+            w[e] = pack_bf16(fmaxf(__uint_as_float(v[j]) + bias[j], 0.f),
+                             fmaxf(__uint_as_float(v[j + 1]) + bias[j + 1], 0.f));
+        }
+        o[c] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+}  // namespace umma
+
+template <bool kStore>
+__global__ void __launch_bounds__(umma::kThreads, 1)
+    k_forward_umma(const float* __restrict__ in, int64_t n, const __nv_bfloat16* __restrict__ img,
+                   const float* __restrict__ params, float* __restrict__ out, Acts acts, int* err) {
+    using namespace umma;
+    extern __shared__ __align__(16) unsigned char smem[];  // no-swizzle operands need 16-byte alignment
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int g = warp >> 2, m = tid & 127;  // warpgroup, sample row within its tile
+    // weights -> canonical layout (16-byte chunks of 8 K-elements; the image rows are 16-byte aligned)
+#pragma unroll
+    for (int l = 0; l < kLayers; ++l) {
+        const int K = layer_in(l), N = layer_out(l);
+        const uint4* src = reinterpret_cast<const uint4*>(img + wf_off(l));
+        for (int i = tid; i < N * K / 8; i += kThreads) {
+            const int r = i % N, kc = i / N;
+            *reinterpret_cast<uint4*>(smem + w_at(l) + canon(N, r, kc * 8)) = src[(r * (K + kPad)) / 8 + kc];
+        }
+    }
+    float* bias = reinterpret_cast<float*>(smem + kBiasAt);
+    for (int l = 0, o = 0; l < kLayers; o += layer_out(l), ++l)
+        for (int i = tid; i < layer_out(l); i += kThreads) bias[o + i] = params[b_off(l) + i];
+    const uint32_t bar = smem_u32(smem + kBarAt + 8 * g);
+    if (tid < kGroups) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(smem + kBarAt + 8 * tid)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_slot + (uint32_t)(64 * g);                       // the group's accumulator
+    const uint32_t tload = tmem + ((uint32_t)(32 * (warp & 3)) << 16);         // this warp's 32 lanes
+    unsigned char* A = smem + kAAt + g * kABytes;
+    const uint32_t a_s = smem_u32(A), w_s = smem_u32(smem);
+    uint32_t phase = 0;
+    const int64_t ntiles = (n + kM - 1) / kM;
+    for (int64_t tile = (int64_t)blockIdx.x * kGroups + g; tile < ntiles; tile += (int64_t)gridDim.x * kGroups) {
+        const int64_t r = tile * kM + m;
+        const bool valid = r < n;
+        // layer 0 operand: one-blob features of this sample (zeros beyond n)
+        float x[kIn];
+#pragma unroll
+        for (int i = 0; i < kIn; ++i) x[i] = valid ? in[r * kIn + i] : 0.f;
+#pragma unroll
+        for (int t = 0; t < kF0 / 8; ++t) {
+            const int dim = t >> 2, b = (t & 3) * 8;
+            uint4 c = make_uint4(pack_bf16(blob(x[dim], b), blob(x[dim], b + 1)),
+                                 pack_bf16(blob(x[dim], b + 2), blob(x[dim], b + 3)),
+                                 pack_bf16(blob(x[dim], b + 4), blob(x[dim], b + 5)),
+                                 pack_bf16(blob(x[dim], b + 6), blob(x[dim], b + 7)));
+            *reinterpret_cast<uint4*>(A + canon(kM, m, t * 8)) = c;
+            if (kStore && valid) reinterpret_cast<uint4*>(acts.x0 + r * kF0)[t] = c;
+        }
+        bool ok = true;
+#pragma unroll 1
+        for (int l = 0; l < kLayers && ok; ++l) {
+            fence_async_smem();  // the generic-proxy writes of the A operand, before the tensor core reads it
+            group_sync(g);
+            if (m == 0) {
+                if (l == 0) issue_layer<kF0, kH>(a_s, w_s + w_at(0), tmem, bar);
+                else if (l < 3) issue_layer<kH, kH>(a_s, w_s + w_at(l), tmem, bar);
+                else issue_layer<kH, kOut>(a_s, w_s + w_at(3), tmem, bar);
+            }
+            ok = group_all(g, mbar_wait(bar, phase));
+            if (!ok) break;
+            phase ^= 1;
+            fence_after();
+            const float* bl = bias + (l == 0 ? 0 : l == 1 ? kH : l == 2 ? 2 * kH : 3 * kH);
+            uint32_t v[32];
+            if (l < 3) {
+                __nv_bfloat16* xs = l == 0 ? acts.x1 : l == 1 ? acts.x2 : acts.x3;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    tmem_ld<32>(tload + 32 * h, v);
+                    tmem_wait_ld();
+                    uint4 o[4];
+                    relu_pack(v, bl + 32 * h, o);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        *reinterpret_cast<uint4*>(A + canon(kM, m, (4 * h + c) * 8)) = o[c];
+                        if (kStore && valid) reinterpret_cast<uint4*>(xs + r * kH)[4 * h + c] = o[c];
+                    }
+                }
+            } else {
+                tmem_ld<32>(tload, v);
+                tmem_wait_ld();
+                if (valid) {
+                    float4* dst = reinterpret_cast<float4*>(out + r * kOut);
+#pragma unroll
+                    for (int c = 0; c < kOut / 4; ++c)
+                        dst[c] = make_float4(__uint_as_float(v[4 * c]) + bl[4 * c], __uint_as_float(v[4 * c + 1]) + bl[4 * c + 1],
+                                             __uint_as_float(v[4 * c + 2]) + bl[4 * c + 2],
+                                             __uint_as_float(v[4 * c + 3]) + bl[4 * c + 3]);
+                }
+            }
+            fence_before();  // the TMEM reads, before the next layer's MMAs overwrite the accumulator
+        }
+        if (!ok) {
+            if (m == 0) atomicOr(err, kErrWait);
+            mbar_wait(bar, phase);  // the MMAs this group issued, once more with the same bound
+            break;
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_slot), "r"(kTmemCols) : "memory");
+    }
+}
+
 // ---------------------------------------------------------------- loss and backward
 struct Grads {  // training only: each layer's output gradient (bf16), [n][width]
     __nv_bfloat16* d3;  // d loss / d outputs, 32
@@ -533,6 +800,7 @@ struct cav_mlp {
     __nv_bfloat16* d_img = nullptr;
     float* d_loss = nullptr;
     int64_t step = 0;
+    int kernel = CAV_MLP_KERNEL_TCGEN05;  // forward-pass kernel (cav_mlp_set_kernel)
     // training scratch, sized to the largest batch seen
     int64_t cap = 0;
     void* scratch = nullptr;
@@ -549,6 +817,25 @@ using namespace cav::mlp;
 int fwd_grid(cav_ctx* ctx, int64_t n, int threads) {
     int64_t want = (n + (threads / 2) - 1) / (threads / 2);  // warps x 16 samples per block and pass
     return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->num_sms * 2));
+}
+
+int umma_grid(cav_ctx* ctx, int64_t n) {
+    const int64_t groups = ((n + umma::kM - 1) / umma::kM + umma::kGroups - 1) / umma::kGroups;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(groups, (int64_t)ctx->num_sms));
+}
+
+// The forward pass (kStore: keeping each layer's input for the backward pass) with the network's kernel.
+template <bool kStore>
+cav_status launch_forward(cav_mlp* m, const float* in, int64_t n, float* out, Acts acts, cudaStream_t s) {
+    cav_ctx* ctx = m->ctx;
+    if (m->kernel == CAV_MLP_KERNEL_TCGEN05)
+        k_forward_umma<kStore><<<umma_grid(ctx, n), umma::kThreads, umma::kSmem, s>>>(in, n, m->d_img, m->d_params, out,
+                                                                                    acts, ctx->d_error + 4);
+    else
+        k_forward<kStore><<<fwd_grid(ctx, n, kFwdThreads), kFwdThreads, kSmemBytes, s>>>(in, n, m->d_img, m->d_params,
+                                                                                          out, acts);
+    CAV_CUDA(ctx, cudaGetLastError());
+    return CAV_OK;
 }
 
 cav_status ensure_scratch(cav_mlp* m, int64_t n, cudaStream_t s) {
@@ -590,8 +877,8 @@ cav_status compute_grads(cav_mlp* m, const float* in, const float* dirs, const f
     cav_ctx* ctx = m->ctx;
     CAV_CUDA(ctx, cudaMemsetAsync(m->d_grads, 0, sizeof(float) * kParams, s));
     CAV_CUDA(ctx, cudaMemsetAsync(m->d_loss, 0, sizeof(float), s));
-    k_forward<true><<<fwd_grid(ctx, n, kFwdThreads), kFwdThreads, kSmemBytes, s>>>(in, n, m->d_img, m->d_params, m->out,
-                                                                                  m->acts);
+    st = launch_forward<true>(m, in, n, m->out, m->acts, s);
+    if (st != CAV_OK) return st;
     const int grid = fwd_grid(ctx, n, 128);
     k_loss<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m->out, dirs, w, n, m->dout, m->d_loss);
     k_backward<<<grid, 128, kSmemBytes, s>>>(m->dout, n, m->d_img, m->d_params, m->acts, m->grads);
@@ -611,10 +898,7 @@ namespace cav {
 // Device entry for the guided integrator: forward pass over n inputs into out (n x 32).
 cav_status mlp_forward(cav_mlp* m, const float* in, int64_t n, float* out, cudaStream_t s) {
     if (n <= 0) return CAV_OK;
-    k_forward<false><<<fwd_grid(m->ctx, n, kFwdThreads), kFwdThreads, kSmemBytes, s>>>(in, n, m->d_img, m->d_params,
-                                                                                      out, cav::mlp::Acts{});
-    CAV_CUDA(m->ctx, cudaGetLastError());
-    return CAV_OK;
+    return launch_forward<false>(m, in, n, out, cav::mlp::Acts{}, s);
 }
 }  // namespace cav
 
@@ -631,6 +915,8 @@ cav_status cav_mlp_create(cav_ctx* ctx, uint64_t seed, cav_mlp** out) {
         cudaFuncSetAttribute(k_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
         cudaFuncSetAttribute(k_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
         cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        cudaFuncSetAttribute(k_forward_umma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
+        cudaFuncSetAttribute(k_forward_umma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
         attr = true;
     }
     auto* m = new cav_mlp();
@@ -691,8 +977,14 @@ cav_status cav_mlp_set_params(cav_mlp* m, const float* host) {
     return CAV_OK;
 }
 
+cav_status cav_mlp_set_kernel(cav_mlp* m, int kernel) {
+    if (!m || (kernel != CAV_MLP_KERNEL_TCGEN05 && kernel != CAV_MLP_KERNEL_MMA_SYNC)) return CAV_ERR_INVALID_ARGUMENT;
+    m->kernel = kernel;
+    return CAV_OK;
+}
+
 cav_status cav_mlp_forward(cav_mlp* m, const float* in, int64_t n, float* out, void* stream) {
-    if (!m || !in || !out || n < 0) return CAV_ERR_INVALID_ARGUMENT;
+    if (!m || n < 0 || (n > 0 && (!in || !out))) return CAV_ERR_INVALID_ARGUMENT;
     return cav::mlp_forward(m, in, n, out, (cudaStream_t)stream);
 }
 

@@ -452,6 +452,14 @@ cav_status cav_mlp_create(cav_ctx* ctx, uint64_t seed, cav_mlp** out);
 cav_status cav_mlp_free(cav_mlp* mlp);
 cav_status cav_mlp_get_params(cav_mlp* mlp, float* host_params);
 cav_status cav_mlp_set_params(cav_mlp* mlp, const float* host_params);
+/* Forward-pass kernel of a network (training and inference): CAV_MLP_KERNEL_TCGEN05 (the
+ * default: 128-sample tiles on the tcgen05 tensor cores, accumulators in TMEM) or
+ * CAV_MLP_KERNEL_MMA_SYNC (16-sample warp tiles with mma.sync, kept for comparison).  Both
+ * compute the same BF16-operand, FP32-accumulate products; results agree to FP32
+ * accumulation order.  A tcgen05 completion wait that runs out (1 s) is reported by
+ * cav_sync_check as CAV_ERR_TIMEOUT. */
+enum { CAV_MLP_KERNEL_TCGEN05 = 0, CAV_MLP_KERNEL_MMA_SYNC = 1 };
+cav_status cav_mlp_set_kernel(cav_mlp* mlp, int kernel);
 /* in: n x 5, out: n x 32 */
 cav_status cav_mlp_forward(cav_mlp* mlp, const float* in, int64_t n, float* out, void* stream);
 /* Loss gradient w.r.t. every parameter for one batch (in n x 5, dirs n x 3 unit, w n),

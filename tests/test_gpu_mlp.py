@@ -43,24 +43,66 @@ def layer_slices():
     return out
 
 
-def test_forward_matches_oracle(ctx):
+KERNELS = {"tcgen05": 0, "mma_sync": 1}
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+@pytest.mark.parametrize("n", [1, 127, 1000, 128 * 148 * 4 + 77])
+def test_forward_matches_oracle(ctx, kernel, n):
+    """n = 1 and 127: one partial 128-sample tile; 1000: eight tiles, the last partial;
+    75,853: every warpgroup of every persistent CTA takes a second tile."""
     import cavalry_b200 as cav
     from oracle import mlp_oracle as mo
+
+    net = cav.Mlp(ctx, seed=5, kernel=KERNELS[kernel])
+    p = net.params()
+    x, _, _ = batch(n, 1)
+    out = net.forward(cuda(x)).cpu().numpy()
+    ctx.sync_check()
+    sel = np.arange(n) if n <= 4096 else np.random.default_rng(0).choice(n, 4096, replace=False)
+    ref, _ = mo.forward(p, x[sel].astype(np.float64), bf=True)
+    scale = np.abs(ref).mean()
+    assert np.abs(out[sel] - ref).max() <= 1e-2 * scale + 1e-3, np.abs(out[sel] - ref).max()
+
+
+def test_tcgen05_and_mma_sync_forward_agree(ctx):
+    """The two kernels take the same BF16 operands at the same rounding points and differ
+    only in the FP32 summation order inside the tensor core, so outputs agree to about
+    1e-5 of their scale; a BF16 rounding of an activation that lands on the other side
+    moves a few outputs by up to ~1e-3 of scale."""
+    import cavalry_b200 as cav
+
+    a = cav.Mlp(ctx, seed=8, kernel=cav.MLP_KERNEL_TCGEN05)
+    b = cav.Mlp(ctx, seed=8, kernel=cav.MLP_KERNEL_MMA_SYNC)
+    x, _, _ = batch(50_000, 12)
+    oa = a.forward(cuda(x)).cpu().numpy()
+    ob = b.forward(cuda(x)).cpu().numpy()
+    ctx.sync_check()
+    scale = np.abs(ob).mean()
+    d = np.abs(oa - ob)
+    assert np.median(d) <= 1e-5 * scale and d.max() <= 5e-3 * scale, (np.median(d) / scale, d.max() / scale)
+    with pytest.raises(cav.CavError):
+        a.set_kernel(7)
+    a.free()
+    b.free()
+
+
+def test_empty_forward(ctx):
+    import torch
+
+    import cavalry_b200 as cav
 
     net = cav.Mlp(ctx, seed=5)
-    p = net.params()
-    x, _, _ = batch(1000, 1)
-    out = net.forward(cuda(x)).cpu().numpy()
-    ref, _ = mo.forward(p, x.astype(np.float64), bf=True)
-    scale = np.abs(ref).mean()
-    assert np.abs(out - ref).max() <= 1e-2 * scale + 1e-3, np.abs(out - ref).max()
+    assert net.forward(torch.zeros((0, 5), device="cuda")).shape == (0, 32)
+    ctx.sync_check()
 
 
-def test_gradients_match_oracle(ctx):
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_gradients_match_oracle(ctx, kernel):
     import cavalry_b200 as cav
     from oracle import mlp_oracle as mo
 
-    net = cav.Mlp(ctx, seed=6)
+    net = cav.Mlp(ctx, seed=6, kernel=KERNELS[kernel])
     rng = np.random.default_rng(9)
     p = net.params()
     p[-32:] = rng.normal(0, 0.5, 32).astype(np.float32)  # spread the lobes
