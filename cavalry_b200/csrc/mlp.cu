@@ -78,10 +78,21 @@ __device__ __forceinline__ void mma(float (&d)[4], const uint32_t (&a)[4], uint3
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// One-blob encoding: bin b of input x has value exp(-0.5 ((x - (b + 0.5) / 32) * 32)^2).
-__device__ __forceinline__ float blob(float x, int b) {
-    float z = (x - ((float)b + 0.5f) * (1.f / kBins)) * (float)kBins;
-    return __expf(-0.5f * z * z);
+// One-blob encoding: bin b of input x has value exp(-0.5 ((x - (b + 0.5) / 32) * 32)^2),
+// evaluated as 2^-(s z)^2 with s = sqrt(0.5 log2 e) folded into the bin offset: a subtract,
+// a multiply and the hardware base-2 exponential per bin.  `xs` is x * 32 s (blob_scale).
+// The offset (b + 0.5) s is rounded on its own: with b known at compile time (blob) it folds
+// to a constant; with b computed at run time (blob_rt) the explicit round-to-nearest product
+// and difference keep the compiler from fusing them, so both build the same features.
+constexpr float kBlobS = 0.84932180028801907f;  // sqrt(0.5 / ln 2)
+__device__ __forceinline__ float blob_scale(float x) { return x * ((float)kBins * kBlobS); }
+__device__ __forceinline__ float blob(float xs, int b) {
+    const float z = xs - ((float)b + 0.5f) * kBlobS;
+    return exp2f(-(z * z));
+}
+__device__ __forceinline__ float blob_rt(float xs, int b) {
+    const float z = __fsub_rn(xs, __fmul_rn((float)b + 0.5f, kBlobS));
+    return exp2f(-(z * z));
 }
 
 // ---------------------------------------------------------------- mixture of vMF lobes
@@ -299,18 +310,18 @@ __global__ void __launch_bounds__(kFwdThreads) k_forward(const float* __restrict
         float xa[kIn], xb[kIn];
 #pragma unroll
         for (int i = 0; i < kIn; ++i) {
-            xa[i] = ra < n ? in[ra * kIn + i] : 0.f;
-            xb[i] = rb < n ? in[rb * kIn + i] : 0.f;
+            xa[i] = blob_scale(ra < n ? in[ra * kIn + i] : 0.f);
+            xb[i] = blob_scale(rb < n ? in[rb * kIn + i] : 0.f);
         }
         // layer 0: one-blob features built straight into A fragments (a k-tile = 16 bins of one input)
         uint32_t A0[kF0 / 16][4];
 #pragma unroll
         for (int t = 0; t < kF0 / 16; ++t) {
             const int dim = t >> 1, b = (t & 1) * 16 + 2 * q;
-            A0[t][0] = pack_bf16(blob(xa[dim], b), blob(xa[dim], b + 1));
-            A0[t][1] = pack_bf16(blob(xb[dim], b), blob(xb[dim], b + 1));
-            A0[t][2] = pack_bf16(blob(xa[dim], b + 8), blob(xa[dim], b + 9));
-            A0[t][3] = pack_bf16(blob(xb[dim], b + 8), blob(xb[dim], b + 9));
+            A0[t][0] = pack_bf16(blob_rt(xa[dim], b), blob_rt(xa[dim], b + 1));
+            A0[t][1] = pack_bf16(blob_rt(xb[dim], b), blob_rt(xb[dim], b + 1));
+            A0[t][2] = pack_bf16(blob_rt(xa[dim], b + 8), blob_rt(xa[dim], b + 9));
+            A0[t][3] = pack_bf16(blob_rt(xb[dim], b + 8), blob_rt(xb[dim], b + 9));
         }
         if (kStore) store_a(A0, acts.x0, kF0, r0, n);
         float D[8][4];
@@ -347,14 +358,17 @@ __global__ void __launch_bounds__(kFwdThreads) k_forward(const float* __restrict
 // BF16 weights in shared memory in the UMMA K-major canonical layout (no swizzle: an 8-row
 // x 16-byte core matrix is 128 contiguous bytes, 8-row groups 128 bytes apart, the two
 // 8-element K halves of one instruction R*16 bytes apart for an R-row operand) and runs
-// kGroups independent 128-sample tiles, one per warpgroup.  Per tile: each thread builds
-// its sample's 160 one-blob features into the tile's A buffer; one thread issues the
-// layer's UMMAs (M = 128, N = 64 or 32, K = 16 each) with the FP32 accumulator in the
-// warpgroup's 64 TMEM columns and commits them to the warpgroup's mbarrier; every thread
-// then reads its sample's row back (tcgen05.ld 32x32b: warp w of the group owns TMEM lanes
-// 32w..32w+31, i.e. samples 32w..32w+31), adds the bias, applies ReLU and writes the next
-// layer's A operand (BF16, the same rounding points as the mma.sync kernel) in place.
-// The last layer's row goes to global memory as 32 FP32 outputs.
+// kGroups streams of 128-sample tiles, one per warpgroup.  Each thread owns one sample of
+// its group's tile.  Layer 0 reads the features operand F (160 one-blob features per
+// sample), layers 1-3 the activations operand H.  For each layer one thread issues the
+// UMMAs (M = 128, N = 64 or 32, K = 16 each) with the FP32 accumulator in the group's 64
+// TMEM columns and commits them to the group's mbarrier; every thread then reads its
+// sample's row back (tcgen05.ld 32x32b: warp w of the group owns TMEM lanes 32w..32w+31),
+// adds the bias, applies ReLU and writes H (BF16, the same rounding points as the mma.sync
+// kernel).  The tile is software-pipelined: once layer 0 has read F, the threads build the
+// NEXT tile's features into F while the tensor core runs layers 1 and 2, so the 160
+// exponentials per sample overlap the MMA latencies; inputs are loaded two tiles ahead.
+// The last layer's rows are staged in H and written out as one contiguous block.
 //
 // Waits are bounded: a warpgroup whose commit does not arrive within kWaitNs sets bit 1 of
 // the error word, waits once more (bounded) for the MMAs it issued, and stops; TMEM is
@@ -362,9 +376,9 @@ __global__ void __launch_bounds__(kFwdThreads) k_forward(const float* __restrict
 namespace umma {
 
 constexpr int kM = 128;        // samples per tile = UMMA M = TMEM lanes
-constexpr int kGroups = 4;     // warpgroups (independent tiles) per CTA
+constexpr int kGroups = 3;     // warpgroups (independent tile streams) per CTA
 constexpr int kThreads = 128 * kGroups;
-constexpr int kTmemCols = 64 * kGroups;  // one 64-column FP32 accumulator per warpgroup
+constexpr int kTmemCols = 256;  // one 64-column FP32 accumulator per warpgroup, rounded up to a power of two
 constexpr uint64_t kWaitNs = 1000000000ull;
 constexpr int kErrWait = 1;
 
@@ -374,12 +388,16 @@ __host__ __device__ constexpr int w_at(int l) {  // byte offset of layer l's wei
     return o;
 }
 constexpr int kBiasAt = w_at(kLayers);  // 40,960
-constexpr int kAAt = kBiasAt + 1024;    // FP32 biases (896 bytes), then the A buffers
-constexpr int kABytes = kM * kF0 * 2;   // a tile's widest operand: 160 BF16 features per sample
-constexpr int kBarAt = kAAt + kGroups * kABytes;
+constexpr int kFAt = kBiasAt + 1024;    // FP32 biases (896 bytes), then per group F, then per group H
+constexpr int kFBytes = kM * kF0 * 2;   // layer-0 operand: 160 BF16 features per sample
+constexpr int kHAt = kFAt + kGroups * kFBytes;
+constexpr int kHBytes = kM * kH * 2;    // layers 1-3 operand: 64 BF16 activations per sample
+static_assert(kM * kOut * 4 <= kHBytes, "output staging must fit in H");
+constexpr int kBarAt = kHAt + kGroups * kHBytes;
 constexpr int kSmem = kBarAt + 8 * kGroups + 16;
 static_assert(kSmem <= 227 * 1024, "tcgen05 forward exceeds the shared-memory limit");
-static_assert(kTmemCols <= 512 && (kTmemCols & (kTmemCols - 1)) == 0, "TMEM allocation must be a power of two");
+static_assert(kTmemCols <= 512 && (kTmemCols & (kTmemCols - 1)) == 0 && kTmemCols >= 64 * kGroups,
+              "TMEM allocation must be a power of two that holds every group's accumulator");
 
 // byte offset of element (row r, column k) in a K-major canonical operand of R rows
 __device__ __forceinline__ uint32_t canon(int R, int r, int k) {
@@ -474,6 +492,14 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, uint32_t (&v)[32]) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// ReLU and round-to-nearest BF16 of two floats in one conversion (lo in the low half); the
+// two operations commute, so this equals pack_bf16(fmaxf(lo, 0), fmaxf(hi, 0)).
+__device__ __forceinline__ uint32_t relu_pack_bf16(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
 // bias + ReLU of 32 accumulator columns, packed to BF16 as 4 x 8-element K chunks of the next A
 __device__ __forceinline__ void relu_pack(const uint32_t (&v)[32], const float* bias, uint4 (&o)[4]) {
 #pragma unroll
@@ -482,14 +508,29 @@ __device__ __forceinline__ void relu_pack(const uint32_t (&v)[32], const float* 
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const int j = c * 8 + 2 * e;
-            w[e] = pack_bf16(fmaxf(__uint_as_float(v[j]) + bias[j], 0.f),
-                             fmaxf(__uint_as_float(v[j + 1]) + bias[j + 1], 0.f));
+            w[e] = relu_pack_bf16(__uint_as_float(v[j]) + bias[j], __uint_as_float(v[j + 1]) + bias[j + 1]);
         }
         o[c] = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
 }  // namespace umma
+
+// One-blob features of one sample for the K chunks [T0, T1) (8 bins each) into the
+// canonical layer-0 operand; with kStore also into the stored activations.
+template <bool kStore, int T0, int T1>
+__device__ __forceinline__ void build_features(unsigned char* F, int m, const float (&x)[kIn], __nv_bfloat16* x0row) {
+#pragma unroll
+    for (int t = T0; t < T1; ++t) {
+        const int dim = t >> 2, b = (t & 3) * 8;
+        uint4 c = make_uint4(pack_bf16(blob(x[dim], b), blob(x[dim], b + 1)),
+                             pack_bf16(blob(x[dim], b + 2), blob(x[dim], b + 3)),
+                             pack_bf16(blob(x[dim], b + 4), blob(x[dim], b + 5)),
+                             pack_bf16(blob(x[dim], b + 6), blob(x[dim], b + 7)));
+        *reinterpret_cast<uint4*>(F + umma::canon(umma::kM, m, t * 8)) = c;
+        if (kStore && x0row) reinterpret_cast<uint4*>(x0row)[t] = c;
+    }
+}
 
 template <bool kStore>
 __global__ void __launch_bounds__(umma::kThreads, 1)
@@ -528,78 +569,131 @@ __global__ void __launch_bounds__(umma::kThreads, 1)
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = tmem_slot + (uint32_t)(64 * g);                       // the group's accumulator
-    const uint32_t tload = tmem + ((uint32_t)(32 * (warp & 3)) << 16);         // this warp's 32 lanes
-    unsigned char* A = smem + kAAt + g * kABytes;
-    const uint32_t a_s = smem_u32(A), w_s = smem_u32(smem);
+    const uint32_t tmem = tmem_slot + (uint32_t)(64 * g);                // the group's accumulator
+    const uint32_t tload = tmem + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's 32 lanes
+    unsigned char* F = smem + kFAt + g * kFBytes;  // layer-0 operand (features)
+    unsigned char* H = smem + kHAt + g * kHBytes;  // layers 1-3 operand, then the output staging
+    const uint32_t f_s = smem_u32(F), h_s = smem_u32(H), w_s = smem_u32(smem);
     uint32_t phase = 0;
     const int64_t ntiles = (n + kM - 1) / kM;
-    for (int64_t tile = (int64_t)blockIdx.x * kGroups + g; tile < ntiles; tile += (int64_t)gridDim.x * kGroups) {
-        const int64_t r = tile * kM + m;
-        const bool valid = r < n;
-        // layer 0 operand: one-blob features of this sample (zeros beyond n)
-        float x[kIn];
+    const int64_t stride = (int64_t)gridDim.x * kGroups;
+    const int64_t first = (int64_t)blockIdx.x * kGroups + g;
+
+    float xn[kIn];  // this sample's inputs of the next tile (zeros beyond n)
+    auto load_inputs = [&](int64_t t) {
+        const int64_t rr = t * kM + m;
 #pragma unroll
-        for (int i = 0; i < kIn; ++i) x[i] = valid ? in[r * kIn + i] : 0.f;
-#pragma unroll
-        for (int t = 0; t < kF0 / 8; ++t) {
-            const int dim = t >> 2, b = (t & 3) * 8;
-            uint4 c = make_uint4(pack_bf16(blob(x[dim], b), blob(x[dim], b + 1)),
-                                 pack_bf16(blob(x[dim], b + 2), blob(x[dim], b + 3)),
-                                 pack_bf16(blob(x[dim], b + 4), blob(x[dim], b + 5)),
-                                 pack_bf16(blob(x[dim], b + 6), blob(x[dim], b + 7)));
-            *reinterpret_cast<uint4*>(A + canon(kM, m, t * 8)) = c;
-            if (kStore && valid) reinterpret_cast<uint4*>(acts.x0 + r * kF0)[t] = c;
+        for (int i = 0; i < kIn; ++i) xn[i] = (t < ntiles && rr < n) ? in[rr * kIn + i] : 0.f;
+    };
+    auto x0row = [&](int64_t t) -> __nv_bfloat16* {
+        const int64_t rr = t * kM + m;
+        return (kStore && rr < n) ? acts.x0 + rr * kF0 : nullptr;
+    };
+    // Layer l's UMMAs on the operand the group just wrote, issued by one thread.
+    auto issue = [&](int l) {
+        fence_before();      // this thread's TMEM reads, before the MMAs overwrite the accumulator
+        fence_async_smem();  // its generic-proxy operand writes, before the tensor core reads them
+        group_sync(g);
+        if (m == 0) {
+            if (l == 0) issue_layer<kF0, kH>(f_s, w_s + w_at(0), tmem, bar);
+            else if (l < 3) issue_layer<kH, kH>(h_s, w_s + w_at(l), tmem, bar);
+            else issue_layer<kH, kOut>(h_s, w_s + w_at(3), tmem, bar);
         }
-        bool ok = true;
-#pragma unroll 1
-        for (int l = 0; l < kLayers && ok; ++l) {
-            fence_async_smem();  // the generic-proxy writes of the A operand, before the tensor core reads it
-            group_sync(g);
-            if (m == 0) {
-                if (l == 0) issue_layer<kF0, kH>(a_s, w_s + w_at(0), tmem, bar);
-                else if (l < 3) issue_layer<kH, kH>(a_s, w_s + w_at(l), tmem, bar);
-                else issue_layer<kH, kOut>(a_s, w_s + w_at(3), tmem, bar);
-            }
-            ok = group_all(g, mbar_wait(bar, phase));
-            if (!ok) break;
+    };
+    auto wait = [&]() -> bool {
+        const bool ok = group_all(g, mbar_wait(bar, phase));
+        if (ok) {
             phase ^= 1;
             fence_after();
-            const float* bl = bias + (l == 0 ? 0 : l == 1 ? kH : l == 2 ? 2 * kH : 3 * kH);
-            uint32_t v[32];
-            if (l < 3) {
-                __nv_bfloat16* xs = l == 0 ? acts.x1 : l == 1 ? acts.x2 : acts.x3;
+        }
+        return ok;
+    };
+    // bias + ReLU of layer l's accumulator into the next operand (H), and the stored activations
+    auto hidden = [&](int l, int64_t r) {
+        const float* bl = bias + l * kH;
+        __nv_bfloat16* xs = l == 0 ? acts.x1 : l == 1 ? acts.x2 : acts.x3;
+        uint32_t v[32], v1[32];
+        tmem_ld<32>(tload, v);
+        if (!kStore) tmem_ld<32>(tload + 32, v1);  // both halves in flight (the storing variant keeps to its registers)
+        tmem_wait_ld();
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    tmem_ld<32>(tload + 32 * h, v);
-                    tmem_wait_ld();
-                    uint4 o[4];
-                    relu_pack(v, bl + 32 * h, o);
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        *reinterpret_cast<uint4*>(A + canon(kM, m, (4 * h + c) * 8)) = o[c];
-                        if (kStore && valid) reinterpret_cast<uint4*>(xs + r * kH)[4 * h + c] = o[c];
-                    }
-                }
-            } else {
-                tmem_ld<32>(tload, v);
+        for (int h = 0; h < 2; ++h) {
+            if (kStore && h == 1) {
+                tmem_ld<32>(tload + 32, v1);
                 tmem_wait_ld();
-                if (valid) {
-                    float4* dst = reinterpret_cast<float4*>(out + r * kOut);
-#pragma unroll
-                    for (int c = 0; c < kOut / 4; ++c)
-                        dst[c] = make_float4(__uint_as_float(v[4 * c]) + bl[4 * c], __uint_as_float(v[4 * c + 1]) + bl[4 * c + 1],
-                                             __uint_as_float(v[4 * c + 2]) + bl[4 * c + 2],
-                                             __uint_as_float(v[4 * c + 3]) + bl[4 * c + 3]);
-                }
             }
-            fence_before();  // the TMEM reads, before the next layer's MMAs overwrite the accumulator
+            uint4 o[4];
+            relu_pack(h ? v1 : v, bl + 32 * h, o);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                *reinterpret_cast<uint4*>(H + canon(kM, m, (4 * h + c) * 8)) = o[c];
+                if (kStore && r < n) reinterpret_cast<uint4*>(xs + r * kH)[4 * h + c] = o[c];
+            }
         }
-        if (!ok) {
-            if (m == 0) atomicOr(err, kErrWait);
-            mbar_wait(bar, phase);  // the MMAs this group issued, once more with the same bound
-            break;
+    };
+
+    // prologue: the first tile's features; the inputs of the one after
+    load_inputs(first);
+    if (first < ntiles) {
+        float x[kIn];
+#pragma unroll
+        for (int i = 0; i < kIn; ++i) x[i] = blob_scale(xn[i]);
+        build_features<kStore, 0, kF0 / 8>(F, m, x, x0row(first));
+    }
+    load_inputs(first + stride);
+    bool ok = true;
+    for (int64_t tile = first; tile < ntiles && ok; tile += stride) {
+        const int64_t r = tile * kM + m;
+        const int64_t next = tile + stride;
+        const bool has_next = next < ntiles;  // uniform over the group
+        float x[kIn];
+#pragma unroll
+        for (int i = 0; i < kIn; ++i) x[i] = blob_scale(xn[i]);
+        issue(0);
+        if (!(ok = wait())) break;
+        hidden(0, r);
+        issue(1);
+        // F is free once layer 0 completed: the next tile's features are built while the
+        // tensor core runs layers 1 and 2
+        if (has_next) build_features<kStore, 0, 12>(F, m, x, x0row(next));
+        if (!(ok = wait())) break;
+        hidden(1, r);
+        issue(2);
+        if (has_next) build_features<kStore, 12, kF0 / 8>(F, m, x, x0row(next));
+        load_inputs(next + stride);
+        if (!(ok = wait())) break;
+        hidden(2, r);
+        issue(3);
+        if (!(ok = wait())) break;
+        {
+            // The tile's 128 output rows are staged in H (free once layer 3 completed; 16-byte
+            // chunks XOR-swizzled by row against bank conflicts) and leave as one contiguous
+            // 16 KB block; a row per thread would put every store of a warp on 32 lines.
+            const float* bl = bias + 3 * kH;
+            uint32_t v[32];
+            tmem_ld<32>(tload, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < kOut / 4; ++c)
+                *reinterpret_cast<float4*>(H + m * 128 + ((c ^ (m & 7)) << 4)) =
+                    make_float4(__uint_as_float(v[4 * c]) + bl[4 * c], __uint_as_float(v[4 * c + 1]) + bl[4 * c + 1],
+                                __uint_as_float(v[4 * c + 2]) + bl[4 * c + 2],
+                                __uint_as_float(v[4 * c + 3]) + bl[4 * c + 3]);
+            group_sync(g);
+            const int64_t row0 = tile * kM;
+            const int rows = (int)(n - row0 < kM ? n - row0 : kM);
+            float4* dst = reinterpret_cast<float4*>(out + row0 * kOut);
+#pragma unroll
+            for (int j = 0; j < kM * kOut / 4 / 128; ++j) {
+                const int i = m + 128 * j, row = i >> 3, c = i & 7;
+                if (row < rows) dst[i] = *reinterpret_cast<const float4*>(H + row * 128 + ((c ^ (row & 7)) << 4));
+            }
+            // the next write of H (the next tile's layer-0 epilogue) follows the group barrier in issue(0)
         }
+    }
+    if (!ok) {
+        if (m == 0) atomicOr(err, kErrWait);
+        mbar_wait(bar, phase);  // the MMAs this group issued, once more with the same bound
     }
     fence_before();
     __syncthreads();
