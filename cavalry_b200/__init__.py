@@ -193,7 +193,8 @@ class Context:
         self._check(lib().cav_ctx_set_limits(self.handle, sort_wait_s, max_trace_steps), "cav_ctx_set_limits")
 
     def inject(self, what: int, count: int = 1):
-        """Failure injection for tests (INJECT_SORT_STALL, INJECT_ALLOC_FAIL, INJECT_NONE)."""
+        """Failure injection for tests (INJECT_SORT_STALL, INJECT_ALLOC_FAIL, INJECT_MLP_STALL,
+        INJECT_NONE)."""
         self._check(lib().cav_ctx_inject(self.handle, what, count), "cav_ctx_inject")
 
     def set_trace_config(self, block_threads: int = 0, blocks_per_sm: int = 0, batch: int = 0):
@@ -496,7 +497,7 @@ class ServerStats(ctypes.Structure):
 
 
 JOB_PENDING, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
-INJECT_NONE, INJECT_SORT_STALL, INJECT_ALLOC_FAIL = 0, 1, 2
+INJECT_NONE, INJECT_SORT_STALL, INJECT_ALLOC_FAIL, INJECT_MLP_STALL = 0, 1, 2, 3
 SERVE_MERGED, SERVE_SEQUENTIAL = 0, 1
 
 

@@ -301,12 +301,16 @@ cav_status cav_ctx_inject(cav_ctx* ctx, int what, int count) {
         case CAV_INJECT_NONE:
             ctx->inject_sort_stall = 0;
             ctx->inject_alloc_fail = 0;
+            ctx->inject_mlp_stall = 0;
             return CAV_OK;
         case CAV_INJECT_SORT_STALL:
             ctx->inject_sort_stall = count > 0 ? 1 : 0;
             return CAV_OK;
         case CAV_INJECT_ALLOC_FAIL:
             ctx->inject_alloc_fail = count;
+            return CAV_OK;
+        case CAV_INJECT_MLP_STALL:
+            ctx->inject_mlp_stall = count > 0 ? 1 : 0;
             return CAV_OK;
         default:
             return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_ctx_inject: unknown failure");

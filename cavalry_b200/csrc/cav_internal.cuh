@@ -124,10 +124,11 @@ struct cav_ctx {
     int trace_stack = 0;  // 64 selects the short traversal stack for trees known to be shallow
     // bounded device-side waits (cav_ctx_set_limits)
     uint32_t max_trace_steps = 1u << 22;     // node + triangle visits allowed one ray
-    uint64_t sort_wait_ns = 2000000000ull;  // a sort tile's look-back wait before it gives up
+    uint64_t sort_wait_ns = 2000000000ull;  // a sort tile's look-back wait, and a tcgen05 completion wait
     // failure injection for tests (cav_ctx_inject); lanes of a server read them concurrently
     std::atomic<int> inject_sort_stall{0};
     std::atomic<int> inject_alloc_fail{0};  // k > 0: the k-th next device allocation fails
+    std::atomic<int> inject_mlp_stall{0};   // the tcgen05 MLP forward skips each group's first commit
     // launch configuration of the fast (compressed 8-wide) mode (0 = defaults)
     int wide_block = 0;
     int wide_batch = 0;

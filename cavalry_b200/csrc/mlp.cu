@@ -370,16 +370,18 @@ __global__ void __launch_bounds__(kFwdThreads) k_forward(const float* __restrict
 // exponentials per sample overlap the MMA latencies; inputs are loaded two tiles ahead.
 // The last layer's rows are staged in H and written out as one contiguous block.
 //
-// Waits are bounded: a warpgroup whose commit does not arrive within kWaitNs sets bit 1 of
-// the error word, waits once more (bounded) for the MMAs it issued, and stops; TMEM is
-// freed on every path.
+// Waits are bounded: a warpgroup whose commit does not arrive within the context's wait
+// limit (cav_ctx_set_limits) sets bit 1 of the error word, waits once more (bounded) for the
+// MMAs it issued, and stops; the outcome of a wait is agreed over the group by a reducing
+// barrier, so the group's collective TMEM loads and barriers stay uniform; TMEM is freed on
+// every path.  kStall (failure injection) issues nothing for each group's first layer, so its
+// wait runs out.
 namespace umma {
 
 constexpr int kM = 128;        // samples per tile = UMMA M = TMEM lanes
 constexpr int kGroups = 3;     // warpgroups (independent tile streams) per CTA
 constexpr int kThreads = 128 * kGroups;
 constexpr int kTmemCols = 256;  // one 64-column FP32 accumulator per warpgroup, rounded up to a power of two
-constexpr uint64_t kWaitNs = 1000000000ull;
 constexpr int kErrWait = 1;
 
 __host__ __device__ constexpr int w_at(int l) {  // byte offset of layer l's weights
@@ -446,7 +448,7 @@ __device__ __forceinline__ uint64_t now_ns() {
     return t;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
     uint64_t t0 = 0;
     for (;;) {
         uint32_t done;
@@ -458,7 +460,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         if (done) return true;
         const uint64_t t = now_ns();
         if (t0 == 0) t0 = t;
-        else if (t - t0 > kWaitNs) return false;
+        else if (t - t0 > limit_ns) return false;
     }
 }
 
@@ -532,10 +534,10 @@ __device__ __forceinline__ void build_features(unsigned char* F, int m, const fl
     }
 }
 
-template <bool kStore>
+template <bool kStore, bool kStall>
 __global__ void __launch_bounds__(umma::kThreads, 1)
     k_forward_umma(const float* __restrict__ in, int64_t n, const __nv_bfloat16* __restrict__ img,
-                   const float* __restrict__ params, float* __restrict__ out, Acts acts, int* err) {
+                   const float* __restrict__ params, float* __restrict__ out, Acts acts, int* err, uint64_t wait_ns) {
     using namespace umma;
     extern __shared__ __align__(16) unsigned char smem[];  // no-swizzle operands need 16-byte alignment
     __shared__ uint32_t tmem_slot;
@@ -590,18 +592,21 @@ __global__ void __launch_bounds__(umma::kThreads, 1)
         return (kStore && rr < n) ? acts.x0 + rr * kF0 : nullptr;
     };
     // Layer l's UMMAs on the operand the group just wrote, issued by one thread.
+    bool first_issue = true;
     auto issue = [&](int l) {
         fence_before();      // this thread's TMEM reads, before the MMAs overwrite the accumulator
         fence_async_smem();  // its generic-proxy operand writes, before the tensor core reads them
         group_sync(g);
-        if (m == 0) {
+        const bool skip = kStall && first_issue;
+        first_issue = false;
+        if (m == 0 && !skip) {
             if (l == 0) issue_layer<kF0, kH>(f_s, w_s + w_at(0), tmem, bar);
             else if (l < 3) issue_layer<kH, kH>(h_s, w_s + w_at(l), tmem, bar);
             else issue_layer<kH, kOut>(h_s, w_s + w_at(3), tmem, bar);
         }
     };
     auto wait = [&]() -> bool {
-        const bool ok = group_all(g, mbar_wait(bar, phase));
+        const bool ok = group_all(g, mbar_wait(bar, phase, wait_ns));
         if (ok) {
             phase ^= 1;
             fence_after();
@@ -693,7 +698,7 @@ __global__ void __launch_bounds__(umma::kThreads, 1)
     }
     if (!ok) {
         if (m == 0) atomicOr(err, kErrWait);
-        mbar_wait(bar, phase);  // the MMAs this group issued, once more with the same bound
+        mbar_wait(bar, phase, wait_ns);  // the MMAs this group issued, once more with the same bound
     }
     fence_before();
     __syncthreads();
@@ -922,9 +927,12 @@ int umma_grid(cav_ctx* ctx, int64_t n) {
 template <bool kStore>
 cav_status launch_forward(cav_mlp* m, const float* in, int64_t n, float* out, Acts acts, cudaStream_t s) {
     cav_ctx* ctx = m->ctx;
-    if (m->kernel == CAV_MLP_KERNEL_TCGEN05)
-        k_forward_umma<kStore><<<umma_grid(ctx, n), umma::kThreads, umma::kSmem, s>>>(in, n, m->d_img, m->d_params, out,
-                                                                                    acts, ctx->d_error + 4);
+    if (m->kernel == CAV_MLP_KERNEL_TCGEN05 && ctx->inject_mlp_stall.load())
+        k_forward_umma<kStore, true><<<umma_grid(ctx, n), umma::kThreads, umma::kSmem, s>>>(
+            in, n, m->d_img, m->d_params, out, acts, ctx->d_error + 4, ctx->sort_wait_ns);
+    else if (m->kernel == CAV_MLP_KERNEL_TCGEN05)
+        k_forward_umma<kStore, false><<<umma_grid(ctx, n), umma::kThreads, umma::kSmem, s>>>(
+            in, n, m->d_img, m->d_params, out, acts, ctx->d_error + 4, ctx->sort_wait_ns);
     else
         k_forward<kStore><<<fwd_grid(ctx, n, kFwdThreads), kFwdThreads, kSmemBytes, s>>>(in, n, m->d_img, m->d_params,
                                                                                           out, acts);
@@ -1009,8 +1017,10 @@ cav_status cav_mlp_create(cav_ctx* ctx, uint64_t seed, cav_mlp** out) {
         cudaFuncSetAttribute(k_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
         cudaFuncSetAttribute(k_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
         cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-        cudaFuncSetAttribute(k_forward_umma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
-        cudaFuncSetAttribute(k_forward_umma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
+        cudaFuncSetAttribute(k_forward_umma<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
+        cudaFuncSetAttribute(k_forward_umma<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
+        cudaFuncSetAttribute(k_forward_umma<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
+        cudaFuncSetAttribute(k_forward_umma<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
         attr = true;
     }
     auto* m = new cav_mlp();

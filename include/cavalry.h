@@ -55,7 +55,8 @@ cav_status cav_sync_check(cav_ctx* ctx, void* stream);
 
 /* Bounds of the device-side waits of this context (no wait in any kernel is unbounded):
  *   sort_wait_s     : how long a radix-sort tile waits for its predecessors' published
- *                     digit counts before it gives up (<= 0: 2 s);
+ *                     digit counts before it gives up, and how long the tcgen05 MLP
+ *                     forward waits for a layer's tensor-core completion (<= 0: 2 s);
  *   max_trace_steps : node + triangle visits one ray may take before the traversal stops it
  *                     (prim_id -2 / occluded 2) (<= 0: 2^22).
  * Either ends in CAV_ERR_TIMEOUT from cav_sync_check; the context stays usable. */
@@ -68,8 +69,12 @@ cav_status cav_ctx_set_limits(cav_ctx* ctx, double sort_wait_s, int64_t max_trac
  *   CAV_INJECT_ALLOC_FAIL: the count-th next device allocation made for this context (build
  *     arenas and scratch, scene uploads, render path state, server job buffers) fails once,
  *     and the call that made it returns CAV_ERR_OUT_OF_MEMORY (the others succeed);
- *   CAV_INJECT_NONE clears both.  Nothing here faults, traps or hangs the device. */
-enum { CAV_INJECT_NONE = 0, CAV_INJECT_SORT_STALL = 1, CAV_INJECT_ALLOC_FAIL = 2 };
+ *   CAV_INJECT_MLP_STALL (count > 0 on, 0 off): in the tcgen05 MLP forward, each warpgroup
+ *     issues no MMA and no commit for its first tile, so its bounded completion wait runs
+ *     out; the call ends with CAV_ERR_TIMEOUT from cav_sync_check and outputs that are not
+ *     meaningful;
+ *   CAV_INJECT_NONE clears them all.  Nothing here faults, traps or hangs the device. */
+enum { CAV_INJECT_NONE = 0, CAV_INJECT_SORT_STALL = 1, CAV_INJECT_ALLOC_FAIL = 2, CAV_INJECT_MLP_STALL = 3 };
 cav_status cav_ctx_inject(cav_ctx* ctx, int what, int count);
 
 /*

@@ -4,6 +4,9 @@ the kernels' own checks turn into an error status (no fault, trap or hang is pro
 * A vertex index outside [0, num_vertices) is flagged by the build's leaf-box pass (no load
   leaves the position array) and reported as CAV_ERR_INVALID_ARGUMENT by cav_sync_check;
   the context stays usable and the next build of valid input is exact.
+* Bounded waits (sort look-back, tcgen05 completion) are made to run out by injected stalls
+  that withhold what they wait for; the traversal step limit by a small limit.
+* Device allocations fail by injection at a chosen point.
 """
 import numpy as np
 import pytest
@@ -194,5 +197,38 @@ def test_injected_allocation_failure_in_build_and_render(fail, tmp_path):
         s1, w1, _ = sc.render()
         assert np.array_equal(w0, w1) and np.allclose(s0, s1, rtol=2e-5, atol=1e-6)
         sc.free()
+    finally:
+        ctx.close()
+
+
+def test_mlp_completion_wait_runs_out_and_reports():
+    """CAV_INJECT_MLP_STALL: every warpgroup of the tcgen05 forward issues no MMA and no
+    commit for its first tile, so its completion wait (bounded at 50 ms here) runs out.  The
+    forward returns, cav_sync_check reports CAV_ERR_TIMEOUT, and with the injection cleared
+    the same network's outputs equal the mma.sync kernel's within their usual agreement."""
+    import torch
+
+    import cavalry_b200 as cav
+
+    ctx = cav.Context(0)
+    try:
+        net = cav.Mlp(ctx, seed=3, kernel=cav.MLP_KERNEL_TCGEN05)
+        ref = cav.Mlp(ctx, seed=3, kernel=cav.MLP_KERNEL_MMA_SYNC)
+        x = torch.rand((20000, 5), device="cuda", generator=torch.Generator("cuda").manual_seed(4))
+        want = ref.forward(x).cpu().numpy()
+        ctx.set_limits(sort_wait_s=0.05)
+        ctx.inject(cav.INJECT_MLP_STALL, 1)
+        net.forward(x)
+        with pytest.raises(cav.CavError) as e:
+            ctx.sync_check()
+        assert e.value.status == CAV_ERR_TIMEOUT
+        ctx.inject(cav.INJECT_NONE)
+        ctx.set_limits()
+        got = net.forward(x).cpu().numpy()
+        ctx.sync_check()
+        scale = np.abs(want).mean()
+        assert np.abs(got - want).max() <= 5e-3 * scale
+        net.free()
+        ref.free()
     finally:
         ctx.close()
