@@ -857,6 +857,225 @@ __global__ void __launch_bounds__(128) k_weight_grad(const __nv_bfloat16* __rest
     if (threadIdx.x < M) atomicAdd(db + threadIdx.x, bsum);
 }
 
+// ---------------------------------------------------------------- tcgen05 weight gradients
+// All four layers' weight and bias gradients in one pass over the samples.  CTA b reduces a
+// contiguous range of samples into TMEM and writes its partial sums to part[b][kParams];
+// k_wgrad_reduce adds the partials (a fixed order: the gradient is deterministic).
+//
+// With the samples as the reduction dimension K, layer l's gradient transposed is
+// dW_l^T[in][out] = sum_s X_l[s][in] dY_l[s][out]: an UMMA with A = X_l (M = inputs) and
+// B = dY_l (N = outputs), both stored sample-major, i.e. MN-major operands.  Staged in shared
+// memory without swizzle, an operand is a row of "blocks", one per 8 consecutive features:
+// a block holds those 8 features (16 bytes) of each of the stage's kS samples, 16 bytes
+// apart (so the 8-sample K groups are 128 bytes apart, the descriptor's leading offset, and
+// blocks kS * 16 bytes apart, its stride offset).  M must be 128, so the layers share tiles
+// and the off-diagonal products are discarded (the tensor core is far from busy here):
+//   G1: A = X0 features 0..127             B = dY0 (64)              -> dW0[:, 0:128]
+//   G2: A = [X1 ; X2]                      B = [dY1 | dY2] (128)     -> dW1, dW2 (diagonal)
+//   G3: A = [X3 ; X0 128..159 ; 1 ; 0]     B = [dY3 | dY0] (96)      -> dW3, dW0[:, 128:160],
+//                                                                       row 96: db3, db0
+//   G4: A = G3's A                         B = [dY1 | dY2]           -> row 96: db1, db2
+// where row 96 of G3's A is 1 for every sample (its padding samples have dY = 0).
+namespace wgrad {
+constexpr int kS = 64;          // samples per stage
+constexpr int kBlk = kS * 16;   // one block: 8 features of kS samples
+// block index of each operand within a stage
+constexpr int kA1 = 0;          // X0 features 0..127 (16 blocks)
+constexpr int kA2 = 16;         // X1 (8), X2 (8)
+constexpr int kA3 = 32;         // X3 (8), X0 features 128..159 (4), the ones row's block, 3 zero blocks
+constexpr int kOnes = kA3 + 12;
+constexpr int kB3 = 48;         // dY3 (4) followed by dY0 (8): G3's B; dY0 alone is G1's B
+constexpr int kB1 = kB3 + 4;
+constexpr int kB2 = 60;         // dY1 (8), dY2 (8)
+constexpr int kBlocks = 76;
+constexpr int kStage = kBlocks * kBlk;  // 77,824 bytes
+constexpr int kStages = 2;
+constexpr int kSmem = kStages * kStage;
+static_assert(kSmem <= 227 * 1024, "weight-gradient stages exceed the shared-memory limit");
+// TMEM columns of the four accumulators (512 allocated)
+constexpr int kT1 = 0, kT2 = 64, kT3 = 192, kT4 = 288, kCols = 512;
+constexpr int kThreads = 128;
+
+// instruction descriptor: FP32 accumulate, BF16 A and B, both MN-major, M = 128, N = n
+__host__ __device__ constexpr uint32_t idesc_mn(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(umma::kM >> 4) << 24);
+}
+
+__device__ __forceinline__ void cp16(uint32_t dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+}  // namespace wgrad
+
+__global__ void __launch_bounds__(wgrad::kThreads, 1)
+    k_wgrad_umma(Acts acts, Grads grads, int64_t n, int64_t per, float* __restrict__ part, int* err, uint64_t wait_ns) {
+    using namespace wgrad;
+    using umma::smem_u32;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t tmem_slot;
+    __shared__ __align__(8) uint64_t bars[kStages];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t s_begin = (int64_t)blockIdx.x * per;
+    const int64_t s_end = s_begin + per < n ? s_begin + per : n;
+    const int nstages = (int)((s_end - s_begin + kS - 1) / kS);
+    // the constant blocks of every stage buffer: the ones row (feature 0 of its block) and zeros
+    for (int i = tid; i < kStages * 4 * kS; i += kThreads) {
+        const int b = i / (4 * kS), blk = kOnes + (i / kS) % 4, s = i % kS;
+        *reinterpret_cast<uint4*>(smem + b * kStage + blk * kBlk + s * 16) =
+            make_uint4(blk == kOnes ? 0x3f80u : 0u, 0u, 0u, 0u);  // BF16 1.0 in the low half
+    }
+    if (tid < kStages) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[tid])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    umma::fence_async_smem();
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    // one stage's samples [s0, s0 + kS) of this CTA's range into buffer `buf` (zeros past the range)
+    auto stage_in = [&](int buf, int64_t s0) {
+        const uint32_t base = smem_u32(smem + buf * kStage);
+        const int cnt = (int)(s_end - s0 < kS ? s_end - s0 : kS);
+        auto put = [&](const __nv_bfloat16* arr, int width, int chunks, int blk0, int split, int blk1) {
+            for (int i = tid; i < kS * chunks; i += kThreads) {
+                const int s = i / chunks, c = i % chunks;
+                const int blk = c < split ? blk0 + c : blk1 + (c - split);
+                const bool valid = s < cnt;
+                cp16(base + blk * kBlk + s * 16, arr + (s0 + (valid ? s : 0)) * width + c * 8, valid);
+            }
+        };
+        put(acts.x0, kF0, kF0 / 8, kA1, 16, kA3 + 8);
+        put(acts.x1, kH, kH / 8, kA2, 8, 0);
+        put(acts.x2, kH, kH / 8, kA2 + 8, 8, 0);
+        put(acts.x3, kH, kH / 8, kA3, 8, 0);
+        put(grads.d0, kH, kH / 8, kB1, 8, 0);
+        put(grads.d1, kH, kH / 8, kB2, 8, 0);
+        put(grads.d2, kH, kH / 8, kB2 + 8, 8, 0);
+        put(grads.d3, kOut, kOut / 8, kB3, 4, 0);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    uint32_t parity[kStages] = {0, 0};
+    bool ok = true;
+    int fail_bar = -1;  // the barrier whose bounded wait ran out (its MMAs may still be running)
+    if (nstages > 0) stage_in(0, s_begin);
+    for (int st = 0; st < nstages && ok; ++st) {
+        const int buf = st % kStages;
+        if (st + 1 < nstages) {
+            const int nb = (st + 1) % kStages;
+            if (st + 1 >= kStages) {  // the MMAs that read buffer nb (stage st - 1) must be done
+                ok = __syncthreads_and(umma::mbar_wait(smem_u32(&bars[nb]), parity[nb], wait_ns));
+                if (!ok) {
+                    fail_bar = nb;
+                    break;
+                }
+                parity[nb] ^= 1;
+            }
+            stage_in(nb, s_begin + (int64_t)(st + 1) * kS);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        umma::fence_async_smem();  // the staged operands, before the tensor core reads them
+        __syncthreads();
+        if (tid == 0) {
+            umma::fence_after();
+            const uint32_t b = smem_u32(smem + buf * kStage);
+            auto desc = [&](int blk, int j) { return umma::sdesc(b + blk * kBlk + j * 256, 128, kBlk); };
+#pragma unroll
+            for (int j = 0; j < kS / 16; ++j) {
+                const uint32_t acc = (st > 0 || j > 0) ? 1u : 0u;
+                umma::mma_bf16(tmem + kT1, desc(kA1, j), desc(kB1, j), idesc_mn(64), acc);
+                umma::mma_bf16(tmem + kT2, desc(kA2, j), desc(kB2, j), idesc_mn(128), acc);
+                umma::mma_bf16(tmem + kT3, desc(kA3, j), desc(kB3, j), idesc_mn(96), acc);
+                umma::mma_bf16(tmem + kT4, desc(kA3, j), desc(kB2, j), idesc_mn(128), acc);
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&bars[buf]))
+                         : "memory");
+        }
+    }
+    // the last stage's MMAs (every earlier commit completes before it)
+    if (ok && nstages > 0) {
+        const int lb = (nstages - 1) % kStages;
+        ok = __syncthreads_and(umma::mbar_wait(smem_u32(&bars[lb]), parity[lb], wait_ns));
+        if (!ok) fail_bar = lb;
+    }
+    if (ok) {
+        umma::fence_after();
+        float* P = part + (int64_t)blockIdx.x * kParams;
+        const int row = 32 * warp + lane;  // TMEM lane = A row
+        const uint32_t tl = tmem + ((uint32_t)(32 * warp) << 16);
+        uint32_t v[32];
+        auto load = [&](int col) {
+            umma::tmem_ld<32>(tl + col, v);
+            umma::tmem_wait_ld();
+        };
+        const bool empty = nstages == 0;  // no samples: the partial sums are zero
+        auto val = [&](int j) { return empty ? 0.f : __uint_as_float(v[j]); };
+        // G1: dW0[o][row], rows 0..127
+        for (int c = 0; c < 64; c += 32) {
+            load(kT1 + c);
+            for (int j = 0; j < 32; ++j) P[w_off(0) + (c + j) * kF0 + row] = val(j);
+        }
+        // G2: rows 0..63 x columns 0..63 -> dW1, rows 64..127 x columns 64..127 -> dW2
+        for (int c = 0; c < 64; c += 32) {
+            load(kT2 + c + (warp < 2 ? 0 : 64));
+            for (int j = 0; j < 32; ++j)
+                P[warp < 2 ? w_off(1) + (c + j) * kH + row : w_off(2) + (c + j) * kH + row - 64] = val(j);
+        }
+        // G3: rows 0..63 x columns 0..31 -> dW3; rows 64..95 x columns 32..95 -> dW0 inputs 128..159;
+        // row 96 -> db3 (columns 0..31), db0 (columns 32..95)
+        if (warp < 2) {
+            load(kT3);
+            for (int j = 0; j < 32; ++j) P[w_off(3) + j * kH + row] = val(j);
+        } else if (warp == 2) {
+            for (int c = 0; c < 64; c += 32) {
+                load(kT3 + 32 + c);
+                for (int j = 0; j < 32; ++j) P[w_off(0) + (c + j) * kF0 + 128 + row - 64] = val(j);
+            }
+        } else {
+            for (int c = 0; c < 96; c += 32) {
+                load(kT3 + c);
+                if (lane == 0)
+                    for (int j = 0; j < 32; ++j) P[c + j < 32 ? b_off(3) + c + j : b_off(0) + c + j - 32] = val(j);
+            }
+            // G4: row 96 -> db1 (columns 0..63), db2 (columns 64..127)
+            for (int c = 0; c < 128; c += 32) {
+                load(kT4 + c);
+                if (lane == 0)
+                    for (int j = 0; j < 32; ++j) P[c + j < 64 ? b_off(1) + c + j : b_off(2) + c + j - 64] = val(j);
+            }
+        }
+    } else if (tid == 0) {
+        atomicOr(err, umma::kErrWait);
+        if (fail_bar >= 0) umma::mbar_wait(smem_u32(&bars[fail_bar]), parity[fail_bar], wait_ns);  // once more
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");  // no copy may land after the CTA ends
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_slot), "r"(kCols) : "memory");
+    }
+}
+
+// grads[p] = sum over the CTAs' partials, in CTA order
+__global__ void k_wgrad_reduce(const float* __restrict__ part, int blocks, float* __restrict__ grads) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kParams) return;
+    float s = 0.f;
+    for (int b = 0; b < blocks; ++b) s += part[(int64_t)b * kParams + p];
+    grads[p] = s;
+}
+
 __global__ void k_adam(float* p, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
                        float c1, float c2) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -907,6 +1126,7 @@ struct cav_mlp {
     float* dout = nullptr;
     cav::mlp::Acts acts{};
     cav::mlp::Grads grads{};
+    float* wpart = nullptr;  // per-CTA partial weight gradients of the tcgen05 reduction, num_sms x params
 };
 
 namespace {
@@ -944,7 +1164,8 @@ cav_status ensure_scratch(cav_mlp* m, int64_t n, cudaStream_t s) {
     if (n <= m->cap) return CAV_OK;
     if (m->scratch) cudaFreeAsync(m->scratch, s);
     m->scratch = nullptr;
-    const size_t bytes = (size_t)n * (4 * kOut * 2 + 2 * (kF0 + 3 * kH) + 2 * (kOut + 3 * kH)) + 8 * 256;
+    const size_t bytes = (size_t)n * (4 * kOut * 2 + 2 * (kF0 + 3 * kH) + 2 * (kOut + 3 * kH)) +
+                         (size_t)m->ctx->num_sms * kParams * 4 + 9 * 256;
     CAV_CUDA(m->ctx, cudaMallocAsync(&m->scratch, bytes, s));
     unsigned char* p = (unsigned char*)m->scratch;
     auto carve = [&](size_t b) {
@@ -962,6 +1183,7 @@ cav_status ensure_scratch(cav_mlp* m, int64_t n, cudaStream_t s) {
     m->grads.d2 = (__nv_bfloat16*)carve(2ull * kH * n);
     m->grads.d1 = (__nv_bfloat16*)carve(2ull * kH * n);
     m->grads.d0 = (__nv_bfloat16*)carve(2ull * kH * n);
+    m->wpart = (float*)carve(4ull * kParams * m->ctx->num_sms);
     m->cap = n;
     return CAV_OK;
 }
@@ -984,12 +1206,22 @@ cav_status compute_grads(cav_mlp* m, const float* in, const float* dirs, const f
     const int grid = fwd_grid(ctx, n, 128);
     k_loss<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m->out, dirs, w, n, m->dout, m->d_loss);
     k_backward<<<grid, 128, kSmemBytes, s>>>(m->dout, n, m->d_img, m->d_params, m->acts, m->grads);
-    const int wg = (int)std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, (int64_t)ctx->num_sms * 4));
     float* G = m->d_grads;
-    k_weight_grad<kOut, kH><<<wg, 128, 0, s>>>(m->grads.d3, m->acts.x3, n, G + w_off(3), G + b_off(3));
-    k_weight_grad<kH, kH><<<wg, 128, 0, s>>>(m->grads.d2, m->acts.x2, n, G + w_off(2), G + b_off(2));
-    k_weight_grad<kH, kH><<<wg, 128, 0, s>>>(m->grads.d1, m->acts.x1, n, G + w_off(1), G + b_off(1));
-    k_weight_grad<kH, kF0><<<wg, 128, 0, s>>>(m->grads.d0, m->acts.x0, n, G + w_off(0), G + b_off(0));
+    if (m->kernel == CAV_MLP_KERNEL_TCGEN05) {
+        // one CTA per SM, each over a contiguous range of samples (a multiple of 16), then the
+        // partial sums added in CTA order
+        const int64_t per = std::max<int64_t>(16, ((n + ctx->num_sms - 1) / ctx->num_sms + 15) / 16 * 16);
+        const int blocks = (int)std::max<int64_t>(1, (n + per - 1) / per);
+        k_wgrad_umma<<<blocks, wgrad::kThreads, wgrad::kSmem, s>>>(m->acts, m->grads, n, per, m->wpart,
+                                                                   ctx->d_error + 4, ctx->sort_wait_ns);
+        k_wgrad_reduce<<<(kParams + 255) / 256, 256, 0, s>>>(m->wpart, blocks, G);
+    } else {
+        const int wg = (int)std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, (int64_t)ctx->num_sms * 4));
+        k_weight_grad<kOut, kH><<<wg, 128, 0, s>>>(m->grads.d3, m->acts.x3, n, G + w_off(3), G + b_off(3));
+        k_weight_grad<kH, kH><<<wg, 128, 0, s>>>(m->grads.d2, m->acts.x2, n, G + w_off(2), G + b_off(2));
+        k_weight_grad<kH, kH><<<wg, 128, 0, s>>>(m->grads.d1, m->acts.x1, n, G + w_off(1), G + b_off(1));
+        k_weight_grad<kH, kF0><<<wg, 128, 0, s>>>(m->grads.d0, m->acts.x0, n, G + w_off(0), G + b_off(0));
+    }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;
 }
@@ -1021,6 +1253,7 @@ cav_status cav_mlp_create(cav_ctx* ctx, uint64_t seed, cav_mlp** out) {
         cudaFuncSetAttribute(k_forward_umma<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
         cudaFuncSetAttribute(k_forward_umma<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
         cudaFuncSetAttribute(k_forward_umma<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmem);
+        cudaFuncSetAttribute(k_wgrad_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, wgrad::kSmem);
         attr = true;
     }
     auto* m = new cav_mlp();

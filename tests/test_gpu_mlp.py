@@ -117,6 +117,36 @@ def test_gradients_match_oracle(ctx, kernel):
             assert err < 3e-2, (k, err)
 
 
+@pytest.mark.parametrize("n", [37, 1000, 16384, 100_003])
+def test_tcgen05_and_mma_sync_gradients_agree(ctx, n):
+    """The weight gradients of the tcgen05 reduction (per-CTA TMEM partial sums over sample
+    ranges, then a fixed-order sum) against the mma.sync kernel's (FP32 atomics) on the same
+    batch: both sum the same BF16 products in FP32, so each layer's weights and biases agree
+    to FP32 summation order (relative L2 1e-3, allowing a rare activation whose BF16 rounding
+    differs between the two forward kernels).  n = 37: one partial stage in one CTA; 1000:
+    a stage per CTA; 16,384: the training batch; 100,003: 11 stages per CTA, the last ragged."""
+    import cavalry_b200 as cav
+
+    a = cav.Mlp(ctx, seed=6, kernel=cav.MLP_KERNEL_TCGEN05)
+    b = cav.Mlp(ctx, seed=6, kernel=cav.MLP_KERNEL_MMA_SYNC)
+    rng = np.random.default_rng(9)
+    p = a.params()
+    p[-32:] = rng.normal(0, 0.5, 32).astype(np.float32)
+    a.set_params(p)
+    b.set_params(p)
+    x, d, w = batch(n, 3)
+    ga, la = a.gradients(cuda(x), cuda(d), cuda(w))
+    gb, lb = b.gradients(cuda(x), cuda(d), cuda(w))
+    ctx.sync_check()
+    assert abs(la - lb) <= 1e-4 * abs(lb)
+    for k, (sw, sb) in enumerate(layer_slices()):
+        for s in (sw, sb):
+            err = np.linalg.norm(ga[s] - gb[s]) / max(np.linalg.norm(gb[s]), 1e-12)
+            assert err < 1e-3, (k, err)
+    a.free()
+    b.free()
+
+
 def test_mixture_pdf_and_sampling(ctx):
     import torch
 
