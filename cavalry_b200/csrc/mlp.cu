@@ -1067,13 +1067,26 @@ __global__ void __launch_bounds__(wgrad::kThreads, 1)
     }
 }
 
-// grads[p] = sum over the CTAs' partials, in CTA order
-__global__ void k_wgrad_reduce(const float* __restrict__ part, int blocks, float* __restrict__ grads) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= kParams) return;
+// grads[p] = sum over the CTAs' partials: a block per 32 parameters, warp w summing the
+// partials b = w, w + 8, ... (a lane per parameter, 128-byte loads), the 8 warp sums then
+// added in warp order, so the result does not depend on scheduling.
+constexpr int kReduceWarps = 8;
+__global__ void __launch_bounds__(32 * kReduceWarps) k_wgrad_reduce(const float* __restrict__ part, int blocks,
+                                                                    float* __restrict__ grads) {
+    __shared__ float ws[kReduceWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int p = blockIdx.x * 32 + lane;
     float s = 0.f;
-    for (int b = 0; b < blocks; ++b) s += part[(int64_t)b * kParams + p];
-    grads[p] = s;
+    if (p < kParams)
+        for (int b = warp; b < blocks; b += kReduceWarps) s += part[(int64_t)b * kParams + p];
+    ws[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && p < kParams) {
+        float t = 0.f;
+#pragma unroll
+        for (int w = 0; w < kReduceWarps; ++w) t += ws[w][lane];
+        grads[p] = t;
+    }
 }
 
 __global__ void k_adam(float* p, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
@@ -1214,7 +1227,7 @@ cav_status compute_grads(cav_mlp* m, const float* in, const float* dirs, const f
         const int blocks = (int)std::max<int64_t>(1, (n + per - 1) / per);
         k_wgrad_umma<<<blocks, wgrad::kThreads, wgrad::kSmem, s>>>(m->acts, m->grads, n, per, m->wpart,
                                                                    ctx->d_error + 4, ctx->sort_wait_ns);
-        k_wgrad_reduce<<<(kParams + 255) / 256, 256, 0, s>>>(m->wpart, blocks, G);
+        k_wgrad_reduce<<<(kParams + 31) / 32, 32 * kReduceWarps, 0, s>>>(m->wpart, blocks, G);
     } else {
         const int wg = (int)std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, (int64_t)ctx->num_sms * 4));
         k_weight_grad<kOut, kH><<<wg, 128, 0, s>>>(m->grads.d3, m->acts.x3, n, G + w_off(3), G + b_off(3));
