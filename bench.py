@@ -56,7 +56,8 @@ def parse():
                    help="soup workload: BLOCK,CHUNK for the exact traversal instead of the autotuner's pick")
     p.add_argument("--no-reference-cuda", action="store_true",
                    help="soup workload: skip the reference CUDA timings and the config-1 block")
-    p.add_argument("--workload", default="soup", choices=["soup", "render", "serve", "guided", "mlp", "capture"],
+    p.add_argument("--workload", default="soup",
+                   choices=["soup", "render", "serve", "guided", "mlp", "capture", "batch"],
                    help="soup: BVH + 4M closest-hit rays (default); render: the 5.24M-triangle path-traced scene; "
                         "serve: a Poisson stream of render and ray-query jobs, merged server vs sequential loop")
     p.add_argument("--jobs", type=int, default=256, help="jobs in the served stream (serve workload)")
@@ -1115,6 +1116,59 @@ def run_guided(args):
     print(json.dumps(out))
 
 
+# ------------------------------------------------------------------------ batched builds
+def run_batch(args):
+    """Many scenes built at once: `cav_bvh_build_batch` (one launch per LBVH stage over all
+    scenes, treelet rounds per group of scenes, one shared arena) against one `cav_bvh_build`
+    per scene, for three mixes of seeded soups with log-uniform triangle counts, at 0 and 3
+    treelet rounds.  Wall time of the whole build (host call to device completion), min of
+    3 repetitions after a warm-up, inputs resident on the device."""
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    ctx = cav.Context(0)
+    mixes = [(256, 1_000, 30_000), (64, 1_000, 100_000), (16, 10_000, 2_000_000)]
+    rows = []
+    for k, lo, hi in mixes:
+        rng = np.random.default_rng(k)
+        sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), k)).astype(int)
+        data = []
+        for i, nt in enumerate(sizes):
+            pos, idx = scenes.soup(int(nt), seed=100 + i)
+            data.append((torch.from_numpy(pos).cuda(), torch.from_numpy(idx).cuda()))
+        for rounds in (0, 3):
+            def batched():
+                return ctx.build_batch(data, rounds=rounds)
+
+            def single():
+                return [ctx.build(p, i, rounds=rounds) for p, i in data]
+
+            best = {}
+            for name, fn in (("batched", batched), ("one_by_one", single)):
+                t = []
+                for rep in range(4):
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    trees = fn()
+                    torch.cuda.synchronize()
+                    t.append(time.perf_counter() - t0)
+                    ctx.sync_check()
+                    for tr in trees:
+                        tr.free()
+                best[name] = min(t[1:]) * 1e3  # the first repetition warms the allocator
+            rows.append({"scenes": k, "triangles": int(sizes.sum()), "range": [lo, hi], "rounds": rounds,
+                         "batched_ms": round(best["batched"], 2), "one_by_one_ms": round(best["one_by_one"], 2),
+                         "ratio": round(best["one_by_one"] / best["batched"], 2)})
+    print(json.dumps({"metric": "batched BVH build speed-up over one build per scene", "unit": "x",
+                      "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded soups)",
+                      "config": {"workload": "batched_builds_3_mixes", "timing": "wall, min of 3 after one warm-up"},
+                      "rows": rows}))
+
+
 # ------------------------------------------------------------------------ mlp workload
 def run_mlp(args):
     """The learned proposal's kernels alone: forward passes over 4M vertices (--small: 1M)
@@ -1189,6 +1243,8 @@ def main():
     args = parse()
     if args.workload == "mlp":
         run_mlp(args)
+    elif args.workload == "batch":
+        run_batch(args)
     elif args.workload == "guided":
         run_guided(args)
     elif args.workload == "serve":

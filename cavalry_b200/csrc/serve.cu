@@ -2,9 +2,18 @@
 // admitted as they arrive (FIFO, under an HBM budget and a live-job limit), and every tick
 // advances all live jobs of a lane by one bounce with ONE closest-hit and ONE any-hit
 // traversal launch over the merged wavefronts of all of them (trace_*_segments: each
-// segment is one job's rays against its own resident BVH).  Shading stays per job (its own
-// kernels on the lane's stream).  Scenes and their BVHs are resident (cav_scene / cav_bvh
-// handles owned by the caller); path state lives on the device for the job's lifetime.
+// segment is one job's rays against its own BVH).  Shading stays per job (its own kernels
+// on the lane's stream); path state lives on the device for the job's lifetime.
+//
+// Scenes: a job either names a resident scene or tree (cav_scene / cav_bvh handles owned
+// by the caller) or brings its own .pbrt file (cav_server_submit_scene).  Loader threads
+// parse those files as they arrive; the lane that admits such a job uploads its scene
+// stream-ordered, builds the trees of all scenes it admitted in that round with one
+// batched build (per treelet round count), and releases the scene when the job ends.
+// Small renders (at most graph_max_paths paths) are replayed as one CUDA graph of the whole
+// render instead of joining the per-tick merged launches.  Jobs can be cancelled (pending:
+// dropped; running: removed by their lane before its next bounce), and a job whose
+// estimated bytes exceed the HBM budget can be refused at submission.
 //
 // Lanes: a few host threads, each with its own stream and share of the live jobs, tick
 // independently, so the GPU runs one lane's traversal while the other lane's launches
