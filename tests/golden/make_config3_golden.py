@@ -39,4 +39,4 @@ def main(out: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else str(ROOT / "tests" / "golden" / "spheres5m_ref_sub4.npz"))
+    main(sys.argv[1] if len(sys.argv) > 1 else str(ROOT / "tests" / "golden" / "render_spheres5m_sub4.npz"))

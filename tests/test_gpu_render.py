@@ -280,7 +280,7 @@ def test_sample_ranges_sum_to_the_whole_render(ctx, tmp_path):
     ctx.sync_check()
 
 
-CONFIG3 = Path(__file__).resolve().parent / "golden" / "spheres5m_ref_sub4.npz"
+CONFIG3 = Path(__file__).resolve().parent / "golden" / "render_spheres5m_sub4.npz"
 
 
 @pytest.mark.skipif(not CONFIG3.exists(), reason="fixture made by tests/golden/make_config3_golden.py")
