@@ -377,12 +377,21 @@ __global__ void k_leaf_list(const BNode* __restrict__ nodes, int64_t count, int3
 
 // optimizeBVHImpl (Optimization.cu:467-507): one warp per starting leaf; the second
 // arrival at a node optimises the treelet rooted there and continues upwards.
+//
+// Each walker carries the number of leaves under its node (saturated at 7) in the arrival
+// counter: an arrival adds (leaves << 2) | 1, so the second arrival learns its sibling's
+// count.  A subtree of fewer than 7 leaves cannot form a treelet: the reference's formation
+// then expands every internal node of it and gives up without writing anything (with 7 or
+// more leaves an internal node always remains to expand), so such nodes skip formation and
+// the tree is unchanged.  The counter's update is an acquire-release atomic: the lanes'
+// record writes precede it (warp barrier), and the second arrival's reads follow it.
 __device__ void treelet_walk(BNode* nodes, int32_t curr, int32_t count, uint32_t* visited, WarpSmem& S, int* err) {
     const int lane = threadIdx.x & 31;
     if (curr < 0 || curr >= count) {
         if (lane == 0) atomicExch(err, 2);
         return;
     }
+    uint32_t leaves = 1;  // under curr, saturated at 7
     for (;;) {
         if (curr == 0) break;
         int32_t parent = __ldcg(&nodes[curr].parent);
@@ -391,16 +400,21 @@ __device__ void treelet_walk(BNode* nodes, int32_t curr, int32_t count, uint32_t
             return;
         }
         uint32_t old = 0;
-        if (lane == 0) old = atomicAdd(visited + parent, 1u);
+        if (lane == 0)
+            asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+                         : "=r"(old)
+                         : "l"(visited + parent), "r"((leaves << 2) | 1u)
+                         : "memory");
         old = __shfl_sync(kFull, old, 0);
-        if (old != 1) return;  // first arrival stops; the second optimises the parent
-        __threadfence();
+        if ((old & 3u) != 1u) return;  // first arrival stops; the second optimises the parent
+        __syncwarp();
+        leaves = min(7u, leaves + (old >> 2));
         curr = parent;
-        if (!optimize_treelet(nodes, curr, count, S)) {
+        if (leaves >= 7 && !optimize_treelet(nodes, curr, count, S)) {
             if (lane == 0) atomicExch(err, 2);
             return;
         }
-        __threadfence();
+        __syncwarp();
     }
 }
 
