@@ -19,6 +19,8 @@
 //     smaller subsets, so the order between subsets does not change any value).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "cav_internal.cuh"
 
 namespace cav {
@@ -54,6 +56,7 @@ struct WarpSmem {
     float cost[128];
     signed char part[128];
     int leaf_lane[8];
+    float lbox[7][6];  // the treelet leaves' boxes (read by every lane: broadcast)
 };
 
 struct Rec {
@@ -134,17 +137,15 @@ __device__ bool optimize_treelet(BNode* nodes, int32_t root, int32_t count, Warp
     __syncwarp();
 
     // ---- subset areas (Optimization.cu:126-163)
-    float lbox[7][6];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        int src = S.leaf_lane[k];
-        lbox[k][0] = __shfl_sync(kFull, rec.lo_x, src);
-        lbox[k][1] = __shfl_sync(kFull, rec.lo_y, src);
-        lbox[k][2] = __shfl_sync(kFull, rec.lo_z, src);
-        lbox[k][3] = __shfl_sync(kFull, rec.hi_x, src);
-        lbox[k][4] = __shfl_sync(kFull, rec.hi_y, src);
-        lbox[k][5] = __shfl_sync(kFull, rec.hi_z, src);
+    // the leaves' boxes go through shared memory rather than 42 registers per lane (the
+    // walk's occupancy is set by its registers)
+    if (in_treelet && !expanded) {
+        float* b = S.lbox[my_leaf];
+        b[0] = rec.lo_x; b[1] = rec.lo_y; b[2] = rec.lo_z;
+        b[3] = rec.hi_x; b[4] = rec.hi_y; b[5] = rec.hi_z;
     }
+    __syncwarp();
+    const float(&lbox)[7][6] = S.lbox;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         int s = (q << 5) | lane;
@@ -418,19 +419,30 @@ __device__ void treelet_walk(BNode* nodes, int32_t curr, int32_t count, uint32_t
     }
 }
 
-// One warp per block, 32 blocks per SM (64 registers): the walk waits on atomics and
-// dependent loads, so resident warps matter more than registers, and most warps exit after
-// one step (first arrivals), which frees a one-warp block's slot at once, where a larger
-// block holds its slots until its last warp reaches the top.  Measured on 3 rounds over a
-// 1M-triangle soup: 8 warps per block at 98 registers 17.4 ms, at 80 15.0, at 64 11.4;
-// 2 warps per block 9.2; 1 warp 8.3.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 32) k_treelet(BNode* nodes, const int32_t* __restrict__ list,
-                                                                 int64_t n, uint32_t* visited, int* err) {
-    __shared__ WarpSmem smem[kWarpsPerBlock];
-    const int w = threadIdx.x >> 5;
-    int64_t gw = (int64_t)blockIdx.x * kWarpsPerBlock + w;
-    if (gw >= n) return;
-    treelet_walk(nodes, list[gw], (int32_t)(2 * n - 1), visited, smem[w], err);
+// Persistent walkers: a fixed grid of 2-warp blocks, 24 per SM (48 warps at 40 registers),
+// each warp claiming starting leaves from a counter until the list is exhausted.  The walk
+// waits on atomics and dependent loads, so resident walkers matter more than registers,
+// and a persistent warp never waits for a block launch after a first arrival ends its walk.
+// Measured on 3 rounds over a 1M-triangle soup: one launched warp per leaf in 1-warp blocks
+// (32 per SM, 64 registers) 7.14 ms; persistent 1-warp blocks at 64 registers 5.67;
+// 2-warp blocks at 48 registers (40 per SM) 5.46; at 40 registers 5.34, and 5.00 with the
+// leaf boxes in shared memory; at 32 registers (64 per SM) 5.99 (spills).  Claiming 4 or
+// 16 leaves per atomic did not help.
+constexpr int kWalkWarps = 2;
+constexpr int kWalkBlocksPerSm = 24;
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkBlocksPerSm)
+    k_treelet(BNode* nodes, const int32_t* __restrict__ list, int64_t n, uint32_t* visited, int* err, uint32_t* claim) {
+    __shared__ WarpSmem smem[kWalkWarps];
+    WarpSmem& S = smem[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(claim, 1u);
+        i = __shfl_sync(kFull, i, 0);
+        if (i >= (uint32_t)n) return;
+        treelet_walk(nodes, list[i], (int32_t)(2 * n - 1), visited, S, err);
+        __syncwarp();
+    }
 }
 
 // ---- many trees per launch (the batched build): tree k owns leaves [leaf_off[k],
@@ -495,14 +507,15 @@ cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int
                           uint32_t* counter, cudaStream_t s) {
     if (rounds <= 0) return CAV_OK;
     const int64_t count = 2 * n - 1;
-    // counter: the leaf list's positions, in the build's own scratch (builds on different
-    // streams, such as a server's lanes, never share it)
+    // counter[0]: the leaf list's positions, counter[1]: the walkers' claims; both in the
+    // build's own scratch (builds on different streams, such as a server's lanes, never share it)
+    const int64_t grid = std::min<int64_t>(div_up(n, kWalkWarps), (int64_t)ctx->num_sms * kWalkBlocksPerSm);
     for (int r = 0; r < rounds; ++r) {
         CAV_CUDA(ctx, cudaMemsetAsync(visited, 0, sizeof(uint32_t) * count, s));
-        CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), s));
+        CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, 2 * sizeof(uint32_t), s));
         k_leaf_list<<<div_up(count, 256), 256, 0, s>>>(nodes, count, leaf_list, counter);
-        k_treelet<<<div_up(n, kWarpsPerBlock), kWarpsPerBlock * 32, 0, s>>>(nodes, leaf_list, n, visited,
-                                                                          ctx->d_error + 1);
+        k_treelet<<<(unsigned)grid, kWalkWarps * 32, 0, s>>>(nodes, leaf_list, n, visited, ctx->d_error + 1,
+                                                             counter + 1);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;
@@ -515,8 +528,8 @@ cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int
 // 0.5-2M triangles, and launch overhead does not matter there).  Each tree's result is the
 // single-tree one: within a tree the walk is the same, and trees share no nodes.  segs /
 // leaf_off: device tables (K trees, K + 1 leaf offsets), segs_host / leaf_off_host the same
-// on the host; leaf_list holds leaf_off[K] entries, visited 2 leaf_off[K] - K, counters K + 1
-// (per tree leaf-list positions, then one for a tree that runs the single-tree pass).
+// on the host; leaf_list holds leaf_off[K] entries, visited 2 leaf_off[K] - K, counters K + 2
+// (per tree leaf-list positions, then the two of a tree that runs the single-tree pass).
 cav_status treelet_rounds_batch(cav_ctx* ctx, const TreeletSeg* segs, const TreeletSeg* segs_host,
                                 const int64_t* leaf_off, const int64_t* leaf_off_host, int K, int rounds,
                                 int32_t* leaf_list, uint32_t* counters, uint32_t* visited, cudaStream_t s) {
