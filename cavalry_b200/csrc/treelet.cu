@@ -57,6 +57,7 @@ struct WarpSmem {
     signed char part[128];
     int leaf_lane[8];
     float lbox[7][6];  // the treelet leaves' boxes (read by every lane: broadcast)
+    int32_t lrec[7][4];  // and their left, right, prim, is_leaf
 };
 
 struct Rec {
@@ -137,12 +138,14 @@ __device__ bool optimize_treelet(BNode* nodes, int32_t root, int32_t count, Warp
     __syncwarp();
 
     // ---- subset areas (Optimization.cu:126-163)
-    // the leaves' boxes go through shared memory rather than 42 registers per lane (the
-    // walk's occupancy is set by its registers)
+    // the leaves' records go through shared memory rather than registers (the walk's
+    // occupancy is set by its registers)
     if (in_treelet && !expanded) {
         float* b = S.lbox[my_leaf];
         b[0] = rec.lo_x; b[1] = rec.lo_y; b[2] = rec.lo_z;
         b[3] = rec.hi_x; b[4] = rec.hi_y; b[5] = rec.hi_z;
+        int32_t* r = S.lrec[my_leaf];
+        r[0] = rec.left; r[1] = rec.right; r[2] = rec.prim; r[3] = rec.is_leaf;
     }
     __syncwarp();
     const float(&lbox)[7][6] = S.lbox;
@@ -289,18 +292,17 @@ __device__ bool optimize_treelet(BNode* nodes, int32_t root, int32_t count, Warp
 
     // ---- new records (Optimization.cu:400-461)
     int leaf_id = (in_treelet && !exp_r) ? __ffs(my_subset) - 1 : 0;
-    int src = S.leaf_lane[leaf_id];
     Rec o;
-    o.lo_x = __shfl_sync(kFull, rec.lo_x, src);
-    o.lo_y = __shfl_sync(kFull, rec.lo_y, src);
-    o.lo_z = __shfl_sync(kFull, rec.lo_z, src);
-    o.hi_x = __shfl_sync(kFull, rec.hi_x, src);
-    o.hi_y = __shfl_sync(kFull, rec.hi_y, src);
-    o.hi_z = __shfl_sync(kFull, rec.hi_z, src);
-    o.left = __shfl_sync(kFull, rec.left, src);
-    o.right = __shfl_sync(kFull, rec.right, src);
-    o.prim = __shfl_sync(kFull, rec.prim, src);
-    o.is_leaf = __shfl_sync(kFull, rec.is_leaf, src);
+    o.lo_x = lbox[leaf_id][0];
+    o.lo_y = lbox[leaf_id][1];
+    o.lo_z = lbox[leaf_id][2];
+    o.hi_x = lbox[leaf_id][3];
+    o.hi_y = lbox[leaf_id][4];
+    o.hi_z = lbox[leaf_id][5];
+    o.left = S.lrec[leaf_id][0];
+    o.right = S.lrec[leaf_id][1];
+    o.prim = S.lrec[leaf_id][2];
+    o.is_leaf = S.lrec[leaf_id][3];
     int32_t child_l = __shfl_sync(kFull, nid, cl_lane);
     int32_t child_r = __shfl_sync(kFull, nid, cr_lane);
 
@@ -425,9 +427,9 @@ __device__ void treelet_walk(BNode* nodes, int32_t curr, int32_t count, uint32_t
 // and a persistent warp never waits for a block launch after a first arrival ends its walk.
 // Measured on 3 rounds over a 1M-triangle soup: one launched warp per leaf in 1-warp blocks
 // (32 per SM, 64 registers) 7.14 ms; persistent 1-warp blocks at 64 registers 5.67;
-// 2-warp blocks at 48 registers (40 per SM) 5.46; at 40 registers 5.34, and 5.00 with the
-// leaf boxes in shared memory; at 32 registers (64 per SM) 5.99 (spills).  Claiming 4 or
-// 16 leaves per atomic did not help.
+// 2-warp blocks at 48 registers (40 per SM) 5.46; at 40 registers 5.34, 5.00 with the leaf
+// boxes in shared memory, 4.93 with the leaf records there too; at 32 registers (64 per SM)
+// 5.99 (spills).  Claiming 4 or 16 leaves per atomic did not help.
 constexpr int kWalkWarps = 2;
 constexpr int kWalkBlocksPerSm = 24;
 __global__ void __launch_bounds__(kWalkWarps * 32, kWalkBlocksPerSm)
