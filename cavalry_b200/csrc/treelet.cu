@@ -16,7 +16,10 @@
 //     global memory without __syncwarp, :445-460; its converged values are the same);
 //   * subsets of 2..5 leaves are processed grouped by size instead of by the
 //     reference's hand-packed 5-round table (each subset's result depends only on the
-//     smaller subsets, so the order between subsets does not change any value).
+//     smaller subsets, so the order between subsets does not change any value);
+//   * a node whose subtree holds fewer than 7 leaves is not visited by the formation at
+//     all (the reference's formation expands such a subtree and gives up without writing);
+//   * the walkers are persistent warps that claim their starting leaves from a counter.
 #include <cuda_runtime.h>
 
 #include <algorithm>
