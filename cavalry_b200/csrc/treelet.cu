@@ -30,7 +30,6 @@ namespace cav {
 
 namespace {
 
-constexpr int kWarpsPerBlock = 1;  // see k_treelet
 constexpr unsigned kFull = 0xffffffffu;
 
 struct SubsetTable {
@@ -489,21 +488,31 @@ __global__ void k_leaf_list_batch(const TreeletSeg* __restrict__ segs, const int
     if (pos < (uint32_t)n) list[leaf_off[k] + pos] = (int32_t)local;
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 32)
+// The same persistent walkers over a group of trees: a claimed index g of the group's
+// concatenated leaf list belongs to the tree whose leaf range holds it.
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkBlocksPerSm)
     k_treelet_batch(const TreeletSeg* __restrict__ segs, const int64_t* __restrict__ leaf_off, int k0, int k1,
-                    const int32_t* __restrict__ list, uint32_t* visited, int* err) {
-    __shared__ WarpSmem smem[kWarpsPerBlock];
-    const int w = threadIdx.x >> 5;
-    const int64_t g = leaf_off[k0] + (int64_t)blockIdx.x * kWarpsPerBlock + w;
-    if (g >= leaf_off[k1]) return;
-    int lo = k0, hi = k1 - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (leaf_off[mid] <= g) lo = mid;
-        else hi = mid - 1;
+                    const int32_t* __restrict__ list, uint32_t* visited, int* err, uint32_t* claim) {
+    __shared__ WarpSmem smem[kWalkWarps];
+    WarpSmem& S = smem[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int64_t first = leaf_off[k0], total = leaf_off[k1] - first;
+    for (;;) {
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(claim, 1u);
+        i = __shfl_sync(kFull, i, 0);
+        if ((int64_t)i >= total) return;
+        const int64_t g = first + i;
+        int lo = k0, hi = k1 - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (leaf_off[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const int64_t n = segs[lo].n;
+        treelet_walk(segs[lo].nodes, list[g], (int32_t)(2 * n - 1), visited + node_off(leaf_off, lo), S, err);
+        __syncwarp();
     }
-    const int64_t n = segs[lo].n;
-    treelet_walk(segs[lo].nodes, list[g], (int32_t)(2 * n - 1), visited + node_off(leaf_off, lo), smem[w], err);
 }
 
 }  // namespace
@@ -553,12 +562,14 @@ cav_status treelet_rounds_batch(cav_ctx* ctx, const TreeletSeg* segs, const Tree
             k0 = k1;
             continue;
         }
+        const int64_t grid = std::min<int64_t>(div_up(leaves, kWalkWarps), (int64_t)ctx->num_sms * kWalkBlocksPerSm);
         for (int r = 0; r < rounds; ++r) {
             CAV_CUDA(ctx, cudaMemsetAsync(visited + node_off_h(k0), 0, sizeof(uint32_t) * nodes, s));
             CAV_CUDA(ctx, cudaMemsetAsync(counters + k0, 0, sizeof(uint32_t) * (k1 - k0), s));
+            CAV_CUDA(ctx, cudaMemsetAsync(counters + K + 1, 0, sizeof(uint32_t), s));  // the walkers' claims
             k_leaf_list_batch<<<div_up(nodes, 256), 256, 0, s>>>(segs, leaf_off, k0, k1, leaf_list, counters);
-            k_treelet_batch<<<div_up(leaves, kWarpsPerBlock), kWarpsPerBlock * 32, 0, s>>>(
-                segs, leaf_off, k0, k1, leaf_list, visited, ctx->d_error + 1);
+            k_treelet_batch<<<(unsigned)grid, kWalkWarps * 32, 0, s>>>(segs, leaf_off, k0, k1, leaf_list, visited,
+                                                                      ctx->d_error + 1, counters + K + 1);
         }
         k0 = k1;
     }
