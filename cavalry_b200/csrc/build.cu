@@ -283,24 +283,42 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
     } else {
         atomicExch(my_status, kFlagAgg | total);
     }
+    // Look-back in windows of kLookWin predecessors: their statuses are read at once (one
+    // round trip instead of one per tile), then aggregates are summed back to the first
+    // inclusive prefix; an entry not yet published is waited on (bounded) and read again.
+    // Every tile publishes its aggregate before its own look-back, so the walk back from
+    // tile t otherwise takes about t/2 dependent loads.
+    constexpr int kLookWin = 8;
     uint32_t excl = 0;
     if (tile > 0) {
         int p = tile - 1;
         uint64_t t0 = 0;
         while (p >= 0) {
-            uint32_t s = *((volatile uint32_t*)(status + (size_t)p * 256 + digit));
-            if ((s & ~kCountMask) == 0) {
-                if (t0 == 0) t0 = globaltimer_ns();
-                else if (globaltimer_ns() - t0 > wait_ns) {  // give up and flag the error
-                    atomicOr(err, kErrLookback);
-                    break;
-                }
-                continue;
+            uint32_t st[kLookWin];
+#pragma unroll
+            for (int w = 0; w < kLookWin; ++w)
+                st[w] = p - w >= 0 ? (uint32_t) * ((volatile uint32_t*)(status + (size_t)(p - w) * 256 + digit))
+                                   : (uint32_t)kFlagInc;  // before tile 0: an empty inclusive prefix
+            int w = 0;
+            bool done = false;
+#pragma unroll
+            for (int k = 0; k < kLookWin; ++k) {
+                if (done || w < k) break;  // stopped at an inclusive prefix or an unpublished entry
+                const uint32_t f = st[k] & ~kCountMask;
+                if (f == 0) break;
+                excl += st[k] & kCountMask;
+                if (f == kFlagInc) done = true;
+                else w = k + 1;
             }
-            t0 = 0;
-            excl += s & kCountMask;
-            if ((s & ~kCountMask) == kFlagInc) break;
-            --p;
+            if (done) break;
+            if (w > 0) t0 = 0;  // progress: the wait restarts at the first unpublished entry
+            p -= w;
+            if (w == kLookWin) continue;
+            if (t0 == 0) t0 = globaltimer_ns();
+            else if (globaltimer_ns() - t0 > wait_ns) {  // give up and flag the error
+                atomicOr(err, kErrLookback);
+                break;
+            }
         }
         __threadfence();
         atomicExch(my_status, kFlagInc | (excl + total));
