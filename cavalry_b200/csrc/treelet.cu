@@ -152,26 +152,33 @@ __device__ bool optimize_treelet(BNode* nodes, int32_t root, int32_t count, Warp
     __syncwarp();
     const float(&lbox)[7][6] = S.lbox;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        int s = (q << 5) | lane;
-        bool any = false;
-        f3 lo = mk(0, 0, 0), hi = mk(0, 0, 0);
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-            if ((s >> k) & 1) {
-                f3 blo = mk(lbox[k][0], lbox[k][1], lbox[k][2]);
-                f3 bhi = mk(lbox[k][3], lbox[k][4], lbox[k][5]);
-                if (!any) {
-                    lo = blo;
-                    hi = bhi;
-                    any = true;
-                } else {
-                    lo = vmin3(lo, blo);
-                    hi = vmax3(hi, bhi);
-                }
-            }
+    // Subset s = (q << 5) | lane: the union of the lane's leaves 0-4 (its low five bits) is
+    // taken once, then leaves 5 and 6 per quarter q (min/max unions are exact in any order).
+    bool any = false;
+    f3 lo = mk(0, 0, 0), hi = mk(0, 0, 0);
+    auto unite = [&](int k, bool& a, f3& l, f3& h) {
+        const f3 blo = mk(lbox[k][0], lbox[k][1], lbox[k][2]);
+        const f3 bhi = mk(lbox[k][3], lbox[k][4], lbox[k][5]);
+        if (!a) {
+            l = blo;
+            h = bhi;
+            a = true;
+        } else {
+            l = vmin3(l, blo);
+            h = vmax3(h, bhi);
         }
-        S.area[s] = any ? surface_area(lo, hi) : 0.f;
+    };
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+        if ((lane >> k) & 1) unite(k, any, lo, hi);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        bool qany = any;
+        f3 qlo = lo, qhi = hi;
+        if (q & 1) unite(5, qany, qlo, qhi);
+        if (q & 2) unite(6, qany, qlo, qhi);
+        const int s = (q << 5) | lane;
+        S.area[s] = qany ? surface_area(qlo, qhi) : 0.f;
         S.cost[s] = -1.f;
     }
     __syncwarp();
@@ -430,8 +437,9 @@ __device__ void treelet_walk(BNode* nodes, int32_t curr, int32_t count, uint32_t
 // Measured on 3 rounds over a 1M-triangle soup: one launched warp per leaf in 1-warp blocks
 // (32 per SM, 64 registers) 7.14 ms; persistent 1-warp blocks at 64 registers 5.67;
 // 2-warp blocks at 48 registers (40 per SM) 5.46; at 40 registers 5.34, 5.00 with the leaf
-// boxes in shared memory, 4.93 with the leaf records there too; at 32 registers (64 per SM)
-// 5.99 (spills).  Claiming 4 or 16 leaves per atomic did not help.
+// boxes in shared memory, 4.93 with the leaf records there too, 4.72 with the subset boxes
+// built from per-lane partial unions; at 32 registers (64 per SM) 5.99 (spills).  Claiming
+// 4 or 16 leaves per atomic did not help.
 constexpr int kWalkWarps = 2;
 constexpr int kWalkBlocksPerSm = 24;
 __global__ void __launch_bounds__(kWalkWarps * 32, kWalkBlocksPerSm)
