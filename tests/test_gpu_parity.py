@@ -286,3 +286,34 @@ def test_invalid_arguments_are_reported(cuda_ctx):
         cuda_ctx.build(pos, idx, rounds=0)  # a single triangle is below the minimum of 2
     with pytest.raises(cav.CavError):
         cuda_ctx.set_trace_config(block_threads=33)
+
+
+def test_host_buffer_path_over_several_chunks(cuda_ctx):
+    """The host-buffer entry points pipeline chunks of 4M rays over two streams.  4,195,304
+    rays make two chunks, the second ragged; with pageable (numpy) and with pinned (torch)
+    buffers, closest and any hit equal the device path's results."""
+    import torch
+
+    from cavalry_b200 import scenes
+
+    pos, idx = scenes.soup(20_000, seed=61)
+    bvh = cuda_ctx.build(torch.from_numpy(pos).cuda(), torch.from_numpy(idx).cuda(), rounds=2)
+    n = (1 << 22) + 1000
+    rays = scenes.closest_rays(n, seed=62)
+    srays, lim = scenes.shadow_rays(n, seed=63)
+    prim_d, t_d, uv_d = (a.cpu().numpy() for a in bvh.trace_closest(torch.from_numpy(rays).cuda()))
+    occ_d = bvh.trace_any(torch.from_numpy(srays).cuda(), torch.from_numpy(lim).cuda()).cpu().numpy()
+    prim_h, t_h, uv_h = bvh.trace_closest_host(rays)
+    occ_h = bvh.trace_any_host(srays, lim)
+    assert np.array_equal(prim_h, prim_d) and np.array_equal(t_h.view(np.uint32), t_d.view(np.uint32))
+    assert np.array_equal(uv_h.view(np.uint32), uv_d.view(np.uint32)) and np.array_equal(occ_h, occ_d)
+    h_rays = torch.from_numpy(rays).pin_memory()
+    out = (torch.empty(n, dtype=torch.int32).pin_memory(), torch.empty(n, dtype=torch.float32).pin_memory(),
+           torch.empty((n, 2), dtype=torch.float32).pin_memory())
+    bvh.trace_closest_host(h_rays, out=out)
+    occ_p = torch.empty(n, dtype=torch.uint8).pin_memory()
+    bvh.trace_any_host(torch.from_numpy(srays).pin_memory(), torch.from_numpy(lim).pin_memory(), out=occ_p)
+    cuda_ctx.sync_check()
+    assert np.array_equal(out[0].numpy(), prim_d) and np.array_equal(out[1].numpy().view(np.uint32), t_d.view(np.uint32))
+    assert np.array_equal(occ_p.numpy(), occ_d)
+    bvh.free()
