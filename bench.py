@@ -457,7 +457,8 @@ def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, close
     our LBVH build of the same 1M soup; its BVH::intersect (BVH/BVH.h:23-107) on this step's
     rays over our 3-round tree; and, on the 5.24M-triangle icosphere scene at 0 rounds (its
     own LBVH, bit-exact topology with ours), its BVH::intersect against ours on the renderer's
-    bounce-0 and bounce-1 extend rays."""
+    bounce-0 and bounce-1 extend rays.  Beside them, config 3 as this renderer renders it
+    (the whole 1920 x 1080 x 64-spp film of that scene)."""
     import os as _os
     import tempfile
 
@@ -502,6 +503,7 @@ def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, close
     path = _os.path.join(tmp, "spheres.pbrt")
     scenes.write_pbrt(path, sc_np, width=1920, height=1080, spp=64, max_depth=8)
     sc = ctx.load_pbrt(path, bvh_rounds=0)
+    sc_r = ctx.load_pbrt(path, bvh_rounds=3)  # the same file as this renderer renders it
     _os.remove(path)
     sb = sc.bvh()
     R = po.RefScene(sc_np["positions"], sc_np["indices"], sc_np["mesh_ids"], rounds=0, id_mode=0, dump=False)
@@ -539,9 +541,19 @@ def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, close
                                   "speedup_fast": round(mine["fast"] / ref_v, 2)}
     R.free()
     sc.free()
+    out["spheres_5M_closest_0_rounds"] = {"triangles": int(len(sc_np["indices"])), "topology_bit_exact": topo, **rows}
+    # (4) config 3 rendered whole by this renderer: 1920 x 1080 x 64 spp, depth 8, 3 treelet
+    # rounds, fast traversal (device time of the render, median of 2 after a short warm-up)
+    sc_r.render(spp=2, fast_trace=True)
+    times = [sc_r.render(fast_trace=True)[2] for _ in range(2)]
+    ms3 = statistics.median(times)
+    samples = 1920 * 1080 * 64
+    out["config3_render"] = {"workload": "spheres_5M_1920x1080_64spp_depth8_path", "treelet_rounds": 3,
+                             "trace_mode": "fast", "render_s": round(ms3 / 1e3, 4),
+                             "samples_per_s": round(samples / (ms3 * 1e-3), 1)}
+    sc_r.free()
     # the soup bench's own launch shape is restored for anything measured after this block
     ctx.set_trace_config(closest_shape["block_threads"], 0, closest_shape["batch"])
-    out["spheres_5M_closest_0_rounds"] = {"triangles": int(len(sc_np["indices"])), "topology_bit_exact": topo, **rows}
     return out
 
 
