@@ -231,12 +231,21 @@ __device__ __forceinline__ const float* bias_smem(const unsigned char* smem, int
     return bs + o;
 }
 
-// D[NT] = A[KT] * W^T for one layer: W is [out][in + pad] in shared memory.
+// D[NT] = bias + A[KT] * W^T for one layer: W is [out][in + pad] in shared memory; the
+// accumulators start from the layer's bias (zero without one), the order the tcgen05
+// kernel sums in as well.
 template <int KT, int NT>
-__device__ __forceinline__ void layer_mma(const uint32_t (&A)[KT][4], const __nv_bfloat16* W, int ld, float (&D)[NT][4]) {
+__device__ __forceinline__ void layer_mma(const uint32_t (&A)[KT][4], const __nv_bfloat16* W, int ld, float (&D)[NT][4],
+                                          const float* bias = nullptr) {
     const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
 #pragma unroll
-    for (int nt = 0; nt < NT; ++nt) D[nt][0] = D[nt][1] = D[nt][2] = D[nt][3] = 0.f;
+    for (int nt = 0; nt < NT; ++nt) {
+        const float b0 = bias ? bias[nt * 8 + 2 * q] : 0.f, b1 = bias ? bias[nt * 8 + 2 * q + 1] : 0.f;
+        D[nt][0] = b0;
+        D[nt][1] = b1;
+        D[nt][2] = b0;
+        D[nt][3] = b1;
+    }
 #pragma unroll
     for (int kt = 0; kt < KT; ++kt) {
 #pragma unroll
@@ -249,17 +258,16 @@ __device__ __forceinline__ void layer_mma(const uint32_t (&A)[KT][4], const __nv
     }
 }
 
-// bias + ReLU, then the accumulators of tiles (2kt, 2kt+1) become k-tile kt of the next A
+// ReLU (the bias is already in the accumulators), then the accumulators of tiles
+// (2kt, 2kt+1) become k-tile kt of the next A
 template <int NT>
-__device__ __forceinline__ void relu_to_a(float (&D)[NT][4], const float* bias, uint32_t (&A)[NT / 2][4]) {
-    const int lane = threadIdx.x & 31, q = lane & 3;
+__device__ __forceinline__ void relu_to_a(float (&D)[NT][4], uint32_t (&A)[NT / 2][4]) {
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
-        const float b0 = bias[nt * 8 + 2 * q], b1 = bias[nt * 8 + 2 * q + 1];
-        D[nt][0] = fmaxf(D[nt][0] + b0, 0.f);
-        D[nt][1] = fmaxf(D[nt][1] + b1, 0.f);
-        D[nt][2] = fmaxf(D[nt][2] + b0, 0.f);
-        D[nt][3] = fmaxf(D[nt][3] + b1, 0.f);
+        D[nt][0] = fmaxf(D[nt][0], 0.f);
+        D[nt][1] = fmaxf(D[nt][1], 0.f);
+        D[nt][2] = fmaxf(D[nt][2], 0.f);
+        D[nt][3] = fmaxf(D[nt][3], 0.f);
     }
 #pragma unroll
     for (int kt = 0; kt < NT / 2; ++kt) {
@@ -326,28 +334,27 @@ __global__ void __launch_bounds__(kFwdThreads) k_forward(const float* __restrict
         if (kStore) store_a(A0, acts.x0, kF0, r0, n);
         float D[8][4];
         uint32_t A[4][4];
-        layer_mma(A0, W + wf_off(0), kF0 + kPad, D);
-        relu_to_a(D, bias_smem(smem, 0), A);
+        layer_mma(A0, W + wf_off(0), kF0 + kPad, D, bias_smem(smem, 0));
+        relu_to_a(D, A);
         if (kStore) store_a(A, acts.x1, kH, r0, n);
-        layer_mma(A, W + wf_off(1), kH + kPad, D);
-        relu_to_a(D, bias_smem(smem, 1), A);
+        layer_mma(A, W + wf_off(1), kH + kPad, D, bias_smem(smem, 1));
+        relu_to_a(D, A);
         if (kStore) store_a(A, acts.x2, kH, r0, n);
-        layer_mma(A, W + wf_off(2), kH + kPad, D);
-        relu_to_a(D, bias_smem(smem, 2), A);
+        layer_mma(A, W + wf_off(2), kH + kPad, D, bias_smem(smem, 2));
+        relu_to_a(D, A);
         if (kStore) store_a(A, acts.x3, kH, r0, n);
         float O[4][4];
-        layer_mma(A, W + wf_off(3), kH + kPad, O);
-        const float* b3 = bias_smem(smem, 3);
+        layer_mma(A, W + wf_off(3), kH + kPad, O, bias_smem(smem, 3));
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
             const int c = nt * 8 + 2 * q;
             if (ra < n) {
-                out[ra * kOut + c] = O[nt][0] + b3[c];
-                out[ra * kOut + c + 1] = O[nt][1] + b3[c + 1];
+                out[ra * kOut + c] = O[nt][0];
+                out[ra * kOut + c + 1] = O[nt][1];
             }
             if (rb < n) {
-                out[rb * kOut + c] = O[nt][2] + b3[c];
-                out[rb * kOut + c + 1] = O[nt][3] + b3[c + 1];
+                out[rb * kOut + c] = O[nt][2];
+                out[rb * kOut + c + 1] = O[nt][3];
             }
         }
     }
@@ -438,7 +445,7 @@ __device__ __forceinline__ void issue_layer(uint32_t a_s, uint32_t w_s, uint32_t
 #pragma unroll
     for (int j = 0; j < K / 16; ++j)
         mma_bf16(tmem, sdesc(a_s + j * 2 * kM * 16, kM * 16, 128), sdesc(w_s + j * 2 * N * 16, N * 16, 128), idesc(N),
-                 j > 0);
+                 1u);  // onto the bias the epilogue stored in the accumulator
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
@@ -494,6 +501,31 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, uint32_t (&v)[32]) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// 32 columns of this thread's TMEM lane from 32 floats in shared memory (the same row for
+// every thread: a broadcast read)
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float* src) {
+    uint32_t v[32];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float4 f = reinterpret_cast<const float4*>(src)[i];
+        v[4 * i] = __float_as_uint(f.x);
+        v[4 * i + 1] = __float_as_uint(f.y);
+        v[4 * i + 2] = __float_as_uint(f.z);
+        v[4 * i + 3] = __float_as_uint(f.w);
+    }
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+        "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n"
+        :
+        : "r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+          "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]),
+          "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]),
+          "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // ReLU and round-to-nearest BF16 of two floats in one conversion (lo in the low half); the
 // two operations commute, so this equals pack_bf16(fmaxf(lo, 0), fmaxf(hi, 0)).
 __device__ __forceinline__ uint32_t relu_pack_bf16(float lo, float hi) {
@@ -502,15 +534,16 @@ __device__ __forceinline__ uint32_t relu_pack_bf16(float lo, float hi) {
     return r;
 }
 
-// bias + ReLU of 32 accumulator columns, packed to BF16 as 4 x 8-element K chunks of the next A
-__device__ __forceinline__ void relu_pack(const uint32_t (&v)[32], const float* bias, uint4 (&o)[4]) {
+// ReLU of 32 accumulator columns (which started from the bias), packed to BF16 as 4 x
+// 8-element K chunks of the next A
+__device__ __forceinline__ void relu_pack(const uint32_t (&v)[32], uint4 (&o)[4]) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         uint32_t w[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const int j = c * 8 + 2 * e;
-            w[e] = relu_pack_bf16(__uint_as_float(v[j]) + bias[j], __uint_as_float(v[j + 1]) + bias[j + 1]);
+            w[e] = relu_pack_bf16(__uint_as_float(v[j]), __uint_as_float(v[j + 1]));
         }
         o[c] = make_uint4(w[0], w[1], w[2], w[3]);
     }
@@ -613,9 +646,11 @@ __global__ void __launch_bounds__(umma::kThreads, 1)
         }
         return ok;
     };
-    // bias + ReLU of layer l's accumulator into the next operand (H), and the stored activations
+    // ReLU of layer l's accumulator into the next operand (H), and the stored activations.
+    // Once a half of the accumulator has been read, layer l + 1's bias goes into it, so the
+    // next layer's MMAs accumulate onto the bias (layer 3 has 32 columns).
     auto hidden = [&](int l, int64_t r) {
-        const float* bl = bias + l * kH;
+        const float* bn = bias + (l + 1) * kH;
         __nv_bfloat16* xs = l == 0 ? acts.x1 : l == 1 ? acts.x2 : acts.x3;
         uint32_t v[32], v1[32];
         tmem_ld<32>(tload, v);
@@ -628,16 +663,24 @@ __global__ void __launch_bounds__(umma::kThreads, 1)
                 tmem_wait_ld();
             }
             uint4 o[4];
-            relu_pack(h ? v1 : v, bl + 32 * h, o);
+            relu_pack(h ? v1 : v, o);
+            // this half has been read: the next layer's bias goes in (after the second half's
+            // load in the storing variant, which reads the halves one at a time)
+            if (h == 0 || l < 2) tmem_st32(tload + 32 * h, bn + 32 * h);
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 *reinterpret_cast<uint4*>(H + canon(kM, m, (4 * h + c) * 8)) = o[c];
                 if (kStore && r < n) reinterpret_cast<uint4*>(xs + r * kH)[4 * h + c] = o[c];
             }
         }
+        tmem_wait_st();
     };
 
-    // prologue: the first tile's features; the inputs of the one after
+    // prologue: layer 0's bias in the accumulator, the first tile's features, the inputs of
+    // the one after
+    tmem_st32(tload, bias);
+    tmem_st32(tload + 32, bias + 32);
+    tmem_wait_st();
     load_inputs(first);
     if (first < ntiles) {
         float x[kIn];
@@ -674,16 +717,17 @@ __global__ void __launch_bounds__(umma::kThreads, 1)
             // The tile's 128 output rows are staged in H (free once layer 3 completed; 16-byte
             // chunks XOR-swizzled by row against bank conflicts) and leave as one contiguous
             // 16 KB block; a row per thread would put every store of a warp on 32 lines.
-            const float* bl = bias + 3 * kH;
             uint32_t v[32];
             tmem_ld<32>(tload, v);
             tmem_wait_ld();
+            tmem_st32(tload, bias);  // the next tile's layer 0 starts from its bias
+            tmem_st32(tload + 32, bias + 32);
 #pragma unroll
             for (int c = 0; c < kOut / 4; ++c)
                 *reinterpret_cast<float4*>(H + m * 128 + ((c ^ (m & 7)) << 4)) =
-                    make_float4(__uint_as_float(v[4 * c]) + bl[4 * c], __uint_as_float(v[4 * c + 1]) + bl[4 * c + 1],
-                                __uint_as_float(v[4 * c + 2]) + bl[4 * c + 2],
-                                __uint_as_float(v[4 * c + 3]) + bl[4 * c + 3]);
+                    make_float4(__uint_as_float(v[4 * c]), __uint_as_float(v[4 * c + 1]), __uint_as_float(v[4 * c + 2]),
+                                __uint_as_float(v[4 * c + 3]));
+            tmem_wait_st();
             group_sync(g);
             const int64_t row0 = tile * kM;
             const int rows = (int)(n - row0 < kM ? n - row0 : kM);
