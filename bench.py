@@ -3,9 +3,12 @@
 Workload (the reference's soup configuration): LBVH + 3 treelet rounds over a seeded
 1,000,000-triangle FP32 soup; each step traces 4,194,304 closest-hit rays (origins
 uniform in [-0.1,1.1]^3, directions uniform on the sphere, tmax = inf) against the
-resident BVH.  `value` is device-timed closest-hit Mrays/s with rays already in HBM
-(L2 flushed between steps); `e2e` is the same metric through the C ABI's host-buffer
-entry point (pinned host rays in, hits out, copies inside the timed region).
+resident BVH, in the exact mode, traced in the Morton order of the ray origins
+(CAV_TRACE_REORDER: the sort and the write-back of every ray's results to its own index
+are inside the timed step; the hits equal those of the given order, which is timed too).
+`value` is device-timed closest-hit Mrays/s with rays already in HBM (L2 flushed between
+steps); `e2e` is the same metric through the C ABI's host-buffer entry point (pinned host
+rays in, hits out, copies inside the timed region).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -206,8 +209,12 @@ def run_ours(args):
     tris_per_ray = tris_t / N_RAYS
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
 
+    # The batch is traced in the Morton order of its ray origins (CAV_TRACE_REORDER: key,
+    # sort, gather, traversal and scatter back, all inside each timed step); the results are
+    # those of the given order, which is also timed below.
+    flags = cav.TRACE_EXACT | cav.TRACE_REORDER
     for _ in range(args.warmup):
-        bvh.trace_closest(rays, out=out)
+        bvh.trace_closest(rays, flags=flags, out=out)
     torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -219,7 +226,7 @@ def run_ours(args):
     for k in range(args.steps):
         flush.fill_(float(k))
         ev[k][0].record()
-        bvh.trace_closest(rays, out=out)
+        bvh.trace_closest(rays, flags=flags, out=out)
         ev[k][1].record()
     torch.cuda.synchronize()
     barrier()
@@ -234,6 +241,20 @@ def run_ours(args):
     ctx.sync_check()
     ms_per_step = total_ms / args.steps
     value = N_RAYS * world / (ms_per_step * 1e-3) / 1e6
+    # the same rays in the given order (secondary)
+    out_g = (torch.empty_like(prim), torch.empty_like(tt), torch.empty_like(uv))
+    bvh.trace_closest(rays, out=out_g)
+    given_ms = []
+    for k in range(3):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        bvh.trace_closest(rays, out=out_g)
+        b.record()
+        torch.cuda.synchronize()
+        given_ms.append(a.elapsed_time(b))
+    assert all(torch.equal(x, y) for x, y in zip(out, out_g)), "reordered and given-order results differ"
+    given_value = N_RAYS / (statistics.mean(given_ms) * 1e-3) / 1e6
 
     # any-hit (secondary)
     srays_np, lim_np = scenes.shadow_rays(N_RAYS, seed=21 + rank)
@@ -291,14 +312,14 @@ def run_ours(args):
     h_uv = torch.empty((N_RAYS, 2), dtype=torch.float32).pin_memory()
     hout = (h_prim, h_t, h_uv)
     for _ in range(2):
-        bvh.trace_closest_host(h_rays, out=hout)
+        bvh.trace_closest_host(h_rays, flags=flags, out=hout)
     barrier()
     torch.cuda.synchronize()
     e2e_ms = []
     for k in range(args.steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        bvh.trace_closest_host(h_rays, out=hout)
+        bvh.trace_closest_host(h_rays, flags=flags, out=hout)
         b.record()
         torch.cuda.synchronize()
         e2e_ms.append(a.elapsed_time(b))
@@ -322,7 +343,8 @@ def run_ours(args):
     ref_cuda = cfg1 = None
     if rank == 0 and world == 1 and not args.no_reference_cuda:
         try:
-            ref_cuda = reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, round(value, 2), tuned)
+            ref_cuda = reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, round(value, 2), tuned,
+                                            round(given_value, 2))
         except Exception as e:  # a reported baseline: note the failure, keep the bench line
             ref_cuda = {"error": str(e)[:300]}
         cfg1 = config1_block(ctx)
@@ -346,12 +368,15 @@ def run_ours(args):
             "rays_per_step": N_RAYS,
             "treelet_rounds": ROUNDS,
             "trace_mode": "exact (reference order and pruning)",
+            "ray_order": "Morton order of the ray origins (CAV_TRACE_REORDER): keys, sort, gather, traversal and "
+                         "scatter of the results back to each ray's index inside every timed step",
             "launch_shape": {"block": tuned["block_threads"], "queue_chunk": tuned["batch"], "stack": tuned["stack"],
                              "picked_by": tuned.get("picked_by", "cav_trace_autotune on a separate 1M-ray sample")},
             "l2": "flushed between timed steps (256 MiB write); rays 128 MiB > L2",
             "parallelism": f"replicas x{world}",
         },
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * 9,  # per step: keys, histogram, 4 sort passes, gather, traversal, scatter
+        "given_order_mrays_s": round(given_value, 2),
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * RAY_BYTES,
                 "d2h_bytes_per_step": N_RAYS * HIT_BYTES},
         "roofline": {
@@ -450,7 +475,7 @@ def _median(xs):
     return float(statistics.median(xs))
 
 
-def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, closest_shape):
+def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, closest_shape, given_value=None):
     """The reference's own CUDA code on this B200 beside ours (a reported baseline, like
     cpu_baseline): its BVH::build (BVH/BVH.cu:317-370, replayed stage by stage with CUDA events
     by oracle/ref_harness.cu, 0 treelet rounds: its treelet kernel faults on the B200) against
@@ -496,6 +521,7 @@ def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, close
     ref_mrays = len(rays_np) / (ms * 1e-3) / 1e6
     R.free()
     out["soup_1M_closest_3_rounds"] = {"ref_mrays_s": round(ref_mrays, 2), "ours_mrays_s": value,
+                                       "ours_given_order_mrays_s": given_value,
                                        "speedup": round(value / ref_mrays, 2), "rays": len(rays_np)}
     # (3) the 5.24M-triangle scene at 0 rounds: the north-star comparison
     sc_np = scenes.sphere_scene(64, 6, seed=9)

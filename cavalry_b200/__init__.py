@@ -28,6 +28,7 @@ _LIB_PATH = _PKG / "libcavalry_b200.so"
 TRACE_EXACT = 0
 TRACE_CULL_ON_POP = 1
 TRACE_FAST = 2
+TRACE_REORDER = 4  # with either mode: trace a large batch in the Morton order of its ray origins
 
 STATUS = {
     0: "ok",

@@ -1226,6 +1226,33 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     return CAV_OK;
 }
 
+size_t sort_status_words(int64_t n, int passes) { return (size_t)passes * div_up(n, kSortTile) * 256; }
+
+cav_status sort_pairs(cav_ctx* ctx, uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp, int64_t n,
+                      int passes, uint32_t* hist, uint32_t* status, uint32_t* counters, int* err, cudaStream_t s) {
+    if (n <= 0) return CAV_OK;
+    if (passes <= 0 || passes > 8 || (passes & 1)) return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "sort_pairs: passes");
+    const int tiles = div_up(n, kSortTile);
+    CAV_CUDA(ctx, cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, s));
+    CAV_CUDA(ctx, cudaMemsetAsync(status, 0, sizeof(uint32_t) * sort_status_words(n, passes), s));
+    CAV_CUDA(ctx, cudaMemsetAsync(counters, 0, sizeof(uint32_t) * passes, s));
+    CAV_CUDA(ctx, cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem)));
+    k_sort_hist<<<std::min(div_up(n, kThreads), ctx->num_sms * 8), kSortThreads, 0, s>>>(keys, n, hist);
+    uint64_t* kin = keys;
+    uint64_t* kout = keys_tmp;
+    uint32_t* vin = vals;
+    uint32_t* vout = vals_tmp;
+    for (int pass = 0; pass < passes; ++pass) {
+        k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, n, 8 * pass, hist + 256 * pass,
+                                                                  status + (size_t)pass * tiles * 256, counters + pass,
+                                                                  err, ctx->sort_wait_ns, 0);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    CAV_CUDA(ctx, cudaGetLastError());
+    return CAV_OK;
+}
+
 }  // namespace cav
 
 // ------------------------------------------------------- allocation-free entry point

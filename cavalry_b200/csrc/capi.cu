@@ -283,6 +283,9 @@ cav_status cav_sync_check(cav_ctx* ctx, void* stream) {
     if ((flags[2] | flags[3]) & kFlagStepLimit)
         return set_error(ctx, CAV_ERR_TIMEOUT, "traversal step limit reached (rays stopped)");
     if (flags[4]) return set_error(ctx, CAV_ERR_TIMEOUT, "MLP forward: a tensor-core completion wait gave up");
+    if (flags[5] & kErrLookback)
+        return set_error(ctx, CAV_ERR_TIMEOUT, "ray reordering: the sort's look-back wait gave up (results not meaningful)");
+    if (flags[5]) return set_error(ctx, CAV_ERR_CUDA, "ray reordering: a sort invariant broke (results not meaningful)");
     return CAV_OK;
 }
 

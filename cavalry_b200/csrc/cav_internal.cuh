@@ -200,8 +200,15 @@ size_t bvh_arena_bytes(int64_t n);
 cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int32_t* indices,
                      const int32_t* mesh_ids, int64_t n, const float* bounds, int rounds, cudaStream_t s,
                      cav_bvh** out);
+// Stable LSD radix sort of (key, value) pairs by the low 8 * passes bits of the keys (passes
+// even, so the result ends in keys / vals), with the build's kernels: keys_tmp / vals_tmp hold
+// n entries, hist 8 x 256 words, status sort_status_words(n, passes) words, counters `passes`
+// words; all are cleared here.  A look-back wait that runs out sets kErrLookback in *err.
+size_t sort_status_words(int64_t n, int passes);
+cav_status sort_pairs(cav_ctx* ctx, uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp, int64_t n,
+                      int passes, uint32_t* hist, uint32_t* status, uint32_t* counters, int* err, cudaStream_t s);
 // treelet.cu
-// counters: device words of the caller's scratch ([0]: leaf-list positions)
+// counters: device words of the caller's scratch ([0]: leaf-list positions, [1]: the walkers' claims)
 cav_status treelet_rounds(cav_ctx* ctx, BNode* nodes, int64_t n, int rounds, int32_t* leaf_list, uint32_t* visited,
                           uint32_t* counters, cudaStream_t s);
 struct TreeletSeg {  // one tree of a batched treelet pass
