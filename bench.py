@@ -381,9 +381,10 @@ def run_ours(args):
                 "d2h_bytes_per_step": N_RAYS * HIT_BYTES},
         "roofline": {
             # The node-fetch stream is measured against the HBM copy peak (the algorithmic
-            # bytes of the scope table), but 83 % of it is served by L2 and DRAM carries a
-            # twentieth of the peak: the kernel is bound by the L1 data pipe's wavefronts
-            # (one per lane per 32-byte node half, ncu) and L2 latency, not by HBM.
+            # bytes of the scope table), but with the rays in Morton order 90 % of it is
+            # served by L2 and DRAM carries well under a percent of the peak: the kernel is
+            # bound by the L1 data pipe's wavefronts (one per lane per 32-byte node half,
+            # ncu) and L2 latency, not by HBM.  The time is the whole step's (sort included).
             "bound": "l1/l2",
             "achieved": round(achieved, 1),
             "peak": peak,
