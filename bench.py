@@ -203,6 +203,8 @@ def run_ours(args):
         ctx.set_trace_config(blk, 0, chunk)
         tuned = {"block_threads": blk, "batch": chunk, "stack": 128, "picked_by": "--launch-shape"}
     else:
+        # tuned on the given order: tuning on the reordered sample picked 128 x 16 with the short
+        # stack, 70.9 Mrays/s on the reordered step against 71.6 with this shape
         tuned = bvh.autotune(torch.from_numpy(scenes.closest_rays(1 << 20, seed=90 + rank)).to(dev))
     nodes_v, tris_t = bvh.trace_stats(rays)
     nodes_per_ray = nodes_v / N_RAYS

@@ -692,8 +692,8 @@ extern "C" cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh,
                                                void* stream, cav_trace_config_t* best_out) {
     using namespace cav;
     if (!ctx || !bvh || !rays || n <= 0) return CAV_ERR_INVALID_ARGUMENT;
-    if (flags & ~(uint32_t)CAV_TRACE_FAST) return CAV_ERR_INVALID_ARGUMENT;
-    const bool wide = (flags & CAV_TRACE_FAST) != 0;
+    if (flags & ~(uint32_t)(CAV_TRACE_FAST | CAV_TRACE_REORDER)) return CAV_ERR_INVALID_ARGUMENT;
+    const bool wide = (flags & CAV_TRACE_FAST) != 0;  // with CAV_TRACE_REORDER every candidate traces the reordered sample
     if (cudaSetDevice(ctx->device) != cudaSuccess) return cuda_error(ctx, cudaGetLastError(), "cudaSetDevice");
     cudaStream_t s = (cudaStream_t)stream;
     if (bvh->depth < 0) {

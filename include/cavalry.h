@@ -443,8 +443,10 @@ typedef struct cav_trace_config_t {
 } cav_trace_config_t;
 cav_status cav_trace_autotune(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
                               const float* limit, const int32_t* excl, void* stream, cav_trace_config_t* best);
-/* The same search for the traversal mode in flags (CAV_TRACE_EXACT or CAV_TRACE_FAST); each
- * mode keeps its own tuned shape in ctx (stack is 0 for the fast mode). */
+/* The same search for the traversal mode in flags (CAV_TRACE_EXACT or CAV_TRACE_FAST, with
+ * CAV_TRACE_REORDER when the batches will be traced reordered: every candidate then traces
+ * the reordered sample); each mode keeps its own tuned shape in ctx (stack is 0 for the
+ * fast mode). */
 cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
                                     const float* limit, const int32_t* excl, uint32_t flags, void* stream,
                                     cav_trace_config_t* best);

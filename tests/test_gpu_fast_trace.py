@@ -110,6 +110,9 @@ def test_reordered_batches_return_the_same_results(n):
             occ_w = bvh.trace_any(srays, lim, flags=mode).cpu().numpy()
             occ_g = bvh.trace_any(srays, lim, flags=mode | cav.TRACE_REORDER).cpu().numpy()
             assert np.array_equal(occ_w, occ_g)
+        if n > 70_001:  # the autotuner accepts the flag and tunes on the reordered sample
+            shape = bvh.autotune(rays[:200_000].contiguous(), flags=cav.TRACE_EXACT | cav.TRACE_REORDER)
+            assert shape["block_threads"] > 0 and shape["ms"] > 0
         ctx.sync_check()
         bvh.free()
     finally:
