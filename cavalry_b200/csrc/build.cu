@@ -181,26 +181,35 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1;
 
+// The histograms of the low `digits` bytes of every key (the digits the sort's passes read),
+// in one read of the keys.  Shared counters per block; a warp whose keys share a digit (the
+// high digits of spatially coherent primitives) adds them with one atomic, otherwise each
+// key adds its own (random digits rarely meet in one warp).
 __global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint64_t* __restrict__ keys, int64_t n,
-                                                            uint32_t* __restrict__ hist /*8x256*/) {
+                                                            int digits, uint32_t* __restrict__ hist /*8x256*/) {
     __shared__ uint32_t h[8][256];
     for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
     __syncthreads();
-    int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
+    // lane 0 of every iterating warp holds a key: i - lane < n
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i - lane < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        bool valid = i < n;
-        uint64_t k = valid ? keys[i] : 0;
-#pragma unroll
-        for (int p = 0; p < 8; ++p) {
-            uint32_t d = (uint32_t)(k >> (8 * p)) & 255u;
-            uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u);
-            if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+        const bool valid = i < n;
+        const uint64_t k = valid ? keys[i] : 0;
+        const uint32_t count = __popc(__ballot_sync(0xffffffffu, valid));
+        for (int p = 0; p < digits; ++p) {
+            const uint32_t d = (uint32_t)(k >> (8 * p)) & 255u;
+            const uint32_t d0 = __shfl_sync(0xffffffffu, d, 0);
+            if (__all_sync(0xffffffffu, !valid || d == d0)) {
+                if (lane == 0) atomicAdd(&h[p][d0], count);
+            } else if (valid) {
+                atomicAdd(&h[p][d], 1u);
+            }
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) {
-        uint32_t c = (&h[0][0])[i];
+    for (int i = threadIdx.x; i < digits * 256; i += blockDim.x) {
+        const uint32_t c = (&h[0][0])[i];
         if (c) atomicAdd(hist + i, c);
     }
 }
@@ -822,7 +831,7 @@ cav_status build_bvh(cav_ctx* ctx, const float* positions, int64_t nv, const int
     cudaEventRecord(bvh->ev[1], s);
 
     // sort: 8 passes ping-ponging codes_sorted <-> keys_b, vals_a <-> vals_b; ends in A
-    k_sort_hist<<<std::min(gb, ctx->num_sms * 8), kSortThreads, 0, s>>>(bvh->codes_sorted, n, hist);
+    k_sort_hist<<<std::min(gb, ctx->num_sms * 8), kSortThreads, 0, s>>>(bvh->codes_sorted, n, 8, hist);
     CAV_CUDA(ctx, cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem)));
     uint64_t* kin = bvh->codes_sorted;
     uint64_t* kout = keys_b;
@@ -1159,7 +1168,7 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     for (int k = 0; k < K; ++k) cudaEventRecord(bv[k]->ev[1], s);
     // sort by code (8 passes, stable), then by scene (1-2 passes, stable)
     CAV_CUDA(ctx, cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem)));
-    k_sort_hist<<<std::min(gb, ctx->num_sms * 8), kSortThreads, 0, s>>>(codes, total, hist);
+    k_sort_hist<<<std::min(gb, ctx->num_sms * 8), kSortThreads, 0, s>>>(codes, total, 8, hist);
     uint64_t* kin = codes;
     uint64_t* kout = keys_b;
     uint32_t* vin = vals_a;
@@ -1174,7 +1183,7 @@ cav_status build_bvh_batch(cav_ctx* ctx, int K, const float* const* positions, c
     }
     // kin/vin: codes in code order; now key by scene index
     k_scene_keys<<<gb, kThreads, 0, s>>>(vin, d_leaf, K, total, kin);
-    k_sort_hist<<<std::min(gb, ctx->num_sms * 8), kSortThreads, 0, s>>>(kin, total, hist + 8 * 256);
+    k_sort_hist<<<std::min(gb, ctx->num_sms * 8), kSortThreads, 0, s>>>(kin, total, passes2, hist + 8 * 256);
     for (int pass = 0; pass < passes2; ++pass) {
         k_onesweep<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(kin, vin, kout, vout, total, 8 * pass,
                                                                   hist + 8 * 256 + 256 * pass,
@@ -1237,7 +1246,7 @@ cav_status sort_pairs(cav_ctx* ctx, uint64_t* keys, uint32_t* vals, uint64_t* ke
     CAV_CUDA(ctx, cudaMemsetAsync(status, 0, sizeof(uint32_t) * sort_status_words(n, passes), s));
     CAV_CUDA(ctx, cudaMemsetAsync(counters, 0, sizeof(uint32_t) * passes, s));
     CAV_CUDA(ctx, cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem)));
-    k_sort_hist<<<std::min(div_up(n, kThreads), ctx->num_sms * 8), kSortThreads, 0, s>>>(keys, n, hist);
+    k_sort_hist<<<std::min(div_up(n, kThreads), ctx->num_sms * 8), kSortThreads, 0, s>>>(keys, n, passes, hist);
     uint64_t* kin = keys;
     uint64_t* kout = keys_tmp;
     uint32_t* vin = vals;
@@ -1365,7 +1374,7 @@ extern "C" cav_status cav_morton_sort_noalloc(const float* positions, int64_t nu
     }
     // keys_b receives the unsorted copy; the first sort pass overwrites it
     k_morton<<<gb, kThreads, 0, s>>>(leafbox, n, dbounds, hb, use_dev, keys_a, keys_b, vals_a);
-    k_sort_hist<<<std::min(gb, num_sms * 8), kSortThreads, 0, s>>>(keys_a, n, hist);
+    k_sort_hist<<<std::min(gb, num_sms * 8), kSortThreads, 0, s>>>(keys_a, n, 8, hist);
     if (cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem)) !=
         cudaSuccess) {
         cudaGetLastError();
