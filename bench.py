@@ -56,7 +56,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--launch-shape", default=None,
-                   help="soup workload: BLOCK,CHUNK for the exact traversal instead of the autotuner's pick")
+                   help="soup workload: BLOCK,CHUNK[,SMEM_STACK] for the exact traversal instead of the "
+                        "autotuner's pick")
     p.add_argument("--no-reference-cuda", action="store_true",
                    help="soup workload: skip the reference CUDA timings and the config-1 block")
     p.add_argument("--workload", default="soup",
@@ -197,15 +198,20 @@ def run_ours(args):
     tt = torch.empty(N_RAYS, dtype=torch.float32, device=dev)
     uv = torch.empty((N_RAYS, 2), dtype=torch.float32, device=dev)
     out = (prim, tt, uv)
-    # launch shape picked by the project's autotuner on a separate 1M-ray sample
+    # launch shape picked by the project's autotuner on a separate 4M-ray sample
     if args.launch_shape:
-        blk, chunk = (int(x) for x in args.launch_shape.split(","))
+        vals = [int(x) for x in args.launch_shape.split(",")]
+        blk, chunk, smem = vals[0], vals[1], (vals[2] if len(vals) > 2 else 0)
         ctx.set_trace_config(blk, 0, chunk)
-        tuned = {"block_threads": blk, "batch": chunk, "stack": 128, "picked_by": "--launch-shape"}
+        ctx.set_trace_stack(128, smem)
+        tuned = {"block_threads": blk, "batch": chunk, "stack": 128, "smem_stack": smem, "picked_by": "--launch-shape"}
     else:
-        # tuned on the given order: tuning on the reordered sample picked 128 x 16 with the short
-        # stack, 70.9 Mrays/s on the reordered step against 71.6 with this shape
-        tuned = bvh.autotune(torch.from_numpy(scenes.closest_rays(1 << 20, seed=90 + rank)).to(dev))
+        # tuned on a separate sample of the step's size in the given order: a 1M-ray sample,
+        # whose launches end in a relatively longer tail, picked shapes 0.2-4 % slower on the
+        # 4M step (the local-memory stack, or 128 x 16 when tuned on reordered rays)
+        tune_rays = torch.from_numpy(scenes.closest_rays(N_RAYS, seed=90 + rank)).to(dev)
+        tuned = bvh.autotune(tune_rays)
+        del tune_rays
     nodes_v, tris_t = bvh.trace_stats(rays)
     nodes_per_ray = nodes_v / N_RAYS
     tris_per_ray = tris_t / N_RAYS
@@ -277,7 +283,7 @@ def run_ours(args):
 
     # the compressed 8-wide fast mode on the same rays (secondary): same closest-hit
     # distances, a different triangle only at an equal-distance tie
-    tuned_fast = bvh.autotune(torch.from_numpy(scenes.closest_rays(1 << 20, seed=90 + rank)).to(dev),
+    tuned_fast = bvh.autotune(torch.from_numpy(scenes.closest_rays(N_RAYS, seed=90 + rank)).to(dev),
                               flags=cav.TRACE_FAST)
     fnodes, ftris = bvh.trace_stats(rays, flags=cav.TRACE_FAST)
     fout = (torch.empty_like(prim), torch.empty_like(tt), torch.empty_like(uv))
@@ -388,7 +394,8 @@ def run_ours(args):
             "ray_order": "Morton order of the ray origins (CAV_TRACE_REORDER): keys, sort, gather, traversal and "
                          "scatter of the results back to each ray's index inside every timed step",
             "launch_shape": {"block": tuned["block_threads"], "queue_chunk": tuned["batch"], "stack": tuned["stack"],
-                             "picked_by": tuned.get("picked_by", "cav_trace_autotune on a separate 1M-ray sample")},
+                             "smem_stack": tuned.get("smem_stack", 0),
+                             "picked_by": tuned.get("picked_by", "cav_trace_autotune on a separate 4M-ray sample")},
             "l2": "flushed between timed steps (256 MiB write); rays 128 MiB > L2",
             "parallelism": f"replicas x{world}",
         },
@@ -599,6 +606,7 @@ def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, close
     sc_r.free()
     # the soup bench's own launch shape is restored for anything measured after this block
     ctx.set_trace_config(closest_shape["block_threads"], 0, closest_shape["batch"])
+    ctx.set_trace_stack(closest_shape["stack"], closest_shape.get("smem_stack", 0))
     return out
 
 

@@ -89,6 +89,7 @@ def lib() -> ctypes.CDLL:
         "cav_trace_closest_host": ([P, P, P, I64, P, P, P, U32], ctypes.c_int),
         "cav_trace_any_host": ([P, P, P, P, P, I64, P, U32], ctypes.c_int),
         "cav_set_trace_config": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "cav_set_trace_stack": ([P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "cav_ctx_set_limits": ([P, ctypes.c_double, I64], ctypes.c_int),
         "cav_ctx_inject": ([P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "cav_server_cancel": ([P, I64], ctypes.c_int),
@@ -201,6 +202,11 @@ class Context:
     def set_trace_config(self, block_threads: int = 0, blocks_per_sm: int = 0, batch: int = 0):
         self._check(lib().cav_set_trace_config(self.handle, block_threads, blocks_per_sm, batch),
                     "cav_set_trace_config")
+
+    def set_trace_stack(self, stack: int = 0, smem_stack: int = 0):
+        """Exact-mode traversal stack: 64 or 128 entries (0 = 128), the first 16 in shared
+        memory (smem_stack=16) or all in local memory (0)."""
+        self._check(lib().cav_set_trace_stack(self.handle, stack, smem_stack), "cav_set_trace_stack")
 
     def build_batch(self, scenes, rounds: int = 0, stream=None) -> list:
         """Build many BVHs with one launch per LBVH stage: scenes = [(positions, indices) or
@@ -726,7 +732,7 @@ def film_to_rgb8(film_sum: np.ndarray, film_weight: np.ndarray) -> np.ndarray:
 
 class TraceConfig(ctypes.Structure):
     _fields_ = [("block_threads", ctypes.c_int), ("blocks_per_sm", ctypes.c_int), ("batch", ctypes.c_int),
-                ("stack", ctypes.c_int), ("ms", ctypes.c_float)]
+                ("stack", ctypes.c_int), ("ms", ctypes.c_float), ("smem_stack", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -153,6 +153,15 @@ cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_
     return CAV_OK;
 }
 
+cav_status cav_set_trace_stack(cav_ctx* ctx, int stack, int smem_stack) {
+    if (!ctx) return CAV_ERR_INVALID_ARGUMENT;
+    if ((stack != 0 && stack != 64 && stack != 128) || (smem_stack != 0 && smem_stack != 16))
+        return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_set_trace_stack: stack 0/64/128, smem_stack 0/16");
+    ctx->trace_stack = stack;
+    ctx->trace_smem_stack = smem_stack;
+    return CAV_OK;
+}
+
 cav_status cav_bvh_build_batch(cav_ctx* ctx, int num_scenes, const float* const* positions,
                                const int64_t* num_vertices, const int32_t* const* indices,
                                const int32_t* const* mesh_ids, const int64_t* num_triangles,

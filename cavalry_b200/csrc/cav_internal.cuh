@@ -122,6 +122,7 @@ struct cav_ctx {
     int trace_blocks_per_sm = 0;
     int trace_batch = 0;
     int trace_stack = 0;  // 64 selects the short traversal stack for trees known to be shallow
+    int trace_smem_stack = 0;  // > 0: the first stack entries of the exact kernels in shared memory
     // bounded device-side waits (cav_ctx_set_limits)
     uint32_t max_trace_steps = 1u << 22;     // node + triangle visits allowed one ray
     uint64_t sort_wait_ns = 2000000000ull;  // a sort tile's look-back wait, and a tcgen05 completion wait

@@ -28,6 +28,29 @@ constexpr int kStack = 128;
 // The short stack is used only for trees whose depth is known to fit: a traversal holds at
 // most one deferred sibling per level, so depth + 1 entries always suffice.
 constexpr int kShortStack = 64;
+// Optionally the first kSmemStack entries of a lane's stack live in shared memory laid out
+// [entry][thread]: the 32 lanes of a warp sit in 32 different banks whatever entries they
+// touch, so a push or a pop is one L1 wavefront, where in local memory every distinct entry
+// among the lanes is its own cache line (ncu on the 1M soup: 4.5 sectors per stack store,
+// 7.3 per load, 19 % of the kernel's L1 wavefronts, 77 % of the loads missing L1).  Deeper
+// entries stay in local memory.  On the soup 99.85 % of pushes land in the first 16 entries.
+constexpr int kSmemStack = 16;
+
+inline size_t stack_smem(int block, int entries) { return sizeof(int32_t) * entries * (size_t)block; }
+
+// With kSmemN == 0 the whole stack is in local memory (the better choice where the
+// traversal lives off L1 hits, e.g. coherent rays on a well-built tree: the shared stacks
+// shrink the L1); the autotuner times both.
+template <int kSmemN>
+__device__ __forceinline__ void stack_put(int32_t* sst, int32_t* lst, int i, int32_t v) {
+    if (kSmemN > 0 && i < kSmemN) sst[i * (int)blockDim.x] = v;
+    else lst[i - kSmemN] = v;
+}
+
+template <int kSmemN>
+__device__ __forceinline__ int32_t stack_get(const int32_t* sst, const int32_t* lst, int i) {
+    return kSmemN > 0 && i < kSmemN ? sst[i * (int)blockDim.x] : lst[i - kSmemN];
+}
 
 __device__ inline float imax_f(float a, float b) { return __int_as_float(max(__float_as_int(a), __float_as_int(b))); }
 __device__ inline float imin_f(float a, float b) { return __int_as_float(min(__float_as_int(a), __float_as_int(b))); }
@@ -83,7 +106,7 @@ constexpr int kTraceRegs = 48;
 // Segments: one traversal launch over the rays of several jobs, each with its own BVH and
 // output arrays.  A lane that claims global ray g finds its segment by binary search over
 // the segment starts (staged in shared memory) and switches to that segment's tree.
-template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack>
+template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack, int kSmemN = 0>
 __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
                           unsigned long long* counter, int refill, uint32_t max_steps, int* flag,
                           unsigned long long* stats) {
@@ -100,7 +123,9 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg
         rb0 = one.root_box[0]; rb1 = one.root_box[1]; rb2 = one.root_box[2];
         rb3 = one.root_box[3]; rb4 = one.root_box[4]; rb5 = one.root_box[5];
     }
-    int32_t stack[kStackN];
+    extern __shared__ int32_t sstack[];
+    int32_t* const sst = sstack + threadIdx.x;
+    int32_t lst[kStackN - kSmemN];
     float sdist[kCullPop ? kStackN : 1];
     TraceStats st;
     bool more = true;
@@ -166,14 +191,12 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg
             if (okl && okr) {
                 if (top + 1 >= kStackN) {
                     overflow = true;  // finish below with the flag
-                } else if (ml > mr) {  // the reference pushes the farther child, pops the nearer
-                    stack[++top] = dd.x;
-                    if (kCullPop) sdist[top] = ml;
-                    ref = dd.y;
-                } else {
-                    stack[++top] = dd.y;
-                    if (kCullPop) sdist[top] = mr;
-                    ref = dd.x;
+                } else {  // the reference pushes the farther child, pops the nearer
+                    const bool lfar = ml > mr;
+                    ++top;
+                    stack_put<kSmemN>(sst, lst, top, lfar ? dd.x : dd.y);
+                    if (kCullPop) sdist[top] = lfar ? ml : mr;
+                    ref = lfar ? dd.y : dd.x;
                 }
             } else if (okl) {
                 ref = dd.x;
@@ -210,7 +233,7 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg
                 while (top >= 0 && !(sdist[top] < best)) --top;
             }
             if (top < 0) finished = true;
-            else ref = stack[top--];
+            else ref = stack_get<kSmemN>(sst, lst, top--);
         }
         if (finished) {
             const TraceSeg& S = kSeg ? segs[seg] : one;
@@ -223,7 +246,7 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_closest(TraceSeg
     flush_stats<kStats>(st, stats);
 }
 
-template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack>
+template <bool kCullPop, bool kStats, bool kSeg, int kStackN = kStack, int kSmemN = 0>
 __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_any(TraceSeg one, const TraceSeg* __restrict__ segs, int nseg, int64_t n,
                       unsigned long long* counter, int refill, uint32_t max_steps, int* flag,
                       unsigned long long* stats) {
@@ -235,7 +258,9 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_any(TraceSeg one
     if (!kSeg && one.n_dev) n = *one.n_dev;
     const TNode* __restrict__ nodes = one.nodes;
     const TriRec* __restrict__ tris = one.tris;
-    int32_t stack[kStackN];
+    extern __shared__ int32_t sstack[];
+    int32_t* const sst = sstack + threadIdx.x;
+    int32_t lst[kStackN - kSmemN];
     TraceStats st;
     bool more = true;
     int64_t ray = -1;
@@ -305,12 +330,10 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_any(TraceSeg one
                 if (top + 1 >= kStackN) {
                     result = 2;
                     atomicOr(flag, kFlagStackOverflow);
-                } else if (ml > mr) {
-                    stack[++top] = dd.x;
-                    ref = dd.y;
                 } else {
-                    stack[++top] = dd.y;
-                    ref = dd.x;
+                    const bool lfar = ml > mr;
+                    stack_put<kSmemN>(sst, lst, ++top, lfar ? dd.x : dd.y);
+                    ref = lfar ? dd.y : dd.x;
                 }
             } else if (okl) {
                 ref = dd.x;
@@ -338,7 +361,7 @@ __global__ void __maxnreg__(kSeg || kStats ? 56 : kTraceRegs) k_any(TraceSeg one
         }
         if (result < 0 && pop) {
             if (top < 0) result = 0;
-            else ref = stack[top--];
+            else ref = stack_get<kSmemN>(sst, lst, top--);
         }
         if (result >= 0) {
             (kSeg ? segs[seg] : one).occ[ray] = (uint8_t)result;
@@ -361,25 +384,39 @@ TraceSeg seg_of(const cav_bvh* bvh) {
     return g;
 }
 
+// A persistent traversal launch: the grid fills every SM to the kernel's occupancy with
+// `dyn` bytes of shared traversal stacks per block.
+template <typename... P, typename... A>
+void run_trace(cav_ctx* ctx, void (*kernel)(P...), int block, size_t dyn, cudaStream_t s, A... args) {
+    const int grid = grid_for(ctx, kernel, block, dyn);
+    kernel<<<grid, block, dyn, s>>>(args...);
+}
+
 template <bool kStats, bool kSeg>
 cav_status launch_closest(cav_ctx* ctx, const TraceSeg& one, const TraceSeg* segs, int nseg, int64_t n, uint32_t flags,
                           cudaStream_t s, unsigned long long* counter, unsigned long long* stats, bool short_stack = false) {
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
     const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
     const uint32_t ms = ctx->max_trace_steps;
+    int* flag = ctx->d_error + 2;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
-    if (!kStats && !kSeg && short_stack && !(flags & CAV_TRACE_CULL_ON_POP)) {
-        int grid = grid_for(ctx, k_closest<false, false, false, kShortStack>, block);
-        k_closest<false, false, false, kShortStack><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms,
-                                                                          ctx->d_error + 2, stats);
+    const bool plain = !kStats && !kSeg && !(flags & CAV_TRACE_CULL_ON_POP);
+    const bool smem = plain && ctx->trace_smem_stack > 0;
+    const size_t dyn = smem ? stack_smem(block, kSmemStack) : 0;
+    if (plain && short_stack) {
+        if (smem)
+            run_trace(ctx, k_closest<false, false, false, kShortStack, kSmemStack>, block, dyn, s, one, segs, nseg, n,
+                      counter, batch, ms, flag, stats);
+        else
+            run_trace(ctx, k_closest<false, false, false, kShortStack>, block, dyn, s, one, segs, nseg, n, counter,
+                      batch, ms, flag, stats);
+    } else if (plain && smem) {
+        run_trace(ctx, k_closest<false, false, false, kStack, kSmemStack>, block, dyn, s, one, segs, nseg, n, counter,
+                  batch, ms, flag, stats);
     } else if (flags & CAV_TRACE_CULL_ON_POP) {
-        int grid = grid_for(ctx, k_closest<true, kStats, kSeg>, block);
-        k_closest<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms, ctx->d_error + 2,
-                                                             stats);
+        run_trace(ctx, k_closest<true, kStats, kSeg>, block, dyn, s, one, segs, nseg, n, counter, batch, ms, flag, stats);
     } else {
-        int grid = grid_for(ctx, k_closest<false, kStats, kSeg>, block);
-        k_closest<false, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms, ctx->d_error + 2,
-                                                              stats);
+        run_trace(ctx, k_closest<false, kStats, kSeg>, block, dyn, s, one, segs, nseg, n, counter, batch, ms, flag, stats);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;
@@ -391,17 +428,25 @@ cav_status launch_any(cav_ctx* ctx, const TraceSeg& one, const TraceSeg* segs, i
     const int block = ctx->trace_block > 0 ? ctx->trace_block : 128;
     const int batch = ctx->trace_batch > 0 ? ctx->trace_batch : kDefaultRefill;
     const uint32_t ms = ctx->max_trace_steps;
+    int* flag = ctx->d_error + 3;
     CAV_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
-    if (!kStats && !kSeg && short_stack && !(flags & CAV_TRACE_CULL_ON_POP)) {
-        int grid = grid_for(ctx, k_any<false, false, false, kShortStack>, block);
-        k_any<false, false, false, kShortStack><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms,
-                                                                      ctx->d_error + 3, stats);
+    const bool plain = !kStats && !kSeg && !(flags & CAV_TRACE_CULL_ON_POP);
+    const bool smem = plain && ctx->trace_smem_stack > 0;
+    const size_t dyn = smem ? stack_smem(block, kSmemStack) : 0;
+    if (plain && short_stack) {
+        if (smem)
+            run_trace(ctx, k_any<false, false, false, kShortStack, kSmemStack>, block, dyn, s, one, segs, nseg, n,
+                      counter, batch, ms, flag, stats);
+        else
+            run_trace(ctx, k_any<false, false, false, kShortStack>, block, dyn, s, one, segs, nseg, n, counter, batch,
+                      ms, flag, stats);
+    } else if (plain && smem) {
+        run_trace(ctx, k_any<false, false, false, kStack, kSmemStack>, block, dyn, s, one, segs, nseg, n, counter,
+                  batch, ms, flag, stats);
     } else if (flags & CAV_TRACE_CULL_ON_POP) {
-        int grid = grid_for(ctx, k_any<true, kStats, kSeg>, block);
-        k_any<true, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms, ctx->d_error + 3, stats);
+        run_trace(ctx, k_any<true, kStats, kSeg>, block, dyn, s, one, segs, nseg, n, counter, batch, ms, flag, stats);
     } else {
-        int grid = grid_for(ctx, k_any<false, kStats, kSeg>, block);
-        k_any<false, kStats, kSeg><<<grid, block, 0, s>>>(one, segs, nseg, n, counter, batch, ms, ctx->d_error + 3, stats);
+        run_trace(ctx, k_any<false, kStats, kSeg>, block, dyn, s, one, segs, nseg, n, counter, batch, ms, flag, stats);
     }
     CAV_CUDA(ctx, cudaGetLastError());
     return CAV_OK;
@@ -710,40 +755,45 @@ extern "C" cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh,
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    const int saved[6] = {ctx->trace_block, ctx->trace_blocks_per_sm, ctx->trace_batch, ctx->trace_stack,
-                          ctx->wide_block, ctx->wide_batch};
-    cav_trace_config_t best{0, 0, 0, 0, 1e30f};
+    const int saved[7] = {ctx->trace_block, ctx->trace_blocks_per_sm, ctx->trace_batch, ctx->trace_stack,
+                          ctx->wide_block, ctx->wide_batch, ctx->trace_smem_stack};
+    cav_trace_config_t best{0, 0, 0, 0, 1e30f, 0};
     const int blocks[] = {64, 128, 256};
     const int batches[] = {1, 2, 4, 8, 16, 32};
     const int stacks[] = {kStack, kShortStack};
+    const int smems[] = {0, kSmemStack};
     cav_status st = CAV_OK;
     for (int stk : stacks) {
-        if (stk == kShortStack && (wide || !(bvh->depth + 1 < kShortStack))) continue;
-        for (int blk : blocks)
-            for (int bat : batches) {
-                if (wide) {
-                    ctx->wide_block = blk;
-                    ctx->wide_batch = bat;
-                } else {
-                    ctx->trace_block = blk;
-                    ctx->trace_blocks_per_sm = 0;
-                    ctx->trace_batch = bat;
-                    ctx->trace_stack = stk;
+        for (int sm : smems) {
+            if (stk == kShortStack && (wide || !(bvh->depth + 1 < kShortStack))) continue;
+            if (sm > 0 && wide) continue;
+            for (int blk : blocks)
+                for (int bat : batches) {
+                    if (wide) {
+                        ctx->wide_block = blk;
+                        ctx->wide_batch = bat;
+                    } else {
+                        ctx->trace_block = blk;
+                        ctx->trace_blocks_per_sm = 0;
+                        ctx->trace_batch = bat;
+                        ctx->trace_stack = stk;
+                        ctx->trace_smem_stack = sm;
+                    }
+                    float ms_best = 1e30f;
+                    for (int rep = 0; rep < 3 && st == CAV_OK; ++rep) {  // first repetition warms up
+                        cudaEventRecord(a, s);
+                        st = any_hit ? trace_any(ctx, bvh, rays, limit, excl, n, occ, flags, s, ctx->d_counters + 5)
+                                     : trace_closest(ctx, bvh, rays, n, prim, t, uv, flags, s, ctx->d_counters + 5);
+                        cudaEventRecord(b, s);
+                        cudaEventSynchronize(b);
+                        float ms = 0;
+                        cudaEventElapsedTime(&ms, a, b);
+                        if (rep > 0) ms_best = std::min(ms_best, ms);
+                    }
+                    if (st != CAV_OK) break;
+                    if (ms_best < best.ms) best = cav_trace_config_t{blk, 0, bat, stk, ms_best, sm};
                 }
-                float ms_best = 1e30f;
-                for (int rep = 0; rep < 3 && st == CAV_OK; ++rep) {  // first repetition warms up
-                    cudaEventRecord(a, s);
-                    st = any_hit ? trace_any(ctx, bvh, rays, limit, excl, n, occ, flags, s, ctx->d_counters + 5)
-                                 : trace_closest(ctx, bvh, rays, n, prim, t, uv, flags, s, ctx->d_counters + 5);
-                    cudaEventRecord(b, s);
-                    cudaEventSynchronize(b);
-                    float ms = 0;
-                    cudaEventElapsedTime(&ms, a, b);
-                    if (rep > 0) ms_best = std::min(ms_best, ms);
-                }
-                if (st != CAV_OK) break;
-                if (ms_best < best.ms) best = cav_trace_config_t{blk, 0, bat, stk, ms_best};
-            }
+        }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -755,6 +805,7 @@ extern "C" cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh,
         ctx->trace_stack = saved[3];
         ctx->wide_block = saved[4];
         ctx->wide_batch = saved[5];
+        ctx->trace_smem_stack = saved[6];
         return st != CAV_OK ? st : set_error(ctx, CAV_ERR_CUDA, "cav_trace_autotune: no candidate ran");
     }
     if (wide) {
@@ -762,14 +813,17 @@ extern "C" cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh,
         ctx->trace_blocks_per_sm = saved[1];
         ctx->trace_batch = saved[2];
         ctx->trace_stack = saved[3];
+        ctx->trace_smem_stack = saved[6];
         ctx->wide_block = best.block_threads;
         ctx->wide_batch = best.batch;
         best.stack = 0;
+        best.smem_stack = 0;
     } else {
         ctx->trace_block = best.block_threads;
         ctx->trace_blocks_per_sm = 0;
         ctx->trace_batch = best.batch;
         ctx->trace_stack = best.stack;
+        ctx->trace_smem_stack = best.smem_stack;
         ctx->wide_block = saved[4];
         ctx->wide_batch = saved[5];
     }

@@ -95,10 +95,11 @@ __device__ inline void flush_stats(const TraceStats& st, unsigned long long* sta
 // Blocks of a persistent traversal launch: every SM filled to the kernel's occupancy (or
 // the context's configured blocks per SM).
 template <typename K>
-int grid_for(cav_ctx* ctx, K kernel, int block) {
+int grid_for(cav_ctx* ctx, K kernel, int block, size_t dyn_smem = 0) {
+    if (dyn_smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
     int per_sm = ctx->trace_blocks_per_sm;
     if (per_sm <= 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, dyn_smem);
         if (per_sm < 1) per_sm = 1;
     }
     return ctx->num_sms * per_sm;

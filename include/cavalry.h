@@ -204,6 +204,15 @@ cav_status cav_trace_any_host(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* r
  *                   that many new rays from the work counter with one atomic
  */
 cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_sm, int batch);
+/*
+ * Traversal-stack override of the exact mode's single-tree launches (the autotuner sets it):
+ *   stack      : 64 (used only where the tree's depth fits) or 128 entries per lane; 0 = 128
+ *   smem_stack : 16 keeps the stack's first 16 entries in shared memory (one L1 wavefront per
+ *                push or pop whatever the lanes' depths; less L1 for node data), 0 keeps the
+ *                whole stack in local memory
+ * Results do not depend on either choice.
+ */
+cav_status cav_set_trace_stack(cav_ctx* ctx, int stack, int smem_stack);
 
 /*
  * Allocation-free Morton codes + stable sort (the first stages of BVH::build,
@@ -434,12 +443,15 @@ cav_status cav_server_stats(cav_server* server, cav_server_stats_t* out);
 
 /* Launch-shape autotuner: times the closest-hit (any_hit = 0) or any-hit traversal of a
  * DEVICE ray sample over candidate shapes (64/128/256 threads per block; queue chunk 1-32;
- * a 64-entry traversal stack when the tree's depth allows it, else 128) and installs the
- * fastest in ctx for later single-tree traversals (merged launches always use the full
- * stack).  ms is the best launch time of the chosen shape on the sample. */
+ * a 64-entry traversal stack when the tree's depth allows it, else 128; the stack's first
+ * 16 entries in shared memory or all of it in local memory) and installs the fastest in ctx
+ * for later single-tree traversals (merged launches always use the full stack in local
+ * memory).  ms is the best launch time of the chosen shape on the sample; smem_stack is the
+ * number of stack entries per lane the chosen shape keeps in shared memory (16 or 0). */
 typedef struct cav_trace_config_t {
     int block_threads, blocks_per_sm, batch, stack;
     float ms;
+    int smem_stack;
 } cav_trace_config_t;
 cav_status cav_trace_autotune(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, int64_t n, int any_hit,
                               const float* limit, const int32_t* excl, void* stream, cav_trace_config_t* best);

@@ -57,3 +57,43 @@ def test_autotune_fast_mode_keeps_results_and_its_own_shape():
     pe, te, _ = bvh.trace_closest(rays)
     assert exact["ms"] > 0 and (pe.cpu().numpy() >= -1).all()
     ctx.sync_check()
+
+
+def test_every_stack_placement_gives_the_same_hits():
+    """The exact kernels' stack in local memory or with its first 16 entries in shared memory
+    (deeper entries spill to local memory: some of these rays go deeper than 16), short or
+    full, under several block sizes: identical closest and any hits."""
+    import torch
+
+    import cavalry_b200 as cav
+    from cavalry_b200 import scenes
+
+    ctx = cav.Context(0)
+    try:
+        pos, idx = scenes.soup(200_000, seed=17)
+        bvh = ctx.build(torch.from_numpy(pos).cuda(), torch.from_numpy(idx).cuda(), rounds=2)
+        rays = torch.from_numpy(scenes.closest_rays(300_000, seed=18)).cuda()
+        srays, lim = scenes.shadow_rays(300_000, seed=19)
+        srays, lim = torch.from_numpy(srays).cuda(), torch.from_numpy(lim).cuda()
+        ref = None
+        for stack in (128, 64):
+            for smem in (0, 16):
+                for block in (64, 256):
+                    ctx.set_trace_config(block, 0, 4)
+                    ctx.set_trace_stack(stack, smem)
+                    p, t, uv = bvh.trace_closest(rays)
+                    o = bvh.trace_any(srays, lim)
+                    got = (p.cpu().numpy(), t.cpu().numpy().view(np.uint32), uv.cpu().numpy().view(np.uint32),
+                           o.cpu().numpy())
+                    if ref is None:
+                        ref = got
+                    else:
+                        for a, b in zip(ref, got):
+                            assert np.array_equal(a, b), (stack, smem, block)
+        with pytest.raises(RuntimeError):
+            ctx.set_trace_stack(128, 8)
+        ctx.set_trace_stack(0, 0)
+        ctx.sync_check()
+        bvh.free()
+    finally:
+        ctx.close()
