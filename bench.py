@@ -203,7 +203,7 @@ def run_ours(args):
         vals = [int(x) for x in args.launch_shape.split(",")]
         blk, chunk, smem = vals[0], vals[1], (vals[2] if len(vals) > 2 else 0)
         ctx.set_trace_config(blk, 0, chunk)
-        ctx.set_trace_stack(128, smem)
+        ctx.set_trace_stack(128, smem, flags=cav.TRACE_EXACT)
         tuned = {"block_threads": blk, "batch": chunk, "stack": 128, "smem_stack": smem, "picked_by": "--launch-shape"}
     else:
         # tuned on a separate sample of the step's size in the given order: a 1M-ray sample,
@@ -436,7 +436,8 @@ def run_ours(args):
             "wide_nodes_per_ray": round(fnodes / N_RAYS, 3), "tris_per_ray": round(ftris / N_RAYS, 3),
             "algorithmic_bytes_per_ray": round(fast_bytes, 2),
             "achieved_gbs": round(fast_bytes * N_RAYS / (fast_ms_step * 1e-3) / 1e9, 1),
-            "launch_shape": {"block": tuned_fast["block_threads"], "queue_chunk": tuned_fast["batch"]},
+            "launch_shape": {"block": tuned_fast["block_threads"], "queue_chunk": tuned_fast["batch"],
+                             "smem_stack": tuned_fast.get("smem_stack", 0)},
             "kernel": "k_trace_wide<false,false> (compressed 8-wide nodes, 80 B)",
         },
         "build": {
@@ -606,7 +607,7 @@ def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, close
     sc_r.free()
     # the soup bench's own launch shape is restored for anything measured after this block
     ctx.set_trace_config(closest_shape["block_threads"], 0, closest_shape["batch"])
-    ctx.set_trace_stack(closest_shape["stack"], closest_shape.get("smem_stack", 0))
+    ctx.set_trace_stack(closest_shape["stack"], closest_shape.get("smem_stack", 0), flags=cav.TRACE_EXACT)
     return out
 
 

@@ -89,7 +89,7 @@ def lib() -> ctypes.CDLL:
         "cav_trace_closest_host": ([P, P, P, I64, P, P, P, U32], ctypes.c_int),
         "cav_trace_any_host": ([P, P, P, P, P, I64, P, U32], ctypes.c_int),
         "cav_set_trace_config": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
-        "cav_set_trace_stack": ([P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "cav_set_trace_stack": ([P, ctypes.c_uint32, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "cav_ctx_set_limits": ([P, ctypes.c_double, I64], ctypes.c_int),
         "cav_ctx_inject": ([P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "cav_server_cancel": ([P, I64], ctypes.c_int),
@@ -203,10 +203,11 @@ class Context:
         self._check(lib().cav_set_trace_config(self.handle, block_threads, blocks_per_sm, batch),
                     "cav_set_trace_config")
 
-    def set_trace_stack(self, stack: int = 0, smem_stack: int = 0):
-        """Exact-mode traversal stack: 64 or 128 entries (0 = 128), the first 16 in shared
-        memory (smem_stack=16) or all in local memory (0)."""
-        self._check(lib().cav_set_trace_stack(self.handle, stack, smem_stack), "cav_set_trace_stack")
+    def set_trace_stack(self, stack: int = 0, smem_stack: int = 0, flags: int = 0):
+        """Traversal stack of the exact mode (flags=TRACE_EXACT): 64 or 128 entries (0 = 128),
+        the first 16 in shared memory (smem_stack=16) or all in local memory (0); of the fast
+        mode (flags=TRACE_FAST): stack 0, the first 8 node groups in shared memory or none."""
+        self._check(lib().cav_set_trace_stack(self.handle, flags, stack, smem_stack), "cav_set_trace_stack")
 
     def build_batch(self, scenes, rounds: int = 0, stream=None) -> list:
         """Build many BVHs with one launch per LBVH stage: scenes = [(positions, indices) or

@@ -153,9 +153,16 @@ cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_
     return CAV_OK;
 }
 
-cav_status cav_set_trace_stack(cav_ctx* ctx, int stack, int smem_stack) {
+cav_status cav_set_trace_stack(cav_ctx* ctx, uint32_t flags, int stack, int smem_stack) {
     if (!ctx) return CAV_ERR_INVALID_ARGUMENT;
-    if ((stack != 0 && stack != 64 && stack != 128) || (smem_stack != 0 && smem_stack != 16))
+    if (flags & CAV_TRACE_FAST) {
+        if (flags != CAV_TRACE_FAST || stack != 0 || (smem_stack != 0 && smem_stack != kWideSmemStack))
+            return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_set_trace_stack: fast mode takes stack 0, smem_stack 0/8");
+        ctx->wide_smem_stack = smem_stack;
+        return CAV_OK;
+    }
+    if (flags != CAV_TRACE_EXACT || (stack != 0 && stack != 64 && stack != 128) ||
+        (smem_stack != 0 && smem_stack != 16))
         return set_error(ctx, CAV_ERR_INVALID_ARGUMENT, "cav_set_trace_stack: stack 0/64/128, smem_stack 0/16");
     ctx->trace_stack = stack;
     ctx->trace_smem_stack = smem_stack;

@@ -133,6 +133,7 @@ struct cav_ctx {
     // launch configuration of the fast (compressed 8-wide) mode (0 = defaults)
     int wide_block = 0;
     int wide_batch = 0;
+    int wide_smem_stack = 0;  // > 0: the fast mode's first stack entries in shared memory
     // persistent work counters (device), one per concurrent trace kind
     unsigned long long* d_counters = nullptr;
     int* d_error = nullptr;

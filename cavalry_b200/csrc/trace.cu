@@ -755,23 +755,23 @@ extern "C" cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh,
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    const int saved[7] = {ctx->trace_block, ctx->trace_blocks_per_sm, ctx->trace_batch, ctx->trace_stack,
-                          ctx->wide_block, ctx->wide_batch, ctx->trace_smem_stack};
+    const int saved[8] = {ctx->trace_block, ctx->trace_blocks_per_sm, ctx->trace_batch, ctx->trace_stack,
+                          ctx->wide_block, ctx->wide_batch, ctx->trace_smem_stack, ctx->wide_smem_stack};
     cav_trace_config_t best{0, 0, 0, 0, 1e30f, 0};
     const int blocks[] = {64, 128, 256};
     const int batches[] = {1, 2, 4, 8, 16, 32};
     const int stacks[] = {kStack, kShortStack};
-    const int smems[] = {0, kSmemStack};
+    const int smems[] = {0, wide ? kWideSmemStack : kSmemStack};
     cav_status st = CAV_OK;
     for (int stk : stacks) {
         for (int sm : smems) {
             if (stk == kShortStack && (wide || !(bvh->depth + 1 < kShortStack))) continue;
-            if (sm > 0 && wide) continue;
             for (int blk : blocks)
                 for (int bat : batches) {
                     if (wide) {
                         ctx->wide_block = blk;
                         ctx->wide_batch = bat;
+                        ctx->wide_smem_stack = sm;
                     } else {
                         ctx->trace_block = blk;
                         ctx->trace_blocks_per_sm = 0;
@@ -806,6 +806,7 @@ extern "C" cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh,
         ctx->wide_block = saved[4];
         ctx->wide_batch = saved[5];
         ctx->trace_smem_stack = saved[6];
+        ctx->wide_smem_stack = saved[7];
         return st != CAV_OK ? st : set_error(ctx, CAV_ERR_CUDA, "cav_trace_autotune: no candidate ran");
     }
     if (wide) {
@@ -816,8 +817,8 @@ extern "C" cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh,
         ctx->trace_smem_stack = saved[6];
         ctx->wide_block = best.block_threads;
         ctx->wide_batch = best.batch;
+        ctx->wide_smem_stack = best.smem_stack;
         best.stack = 0;
-        best.smem_stack = 0;
     } else {
         ctx->trace_block = best.block_threads;
         ctx->trace_blocks_per_sm = 0;
@@ -826,6 +827,7 @@ extern "C" cav_status cav_trace_autotune_flags(cav_ctx* ctx, const cav_bvh* bvh,
         ctx->trace_smem_stack = best.smem_stack;
         ctx->wide_block = saved[4];
         ctx->wide_batch = saved[5];
+        ctx->wide_smem_stack = saved[7];
     }
     if (best_out) *best_out = best;
     return CAV_OK;

@@ -12,6 +12,9 @@ constexpr uint32_t kMaxSteps = 1u << 22;  // default node+triangle visits per ra
 constexpr int kFlagStackOverflow = 1;  // a push found the traversal stack full
 constexpr int kFlagStepLimit = 2;      // a ray reached the context's step limit
 constexpr int kDefaultRefill = 4;         // idle lanes that trigger a warp's next claim
+// Node groups of the fast mode's stack kept per lane in shared memory when the autotuner
+// picks that placement (a lane holds at most one group per wide level).
+constexpr int kWideSmemStack = 8;
 constexpr unsigned kFull = 0xffffffffu;
 
 // rayTriangleIntersection (Core/Triangle.h:7-57) on precomputed edges.

@@ -288,7 +288,21 @@ __device__ __forceinline__ uint32_t node_hits(const CNode* __restrict__ cn, uint
 // 64 registers, unconstrained: the kernel is ALU-bound, and capping it for more resident
 // warps made the 5.24M-triangle render's extend stage slower (231 ms at 64 registers, 263 at
 // 48, 302 at 40).
-template <bool kAny, bool kStats, bool kSeg>
+// The first kSmemN node groups of a lane's stack in shared memory, [entry][thread] (a warp's
+// push or pop is two conflict-free wavefronts whatever the lanes' depths), the rest in local
+// memory; kSmemN == 0 keeps all of it in local memory.
+template <int kSmemN>
+__device__ __forceinline__ void wstack_put(uint2* sst, uint2* lst, int i, uint2 v) {
+    if (kSmemN > 0 && i < kSmemN) sst[i * (int)blockDim.x] = v;
+    else lst[i - kSmemN] = v;
+}
+
+template <int kSmemN>
+__device__ __forceinline__ uint2 wstack_get(const uint2* sst, const uint2* lst, int i) {
+    return kSmemN > 0 && i < kSmemN ? sst[i * (int)blockDim.x] : lst[i - kSmemN];
+}
+
+template <bool kAny, bool kStats, bool kSeg, int kSmemN = 0>
 __global__ void __launch_bounds__(256)
     k_trace_wide(const CNode* __restrict__ cn0, const TriRec* __restrict__ tris0, const cav_ray* __restrict__ rays0,
                  int64_t n, const uint32_t* n_dev, int32_t* prim0, float* tout0, float* uv0,
@@ -306,7 +320,9 @@ __global__ void __launch_bounds__(256)
     const TriRec* __restrict__ tris = tris0;
     int seg = 0;
     TraceStats st;
-    uint2 stack[kWideStack];
+    extern __shared__ uint2 wsstack[];
+    uint2* const sst = wsstack + threadIdx.x;
+    uint2 lst[kWideStack - kSmemN];
     bool more = true;
     int64_t ray = -1;
     WideRay R{};
@@ -387,7 +403,7 @@ __global__ void __launch_bounds__(256)
                     finished = true;
                     result = 0;
                 } else {
-                    grp = stack[top--];
+                    grp = wstack_get<kSmemN>(sst, lst, top--);
                 }
             }
             if (!finished) {
@@ -397,7 +413,7 @@ __global__ void __launch_bounds__(256)
                 const uint32_t idx = grp.x + __popc(grp.y & 0xFFu & ((1u << slot) - 1u));
                 if (grp.y & 0xFF000000u) {
                     if (top + 1 >= kWideStack) overflow = true;  // flagged below
-                    else stack[++top] = grp;
+                    else wstack_put<kSmemN>(sst, lst, ++top, grp);
                 }
                 uint32_t cbase, tbase, imask;
                 const float bound = kAny ? lim : fminf(best, tmax);
@@ -471,6 +487,12 @@ cav_status launch_wide(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* rays, in
         k_trace_wide<kAny, true, false><<<grid, block, 0, s>>>(bvh->cnodes, bvh->ctris, rays, n, n_dev, prim, t, uv,
                                                                limit, excl, occ, counter, batch, ctx->max_trace_steps, flag, stats,
                                                                nullptr, 0);
+    } else if (ctx->wide_smem_stack > 0) {
+        const size_t dyn = sizeof(uint2) * kWideSmemStack * (size_t)block;
+        const int grid = grid_for(ctx, k_trace_wide<kAny, false, false, kWideSmemStack>, block, dyn);
+        k_trace_wide<kAny, false, false, kWideSmemStack><<<grid, block, dyn, s>>>(
+            bvh->cnodes, bvh->ctris, rays, n, n_dev, prim, t, uv, limit, excl, occ, counter, batch,
+            ctx->max_trace_steps, flag, nullptr, nullptr, 0);
     } else {
         const int grid = grid_for(ctx, k_trace_wide<kAny, false, false>, block);
         k_trace_wide<kAny, false, false><<<grid, block, 0, s>>>(bvh->cnodes, bvh->ctris, rays, n, n_dev, prim, t, uv,

@@ -205,14 +205,16 @@ cav_status cav_trace_any_host(cav_ctx* ctx, const cav_bvh* bvh, const cav_ray* r
  */
 cav_status cav_set_trace_config(cav_ctx* ctx, int block_threads, int blocks_per_sm, int batch);
 /*
- * Traversal-stack override of the exact mode's single-tree launches (the autotuner sets it):
- *   stack      : 64 (used only where the tree's depth fits) or 128 entries per lane; 0 = 128
- *   smem_stack : 16 keeps the stack's first 16 entries in shared memory (one L1 wavefront per
- *                push or pop whatever the lanes' depths; less L1 for node data), 0 keeps the
- *                whole stack in local memory
+ * Traversal-stack override of a mode's single-tree launches (the autotuner sets it):
+ *   flags      : CAV_TRACE_EXACT or CAV_TRACE_FAST, the mode whose stack is set
+ *   stack      : exact mode: 64 (used only where the tree's depth fits) or 128 entries per
+ *                lane, 0 = 128; fast mode: 0
+ *   smem_stack : entries per lane kept in shared memory (exact: 16 or 0, fast: 8 or 0); the
+ *                rest of the stack is in local memory.  Shared entries cost one L1 wavefront
+ *                per push or pop whatever the lanes' depths, and leave less L1 for node data.
  * Results do not depend on either choice.
  */
-cav_status cav_set_trace_stack(cav_ctx* ctx, int stack, int smem_stack);
+cav_status cav_set_trace_stack(cav_ctx* ctx, uint32_t flags, int stack, int smem_stack);
 
 /*
  * Allocation-free Morton codes + stable sort (the first stages of BVH::build,
@@ -447,7 +449,8 @@ cav_status cav_server_stats(cav_server* server, cav_server_stats_t* out);
  * 16 entries in shared memory or all of it in local memory) and installs the fastest in ctx
  * for later single-tree traversals (merged launches always use the full stack in local
  * memory).  ms is the best launch time of the chosen shape on the sample; smem_stack is the
- * number of stack entries per lane the chosen shape keeps in shared memory (16 or 0). */
+ * number of stack entries per lane the chosen shape keeps in shared memory (exact mode 16 or
+ * 0, fast mode 8 or 0). */
 typedef struct cav_trace_config_t {
     int block_threads, blocks_per_sm, batch, stack;
     float ms;

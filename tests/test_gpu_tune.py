@@ -93,6 +93,22 @@ def test_every_stack_placement_gives_the_same_hits():
         with pytest.raises(RuntimeError):
             ctx.set_trace_stack(128, 8)
         ctx.set_trace_stack(0, 0)
+        # the fast mode's node-group stack: the first 8 groups in shared memory or none
+        fref = None
+        for smem in (0, 8):
+            ctx.set_trace_stack(0, smem, flags=cav.TRACE_FAST)
+            p, t, uv = bvh.trace_closest(rays, flags=cav.TRACE_FAST)
+            o = bvh.trace_any(srays, lim, flags=cav.TRACE_FAST)
+            got = (p.cpu().numpy(), t.cpu().numpy().view(np.uint32), uv.cpu().numpy().view(np.uint32), o.cpu().numpy())
+            if fref is None:
+                fref = got
+            else:
+                for a, b in zip(fref, got):
+                    assert np.array_equal(a, b), ("fast", smem)
+        assert np.array_equal(fref[3], ref[3])  # any-hit answers agree across the modes
+        with pytest.raises(RuntimeError):
+            ctx.set_trace_stack(0, 16, flags=cav.TRACE_FAST)
+        ctx.set_trace_stack(0, 0, flags=cav.TRACE_FAST)
         ctx.sync_check()
         bvh.free()
     finally:
