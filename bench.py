@@ -550,7 +550,7 @@ def reference_cuda_block(ctx, d_pos, d_idx, pos, idx, bvh, rays_np, value, close
     out["soup_1M_closest_3_rounds"] = {"ref_mrays_s": round(ref_mrays, 2), "ours_mrays_s": value,
                                        "ours_given_order_mrays_s": given_value,
                                        "speedup": round(value / ref_mrays, 2), "rays": len(rays_np)}
-    # (3) the 5.24M-triangle scene at 0 rounds: the north-star comparison
+    # (3) the 5.24M-triangle scene at 0 rounds: closest hit against the reference on its own LBVH
     sc_np = scenes.sphere_scene(64, 6, seed=9)
     tmp = tempfile.mkdtemp()
     path = _os.path.join(tmp, "spheres.pbrt")
