@@ -90,6 +90,40 @@ __device__ inline void store_rec(BNode* nodes, int32_t id, const Rec& r) {
 
 __device__ inline bool is_pow2(int n) { return (n & (n - 1)) == 0; }
 
+// The reference's warp reduction of partition costs (Optimization.cu:224-266, :271-324): for
+// d = 16, 8, 4, 2, 1 lane l takes lane min(l + d, 31)'s candidate when its own is the empty
+// -1 or the other is smaller.  Lane 0 ends with the smallest cost; among equal costs with the
+// lane whose 5-bit index read backwards is smallest (the bracket keeps the lower lane of
+// every pair), and an empty candidate (only lane 0's can be) loses to any other.  Costs are
+// non-negative floats, whose bit patterns order like their values, so two min-reductions find
+// the same winner; a NaN or negative cost anywhere takes the reference's own loop.  Every lane
+// returns lane 0's result.
+__device__ inline void reduce_partition(float& tc, int& p) {
+    const int lane = threadIdx.x & 31;
+    const bool empty = tc == -1.f;
+    if (__any_sync(kFull, !empty && !(tc >= 0.f))) {
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+            const int o = min(lane + d, 31);
+            const float oc = __shfl_sync(kFull, tc, o);
+            const int op = __shfl_sync(kFull, p, o);
+            if (tc == -1.f || oc < tc) {
+                tc = oc;
+                p = op;
+            }
+        }
+        tc = __shfl_sync(kFull, tc, 0);
+        p = __shfl_sync(kFull, p, 0);
+        return;
+    }
+    const unsigned key = empty ? 0xffffffffu : __float_as_uint(tc + 0.f);  // +0 for a -0 cost
+    const unsigned best = __reduce_min_sync(kFull, key);
+    const unsigned rev = __brev((unsigned)lane) >> 27;
+    const unsigned win = __brev(__reduce_min_sync(kFull, key == best ? rev : 0xffffffffu)) >> 27;
+    tc = __shfl_sync(kFull, tc, (int)win);
+    p = __shfl_sync(kFull, p, (int)win);
+}
+
 // optimizeTreelet semantics for the subtree rooted at `root`.  Returns false only on
 // an internal inconsistency (recorded in *err by the caller).
 __device__ bool optimize_treelet(BNode* nodes, int32_t root, int32_t count, WarpSmem& S) {
@@ -106,16 +140,25 @@ __device__ bool optimize_treelet(BNode* nodes, int32_t root, int32_t count, Warp
     bool expanded = false;
     int size = 1;
     while (size < 13) {
-        float my_area = rec.area;
-        if (rec.is_leaf || expanded) my_area = -1.f;
+        // the first of lanes 0..size-1 with the largest area above -1 (lane 0 when none):
+        // areas are non-negative, so their bit patterns order like their values
+        const bool cand = lane < size && !(rec.is_leaf || expanded) && rec.area > -1.f;
         int max_lane = 0;
-        float max_area = -1.f;
-        for (int i = 0; i < size; ++i) {
-            float a = __shfl_sync(kFull, my_area, i);
-            if (a > max_area) {
-                max_area = a;
-                max_lane = i;
+        if (__any_sync(kFull, cand && !(rec.area >= 0.f))) {  // a negative area: a plain scan
+            float my_area = rec.area;
+            if (rec.is_leaf || expanded) my_area = -1.f;
+            float max_area = -1.f;
+            for (int i = 0; i < size; ++i) {
+                float a = __shfl_sync(kFull, my_area, i);
+                if (a > max_area) {
+                    max_area = a;
+                    max_lane = i;
+                }
             }
+        } else {
+            const unsigned key = cand ? __float_as_uint(rec.area + 0.f) + 1u : 0u;
+            const unsigned top = __reduce_max_sync(kFull, key);
+            if (top != 0u) max_lane = __ffs(__ballot_sync(kFull, key == top)) - 1;
         }
         int stop = __shfl_sync(kFull, (int)(expanded || rec.is_leaf), max_lane);
         if (stop) return true;  // fewer than 7 leaves reachable: leave the subtree as it is
@@ -222,16 +265,7 @@ __device__ bool optimize_treelet(BNode* nodes, int32_t root, int32_t count, Warp
         int p = (lane & ((1 << eb) - 1)) | hi;
         float tc = -1.f;
         if (p != 0) tc = S.cost[p] + S.cost[s ^ p];
-#pragma unroll
-        for (int d = 16; d >= 1; d >>= 1) {
-            int o = min(lane + d, 31);
-            float oc = __shfl_sync(kFull, tc, o);
-            int op = __shfl_sync(kFull, p, o);
-            if (tc == -1.f || oc < tc) {
-                tc = oc;
-                p = op;
-            }
-        }
+        reduce_partition(tc, p);
         if (lane == 0) {
             S.cost[s] = internal_cost(S.area[s], tc);
             S.part[s] = (signed char)p;
@@ -251,16 +285,7 @@ __device__ bool optimize_treelet(BNode* nodes, int32_t root, int32_t count, Warp
             tc = otc;
             p = op;
         }
-#pragma unroll
-        for (int d = 16; d >= 1; d >>= 1) {
-            int o = min(lane + d, 31);
-            float oc = __shfl_sync(kFull, tc, o);
-            int opp = __shfl_sync(kFull, p, o);
-            if (tc == -1.f || oc < tc) {
-                tc = oc;
-                p = opp;
-            }
-        }
+        reduce_partition(tc, p);
         if (lane == 0) {
             S.cost[s] = internal_cost(S.area[s], tc);
             S.part[s] = (signed char)p;
