@@ -60,6 +60,16 @@ struct PlyElem {
     std::vector<PlyProp> props;
 };
 
+// The fewest bytes one row of an element can take: binary, its scalar properties and the
+// count of each list; ASCII, one character per scalar or list count.  A header whose element
+// count cannot fit in the rest of the file is refused with this before anything is allocated
+// for the element (a damaged count would otherwise reserve gigabytes first).
+size_t min_row_bytes(const PlyElem& e, int fmt) {
+    size_t b = 0;
+    for (const PlyProp& p : e.props) b += fmt == 0 ? 1 : (size_t)type_size(p.list ? p.count_type : p.type);
+    return b;
+}
+
 // Sequential reader over the body: binary (either byte order) or ASCII tokens.
 struct PlyBody {
     const std::string& data;
@@ -171,6 +181,11 @@ PlyMesh read_ply(const std::string& path) {
     bool have_vertex = false, have_face = false;
     PlyBody body{data, pos, fmt, path};
     for (const PlyElem& e : elems) {
+        const size_t row = min_row_bytes(e, fmt);
+        const size_t left = body.pos <= data.size() ? data.size() - body.pos : 0;
+        if (row > 0 && (uint64_t)e.count > left / row)
+            throw ParseError("read ply file failed, element '" + e.name + "' count " + std::to_string(e.count) +
+                             " exceeds the data in " + path);
         if (e.name == "vertex") {
             have_vertex = true;
             int ix = -1, iy = -1, iz = -1, inx = -1, iny = -1, inz = -1, iu = -1, iv = -1;
