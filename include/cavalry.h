@@ -292,8 +292,9 @@ cav_status cav_pbrt_parse_info(const char* path, int spp_override, const char* i
 /* Host-only: decode a texture image exactly as scene loading does (Core/Texture.cu:27-83):
  * 8-bit RGBA, rows bottom-up (flipped on load), colour channels of a .png through the inverse
  * sRGB curve and truncated to 8 bits, alpha unchanged.  PNG only (greyscale, grey + alpha,
- * RGB, RGBA, palette; 8 or 16 bits; not interlaced).  With rgba null only width and height
- * are returned; otherwise capacity_bytes must hold 4 * width * height bytes. */
+ * RGB, RGBA, palette; 8 or 16 bits; not interlaced; at most 32768 texels per side).  With
+ * rgba null only width and height are returned; otherwise capacity_bytes must hold
+ * 4 * width * height bytes. */
 cav_status cav_load_texture_png(const char* path, uint8_t* rgba, int64_t capacity_bytes, int* width, int* height,
                                 char* err, int err_len);
 /* Host-only: decode an OpenEXR texture exactly as scene loading does for a file name ending in
@@ -302,8 +303,8 @@ cav_status cav_load_texture_png(const char* path, uint8_t* rgba, int64_t capacit
  * dropped), a missing A reads 1, a single channel fills all four.  Scanline images with NONE,
  * RLE, ZIPS or ZIP compression and HALF or FLOAT channels; tiled and multi-part files, UINT
  * channels and the PIZ / PXR24 / B44 / DWA codecs are refused (CAV_ERR_INVALID_ARGUMENT, the
- * reason in err).  With rgba null only width and height are returned; otherwise
- * capacity_floats must hold 4 * width * height floats. */
+ * reason in err), as is a data window of more than 2^28 pixels.  With rgba null only width
+ * and height are returned; otherwise capacity_floats must hold 4 * width * height floats. */
 cav_status cav_load_texture_exr(const char* path, float* rgba, int64_t capacity_floats, int* width, int* height,
                                 char* err, int err_len);
 cav_status cav_pbrt_load_triangles(const char* path, float* positions, int64_t max_vertices, int32_t* indices,
