@@ -6,7 +6,9 @@
 // Loads the scene with the host .pbrt parser, builds the BVH (R treelet rounds; -1 = the
 // reference's default), renders on the GPU and writes the 8-bit PNG the reference writes
 // (plus, with --pfm, the float film).
+#include <cerrno>
 #include <chrono>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -19,6 +21,19 @@ static void usage() {
     std::fprintf(stderr,
                  "usage: cavalry --input scene.pbrt [--output out.png] [--spp N] [--integrator path|rlpath]\n"
                  "               [--bvh-opt-rounds R] [--pfm film.pfm] [--device D]\n");
+}
+
+// A whole decimal int or exit 2: the reference reads these flags as ints through cxxopts,
+// which refuses anything else (std::atoi would read "abc" as 0 and overflow on long input).
+static int int_arg(const char* name, const std::string& v) {
+    errno = 0;
+    char* end = nullptr;
+    const long x = std::strtol(v.c_str(), &end, 10);
+    if (v.empty() || end != v.c_str() + v.size() || errno == ERANGE || x < INT_MIN || x > INT_MAX) {
+        std::fprintf(stderr, "invalid integer value '%s' for %s\n", v.c_str(), name);
+        std::exit(2);
+    }
+    return (int)x;
 }
 
 int main(int argc, char** argv) {
@@ -35,11 +50,11 @@ int main(int argc, char** argv) {
         };
         if (a == "--input") input = next("--input");
         else if (a == "--output") output = next("--output");
-        else if (a == "--spp") spp = std::atoi(next("--spp").c_str());
+        else if (a == "--spp") spp = int_arg("--spp", next("--spp"));
         else if (a == "--integrator") integrator = next("--integrator");
-        else if (a == "--bvh-opt-rounds") rounds = std::atoi(next("--bvh-opt-rounds").c_str());
+        else if (a == "--bvh-opt-rounds") rounds = int_arg("--bvh-opt-rounds", next("--bvh-opt-rounds"));
         else if (a == "--pfm") pfm = next("--pfm");
-        else if (a == "--device") device = std::atoi(next("--device").c_str());
+        else if (a == "--device") device = int_arg("--device", next("--device"));
         else if (a == "--help" || a == "-h") {
             usage();
             return 0;

@@ -411,3 +411,29 @@ def test_lexer_rejects_numbers_stof_rejects(tmp_path, text):
     p.write_text(f'LookAt 0 0 -3  0 0 0  0 1 0\nCamera "perspective" "float fov" [{text}]\nWorldBegin\nWorldEnd\n')
     with pytest.raises(cav.CavError, match="bad number"):
         cav.parse_pbrt(str(p))
+
+
+@pytest.mark.parametrize("args,msg", [
+    ([], "usage"),
+    (["--input"], "missing value for --input"),
+    (["--bogus"], "unknown argument --bogus"),
+    (["--input", "x.pbrt", "--spp", "abc"], "invalid integer value 'abc' for --spp"),
+    (["--input", "x.pbrt", "--spp", "12x"], "invalid integer value '12x' for --spp"),
+    (["--input", "x.pbrt", "--spp", "99999999999999"], "invalid integer value"),
+    (["--input", "x.pbrt", "--bvh-opt-rounds", ""], "invalid integer value '' for --bvh-opt-rounds"),
+    (["--input", "x.pbrt", "--device", "1.5"], "invalid integer value '1.5' for --device"),
+])
+def test_cli_refuses_bad_arguments(args, msg):
+    """The `cavalry` CLI reads --spp, --bvh-opt-rounds and --device as whole ints (the reference
+    parses them as ints through cxxopts, main.cu:25-96) and exits with status 2 on bad or
+    missing arguments, before it touches a GPU."""
+    import subprocess
+
+    from cavalry_b200 import build_ext
+
+    cli = build_ext.CLI
+    if not cli.exists():
+        build_ext.build_cli()
+    r = subprocess.run([str(cli), *args], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2
+    assert msg in r.stderr
