@@ -361,6 +361,10 @@ struct Parser {
     std::filesystem::path base;
     Scene& scene;
     std::map<std::string, Material> named;
+    // Included files whose spliced tokens are still ahead, innermost last: the file and the
+    // index just past its tokens.  A file that includes itself, directly or through others,
+    // would splice without end; it is refused instead.
+    std::vector<std::pair<std::string, size_t>> includes;
 
     Parser(const std::string& text, std::filesystem::path b, Scene& s) : base(std::move(b)), scene(s) {
         toks = lex(text, arena);
@@ -763,10 +767,19 @@ struct Parser {
                 if (it == named.end()) throw ParseError("Named material not found: " + n);
                 current_material = add_material(it->second);
             } else if (w == "Include") {
+                const size_t at = i;  // the directive's own position decides which includes enclose it
                 ++i;
                 std::string file = pop(Tok::String, "file name").text();
+                while (!includes.empty() && includes.back().second <= at) includes.pop_back();
+                std::error_code ec;
+                std::string key = std::filesystem::weakly_canonical(base / file, ec).string();
+                if (ec) key = (base / file).string();
+                for (const auto& open : includes)
+                    if (open.first == key) throw ParseError("Include cycle: " + file + " includes itself");
                 std::vector<Token> inc = lex(read_text(base / file), arena);
                 toks.insert(toks.begin() + (long)i, inc.begin(), inc.end());
+                for (auto& open : includes) open.second += inc.size();
+                includes.emplace_back(key, i + inc.size());
             } else if (w == "ReverseOrientation") {
                 ++i;
                 reverse = true;

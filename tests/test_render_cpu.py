@@ -178,6 +178,33 @@ def test_parser_include_and_named_material(tmp_path):
     assert info.meshes == 2 and info.lights == 1 and info.triangles == 4
 
 
+def test_parser_refuses_include_cycles_and_keeps_repeated_includes(tmp_path):
+    """Included files are spliced in place; a file that includes itself, directly, through
+    another file or as its last directive, would splice without end and is refused, while
+    including the same file several times without a cycle is kept."""
+    import cavalry_b200 as cav
+
+    light = 'AttributeBegin\nAreaLightSource "diffuse" "rgb L" [1 1 1]\n' + QUAD + 'AttributeEnd\n'
+    write(tmp_path, "leaf.pbrt", QUAD)
+    write(tmp_path, "twice.pbrt", 'Include "leaf.pbrt"\nInclude "leaf.pbrt"\n')
+    write(tmp_path, "self.pbrt", QUAD + 'Include "self.pbrt"\n')
+    write(tmp_path, "a.pbrt", 'Include "b.pbrt"\n')
+    write(tmp_path, "b.pbrt", QUAD + 'Include "a.pbrt"\n')
+    ok = write(tmp_path, "ok.pbrt", HEADER + "WorldBegin\n" + light +
+               'Include "twice.pbrt"\nInclude "leaf.pbrt"\nWorldEnd\n')
+    info, _ = cav.parse_pbrt(ok)
+    assert info.meshes == 4 and info.triangles == 8
+    for target in ("self.pbrt", "a.pbrt"):
+        p = write(tmp_path, "main.pbrt", HEADER + "WorldBegin\n" + light + f'Include "{target}"\nWorldEnd\n')
+        with pytest.raises(cav.CavError, match="Include cycle"):
+            cav.parse_pbrt(p)
+        with pytest.raises(cav.CavError, match="Include cycle"):
+            cav.load_pbrt_triangles(p)
+    p = write(tmp_path, "main.pbrt", HEADER + "WorldBegin\n" + light + 'Include "main.pbrt"\nWorldEnd\n')
+    with pytest.raises(cav.CavError, match="Include cycle"):
+        cav.parse_pbrt(p)
+
+
 @pytest.mark.parametrize("text,msg", [
     ('Camera "perspective" "float fov" [1e+05]\n', "unrecognized character"),
     ("Frobnicate 1 2 3\n", "Unrecognized Keyword"),
