@@ -152,6 +152,22 @@ def _ptr(t) -> int | None:
     return t.data_ptr()
 
 
+def _require_cuda(x, dtype, numel: int, name: str, device_index: int) -> None:
+    """Raise ValueError unless `x` is a contiguous CUDA tensor of `dtype` on GPU `device_index`
+    with at least `numel` elements: the kernels read or write that many through the raw
+    pointer, so a smaller or mistyped buffer would be overrun on the device."""
+    if not getattr(x, "is_cuda", False):
+        raise ValueError(f"{name}: expected a CUDA tensor")
+    if x.dtype != dtype:
+        raise ValueError(f"{name}: expected dtype {dtype}, got {x.dtype}")
+    if not x.is_contiguous():
+        raise ValueError(f"{name}: expected a contiguous tensor")
+    if x.device.index != device_index:
+        raise ValueError(f"{name}: on cuda:{x.device.index}, the context is on cuda:{device_index}")
+    if x.numel() < numel:
+        raise ValueError(f"{name}: {x.numel()} elements, at least {numel} needed")
+
+
 def _stream_ptr(stream) -> int | None:
     import torch
 
@@ -789,6 +805,14 @@ class Bvh:
                  stream=None) -> dict:
         """Pick and install the fastest traversal launch shape for this tree on a CUDA ray sample,
         for the exact mode or (flags=TRACE_FAST) the compressed 8-wide mode."""
+        import torch
+
+        n = rays.shape[0]
+        _require_cuda(rays, torch.float32, 8 * n, "rays", self.ctx.device)
+        if limit is not None:
+            _require_cuda(limit, torch.float32, n, "limit", self.ctx.device)
+        if excl is not None:
+            _require_cuda(excl, torch.int32, 2 * n, "excl", self.ctx.device)
         out = TraceConfig()
         st = lib().cav_trace_autotune_flags(self.ctx.handle, self.handle, _ptr(rays), rays.shape[0], int(any_hit),
                                             _ptr(limit), _ptr(excl), flags, _stream_ptr(stream),
@@ -806,12 +830,19 @@ class Bvh:
 
         assert rays.is_cuda and rays.dtype == torch.float32 and rays.is_contiguous() and rays.shape[-1] == 8
         n = rays.shape[0]
+        dev = self.ctx.device
+        _require_cuda(rays, torch.float32, 8 * n, "rays", dev)
         if out is None:
             prim = torch.empty(n, dtype=torch.int32, device=rays.device)
             t = torch.empty(n, dtype=torch.float32, device=rays.device)
             uv = torch.empty((n, 2), dtype=torch.float32, device=rays.device)
         else:
             prim, t, uv = out
+            _require_cuda(prim, torch.int32, n, "out prim", dev)
+            if t is not None:
+                _require_cuda(t, torch.float32, n, "out t", dev)
+            if uv is not None:
+                _require_cuda(uv, torch.float32, 2 * n, "out uv", dev)
         st = lib().cav_trace_closest(self.ctx.handle, self.handle, _ptr(rays), n, _ptr(prim), _ptr(t), _ptr(uv),
                                      int(flags), _stream_ptr(stream))
         self.ctx._check(st, "cav_trace_closest")
@@ -823,7 +854,14 @@ class Bvh:
 
         assert rays.is_cuda and rays.dtype == torch.float32 and rays.is_contiguous() and rays.shape[-1] == 8
         n = rays.shape[0]
+        dev = self.ctx.device
+        _require_cuda(rays, torch.float32, 8 * n, "rays", dev)
+        if limit is not None:
+            _require_cuda(limit, torch.float32, n, "limit", dev)
+        if excl is not None:
+            _require_cuda(excl, torch.int32, 2 * n, "excl", dev)
         occ = out if out is not None else torch.empty(n, dtype=torch.uint8, device=rays.device)
+        _require_cuda(occ, torch.uint8, n, "out", dev)
         st = lib().cav_trace_any(self.ctx.handle, self.handle, _ptr(rays), _ptr(limit), _ptr(excl), n, _ptr(occ),
                                  int(flags), _stream_ptr(stream))
         self.ctx._check(st, "cav_trace_any")
