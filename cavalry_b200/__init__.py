@@ -168,6 +168,27 @@ def _require_cuda(x, dtype, numel: int, name: str, device_index: int) -> None:
         raise ValueError(f"{name}: {x.numel()} elements, at least {numel} needed")
 
 
+def _require_host(x, dtype, numel: int, name: str) -> None:
+    """Raise ValueError unless `x` is a C-contiguous numpy array or CPU torch tensor of numpy
+    `dtype` with at least `numel` elements: the host-buffer entry points copy that many
+    elements through the raw pointer (a CUDA tensor's pointer is not host memory)."""
+    if isinstance(x, np.ndarray):
+        ok_dtype, contiguous, size = x.dtype == np.dtype(dtype), x.flags["C_CONTIGUOUS"], x.size
+    else:
+        if getattr(x, "is_cuda", True):
+            raise ValueError(f"{name}: expected a numpy array or a CPU tensor")
+        import torch
+
+        ok_dtype = x.dtype == torch.from_numpy(np.empty(0, dtype)).dtype
+        contiguous, size = x.is_contiguous(), x.numel()
+    if not ok_dtype:
+        raise ValueError(f"{name}: expected dtype {np.dtype(dtype)}, got {x.dtype}")
+    if not contiguous:
+        raise ValueError(f"{name}: expected a contiguous array")
+    if size < numel:
+        raise ValueError(f"{name}: {size} elements, at least {numel} needed")
+
+
 def _stream_ptr(stream) -> int | None:
     import torch
 
@@ -258,8 +279,11 @@ class Context:
 
         assert positions.is_cuda and positions.dtype == torch.float32 and positions.is_contiguous()
         assert indices.is_cuda and indices.dtype == torch.int32 and indices.is_contiguous()
+        _require_cuda(positions, torch.float32, 0, "positions", self.device)  # counts: the library checks
+        _require_cuda(indices, torch.int32, 0, "indices", self.device)
         if mesh_ids is not None:
             assert mesh_ids.is_cuda and mesh_ids.dtype == torch.int32 and mesh_ids.is_contiguous()
+            _require_cuda(mesh_ids, torch.int32, indices.numel() // 3, "mesh_ids", self.device)
         nb = None
         if scene_bounds is not None:
             nb = np.ascontiguousarray(np.asarray(scene_bounds, dtype=np.float32).reshape(6))
@@ -878,12 +902,18 @@ class Bvh:
     def trace_closest_host(self, rays: np.ndarray, flags: int = TRACE_EXACT, out=None):
         """Host-buffer variant (numpy in and out; pinned torch CPU tensors also accepted)."""
         n = rays.shape[0]
+        _require_host(rays, np.float32, 8 * n, "rays")
         if out is None:
             prim = np.empty(n, np.int32)
             t = np.empty(n, np.float32)
             uv = np.empty((n, 2), np.float32)
         else:
             prim, t, uv = out
+            _require_host(prim, np.int32, n, "out prim")
+            if t is not None:
+                _require_host(t, np.float32, n, "out t")
+            if uv is not None:
+                _require_host(uv, np.float32, 2 * n, "out uv")
         st = lib().cav_trace_closest_host(self.ctx.handle, self.handle, _ptr(rays), n, _ptr(prim), _ptr(t), _ptr(uv),
                                           int(flags))
         self.ctx._check(st, "cav_trace_closest_host")
@@ -891,7 +921,13 @@ class Bvh:
 
     def trace_any_host(self, rays, limit=None, excl=None, flags: int = TRACE_EXACT, out=None):
         n = rays.shape[0]
+        _require_host(rays, np.float32, 8 * n, "rays")
+        if limit is not None:
+            _require_host(limit, np.float32, n, "limit")
+        if excl is not None:
+            _require_host(excl, np.int32, 2 * n, "excl")
         occ = out if out is not None else np.empty(n, np.uint8)
+        _require_host(occ, np.uint8, n, "out")
         st = lib().cav_trace_any_host(self.ctx.handle, self.handle, _ptr(rays), _ptr(limit), _ptr(excl), n, _ptr(occ),
                                       int(flags))
         self.ctx._check(st, "cav_trace_any_host")

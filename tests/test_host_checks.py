@@ -108,3 +108,45 @@ def test_rays_on_another_gpu_are_refused(bvh):
     with pytest.raises(ValueError, match="cuda:3"):
         bvh.autotune(FakeCuda((64, 8), torch.float32, device=3))
     assert bvh.fake.calls == []
+
+
+def test_host_buffer_variants_check_their_arrays(bvh):
+    n = 50
+    rays = np.zeros((n, 8), np.float32)
+    bvh.trace_closest_host(rays)
+    bvh.trace_closest_host(torch.zeros((n, 8)), out=(torch.zeros(n, dtype=torch.int32), None, None))
+    bvh.trace_any_host(rays, np.ones(n, np.float32), np.zeros((n, 2), np.int32))
+    assert bvh.fake.calls == ["cav_trace_closest_host"] * 2 + ["cav_trace_any_host"]
+    bad = [
+        lambda: bvh.trace_closest_host(rays.astype(np.float64)),
+        lambda: bvh.trace_closest_host(np.asfortranarray(np.zeros((n, 8), np.float32))),
+        lambda: bvh.trace_closest_host(rays, out=(np.zeros(n - 1, np.int32), None, None)),
+        lambda: bvh.trace_closest_host(rays, out=(np.zeros(n, np.int32), None, np.zeros((n, 1), np.float32))),
+        lambda: bvh.trace_closest_host(FakeCuda((n, 8), torch.float32)),
+        lambda: bvh.trace_any_host(rays, np.ones(n, np.float64)),
+        lambda: bvh.trace_any_host(rays, None, np.zeros((n, 2), np.int64)),
+        lambda: bvh.trace_any_host(rays, out=np.zeros(n - 1, np.uint8)),
+    ]
+    for call in bad:
+        with pytest.raises(ValueError):
+            call()
+    assert len(bvh.fake.calls) == 3
+
+
+def test_build_checks_devices_and_mesh_ids(monkeypatch):
+    fake = FakeLib()
+    monkeypatch.setattr(cav, "lib", lambda: fake)
+    monkeypatch.setattr(cav, "_stream_ptr", lambda stream: None)
+    ctx = object.__new__(cav.Context)
+    ctx.device, ctx.handle = 0, None
+    monkeypatch.setattr(ctx, "_check", lambda st, what: None, raising=False)
+    pos, idx = FakeCuda((10, 3), torch.float32), FakeCuda((4, 3), torch.int32)
+    ctx.build(pos, idx, mesh_ids=FakeCuda((4,), torch.int32))
+    assert fake.calls == ["cav_bvh_build"]
+    with pytest.raises(ValueError, match="mesh_ids"):
+        ctx.build(pos, idx, mesh_ids=FakeCuda((3,), torch.int32))
+    with pytest.raises(ValueError, match="cuda:1"):
+        ctx.build(FakeCuda((10, 3), torch.float32, device=1), idx)
+    # the triangle and vertex counts stay the library's to check (it returns its own status)
+    ctx.build(FakeCuda((3, 3), torch.float32), FakeCuda((1, 3), torch.int32))
+    assert fake.calls == ["cav_bvh_build"] * 2
