@@ -582,9 +582,15 @@ class Server:
 
     def submit_rays(self, bvh: "Bvh", rays: np.ndarray, any_hit: bool = False, limit=None, excl=None):
         rays = np.ascontiguousarray(rays, np.float32)
+        if rays.ndim != 2 or rays.shape[1] != 8:
+            raise ValueError(f"rays: expected an [n, 8] array, got shape {rays.shape}")
         n = rays.shape[0]
         lim = None if limit is None else np.ascontiguousarray(limit, np.float32)
         ex = None if excl is None else np.ascontiguousarray(excl, np.int32)
+        if lim is not None:
+            _require_host(lim, np.float32, n, "limit")
+        if ex is not None:
+            _require_host(ex, np.int32, 2 * n, "excl")
         job = ctypes.c_int64(0)
         if any_hit:
             out = (np.zeros(n, np.uint8),)
@@ -618,9 +624,15 @@ class Server:
                           bvh_rounds: int = -1):
         """A ray-query job against its own scene's tree: returns (job id, *outputs) as submit_rays."""
         rays = np.ascontiguousarray(rays, np.float32)
+        if rays.ndim != 2 or rays.shape[1] != 8:
+            raise ValueError(f"rays: expected an [n, 8] array, got shape {rays.shape}")
         n = rays.shape[0]
         lim = None if limit is None else np.ascontiguousarray(limit, np.float32)
         ex = None if excl is None else np.ascontiguousarray(excl, np.int32)
+        if lim is not None:
+            _require_host(lim, np.float32, n, "limit")
+        if ex is not None:
+            _require_host(ex, np.int32, 2 * n, "excl")
         if any_hit:
             out = (np.zeros(n, np.uint8),)
             spec = SceneJob(pbrt_path.encode(), SCENE_ANY, bvh_rounds, RenderOpts(), None, None, rays.ctypes.data,

@@ -150,3 +150,24 @@ def test_build_checks_devices_and_mesh_ids(monkeypatch):
     # the triangle and vertex counts stay the library's to check (it returns its own status)
     ctx.build(FakeCuda((3, 3), torch.float32), FakeCuda((1, 3), torch.int32))
     assert fake.calls == ["cav_bvh_build"] * 2
+
+
+def test_server_ray_jobs_check_shapes(monkeypatch):
+    fake = FakeLib()
+    monkeypatch.setattr(cav, "lib", lambda: fake)
+    sv = object.__new__(cav.Server)
+    sv.handle, sv.ctx, sv._keep = 1, FakeCtx(), {}
+    try:
+        bvh = cav.Bvh(FakeCtx(), 2, 10, owned=False)
+        rays = np.zeros((20, 8), np.float32)
+        sv.submit_rays(bvh, rays, any_hit=True, limit=np.ones(20))
+        sv.submit_scene_rays("x.pbrt", rays)
+        assert fake.calls == ["cav_server_submit_rays", "cav_server_submit_scene"]
+        for call in (lambda: sv.submit_rays(bvh, np.zeros((20, 6), np.float32)),
+                     lambda: sv.submit_rays(bvh, rays, any_hit=True, limit=np.ones(19)),
+                     lambda: sv.submit_scene_rays("x.pbrt", rays, any_hit=True, excl=np.zeros((20, 1), np.int32))):
+            with pytest.raises(ValueError):
+                call()
+        assert len(fake.calls) == 2
+    finally:
+        sv.handle = None  # the stand-in handle must never reach the real library's destroy
